@@ -1,0 +1,1195 @@
+// engine.cu — host side of the multislice engine and the C ABI of include/mslice.h.
+//
+// The simulation object mirrors clTEM's SimulationGeneral / SimulationStem / SimulationCbed /
+// SimulationCtem state (src/simulation/microscope/*.cpp): geometry derived from the config as
+// SimulationManager / SimulationCell do, binned atoms, the band-limited transmission function of every
+// slice, and a batch of waves that the fused row / column passes (passes.cuh) step through the slices.
+#include "../../include/mslice.h"
+#include "launch.cuh"
+#include "misc.cuh"
+#include "plain.h"
+#include "potential.cuh"
+#include "potential_launch.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace ms {
+
+static thread_local std::string g_last_error;
+
+struct ArgError : std::runtime_error { using std::runtime_error::runtime_error; };
+struct StateError : std::runtime_error { using std::runtime_error::runtime_error; };
+struct OomError : std::runtime_error { using std::runtime_error::runtime_error; };
+struct Cancelled : std::runtime_error { using std::runtime_error::runtime_error; };
+struct Unsupported : std::runtime_error { using std::runtime_error::runtime_error; };
+
+// ------------------------------------------------------------------------------------------------
+// Geometry (host): SimulationArea / SimulationCell / SimulationManager / MicroscopeParameters
+// ------------------------------------------------------------------------------------------------
+static const double kPi = M_PI;
+
+static double wavelength_of(double V) {   // commonstructs.h:269-271
+    const double h = 6.6262e-034, c = 299792458.0, e = 1.6021773e-019, m = 9.10938291e-031;
+    return h * c / std::sqrt(e * (V * 1000) * (2 * m * c * c + e * (V * 1000))) * 1e+10;
+}
+static double sigma_of(double V) {   // commonstructs.h:278-280
+    const double c = 299792458.0, e = 1.6021773e-019, m = 9.10938291e-031;
+    return (2 * kPi / (wavelength_of(V) * (V * 1000))) * (m * c * c + e * (V * 1000)) / (2 * m * c * c + e * (V * 1000));
+}
+
+static bool valid_resolution(const mslice_config &c) {
+    int r = c.resolution;
+    if (c.allow_any_resolution) {
+        int m = r % 3 == 0 ? r / 3 : r;
+        return r >= 64 && (m & (m - 1)) == 0;
+    }
+    return r == 256 || r == 512 || r == 768 || r == 1024 || r == 1536 || r == 2048 || r == 3072 || r == 4096 || r == 8192;
+}
+
+static void corrected_limits(double xs, double xf, double ys, double yf, double pad, double *x, double *y) {
+    // SimulationArea::getCorrectedLimitsX/Y (commonstructs.cpp:33-59)
+    double range_x = xf - xs, range_y = yf - ys;
+    double range_total = std::max(range_x, range_y) + pad;
+    double x_diff = (range_total - range_x) / 2, y_diff = (range_total - range_y) / 2;
+    x[0] = xs - x_diff; x[1] = xf + x_diff;
+    y[0] = ys - y_diff; y[1] = yf + y_diff;
+}
+
+struct HostGeom {
+    mslice_geometry g;
+    std::vector<double> kx, ky;
+};
+
+static void compute_geometry(const mslice_config &c, HostGeom &H) {
+    if (c.mode != MSLICE_MODE_CTEM && c.mode != MSLICE_MODE_STEM && c.mode != MSLICE_MODE_CBED)
+        throw ArgError("unknown simulation mode " + std::to_string(c.mode));
+    if (!valid_resolution(c)) throw ArgError("invalid resolution " + std::to_string(c.resolution));
+    if (!(c.slice_thickness > 0)) throw ArgError("slice thickness must be positive");
+    if (!(c.voltage > 0)) throw ArgError("voltage must be positive");
+    if (c.full3d && c.full3d_integrals < 1) throw ArgError("full 3d integrals must be >= 1");
+    if (c.n_detectors < 0 || c.n_detectors > MSLICE_MAX_DETECTORS) throw ArgError("too many detectors");
+    if (c.mode == MSLICE_MODE_STEM && (c.stem_pixels_x < 1 || c.stem_pixels_y < 1)) throw ArgError("STEM scan needs pixels");
+    mslice_geometry &g = H.g;
+    std::memset(&g, 0, sizeof(g));
+    double fx[2], fy[2];
+    if (c.mode == MSLICE_MODE_STEM)
+        corrected_limits(c.stem_area[0], c.stem_area[1], c.stem_area[2], c.stem_area[3], c.stem_padding, fx, fy);
+    else if (c.mode == MSLICE_MODE_CBED)
+        corrected_limits(c.cbed_x, c.cbed_x, c.cbed_y, c.cbed_y, c.cbed_padding, fx, fy);
+    else
+        corrected_limits(c.ctem_area[0], c.ctem_area[1], c.ctem_area[2], c.ctem_area[3], 0.0, fx, fy);
+    // + SimulationCell padding (paddedFullLimitsX/Y, simulationmanager.cpp:446-452)
+    fx[0] += -c.padding_xy; fx[1] += c.padding_xy;
+    fy[0] += -c.padding_xy; fy[1] += c.padding_xy;
+    g.full_x[0] = g.sim_x[0] = fx[0]; g.full_x[1] = g.sim_x[1] = fx[1];
+    g.full_y[0] = g.sim_y[0] = fy[0]; g.full_y[1] = g.sim_y[1] = fy[1];
+
+    // SimulationCell::roundPaddingZ (simulationcell.cpp:43-61) and sliceCount (:75-83)
+    const double dz = c.slice_thickness, off = c.slice_offset;
+    int pad_slices_pre = (int)std::ceil((std::abs(c.padding_z) - off) / dz);
+    double pre_pad = off + pad_slices_pre * dz;
+    double zw = c.struct_limits[5] - c.struct_limits[4];
+    int struct_slices = (int)std::ceil((zw + off) / dz);
+    double left_over = struct_slices * dz - off - zw;
+    int pad_slices_post = (int)std::ceil((std::abs(-c.padding_z) - left_over) / dz);
+    double post_pad = pad_slices_post * dz + left_over;
+    g.padding_z[0] = -post_pad; g.padding_z[1] = pre_pad;
+    g.z_lims[0] = c.struct_limits[4] + g.padding_z[0];
+    g.z_lims[1] = c.struct_limits[5] + g.padding_z[1];
+    unsigned int ns = (unsigned int)std::ceil(((g.z_lims[1] - g.z_lims[0]) / dz) - 0.000001);
+    ns += (ns == 0);
+    g.n_slices = (int)ns;
+    g.pre_slices = (int)(unsigned int)(g.padding_z[1] / dz);
+    g.dz = dz;
+
+    const int res = c.resolution;
+    double x_r = g.sim_x[1] - g.sim_x[0], y_r = g.sim_y[1] - g.sim_y[0];
+    g.real_scale = std::max(x_r, y_r) / res;                 // simulationmanager.cpp:211-222
+    g.inverse_scale = 1.0 / (g.real_scale * res);            // :224-230
+    g.wavelength = wavelength_of(c.voltage);
+    g.wavenumber = 1.0 / g.wavelength;
+    g.angle_scale = 1000.0 * g.inverse_scale * g.wavelength;  // :241-247
+    const double k = g.wavenumber;
+    g.wavevector[0] = k * std::sin(c.beam_tilt / 1000.0) * std::cos(c.beam_azimuth);
+    g.wavevector[1] = k * std::sin(c.beam_tilt / 1000.0) * std::sin(c.beam_azimuth);
+    g.wavevector[2] = k * std::cos(c.beam_tilt / 1000.0);
+    g.sigma = sigma_of(c.voltage) * g.wavenumber / g.wavevector[2];   // simulationgeneral.cpp:418
+
+    double xr = g.full_x[1] - g.full_x[0], yr = g.full_y[1] - g.full_y[0];
+    int nb = (int)std::ceil(std::max(xr, yr) / 8.0);            // calculateBlocks :393-408
+    if (nb < 1) throw ArgError("empty simulation area");
+    g.blocks_x = g.blocks_y = nb;
+    g.block_scale_x = xr / nb; g.block_scale_y = yr / nb;
+    g.load_blocks_x = (int)std::ceil(8.0 / g.block_scale_x);    // simulationgeneral.cpp:517-521
+    g.load_blocks_y = (int)std::ceil(8.0 / g.block_scale_y);
+    g.load_blocks_z = (int)std::ceil(3.0 / dz);
+
+    // k tables + bandwidth k_max (simulationgeneral.cpp:427-455)
+    const double L = g.real_scale * res;
+    H.kx.resize(res); H.ky.resize(res);
+    unsigned int imid = (unsigned int)std::floor(static_cast<double>(res) / 2.0 + 0.5);
+    for (int i = 0; i < res; i++) H.kx[i] = H.ky[i] = (i >= (int)imid) ? double(i - res) / L : i / L;
+    g.k_max = std::min(std::abs(H.ky[imid]), std::abs(H.kx[imid]));
+
+    double rx0, rx1, ry0, ry1;   // raw limits of the mode's area (imageCrop, :410-428)
+    if (c.mode == MSLICE_MODE_STEM) { rx0 = c.stem_area[0]; rx1 = c.stem_area[1]; ry0 = c.stem_area[2]; ry1 = c.stem_area[3]; }
+    else if (c.mode == MSLICE_MODE_CBED) { rx0 = rx1 = c.cbed_x; ry0 = ry1 = c.cbed_y; }
+    else { rx0 = c.ctem_area[0]; rx1 = c.ctem_area[1]; ry0 = c.ctem_area[2]; ry1 = c.ctem_area[3]; }
+    double crop_lr = (std::floor(x_r - (rx1 - rx0)) / g.real_scale);
+    double crop_tb = (std::floor(y_r - (ry1 - ry0)) / g.real_scale);
+    unsigned int cl = (unsigned int)std::floor(crop_lr / 2.0), cb = (unsigned int)std::floor(crop_tb / 2.0);
+    g.crop[0] = (unsigned int)(crop_tb - cb); g.crop[1] = cl; g.crop[2] = cb; g.crop[3] = (unsigned int)(crop_lr - cl);
+    g.n_outputs = c.intermediate_slices > 0 ? (int)std::ceil((float)g.n_slices / c.intermediate_slices) : 1;
+}
+
+// output slices: (s+1) % step == 0, then the exit if the count is not reached (simulationstem.cpp:237-275)
+static std::vector<int> output_slices(const mslice_config &c, const mslice_geometry &g) {
+    std::vector<int> o;
+    if (c.intermediate_slices > 0)
+        for (int s = 0; s < g.n_slices; s++)
+            if ((s + 1) % c.intermediate_slices == 0) o.push_back(s);
+    if ((int)o.size() < g.n_outputs) o.push_back(g.n_slices - 1);
+    return o;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Context
+// ------------------------------------------------------------------------------------------------
+struct Params {
+    int form = -1, i_count = 0;
+    std::vector<double> values;
+    int max_z = 0;
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    size_t mem_limit = 0, mem_used = 0;
+    unsigned long long launches = 0;
+    Params params;
+    double *prm_d = nullptr;
+    float *prm_f = nullptr;
+    size_t prm_n = 0;
+    std::map<int, void *> tw_f, tw_d;   // twiddle tables per size
+    std::mutex mtx;
+
+    void *alloc(size_t bytes) {
+        if (bytes == 0) return nullptr;
+        if (mem_limit && mem_used + bytes > mem_limit) throw OomError("device memory limit of the context exceeded");
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); throw OomError("cudaMalloc of " + std::to_string(bytes) + " bytes failed"); }
+        MS_CUDA(e);
+        mem_used += bytes;
+        return p;
+    }
+    void release(void *p, size_t bytes) {
+        if (!p) return;
+        cudaFree(p);
+        mem_used -= std::min(mem_used, bytes);
+    }
+    template <class R> const cplx<R> *twiddles(int n) {
+        auto &m = sizeof(R) == 4 ? tw_f : tw_d;
+        auto it = m.find(n);
+        if (it != m.end()) return (const cplx<R> *)it->second;
+        std::vector<cplx<R>> h(n);
+        for (int i = 0; i < n; i++) {
+            long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)i / (long double)n;
+            h[i] = mk<R>((R)std::cos(a), (R)std::sin(a));
+        }
+        void *d = alloc(sizeof(cplx<R>) * n);
+        MS_CUDA(cudaMemcpy(d, h.data(), sizeof(cplx<R>) * n, cudaMemcpyHostToDevice));
+        m[n] = d;
+        return (const cplx<R> *)d;
+    }
+    ~Ctx() {
+        cudaSetDevice(device);
+        for (auto &kv : tw_f) cudaFree(kv.second);
+        for (auto &kv : tw_d) cudaFree(kv.second);
+        cudaFree(prm_d);
+        cudaFree(prm_f);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+template <class T> struct DevBuf {
+    Ctx *ctx = nullptr;
+    T *p = nullptr;
+    size_t n = 0;
+    void ensure(Ctx *c, size_t count) {
+        if (count <= n && p) return;
+        free();
+        ctx = c;
+        p = (T *)c->alloc(sizeof(T) * std::max<size_t>(count, 1));
+        n = std::max<size_t>(count, 1);
+    }
+    void free() {
+        if (p && ctx) ctx->release(p, sizeof(T) * n);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { free(); }
+};
+
+// ------------------------------------------------------------------------------------------------
+// Simulation
+// ------------------------------------------------------------------------------------------------
+struct SimBase {
+    Ctx *ctx;
+    mslice_config cfg;
+    HostGeom H;
+    std::atomic<bool> cancel{false};
+    mslice_progress_cb progress = nullptr;
+    void *progress_user = nullptr;
+    double timing[3] = {0, 0, 0};
+    virtual ~SimBase() = default;
+    virtual void set_atoms(const int *Z, const double *x, const double *y, const double *z, size_t n, bool host) = 0;
+    virtual void get_sorted(int *Z, double *x, double *y, double *z, size_t cap, int *bs, size_t cap_bs, int *bid, int *zid,
+                            size_t *n_out) = 0;
+    virtual void build_transmission() = 0;
+    virtual void get_transmission(int slice, int band_limited, double *out) = 0;
+    virtual void get_propagator(double *out) = 0;
+    virtual void get_probe(double x, double y, double *out) = 0;
+    virtual void stem_run(const int *pixels, size_t n, double *out) = 0;
+    virtual void cbed_run(double *diff) = 0;
+    virtual void ctem_run(double *ew, double *diff, double *image) = 0;
+    virtual void stage(int n_configs, const size_t *counts, const int *Z, const double *x, const double *y, const double *z) = 0;
+    virtual void run_staged(int mode) = 0;
+    virtual void staged_result(double *out, size_t cap) = 0;
+    virtual void stem_plain(const int *pixels, size_t n, double *out) = 0;
+};
+
+template <class R>
+struct Sim : SimBase {
+    using C = cplx<R>;
+    int N = 0;
+    size_t NN = 0;
+    PassOps<R> ops;
+    double s2d = 0;   // clFFT scale 1/sqrtf(N*N)
+
+    // tables
+    DevBuf<double> kx, ky, kx2, ky2;
+    DevBuf<C> px, py;
+    DevBuf<double2> chi;
+    DevBuf<uint16_t> detmask;
+    double k_prop = 0;   // k_max * limit factor of the propagator cut
+    // atoms
+    size_t n_atoms = 0, atom_cap = 0;
+    bool atoms_set = false, trans_built = false;
+    DevBuf<int> aZ, aZs, keys_in, keys_out, idx_in, idx_out, bid, zid, kept, counts, block_start;
+    DevBuf<double> ax, ay, az, axs, ays, azs;
+    DevBuf<unsigned char> cub_temp;
+    size_t cub_bytes = 0;
+    // transmission
+    DevBuf<C> trans;
+    // waves
+    int batch_cap = 0;
+    DevBuf<C> wave, recip, tmp;
+    DevBuf<double> partials;
+    DevBuf<int> pix;
+    DevBuf<double2> pos;
+    std::vector<int> h_pix;
+    std::vector<double2> h_pos;
+    // staged configurations and accumulators
+    int n_configs = 0;
+    std::vector<size_t> cfg_counts, cfg_offsets;
+    DevBuf<int> sZ;
+    DevBuf<double> sx, sy, sz;
+    DevBuf<double> acc, comp;
+    size_t acc_n = 0;
+    int acc_configs = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    cudaStream_t st() const { return ctx->stream; }
+
+    Sim(Ctx *c, const mslice_config &cf) {
+        ctx = c;
+        cfg = cf;
+        compute_geometry(cfg, H);
+        N = cfg.resolution;
+        NN = (size_t)N * N;
+        ops = pass_ops<R>(N);
+        s2d = (double)(1.0f / sqrtf((float)((size_t)N * N)));
+        if (ctx->params.form < 0) throw StateError("no parameterisation loaded (mslice_params_load)");
+        if (cfg.full3d && ctx->params.form < 0) throw StateError("no parameterisation loaded");
+        const mslice_geometry &g = H.g;
+        // k tables
+        std::vector<double> hx2(N), hy2(N);
+        for (int i = 0; i < N; i++) { hx2[i] = H.kx[i] * H.kx[i]; hy2[i] = H.ky[i] * H.ky[i]; }
+        kx.ensure(ctx, N); ky.ensure(ctx, N); kx2.ensure(ctx, N); ky2.ensure(ctx, N);
+        MS_CUDA(cudaMemcpyAsync(kx.p, H.kx.data(), N * sizeof(double), cudaMemcpyHostToDevice, st()));
+        MS_CUDA(cudaMemcpyAsync(ky.p, H.ky.data(), N * sizeof(double), cudaMemcpyHostToDevice, st()));
+        MS_CUDA(cudaMemcpyAsync(kx2.p, hx2.data(), N * sizeof(double), cudaMemcpyHostToDevice, st()));
+        MS_CUDA(cudaMemcpyAsync(ky2.p, hy2.data(), N * sizeof(double), cudaMemcpyHostToDevice, st()));
+        // separable propagator (propagator_d.cl:18-52): phase pi dz s, s = (k^2 - kz^2 - (kx+bx)^2 - (ky+by)^2)/kz
+        k_prop = g.k_max * cfg.inverse_limit_factor;
+        {
+            const double bk = g.wavenumber, bx = g.wavevector[0], by = g.wavevector[1], bz = g.wavevector[2];
+            const double f = bz / bk;
+            const double c0 = kPi * g.dz * (bk * bk - bz * bz) / bz;
+            std::vector<C> hpx(N), hpy(N);
+            for (int i = 0; i < N; i++) {
+                double ax_ = -kPi * g.dz * (bx + H.kx[i]) * (bx + H.kx[i]) / bz + c0;
+                double ay_ = -kPi * g.dz * (by + H.ky[i]) * (by + H.ky[i]) / bz;
+                hpx[i] = mk<R>((R)(f * std::cos(ax_)), (R)(f * std::sin(ax_)));
+                hpy[i] = mk<R>((R)std::cos(ay_), (R)std::sin(ay_));
+            }
+            px.ensure(ctx, N); py.ensure(ctx, N);
+            MS_CUDA(cudaMemcpyAsync(px.p, hpx.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
+            MS_CUDA(cudaMemcpyAsync(py.p, hpy.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
+            MS_CUDA(cudaStreamSynchronize(st()));
+        }
+        // probe aberration table
+        chi.ensure(ctx, NN);
+        chi_table(st(), N, kx.p, ky.p, g.wavelength, aberr(cfg.C10), cfg.cond_ap, cfg.cond_ap_smooth, chi.p);
+        ctx->launches++;
+        // detectors (getStemPixel, simulationstem.cpp:105-109)
+        detmask.ensure(ctx, NN);
+        double in[16] = {}, out[16] = {}, xc[16] = {}, yc[16] = {};
+        for (int d = 0; d < cfg.n_detectors; d++) {
+            in[d] = cfg.detectors[d].inner / g.angle_scale;
+            out[d] = cfg.detectors[d].outer / g.angle_scale;
+            xc[d] = cfg.detectors[d].xcentre / g.angle_scale;
+            yc[d] = cfg.detectors[d].ycentre / g.angle_scale;
+        }
+        detector_masks(st(), N, cfg.n_detectors, in, out, xc, yc, detmask.p);
+        ctx->launches++;
+        trans.ensure(ctx, (size_t)g.n_slices * NN);
+        for (int i = 0; i < 4; i++) MS_CUDA(cudaEventCreate(&ev[i]));
+        MS_CUDA(cudaStreamSynchronize(st()));
+    }
+    ~Sim() override {
+        for (auto e : ev) if (e) cudaEventDestroy(e);
+    }
+
+    AberrD aberr(double c10) const {
+        auto cx = [](mslice_aberration a) { return make_double2(a.mag * std::cos(a.ang), a.mag * std::sin(a.ang)); };
+        AberrD A;
+        A.C10 = c10; A.C30 = cfg.C30; A.C50 = cfg.C50;
+        A.C12 = cx(cfg.C12); A.C21 = cx(cfg.C21); A.C23 = cx(cfg.C23); A.C32 = cx(cfg.C32); A.C34 = cx(cfg.C34);
+        A.C41 = cx(cfg.C41); A.C43 = cx(cfg.C43); A.C45 = cx(cfg.C45); A.C52 = cx(cfg.C52); A.C54 = cx(cfg.C54);
+        A.C56 = cx(cfg.C56);
+        return A;
+    }
+
+    const R *params_dev() {
+        if constexpr (sizeof(R) == 8) return ctx->prm_d;
+        else return ctx->prm_f;
+    }
+
+    SortGeom sort_geom() const {
+        const mslice_geometry &g = H.g;
+        SortGeom s;
+        s.full_x0 = g.full_x[0]; s.full_x1 = g.full_x[1]; s.full_y0 = g.full_y[0]; s.full_y1 = g.full_y[1];
+        s.z0 = g.z_lims[0]; s.z1 = g.z_lims[1]; s.dz = g.dz;
+        s.blocks_x = g.blocks_x; s.blocks_y = g.blocks_y; s.n_slices = g.n_slices;
+        return s;
+    }
+
+    void ensure_atom_capacity(size_t n) {
+        const mslice_geometry &g = H.g;
+        const int n_bins = g.n_slices * g.blocks_x * g.blocks_y;
+        if (n > (size_t)0x7fffffff) throw ArgError("too many atoms");
+        if (n > atom_cap || atom_cap == 0) {
+            size_t cap = std::max<size_t>(n, 1);
+            aZ.ensure(ctx, cap); ax.ensure(ctx, cap); ay.ensure(ctx, cap); az.ensure(ctx, cap);
+            aZs.ensure(ctx, cap); axs.ensure(ctx, cap); ays.ensure(ctx, cap); azs.ensure(ctx, cap);
+            keys_in.ensure(ctx, cap); keys_out.ensure(ctx, cap); idx_in.ensure(ctx, cap); idx_out.ensure(ctx, cap);
+            bid.ensure(ctx, cap); zid.ensure(ctx, cap); kept.ensure(ctx, cap);
+            cub_bytes = atom_sort_temp_bytes((int)cap, n_bins);
+            cub_temp.ensure(ctx, cub_bytes);
+            atom_cap = cap;
+        }
+        counts.ensure(ctx, (size_t)n_bins + 1);
+        block_start.ensure(ctx, (size_t)n_bins + 1);
+    }
+
+    void check_Z(const int *Z, size_t n) const {
+        int maxz = ctx->params.max_z;
+        for (size_t i = 0; i < n; i++)
+            if (Z[i] < 1 || Z[i] > maxz)
+                throw ArgError("atomic number " + std::to_string(Z[i]) + " not covered by the loaded parameterisation");
+    }
+
+    // device-resident atom arrays (already in ax/ay/az/aZ or given device pointers) -> sorted + bins
+    void sort_device(const int *Z, const double *x, const double *y, const double *z, size_t n) {
+        AtomSortBuffers b{keys_in.p, keys_out.p, idx_in.p, idx_out.p, bid.p, zid.p, kept.p, counts.p, cub_temp.p, cub_bytes};
+        atom_sort(st(), sort_geom(), (int)n, Z, x, y, z, b, block_start.p, aZs.p, axs.p, ays.p, azs.p);
+        ctx->launches += 5;
+        n_atoms = n;
+        atoms_set = true;
+        trans_built = false;
+    }
+
+    void set_atoms(const int *Z, const double *x, const double *y, const double *z, size_t n, bool host) override {
+        if (host) check_Z(Z, n);
+        ensure_atom_capacity(n);
+        if (host) {
+            if (n) {
+                MS_CUDA(cudaMemcpyAsync(aZ.p, Z, n * sizeof(int), cudaMemcpyHostToDevice, st()));
+                MS_CUDA(cudaMemcpyAsync(ax.p, x, n * sizeof(double), cudaMemcpyHostToDevice, st()));
+                MS_CUDA(cudaMemcpyAsync(ay.p, y, n * sizeof(double), cudaMemcpyHostToDevice, st()));
+                MS_CUDA(cudaMemcpyAsync(az.p, z, n * sizeof(double), cudaMemcpyHostToDevice, st()));
+            }
+            sort_device(aZ.p, ax.p, ay.p, az.p, n);
+        } else {
+            sort_device(Z, x, y, z, n);
+        }
+    }
+
+    void get_sorted(int *Z, double *x, double *y, double *z, size_t cap, int *bs, size_t cap_bs, int *bido, int *zido,
+                    size_t *n_out) override {
+        if (!atoms_set) throw StateError("atoms not set");
+        const mslice_geometry &g = H.g;
+        const size_t nbins = (size_t)g.n_slices * g.blocks_x * g.blocks_y + 1;
+        if (cap_bs < nbins) throw ArgError("block_start capacity too small");
+        std::vector<int> hkept(n_atoms), hbid(n_atoms), hzid(n_atoms), hbs(nbins);
+        MS_CUDA(cudaStreamSynchronize(st()));
+        if (n_atoms) {
+            MS_CUDA(cudaMemcpy(hkept.data(), kept.p, n_atoms * sizeof(int), cudaMemcpyDeviceToHost));
+            MS_CUDA(cudaMemcpy(hbid.data(), bid.p, n_atoms * sizeof(int), cudaMemcpyDeviceToHost));
+            MS_CUDA(cudaMemcpy(hzid.data(), zid.p, n_atoms * sizeof(int), cudaMemcpyDeviceToHost));
+        }
+        MS_CUDA(cudaMemcpy(hbs.data(), block_start.p, nbins * sizeof(int), cudaMemcpyDeviceToHost));
+        size_t nf = 0;
+        for (size_t i = 0; i < n_atoms; i++) nf += hkept[i] ? 1 : 0;
+        if (nf > cap) throw ArgError("atom capacity too small");
+        size_t nin = (size_t)hbs[nbins - 1];
+        if (nin) {
+            MS_CUDA(cudaMemcpy(Z, aZs.p, nin * sizeof(int), cudaMemcpyDeviceToHost));
+            MS_CUDA(cudaMemcpy(x, axs.p, nin * sizeof(double), cudaMemcpyDeviceToHost));
+            MS_CUDA(cudaMemcpy(y, ays.p, nin * sizeof(double), cudaMemcpyDeviceToHost));
+            MS_CUDA(cudaMemcpy(z, azs.p, nin * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+        std::copy(hbs.begin(), hbs.end(), bs);
+        size_t k = 0;
+        for (size_t i = 0; i < n_atoms; i++)
+            if (hkept[i]) {
+                if (bido) bido[k] = hbid[i];
+                if (zido) zido[k] = hzid[i];
+                k++;
+            }
+        *n_out = nf;
+    }
+
+    PotParams pot_params(int slice0) const {
+        const mslice_geometry &g = H.g;
+        PotParams p;
+        p.width = N; p.height = N; p.total_slices = g.n_slices; p.slice0 = slice0;
+        p.dz = g.dz; p.pixelscale = g.real_scale;
+        p.blocks_x = g.blocks_x; p.blocks_y = g.blocks_y;
+        p.max_x = g.full_x[1]; p.min_x = g.full_x[0]; p.max_y = g.full_y[1]; p.min_y = g.full_y[0];
+        p.load_x = g.load_blocks_x; p.load_y = g.load_blocks_y; p.load_z = g.load_blocks_z;
+        p.sigma = g.sigma; p.startx = g.sim_x[0]; p.starty = g.sim_y[0];
+        p.beam_theta_mrad = cfg.beam_tilt; p.beam_phi = cfg.beam_azimuth;
+        p.z0 = g.z_lims[0];
+        p.integrals = cfg.full3d_integrals > 0 ? cfg.full3d_integrals : 1;
+        p.shift_x = (g.wavevector[0] / g.wavevector[2]) * g.dz / p.integrals;   // simulationgeneral.cpp:562-563
+        p.shift_y = (g.wavevector[1] / g.wavevector[2]) * g.dz / p.integrals;
+        p.form = ctx->params.form; p.i_count = ctx->params.i_count;
+        return p;
+    }
+
+    void potentials(C *out, int slice0, int count) {
+        launch_potential<R>(st(), cfg.full3d != 0, out, count, axs.p, ays.p, azs.p, aZs.p, block_start.p, params_dev(),
+                            pot_params(slice0));
+        ctx->launches++;
+    }
+
+    void band_limit(C *t, int count) {
+        // FFT -> band_limit (k <= k_max * factor, inclusive) -> IFFT, clFFT scale s2d per transform
+        const cplx<R> *tw = ctx->twiddles<R>(N);
+        ops.row_fft(st(), t, t, count, tw, (R)1, -1);
+        ops.col_bandlimit(st(), t, count, tw, kx2.p, ky2.p, H.g.k_max * cfg.inverse_limit_factor, (R)(s2d * s2d));
+        ops.row_fft(st(), t, t, count, tw, (R)1, +1);
+        ctx->launches += 3;
+    }
+
+    void build_transmission() override {
+        if (!atoms_set) throw StateError("atoms not set (mslice_set_atoms)");
+        const int S = H.g.n_slices;
+        // slices in chunks so one launch's grid stays within limits
+        const int chunk = 1024;
+        for (int s0 = 0; s0 < S; s0 += chunk) {
+            int cnt = std::min(chunk, S - s0);
+            potentials(trans.p + (size_t)s0 * NN, s0, cnt);
+            band_limit(trans.p + (size_t)s0 * NN, cnt);
+        }
+        trans_built = true;
+    }
+
+    void copy_out_complex(const C *d, size_t count, double *out) {
+        std::vector<C> h(count);
+        MS_CUDA(cudaMemcpyAsync(h.data(), d, count * sizeof(C), cudaMemcpyDeviceToHost, st()));
+        MS_CUDA(cudaStreamSynchronize(st()));
+        for (size_t i = 0; i < count; i++) { out[2 * i] = (double)h[i].x; out[2 * i + 1] = (double)h[i].y; }
+    }
+
+    void get_transmission(int slice, int band_limited, double *out) override {
+        if (slice < 0 || slice >= H.g.n_slices) throw ArgError("slice out of range");
+        if (band_limited) {
+            if (!trans_built) throw StateError("transmission not built (mslice_build_transmission)");
+            copy_out_complex(trans.p + (size_t)slice * NN, NN, out);
+        } else {
+            if (!atoms_set) throw StateError("atoms not set");
+            ensure_waves(1);
+            potentials(tmp.p, slice, 1);
+            copy_out_complex(tmp.p, NN, out);
+        }
+    }
+
+    void get_propagator(double *out) override {
+        std::vector<C> hpx(N), hpy(N);
+        MS_CUDA(cudaMemcpy(hpx.data(), px.p, N * sizeof(C), cudaMemcpyDeviceToHost));
+        MS_CUDA(cudaMemcpy(hpy.data(), py.p, N * sizeof(C), cudaMemcpyDeviceToHost));
+        const double km2 = k_prop * k_prop;
+        for (int y = 0; y < N; y++)
+            for (int x = 0; x < N; x++) {
+                size_t i = (size_t)y * N + x;
+                bool in = H.kx[x] * H.kx[x] + H.ky[y] * H.ky[y] < km2;
+                C v = in ? cmul(hpx[x], hpy[y]) : mk<R>(0, 0);
+                out[2 * i] = (double)v.x;
+                out[2 * i + 1] = (double)v.y;
+            }
+    }
+
+    void ensure_waves(int b) {
+        if (b <= batch_cap && wave.p) return;
+        wave.ensure(ctx, (size_t)b * NN);
+        recip.ensure(ctx, (size_t)b * NN);
+        tmp.ensure(ctx, (size_t)b * NN);
+        partials.ensure(ctx, (size_t)b * std::max(1, cfg.n_detectors) * ops.col_blocks);
+        pix.ensure(ctx, b);
+        pos.ensure(ctx, b);
+        batch_cap = b;
+    }
+
+    void get_probe(double x, double y, double *out) override {
+        // reciprocal-space probe: generate + column IFFT into wave, then undo the column IFFT with a
+        // forward column FFT (scale compensates), read back
+        ensure_waves(1);
+        const mslice_geometry &g = H.g;
+        double2 p = make_double2(x - g.sim_x[0], y - g.sim_y[0]);
+        MS_CUDA(cudaMemcpyAsync(pos.p, &p, sizeof(double2), cudaMemcpyHostToDevice, st()));
+        const cplx<R> *tw = ctx->twiddles<R>(N);
+        ops.col_probe(st(), wave.p, 1, tw, chi.p, kx.p, ky.p, pos.p, (R)1);
+        ops.col_fft(st(), wave.p, wave.p, 1, tw, (R)(1.0 / N), -1);
+        ctx->launches += 2;
+        copy_out_complex(wave.p, NN, out);
+    }
+
+    int default_batch() const {
+        if (cfg.probe_batch > 0) return cfg.probe_batch;
+        size_t bytes = NN * sizeof(C);
+        int b = (int)std::max<size_t>(1, ((size_t)256 << 20) / bytes);   // ~256 MB of waves per pass
+        return std::min(b, 4096);
+    }
+
+    // STEM probe positions of scan pixels (simulationstem.cpp:152-188)
+    double2 probe_pos(int p) const {
+        const mslice_geometry &g = H.g;
+        int num_x = cfg.stem_pixels_x;
+        double step_x = (cfg.stem_area[1] - cfg.stem_area[0]) / cfg.stem_pixels_x;
+        double step_y = (cfg.stem_area[3] - cfg.stem_area[2]) / cfg.stem_pixels_y;
+        int x_i = p % num_x;
+        int y_i = (int)std::floor(p / num_x);
+        double x_pos = cfg.stem_area[0] + x_i * step_x, y_pos = cfg.stem_area[2] + y_i * step_y;
+        return make_double2(x_pos - g.sim_x[0], y_pos - g.sim_y[0]);
+    }
+
+    void check_cancel() {
+        if (cancel.load()) {
+            cancel.store(false);
+            cudaStreamSynchronize(st());
+            throw Cancelled("simulation cancelled");
+        }
+    }
+
+    // Propagate `nb` STEM probes (scan pixel ids ids[0..nb)) through all slices; detector values of
+    // output slice o go to out[(o*n_det + d)*n_pix + out_index[i]] (Kahan-accumulated if comp).
+    void stem_batch(const int *ids, const int *out_index, int nb, int n_pix, double *out, double *comp) {
+        const mslice_geometry &g = H.g;
+        const cplx<R> *tw = ctx->twiddles<R>(N);
+        h_pos.resize(nb);
+        h_pix.assign(out_index, out_index + nb);
+        for (int i = 0; i < nb; i++) h_pos[i] = probe_pos(ids[i]);
+        MS_CUDA(cudaMemcpyAsync(pos.p, h_pos.data(), nb * sizeof(double2), cudaMemcpyHostToDevice, st()));
+        MS_CUDA(cudaMemcpyAsync(pix.p, h_pix.data(), nb * sizeof(int), cudaMemcpyHostToDevice, st()));
+        ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N));
+        ctx->launches++;
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
+        DetArgs det{detmask.p, cfg.n_detectors, partials.p};
+        std::vector<int> outs = output_slices(cfg, g);
+        size_t oi = 0;
+        const R a = (R)(1.0 / N), b = (R)(s2d * s2d * N), ds = (R)s2d;
+        for (int s = 0; s < g.n_slices; s++) {
+            ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a);
+            bool is_out = oi < outs.size() && outs[oi] == s;
+            int mode = !is_out ? COL_STEP : (s == g.n_slices - 1 ? COL_DET_ONLY : COL_STEP_DET);
+            ops.col_step(st(), wave.p, nb, tw, pt, b, ds, det, nullptr, mode);
+            ctx->launches += 2;
+            if (is_out) {
+                detector_reduce(st(), partials.p, ops.col_blocks, cfg.n_detectors, nb, pix.p, n_pix, (int)oi, out, comp);
+                ctx->launches++;
+                oi++;
+            }
+        }
+    }
+
+    void stem_run(const int *pixels, size_t n, double *out) override {
+        if (cfg.mode != MSLICE_MODE_STEM) throw StateError("simulation is not in STEM mode");
+        if (!trans_built) build_transmission();
+        const int np = cfg.stem_pixels_x * cfg.stem_pixels_y;
+        for (size_t i = 0; i < n; i++)
+            if (pixels[i] < 0 || pixels[i] >= np) throw ArgError("scan pixel index out of range");
+        const int B = default_batch();
+        ensure_waves(std::min<int>(B, (int)std::max<size_t>(n, 1)));
+        const mslice_geometry &g = H.g;
+        DevBuf<double> dout;
+        size_t tot = (size_t)g.n_outputs * cfg.n_detectors * n;
+        dout.ensure(ctx, tot);
+        MS_CUDA(cudaMemsetAsync(dout.p, 0, std::max<size_t>(tot, 1) * sizeof(double), st()));
+        std::vector<int> idx(n);
+        for (size_t i = 0; i < n; i++) idx[i] = (int)i;
+        for (size_t b0 = 0; b0 < n; b0 += batch_cap) {
+            check_cancel();
+            int nb = (int)std::min<size_t>(batch_cap, n - b0);
+            stem_batch(pixels + b0, idx.data() + b0, nb, (int)n, dout.p, nullptr);
+            MS_CUDA(cudaStreamSynchronize(st()));
+            if (progress) progress((double)(b0 + nb) / n, progress_user);
+        }
+        if (tot) MS_CUDA(cudaMemcpy(out, dout.p, tot * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+
+    // one probe (CBED) or plane wave (CTEM) through all slices with outputs at the output slices
+    template <class F>
+    void single_wave(bool plane, F &&on_output) {
+        const mslice_geometry &g = H.g;
+        const cplx<R> *tw = ctx->twiddles<R>(N);
+        ensure_waves(1);
+        if (plane) {
+            plane_wave_state<R>(st(), N, wave.p);
+        } else {
+            double2 p = make_double2(cfg.cbed_x - g.sim_x[0], cfg.cbed_y - g.sim_y[0]);
+            MS_CUDA(cudaMemcpyAsync(pos.p, &p, sizeof(double2), cudaMemcpyHostToDevice, st()));
+            ops.col_probe(st(), wave.p, 1, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N));
+        }
+        ctx->launches++;
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
+        DetArgs det{detmask.p, 0, partials.p};
+        std::vector<int> outs = output_slices(cfg, g);
+        size_t oi = 0;
+        const R a = (R)(1.0 / N), b = (R)(s2d * s2d * N), ds = (R)s2d;
+        for (int s = 0; s < g.n_slices; s++) {
+            check_cancel();
+            ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a);
+            bool is_out = oi < outs.size() && outs[oi] == s;
+            ops.col_step(st(), wave.p, 1, tw, pt, b, ds, det, is_out ? recip.p : nullptr, is_out ? COL_STEP_DET : COL_STEP);
+            ctx->launches += 2;
+            if (is_out) { on_output((int)oi); oi++; }
+            if (progress) progress((double)(s + 1) / g.n_slices, progress_user);
+        }
+    }
+
+    void cbed_run(double *diff) override {
+        if (cfg.mode != MSLICE_MODE_CBED) throw StateError("simulation is not in CBED mode");
+        if (!trans_built) build_transmission();
+        DevBuf<double> d;
+        d.ensure(ctx, (size_t)H.g.n_outputs * NN);
+        single_wave(false, [&](int o) {
+            diffraction<R>(st(), N, recip.p, d.p + (size_t)o * NN, nullptr);
+            ctx->launches++;
+        });
+        MS_CUDA(cudaStreamSynchronize(st()));
+        MS_CUDA(cudaMemcpy(diff, d.p, (size_t)H.g.n_outputs * NN * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+
+    void ctem_run(double *ew, double *diff, double *image) override {
+        if (cfg.mode != MSLICE_MODE_CTEM) throw StateError("simulation is not in CTEM mode");
+        if (!trans_built) build_transmission();
+        const int no = H.g.n_outputs;
+        DevBuf<double> dd, di;
+        DevBuf<double2> de;
+        if (ew) de.ensure(ctx, (size_t)no * NN);
+        if (diff) dd.ensure(ctx, (size_t)no * NN);
+        if (image && cfg.ctem_image) di.ensure(ctx, (size_t)no * NN);
+        const cplx<R> *tw = ctx->twiddles<R>(N);
+        const mslice_geometry &g = H.g;
+        single_wave(true, [&](int o) {
+            if (ew) {   // psi = (1/N) Dinv_r phi  (getExitWaveImage, simulationgeneral.cpp:808-830)
+                ops.row_fft(st(), wave.p, tmp.p, 1, tw, (R)(1.0 / N), +1);
+                convert_to_double<R>(st(), NN, tmp.p, de.p + (size_t)o * NN);
+                ctx->launches += 2;
+            }
+            if (diff) { diffraction<R>(st(), N, recip.p, dd.p + (size_t)o * NN, nullptr); ctx->launches++; }
+            if (image && cfg.ctem_image) {   // simulateImagePerfect (simulationctem.cpp:114-166)
+                ctem_transfer<R>(st(), N, recip.p, tmp.p, kx.p, ky.p, g.wavelength, aberr(cfg.C10), cfg.obj_ap,
+                                 cfg.obj_ap_smooth, cfg.alpha, cfg.delta);
+                ops.row_fft(st(), tmp.p, tmp.p, 1, tw, (R)1, +1);
+                ops.col_fft(st(), tmp.p, tmp.p, 1, tw, (R)s2d, +1);
+                sqabs_to_double<R>(st(), NN, tmp.p, di.p + (size_t)o * NN);
+                ctx->launches += 4;
+            }
+        });
+        MS_CUDA(cudaStreamSynchronize(st()));
+        if (ew) MS_CUDA(cudaMemcpy(ew, de.p, (size_t)no * NN * sizeof(double2), cudaMemcpyDeviceToHost));
+        if (diff) MS_CUDA(cudaMemcpy(diff, dd.p, (size_t)no * NN * sizeof(double), cudaMemcpyDeviceToHost));
+        if (image && cfg.ctem_image) MS_CUDA(cudaMemcpy(image, di.p, (size_t)no * NN * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+
+    // ---- staged frozen-phonon configurations ------------------------------------------------
+    void stage(int nc, const size_t *cnt, const int *Z, const double *x, const double *y, const double *z) override {
+        if (nc < 1) throw ArgError("need at least one configuration");
+        size_t tot = 0, mx = 0;
+        cfg_counts.assign(cnt, cnt + nc);
+        cfg_offsets.resize(nc);
+        for (int c = 0; c < nc; c++) { cfg_offsets[c] = tot; tot += cnt[c]; mx = std::max(mx, cnt[c]); }
+        check_Z(Z, tot);
+        sZ.ensure(ctx, tot); sx.ensure(ctx, tot); sy.ensure(ctx, tot); sz.ensure(ctx, tot);
+        if (tot) {
+            MS_CUDA(cudaMemcpyAsync(sZ.p, Z, tot * sizeof(int), cudaMemcpyHostToDevice, st()));
+            MS_CUDA(cudaMemcpyAsync(sx.p, x, tot * sizeof(double), cudaMemcpyHostToDevice, st()));
+            MS_CUDA(cudaMemcpyAsync(sy.p, y, tot * sizeof(double), cudaMemcpyHostToDevice, st()));
+            MS_CUDA(cudaMemcpyAsync(sz.p, z, tot * sizeof(double), cudaMemcpyHostToDevice, st()));
+        }
+        ensure_atom_capacity(mx);
+        n_configs = nc;
+    }
+
+    void run_staged(int mode) override {
+        if (n_configs < 1) throw StateError("no configurations staged (mslice_stage_configs)");
+        if (mode != cfg.mode) throw StateError("staged run of the wrong mode");
+        const mslice_geometry &g = H.g;
+        const int np = cfg.stem_pixels_x * cfg.stem_pixels_y;
+        if (mode == MSLICE_MODE_STEM) acc_n = (size_t)g.n_outputs * cfg.n_detectors * np;
+        else acc_n = (size_t)g.n_outputs * NN;
+        acc.ensure(ctx, acc_n); comp.ensure(ctx, acc_n);
+        MS_CUDA(cudaMemsetAsync(acc.p, 0, std::max<size_t>(acc_n, 1) * sizeof(double), st()));
+        MS_CUDA(cudaMemsetAsync(comp.p, 0, std::max<size_t>(acc_n, 1) * sizeof(double), st()));
+        std::vector<int> ids(np);
+        for (int i = 0; i < np; i++) ids[i] = i;
+        if (mode == MSLICE_MODE_STEM) ensure_waves(std::min(default_batch(), np));
+        float t_build = 0, t_prop = 0;
+        MS_CUDA(cudaEventRecord(ev[2], st()));
+        for (int c = 0; c < n_configs; c++) {
+            check_cancel();
+            MS_CUDA(cudaEventRecord(ev[0], st()));
+            sort_device(sZ.p + cfg_offsets[c], sx.p + cfg_offsets[c], sy.p + cfg_offsets[c], sz.p + cfg_offsets[c], cfg_counts[c]);
+            build_transmission();
+            MS_CUDA(cudaEventRecord(ev[1], st()));
+            if (mode == MSLICE_MODE_STEM) {
+                for (int b0 = 0; b0 < np; b0 += batch_cap) {
+                    check_cancel();
+                    int nb = std::min(batch_cap, np - b0);
+                    stem_batch(ids.data() + b0, ids.data() + b0, nb, np, acc.p, comp.p);
+                }
+            } else {
+                single_wave(false, [&](int o) {
+                    diffraction<R>(st(), N, recip.p, acc.p + (size_t)o * NN, comp.p + (size_t)o * NN);
+                    ctx->launches++;
+                });
+            }
+            MS_CUDA(cudaEventRecord(ev[3], st()));
+            MS_CUDA(cudaEventSynchronize(ev[3]));
+            float a = 0, b = 0;
+            MS_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
+            MS_CUDA(cudaEventElapsedTime(&b, ev[1], ev[3]));
+            t_build += a;
+            t_prop += b;
+            if (progress) progress((double)(c + 1) / n_configs, progress_user);
+        }
+        float tot = 0;
+        MS_CUDA(cudaEventElapsedTime(&tot, ev[2], ev[3]));
+        timing[0] = t_build; timing[1] = t_prop; timing[2] = tot;
+        acc_configs = n_configs;
+    }
+
+    void staged_result(double *out, size_t cap) override {
+        if (acc_configs < 1) throw StateError("no staged run");
+        if (cap < acc_n) throw ArgError("output capacity too small");
+        MS_CUDA(cudaStreamSynchronize(st()));
+        MS_CUDA(cudaMemcpy(out, acc.p, acc_n * sizeof(double), cudaMemcpyDeviceToHost));
+        // Image::getWeightedSlice: sum / weight, weight = number of configurations per pixel
+        for (size_t i = 0; i < acc_n; i++) out[i] /= (double)acc_configs;
+    }
+
+    void stem_plain(const int *pixels, size_t n, double *out) override {
+        if constexpr (sizeof(R) != 8) {
+            (void)pixels; (void)n; (void)out;
+            throw StateError("the plain path is the FP64 path: create the simulation with double_precision = 1");
+        } else {
+            if (cfg.mode != MSLICE_MODE_STEM) throw StateError("simulation is not in STEM mode");
+            if (!trans_built) build_transmission();
+            const mslice_geometry &g = H.g;
+            PlainArgs a;
+            std::memset(&a, 0, sizeof(a));
+            a.n = N; a.n_slices = g.n_slices; a.n_det = cfg.n_detectors; a.n_outputs = g.n_outputs;
+            a.slice_step = cfg.intermediate_slices; a.scan_nx = cfg.stem_pixels_x;
+            a.kx = kx.p; a.ky = ky.p; a.chi = chi.p; a.trans = (const double2 *)trans.p;
+            a.dz = g.dz; a.beam_k = g.wavenumber; a.beam_kx = g.wavevector[0]; a.beam_ky = g.wavevector[1];
+            a.beam_kz = g.wavevector[2]; a.k_max_prop = k_prop;
+            a.start_x = cfg.stem_area[0]; a.start_y = cfg.stem_area[2];
+            a.step_x = (cfg.stem_area[1] - cfg.stem_area[0]) / cfg.stem_pixels_x;
+            a.step_y = (cfg.stem_area[3] - cfg.stem_area[2]) / cfg.stem_pixels_y;
+            a.sim_x0 = g.sim_x[0]; a.sim_y0 = g.sim_y[0];
+            a.fft_scale = s2d;
+            for (int d = 0; d < cfg.n_detectors; d++) {
+                a.innerPx[d] = cfg.detectors[d].inner / g.angle_scale;
+                a.outerPx[d] = cfg.detectors[d].outer / g.angle_scale;
+                a.xcPx[d] = cfg.detectors[d].xcentre / g.angle_scale;
+                a.ycPx[d] = cfg.detectors[d].ycentre / g.angle_scale;
+            }
+            a.launches = &ctx->launches;
+            plain_stem(st(), a, pixels, n, out);
+        }
+    }
+};
+
+template <class R> PassOps<R> pass_ops(int n) {
+    switch (n) {
+#define MS_CASE(N) case N: return make_pass_ops<R, N>();
+        MS_SIZES(MS_CASE)
+#undef MS_CASE
+    }
+    throw Unsupported("grid size " + std::to_string(n) + " is not built into this library");
+}
+template PassOps<float> pass_ops<float>(int);
+template PassOps<double> pass_ops<double>(int);
+
+}  // namespace ms
+
+// =================================================================================================
+// C ABI
+// =================================================================================================
+struct mslice_ctx { ms::Ctx impl; };
+struct mslice_sim {
+    mslice_ctx *ctx;
+    std::unique_ptr<ms::SimBase> impl;
+};
+
+namespace {
+template <class F> int guarded(F &&f) {
+    try {
+        f();
+        return MSLICE_OK;
+    } catch (const ms::ArgError &e) { ms::g_last_error = e.what(); return MSLICE_ERR_ARG; }
+    catch (const ms::StateError &e) { ms::g_last_error = e.what(); return MSLICE_ERR_STATE; }
+    catch (const ms::OomError &e) { ms::g_last_error = e.what(); return MSLICE_ERR_OOM; }
+    catch (const ms::Cancelled &e) { ms::g_last_error = e.what(); return MSLICE_ERR_CANCELLED; }
+    catch (const ms::Unsupported &e) { ms::g_last_error = e.what(); return MSLICE_ERR_UNSUPPORTED; }
+    catch (const ms::CudaError &e) { ms::g_last_error = e.what(); return MSLICE_ERR_CUDA; }
+    catch (const std::bad_alloc &) { ms::g_last_error = "host allocation failed"; return MSLICE_ERR_OOM; }
+    catch (const std::exception &e) { ms::g_last_error = e.what(); return MSLICE_ERR_ARG; }
+    catch (...) { ms::g_last_error = "unknown error"; return MSLICE_ERR_ARG; }
+}
+void need(bool c, const char *what) {
+    if (!c) throw ms::ArgError(what);
+}
+void use_device(mslice_ctx *c) { MS_CUDA(cudaSetDevice(c->impl.device)); }
+}  // namespace
+
+extern "C" {
+
+const char *mslice_version(void) { return "mslice-b200 1 (sm_100a)"; }
+const char *mslice_last_error(void) { return ms::g_last_error.c_str(); }
+
+int mslice_ctx_create(int device, mslice_ctx **out) {
+    return guarded([&] {
+        need(out != nullptr, "out is null");
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            throw ms::CudaError(std::string("no CUDA device available: ") + cudaGetErrorString(e));
+        }
+        need(device >= 0 && device < n, "device index out of range");
+        MS_CUDA(cudaSetDevice(device));
+        auto c = std::make_unique<mslice_ctx>();
+        c->impl.device = device;
+        MS_CUDA(cudaStreamCreateWithFlags(&c->impl.stream, cudaStreamNonBlocking));
+        *out = c.release();
+    });
+}
+
+int mslice_ctx_destroy(mslice_ctx *ctx) {
+    return guarded([&] {
+        if (!ctx) return;
+        cudaSetDevice(ctx->impl.device);
+        delete ctx;
+    });
+}
+
+int mslice_ctx_set_memory_limit(mslice_ctx *ctx, size_t bytes) {
+    return guarded([&] {
+        need(ctx != nullptr, "ctx is null");
+        ctx->impl.mem_limit = bytes;
+    });
+}
+
+int mslice_params_load(mslice_ctx *ctx, int form, int i_per_atom, const double *p, size_t n) {
+    return guarded([&] {
+        need(ctx != nullptr && (p != nullptr || n == 0), "null argument");
+        need(form >= 0 && form <= 2, "unknown parameterisation form");
+        need(i_per_atom > 0, "terms per atom must be positive");
+        size_t per = (size_t)i_per_atom * (form == MSLICE_KIRKLAND ? 4 : 2);
+        if (form == MSLICE_KIRKLAND) need(i_per_atom <= 3, "Kirkland tables hold at most 3 terms of each kind");
+        else need(i_per_atom <= 5, "Peng/Lobato tables hold at most 5 terms");
+        // Parameterisation (structureparameters.h:30-33)
+        if (n % per != 0 || n == 0) throw ms::ArgError("Parameterisation does not contain correct parameters per atom");
+        // the kernels index (Z-1)*12 or (Z-1)*10 (projected_d.cl:110,148,167)
+        size_t stride = form == MSLICE_KIRKLAND ? 12 : 10;
+        need(n % stride == 0, "parameter table must hold 12 (Kirkland) or 10 (Peng/Lobato) values per element");
+        use_device(ctx);
+        ms::Ctx &c = ctx->impl;
+        c.params.form = form;
+        c.params.i_count = i_per_atom;
+        c.params.values.assign(p, p + n);
+        c.params.max_z = (int)(n / stride);
+        if (c.prm_d) { c.release(c.prm_d, c.prm_n * sizeof(double)); c.prm_d = nullptr; }
+        if (c.prm_f) { c.release(c.prm_f, c.prm_n * sizeof(float)); c.prm_f = nullptr; }
+        c.prm_n = n;
+        c.prm_d = (double *)c.alloc(n * sizeof(double));
+        c.prm_f = (float *)c.alloc(n * sizeof(float));
+        std::vector<float> pf(p, p + n);
+        MS_CUDA(cudaMemcpy(c.prm_d, p, n * sizeof(double), cudaMemcpyHostToDevice));
+        MS_CUDA(cudaMemcpy(c.prm_f, pf.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    });
+}
+
+int mslice_geometry_compute(const mslice_config *cfg, mslice_geometry *out) {
+    return guarded([&] {
+        need(cfg && out, "null argument");
+        ms::HostGeom H;
+        ms::compute_geometry(*cfg, H);
+        *out = H.g;
+    });
+}
+
+int mslice_sim_create(mslice_ctx *ctx, const mslice_config *cfg, mslice_sim **out) {
+    return guarded([&] {
+        need(ctx && cfg && out, "null argument");
+        use_device(ctx);
+        auto s = std::make_unique<mslice_sim>();
+        s->ctx = ctx;
+        if (cfg->double_precision) s->impl = std::make_unique<ms::Sim<double>>(&ctx->impl, *cfg);
+        else s->impl = std::make_unique<ms::Sim<float>>(&ctx->impl, *cfg);
+        *out = s.release();
+    });
+}
+
+int mslice_sim_destroy(mslice_sim *sim) {
+    return guarded([&] {
+        if (!sim) return;
+        use_device(sim->ctx);
+        cudaStreamSynchronize(sim->ctx->impl.stream);
+        delete sim;
+    });
+}
+
+int mslice_sim_geometry(mslice_sim *sim, mslice_geometry *out) {
+    return guarded([&] {
+        need(sim && out, "null argument");
+        *out = sim->impl->H.g;
+    });
+}
+
+int mslice_set_progress(mslice_sim *sim, mslice_progress_cb cb, void *user) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        sim->impl->progress = cb;
+        sim->impl->progress_user = user;
+    });
+}
+
+int mslice_cancel(mslice_sim *sim) {
+    if (!sim) return MSLICE_ERR_ARG;
+    sim->impl->cancel.store(true);
+    return MSLICE_OK;
+}
+
+int mslice_set_atoms(mslice_sim *sim, const int *Z, const double *x, const double *y, const double *z, size_t n) {
+    return guarded([&] {
+        need(sim && (n == 0 || (Z && x && y && z)), "null argument");
+        use_device(sim->ctx);
+        sim->impl->set_atoms(Z, x, y, z, n, true);
+    });
+}
+
+int mslice_get_sorted_atoms(mslice_sim *sim, int *Z, double *x, double *y, double *z, size_t cap, int *block_start,
+                            size_t cap_block_start, int *block_ids, int *z_ids, size_t *n_out) {
+    return guarded([&] {
+        need(sim && Z && x && y && z && block_start && n_out, "null argument");
+        use_device(sim->ctx);
+        sim->impl->get_sorted(Z, x, y, z, cap, block_start, cap_block_start, block_ids, z_ids, n_out);
+    });
+}
+
+int mslice_build_transmission(mslice_sim *sim) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        use_device(sim->ctx);
+        sim->impl->build_transmission();
+        MS_CUDA(cudaStreamSynchronize(sim->ctx->impl.stream));
+    });
+}
+
+int mslice_get_transmission(mslice_sim *sim, int slice, int band_limited, double *out) {
+    return guarded([&] {
+        need(sim && out, "null argument");
+        use_device(sim->ctx);
+        sim->impl->get_transmission(slice, band_limited, out);
+    });
+}
+
+int mslice_get_propagator(mslice_sim *sim, double *out) {
+    return guarded([&] {
+        need(sim && out, "null argument");
+        use_device(sim->ctx);
+        sim->impl->get_propagator(out);
+    });
+}
+
+int mslice_get_probe(mslice_sim *sim, double x, double y, double *out) {
+    return guarded([&] {
+        need(sim && out, "null argument");
+        use_device(sim->ctx);
+        sim->impl->get_probe(x, y, out);
+    });
+}
+
+int mslice_stem_run(mslice_sim *sim, const int *pixels, size_t n_pixels, double *out) {
+    return guarded([&] {
+        need(sim && (n_pixels == 0 || (pixels && out)), "null argument");
+        use_device(sim->ctx);
+        sim->impl->stem_run(pixels, n_pixels, out);
+    });
+}
+
+int mslice_cbed_run(mslice_sim *sim, double *diff) {
+    return guarded([&] {
+        need(sim && diff, "null argument");
+        use_device(sim->ctx);
+        sim->impl->cbed_run(diff);
+    });
+}
+
+int mslice_ctem_run(mslice_sim *sim, double *ew, double *diff, double *image) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        use_device(sim->ctx);
+        sim->impl->ctem_run(ew, diff, image);
+    });
+}
+
+int mslice_stage_configs(mslice_sim *sim, int n_configs, const size_t *counts, const int *Z, const double *x,
+                         const double *y, const double *z) {
+    return guarded([&] {
+        need(sim && counts && n_configs > 0, "null argument");
+        use_device(sim->ctx);
+        sim->impl->stage(n_configs, counts, Z, x, y, z);
+    });
+}
+
+int mslice_stem_run_staged(mslice_sim *sim) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        use_device(sim->ctx);
+        sim->impl->run_staged(MSLICE_MODE_STEM);
+    });
+}
+
+int mslice_cbed_run_staged(mslice_sim *sim) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        use_device(sim->ctx);
+        sim->impl->run_staged(MSLICE_MODE_CBED);
+    });
+}
+
+int mslice_staged_result(mslice_sim *sim, double *out, size_t cap) {
+    return guarded([&] {
+        need(sim && out, "null argument");
+        use_device(sim->ctx);
+        sim->impl->staged_result(out, cap);
+    });
+}
+
+int mslice_stem_simulate(mslice_sim *sim, int n_configs, const size_t *counts, const int *Z, const double *x,
+                         const double *y, const double *z, double *out, size_t cap) {
+    return guarded([&] {
+        need(sim && counts && out && n_configs > 0, "null argument");
+        use_device(sim->ctx);
+        sim->impl->stage(n_configs, counts, Z, x, y, z);
+        sim->impl->run_staged(MSLICE_MODE_STEM);
+        sim->impl->staged_result(out, cap);
+    });
+}
+
+int mslice_stem_run_plain(mslice_sim *sim, const int *pixels, size_t n_pixels, double *out) {
+    return guarded([&] {
+        need(sim && (n_pixels == 0 || (pixels && out)), "null argument");
+        use_device(sim->ctx);
+        sim->impl->stem_plain(pixels, n_pixels, out);
+    });
+}
+
+int mslice_fft2(mslice_ctx *ctx, int n, int inverse, int double_precision, int batch, const double *in, double *out) {
+    return guarded([&] {
+        need(ctx && in && out && batch > 0, "null argument");
+        use_device(ctx);
+        ms::Ctx &c = ctx->impl;
+        const size_t NN = (size_t)n * n, tot = NN * batch;
+        const double s2d = (double)(1.0f / sqrtf((float)NN));
+        auto run = [&](auto tag) {
+            using R = decltype(tag);
+            ms::PassOps<R> ops = ms::pass_ops<R>(n);
+            ms::DevBuf<ms::cplx<R>> d;
+            ms::DevBuf<double2> dd;
+            d.ensure(&c, tot);
+            dd.ensure(&c, tot);
+            MS_CUDA(cudaMemcpyAsync(dd.p, in, tot * sizeof(double2), cudaMemcpyHostToDevice, c.stream));
+            ms::convert_from_double<R>(c.stream, tot, dd.p, d.p);
+            const ms::cplx<R> *tw = c.twiddles<R>(n);
+            int sign = inverse ? +1 : -1;
+            ops.row_fft(c.stream, d.p, d.p, batch, tw, (R)1, sign);
+            ops.col_fft(c.stream, d.p, d.p, batch, tw, (R)s2d, sign);
+            ms::convert_to_double<R>(c.stream, tot, d.p, dd.p);
+            c.launches += 4;
+            MS_CUDA(cudaMemcpyAsync(out, dd.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, c.stream));
+            MS_CUDA(cudaStreamSynchronize(c.stream));
+        };
+        if (double_precision) run(double(0));
+        else run(float(0));
+    });
+}
+
+int mslice_ctx_stream(mslice_ctx *ctx, void **stream) {
+    return guarded([&] {
+        need(ctx && stream, "null argument");
+        *stream = (void *)ctx->impl.stream;
+    });
+}
+
+int mslice_ctx_launch_count(mslice_ctx *ctx, unsigned long long *count) {
+    return guarded([&] {
+        need(ctx && count, "null argument");
+        *count = ctx->impl.launches;
+    });
+}
+
+int mslice_last_timing(mslice_sim *sim, double *ms3) {
+    return guarded([&] {
+        need(sim && ms3, "null argument");
+        for (int i = 0; i < 3; i++) ms3[i] = sim->impl->timing[i];
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,177 @@
+// fft.cuh — batched Stockham FFT building blocks staged in shared memory.
+//
+// One transform of length N is done by NT = N/E threads, each holding E elements in registers.
+// Stage s (radix RAD, Ns = product of the radices before s) computes, for butterfly j in [0, N/RAD):
+//     v[r] = x[j + r*N/RAD] * W_{Ns*RAD}^{r*(j mod Ns)},   y = DFT_RAD(v),
+//     out[(j/Ns)*Ns*RAD + (j mod Ns) + m*Ns] = y[m]
+// (the autosort Stockham formulation, Govindaraju et al., SC 2008). Thread t owns butterflies
+// j = t + b*NT, b < E/RAD. With that assignment the first stage reads exactly the elements
+// t + m*NT a thread loads from global memory, and the last stage writes exactly the elements
+// t + m*NT it stores, so only the inner stage boundaries go through shared memory.
+//
+// Sizes: N = 2^k (E = 8, radix-8 stages plus one radix-2/4 stage) and N = 3*2^k (E = 12, radix-4
+// stages, an optional radix-2 stage and one radix-3 stage). Unnormalised transforms; callers scale.
+#pragma once
+
+#include "common.cuh"
+
+namespace ms {
+
+__host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
+__host__ __device__ constexpr bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+template <int N>
+struct Plan {
+    static constexpr bool pow2 = is_pow2(N);
+    static_assert(pow2 || (N % 3 == 0 && is_pow2(N / 3)), "FFT length must be 2^k or 3*2^k");
+    static constexpr int E = pow2 ? 8 : 12;
+    static constexpr int NT = N / E;
+    static constexpr int K = pow2 ? ilog2c(N) : ilog2c(N / 3);
+    // pow2: K/3 radix-8 stages, then one radix-2 or radix-4 stage if K%3 != 0
+    // 3*2^k: K/2 radix-4 stages, a radix-2 stage if K odd, then a radix-3 stage
+    static constexpr int nstages = pow2 ? (K / 3 + (K % 3 ? 1 : 0)) : (K / 2 + (K % 2) + 1);
+    __host__ __device__ static constexpr int radix(int s) {
+        return pow2 ? (s < K / 3 ? 8 : (K % 3 == 1 ? 2 : 4))
+                    : (s < K / 2 ? 4 : ((K % 2 && s == K / 2) ? 2 : 3));
+    }
+    __host__ __device__ static constexpr int ns(int s) { return s == 0 ? 1 : ns(s - 1) * radix(s - 1); }
+};
+
+// ---- small DFTs in registers; SIGN = -1 forward, +1 inverse --------------------------------------
+template <class C> __device__ __forceinline__ C mul_i(C a, int sign) {   // a * (sign * i)
+    C r;
+    if (sign > 0) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+    return r;
+}
+
+template <class R, int SIGN> __device__ __forceinline__ void dft2(cplx<R> &a0, cplx<R> &a1) {
+    cplx<R> t = a0;
+    a0 = cadd(t, a1);
+    a1 = csub(t, a1);
+}
+template <class R, int SIGN> __device__ __forceinline__ void dft4(cplx<R> &a0, cplx<R> &a1, cplx<R> &a2, cplx<R> &a3) {
+    cplx<R> A0 = cadd(a0, a2), A1 = csub(a0, a2), A2 = cadd(a1, a3), A3 = mul_i(csub(a1, a3), SIGN);
+    a0 = cadd(A0, A2);
+    a2 = csub(A0, A2);
+    a1 = cadd(A1, A3);
+    a3 = csub(A1, A3);
+}
+template <class R, int SIGN> __device__ __forceinline__ void dft3(cplx<R> &a0, cplx<R> &a1, cplx<R> &a2) {
+    const R h = (R)0.86602540378443864676;   // sqrt(3)/2
+    cplx<R> t1 = cadd(a1, a2), t2 = csub(a1, a2);
+    cplx<R> m = mk<R>(a0.x - (R)0.5 * t1.x, a0.y - (R)0.5 * t1.y);
+    cplx<R> s = mul_i(cscale(t2, h), SIGN);
+    a0 = cadd(a0, t1);
+    a1 = cadd(m, s);
+    a2 = csub(m, s);
+}
+template <class R, int SIGN> __device__ __forceinline__ void dft8(cplx<R> *a) {
+    const R q = (R)0.70710678118654752440;   // 1/sqrt(2)
+    cplx<R> e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6];
+    cplx<R> o0 = a[1], o1 = a[3], o2 = a[5], o3 = a[7];
+    dft4<R, SIGN>(e0, e1, e2, e3);
+    dft4<R, SIGN>(o0, o1, o2, o3);
+    // W8^1 = (1 + SIGN i)/sqrt2, W8^2 = SIGN i, W8^3 = (-1 + SIGN i)/sqrt2
+    cplx<R> w1o1, w2o2, w3o3;
+    if (SIGN < 0) {
+        w1o1 = mk<R>((o1.x + o1.y) * q, (o1.y - o1.x) * q);
+        w3o3 = mk<R>((o3.y - o3.x) * q, (-o3.x - o3.y) * q);
+    } else {
+        w1o1 = mk<R>((o1.x - o1.y) * q, (o1.y + o1.x) * q);
+        w3o3 = mk<R>((-o3.x - o3.y) * q, (o3.x - o3.y) * q);
+    }
+    w2o2 = mul_i(o2, SIGN);
+    a[0] = cadd(e0, o0);
+    a[4] = csub(e0, o0);
+    a[1] = cadd(e1, w1o1);
+    a[5] = csub(e1, w1o1);
+    a[2] = cadd(e2, w2o2);
+    a[6] = csub(e2, w2o2);
+    a[3] = cadd(e3, w3o3);
+    a[7] = csub(e3, w3o3);
+}
+
+template <class R, int RAD, int SIGN> __device__ __forceinline__ void dft(cplx<R> *a) {
+    if constexpr (RAD == 2) dft2<R, SIGN>(a[0], a[1]);
+    else if constexpr (RAD == 3) dft3<R, SIGN>(a[0], a[1], a[2]);
+    else if constexpr (RAD == 4) dft4<R, SIGN>(a[0], a[1], a[2], a[3]);
+    else dft8<R, SIGN>(a);
+}
+
+// ---- shared-memory addressing of one transform's elements ---------------------------------------
+// Row transforms: one padding element per 8 keeps the stride-8 Stockham writes conflict free.
+struct RowAddr {
+    __device__ __forceinline__ int operator()(int i) const { return i + (i >> 3); }
+    static constexpr int size(int n) { return n + n / 8 + 1; }
+};
+// Column tiles: element i of column c lives at i*COLS + c (threads of one row are consecutive).
+template <int COLS> struct ColAddr {
+    __device__ __forceinline__ int operator()(int i) const { return i * COLS; }
+};
+
+// ---- the stage recursion ----------------------------------------------------------------------
+// v: E elements in "natural strided" order v[m] = x[t + m*NT] on entry and exit.
+// sm: this transform's shared memory (element 0), ad: addressing, tw: W_N^m twiddles (m < N).
+// All threads of the block must call this together (it contains __syncthreads()).
+template <class R, int N, int SIGN, int S, class Addr>
+__device__ __forceinline__ void fft_stages(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm, Addr ad, int t, const cplx<R> *tw) {
+    using P = Plan<N>;
+    constexpr int E = P::E, NT = P::NT;
+    constexpr int RAD = P::radix(S);
+    constexpr int Ns = P::ns(S);
+    constexpr int NB = E / RAD;          // butterflies per thread
+    constexpr bool last = (S == P::nstages - 1);
+    constexpr int TWS = N / (Ns * RAD);  // twiddle index stride
+    if constexpr (S > 0) {
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            int j = t + b * NT;
+#pragma unroll
+            for (int r = 0; r < RAD; r++) v[b + r * NB] = sm[ad(j + r * (N / RAD))];
+        }
+    }
+    cplx<R> out[E];
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        int j = t + b * NT;
+        int k = j % Ns;
+        cplx<R> a[RAD];
+#pragma unroll
+        for (int r = 0; r < RAD; r++) {
+            cplx<R> x = v[b + r * NB];
+            if constexpr (S > 0) {
+                if (r > 0) {
+                    cplx<R> w = tw[r * k * TWS];
+                    x = (SIGN < 0) ? cmul(x, w) : cmulc(x, w);
+                }
+            }
+            a[r] = x;
+        }
+        dft<R, RAD, SIGN>(a);
+#pragma unroll
+        for (int m = 0; m < RAD; m++) out[b + m * NB] = a[m];
+    }
+    if constexpr (last) {
+#pragma unroll
+        for (int i = 0; i < E; i++) v[i] = out[i];
+    } else {
+        __syncthreads();
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            int j = t + b * NT;
+            int k = j % Ns;
+            int idxD = (j / Ns) * Ns * RAD + k;
+#pragma unroll
+            for (int m = 0; m < RAD; m++) sm[ad(idxD + m * Ns)] = out[b + m * NB];
+        }
+        __syncthreads();
+        fft_stages<R, N, SIGN, S + 1, Addr>(v, sm, ad, t, tw);
+    }
+}
+
+template <class R, int N, int SIGN, class Addr>
+__device__ __forceinline__ void fft(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm, Addr ad, int t, const cplx<R> *tw) {
+    fft_stages<R, N, SIGN, 0, Addr>(v, sm, ad, t, tw);
+}
+
+}  // namespace ms

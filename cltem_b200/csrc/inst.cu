@@ -1,0 +1,104 @@
+// inst.cu — instantiates the pass kernels for one precision and one size.
+// Compiled once per (MS_REAL, MS_N) pair by the build (e.g. -DMS_REAL=float -DMS_N=512).
+#include "launch.cuh"
+
+#ifndef MS_REAL
+#error "MS_REAL must be defined"
+#endif
+#ifndef MS_N
+#error "MS_N must be defined"
+#endif
+
+namespace ms {
+
+namespace {
+using R = MS_REAL;
+constexpr int N = MS_N;
+using RC = RowCfg<N, R>;
+using CC = ColCfg<N, R>;
+
+template <class K> void set_smem(K kernel, size_t bytes) {
+    MS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// kernel attributes are per device: set once for each device this process launches on
+bool g_attrs_done[64] = {};
+void ensure_attrs() {
+    int dev = 0;
+    MS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || g_attrs_done[dev]) return;
+    set_smem(k_row_step<R, N>, RC::smem());
+    set_smem(k_row_fft<R, N, -1>, RC::smem());
+    set_smem(k_row_fft<R, N, +1>, RC::smem());
+    set_smem(k_col_step<R, N, COL_STEP>, CC::smem());
+    set_smem(k_col_step<R, N, COL_STEP_DET>, CC::smem());
+    set_smem(k_col_step<R, N, COL_DET_ONLY>, CC::smem());
+    set_smem(k_col_fft<R, N, -1>, CC::smem());
+    set_smem(k_col_fft<R, N, +1>, CC::smem());
+    set_smem(k_col_bandlimit<R, N>, CC::smem());
+    set_smem(k_col_probe<R, N>, CC::smem());
+    g_attrs_done[dev] = true;
+}
+
+inline dim3 row_grid(int batch) { return dim3(N / RC::ROWS, batch); }
+inline dim3 row_block() { return dim3(Plan<N>::NT, RC::ROWS); }
+inline dim3 col_grid(int batch) { return dim3(N / CC::COLS, batch); }
+inline dim3 col_block() { return dim3(CC::COLS, Plan<N>::NT); }
+
+void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a) {
+    ensure_attrs();
+    k_row_step<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a);
+    MS_CUDA(cudaGetLastError());
+}
+void row_fft(cudaStream_t s, const cplx<R> *in, cplx<R> *out, int batch, const cplx<R> *tw, R scale, int sign) {
+    ensure_attrs();
+    if (sign < 0) k_row_fft<R, N, -1><<<row_grid(batch), row_block(), RC::smem(), s>>>(in, out, tw, scale);
+    else k_row_fft<R, N, +1><<<row_grid(batch), row_block(), RC::smem(), s>>>(in, out, tw, scale);
+    MS_CUDA(cudaGetLastError());
+}
+void col_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, PropTables<R> pt, R b, R ds, DetArgs det,
+              cplx<R> *recip, int mode) {
+    ensure_attrs();
+    if (mode == COL_STEP && recip == nullptr)
+        k_col_step<R, N, COL_STEP><<<col_grid(batch), col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip);
+    else if (mode == COL_DET_ONLY)
+        k_col_step<R, N, COL_DET_ONLY><<<col_grid(batch), col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip);
+    else
+        k_col_step<R, N, COL_STEP_DET><<<col_grid(batch), col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip);
+    MS_CUDA(cudaGetLastError());
+}
+void col_fft(cudaStream_t s, const cplx<R> *in, cplx<R> *out, int batch, const cplx<R> *tw, R scale, int sign) {
+    ensure_attrs();
+    if (sign < 0) k_col_fft<R, N, -1><<<col_grid(batch), col_block(), CC::smem(), s>>>(in, out, tw, scale);
+    else k_col_fft<R, N, +1><<<col_grid(batch), col_block(), CC::smem(), s>>>(in, out, tw, scale);
+    MS_CUDA(cudaGetLastError());
+}
+void col_bandlimit(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, const double *kx2, const double *ky2,
+                   double lim, R scale) {
+    ensure_attrs();
+    k_col_bandlimit<R, N><<<col_grid(batch), col_block(), CC::smem(), s>>>(wave, tw, kx2, ky2, lim, scale);
+    MS_CUDA(cudaGetLastError());
+}
+void col_probe(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, const double2 *chi, const double *kx,
+               const double *ky, const double2 *pos, R scale) {
+    ensure_attrs();
+    k_col_probe<R, N><<<col_grid(batch), col_block(), CC::smem(), s>>>(wave, tw, chi, kx, ky, pos, scale);
+    MS_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+template <>
+PassOps<MS_REAL> make_pass_ops<MS_REAL, MS_N>() {
+    PassOps<R> o;
+    o.n = N;
+    o.col_blocks = N / CC::COLS;
+    o.row_step = row_step;
+    o.row_fft = row_fft;
+    o.col_step = col_step;
+    o.col_fft = col_fft;
+    o.col_bandlimit = col_bandlimit;
+    o.col_probe = col_probe;
+    return o;
+}
+
+}  // namespace ms

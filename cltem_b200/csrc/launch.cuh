@@ -1,0 +1,28 @@
+// launch.cuh — host launchers of the pass kernels, one explicit instantiation per (precision, size).
+#pragma once
+
+#include "passes.cuh"
+
+namespace ms {
+
+template <class R>
+struct PassOps {
+    int n = 0;
+    int col_blocks = 0;   // blocks per wave of a column pass (number of detector partials per wave)
+    void (*row_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R) = nullptr;
+    void (*row_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
+    void (*col_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, PropTables<R>, R, R, DetArgs, cplx<R> *, int) = nullptr;
+    void (*col_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
+    void (*col_bandlimit)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const double *, const double *, double, R) = nullptr;
+    void (*col_probe)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const double2 *, const double *, const double *,
+                      const double2 *, R) = nullptr;
+};
+
+// defined in inst.cu for every supported (R, N)
+template <class R, int N> PassOps<R> make_pass_ops();
+// switch over the supported sizes; throws for an unsupported one
+template <class R> PassOps<R> pass_ops(int n);
+
+#define MS_SIZES(X) X(64) X(96) X(128) X(256) X(384) X(512) X(768) X(1024) X(1536) X(2048) X(3072) X(4096)
+
+}  // namespace ms

@@ -1,0 +1,298 @@
+// passes.cuh — the fused row / column passes of the multislice step and their variants.
+//
+// Wave layout in HBM: a batch of res x res complex waves, wave b at wave + b*res*res, row-major with x
+// fastest (element (x, y) at x + res*y, as the reference kernels index it). Between passes a wave is
+// kept "row transformed": state phi = D_r psi, where D_r / D_c are the unnormalised 1-D DFTs along
+// rows / columns. One multislice step of the reference (simulationgeneral.cpp:744-764:
+// Recip = P * FFT(T psi); psi' = IFFT(Recip), clFFT unitary scale s2d = 1/sqrtf(res*res) per 2-D
+// transform) then becomes two passes, each one read + one write of the wave:
+//   row pass    : phi <- D_r( T_s * a * Dinv_r phi )                       (a = 1/res)
+//   column pass : phi <- Dinv_c( b * P * D_c phi )                        (b = s2d^2 * res)
+// and after the column pass's multiply by P the tile holds Recip / s2d, which is where the STEM
+// detectors, the diffraction pattern and the CTEM image are read (times s2d).
+#pragma once
+
+#include "fft.cuh"
+
+namespace ms {
+
+constexpr int kMaxDetectors = 16;
+
+template <class R>
+struct PropTables {
+    const cplx<R> *px;   // res: exp(-i pi dz (kx+bx)^2/kz) * f * exp(i pi dz (k^2-kz^2)/kz)
+    const cplx<R> *py;   // res: exp(-i pi dz (ky+by)^2/kz)
+    const double *kx2;   // res: kx*kx (FP64, the reference's k0x)
+    const double *ky2;   // res: ky*ky
+    double kmax2;        // (k_max * limit_factor)^2 of the propagator's strict cut (propagator_d.cl:34-36)
+};
+
+struct DetArgs {
+    const uint16_t *mask;   // res*res bit masks of the detectors, unshifted k-space pixel order
+    int n_det;
+    double *partials;       // [batch][n_det][gridDim.x]
+};
+
+template <int N, class R> struct RowCfg {
+    static constexpr int ROWS = N <= 128 ? 8 : (N <= 256 ? 8 : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1)));
+    static_assert(N % ROWS == 0, "row tile must divide the grid");
+    static_assert(Plan<N>::NT * ROWS <= 1024, "row block too large");
+    static constexpr int THREADS = Plan<N>::NT * ROWS;
+    static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(N + ROWS * RowAddr::size(N)); }
+};
+__host__ __device__ constexpr int floor_pow2(int v) { return v < 2 ? 1 : 2 * floor_pow2(v / 2); }
+// Columns per tile: a power of two (it must divide N) keeping the tile at <= 64 KB.
+template <int N, class R> struct ColCfg {
+    static constexpr int base = (sizeof(R) == 4) ? 8192 : 4096;
+    static constexpr int c0 = base / N;
+    static constexpr int COLS = c0 > 16 ? 16 : floor_pow2(c0 < 1 ? 1 : c0);
+    static_assert(N % COLS == 0, "column tile must divide the grid");
+    static constexpr int THREADS = Plan<N>::NT * COLS;
+    static_assert(THREADS <= 1024, "column block too large");
+    static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(N + N * COLS); }
+};
+
+template <class R, int N>
+__device__ __forceinline__ void load_twiddles(cplx<R> *tw, const cplx<R> *__restrict__ twg, int tid, int nthreads) {
+    for (int i = tid; i < N; i += nthreads) tw[i] = twg[i];
+}
+
+// ------------------------------------------------------------------------------------------------
+// Row kernels: grid (res/ROWS, batch), block (NT, ROWS)
+// ------------------------------------------------------------------------------------------------
+// The multislice row pass: phi <- D_r(T * a * Dinv_r phi)
+template <class R, int N>
+__global__ void __launch_bounds__(RowCfg<N, R>::THREADS)
+k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const cplx<R> *__restrict__ twg, R a) {
+    using P = Plan<N>;
+    constexpr int ROWS = RowCfg<N, R>::ROWS;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tw + N + threadIdx.y * RowAddr::size(N);
+    const int t = threadIdx.x;
+    load_twiddles<R, N>(tw, twg, t + threadIdx.y * P::NT, P::NT * ROWS);
+    const int y = blockIdx.x * ROWS + threadIdx.y;
+    cplx<R> *row = wave + (size_t)blockIdx.y * N * N + (size_t)y * N;
+    const cplx<R> *trow = trans + (size_t)y * N;
+    cplx<R> v[P::E];
+#pragma unroll
+    for (int m = 0; m < P::E; m++) v[m] = row[t + m * P::NT];
+    __syncthreads();
+    fft<R, N, +1>(v, sm, RowAddr(), t, tw);
+#pragma unroll
+    for (int m = 0; m < P::E; m++) v[m] = cscale(cmul(v[m], trow[t + m * P::NT]), a);
+    fft<R, N, -1>(v, sm, RowAddr(), t, tw);
+#pragma unroll
+    for (int m = 0; m < P::E; m++) row[t + m * P::NT] = v[m];
+}
+
+// A plain row transform (SIGN -1 forward, +1 inverse), scaled, in or out of place.
+template <class R, int N, int SIGN>
+__global__ void __launch_bounds__(RowCfg<N, R>::THREADS)
+k_row_fft(const cplx<R> *in, cplx<R> *out, const cplx<R> *__restrict__ twg, R scale) {
+    using P = Plan<N>;
+    constexpr int ROWS = RowCfg<N, R>::ROWS;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tw + N + threadIdx.y * RowAddr::size(N);
+    const int t = threadIdx.x;
+    load_twiddles<R, N>(tw, twg, t + threadIdx.y * P::NT, P::NT * ROWS);
+    const int y = blockIdx.x * ROWS + threadIdx.y;
+    const size_t off = (size_t)blockIdx.y * N * N + (size_t)y * N;
+    cplx<R> v[P::E];
+#pragma unroll
+    for (int m = 0; m < P::E; m++) v[m] = in[off + t + m * P::NT];
+    __syncthreads();
+    fft<R, N, SIGN>(v, sm, RowAddr(), t, tw);
+#pragma unroll
+    for (int m = 0; m < P::E; m++) out[off + t + m * P::NT] = cscale(v[m], scale);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Column kernels: grid (res/COLS, batch), block (COLS, NT)
+// ------------------------------------------------------------------------------------------------
+template <class R, int N>
+__device__ __forceinline__ void col_load(cplx<R> (&v)[Plan<N>::E], const cplx<R> *base, int x, int t) {
+#pragma unroll
+    for (int m = 0; m < Plan<N>::E; m++) v[m] = base[(size_t)(t + m * Plan<N>::NT) * N + x];
+}
+template <class R, int N>
+__device__ __forceinline__ void col_store(const cplx<R> (&v)[Plan<N>::E], cplx<R> *base, int x, int t) {
+#pragma unroll
+    for (int m = 0; m < Plan<N>::E; m++) base[(size_t)(t + m * Plan<N>::NT) * N + x] = v[m];
+}
+
+// Block-wide sum of one double per thread; the result is valid in thread 0. red: >= 32 doubles.
+__device__ __forceinline__ double block_sum(double v, double *red) {
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int nw = (blockDim.x * blockDim.y + 31) / 32;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((tid & 31) == 0) red[tid >> 5] = v;
+    __syncthreads();
+    double s = 0;
+    if (tid == 0)
+        for (int w = 0; w < nw; w++) s += red[w];
+    return s;
+}
+
+enum ColMode { COL_STEP = 0, COL_STEP_DET = 1, COL_DET_ONLY = 2 };
+
+// The multislice column pass: D_c, * P (strict cut), [detectors / Recip copy], * b, Dinv_c.
+template <class R, int N, int MODE>
+__global__ void __launch_bounds__(ColCfg<N, R>::THREADS)
+k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTables<R> pt, R bscale, R det_scale,
+           DetArgs det, cplx<R> *__restrict__ recip_out) {
+    using P = Plan<N>;
+    constexpr int COLS = ColCfg<N, R>::COLS;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double red[32];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tw + N + threadIdx.x;
+    const int c = threadIdx.x, t = threadIdx.y;
+    load_twiddles<R, N>(tw, twg, c + t * COLS, COLS * P::NT);
+    const int x = blockIdx.x * COLS + c;
+    cplx<R> *base = wave + (size_t)blockIdx.y * N * N;
+    cplx<R> v[P::E];
+    col_load<R, N>(v, base, x, t);
+    __syncthreads();
+    fft<R, N, -1>(v, sm, ColAddr<COLS>(), t, tw);
+    const cplx<R> pxx = pt.px[x];
+    const double kx2 = pt.kx2[x];
+#pragma unroll
+    for (int m = 0; m < P::E; m++) {
+        const int y = t + m * P::NT;
+        cplx<R> p = (kx2 + pt.ky2[y] < pt.kmax2) ? cmul(pxx, pt.py[y]) : mk<R>(0, 0);
+        v[m] = cmul(v[m], p);
+    }
+    if constexpr (MODE == COL_STEP_DET || MODE == COL_DET_ONLY) {
+        if (det.n_det > 0) {
+            double e[P::E];
+            uint16_t mk_[P::E];
+#pragma unroll
+            for (int m = 0; m < P::E; m++) {
+                const int y = t + m * P::NT;
+                double re = (double)v[m].x * (double)det_scale, im = (double)v[m].y * (double)det_scale;
+                e[m] = re * re + im * im;
+                mk_[m] = det.mask[(size_t)y * N + x];
+            }
+            for (int d = 0; d < det.n_det; d++) {
+                double acc = 0;
+#pragma unroll
+                for (int m = 0; m < P::E; m++) acc += ((mk_[m] >> d) & 1) ? e[m] : 0.0;
+                double s = block_sum(acc, red);
+                if (c == 0 && t == 0) det.partials[((size_t)blockIdx.y * det.n_det + d) * gridDim.x + blockIdx.x] = s;
+            }
+        }
+        if (recip_out) {
+            cplx<R> *rb = recip_out + (size_t)blockIdx.y * N * N;
+#pragma unroll
+            for (int m = 0; m < P::E; m++) rb[(size_t)(t + m * P::NT) * N + x] = cscale(v[m], det_scale);
+        }
+    }
+    if constexpr (MODE != COL_DET_ONLY) {
+#pragma unroll
+        for (int m = 0; m < P::E; m++) v[m] = cscale(v[m], bscale);
+        fft<R, N, +1>(v, sm, ColAddr<COLS>(), t, tw);
+        col_store<R, N>(v, base, x, t);
+    }
+}
+
+// A plain column transform, scaled, in or out of place.
+template <class R, int N, int SIGN>
+__global__ void __launch_bounds__(ColCfg<N, R>::THREADS)
+k_col_fft(const cplx<R> *in, cplx<R> *out, const cplx<R> *__restrict__ twg, R scale) {
+    using P = Plan<N>;
+    constexpr int COLS = ColCfg<N, R>::COLS;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tw + N + threadIdx.x;
+    const int c = threadIdx.x, t = threadIdx.y;
+    load_twiddles<R, N>(tw, twg, c + t * COLS, COLS * P::NT);
+    const int x = blockIdx.x * COLS + c;
+    const size_t off = (size_t)blockIdx.y * N * N;
+    cplx<R> v[P::E];
+    col_load<R, N>(v, in + off, x, t);
+    __syncthreads();
+    fft<R, N, SIGN>(v, sm, ColAddr<COLS>(), t, tw);
+#pragma unroll
+    for (int m = 0; m < P::E; m++) v[m] = cscale(v[m], scale);
+    col_store<R, N>(v, out + off, x, t);
+}
+
+// Transmission band limit (simulationgeneral.cpp:596-602, band_limit_d.cl:13-32) on row-transformed
+// slices: D_c, keep sqrt(kx^2+ky^2) <= lim (inclusive) times scale, Dinv_c.
+template <class R, int N>
+__global__ void __launch_bounds__(ColCfg<N, R>::THREADS)
+k_col_bandlimit(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, const double *__restrict__ kx2,
+                const double *__restrict__ ky2, double lim, R scale) {
+    using P = Plan<N>;
+    constexpr int COLS = ColCfg<N, R>::COLS;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tw + N + threadIdx.x;
+    const int c = threadIdx.x, t = threadIdx.y;
+    load_twiddles<R, N>(tw, twg, c + t * COLS, COLS * P::NT);
+    const int x = blockIdx.x * COLS + c;
+    cplx<R> *base = wave + (size_t)blockIdx.y * N * N;
+    cplx<R> v[P::E];
+    col_load<R, N>(v, base, x, t);
+    __syncthreads();
+    fft<R, N, -1>(v, sm, ColAddr<COLS>(), t, tw);
+    const double k2x = kx2[x];
+#pragma unroll
+    for (int m = 0; m < P::E; m++) {
+        double k = sqrt(k2x + ky2[t + m * P::NT]);
+        v[m] = cscale(v[m], (k <= lim) ? scale : (R)0);
+    }
+    fft<R, N, +1>(v, sm, ColAddr<COLS>(), t, tw);
+    col_store<R, N>(v, base, x, t);
+}
+
+// Probe initialisation (init_probe_wave_d.cl:49-118 then the column half of the IFFT,
+// simulationcbed.cpp:91-99): generate the reciprocal-space probe of each wave of the batch, Dinv_c,
+// scale. chi[y*N+x] = (chi(k), inside-aperture flag) in FP64; pos[b] = probe position relative to the
+// simulation start (Å). The phase -2 pi (kx px + ky py) - chi is formed in FP64.
+template <class R, int N>
+__global__ void __launch_bounds__(ColCfg<N, R>::THREADS)
+k_col_probe(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, const double2 *__restrict__ chi,
+            const double *__restrict__ kx, const double *__restrict__ ky, const double2 *__restrict__ pos, R scale) {
+    using P = Plan<N>;
+    constexpr int COLS = ColCfg<N, R>::COLS;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tw + N + threadIdx.x;
+    const int c = threadIdx.x, t = threadIdx.y;
+    load_twiddles<R, N>(tw, twg, c + t * COLS, COLS * P::NT);
+    const int x = blockIdx.x * COLS + c;
+    const double2 pp = pos[blockIdx.y];
+    const double kxx = kx[x];
+    cplx<R> v[P::E];
+#pragma unroll
+    for (int m = 0; m < P::E; m++) {
+        const int y = t + m * P::NT;
+        const double2 ch = chi[(size_t)y * N + x];
+        if (ch.y != 0.0) {
+            double posTerm = 2.0 * M_PI * (kxx * pp.x + ky[y] * pp.y);
+            double arg = -posTerm - ch.x;
+            if constexpr (sizeof(R) == 8) {
+                v[m] = mk<R>((R)cos(arg), (R)sin(arg));
+            } else {
+                double red = arg - 6.283185307179586232 * rint(arg * 0.15915494309189534561);
+                float s, co;
+                sincosf((float)red, &s, &co);
+                v[m] = mk<R>((R)co, (R)s);
+            }
+        } else {
+            v[m] = mk<R>(0, 0);
+        }
+    }
+    __syncthreads();
+    fft<R, N, +1>(v, sm, ColAddr<COLS>(), t, tw);
+#pragma unroll
+    for (int m = 0; m < P::E; m++) v[m] = cscale(v[m], scale);
+    col_store<R, N>(v, wave + (size_t)blockIdx.y * N * N, x, t);
+}
+
+}  // namespace ms

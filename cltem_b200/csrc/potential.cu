@@ -1,0 +1,32 @@
+// potential.cu — launchers of the slice-potential kernels for one precision (compiled per MS_REAL;
+// the FP64 build uses -fmad=false so the _d statements are not contracted).
+#include "potential.cuh"
+#include "potential_launch.h"
+
+#ifndef MS_REAL
+#error "MS_REAL must be defined"
+#endif
+
+namespace ms {
+
+template <>
+void launch_potential<MS_REAL>(cudaStream_t s, bool full3d, cplx<MS_REAL> *out, int n_slices, const double *ax,
+                               const double *ay, const double *az, const int *aZ, const int *block_start,
+                               const MS_REAL *prm, const PotParams &p) {
+    using T = MS_REAL;
+    if (p.width % 16 || p.height % 16) throw std::runtime_error("potential grid must be a multiple of 16");
+    dim3 blk(16, 16), grd(p.width / 16, p.height / 16, n_slices);
+    if (n_slices <= 0) return;
+    if (full3d) {
+        if (p.form == 0) k_potential_3d<T, 0><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
+        else if (p.form == 1) k_potential_3d<T, 1><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
+        else k_potential_3d<T, 2><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
+    } else {
+        if (p.form == 0) k_potential_projected<T, 0><<<grd, blk, 0, s>>>(out, ax, ay, aZ, block_start, prm, p);
+        else if (p.form == 1) k_potential_projected<T, 1><<<grd, blk, 0, s>>>(out, ax, ay, aZ, block_start, prm, p);
+        else k_potential_projected<T, 2><<<grd, blk, 0, s>>>(out, ax, ay, aZ, block_start, prm, p);
+    }
+    MS_CUDA(cudaGetLastError());
+}
+
+}  // namespace ms

@@ -1,0 +1,307 @@
+// potential.cuh — slice transmission functions from binned atoms.
+//
+// One 16x16 thread block per 16x16 pixel tile and one grid z-layer per slice. The bin ranges a tile
+// reads are the reference's (transmission_potentials_projected_d.cl:227-246), so the set of atoms each
+// pixel sums is identical; the atoms of a bin row are staged through shared memory in chunks of 256
+// (the reference's single 256-atom __local load overflows for longer rows, :264-268; chunking keeps
+// every atom). T = cos(sigma V) + i sin(sigma V).
+//
+// FP64 instantiation: the reference's _d statements in the same order (this translation unit is built
+// with -fmad=false). FP32 instantiation: pixel-to-atom offsets in FP64, the potential sum in FP32.
+#pragma once
+
+#include "common.cuh"
+
+namespace ms {
+
+struct PotParams {
+    int width, height, total_slices, slice0;
+    double dz, pixelscale;
+    int blocks_x, blocks_y;
+    double max_x, min_x, max_y, min_y;
+    int load_x, load_y, load_z;
+    double sigma, startx, starty;
+    double beam_theta_mrad, beam_phi;   // projected: tilt
+    double z0;                          // full 3-D: padded z minimum; current_z = z0 + (S - k) dz
+    double shift_x, shift_y;            // full 3-D: per-sub-slice tilt shift
+    int integrals;
+    int form, i_count;
+};
+
+__constant__ double c_k0pi[5] = {1.0, 2.346487949187396e-1, 1.187082088663404e-2, 2.150707366040937e-4, 1.425433617130587e-6};
+__constant__ double c_k0qi[3] = {9.847324170755358e-1, 1.518396076767770e-2, 8.362215678646257e-5};
+__constant__ double c_k0p[5] = {1.159315156584126e-1, 2.770731240515333e-1, 2.066458134619875e-2, 4.574734709978264e-4, 3.454715527986737e-6};
+__constant__ double c_k0q[3] = {9.836249671709183e-1, 1.627693622304549e-2, 9.809660603621949e-5};
+__constant__ double c_k0pp[8] = {1.253314137315499, 1.475731032429900e1, 6.123767403223466e1, 1.121012633939949e2,
+                                 9.285288485892228e1, 3.198289277679660e1, 3.595376024148513, 6.160228690102976e-2};
+__constant__ double c_k0qq[8] = {1.0, 1.189963006673403e1, 5.027773590829784e1, 9.496513373427093e1,
+                                 8.318077493230258e1, 3.181399777449301e1, 4.443672926432041, 1.408295601966600e-1};
+__constant__ double c_k1pi[5] = {0.5, 5.598072040178741e-2, 1.818666382168295e-3, 2.397509908859959e-5, 1.239567816344855e-7};
+__constant__ double c_k1qi[3] = {9.870202601341150e-1, 1.292092053534579e-2, 5.881933053917096e-5};
+__constant__ double c_k1p[5] = {-3.079657578292062e-1, -8.109417631822442e-2, -3.477550948593604e-3, -5.385594871975406e-5, -3.110372465429008e-7};
+__constant__ double c_k1q[3] = {9.861813171751389e-1, 1.375094061153160e-2, 6.774221332947002e-5};
+__constant__ double c_k1pp[8] = {1.253314137315502, 1.457171340220454e1, 6.063161173098803e1, 1.147386690867892e2,
+                                 1.040442011439181e2, 4.356596656837691e1, 7.265230396353690, 3.144418558991021e-1};
+__constant__ double c_k1qq[8] = {1.0, 1.125154514806458e1, 4.427488496597630e1, 7.616113213117645e1,
+                                 5.863377227890893e1, 1.850303673841586e1, 1.857244676566022, 2.538540887654872e-2};
+
+template <class T> __device__ __forceinline__ T dpoly(const double *cof, int n, T x) {
+    T ans = (T)cof[n];
+    for (int i = n - 1; i >= 0; --i) ans = ans * x + (T)cof[i];
+    return ans;
+}
+__device__ __forceinline__ float flog(float x) { return logf(x); }
+__device__ __forceinline__ double flog(double x) { return log(x); }
+__device__ __forceinline__ float fexp(float x) { return expf(x); }
+__device__ __forceinline__ double fexp(double x) { return exp(x); }
+__device__ __forceinline__ float fsqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double fsqrt(double x) { return sqrt(x); }
+
+// Modified Bessel functions K0 / K1: Numerical Recipes in C 2nd ed. section 6.6 rational
+// approximations with the coefficients the reference uses (projected_d.cl:57-102).
+template <class T> __device__ __forceinline__ T bessk0(T x) {
+    T ax = fabs(x);
+    if (ax > (T)0 && ax <= (T)1) {
+        T z = x * x;
+        T term = dpoly<T>(c_k0pi, 4, z) * flog(x) * ((T)1 / dpoly<T>(c_k0qi, 2, (T)1 - z));
+        return dpoly<T>(c_k0p, 4, z) * ((T)1 / dpoly<T>(c_k0q, 2, (T)1 - z)) - term;
+    } else if (ax > (T)1) {
+        T z = (T)1 / x;
+        return fexp(-x) * dpoly<T>(c_k0pp, 7, z) * ((T)1 / dpoly<T>(c_k0qq, 7, z)) * ((T)1 / fsqrt(x));
+    }
+    return (T)1.79769313486231570815e+308;
+}
+template <class T> __device__ __forceinline__ T bessk1(T x) {
+    T ax = fabs(x);
+    if (ax > (T)0 && ax <= (T)1) {
+        T z = x * x;
+        T term = dpoly<T>(c_k1pi, 4, z) * flog(x) * ((T)1 / dpoly<T>(c_k1qi, 2, (T)1 - z));
+        return x * (dpoly<T>(c_k1p, 4, z) * ((T)1 / dpoly<T>(c_k1q, 2, (T)1 - z)) + term) + (T)1 / x;
+    } else if (ax > (T)1) {
+        T z = (T)1 / x;
+        return fexp(-x) * dpoly<T>(c_k1pp, 7, z) * ((T)1 / dpoly<T>(c_k1qq, 7, z)) * ((T)1 / fsqrt(x));
+    }
+    return (T)1.79769313486231570815e+308;
+}
+
+// Projected potentials (projected_d.cl:104-181): Kirkland eq. C.20, Peng (integrated), Lobato eq. 16.
+template <class T> __device__ __forceinline__ T kirkland_p(const T *__restrict__ prm, int i_lim, int Z, T rad) {
+    T suml = 0, sumg = 0;
+    const T *p = prm + (Z - 1) * 12;
+    T x = (T)(2.0 * M_PI) * rad;
+    for (int i = 0; i < i_lim * 2; i += 2) suml += p[i] * bessk0<T>(x * fsqrt(p[i + 1]));
+    x = (T)M_PI * rad;
+    x = x * x;
+    for (int i = i_lim * 2; i < i_lim * 4; i += 2) {
+        T d_inv = (T)1 / p[i + 1];
+        sumg += (p[i] * d_inv) * fexp(-x * d_inv);
+    }
+    return (T)300.8242834 * suml + (T)150.4121417 * sumg;
+}
+template <class T> __device__ __forceinline__ T lobato_p(const T *__restrict__ prm, int i_lim, int Z, T rad) {
+    T sum = 0;
+    const T *p = prm + (Z - 1) * 10;
+    T x = (T)(2.0 * M_PI) * rad;
+    for (int i = 0; i < i_lim; ++i) {
+        T b_inv_root = (T)1 / fsqrt(p[i + 5]);
+        sum += p[i] * (b_inv_root * b_inv_root * b_inv_root) * (bessk0<T>(x * b_inv_root) + rad * bessk1<T>(x * b_inv_root));
+    }
+    return (T)945.090144399935 * sum;
+}
+template <class T> __device__ __forceinline__ T peng_p(const T *__restrict__ prm, int i_lim, int Z, T rad) {
+    T sum = 0;
+    const T *p = prm + (Z - 1) * 10;
+    T x = (T)M_PI * rad;
+    x = x * x;
+    for (int i = 0; i < i_lim; ++i) {
+        T b_inv = (T)1 / p[i + 5];
+        sum += p[i] * b_inv * fexp(-x * b_inv);
+    }
+    return (T)150.4121417 * sum;
+}
+// Full 3-D potentials (full_3d_d.cl:57-134): Kirkland eq. C.19, Peng, Lobato.
+template <class T> __device__ __forceinline__ T kirkland_3(const T *__restrict__ prm, int i_lim, int Z, T rad) {
+    T suml = 0, sumg = 0;
+    const T *p = prm + (Z - 1) * 12;
+    T x = (T)(2.0 * M_PI) * rad;
+    for (int i = 0; i < i_lim * 2; i += 2) suml += p[i] * fexp(-x * fsqrt(p[i + 1]));
+    x = (T)M_PI * rad;
+    x = x * x;
+    for (int i = i_lim * 2; i < i_lim * 4; i += 2) {
+        T d_inv_root = (T)1 / fsqrt(p[i + 1]);
+        sumg += p[i] * (d_inv_root * d_inv_root * d_inv_root) * fexp(-x * ((T)1 / p[i + 1]));
+    }
+    return (T)150.4121417 * ((T)1 / rad) * suml + (T)266.5157269 * sumg;
+}
+template <class T> __device__ __forceinline__ T lobato_3(const T *__restrict__ prm, int i_lim, int Z, T rad) {
+    T sum = 0;
+    const T *p = prm + (Z - 1) * 10;
+    T x = (T)M_PI * rad;
+    for (int i = 0; i < i_lim; ++i) {
+        T b = p[i + 5];
+        T b_inv_root = (T)1 / fsqrt(b);
+        sum += p[i] * (b_inv_root * b_inv_root * b_inv_root) * fexp((T)-2.0 * x * b_inv_root) * (fsqrt(b) * ((T)1 / x) + (T)1);
+    }
+    return (T)472.545072199968 * sum;
+}
+template <class T> __device__ __forceinline__ T peng_3(const T *__restrict__ prm, int i_lim, int Z, T rad) {
+    T sum = 0;
+    const T *p = prm + (Z - 1) * 10;
+    T x = (T)M_PI * rad;
+    x = x * x;
+    for (int i = 0; i < i_lim; ++i) {
+        T b = p[i + 5];
+        T b_inv_root = (T)1 / fsqrt(b);
+        sum += p[i] * (b_inv_root * b_inv_root * b_inv_root) * fexp(-x * ((T)1 / b));
+    }
+    return (T)266.5157269 * sum;
+}
+
+// Bin range of a 16x16 tile, in FP64 exactly as the reference (projected_d.cl:227-246)
+__device__ __forceinline__ void tile_bins(const PotParams &p, int gx, int gy, int &si, int &ei, int &sj, int &ej) {
+    double group_size_x = 16 * p.pixelscale, group_size_y = 16 * p.pixelscale;
+    double group_start_x = p.startx + gx * group_size_x;
+    double group_end_x = group_start_x + group_size_x;
+    double group_start_y = p.starty + gy * group_size_y;
+    double group_end_y = group_start_y + group_size_y;
+    double recip_range_x = 1.0 / (p.max_x - p.min_x);
+    double recip_range_y = 1.0 / (p.max_y - p.min_y);
+    si = (int)fmax(floor(p.blocks_x * (group_start_x - p.min_x) * recip_range_x) - p.load_x, 0.0);
+    ei = (int)fmin(ceil(p.blocks_x * (group_end_x - p.min_x) * recip_range_x) + p.load_x, (double)(p.blocks_x - 1));
+    sj = (int)fmax(floor(p.blocks_y * (group_start_y - p.min_y) * recip_range_y) - p.load_y, 0.0);
+    ej = (int)fmin(ceil(p.blocks_y * (group_end_y - p.min_y) * recip_range_y) + p.load_y, (double)(p.blocks_y - 1));
+}
+
+template <class T> __device__ __forceinline__ void write_trans(cplx<T> *o, T phase);
+template <> __device__ __forceinline__ void write_trans<float>(float2 *o, float phase) {
+    float s, c;
+    sincosf(phase, &s, &c);
+    *o = make_float2(c, s);
+}
+template <> __device__ __forceinline__ void write_trans<double>(double2 *o, double phase) {
+    *o = make_double2(cos(phase), sin(phase));
+}
+
+constexpr int kAtomChunk = 256;
+
+// transmission_potentials_projected: grid (W/16, H/16, n_slices), block (16, 16)
+template <class T, int FORM>
+__global__ void __launch_bounds__(256)
+k_potential_projected(cplx<T> *__restrict__ out, const double *__restrict__ ax, const double *__restrict__ ay,
+                      const int *__restrict__ aZ, const int *__restrict__ block_start, const T *__restrict__ prm,
+                      PotParams p) {
+    __shared__ double sx[kAtomChunk], sy[kAtomChunk];
+    __shared__ int sZ[kAtomChunk];
+    const int lid = threadIdx.x + 16 * threadIdx.y;
+    const int xid = blockIdx.x * 16 + threadIdx.x, yid = blockIdx.y * 16 + threadIdx.y;
+    const int slice = blockIdx.z + p.slice0;
+    int si, ei, sj, ej;
+    tile_bins(p, blockIdx.x, blockIdx.y, si, ei, sj, ej);
+    int k = slice;
+    if (k < 0) k = 0;
+    if (k >= p.total_slices) k = p.total_slices - 1;
+    // tilt geometry, constant per launch (projected_d.cl:221, 283-289)
+    const double beam_theta = M_PI_2 - p.beam_theta_mrad * 0.001;
+    const double cos_beam_phi = cos(p.beam_phi), sin_beam_phi = sin(p.beam_phi);
+    const double sin_beam_2theta = sin(2.0 * beam_theta);
+    const double tan_beam_theta = tan(beam_theta);
+    const double im_pos_x = p.startx + xid * p.pixelscale;
+    const double im_pos_y = p.starty + yid * p.pixelscale;
+    const double r_min = 0.25 * p.pixelscale;
+    T sumz = 0;
+    const size_t nb = (size_t)p.blocks_x * p.blocks_y;
+    for (int j = sj; j <= ej; j++) {
+        const int start = block_start[k * nb + p.blocks_x * j + si];
+        const int end = block_start[k * nb + p.blocks_x * j + ei + 1];
+        for (int c0 = start; c0 < end; c0 += kAtomChunk) {
+            const int cn = min(kAtomChunk, end - c0);
+            __syncthreads();
+            if (lid < cn) { sx[lid] = ax[c0 + lid]; sy[lid] = ay[c0 + lid]; sZ[lid] = aZ[c0 + lid]; }
+            __syncthreads();
+            for (int l = 0; l < cn; l++) {
+                double rad_x = im_pos_x - sx[l];
+                double rad_y = im_pos_y - sy[l];
+                double z_prime = -0.5 * (rad_x * cos_beam_phi + rad_y * sin_beam_phi) * sin_beam_2theta;
+                double z_by_tan_beam_theta = z_prime / tan_beam_theta;
+                double x_prime = rad_x + z_by_tan_beam_theta * cos_beam_phi;
+                double y_prime = rad_y + z_by_tan_beam_theta * sin_beam_phi;
+                double rad_d = sqrt(z_prime * z_prime + x_prime * x_prime + y_prime * y_prime);
+                if (rad_d < r_min) rad_d = r_min;
+                if (rad_d <= 8.0) {
+                    const T rad = (T)rad_d;
+                    if constexpr (FORM == 0) sumz += kirkland_p<T>(prm, p.i_count, sZ[l], rad);
+                    else if constexpr (FORM == 1) sumz += peng_p<T>(prm, p.i_count, sZ[l], rad);
+                    else sumz += lobato_p<T>(prm, p.i_count, sZ[l], rad);
+                }
+            }
+        }
+    }
+    if (xid < p.width && yid < p.height)
+        write_trans<T>(out + (size_t)blockIdx.z * p.width * p.height + (size_t)yid * p.width + xid, (T)p.sigma * sumz);
+}
+
+// transmission_potentials_full_3d: grid (W/16, H/16, n_slices), block (16, 16)
+template <class T, int FORM>
+__global__ void __launch_bounds__(256)
+k_potential_3d(cplx<T> *__restrict__ out, const double *__restrict__ ax, const double *__restrict__ ay,
+               const double *__restrict__ az, const int *__restrict__ aZ, const int *__restrict__ block_start,
+               const T *__restrict__ prm, PotParams p) {
+    __shared__ double sx[kAtomChunk], sy[kAtomChunk], sz[kAtomChunk];
+    __shared__ int sZ[kAtomChunk];
+    const int lid = threadIdx.x + 16 * threadIdx.y;
+    const int xid = blockIdx.x * 16 + threadIdx.x, yid = blockIdx.y * 16 + threadIdx.y;
+    const int slice = blockIdx.z + p.slice0;
+    int si, ei, sj, ej;
+    tile_bins(p, blockIdx.x, blockIdx.y, si, ei, sj, ej);
+    int topz = slice - p.load_z, bottomz = slice + p.load_z;
+    const double int_r = 1.0 / p.integrals;
+    const double sub_slice_thickness = p.dz * int_r;
+    if (topz < 0) topz = 0;
+    if (bottomz >= p.total_slices) bottomz = p.total_slices - 1;
+    const double current_z = p.z0 + (p.total_slices - slice) * p.dz;   // simulationgeneral.cpp:590
+    const double im_pos_x = p.startx + xid * p.pixelscale;
+    const double im_pos_y = p.starty + yid * p.pixelscale;
+    const double r_min = 0.25 * p.pixelscale;
+    T sumz = 0;
+    const size_t nb = (size_t)p.blocks_x * p.blocks_y;
+    for (int k = topz; k <= bottomz; k++) {
+        for (int j = sj; j <= ej; j++) {
+            const int start = block_start[k * nb + p.blocks_x * j + si];
+            const int end = block_start[k * nb + p.blocks_x * j + ei + 1];
+            T p2 = 0;
+            for (int c0 = start; c0 < end; c0 += kAtomChunk) {
+                const int cn = min(kAtomChunk, end - c0);
+                __syncthreads();
+                if (lid < cn) { sx[lid] = ax[c0 + lid]; sy[lid] = ay[c0 + lid]; sz[lid] = az[c0 + lid]; sZ[lid] = aZ[c0 + lid]; }
+                __syncthreads();
+                for (int l = 0; l < cn; l++) {
+                    double rad_x = im_pos_x - sx[l];
+                    double rad_y = im_pos_y - sy[l];
+                    for (int h = 0; h <= p.integrals; h++) {
+                        rad_x -= p.shift_x;   // cumulative (full_3d_d.cl:244-246)
+                        rad_y -= p.shift_y;
+                        double xyrad2 = rad_x * rad_x + rad_y * rad_y;
+                        double im_pos_z = current_z - h * p.dz * int_r;
+                        double rad_z = im_pos_z - sz[l];
+                        double rad_d = sqrt(xyrad2 + rad_z * rad_z);
+                        if (rad_d < r_min) rad_d = r_min;
+                        if (xyrad2 <= 64.0 && rad_z <= 3.0) {
+                            const T rad = (T)rad_d;
+                            T p1;
+                            if constexpr (FORM == 0) p1 = kirkland_3<T>(prm, p.i_count, sZ[l], rad);
+                            else if constexpr (FORM == 1) p1 = peng_3<T>(prm, p.i_count, sZ[l], rad);
+                            else p1 = lobato_3<T>(prm, p.i_count, sZ[l], rad);
+                            sumz += (h != 0) * (p1 + p2) * (T)0.5;
+                            p2 = p1;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (xid < p.width && yid < p.height)
+        write_trans<T>(out + (size_t)blockIdx.z * p.width * p.height + (size_t)yid * p.width + xid,
+                       (T)(sub_slice_thickness * p.sigma) * sumz);
+}
+
+}  // namespace ms

@@ -1,0 +1,186 @@
+"""Structures: .xyz reading, structure limits, seeded synthetic supercells and frozen-phonon configs.
+
+- read_xyz follows CrystalStructure::openXyz (src/simulation/structure/crystalstructure.cpp:44-188):
+  line 1 atom count, line 2 column headers (A x y z [occ] [u] [u1 u2 u3], optional "nm" scale flag),
+  coordinates parsed with std::stof (single precision) and widened to double.
+- limits follow CrystalStructure::updateLimits/resetLimits (crystalstructure.cpp:238-267), including
+  the reference's initial max of DBL_MIN (so an all-negative structure keeps max = DBL_MIN).
+- Frozen-phonon displacements follow PhononScattering::generateTdsFactor
+  (src/simulation/incoherence/inelastic/phonon.cpp:98-128): sqrt(u^2) * N(0,1) per axis along the
+  u1/u2/u3 axes (identity for .xyz input, simulationgeneral.cpp:177-205). The reference seeds its RNG
+  from the wall clock; here every configuration has an explicit seed.
+"""
+from dataclasses import dataclass, field
+import math
+
+import numpy as np
+
+ELEMENTS = [
+    "H", "He", "Li", "Be", "B", "C", "N", "O", "F", "Ne", "Na", "Mg", "Al", "Si", "P", "S", "Cl", "Ar", "K", "Ca",
+    "Sc", "Ti", "V", "Cr", "Mn", "Fe", "Co", "Ni", "Cu", "Zn", "Ga", "Ge", "As", "Se", "Br", "Kr", "Rb", "Sr", "Y",
+    "Zr", "Nb", "Mo", "Tc", "Ru", "Rh", "Pd", "Ag", "Cd", "In", "Sn", "Sb", "Te", "I", "Xe", "Cs", "Ba", "La", "Ce",
+    "Pr", "Nd", "Pm", "Sm", "Eu", "Gd", "Tb", "Dy", "Ho", "Er", "Tm", "Yb", "Lu", "Hf", "Ta", "W", "Re", "Os", "Ir",
+    "Pt", "Au", "Hg", "Tl", "Pb", "Bi", "Po", "At", "Rn", "Fr", "Ra", "Ac", "Th", "Pa", "U", "Np", "Pu", "Am", "Cm",
+    "Bk", "Cf", "Es", "Fm", "Md", "No", "Lr",
+]
+
+
+def symbol_to_z(sym: str) -> int:
+    s = sym.strip()
+    if s.isdigit():
+        return int(s)
+    s = s[:1].upper() + s[1:].lower()
+    if s not in ELEMENTS:
+        raise RuntimeError("Unknown element symbol: " + sym)
+    return ELEMENTS.index(s) + 1
+
+
+@dataclass
+class Structure:
+    Z: np.ndarray          # int32[n]
+    x: np.ndarray          # float64[n], Å
+    y: np.ndarray
+    z: np.ndarray
+    u2: np.ndarray = None  # optional per-atom mean-square displacement (Å^2) per axis, float64[n,3]
+    name: str = ""
+    extra: dict = field(default_factory=dict)
+
+    def __len__(self):
+        return int(self.Z.shape[0])
+
+    def limits(self):
+        """[min_x, max_x, min_y, max_y, min_z, max_z] as CrystalStructure leaves them."""
+        tiny = np.finfo(np.float64).tiny  # std::numeric_limits<double>::min()
+        big = np.finfo(np.float64).max
+        if len(self) == 0:
+            return [big, tiny, big, tiny, big, tiny]
+        return [min(big, float(self.x.min())), max(tiny, float(self.x.max())),
+                min(big, float(self.y.min())), max(tiny, float(self.y.max())),
+                min(big, float(self.z.min())), max(tiny, float(self.z.max()))]
+
+
+def _stof(s: str) -> float:
+    return float(np.float32(float(s)))
+
+
+def read_xyz(path: str) -> Structure:
+    with open(path, "r") as f:
+        lines = f.read().splitlines()
+    try:
+        n = int(lines[0].strip())
+    except Exception as e:  # noqa: BLE001
+        raise RuntimeError(f"Could not parse number of atoms (line 1, {e}).")
+    headers = lines[1].split() if len(lines) > 1 else []
+    scale = 1.0
+    if "nm" in headers:
+        scale = 10.0
+        headers = [h for h in headers if h != "nm"]
+
+    def idx(h):
+        return headers.index(h) if h in headers else -1
+
+    hA, hx, hy, hz = idx("A"), idx("x"), idx("y"), idx("z")
+    hocc, hu, hu1, hu2, hu3 = idx("occ"), idx("u"), idx("u1"), idx("u2"), idx("u3")
+    default = hA == -1 and hx == -1 and hy == -1 and hz == -1
+    if default:
+        hA, hx, hy, hz = 0, 1, 2, 3
+    if -1 in (hA, hx, hy, hz):
+        raise RuntimeError(".xyz file headers not complete (requires A, x, y, z)")
+    if default:
+        hocc, hu, hu1, hu2, hu3 = [h + 4 * (h != -1) for h in (hocc, hu, hu1, hu2, hu3)]
+    max_header = max(hA, hx, hy, hz, hocc, hu, hu1, hu2, hu3)
+    Z, X, Y, Zc, U = [], [], [], [], []
+    defined_u = hu != -1 or hu1 != -1 or hu2 != -1 or hu3 != -1
+    i = 0
+    for line in lines[2:]:
+        if not line:
+            break
+        if i > n:
+            raise RuntimeError(f"Number of atoms does not match .xyz first line ({n})")
+        v = line.split()
+        if len(v) < max_header:
+            raise RuntimeError(f".xyz file columns are fewer than header entries. line: {2 + i}")
+        Z.append(symbol_to_z(v[hA]))
+        X.append(_stof(v[hx]) * scale)
+        Y.append(_stof(v[hy]) * scale)
+        Zc.append(_stof(v[hz]) * scale)
+        if defined_u:
+            u = [0.0, 0.0, 0.0]
+            if hu != -1:
+                u = [_stof(v[hu])] * 3
+            if hu1 != -1:
+                u[0] = _stof(v[hu1])
+            if hu2 != -1:
+                u[1] = _stof(v[hu2])
+            if hu3 != -1:
+                u[2] = _stof(v[hz])  # the reference reads the z column here (crystalstructure.cpp:176-177)
+            U.append([q * scale * scale for q in u])
+        i += 1
+    if i != n:
+        raise RuntimeError(f"Number of atoms does not match .xyz first line: {i} instead of {n}")
+    return Structure(np.asarray(Z, np.int32), np.asarray(X), np.asarray(Y), np.asarray(Zc),
+                     np.asarray(U) if defined_u else None, name=path)
+
+
+def write_xyz(s: Structure, path: str):
+    with open(path, "w") as f:
+        f.write(f"{len(s)}\nA x y z\n")
+        for a, x, y, z in zip(s.Z, s.x, s.y, s.z):
+            f.write(f"{ELEMENTS[int(a) - 1]} {x:.6f} {y:.6f} {z:.6f}\n")
+
+
+def perovskite(nx: int, ny: int, nz: int, a: float = 3.905, A: int = 38, B: int = 22, X: int = 8) -> Structure:
+    """Cubic ABX3 cell: A at (0,0,0), B at (1/2,1/2,1/2), X at face centres, tiled nx*ny*nz."""
+    basis = [(A, 0.0, 0.0, 0.0), (B, 0.5, 0.5, 0.5), (X, 0.5, 0.5, 0.0), (X, 0.5, 0.0, 0.5), (X, 0.0, 0.5, 0.5)]
+    return _tile(basis, a, nx, ny, nz, "perovskite")
+
+
+def fcc(nx: int, ny: int, nz: int, a: float = 4.08, Zn: int = 79) -> Structure:
+    basis = [(Zn, 0.0, 0.0, 0.0), (Zn, 0.5, 0.5, 0.0), (Zn, 0.5, 0.0, 0.5), (Zn, 0.0, 0.5, 0.5)]
+    return _tile(basis, a, nx, ny, nz, "fcc")
+
+
+def _tile(basis, a, nx, ny, nz, name):
+    Z, X, Y, W = [], [], [], []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                for (zn, fx, fy, fz) in basis:
+                    Z.append(zn)
+                    X.append((i + fx) * a)
+                    Y.append((j + fy) * a)
+                    W.append((k + fz) * a)
+    return Structure(np.asarray(Z, np.int32), np.asarray(X, np.float64), np.asarray(Y, np.float64),
+                     np.asarray(W, np.float64), name=f"{name}_{nx}x{ny}x{nz}")
+
+
+def phonon_configs(s: Structure, n_configs: int, u_rms: float, seed: int = 0):
+    """n_configs frozen-phonon configurations: each atom displaced by N(0, u_rms^2) per axis, FP64,
+    configuration c drawn from numpy's PCG64 seeded with (seed, c)."""
+    out = []
+    for c in range(n_configs):
+        rng = np.random.Generator(np.random.PCG64([seed, c]))
+        if s.u2 is not None:
+            sd = np.sqrt(s.u2)
+        else:
+            sd = np.full((len(s), 3), float(u_rms))
+        d = rng.standard_normal((len(s), 3)) * sd
+        out.append(Structure(s.Z.copy(), s.x + d[:, 0], s.y + d[:, 1], s.z + d[:, 2], name=f"{s.name}#ph{c}"))
+    return out
+
+
+def concat_configs(configs):
+    """Concatenate configurations into the flat arrays mslice_stage_configs takes."""
+    counts = np.asarray([len(c) for c in configs], dtype=np.uint64)
+    Z = np.ascontiguousarray(np.concatenate([c.Z for c in configs]).astype(np.int32))
+    x = np.ascontiguousarray(np.concatenate([c.x for c in configs]))
+    y = np.ascontiguousarray(np.concatenate([c.y for c in configs]))
+    z = np.ascontiguousarray(np.concatenate([c.z for c in configs]))
+    return counts, Z, x, y, z
+
+
+def wavelength(voltage_kv: float) -> float:
+    """MicroscopeParameters::Wavelength (commonstructs.h:269-271), Å."""
+    h, c, e, m = 6.6262e-034, 299792458.0, 1.6021773e-019, 9.10938291e-031
+    V = voltage_kv * 1000
+    return h * c / math.sqrt(e * V * (2 * m * c * c + e * V)) * 1e10

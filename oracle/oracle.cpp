@@ -1,0 +1,1184 @@
+// oracle.cpp — CPU restatement of clTEM's multislice path. TEST INFRASTRUCTURE ONLY.
+//
+// This file is the checker for the CUDA engine (cltem_b200/csrc). Only tests/, __graft_entry__.smoke()
+// and bench.py's CPU-baseline / reference arm load it; the engine never links or calls it.
+//
+// What it restates (paths relative to the clTEM project root):
+//   - the double-precision OpenCL kernels kernels/*_d.cl, statement by statement, in the same
+//     evaluation order (built with -ffp-contract=off to mirror the default non-mad OpenCL build,
+//     src/simulation/kernels.h:47-69, kernels.cpp:4: no native_ functions, no -cl-mad-enable);
+//   - the host logic around them: SimulationGeneral (src/simulation/microscope/simulationgeneral.cpp),
+//     SimulationStem/Cbed/Ctem, SimulationManager geometry (src/simulation/simulationmanager.cpp),
+//     SimulationCell (src/simulation/structure/simulationcell.cpp), MicroscopeParameters
+//     (src/simulation/utilities/commonstructs.h:210-290);
+//   - clFFT's 2-D out-of-place transform with scale 1/sqrtf(w*h) in both directions
+//     (src/simulation/clwrapper/clfourier.cpp:30-73). clFFT itself is a third-party library that is
+//     not vendored and has no pinned version (clwrapper/cmake/modules/FindclFFT.cmake only searches
+//     for it); it is restated here as the mathematically defined unitary DFT, checked against
+//     numpy.fft (norm="ortho") in tests/.
+//
+// Pinning: the kernel restatements are checked bit-for-bit against the reference's own .cl sources
+// compiled for the CPU (oracle/build_ref.py -> oracle/_ref/) and against fixtures made from them
+// (tests/golden/). The FFT and the host logic have no reference-produced outputs to pin against.
+//
+// The template parameter T is the kernel precision. T = double is the `_d` path the engine is judged
+// against; T = float is a single-precision variant of the same statements used only as a timed CPU
+// baseline (it is not a bit-exact restatement of the `_f` kernels).
+
+#include "../include/mslice.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+
+// ------------------------------------------------------------------------------------------------
+// Physics constants and microscope helpers (commonstructs.cpp:5-12, commonstructs.h:269-289)
+// ------------------------------------------------------------------------------------------------
+static const double kPi = M_PI;
+static const double eMass = 9.10938291e-031;
+static const double eCharge = 1.6021773e-019;
+static const double hPlanck = 6.6262e-034;
+static const double cLight = 299792458.0;
+
+static double wavelength(double V) {
+    return hPlanck * cLight / std::sqrt(eCharge * (V * 1000) * (2 * eMass * cLight * cLight + eCharge * (V * 1000))) * 1e+10;
+}
+static double sigma_raw(double V) {
+    return (2 * kPi / (wavelength(V) * (V * 1000))) * (eMass * cLight * cLight + eCharge * (V * 1000)) /
+           (2 * eMass * cLight * cLight + eCharge * (V * 1000));
+}
+
+// ------------------------------------------------------------------------------------------------
+// Geometry: SimulationArea / SimulationCell / SimulationManager
+// ------------------------------------------------------------------------------------------------
+struct Lim { double lo, hi; };
+
+// SimulationArea::getCorrectedLimitsX/Y (commonstructs.cpp:33-59)
+static void corrected(double xs, double xf, double ys, double yf, double pad, Lim &x, Lim &y) {
+    double range_x = xf - xs, range_y = yf - ys;
+    double range_max = std::max(range_x, range_y);
+    double range_total = range_max + pad;
+    double x_diff = (range_total - range_x) / 2;
+    double y_diff = (range_total - range_y) / 2;
+    x = {xs - x_diff, xf + x_diff};
+    y = {ys - y_diff, yf + y_diff};
+}
+
+// fullAreaBase (simulationmanager.cpp:470-483) + padding (paddedFullLimitsX/Y :446-452)
+static void full_area(const mslice_config &c, Lim &x, Lim &y) {
+    if (c.mode == MSLICE_MODE_STEM)
+        corrected(c.stem_area[0], c.stem_area[1], c.stem_area[2], c.stem_area[3], c.stem_padding, x, y);
+    else if (c.mode == MSLICE_MODE_CBED)  // CbedPosition::getSimArea (commonstructs.h:342-345)
+        corrected(c.cbed_x, c.cbed_x, c.cbed_y, c.cbed_y, c.cbed_padding, x, y);
+    else
+        corrected(c.ctem_area[0], c.ctem_area[1], c.ctem_area[2], c.ctem_area[3], 0.0, x, y);
+    x.lo += -c.padding_xy; x.hi += c.padding_xy;
+    y.lo += -c.padding_xy; y.hi += c.padding_xy;
+}
+
+static bool resolution_valid(const mslice_config &c) {
+    int r = c.resolution;
+    if (c.allow_any_resolution) {
+        int m = r;
+        if (m % 3 == 0) m /= 3;
+        return r >= 16 && (m & (m - 1)) == 0;
+    }
+    // SimulationManager::resolutionValid (simulationmanager.cpp:430-432)
+    return r == 256 || r == 512 || r == 768 || r == 1024 || r == 1536 || r == 2048 || r == 3072 || r == 4096 || r == 8192;
+}
+
+struct Geo {
+    mslice_geometry g;
+    int res;
+    std::vector<double> kx, ky;  // k0x, k0y (simulationgeneral.cpp:427-449)
+};
+
+static void compute_geometry(const mslice_config &c, Geo &G) {
+    if (!resolution_valid(c)) throw std::invalid_argument("invalid resolution");
+    if (c.slice_thickness <= 0) throw std::invalid_argument("slice thickness must be positive");
+    if (c.voltage <= 0) throw std::invalid_argument("voltage must be positive");
+    mslice_geometry &g = G.g;
+    std::memset(&g, 0, sizeof(g));
+    G.res = c.resolution;
+    Lim fx, fy;
+    full_area(c, fx, fy);
+    // parallel STEM / CTEM / CBED: currentAreaBase == fullAreaBase (simulationmanager.cpp:485-505)
+    g.sim_x[0] = fx.lo; g.sim_x[1] = fx.hi; g.sim_y[0] = fy.lo; g.sim_y[1] = fy.hi;
+    g.full_x[0] = fx.lo; g.full_x[1] = fx.hi; g.full_y[0] = fy.lo; g.full_y[1] = fy.hi;
+
+    // SimulationCell::roundPaddingZ (simulationcell.cpp:43-61)
+    double dz = c.slice_thickness, off = c.slice_offset;
+    double pz0 = -c.padding_z, pz1 = c.padding_z;
+    int pad_slices_pre = (int)std::ceil((std::abs(pz1) - off) / dz);
+    double pre_pad = off + pad_slices_pre * dz;
+    double zw = c.struct_limits[5] - c.struct_limits[4];
+    int struct_slices = (int)std::ceil((zw + off) / dz);
+    double struct_slice_thick = struct_slices * dz;
+    double left_over = struct_slice_thick - off - zw;
+    int pad_slices_post = (int)std::ceil((std::abs(pz0) - left_over) / dz);
+    double post_pad = pad_slices_post * dz + left_over;
+    g.padding_z[0] = -post_pad; g.padding_z[1] = pre_pad;
+    g.z_lims[0] = c.struct_limits[4] + g.padding_z[0];
+    g.z_lims[1] = c.struct_limits[5] + g.padding_z[1];
+    // sliceCount (simulationcell.cpp:75-83), preSliceCount (:85-87)
+    double z_range = g.z_lims[1] - g.z_lims[0];
+    unsigned int n_slices = (unsigned int)std::ceil((z_range / dz) - 0.000001);
+    n_slices += (n_slices == 0);
+    g.n_slices = (int)n_slices;
+    g.pre_slices = (int)(unsigned int)(g.padding_z[1] / dz);
+    g.dz = dz;
+
+    // realScale / inverseScale / inverseScaleAngle (simulationmanager.cpp:211-247)
+    double x_r = g.sim_x[1] - g.sim_x[0], y_r = g.sim_y[1] - g.sim_y[0];
+    g.real_scale = std::max(x_r, y_r) / c.resolution;
+    g.inverse_scale = 1.0 / (g.real_scale * c.resolution);
+    g.wavelength = wavelength(c.voltage);
+    g.wavenumber = 1.0 / g.wavelength;
+    g.angle_scale = 1000.0 * g.inverse_scale * g.wavelength;
+    // Wavevector (commonstructs.h:282-289)
+    double k = g.wavenumber;
+    g.wavevector[0] = k * std::sin(c.beam_tilt / 1000.0) * std::cos(c.beam_azimuth);
+    g.wavevector[1] = k * std::sin(c.beam_tilt / 1000.0) * std::sin(c.beam_azimuth);
+    g.wavevector[2] = k * std::cos(c.beam_tilt / 1000.0);
+    g.sigma = sigma_raw(c.voltage) * g.wavenumber / g.wavevector[2];  // simulationgeneral.cpp:418
+
+    // calculateBlocks (simulationmanager.cpp:393-408), blockScaleX/Y (:371-381)
+    double xr = g.full_x[1] - g.full_x[0], yr = g.full_y[1] - g.full_y[0];
+    int nb = (int)std::ceil(std::max(xr, yr) / 8.0);
+    g.blocks_x = nb; g.blocks_y = nb;
+    g.block_scale_x = xr / nb; g.block_scale_y = yr / nb;
+    // load blocks (simulationgeneral.cpp:517-521)
+    g.load_blocks_x = (int)std::ceil(8.0 / g.block_scale_x);
+    g.load_blocks_y = (int)std::ceil(8.0 / g.block_scale_y);
+    g.load_blocks_z = (int)std::ceil(3.0 / dz);
+
+    // k tables + bandwidth k_max (simulationgeneral.cpp:427-455)
+    int res = c.resolution;
+    double SimSizeX = g.real_scale * res, SimSizeY = SimSizeX;
+    G.kx.resize(res); G.ky.resize(res);
+    unsigned int imid = (unsigned int)std::floor(static_cast<double>(res) / 2.0 + 0.5);
+    for (int i = 0; i < res; i++) {
+        double t = (i >= (int)imid) ? double(i - res) / SimSizeX : i / SimSizeX;
+        G.kx[i] = t;
+    }
+    for (int i = 0; i < res; i++) {
+        double t = (i >= (int)imid) ? double(i - res) / SimSizeY : i / SimSizeY;
+        G.ky[i] = t;
+    }
+    double kmaxx = std::abs(G.kx[imid]), kmaxy = std::abs(G.ky[imid]);
+    g.k_max = std::min(kmaxy, kmaxx);
+
+    // imageCrop (simulationmanager.cpp:410-428); raw sim limits = the raw area of the mode
+    double raw_x0, raw_x1, raw_y0, raw_y1;
+    if (c.mode == MSLICE_MODE_STEM) { raw_x0 = c.stem_area[0]; raw_x1 = c.stem_area[1]; raw_y0 = c.stem_area[2]; raw_y1 = c.stem_area[3]; }
+    else if (c.mode == MSLICE_MODE_CBED) { raw_x0 = raw_x1 = c.cbed_x; raw_y0 = raw_y1 = c.cbed_y; }
+    else { raw_x0 = c.ctem_area[0]; raw_x1 = c.ctem_area[1]; raw_y0 = c.ctem_area[2]; raw_y1 = c.ctem_area[3]; }
+    double crop_lr_total = (std::floor(x_r - (raw_x1 - raw_x0)) / g.real_scale);
+    double crop_tb_total = (std::floor(y_r - (raw_y1 - raw_y0)) / g.real_scale);
+    unsigned int crop_l = (unsigned int)std::floor(crop_lr_total / 2.0);
+    unsigned int crop_b = (unsigned int)std::floor(crop_tb_total / 2.0);
+    unsigned int crop_r = (unsigned int)(crop_lr_total - crop_l);
+    unsigned int crop_t = (unsigned int)(crop_tb_total - crop_b);
+    g.crop[0] = crop_t; g.crop[1] = crop_l; g.crop[2] = crop_b; g.crop[3] = crop_r;
+
+    // output count (simulationstem.cpp:167-170)
+    int step = c.intermediate_slices;
+    g.n_outputs = step > 0 ? (int)std::ceil((float)g.n_slices / step) : 1;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Atom sort + binning: SimulationGeneral::sortAtoms (simulationgeneral.cpp:147-342)
+// ------------------------------------------------------------------------------------------------
+template <class T>
+struct Atoms {
+    std::vector<T> x, y, z;
+    std::vector<int> A;
+    std::vector<int> block_start;   // n_slices*bx*by + 1
+    std::vector<int> block_ids, z_ids;  // atom_sort output for the filtered list
+};
+
+#define recip(x) (1.0 / (x))
+
+// kernels/atom_sort_d.cl:28-69, one work item
+template <class T>
+static void atom_sort_item(int xid, const T *x_input, const T *y_input, const T *z_input, int n_atoms, T min_x, T max_x,
+                           T min_y, T max_y, T min_z, T max_z, int blocks_x, int blocks_y, int *block_ids, int *z_ids,
+                           T dz, int n_slices) {
+    (void)min_z;
+    if (xid < n_atoms) {
+        if (x_input[xid] >= min_x && x_input[xid] <= max_x && y_input[xid] >= min_y && y_input[xid] <= max_y) {
+            int bidx = (int)std::floor((x_input[xid] - min_x) * recip(max_x - min_x) * blocks_x);
+            int bidy = (int)std::floor((y_input[xid] - min_y) * recip(max_y - min_y) * blocks_y);
+            int zid = (int)std::floor((max_z - z_input[xid]) * recip(dz));
+            zid -= (zid == n_slices);
+            bidx -= (bidx == blocks_x);
+            bidy -= (bidy == blocks_y);
+            int bid = bidx + blocks_x * bidy;
+            block_ids[xid] = bid;
+            z_ids[xid] = zid;
+        } else {
+            block_ids[xid] = -1;
+            z_ids[xid] = -1;
+        }
+    }
+}
+
+template <class T>
+static void sort_atoms(const mslice_config &c, const Geo &G, size_t n, const int *Z, const double *x, const double *y,
+                       const double *z, Atoms<T> &out) {
+    const mslice_geometry &g = G.g;
+    std::vector<int> AtomANum;
+    std::vector<T> AtomXPos, AtomYPos, AtomZPos;
+    // host range filter on the padded FULL limits, strict (simulationgeneral.cpp:173-217)
+    for (size_t i = 0; i < n; i++) {
+        double new_x = x[i], new_y = y[i], new_z = z[i];
+        bool in_x = new_x > g.full_x[0] && new_x < g.full_x[1];
+        bool in_y = new_y > g.full_y[0] && new_y < g.full_y[1];
+        bool in_z = new_z > g.z_lims[0] && new_z < g.z_lims[1];
+        if (in_x && in_y && in_z) {
+            AtomANum.push_back(Z[i]);
+            AtomXPos.push_back((T)new_x);
+            AtomYPos.push_back((T)new_y);
+            AtomZPos.push_back((T)new_z);
+        }
+    }
+    int atom_count = (int)AtomANum.size();
+    int BX = g.blocks_x, BY = g.blocks_y, NS = g.n_slices;
+    std::vector<int> bid(atom_count), zid(atom_count);
+    for (int i = 0; i < atom_count; i++)
+        atom_sort_item<T>(i, AtomXPos.data(), AtomYPos.data(), AtomZPos.data(), atom_count, (T)g.full_x[0], (T)g.full_x[1],
+                          (T)g.full_y[0], (T)g.full_y[1], (T)g.z_lims[0], (T)g.z_lims[1], BX, BY, bid.data(), zid.data(),
+                          (T)g.dz, NS);
+    // host binning into z-major, y, x order (simulationgeneral.cpp:269-338)
+    size_t nb = (size_t)BX * BY;
+    std::vector<std::vector<std::vector<int>>> binned(nb, std::vector<std::vector<int>>(NS));
+    int count_in_range = 0;
+    for (int i = 0; i < atom_count; ++i) {
+        if (zid[i] >= 0 && bid[i] >= 0) {
+            binned[bid[i]][zid[i]].push_back(i);
+            ++count_in_range;
+        }
+    }
+    out.x.assign(atom_count, 0); out.y.assign(atom_count, 0); out.z.assign(atom_count, 0); out.A.assign(atom_count, 0);
+    out.block_start.assign((size_t)NS * nb + 1, 0);
+    int it = 0;
+    for (int s = 0; s < NS; s++)
+        for (int j = 0; j < BY; j++)
+            for (int k = 0; k < BX; k++) {
+                out.block_start[(size_t)s * nb + j * BX + k] = it;
+                for (int idx : binned[j * BX + k][s]) {
+                    out.x[it] = AtomXPos[idx]; out.y[it] = AtomYPos[idx]; out.z[it] = AtomZPos[idx]; out.A[it] = AtomANum[idx];
+                    it++;
+                }
+            }
+    out.block_start[(size_t)NS * nb] = count_in_range;
+    out.block_ids = bid; out.z_ids = zid;
+    // entries past count_in_range keep the pre-binning values in the reference (the vectors are
+    // reused in place); they are never read because block_start ends at count_in_range.
+    for (int i = it; i < atom_count; i++) { out.x[i] = AtomXPos[i]; out.y[i] = AtomYPos[i]; out.z[i] = AtomZPos[i]; out.A[i] = AtomANum[i]; }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Projected potential (kernels/transmission_potentials_projected_d.cl)
+// ------------------------------------------------------------------------------------------------
+static const double k0pi[5] = {1.0, 2.346487949187396e-1, 1.187082088663404e-2, 2.150707366040937e-4, 1.425433617130587e-6};
+static const double k0qi[3] = {9.847324170755358e-1, 1.518396076767770e-2, 8.362215678646257e-5};
+static const double k0p[5] = {1.159315156584126e-1, 2.770731240515333e-1, 2.066458134619875e-2, 4.574734709978264e-4, 3.454715527986737e-6};
+static const double k0q[3] = {9.836249671709183e-1, 1.627693622304549e-2, 9.809660603621949e-5};
+static const double k0pp[8] = {1.253314137315499, 1.475731032429900e1, 6.123767403223466e1, 1.121012633939949e2,
+                               9.285288485892228e1, 3.198289277679660e1, 3.595376024148513, 6.160228690102976e-2};
+static const double k0qq[8] = {1.0, 1.189963006673403e1, 5.027773590829784e1, 9.496513373427093e1,
+                               8.318077493230258e1, 3.181399777449301e1, 4.443672926432041, 1.408295601966600e-1};
+static const double k1pi[5] = {0.5, 5.598072040178741e-2, 1.818666382168295e-3, 2.397509908859959e-5, 1.239567816344855e-7};
+static const double k1qi[3] = {9.870202601341150e-1, 1.292092053534579e-2, 5.881933053917096e-5};
+static const double k1p[5] = {-3.079657578292062e-1, -8.109417631822442e-2, -3.477550948593604e-3, -5.385594871975406e-5, -3.110372465429008e-7};
+static const double k1q[3] = {9.861813171751389e-1, 1.375094061153160e-2, 6.774221332947002e-5};
+static const double k1pp[8] = {1.253314137315502, 1.457171340220454e1, 6.063161173098803e1, 1.147386690867892e2,
+                               1.040442011439181e2, 4.356596656837691e1, 7.265230396353690, 3.144418558991021e-1};
+static const double k1qq[8] = {1.0, 1.125154514806458e1, 4.427488496597630e1, 7.616113213117645e1,
+                               5.863377227890893e1, 1.850303673841586e1, 1.857244676566022, 2.538540887654872e-2};
+
+// poly (projected_d.cl:71-76)
+template <class T>
+static T poly(const double *cof, int n, T x) {
+    T ans = (T)cof[n];
+    for (int i = n - 1; i >= 0; --i) ans = ans * x + (T)cof[i];
+    return ans;
+}
+// bessk0 / bessk1 (projected_d.cl:78-102), Numerical Recipes 2nd ed. section 6.6 rational forms
+template <class T>
+static T bessk0(T x) {
+    T ax = std::fabs(x);
+    if (ax > 0.0 && ax <= 1.0) {
+        T z = x * x;
+        T term = poly<T>(k0pi, 4, z) * std::log(x) * (T)recip(poly<T>(k0qi, 2, (T)1.0 - z));
+        return poly<T>(k0p, 4, z) * (T)recip(poly<T>(k0q, 2, (T)1.0 - z)) - term;
+    } else if (ax > 1.0) {
+        T z = (T)recip(x);
+        return std::exp(-x) * poly<T>(k0pp, 7, z) * (T)recip(poly<T>(k0qq, 7, z)) * ((T)1.0 / std::sqrt(x));
+    } else
+        return (T)DBL_MAX;
+}
+template <class T>
+static T bessk1(T x) {
+    T ax = std::fabs(x);
+    if (ax > 0.0 && ax <= 1.0) {
+        T z = x * x;
+        T term = poly<T>(k1pi, 4, z) * std::log(x) * (T)recip(poly<T>(k1qi, 2, (T)1.0 - z));
+        return x * (poly<T>(k1p, 4, z) * (T)recip(poly<T>(k1q, 2, (T)1.0 - z)) + term) + (T)recip(x);
+    } else if (ax > 1.0) {
+        T z = (T)recip(x);
+        return std::exp(-x) * poly<T>(k1pp, 7, z) * (T)recip(poly<T>(k1qq, 7, z)) * ((T)1.0 / std::sqrt(x));
+    } else
+        return (T)DBL_MAX;
+}
+// kirkland (projected_d.cl:104-141): Kirkland eq. C.20
+template <class T>
+static T kirkland_proj(const T *params, int i_lim, int ZNum, T rad) {
+    T suml = 0, sumg = 0, x;
+    int z_ofst = (ZNum - 1) * 12;
+    x = (T)(2.0 * M_PI) * rad;
+    for (int i = 0; i < i_lim * 2; i += 2) {
+        T a = params[z_ofst + i], b = params[z_ofst + i + 1];
+        suml += a * bessk0<T>(x * std::sqrt(b));
+    }
+    x = (T)M_PI * rad;
+    x = x * x;
+    for (int i = i_lim * 2; i < i_lim * 4; i += 2) {
+        T c = params[z_ofst + i], d = params[z_ofst + i + 1];
+        T d_inv = (T)recip(d);
+        sumg += (c * d_inv) * std::exp(-x * d_inv);
+    }
+    return (T)300.8242834 * suml + (T)150.4121417 * sumg;
+}
+// lobato (projected_d.cl:143-160): Lobato 2014 eq. 16
+template <class T>
+static T lobato_proj(const T *params, int i_lim, int ZNum, T rad) {
+    T sum = 0, x;
+    int z_ofst = (ZNum - 1) * 10;
+    x = (T)(2.0 * M_PI) * rad;
+    for (int i = 0; i < i_lim; ++i) {
+        T a = params[z_ofst + i], b = params[z_ofst + i + 5];
+        T b_inv_root = (T)1.0 / std::sqrt(b);
+        sum += a * (b_inv_root * b_inv_root * b_inv_root) * (bessk0<T>(x * b_inv_root) + rad * bessk1<T>(x * b_inv_root));
+    }
+    return (T)945.090144399935 * sum;
+}
+// peng (projected_d.cl:162-181)
+template <class T>
+static T peng_proj(const T *params, int i_lim, int ZNum, T rad) {
+    T sum = 0, x;
+    int z_ofst = (ZNum - 1) * 10;
+    x = (T)M_PI * rad;
+    x = x * x;
+    for (int i = 0; i < i_lim; ++i) {
+        T a = params[z_ofst + i], b = params[z_ofst + i + 5];
+        T b_inv = (T)recip(b);
+        sum += a * b_inv * std::exp(-x * b_inv);
+    }
+    return (T)150.4121417 * sum;
+}
+
+// full-3D helpers (kernels/transmission_potentials_full_3d_d.cl:57-134)
+template <class T>
+static T kirkland_3d(const T *params, int i_lim, int ZNum, T rad) {
+    T suml = 0, sumg = 0, x;
+    int z_ofst = (ZNum - 1) * 12;
+    x = (T)(2.0 * M_PI) * rad;
+    for (int i = 0; i < i_lim * 2; i += 2) {
+        T a = params[z_ofst + i], b = params[z_ofst + i + 1];
+        suml += a * std::exp(-x * std::sqrt(b));
+    }
+    x = (T)M_PI * rad;
+    x = x * x;
+    for (int i = i_lim * 2; i < i_lim * 4; i += 2) {
+        T c = params[z_ofst + i], d = params[z_ofst + i + 1];
+        T d_inv_root = (T)1.0 / std::sqrt(d);
+        sumg += c * (d_inv_root * d_inv_root * d_inv_root) * std::exp(-x * (T)recip(d));
+    }
+    return (T)150.4121417 * (T)recip(rad) * suml + (T)266.5157269 * sumg;
+}
+template <class T>
+static T lobato_3d(const T *params, int i_lim, int ZNum, T rad) {
+    T sum = 0, x;
+    int z_ofst = (ZNum - 1) * 10;
+    x = (T)M_PI * rad;
+    for (int i = 0; i < i_lim; ++i) {
+        T a = params[z_ofst + i], b = params[z_ofst + i + 5];
+        T b_inv_root = (T)1.0 / std::sqrt(b);
+        sum += a * (b_inv_root * b_inv_root * b_inv_root) * std::exp((T)-2.0 * x * b_inv_root) * (std::sqrt(b) * (T)recip(x) + (T)1.0);
+    }
+    return (T)472.545072199968 * sum;
+}
+template <class T>
+static T peng_3d(const T *params, int i_lim, int ZNum, T rad) {
+    T sum = 0, x;
+    int z_ofst = (ZNum - 1) * 10;
+    x = (T)M_PI * rad;
+    x = x * x;
+    for (int i = 0; i < i_lim; ++i) {
+        T a = params[z_ofst + i], b = params[z_ofst + i + 5];
+        T b_inv_root = (T)1.0 / std::sqrt(b);
+        sum += a * (b_inv_root * b_inv_root * b_inv_root) * std::exp(-x * (T)recip(b));
+    }
+    return (T)266.5157269 * sum;
+}
+
+struct PotArgs {
+    int form, i_count;
+    int width, height, current_slice, total_slices;
+    double dz, pixelscale;
+    int blocks_x, blocks_y;
+    double max_x, min_x, max_y, min_y;
+    int block_load_x, block_load_y, slice_load_z;
+    double sigma, startx, starty;
+    double beam_theta, beam_phi;              // projected only
+    double current_z, shift_x, shift_y;      // full 3-D only
+    int integrals;
+};
+
+// Bin ranges of one 16x16 work group (projected_d.cl:227-246 / full_3d_d.cl:191-210)
+template <class T>
+static void group_bins(const PotArgs &a, int gx, int gy, int &starti, int &endi, int &startj, int &endj) {
+    T pixelscale = (T)a.pixelscale;
+    T group_size_x = (T)16 * pixelscale, group_size_y = (T)16 * pixelscale;
+    T group_start_x = (T)a.startx + gx * group_size_x;
+    T group_end_x = group_start_x + group_size_x;
+    T group_start_y = (T)a.starty + gy * group_size_y;
+    T group_end_y = group_start_y + group_size_y;
+    T recip_range_x = (T)recip((T)a.max_x - (T)a.min_x);
+    T recip_range_y = (T)recip((T)a.max_y - (T)a.min_y);
+    starti = (int)std::fmax(std::floor(a.blocks_x * (group_start_x - (T)a.min_x) * recip_range_x) - a.block_load_x, 0);
+    endi = (int)std::fmin(std::ceil(a.blocks_x * (group_end_x - (T)a.min_x) * recip_range_x) + a.block_load_x, a.blocks_x - 1);
+    startj = (int)std::fmax(std::floor(a.blocks_y * (group_start_y - (T)a.min_y) * recip_range_y) - a.block_load_y, 0);
+    endj = (int)std::fmin(std::ceil(a.blocks_y * (group_end_y - (T)a.min_y) * recip_range_y) + a.block_load_y, a.blocks_y - 1);
+}
+
+// transmission_potentials_projected_d (projected_d.cl:183-317), all work items, no 256-atom cap
+template <class T>
+static void potential_projected(const PotArgs &a, const Atoms<T> &at, const T *params, std::complex<T> *out) {
+    int W = a.width, H = a.height;
+    int gxn = (W + 15) / 16, gyn = (H + 15) / 16;
+    T beam_theta = (T)(M_PI_2 - a.beam_theta * 0.001);
+    T beam_phi = (T)a.beam_phi;
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int gy = 0; gy < gyn; gy++)
+        for (int gx = 0; gx < gxn; gx++) {
+            int starti, endi, startj, endj;
+            group_bins<T>(a, gx, gy, starti, endi, startj, endj);
+            int k = a.current_slice;
+            if (k < 0) k = 0;
+            if (k >= a.total_slices) k = a.total_slices - 1;
+            for (int ly = 0; ly < 16; ly++)
+                for (int lx = 0; lx < 16; lx++) {
+                    int xid = gx * 16 + lx, yid = gy * 16 + ly;
+                    T sumz = 0;
+                    for (int j = startj; j <= endj; j++) {
+                        int start = at.block_start[(size_t)k * a.blocks_x * a.blocks_y + a.blocks_x * j + starti];
+                        int end = at.block_start[(size_t)k * a.blocks_x * a.blocks_y + a.blocks_x * j + endi + 1];
+                        for (int l = 0; l < end - start; l++) {
+                            T im_pos_x = (T)a.startx + xid * (T)a.pixelscale;
+                            T rad_x = im_pos_x - at.x[start + l];
+                            T im_pos_y = (T)a.starty + yid * (T)a.pixelscale;
+                            T rad_y = im_pos_y - at.y[start + l];
+                            T cos_beam_phi = std::cos(beam_phi);
+                            T sin_beam_phi = std::sin(beam_phi);
+                            T sin_beam_2theta = std::sin((T)2.0 * beam_theta);
+                            T z_prime = (T)-0.5 * (rad_x * cos_beam_phi + rad_y * sin_beam_phi) * sin_beam_2theta;
+                            T z_by_tan_beam_theta = z_prime / std::tan(beam_theta);
+                            T x_prime = rad_x + z_by_tan_beam_theta * cos_beam_phi;
+                            T y_prime = rad_y + z_by_tan_beam_theta * sin_beam_phi;
+                            T rad = std::sqrt(z_prime * z_prime + x_prime * x_prime + y_prime * y_prime);
+                            T r_min = (T)0.25 * (T)a.pixelscale;
+                            if (rad < r_min) rad = r_min;
+                            if (rad <= 8.0) {
+                                int Zn = at.A[start + l];
+                                if (a.form == 0) sumz += kirkland_proj<T>(params, a.i_count, Zn, rad);
+                                else if (a.form == 1) sumz += peng_proj<T>(params, a.i_count, Zn, rad);
+                                else if (a.form == 2) sumz += lobato_proj<T>(params, a.i_count, Zn, rad);
+                            }
+                        }
+                    }
+                    if (xid < W && yid < H)
+                        out[xid + W * yid] = std::complex<T>(std::cos((T)a.sigma * sumz), std::sin((T)a.sigma * sumz));
+                }
+        }
+}
+
+// transmission_potentials_full_3d_d (full_3d_d.cl:136-290), all work items, no 256-atom cap
+template <class T>
+static void potential_full3d(const PotArgs &a, const Atoms<T> &at, const T *params, std::complex<T> *out) {
+    int W = a.width, H = a.height;
+    int gxn = (W + 15) / 16, gyn = (H + 15) / 16;
+    int topz = a.current_slice - a.slice_load_z, bottomz = a.current_slice + a.slice_load_z;
+    T int_r = (T)recip((T)a.integrals);
+    T dz = (T)a.dz;
+    T sub_slice_thickness = dz * int_r;
+    if (topz < 0) topz = 0;
+    if (bottomz >= a.total_slices) bottomz = a.total_slices - 1;
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int gy = 0; gy < gyn; gy++)
+        for (int gx = 0; gx < gxn; gx++) {
+            int starti, endi, startj, endj;
+            group_bins<T>(a, gx, gy, starti, endi, startj, endj);
+            for (int ly = 0; ly < 16; ly++)
+                for (int lx = 0; lx < 16; lx++) {
+                    int xid = gx * 16 + lx, yid = gy * 16 + ly;
+                    T sumz = 0;
+                    for (int k = topz; k <= bottomz; k++) {
+                        for (int j = startj; j <= endj; j++) {
+                            int start = at.block_start[(size_t)k * a.blocks_x * a.blocks_y + a.blocks_x * j + starti];
+                            int end = at.block_start[(size_t)k * a.blocks_x * a.blocks_y + a.blocks_x * j + endi + 1];
+                            T p2 = 0;
+                            for (int l = 0; l < end - start; l++) {
+                                T im_pos_x = (T)a.startx + xid * (T)a.pixelscale;
+                                T rad_x = im_pos_x - at.x[start + l];
+                                T im_pos_y = (T)a.starty + yid * (T)a.pixelscale;
+                                T rad_y = im_pos_y - at.y[start + l];
+                                for (int h = 0; h <= a.integrals; h++) {
+                                    rad_x -= (T)a.shift_x;   // cumulative shift (full_3d_d.cl:244-246)
+                                    rad_y -= (T)a.shift_y;
+                                    T xyrad2 = rad_x * rad_x + rad_y * rad_y;
+                                    T im_pos_z = (T)a.current_z - h * dz * int_r;
+                                    T rad_z = im_pos_z - at.z[start + l];
+                                    T rad = std::sqrt(xyrad2 + rad_z * rad_z);
+                                    T r_min = (T)0.25 * (T)a.pixelscale;
+                                    if (rad < r_min) rad = r_min;
+                                    if (xyrad2 <= 64.0 && rad_z <= 3.0) {   // one-sided z test (:263)
+                                        T p1 = 0;
+                                        int Zn = at.A[start + l];
+                                        if (a.form == 0) p1 = kirkland_3d<T>(params, a.i_count, Zn, rad);
+                                        else if (a.form == 1) p1 = peng_3d<T>(params, a.i_count, Zn, rad);
+                                        else if (a.form == 2) p1 = lobato_3d<T>(params, a.i_count, Zn, rad);
+                                        sumz += (h != 0) * (p1 + p2) * (T)0.5;
+                                        p2 = p1;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    if (xid < W && yid < H)
+                        out[xid + W * yid] = std::complex<T>(std::cos(sub_slice_thickness * (T)a.sigma * sumz),
+                                                             std::sin(sub_slice_thickness * (T)a.sigma * sumz));
+                }
+        }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Unitary 2-D DFT (clFourier semantics). Stockham autosort, radices 4, 2, 3, 5 and generic.
+// ------------------------------------------------------------------------------------------------
+template <class T>
+struct FFT1 {
+    int n;
+    std::vector<int> radices;
+    std::vector<std::complex<T>> tw;   // exp(-2 pi i m / n)
+    explicit FFT1(int n_) : n(n_) {
+        int m = n;
+        for (int r : {4, 2, 3, 5}) while (m % r == 0) { radices.push_back(r); m /= r; }
+        if (m > 1) radices.push_back(m);
+        tw.resize(n);
+        for (int i = 0; i < n; i++) {
+            double ang = -2.0 * M_PI * (double)i / (double)n;
+            tw[i] = std::complex<T>((T)std::cos(ang), (T)std::sin(ang));
+        }
+    }
+    // in, out, scratch: n elements with element stride `st`; sign -1 forward, +1 inverse
+    void run(std::complex<T> *data, size_t st, int sign, std::complex<T> *buf0, std::complex<T> *buf1) const {
+        for (int i = 0; i < n; i++) buf0[i] = data[i * st];
+        std::complex<T> *src = buf0, *dst = buf1;
+        int Ns = 1;
+        std::vector<std::complex<T>> v(16);
+        for (int R : radices) {
+            if ((int)v.size() < R) v.resize(R);
+            int NR = n / R;
+            for (int j = 0; j < NR; j++) {
+                int k = j % Ns;
+                for (int r = 0; r < R; r++) {
+                    std::complex<T> w = tw[(size_t)((long long)r * k * (n / (Ns * R))) % n];
+                    if (sign > 0) w = std::conj(w);
+                    v[r] = src[j + r * NR] * w;
+                }
+                int idxD = (j / Ns) * Ns * R + k;
+                for (int m = 0; m < R; m++) {
+                    std::complex<T> acc(0, 0);
+                    for (int r = 0; r < R; r++) {
+                        std::complex<T> w = tw[(size_t)((long long)r * m % R) * (n / R)];
+                        if (sign > 0) w = std::conj(w);
+                        acc += v[r] * w;
+                    }
+                    dst[idxD + m * Ns] = acc;
+                }
+            }
+            std::swap(src, dst);
+            Ns *= R;
+        }
+        for (int i = 0; i < n; i++) data[i * st] = src[i];
+    }
+};
+
+template <class T>
+static void fft2(int w, int h, const std::complex<T> *in, std::complex<T> *out, int sign) {
+    if (in != out) std::copy(in, in + (size_t)w * h, out);
+    FFT1<T> fx(w), fy(h);
+#pragma omp parallel
+    {
+        std::vector<std::complex<T>> b0(std::max(w, h)), b1(std::max(w, h));
+#pragma omp for schedule(static)
+        for (int y = 0; y < h; y++) fx.run(out + (size_t)y * w, 1, sign, b0.data(), b1.data());
+#pragma omp for schedule(static)
+        for (int x = 0; x < w; x++) fy.run(out + x, w, sign, b0.data(), b1.data());
+    }
+    // clfftSetPlanScale(..., 1.0f / sqrtf(_width * _height)) (clfourier.cpp:70-73): a float scale
+    T scale = (T)(1.0f / sqrtf((float)(w * h)));
+    for (size_t i = 0; i < (size_t)w * h; i++) out[i] *= scale;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Pointwise kernels
+// ------------------------------------------------------------------------------------------------
+// band_limit_d (kernels/band_limit_d.cl:13-32)
+template <class T>
+static void band_limit(std::complex<T> *io, int W, int H, T k_max, T limit_factor, const T *k_x, const T *k_y) {
+    T lim = k_max * limit_factor;
+    for (int yid = 0; yid < H; yid++)
+        for (int xid = 0; xid < W; xid++) {
+            int id = xid + W * yid;
+            T k = std::sqrt(k_x[xid] * k_x[xid] + k_y[yid] * k_y[yid]);
+            io[id] = std::complex<T>(io[id].real() * (T)(k <= lim), io[id].imag() * (T)(k <= lim));
+        }
+}
+
+// propagator_d (kernels/propagator_d.cl:18-52)
+template <class T>
+static void propagator(std::complex<T> *prop, const T *k_x, const T *k_y, int W, int H, T dz, T beam_k, T beam_k_x,
+                       T beam_k_y, T beam_k_z, T k_max) {
+    for (int yid = 0; yid < H; yid++)
+        for (int xid = 0; xid < W; xid++) {
+            int id = xid + W * yid;
+            T k0x = k_x[xid] * k_x[xid];
+            T k0y = k_y[yid] * k_y[yid];
+            T k_max_2 = k_max * k_max;
+            if (k0x + k0y < k_max_2) {
+                T f = beam_k_z / beam_k;
+                T s_u = beam_k * beam_k - beam_k_z * beam_k_z - (beam_k_x + k_x[xid]) * (beam_k_x + k_x[xid]) -
+                        (beam_k_y + k_y[yid]) * (beam_k_y + k_y[yid]);
+                s_u = s_u / (beam_k_z);
+                prop[id] = std::complex<T>(f * std::cos((T)M_PI * s_u * dz), f * std::sin((T)M_PI * s_u * dz));
+            } else {
+                prop[id] = std::complex<T>(0, 0);
+            }
+        }
+}
+
+// complex helpers of init_probe_wave_d / ctem_image_d (init_probe_wave_d.cl:28-48)
+template <class T> static inline T cModSq(std::complex<T> a) { return a.real() * a.real() + a.imag() * a.imag(); }
+template <class T> static inline std::complex<T> cMult(std::complex<T> a, std::complex<T> b) {
+    return std::complex<T>(a.real() * b.real() - a.imag() * b.imag(), a.real() * b.imag() + a.imag() * b.real());
+}
+template <class T> static inline std::complex<T> cConj(std::complex<T> a) { return std::complex<T>(a.real(), -a.imag()); }
+template <class T> static inline std::complex<T> cPow(std::complex<T> a, int n) {
+    std::complex<T> temp = a;
+    for (int j = 1; j < n; j++) temp = cMult(temp, a);
+    return temp;
+}
+template <class T> static inline std::complex<T> cscale(std::complex<T> a, T s) { return std::complex<T>(a.real() * s, a.imag() * s); }
+template <class T> static inline std::complex<T> cdiv(std::complex<T> a, T s) { return std::complex<T>(a.real() / s, a.imag() / s); }
+
+template <class T>
+struct Aberr {
+    T C10, C30, C50;
+    std::complex<T> C12, C21, C23, C32, C34, C41, C43, C45, C52, C54, C56;
+};
+template <class T>
+static Aberr<T> aberrations(const mslice_config &c, double c10) {
+    auto cx = [](mslice_aberration a) { return std::complex<T>(std::polar(a.mag, a.ang)); };   // ComplexAberration::getComplex
+    Aberr<T> A;
+    A.C10 = (T)c10; A.C30 = (T)c.C30; A.C50 = (T)c.C50;
+    A.C12 = cx(c.C12); A.C21 = cx(c.C21); A.C23 = cx(c.C23); A.C32 = cx(c.C32); A.C34 = cx(c.C34);
+    A.C41 = cx(c.C41); A.C43 = cx(c.C43); A.C45 = cx(c.C45); A.C52 = cx(c.C52); A.C54 = cx(c.C54); A.C56 = cx(c.C56);
+    return A;
+}
+// the cchi sum shared by init_probe_wave_d.cl:83-100 and ctem_image_d.cl:86-102
+template <class T>
+static T cchi_of(const Aberr<T> &A, std::complex<T> w) {
+    std::complex<T> wc = cConj(w);
+    T tC10 = (T)0.5 * A.C10 * cModSq(w);
+    std::complex<T> tC12 = cscale(cMult(A.C12, cPow(wc, 2)), (T)0.5);
+    std::complex<T> tC21 = cdiv(cMult(A.C21, cMult(cPow(wc, 2), w)), (T)3.0);
+    std::complex<T> tC23 = cdiv(cMult(A.C23, cPow(wc, 3)), (T)3.0);
+    T tC30 = (T)0.25 * A.C30 * cModSq(w) * cModSq(w);
+    std::complex<T> tC32 = cscale(cMult(A.C32, cMult(cPow(wc, 3), w)), (T)0.25);
+    std::complex<T> tC34 = cscale(cMult(A.C34, cPow(wc, 4)), (T)0.25);
+    std::complex<T> tC41 = cscale(cMult(A.C41, cMult(cPow(wc, 3), cPow(w, 2))), (T)0.2);
+    std::complex<T> tC43 = cscale(cMult(A.C43, cMult(cPow(wc, 4), w)), (T)0.2);
+    std::complex<T> tC45 = cscale(cMult(A.C45, cPow(wc, 5)), (T)0.2);
+    T tC50 = A.C50 * cModSq(w) * cModSq(w) * cModSq(w) / (T)6.0;
+    std::complex<T> tC52 = cdiv(cMult(A.C52, cMult(cPow(wc, 4), cPow(w, 2))), (T)6.0);
+    std::complex<T> tC54 = cdiv(cMult(A.C54, cMult(cPow(wc, 5), w)), (T)6.0);
+    std::complex<T> tC56 = cdiv(cMult(A.C56, cPow(wc, 6)), (T)6.0);
+    return tC10 + tC12.real() + tC21.real() + tC23.real() + tC30 + tC32.real() + tC34.real() + tC41.real() + tC43.real() +
+           tC45.real() + tC50 + tC52.real() + tC54.real() + tC56.real();
+}
+
+// init_probe_wave_d (kernels/init_probe_wave_d.cl:49-118); the _d kernel computes but does not apply edge_factor
+template <class T>
+static void init_probe(std::complex<T> *out, int W, int H, const T *k_x, const T *k_y, T pos_x, T pos_y, T wavelength,
+                       const Aberr<T> &A, T cond_ap, T ap_smooth) {
+    for (int yid = 0; yid < H; yid++)
+        for (int xid = 0; xid < W; xid++) {
+            int id = xid + yid * W;
+            T cond_ap2 = (cond_ap * (T)0.001) / wavelength;
+            T k = std::sqrt((k_x[xid] * k_x[xid]) + (k_y[yid] * k_y[yid]));
+            T ap_smooth_radius = (ap_smooth * (T)0.001) / wavelength;
+            if (k < cond_ap2 + ap_smooth_radius) {
+                T posTerm = (T)2.0 * (T)M_PI * (k_x[xid] * pos_x + k_y[yid] * pos_y);
+                std::complex<T> w(wavelength * k_x[xid], wavelength * k_y[yid]);
+                T cchi = cchi_of(A, w);
+                T chi = (T)2.0 * (T)M_PI * cchi / wavelength;
+                out[id] = std::complex<T>(std::cos(-posTerm - chi), std::sin(-posTerm - chi));
+            } else {
+                out[id] = std::complex<T>(0, 0);
+            }
+        }
+}
+
+// ctem_image_d (kernels/ctem_image_d.cl:50-119)
+template <class T>
+static void ctem_image(const std::complex<T> *input, std::complex<T> *output, int W, int H, const T *k_x, const T *k_y,
+                       T wavelength, const Aberr<T> &A, T obj_ap, T ap_smooth, T beta, T delta) {
+    for (int yid = 0; yid < H; yid++)
+        for (int xid = 0; xid < W; xid++) {
+            int id = xid + yid * W;
+            T obj_ap2 = (obj_ap * (T)0.001) / wavelength;
+            T beta2 = (beta * (T)0.001) / wavelength;
+            T k = std::sqrt((k_x[xid] * k_x[xid]) + (k_y[yid] * k_y[yid]));
+            T ap_smooth_radius = (ap_smooth * (T)0.001) / wavelength;
+            if (k < obj_ap2 + ap_smooth_radius) {
+                std::complex<T> w(wavelength * k_x[xid], wavelength * k_y[yid]);
+                T temporalCoh = std::exp((T)-0.25 * (T)M_PI * (T)M_PI * delta * delta * cModSq(w) * cModSq(w) / (wavelength * wavelength));
+                T spatialCoh = std::exp((T)-1.0 * (T)M_PI * (T)M_PI * beta2 * beta2 * cModSq(w) *
+                                        std::pow((A.C10 + A.C30 * cModSq(w) + A.C50 * cModSq(w) * cModSq(w)), 2));
+                T cchi = cchi_of(A, w);
+                T chi = (T)2.0 * (T)M_PI * cchi / wavelength;
+                T edge_factor = 1.0;
+                if (std::fabs(k - obj_ap2) < ap_smooth_radius) {
+                    // smoothstep(e0, e1, x) = t*t*(3-2t), t = clamp((x-e0)/(e1-e0), 0, 1) (OpenCL C 1.2 6.12.4)
+                    T e0 = obj_ap2 - ap_smooth_radius, e1 = obj_ap2 + ap_smooth_radius;
+                    T t = std::min(std::max((k - e0) / (e1 - e0), (T)0), (T)1);
+                    edge_factor = (T)1.0 - t * t * ((T)3 - (T)2 * t);
+                }
+                output[id] = std::complex<T>(
+                    edge_factor * temporalCoh * spatialCoh * (input[id].real() * std::cos(chi) + input[id].imag() * std::sin(chi)),
+                    edge_factor * temporalCoh * spatialCoh * (input[id].imag() * std::cos(chi) - input[id].real() * std::sin(chi)));
+            } else {
+                output[id] = std::complex<T>(0, 0);
+            }
+        }
+}
+
+// fft_shift_d (kernels/fft_shift_d.cl:12-48)
+template <class T>
+static void fft_shift(const std::complex<T> *input, std::complex<T> *output, int W, int H) {
+    for (int yid = 0; yid < H; yid++)
+        for (int xid = 0; xid < W; xid++) {
+            int id = xid + yid * W;
+            int Yshift = W * H / 2, Xshift = W / 2, Xmid = W / 2, Ymid = H / 2;
+            if (xid < Xmid && yid < Ymid) output[id + Yshift + Xshift] = input[id];
+            else if (xid >= Xmid && yid < Ymid) output[id + Yshift - Xshift] = input[id];
+            else if (xid < Xmid && yid >= Ymid) output[id - Yshift + Xshift] = input[id];
+            else if (xid >= Xmid && yid >= Ymid) output[id - Yshift - Xshift] = input[id];
+        }
+}
+
+// getStemPixel -> complex_to_real(4) -> band_pass -> sum_reduction -> host sum
+// (simulationstem.cpp:42-132, complex_to_real_d.cl:12-37, band_pass_d.cl:15-38, sum_reduction_d.cl:13-35)
+template <class T>
+static double stem_pixel(const std::complex<T> *recip_wave, int W, int H, double angle_scale, const mslice_detector &d,
+                         std::vector<std::complex<T>> &shift_buf) {
+    fft_shift(recip_wave, shift_buf.data(), W, H);
+    T innerPx = (T)(d.inner / angle_scale), outerPx = (T)(d.outer / angle_scale);
+    T xcPx = (T)(d.xcentre / angle_scale), ycPx = (T)(d.ycentre / angle_scale);
+    unsigned int total = (unsigned int)W * H;
+    unsigned int nGroups = total / 256;
+    double sum = 0;
+    for (unsigned int g = 0; g < nGroups; g++) {
+        T gsum = 0;
+        for (unsigned int i = 0; i < 256; i++) {
+            unsigned int id = g * 256 + i;
+            int xid = (int)(id % W), yid = (int)(id / W);
+            T v = shift_buf[id].real() * shift_buf[id].real() + shift_buf[id].imag() * shift_buf[id].imag();
+            T centX = W / (T)2.0 + xcPx, centY = H / (T)2.0 + ycPx;
+            T radius = std::sqrt((xid - centX) * (xid - centX) + (yid - centY) * (yid - centY));
+            T o = (radius <= outerPx && radius >= innerPx) ? v : (T)0.0;
+            gsum += std::fabs(o);
+        }
+        sum += (double)(gsum * (T)M_SQRT2);
+    }
+    return sum;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Simulation (one configuration = one job)
+// ------------------------------------------------------------------------------------------------
+template <class T>
+struct Sim {
+    mslice_config c;
+    Geo G;
+    int res;
+    size_t N;
+    std::vector<T> kx, ky, params;
+    int form, i_count;
+    Atoms<T> atoms;
+    std::vector<std::vector<std::complex<T>>> trans;   // band-limited T per slice
+    std::vector<std::vector<std::complex<T>>> trans_raw;
+    std::vector<std::complex<T>> prop;
+
+    Sim(const mslice_config &cfg, int form_, int icount, const double *p, size_t np) : c(cfg), form(form_), i_count(icount) {
+        compute_geometry(c, G);
+        res = G.res;
+        N = (size_t)res * res;
+        kx.assign(G.kx.begin(), G.kx.end());
+        ky.assign(G.ky.begin(), G.ky.end());
+        params.assign(p, p + np);
+        prop.resize(N);
+        const mslice_geometry &g = G.g;
+        // propagator set up (simulationgeneral.cpp:623-637)
+        propagator<T>(prop.data(), kx.data(), ky.data(), res, res, (T)g.dz, (T)g.wavenumber, (T)g.wavevector[0],
+                      (T)g.wavevector[1], (T)g.wavevector[2], (T)(g.k_max * c.inverse_limit_factor));
+    }
+
+    PotArgs pot_args(int slice) const {
+        const mslice_geometry &g = G.g;
+        PotArgs a;
+        a.form = form; a.i_count = i_count;
+        a.width = res; a.height = res; a.current_slice = slice; a.total_slices = g.n_slices;
+        a.dz = g.dz; a.pixelscale = g.real_scale;
+        a.blocks_x = g.blocks_x; a.blocks_y = g.blocks_y;
+        a.max_x = g.full_x[1]; a.min_x = g.full_x[0]; a.max_y = g.full_y[1]; a.min_y = g.full_y[0];
+        a.block_load_x = g.load_blocks_x; a.block_load_y = g.load_blocks_y; a.slice_load_z = g.load_blocks_z;
+        a.sigma = g.sigma;
+        a.startx = g.sim_x[0]; a.starty = g.sim_y[0];   // + source-size perturbation (0, not modelled)
+        a.beam_theta = c.beam_tilt; a.beam_phi = c.beam_azimuth;
+        a.current_z = g.z_lims[0] + (g.n_slices - slice) * g.dz;   // simulationgeneral.cpp:590
+        a.shift_x = (g.wavevector[0] / g.wavevector[2]) * g.dz / c.full3d_integrals;   // :562-563
+        a.shift_y = (g.wavevector[1] / g.wavevector[2]) * g.dz / c.full3d_integrals;
+        a.integrals = c.full3d_integrals;
+        return a;
+    }
+
+    void set_atoms(size_t n, const int *Z, const double *x, const double *y, const double *z) {
+        sort_atoms<T>(c, G, n, Z, x, y, z, atoms);
+    }
+
+    void build_transmission() {
+        const mslice_geometry &g = G.g;
+        int S = g.n_slices;
+        trans.assign(S, std::vector<std::complex<T>>(N));
+        trans_raw.assign(S, std::vector<std::complex<T>>(N));
+        std::vector<std::complex<T>> tmp(N);
+        for (int s = 0; s < S; s++) {
+            PotArgs a = pot_args(s);
+            if (c.full3d) potential_full3d<T>(a, atoms, params.data(), trans_raw[s].data());
+            else potential_projected<T>(a, atoms, params.data(), trans_raw[s].data());
+            // FFT -> band_limit -> IFFT (simulationgeneral.cpp:596-602)
+            fft2<T>(res, res, trans_raw[s].data(), tmp.data(), -1);
+            band_limit<T>(tmp.data(), res, res, (T)g.k_max, (T)c.inverse_limit_factor, kx.data(), ky.data());
+            fft2<T>(res, res, tmp.data(), trans[s].data(), +1);
+        }
+    }
+
+    // probe in reciprocal space at an absolute position (SimulationCbed::initialiseProbeWave, simulationcbed.cpp:35-91)
+    void probe_k(double posx, double posy, std::complex<T> *out) const {
+        const mslice_geometry &g = G.g;
+        posx = posx - g.sim_x[0];
+        posy = posy - g.sim_y[0];
+        Aberr<T> A = aberrations<T>(c, c.C10);
+        init_probe<T>(out, res, res, kx.data(), ky.data(), (T)posx, (T)posy, (T)g.wavelength, A, (T)c.cond_ap, (T)c.cond_ap_smooth);
+    }
+
+    // doMultiSliceStep for one wave (simulationgeneral.cpp:744-764)
+    void step(int s, std::vector<std::complex<T>> &real, std::vector<std::complex<T>> &recip_w, std::vector<std::complex<T>> &tmp) const {
+        const auto &Ts = trans[s];
+        for (size_t i = 0; i < N; i++) recip_w[i] = cMult(Ts[i], real[i]);    // complex_multiply_d.cl:12-25
+        fft2<T>(res, res, recip_w.data(), tmp.data(), -1);
+        for (size_t i = 0; i < N; i++) recip_w[i] = cMult(tmp[i], prop[i]);
+        fft2<T>(res, res, recip_w.data(), real.data(), +1);
+    }
+
+    bool is_output(int s) const {
+        int step_n = c.intermediate_slices;
+        return step_n > 0 && (s + 1) % step_n == 0;
+    }
+
+    // STEM for the current configuration: out[(o*n_det + d)*n_pix + i]
+    void stem(const int *pixels, size_t n_pix, double *out) const {
+        const mslice_geometry &g = G.g;
+        int S = g.n_slices;
+        int n_out = g.n_outputs, n_det = c.n_detectors;
+        double start_x = c.stem_area[0], start_y = c.stem_area[2];
+        double step_x = (c.stem_area[1] - c.stem_area[0]) / c.stem_pixels_x;   // StemArea::getScaleX
+        double step_y = (c.stem_area[3] - c.stem_area[2]) / c.stem_pixels_y;
+        int num_x = c.stem_pixels_x;
+        std::fill(out, out + (size_t)n_out * n_det * n_pix, 0.0);
+        for (size_t i = 0; i < n_pix; i++) {
+            int p = pixels[i];
+            int x_i = p % num_x;
+            int y_i = (int)std::floor(p / num_x);
+            double x_pos = start_x + x_i * step_x, y_pos = start_y + y_i * step_y;
+            std::vector<std::complex<T>> real(N), recip_w(N), tmp(N), sh(N);
+            probe_k(x_pos, y_pos, recip_w.data());
+            fft2<T>(res, res, recip_w.data(), real.data(), +1);
+            int oc = 0;
+            for (int s = 0; s < S; s++) {
+                step(s, real, recip_w, tmp);
+                if (is_output(s)) {
+                    for (int d = 0; d < n_det; d++)
+                        out[((size_t)oc * n_det + d) * n_pix + i] = stem_pixel<T>(recip_w.data(), res, res, g.angle_scale, c.detectors[d], sh);
+                    oc++;
+                }
+            }
+            if (oc < n_out)
+                for (int d = 0; d < n_det; d++)
+                    out[((size_t)oc * n_det + d) * n_pix + i] = stem_pixel<T>(recip_w.data(), res, res, g.angle_scale, c.detectors[d], sh);
+        }
+    }
+
+    void diffraction(const std::vector<std::complex<T>> &recip_w, double *out) const {
+        std::vector<std::complex<T>> sh(N);
+        fft_shift(recip_w.data(), sh.data(), res, res);
+        for (size_t i = 0; i < N; i++) out[i] = (double)(sh[i].real() * sh[i].real() + sh[i].imag() * sh[i].imag());
+    }
+
+    void cbed(double *diff) const {
+        const mslice_geometry &g = G.g;
+        int S = g.n_slices;
+        std::vector<std::complex<T>> real(N), recip_w(N), tmp(N);
+        probe_k(c.cbed_x, c.cbed_y, recip_w.data());
+        fft2<T>(res, res, recip_w.data(), real.data(), +1);
+        int oc = 0;
+        for (int s = 0; s < S; s++) {
+            step(s, real, recip_w, tmp);
+            if (is_output(s)) { diffraction(recip_w, diff + (size_t)oc * N); oc++; }
+        }
+        if (oc < g.n_outputs) diffraction(recip_w, diff + (size_t)oc * N);
+    }
+
+    void ctem_outputs(const std::vector<std::complex<T>> &real, const std::vector<std::complex<T>> &recip_w, int oc,
+                      double *ew, double *diff, double *image) const {
+        const mslice_geometry &g = G.g;
+        if (ew) for (size_t i = 0; i < N; i++) { ew[(size_t)oc * 2 * N + 2 * i] = real[i].real(); ew[(size_t)oc * 2 * N + 2 * i + 1] = real[i].imag(); }
+        if (diff) diffraction(recip_w, diff + (size_t)oc * N);
+        if (image && c.ctem_image) {
+            // simulateImagePerfect (simulationctem.cpp:114-166)
+            std::vector<std::complex<T>> im(N), tmp(N);
+            Aberr<T> A = aberrations<T>(c, c.C10);
+            ctem_image<T>(recip_w.data(), im.data(), res, res, kx.data(), ky.data(), (T)g.wavelength, A, (T)c.obj_ap,
+                          (T)c.obj_ap_smooth, (T)c.alpha, (T)c.delta);
+            fft2<T>(res, res, im.data(), tmp.data(), +1);
+            for (size_t i = 0; i < N; i++) image[(size_t)oc * N + i] = (double)(tmp[i].real() * tmp[i].real() + tmp[i].imag() * tmp[i].imag());
+        }
+    }
+
+    void ctem(double *ew, double *diff, double *image) const {
+        const mslice_geometry &g = G.g;
+        int S = g.n_slices;
+        std::vector<std::complex<T>> real(N, std::complex<T>(1, 0)), recip_w(N), tmp(N);   // init_plane_wave value 1.0
+        int oc = 0;
+        for (int s = 0; s < S; s++) {
+            step(s, real, recip_w, tmp);
+            if (is_output(s)) { ctem_outputs(real, recip_w, oc, ew, diff, image); oc++; }
+        }
+        if (oc < g.n_outputs) ctem_outputs(real, recip_w, oc, ew, diff, image);
+    }
+};
+
+}  // namespace orc
+
+// =================================================================================================
+// C API of the oracle (loaded by tests via ctypes)
+// =================================================================================================
+using namespace orc;
+
+static thread_local std::string g_err;
+
+template <class F>
+static int guard(F &&f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
+struct OrcSim {
+    int dp;
+    Sim<double> *sd = nullptr;
+    Sim<float> *sf = nullptr;
+    ~OrcSim() { delete sd; delete sf; }
+};
+
+extern "C" {
+
+const char *orc_last_error(void) { return g_err.c_str(); }
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+int orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#endif
+    (void)n;
+    return 0;
+}
+
+int orc_geometry(const mslice_config *c, mslice_geometry *out, double *kx, double *ky) {
+    return guard([&] {
+        Geo G;
+        compute_geometry(*c, G);
+        *out = G.g;
+        if (kx) std::copy(G.kx.begin(), G.kx.end(), kx);
+        if (ky) std::copy(G.ky.begin(), G.ky.end(), ky);
+    });
+}
+
+int orc_sim_create(const mslice_config *c, int form, int i_count, const double *params, size_t np, int double_precision, OrcSim **out) {
+    return guard([&] {
+        OrcSim *s = new OrcSim();
+        s->dp = double_precision;
+        try {
+            if (double_precision) s->sd = new Sim<double>(*c, form, i_count, params, np);
+            else s->sf = new Sim<float>(*c, form, i_count, params, np);
+        } catch (...) { delete s; throw; }
+        *out = s;
+    });
+}
+int orc_sim_destroy(OrcSim *s) { delete s; return 0; }
+
+int orc_set_atoms(OrcSim *s, size_t n, const int *Z, const double *x, const double *y, const double *z) {
+    return guard([&] { if (s->dp) s->sd->set_atoms(n, Z, x, y, z); else s->sf->set_atoms(n, Z, x, y, z); });
+}
+
+int orc_get_sorted_atoms(OrcSim *s, int *Z, double *x, double *y, double *z, size_t cap, int *bs, size_t cap_bs,
+                         int *bid, int *zid, size_t *n_out) {
+    return guard([&] {
+        auto go = [&](auto *S) {
+            auto &a = S->atoms;
+            size_t n = a.A.size();
+            if (n > cap || a.block_start.size() > cap_bs) throw std::invalid_argument("capacity too small");
+            for (size_t i = 0; i < n; i++) { Z[i] = a.A[i]; x[i] = a.x[i]; y[i] = a.y[i]; z[i] = a.z[i]; }
+            std::copy(a.block_start.begin(), a.block_start.end(), bs);
+            if (bid) std::copy(a.block_ids.begin(), a.block_ids.end(), bid);
+            if (zid) std::copy(a.z_ids.begin(), a.z_ids.end(), zid);
+            *n_out = n;
+        };
+        if (s->dp) go(s->sd); else go(s->sf);
+    });
+}
+
+int orc_build_transmission(OrcSim *s) {
+    return guard([&] { if (s->dp) s->sd->build_transmission(); else s->sf->build_transmission(); });
+}
+
+int orc_get_transmission(OrcSim *s, int slice, int band_limited, double *out) {
+    return guard([&] {
+        auto go = [&](auto *S) {
+            if (slice < 0 || slice >= (int)S->trans.size()) throw std::invalid_argument("slice out of range");
+            const auto &v = band_limited ? S->trans[slice] : S->trans_raw[slice];
+            for (size_t i = 0; i < v.size(); i++) { out[2 * i] = v[i].real(); out[2 * i + 1] = v[i].imag(); }
+        };
+        if (s->dp) go(s->sd); else go(s->sf);
+    });
+}
+
+int orc_get_propagator(OrcSim *s, double *out) {
+    return guard([&] {
+        auto go = [&](auto *S) { for (size_t i = 0; i < S->N; i++) { out[2 * i] = S->prop[i].real(); out[2 * i + 1] = S->prop[i].imag(); } };
+        if (s->dp) go(s->sd); else go(s->sf);
+    });
+}
+
+int orc_get_probe(OrcSim *s, double x, double y, double *out) {
+    return guard([&] {
+        auto go = [&](auto *S) {
+            using C = typename std::remove_reference<decltype(S->prop)>::type::value_type;
+            std::vector<C> v(S->N);
+            S->probe_k(x, y, v.data());
+            for (size_t i = 0; i < S->N; i++) { out[2 * i] = v[i].real(); out[2 * i + 1] = v[i].imag(); }
+        };
+        if (s->dp) go(s->sd); else go(s->sf);
+    });
+}
+
+// STEM over many pixels, parallel over pixels with OpenMP (each pixel is independent)
+int orc_stem_run(OrcSim *s, const int *pixels, size_t n_pix, double *out) {
+    return guard([&] {
+        auto go = [&](auto *S) {
+            int n_out = S->G.g.n_outputs, n_det = S->c.n_detectors;
+            std::vector<double> tmp((size_t)n_out * n_det);
+            std::vector<double> res((size_t)n_out * n_det * n_pix, 0.0);
+#pragma omp parallel for schedule(dynamic)
+            for (long i = 0; i < (long)n_pix; i++) {
+                std::vector<double> one((size_t)n_out * n_det);
+                S->stem(pixels + i, 1, one.data());
+                for (int o = 0; o < n_out; o++)
+                    for (int d = 0; d < n_det; d++) res[((size_t)o * n_det + d) * n_pix + i] = one[(size_t)o * n_det + d];
+            }
+            std::copy(res.begin(), res.end(), out);
+        };
+        if (s->dp) go(s->sd); else go(s->sf);
+    });
+}
+
+int orc_cbed_run(OrcSim *s, double *diff) {
+    return guard([&] { if (s->dp) s->sd->cbed(diff); else s->sf->cbed(diff); });
+}
+
+int orc_ctem_run(OrcSim *s, double *ew, double *diff, double *image) {
+    return guard([&] { if (s->dp) s->sd->ctem(ew, diff, image); else s->sf->ctem(ew, diff, image); });
+}
+
+// standalone building blocks for KATs
+int orc_fft2(int n, int inverse, const double *in, double *out) {
+    return guard([&] {
+        std::vector<std::complex<double>> a((size_t)n * n), b((size_t)n * n);
+        for (size_t i = 0; i < a.size(); i++) a[i] = {in[2 * i], in[2 * i + 1]};
+        fft2<double>(n, n, a.data(), b.data(), inverse ? +1 : -1);
+        for (size_t i = 0; i < b.size(); i++) { out[2 * i] = b[i].real(); out[2 * i + 1] = b[i].imag(); }
+    });
+}
+
+// single-atom projected / 3-D potential values for KATs against the published formulas
+double orc_potential_value(int form, int three_d, const double *params, int i_count, int Z, double rad) {
+    if (three_d) {
+        if (form == 0) return kirkland_3d<double>(params, i_count, Z, rad);
+        if (form == 1) return peng_3d<double>(params, i_count, Z, rad);
+        return lobato_3d<double>(params, i_count, Z, rad);
+    }
+    if (form == 0) return kirkland_proj<double>(params, i_count, Z, rad);
+    if (form == 1) return peng_proj<double>(params, i_count, Z, rad);
+    return lobato_proj<double>(params, i_count, Z, rad);
+}
+
+double orc_bessk0(double x) { return bessk0<double>(x); }
+double orc_bessk1(double x) { return bessk1<double>(x); }
+
+}  // extern "C"
