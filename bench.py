@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""Batched STEM ADF multislice throughput on B200 (probe·slices/s).
+
+Workload (one GPU): cubic perovskite supercell (a = 3.905 Å, Sr/Ti/O) tiled 10x10x20 (10,000 atoms),
+512x512 grid, 300 kV probe with 24 mrad convergence, Cs = 1 um, C1 = 0, 64x64 probe positions on a
+0.2 Å raster, 40 slices of 1.9525 Å, ADF detector 70-200 mrad, frozen phonons with isotropic Gaussian
+displacements u_rms = 0.08 Å (seeded). The complex64 engine (FP64 phase arguments and accumulation).
+
+A step is one frozen-phonon configuration: bin the atoms, build and band-limit the 40 transmission
+functions, generate the 4096 probes and propagate them through all 40 slices with the fused FFT passes,
+and accumulate the ADF image (FP64, Kahan). The default K = 10 steps is the full 10-configuration job.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank runs K configurations of its own (weak scaling); the
+averaged images are combined with one NCCL reduction at the end (the reference merges per-device
+results in SimulationManager::updateImages).
+
+--impl reference times the CPU restatement of the reference's double-precision path (the reference's
+OpenCL build cannot be compiled or run here) on the host cores, on a bounded sample of the same
+workload per step, reported in the same unit.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "STEM probe·slices/s at 512² FP32 vs plain FP64 GPU; adjoint/forward time ratio"
+UNIT = "probe·slices/s"
+WORKLOAD = "stem_adf_perovskite_10x10x20_512x512_64x64probes_40slices_phonon_u0.08"
+BYTES_ROW = 24   # algorithmic bytes per pixel of one wave in the row pass: read psi, read T, write psi (FP32 complex)
+BYTES_COL = 16   # column pass: read psi, write psi
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="mslice", choices=["mslice", "reference"])
+    p.add_argument("--batch", type=int, default=0, help="probes propagated together (0 = engine default)")
+    p.add_argument("--scan", type=int, default=64)
+    p.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline and plain-FP64 legs")
+    p.add_argument("--cpu-probes", type=int, default=32, help="probes in the bounded CPU sample")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+
+
+def workload(scan=64, double_precision=False):
+    from cltem_b200 import config
+    s, st = config.perovskite_stem(n=(10, 10, 20), resolution=512, scan=scan, double_precision=double_precision)
+    return s, st
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples of one GPU during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.uuid:
+                cmd += ["-i", self.uuid]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:  # noqa: BLE001
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:  # noqa: BLE001
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, pw, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+                pw.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------------
+# CPU legs (oracle): the baseline beside our line, and the whole reference arm
+# ---------------------------------------------------------------------------------------------------
+def cpu_sample(n_probes, double_precision, seed=0):
+    """Time the CPU restatement on a bounded sample of one configuration of the workload: the
+    transmission build of all 40 slices plus n_probes probes through all slices; return the implied
+    probe·slices/s for a full 4096-probe configuration."""
+    from oracle import bind as ob
+    from cltem_b200.params import load_default
+    from cltem_b200.structure import phonon_configs
+    s, st = workload()
+    conf = phonon_configs(st, 1, 0.08, seed=1000 + seed)[0]
+    osim = ob.OracleSim(s.cfg, load_default("kirkland"), double_precision=double_precision)
+    osim.set_atoms(conf)
+    t0 = time.perf_counter()
+    osim.build_transmission()
+    t1 = time.perf_counter()
+    npx = s.cfg.stem_pixels_x * s.cfg.stem_pixels_y
+    rng = np.random.default_rng(seed)
+    pix = np.sort(rng.choice(npx, size=n_probes, replace=False)).astype(np.int32)
+    osim.stem(pix)
+    t2 = time.perf_counter()
+    S = osim.geo.n_slices
+    full = npx * S / ((t1 - t0) + (t2 - t1) * npx / n_probes)
+    return full, {"build_s": t1 - t0, "propagate_s": t2 - t1, "probes": n_probes, "slices": S, "configs": 1}
+
+
+def cpu_baseline_leg(n_probes):
+    from oracle import bind as ob
+    threads = ob.num_threads()
+    v, info = cpu_sample(n_probes, double_precision=False)
+    return {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"CPU oracle (C++/OpenMP restatement of the reference path, FP32 instantiation) on one "
+                       f"phonon configuration: transmission build of {info['slices']} slices "
+                       f"({info['build_s']:.1f} s) + {n_probes} of 4096 probes through all slices "
+                       f"({info['propagate_s']:.1f} s), scaled to a 4096-probe configuration"),
+            "threads": threads}
+
+
+def run_reference(args):
+    rank, local, world = dist_env()
+    if world > 1 and rank != 0:
+        return 0
+    from oracle import bind as ob
+    ob.lib()
+    threads = ob.num_threads()
+    n_probes = max(4, args.cpu_probes // 4)
+    for w in range(args.warmup):   # untimed: a tiny sample
+        cpu_sample(1, double_precision=True, seed=100 + w)
+    vals, infos = [], []
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        v, info = cpu_sample(n_probes, double_precision=True, seed=k)
+        vals.append(v)
+        infos.append(info)
+    wall = time.perf_counter() - t0
+    value = statistics.mean(vals)
+    S = infos[0]["slices"]
+    ms_per_step = 4096 * S / value * 1000.0
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": 512, "probes": 4096, "slices": S,
+                   "parallelism": "host threads (OpenMP)", "sample_wall_s": wall},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": (f"per step: transmission build of {S} slices + {n_probes} of 4096 probes "
+                                    f"through all slices of one phonon configuration, FP64 (the reference's _d path), "
+                                    f"scaled to a 4096-probe configuration; the reference's OpenCL CPU-device build "
+                                    f"needs OpenCL headers/ICD and clFFT, absent here")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.warmup < 3:
+        print("warning: the timing rules ask for >= 3 warm-up steps", file=sys.stderr)
+    rank, local, world = dist_env()
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    from cltem_b200.engine import Context, Simulation
+    from cltem_b200.params import load_default
+    from cltem_b200.structure import phonon_configs, concat_configs
+
+    s, st = workload(scan=args.scan)
+    if args.batch:
+        s.cfg.probe_batch = args.batch
+    ctx = Context(local)
+    ctx.load_params(load_default("kirkland"))
+    sim = Simulation(ctx, s.cfg)
+    S = sim.geo.n_slices
+    npx = s.cfg.stem_pixels_x * s.cfg.stem_pixels_y
+    N = 512 * 512
+    ext = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    # warm-up: W configurations (untimed)
+    warm = phonon_configs(st, args.warmup, 0.08, seed=10_000 + rank)
+    sim.stage(warm)
+    sim.run_staged()
+    # timed: K configurations staged in HBM before the timed region (inputs resident)
+    confs = phonon_configs(st, args.steps, 0.08, seed=rank)
+    sim.stage(confs)
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+        uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    except Exception:  # noqa: BLE001
+        uuid = None
+    clocks = ClockSampler(uuid)
+    sim.profile(True)
+    sim.profile_read(reset=True)
+    l0 = ctx.launch_count()
+    barrier()
+    clocks.start()
+    time.sleep(0.4)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    sim.run_staged()
+    e1.record(ext)
+    e1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = ctx.launch_count() - l0
+    prof = sim.profile_read()
+    sim.profile(False)
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    img = sim.staged_result()
+    # one exchange step: sum the per-rank averaged images (SimulationManager::updateImages merge)
+    timg = torch.from_numpy(np.ascontiguousarray(img)).cuda()
+    if world > 1:
+        dist.all_reduce(timg)
+        timg /= world
+
+    probe_slices = npx * S * args.steps * world
+    value = probe_slices / (ms_max / 1000.0)
+
+    # roofline of the dominant kernel (by device time) from the live event timings
+    row_ms, row_n = prof["row_step"]
+    col_ms, col_n = prof["col_step"]
+    wave_px = npx * S * args.steps * N           # pixels of all waves over all slices on this rank
+    row_bytes = BYTES_ROW * wave_px
+    col_bytes = BYTES_COL * wave_px
+    dom = ("row_step", row_bytes, row_ms, row_n) if row_ms >= col_ms else ("col_step", col_bytes, col_ms, col_n)
+    peak, peak_src = peaks()
+    achieved = dom[1] / (dom[2] / 1000.0) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            tj = json.load(f)
+        per_wave = tj[dom[0]]["dram_bytes_per_wave"]
+        traffic = per_wave * (npx * S * args.steps) / max(dom[3], 1)
+    except Exception:  # noqa: BLE001
+        traffic = None
+    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": dom[1] / max(dom[3], 1), "avg_launch_ms": dom[2] / max(dom[3], 1),
+                "pair_achieved_gbs": (row_bytes + col_bytes) / ((row_ms + col_ms) / 1000.0) / 1e9,
+                "kernel_ms": {k: v[0] for k, v in prof.items()}, "kernel_launches": {k: v[1] for k, v in prof.items()}}
+
+    # end to end through the public API: one configuration per step from pinned host memory, result back
+    e2e = None
+    if rank == 0 or world > 1:
+        cnt, Z, x, y, z = concat_configs(confs[:1])
+        pinned = [torch.from_numpy(a).pin_memory() for a in (Z, x, y, z)]
+        out = torch.zeros(sim.result_size(), dtype=torch.float64).pin_memory()
+        cnt_arr = np.ascontiguousarray(cnt)
+        lib = ctx.lib
+        ptr = lambda tns, ty: C.cast(C.c_void_p(tns.data_ptr()), C.POINTER(ty))
+        e2e_confs = phonon_configs(st, min(args.steps, 3), 0.08, seed=50_000 + rank)
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(ext)
+        for c in e2e_confs:
+            _, Zc, xc, yc, zc = concat_configs([c])
+            for dst, src in zip(pinned, (Zc, xc, yc, zc)):
+                dst.numpy()[:] = src
+            rc = lib.mslice_stem_simulate(sim.h, 1, cnt_arr.ctypes.data_as(C.POINTER(C.c_size_t)), ptr(pinned[0], C.c_int),
+                                          ptr(pinned[1], C.c_double), ptr(pinned[2], C.c_double), ptr(pinned[3], C.c_double),
+                                          ptr(out, C.c_double), out.numel())
+            assert rc == 0, lib.mslice_last_error()
+        f1.record(ext)
+        f1.synchronize()
+        ms_e2e = f0.elapsed_time(f1)
+        te = torch.tensor([ms_e2e], device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        ms_e2e = float(te.item())
+        h2d = int(sum(p.numel() * p.element_size() for p in pinned))
+        e2e = {"value": npx * S * len(e2e_confs) * world / (ms_e2e / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(out.numel() * 8),
+               "steps": len(e2e_confs), "ms_per_step": ms_e2e / len(e2e_confs)}
+
+    cpu = plain = None
+    if rank == 0 and world == 1 and not args.no_baseline:
+        # plain per-probe FP64 GPU path (the reference's unfused order with cuFFT Z2Z) on a sample
+        sd, std_ = workload(double_precision=True)
+        simd = Simulation(ctx, sd.cfg)
+        simd.set_atoms(confs[0])
+        simd.build_transmission()
+        pix = np.arange(8, dtype=np.int32)
+        simd.stem_plain(pix[:1])
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(ext)
+        simd.stem_plain(pix)
+        g1.record(ext)
+        g1.synchronize()
+        pms = g0.elapsed_time(g1)
+        pv = len(pix) * S / (pms / 1000.0)
+        plain = {"value": pv, "unit": UNIT, "sample": f"{len(pix)} probes x {S} slices, FP64, one probe at a time",
+                 "fused_fp32_over_plain_fp64": value / pv}
+        simd.close()
+        cpu = cpu_baseline_leg(args.cpu_probes)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": 512, "probes": npx, "slices": S,
+                       "phonon_configs_per_gpu": args.steps, "probe_batch": sim.cfg.probe_batch or "engine default",
+                       "precision": "complex64 waves and FFTs; FP64 phase arguments, offsets and Kahan accumulation",
+                       "l2": "inputs larger than L2 (per configuration: 4096 waves x 2 MiB + 40 transmission slices x 2 MiB)",
+                       "parallelism": f"dp{world} (phonon configurations sharded over GPUs)"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "plain_fp64_gpu": plain,
+            "adjoint_forward_ratio": None,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -250,7 +250,44 @@ struct SimBase {
     mslice_progress_cb progress = nullptr;
     void *progress_user = nullptr;
     double timing[3] = {0, 0, 0};
-    virtual ~SimBase() = default;
+    // per-kernel event timing (mslice_profile_enable)
+    bool prof = false;
+    double prof_ms[MSLICE_K_COUNT] = {};
+    unsigned long long prof_n[MSLICE_K_COUNT] = {};
+    struct Pending { int kind; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> ev_pool;
+    cudaEvent_t take_event() {
+        if (!ev_pool.empty()) { cudaEvent_t e = ev_pool.back(); ev_pool.pop_back(); return e; }
+        cudaEvent_t e;
+        MS_CUDA(cudaEventCreate(&e));
+        return e;
+    }
+    template <class F> void timed(cudaStream_t s, int kind, F &&launch) {
+        if (!prof) { launch(); return; }
+        cudaEvent_t a = take_event(), b = take_event();
+        MS_CUDA(cudaEventRecord(a, s));
+        launch();
+        MS_CUDA(cudaEventRecord(b, s));
+        pending.push_back({kind, a, b});
+    }
+    // after a stream sync: fold the recorded launch durations into the totals
+    void flush_profile() {
+        for (auto &p : pending) {
+            float ms = 0;
+            MS_CUDA(cudaEventSynchronize(p.b));
+            MS_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+            prof_ms[p.kind] += ms;
+            prof_n[p.kind]++;
+            ev_pool.push_back(p.a);
+            ev_pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    virtual ~SimBase() {
+        for (auto &p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+        for (auto e : ev_pool) cudaEventDestroy(e);
+    }
     virtual void set_atoms(const int *Z, const double *x, const double *y, const double *z, size_t n, bool host) = 0;
     virtual void get_sorted(int *Z, double *x, double *y, double *z, size_t cap, int *bs, size_t cap_bs, int *bid, int *zid,
                             size_t *n_out) = 0;
@@ -499,17 +536,21 @@ struct Sim : SimBase {
     }
 
     void potentials(C *out, int slice0, int count) {
-        launch_potential<R>(st(), cfg.full3d != 0, out, count, axs.p, ays.p, azs.p, aZs.p, block_start.p, params_dev(),
-                            pot_params(slice0));
+        timed(st(), MSLICE_K_POTENTIAL, [&] {
+            launch_potential<R>(st(), cfg.full3d != 0, out, count, axs.p, ays.p, azs.p, aZs.p, block_start.p, params_dev(),
+                                pot_params(slice0));
+        });
         ctx->launches++;
     }
 
     void band_limit(C *t, int count) {
         // FFT -> band_limit (k <= k_max * factor, inclusive) -> IFFT, clFFT scale s2d per transform
         const cplx<R> *tw = ctx->twiddles<R>(N);
-        ops.row_fft(st(), t, t, count, tw, (R)1, -1);
-        ops.col_bandlimit(st(), t, count, tw, kx2.p, ky2.p, H.g.k_max * cfg.inverse_limit_factor, (R)(s2d * s2d));
-        ops.row_fft(st(), t, t, count, tw, (R)1, +1);
+        timed(st(), MSLICE_K_BANDLIMIT, [&] {
+            ops.row_fft(st(), t, t, count, tw, (R)1, -1);
+            ops.col_bandlimit(st(), t, count, tw, kx2.p, ky2.p, H.g.k_max * cfg.inverse_limit_factor, (R)(s2d * s2d));
+            ops.row_fft(st(), t, t, count, tw, (R)1, +1);
+        });
         ctx->launches += 3;
     }
 
@@ -623,7 +664,7 @@ struct Sim : SimBase {
         for (int i = 0; i < nb; i++) h_pos[i] = probe_pos(ids[i]);
         MS_CUDA(cudaMemcpyAsync(pos.p, h_pos.data(), nb * sizeof(double2), cudaMemcpyHostToDevice, st()));
         MS_CUDA(cudaMemcpyAsync(pix.p, h_pix.data(), nb * sizeof(int), cudaMemcpyHostToDevice, st()));
-        ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N));
+        timed(st(), MSLICE_K_PROBE, [&] { ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N)); });
         ctx->launches++;
         PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
         DetArgs det{detmask.p, cfg.n_detectors, partials.p};
@@ -631,10 +672,10 @@ struct Sim : SimBase {
         size_t oi = 0;
         const R a = (R)(1.0 / N), b = (R)(s2d * s2d * N), ds = (R)s2d;
         for (int s = 0; s < g.n_slices; s++) {
-            ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a);
+            timed(st(), MSLICE_K_ROW_STEP, [&] { ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a); });
             bool is_out = oi < outs.size() && outs[oi] == s;
             int mode = !is_out ? COL_STEP : (s == g.n_slices - 1 ? COL_DET_ONLY : COL_STEP_DET);
-            ops.col_step(st(), wave.p, nb, tw, pt, b, ds, det, nullptr, mode);
+            timed(st(), MSLICE_K_COL_STEP, [&] { ops.col_step(st(), wave.p, nb, tw, pt, b, ds, det, nullptr, mode); });
             ctx->launches += 2;
             if (is_out) {
                 detector_reduce(st(), partials.p, ops.col_blocks, cfg.n_detectors, nb, pix.p, n_pix, (int)oi, out, comp);
@@ -664,6 +705,7 @@ struct Sim : SimBase {
             int nb = (int)std::min<size_t>(batch_cap, n - b0);
             stem_batch(pixels + b0, idx.data() + b0, nb, (int)n, dout.p, nullptr);
             MS_CUDA(cudaStreamSynchronize(st()));
+            flush_profile();
             if (progress) progress((double)(b0 + nb) / n, progress_user);
         }
         if (tot) MS_CUDA(cudaMemcpy(out, dout.p, tot * sizeof(double), cudaMemcpyDeviceToHost));
@@ -690,9 +732,11 @@ struct Sim : SimBase {
         const R a = (R)(1.0 / N), b = (R)(s2d * s2d * N), ds = (R)s2d;
         for (int s = 0; s < g.n_slices; s++) {
             check_cancel();
-            ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a);
+            timed(st(), MSLICE_K_ROW_STEP, [&] { ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a); });
             bool is_out = oi < outs.size() && outs[oi] == s;
-            ops.col_step(st(), wave.p, 1, tw, pt, b, ds, det, is_out ? recip.p : nullptr, is_out ? COL_STEP_DET : COL_STEP);
+            timed(st(), MSLICE_K_COL_STEP, [&] {
+                ops.col_step(st(), wave.p, 1, tw, pt, b, ds, det, is_out ? recip.p : nullptr, is_out ? COL_STEP_DET : COL_STEP);
+            });
             ctx->launches += 2;
             if (is_out) { on_output((int)oi); oi++; }
             if (progress) progress((double)(s + 1) / g.n_slices, progress_user);
@@ -799,6 +843,7 @@ struct Sim : SimBase {
             }
             MS_CUDA(cudaEventRecord(ev[3], st()));
             MS_CUDA(cudaEventSynchronize(ev[3]));
+            flush_profile();
             float a = 0, b = 0;
             MS_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
             MS_CUDA(cudaEventElapsedTime(&b, ev[1], ev[3]));
@@ -1182,6 +1227,30 @@ int mslice_ctx_launch_count(mslice_ctx *ctx, unsigned long long *count) {
     return guarded([&] {
         need(ctx && count, "null argument");
         *count = ctx->impl.launches;
+    });
+}
+
+int mslice_profile_enable(mslice_sim *sim, int on) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        use_device(sim->ctx);
+        MS_CUDA(cudaStreamSynchronize(sim->ctx->impl.stream));
+        sim->impl->flush_profile();
+        sim->impl->prof = on != 0;
+    });
+}
+
+int mslice_profile_read(mslice_sim *sim, int kernel, double *total_ms, unsigned long long *launches, int reset) {
+    return guarded([&] {
+        need(sim && total_ms && launches, "null argument");
+        need(kernel >= 0 && kernel < MSLICE_K_COUNT, "unknown kernel kind");
+        use_device(sim->ctx);
+        MS_CUDA(cudaStreamSynchronize(sim->ctx->impl.stream));
+        sim->impl->flush_profile();
+        *total_ms = sim->impl->prof_ms[kernel];
+        *launches = sim->impl->prof_n[kernel];
+        if (reset)
+            for (int k = 0; k < MSLICE_K_COUNT; k++) { sim->impl->prof_ms[k] = 0; sim->impl->prof_n[k] = 0; }
     });
 }
 

@@ -244,6 +244,18 @@ int mslice_ctx_launch_count(mslice_ctx *ctx, unsigned long long *count);
  * [transmission build, propagation passes, total]. */
 int mslice_last_timing(mslice_sim *sim, double *ms3);
 
+/* Per-kernel device timing: when enabled, every launch of the kinds below is bracketed by CUDA events
+ * on the ctx stream and its duration accumulated (adds two event records per launch). */
+#define MSLICE_K_ROW_STEP 0   /* fused row pass of the multislice step        */
+#define MSLICE_K_COL_STEP 1   /* fused column pass of the multislice step     */
+#define MSLICE_K_POTENTIAL 2  /* slice potential / transmission kernel        */
+#define MSLICE_K_BANDLIMIT 3  /* the three passes of the transmission band limit */
+#define MSLICE_K_PROBE 4      /* probe generation + column inverse FFT        */
+#define MSLICE_K_COUNT 5
+int mslice_profile_enable(mslice_sim *sim, int on);
+/* Accumulated device ms and launch count of one kernel kind since the last reset; reset != 0 clears. */
+int mslice_profile_read(mslice_sim *sim, int kernel, double *total_ms, unsigned long long *launches, int reset);
+
 #ifdef __cplusplus
 }
 #endif

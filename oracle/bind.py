@@ -57,6 +57,9 @@ def lib():
         L.orc_fft2.argtypes = [C.c_int, C.c_int, _dp, _dp]
         L.orc_geometry.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Geometry), _dp, _dp]
         L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_k_stem_pixel.restype = C.c_double
+        L.orc_k_stem_pixel.argtypes = [_dp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.orc_k_ctem_image.argtypes = [C.POINTER(abi.Config), _dp, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -93,6 +96,25 @@ def fft2(a, inverse=False):
     flat[1::2] = a.imag.ravel()
     out = np.empty_like(flat)
     _chk(lib().orc_fft2(n, int(inverse), _d(flat), _d(out)))
+    return cplx(out).reshape(n, n)
+
+
+def stem_pixel(recip, angle_scale, inner, outer, xc=0.0, yc=0.0):
+    n = recip.shape[0]
+    flat = np.empty(2 * n * n)
+    flat[0::2] = recip.real.ravel()
+    flat[1::2] = recip.imag.ravel()
+    return lib().orc_k_stem_pixel(_d(flat), n, angle_scale, inner, outer, xc, yc)
+
+
+def ctem_image(cfg, recip):
+    g, kx, ky = geometry(cfg)
+    n = recip.shape[0]
+    flat = np.empty(2 * n * n)
+    flat[0::2] = recip.real.ravel()
+    flat[1::2] = recip.imag.ravel()
+    out = np.empty_like(flat)
+    _chk(lib().orc_k_ctem_image(C.byref(cfg), _d(kx), _d(ky), _d(flat), _d(out)))
     return cplx(out).reshape(n, n)
 
 

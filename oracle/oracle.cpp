@@ -1178,6 +1178,30 @@ double orc_potential_value(int form, int three_d, const double *params, int i_co
     return lobato_proj<double>(params, i_count, Z, rad);
 }
 
+// kernel-level entry points used to pin the restatement against the reference's own kernels
+// getStemPixel on a given reciprocal wave (fft_shift + complex_to_real(4) + band_pass + sum_reduction)
+double orc_k_stem_pixel(const double *recip, int n, double angle_scale, double inner, double outer, double xc, double yc) {
+    std::vector<std::complex<double>> r((size_t)n * n), sh((size_t)n * n);
+    for (size_t i = 0; i < r.size(); i++) r[i] = {recip[2 * i], recip[2 * i + 1]};
+    mslice_detector d;
+    std::memset(&d, 0, sizeof(d));
+    d.inner = inner; d.outer = outer; d.xcentre = xc; d.ycentre = yc;
+    return stem_pixel<double>(r.data(), n, n, angle_scale, d, sh);
+}
+
+// ctem_image_d on a given reciprocal wave with a config's aberrations and apertures
+int orc_k_ctem_image(const mslice_config *c, const double *kx, const double *ky, const double *in, double *out) {
+    return guard([&] {
+        int n = c->resolution;
+        std::vector<std::complex<double>> a((size_t)n * n), b((size_t)n * n);
+        for (size_t i = 0; i < a.size(); i++) a[i] = {in[2 * i], in[2 * i + 1]};
+        Aberr<double> A = aberrations<double>(*c, c->C10);
+        ctem_image<double>(a.data(), b.data(), n, n, kx, ky, wavelength(c->voltage), A, c->obj_ap, c->obj_ap_smooth,
+                           c->alpha, c->delta);
+        for (size_t i = 0; i < b.size(); i++) { out[2 * i] = b[i].real(); out[2 * i + 1] = b[i].imag(); }
+    });
+}
+
 double orc_bessk0(double x) { return bessk0<double>(x); }
 double orc_bessk1(double x) { return bessk1<double>(x); }
 
