@@ -24,6 +24,7 @@
 namespace ms {
 
 static thread_local std::string g_last_error;
+void set_last_error(const std::string &msg) { g_last_error = msg; }
 
 struct ArgError : std::runtime_error { using std::runtime_error::runtime_error; };
 struct StateError : std::runtime_error { using std::runtime_error::runtime_error; };

@@ -256,6 +256,22 @@ int mslice_profile_enable(mslice_sim *sim, int on);
 /* Accumulated device ms and launch count of one kernel kind since the last reset; reset != 0 clears. */
 int mslice_profile_read(mslice_sim *sim, int kernel, double *total_ms, unsigned long long *launches, int reset);
 
+/* Atom binning without any device allocation (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc: a host application that manages all device memory through its
+ * own pool, or a pipeline stage that must not take cudaMalloc/cudaFree's latency and implicit device
+ * synchronisation. Bins n atoms exactly like mslice_set_atoms (same order, same block_start) for the
+ * geometry `geo` (from mslice_geometry_compute), reading Z/x/y/z and writing block_start
+ * (n_slices*blocks_x*blocks_y + 1 ints) and the four sorted arrays (n each) — all DEVICE pointers owned by
+ * the caller — on `stream` (a cudaStream_t, NULL for the default stream); it returns once the work is
+ * queued. Its working memory is one fixed 8 MiB device array inside the library, held on every device that
+ * loads the library until the process exits; the limits are 131072 atoms and 65535 bins, and larger
+ * requests fail with MSLICE_ERR_ARG. The first call on a device looks the array up (cudaGetSymbolAddress),
+ * so make that first call before any stream capture. Every call reuses the same array: calls whose work
+ * overlaps on the GPU (two streams, two host threads) race on it, so serialise them. */
+int mslice_bin_atoms_noalloc(const mslice_geometry *geo, const int *Z, const double *x, const double *y, const double *z,
+                             size_t n, int *block_start, int *Z_sorted, double *x_sorted, double *y_sorted,
+                             double *z_sorted, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
