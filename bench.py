@@ -40,6 +40,9 @@ UNIT = "probe·slices/s"
 WORKLOAD = "stem_adf_perovskite_10x10x20_512x512_64x64probes_40slices_phonon_u0.08"
 BYTES_ROW = 24   # algorithmic bytes per pixel of one wave in the row pass: read psi, read T, write psi (FP32 complex)
 BYTES_COL = 16   # column pass: read psi, write psi
+# ncu: dram__bytes_read.sum + dram__bytes_write.sum per wave per launch of the step kernels at 512^2 FP32
+# (profiles/row_col_step_512_b128_ncu.md); updated when the kernels change and are re-captured
+NCU_DRAM_BYTES_PER_WAVE = {"row_step": 481.5e6 / 128, "col_step": 478.1e6 / 128}
 
 
 def parse():
@@ -296,14 +299,11 @@ def main():
     dom = ("row_step", row_bytes, row_ms, row_n) if row_ms >= col_ms else ("col_step", col_bytes, col_ms, col_n)
     peak, peak_src = peaks()
     achieved = dom[1] / (dom[2] / 1000.0) / 1e9
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            tj = json.load(f)
-        per_wave = tj[dom[0]]["dram_bytes_per_wave"]
-        traffic = per_wave * (npx * S * args.steps) / max(dom[3], 1)
-    except Exception:  # noqa: BLE001
-        traffic = None
+    # DRAM bytes per wave per launch from one ncu capture of this build's step kernels
+    # (profiles/row_col_step_512_b128_ncu.md: dram__bytes_read.sum + dram__bytes_write.sum / 128 waves),
+    # scaled to this run's launches
+    per_wave = NCU_DRAM_BYTES_PER_WAVE.get(dom[0])
+    traffic = per_wave * (npx * S * args.steps) / max(dom[3], 1) if per_wave else None
     roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": dom[1] / max(dom[3], 1), "avg_launch_ms": dom[2] / max(dom[3], 1),
