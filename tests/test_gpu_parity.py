@@ -308,3 +308,26 @@ def test_memory_limit(kirkland):
         Simulation(ctx, s.cfg)
     assert e.value.code == abi.ERR_OOM
     ctx.close()
+
+
+# ---------------------------------------------------------------------------------------------------
+# Directly against outputs of the reference's own kernels (tests/golden/ref_kernels.npz)
+# ---------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("dp", [True, False])
+def test_engine_matches_reference_kernel_outputs(gpu_ctx, params_all, dp):
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_kernels.npz"))
+    sub = int(g["sub"])
+    conf = Structure(g["stem_atoms_Z"].astype(np.int32), g["stem_atoms_x"], g["stem_atoms_y"], g["stem_atoms_z"])
+    s, _ = small_stem(double_precision=dp)
+    sim = _sim(gpu_ctx, params_all["kirkland"], s)
+    sim.set_atoms(conf)
+    assert np.array_equal(sim.sorted_atoms(len(conf))["block_start"], g["stem_block_start"])
+    for k in (0, 3):
+        assert rel_l2(sim.transmission(k, band_limited=False)[::sub, ::sub], g[f"stem_kirkland_T{k}"]) < TOL[dp]
+    assert rel_l2(sim.probe(4.3, 4.1)[::sub, ::sub], g["stem_probe_4.3_4.1"]) < TOL[dp]
+    assert rel_l2(sim.propagator()[::sub, ::sub], g["stem_propagator"]) < (1e-14 if dp else 1e-6)
+    s3, st3 = small_cbed(double_precision=dp)
+    sim3 = _sim(gpu_ctx, params_all["lobato"], s3)
+    sim3.set_atoms(st3)
+    assert rel_l2(sim3.transmission(1, band_limited=False)[::sub, ::sub], g["cbed_lobato3d_T1"]) < TOL[dp]
