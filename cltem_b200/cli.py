@@ -1,0 +1,245 @@
+"""Command-line front end with clTEM_cmd's interface (src/console/main.cpp:43-73, 270-792).
+
+    python -m cltem_b200 structure.xyz -c config.json -o outdir [-d device] [-p params_dir]
+
+Reads the same JSON config and .xyz structure, runs the simulation on the GPU(s), and writes the same
+outputs as clTEM_cmd's imageReturned (main.cpp:193-268): for CTEM EW_amplitude / EW_phase / Diff / Image,
+for STEM one image per detector, for CBED Diff; float32 TIFFs (fileio.h:43-76) plus a settings JSON next to
+each, and _NNN suffixes for intermediate-slice stacks (main.cpp:158-191).
+
+Differences from clTEM_cmd, by design: OpenCL devices and math flags (-d platform:device, -f) do not apply
+(-d takes CUDA device indices, "gpu"/"default" or "all"/"gpus"; -f is accepted and ignored); .cif input
+and its supercell options are not part of this engine; the frozen-phonon random draws take an explicit
+seed (--seed) instead of the wall clock.
+"""
+import argparse
+import copy
+import json
+import math
+import os
+import sys
+import threading
+import time
+
+import numpy as np
+
+from . import abi
+from .config import read_config
+from .params import read_params, read_params_json, default_bundle_path
+from .structure import phonon_configs, read_xyz
+from .tiff import write_tiff
+
+VERSION = "mslice-b200 CLI 1"
+
+
+def _parse(argv):
+    p = argparse.ArgumentParser(prog="cltem_b200", description="B200 multislice simulation (clTEM_cmd interface)")
+    p.add_argument("structure", nargs="?")
+    p.add_argument("-c", "--config")
+    p.add_argument("-o", "--output")
+    p.add_argument("-d", "--device", default="default")
+    p.add_argument("-p", "--params", default=None, help="directory holding kirkland.dat / peng.dat / lobato.dat")
+    p.add_argument("-f", "--flags", default="", help="accepted for compatibility; has no effect")
+    p.add_argument("-l", "--list", action="store_true", help="list the CUDA devices and exit")
+    p.add_argument("-v", "--version", action="store_true")
+    p.add_argument("--seed", type=int, default=0, help="seed of the frozen-phonon draws")
+    p.add_argument("--debug", action="store_true")
+    p.add_argument("-s", "--size", default=None)
+    p.add_argument("-z", "--zone", default=None)
+    p.add_argument("-n", "--normal", default=None)
+    p.add_argument("-t", "--tilts", default=None)
+    p.add_argument("--fix", action="store_true")
+    return p.parse_args(argv)
+
+
+def _devices(spec):
+    import torch
+    n = torch.cuda.device_count()
+    if n == 0:
+        raise SystemExit("no CUDA device available")
+    spec = spec.strip().lower()
+    if spec in ("default", "gpu", ""):
+        return [0]
+    if spec in ("all", "gpus"):
+        return list(range(n))
+    if spec in ("cpu", "cpus"):
+        raise SystemExit("this engine has no CPU device; use a GPU")
+    out = []
+    for tok in spec.split(","):
+        tok = tok.split(":")[-1]
+        d = int(tok)
+        if d < 0 or d >= n:
+            raise SystemExit(f"device {d} out of range (have {n})")
+        out.append(d)
+    return out
+
+
+def _load_params(name, params_dir):
+    if params_dir:
+        for fn in sorted(os.listdir(params_dir)):
+            if fn.endswith(".dat"):
+                p = read_params(os.path.join(params_dir, fn))
+                if p.name == name:
+                    return p
+        raise SystemExit(f"Could not find loaded parameters with name {name}")
+    bundle = read_params_json(default_bundle_path())
+    if name not in bundle:
+        raise SystemExit(f"Could not find loaded parameters with name {name}")
+    return bundle[name]
+
+
+def _phonon_u2(raw_json):
+    ph = raw_json.get("incoherence", {}).get("inelastic scattering", {}).get("phonon", {})
+    return float(ph.get("default", {}).get("value", 0.0)), bool(ph.get("force default", True))
+
+
+def _run_share(dev, settings, params, configs, out, idx, errors):
+    """Run a share of the configurations on one device; store (sum of results, count)."""
+    try:
+        from .engine import Context, Simulation
+        ctx = Context(dev)
+        ctx.load_params(params)
+        sim = Simulation(ctx, settings.cfg)
+        mode = settings.cfg.mode
+        if mode in (abi.MODE_STEM, abi.MODE_CBED):
+            sim.stage(configs)
+            sim.run_staged()
+            r = sim.staged_result() * len(configs)
+            out[idx] = ({"main": r}, len(configs))
+        else:
+            acc = None
+            for c in configs:
+                sim.set_atoms(c)
+                ew, diff, img = sim.ctem()
+                cur = {"EW": ew, "Diff": diff, "Image": img}
+                acc = cur if acc is None else {k: acc[k] + cur[k] for k in acc}
+            out[idx] = (acc, len(configs))
+        sim.close()
+        ctx.close()
+    except Exception as e:  # noqa: BLE001
+        errors.append(e)
+
+
+def _save_stack(path_base, stack, settings_json, n_slices, interval):
+    """saveTiffOutput (main.cpp:158-191): one file, or _NNN files for intermediate slices."""
+    if path_base.endswith(".tif"):
+        path_base = path_base[:-4]
+    if stack.shape[0] > 1:
+        if interval < 1:
+            raise RuntimeError("Saving stack with < 0 slice step.")
+        width = len(str(n_slices - 1))
+        for i in range(stack.shape[0]):
+            sid = min((i + 1) * interval - 1, n_slices - 1)
+            write_tiff(f"{path_base}_{sid:0{width}d}.tif", stack[i])
+    else:
+        write_tiff(path_base + ".tif", stack[0])
+
+
+def main(argv=None):
+    a = _parse(argv)
+    if a.version:
+        print(VERSION)
+        return 0
+    if a.list:
+        import torch
+        for i in range(torch.cuda.device_count()):
+            print(f"{i}: {torch.cuda.get_device_name(i)}")
+        return 0
+    if not a.structure or not a.config or not a.output:
+        print("usage: python -m cltem_b200 structure_file -c config.json -o output_dir [-d device]", file=sys.stderr)
+        return 1
+    if a.structure.lower().endswith(".cif") or a.size or a.zone:
+        print("CIF input and supercell construction are not supported by this engine; give an .xyz file",
+              file=sys.stderr)
+        return 1
+    with open(a.config) as f:
+        raw = json.load(f)
+    settings = read_config(raw)
+    structure = read_xyz(a.structure)
+    settings.attach_structure(structure)
+    params = _load_params(settings.potentials, a.params)
+    from .engine import geometry
+    geo = geometry(settings.cfg)
+    os.makedirs(a.output, exist_ok=True)
+
+    # frozen phonon configurations (incoherence iterations; PhononScattering::generateTdsFactor)
+    n_conf = settings.iterations if settings.phonon_enabled else 1
+    u2, force_default = _phonon_u2(raw)
+    if settings.phonon_enabled:
+        if structure.u2 is not None and not force_default:
+            configs = phonon_configs(structure, n_conf, 0.0, seed=a.seed)
+        else:
+            configs = phonon_configs(structure, n_conf, math.sqrt(max(u2, 0.0)), seed=a.seed)
+    else:
+        configs = [structure]
+
+    devs = _devices(a.device)
+    shares = [configs[i::len(devs)] for i in range(len(devs))]
+    results, errors, threads = [None] * len(devs), [], []
+    t0 = time.time()
+    for i, (d, sh) in enumerate(zip(devs, shares)):
+        if not sh:
+            continue
+        th = threading.Thread(target=_run_share, args=(d, settings, params, sh, results, i, errors))
+        th.start()
+        threads.append(th)
+    for th in threads:
+        th.join()
+    if errors:
+        raise errors[0]
+    elapsed = time.time() - t0
+    total = {}
+    for r in results:
+        if r is None:
+            continue
+        imgs, _ = r
+        for k, v in imgs.items():
+            total[k] = v if k not in total else total[k] + v
+    total = {k: v / len(configs) for k, v in total.items()}
+
+    js = copy.deepcopy(raw)
+    js["filename"] = os.path.abspath(a.structure)
+    js["slice count"] = geo.n_slices
+    js["simulation time"] = elapsed
+    interval = settings.cfg.intermediate_slices
+    sep = os.sep
+    mode = settings.cfg.mode
+    if mode == abi.MODE_STEM:
+        r = total["main"]   # [n_out, n_det, py, px]
+        for d, det in enumerate(settings.detectors):
+            name = det[0]
+            jd = copy.deepcopy(js)
+            jd.get("microscope", {}).pop("alpha", None)
+            jd.get("microscope", {}).pop("delta", None)
+            with open(a.output + sep + name + ".json", "w") as f:
+                json.dump(jd, f, indent=4)
+            _save_stack(a.output + sep + name, r[:, d], jd, geo.n_slices, interval)
+    elif mode == abi.MODE_CBED:
+        jd = copy.deepcopy(js)
+        for k in ("aberrations", "alpha", "delta", "objective aperture"):
+            jd.get("microscope", {}).pop(k, None)
+        with open(a.output + sep + "Diff.json", "w") as f:
+            json.dump(jd, f, indent=4)
+        _save_stack(a.output + sep + "Diff", total["main"], jd, geo.n_slices, interval)
+    else:
+        jd = copy.deepcopy(js)
+        for k in ("aberrations", "alpha", "delta", "objective aperture"):
+            jd.get("microscope", {}).pop(k, None)
+        ew = total["EW"]
+        for nm, arr in (("EW_amplitude", np.abs(ew)), ("EW_phase", np.angle(ew))):
+            with open(a.output + sep + nm + ".json", "w") as f:
+                json.dump(jd, f, indent=4)
+            _save_stack(a.output + sep + nm, arr, jd, geo.n_slices, interval)
+        with open(a.output + sep + "Diff.json", "w") as f:
+            json.dump(jd, f, indent=4)
+        _save_stack(a.output + sep + "Diff", total["Diff"], jd, geo.n_slices, interval)
+        if settings.cfg.ctem_image:
+            with open(a.output + sep + "Image.json", "w") as f:
+                json.dump(js, f, indent=4)
+            _save_stack(a.output + sep + "Image", total["Image"], js, geo.n_slices, interval)
+    print(f"simulation finished in {elapsed:.2f} s -> {a.output}")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -5,6 +5,7 @@
 // SimulationManager / SimulationCell do, binned atoms, the band-limited transmission function of every
 // slice, and a batch of waves that the fused row / column passes (passes.cuh) step through the slices.
 #include "../../include/mslice.h"
+#include "fft.cuh"
 #include "launch.cuh"
 #include "misc.cuh"
 #include "plain.h"
@@ -201,10 +202,16 @@ struct Ctx {
         auto &m = sizeof(R) == 4 ? tw_f : tw_d;
         auto it = m.find(n);
         if (it != m.end()) return (const cplx<R> *)it->second;
-        std::vector<cplx<R>> h(n);
-        for (int i = 0; i < n; i++) {
-            long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)i / (long double)n;
-            h[i] = mk<R>((R)std::cos(a), (R)std::sin(a));
+        // packed per-stage table (fft.cuh, plan_tw_index): W_n^(r*k*n/(Ns*R)) = exp(-2 pi i r k / (Ns*R))
+        std::vector<cplx<R>> h(n, mk<R>(0, 0));
+        for (int s = 1; s < plan_nstages(n); s++) {
+            const int Ns = plan_ns(n, s), RAD = plan_radix(n, s);
+            for (int k = 0; k < Ns; k++)
+                for (int r = 1; r < RAD; r++) {
+                    long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)(r * k) /
+                                    (long double)(Ns * RAD);
+                    h[plan_tw_index(n, s, k, r)] = mk<R>((R)std::cos(a), (R)std::sin(a));
+                }
         }
         void *d = alloc(sizeof(cplx<R>) * n);
         MS_CUDA(cudaMemcpy(d, h.data(), sizeof(cplx<R>) * n, cudaMemcpyHostToDevice));

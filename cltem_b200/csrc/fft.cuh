@@ -20,21 +20,34 @@ namespace ms {
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
 __host__ __device__ constexpr bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
+// The radix plan of a length, shared by the device stages and the host twiddle-table builder:
+// 2^k: k/3 radix-8 stages, then one radix-2 or radix-4 stage if k%3 != 0;
+// 3*2^k: k/2 radix-4 stages, a radix-2 stage if k is odd, then a radix-3 stage.
+__host__ __device__ constexpr int plan_k(int n) { return is_pow2(n) ? ilog2c(n) : ilog2c(n / 3); }
+__host__ __device__ constexpr int plan_nstages(int n) {
+    return is_pow2(n) ? (plan_k(n) / 3 + (plan_k(n) % 3 ? 1 : 0)) : (plan_k(n) / 2 + (plan_k(n) % 2) + 1);
+}
+__host__ __device__ constexpr int plan_radix(int n, int s) {
+    return is_pow2(n) ? (s < plan_k(n) / 3 ? 8 : (plan_k(n) % 3 == 1 ? 2 : 4))
+                      : (s < plan_k(n) / 2 ? 4 : ((plan_k(n) % 2 && s == plan_k(n) / 2) ? 2 : 3));
+}
+__host__ __device__ constexpr int plan_ns(int n, int s) { return s == 0 ? 1 : plan_ns(n, s - 1) * plan_radix(n, s - 1); }
+// Twiddle table layout: stage s >= 1 stores W_n^(r*k*n/(Ns*R)) for k < Ns, 1 <= r < R at
+// (Ns - Ns(1)) + k*(R-1) + (r-1): one entry per twiddle a stage uses, ordered so that the threads of a
+// warp (consecutive k) read distinct banks. The table has n - R(0) entries.
+__host__ __device__ constexpr int plan_tw_index(int n, int s, int k, int r) {
+    return (plan_ns(n, s) - plan_ns(n, 1)) + k * (plan_radix(n, s) - 1) + (r - 1);
+}
+
 template <int N>
 struct Plan {
     static constexpr bool pow2 = is_pow2(N);
     static_assert(pow2 || (N % 3 == 0 && is_pow2(N / 3)), "FFT length must be 2^k or 3*2^k");
     static constexpr int E = pow2 ? 8 : 12;
     static constexpr int NT = N / E;
-    static constexpr int K = pow2 ? ilog2c(N) : ilog2c(N / 3);
-    // pow2: K/3 radix-8 stages, then one radix-2 or radix-4 stage if K%3 != 0
-    // 3*2^k: K/2 radix-4 stages, a radix-2 stage if K odd, then a radix-3 stage
-    static constexpr int nstages = pow2 ? (K / 3 + (K % 3 ? 1 : 0)) : (K / 2 + (K % 2) + 1);
-    __host__ __device__ static constexpr int radix(int s) {
-        return pow2 ? (s < K / 3 ? 8 : (K % 3 == 1 ? 2 : 4))
-                    : (s < K / 2 ? 4 : ((K % 2 && s == K / 2) ? 2 : 3));
-    }
-    __host__ __device__ static constexpr int ns(int s) { return s == 0 ? 1 : ns(s - 1) * radix(s - 1); }
+    static constexpr int nstages = plan_nstages(N);
+    __host__ __device__ static constexpr int radix(int s) { return plan_radix(N, s); }
+    __host__ __device__ static constexpr int ns(int s) { return plan_ns(N, s); }
 };
 
 // ---- small DFTs in registers; SIGN = -1 forward, +1 inverse --------------------------------------
@@ -111,7 +124,7 @@ template <int COLS> struct ColAddr {
 
 // ---- the stage recursion ----------------------------------------------------------------------
 // v: E elements in "natural strided" order v[m] = x[t + m*NT] on entry and exit.
-// sm: this transform's shared memory (element 0), ad: addressing, tw: W_N^m twiddles (m < N).
+// sm: this transform's shared memory (element 0), ad: addressing, tw: the packed twiddle table.
 // All threads of the block must call this together (it contains __syncthreads()).
 template <class R, int N, int SIGN, int S, class Addr>
 __device__ __forceinline__ void fft_stages(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm, Addr ad, int t, const cplx<R> *tw) {
@@ -121,7 +134,7 @@ __device__ __forceinline__ void fft_stages(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm
     constexpr int Ns = P::ns(S);
     constexpr int NB = E / RAD;          // butterflies per thread
     constexpr bool last = (S == P::nstages - 1);
-    constexpr int TWS = N / (Ns * RAD);  // twiddle index stride
+    constexpr int TWB = plan_tw_index(N, S > 0 ? S : 1, 0, 1);   // this stage's block of the twiddle table
     if constexpr (S > 0) {
 #pragma unroll
         for (int b = 0; b < NB; b++) {
@@ -141,7 +154,7 @@ __device__ __forceinline__ void fft_stages(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm
             cplx<R> x = v[b + r * NB];
             if constexpr (S > 0) {
                 if (r > 0) {
-                    cplx<R> w = tw[r * k * TWS];
+                    cplx<R> w = tw[TWB + k * (RAD - 1) + (r - 1)];
                     x = (SIGN < 0) ? cmul(x, w) : cmulc(x, w);
                 }
             }

@@ -19,6 +19,8 @@ using CC = ColCfg<N, R>;
 
 template <class K> void set_smem(K kernel, size_t bytes) {
     MS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    // prefer the largest shared-memory carveout so several blocks fit per SM
+    MS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
 }
 
 // kernel attributes are per device: set once for each device this process launches on

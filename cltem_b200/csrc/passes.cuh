@@ -40,12 +40,11 @@ template <int N, class R> struct RowCfg {
     static constexpr int THREADS = Plan<N>::NT * ROWS;
     static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(N + ROWS * RowAddr::size(N)); }
 };
-__host__ __device__ constexpr int floor_pow2(int v) { return v < 2 ? 1 : 2 * floor_pow2(v / 2); }
-// Columns per tile: a power of two (it must divide N) keeping the tile at <= 64 KB.
+// Columns per tile: a power of two dividing N. 512-thread blocks (two per SM) at the common sizes; a
+// tile row of COLS complex values is 64 B (FP32, N <= 512), two 32 B sectors.
 template <int N, class R> struct ColCfg {
-    static constexpr int base = (sizeof(R) == 4) ? 8192 : 4096;
-    static constexpr int c0 = base / N;
-    static constexpr int COLS = c0 > 16 ? 16 : floor_pow2(c0 < 1 ? 1 : c0);
+    static constexpr int COLS = sizeof(R) == 4 ? (N <= 512 ? 8 : (N <= 1024 ? 4 : 2))
+                                               : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1));
     static_assert(N % COLS == 0, "column tile must divide the grid");
     static constexpr int THREADS = Plan<N>::NT * COLS;
     static_assert(THREADS <= 1024, "column block too large");
