@@ -38,8 +38,6 @@ sys.path.insert(0, ROOT)
 METRIC = "STEM probe·slices/s at 512² FP32 vs plain FP64 GPU; adjoint/forward time ratio"
 UNIT = "probe·slices/s"
 WORKLOAD = "stem_adf_perovskite_10x10x20_512x512_64x64probes_40slices_phonon_u0.08"
-BYTES_ROW = 24   # algorithmic bytes per pixel of one wave in the row pass: read psi, read T, write psi (FP32 complex)
-BYTES_COL = 16   # column pass: read psi, write psi
 # ncu: dram__bytes_read.sum + dram__bytes_write.sum per wave per launch of the step kernels at 512^2 FP32
 # (profiles/row_col_step_512_b128_ncu.md); updated when the kernels change and are re-captured
 NCU_DRAM_BYTES_PER_WAVE = {"row_step": 481.5e6 / 128, "col_step": 478.1e6 / 128}
@@ -291,11 +289,14 @@ def main():
     value = probe_slices / (ms_max / 1000.0)
 
     # roofline of the dominant kernel (by device time) from the live event timings
-    row_ms, row_n = prof["row_step"]
-    col_ms, col_n = prof["col_step"]
-    wave_px = npx * S * args.steps * N           # pixels of all waves over all slices on this rank
-    row_bytes = BYTES_ROW * wave_px
-    col_bytes = BYTES_COL * wave_px
+    # algorithmic bytes per kernel, the per-unit model of the multislice step: per probe·slice the row pass
+    # reads psi and T and writes psi (24 N bytes, complex64), the column pass reads and writes psi (16 N).
+    # The engine moves fewer: columns outside the propagator's cut are never read or written; its own count
+    # of the bytes each launch must move is reported beside ("design_bytes").
+    row_ms, row_n, row_dbytes = prof["row_step"]
+    col_ms, col_n, col_dbytes = prof["col_step"]
+    units = npx * S * args.steps              # probe·slices on this rank
+    row_bytes, col_bytes = 24.0 * N * units, 16.0 * N * units
     dom = ("row_step", row_bytes, row_ms, row_n) if row_ms >= col_ms else ("col_step", col_bytes, col_ms, col_n)
     peak, peak_src = peaks()
     achieved = dom[1] / (dom[2] / 1000.0) / 1e9
@@ -308,7 +309,11 @@ def main():
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": dom[1] / max(dom[3], 1), "avg_launch_ms": dom[2] / max(dom[3], 1),
                 "pair_achieved_gbs": (row_bytes + col_bytes) / ((row_ms + col_ms) / 1000.0) / 1e9,
-                "kernel_ms": {k: v[0] for k, v in prof.items()}, "kernel_launches": {k: v[1] for k, v in prof.items()}}
+                "pair_frac": (row_bytes + col_bytes) / ((row_ms + col_ms) / 1000.0) / 1e9 / peak,
+                "design_bytes": {"row_step": row_dbytes, "col_step": col_dbytes},
+                "design_pair_gbs": (row_dbytes + col_dbytes) / ((row_ms + col_ms) / 1000.0) / 1e9,
+                "kernel_ms": {k: v[0] for k, v in prof.items()}, "kernel_launches": {k: v[1] for k, v in prof.items()},
+                "kernel_bytes": {k: v[2] for k, v in prof.items()}}
 
     # end to end through the public API: one configuration per step from pinned host memory, result back
     e2e = None

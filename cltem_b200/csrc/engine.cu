@@ -261,8 +261,9 @@ struct SimBase {
     // per-kernel event timing (mslice_profile_enable)
     bool prof = false;
     double prof_ms[MSLICE_K_COUNT] = {};
+    double prof_bytes[MSLICE_K_COUNT] = {};
     unsigned long long prof_n[MSLICE_K_COUNT] = {};
-    struct Pending { int kind; cudaEvent_t a, b; };
+    struct Pending { int kind; cudaEvent_t a, b; double bytes; };
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> ev_pool;
     cudaEvent_t take_event() {
@@ -271,13 +272,13 @@ struct SimBase {
         MS_CUDA(cudaEventCreate(&e));
         return e;
     }
-    template <class F> void timed(cudaStream_t s, int kind, F &&launch) {
+    template <class F> void timed(cudaStream_t s, int kind, double bytes, F &&launch) {
         if (!prof) { launch(); return; }
         cudaEvent_t a = take_event(), b = take_event();
         MS_CUDA(cudaEventRecord(a, s));
         launch();
         MS_CUDA(cudaEventRecord(b, s));
-        pending.push_back({kind, a, b});
+        pending.push_back({kind, a, b, bytes});
     }
     // after a stream sync: fold the recorded launch durations into the totals
     void flush_profile() {
@@ -286,6 +287,7 @@ struct SimBase {
             MS_CUDA(cudaEventSynchronize(p.b));
             MS_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
             prof_ms[p.kind] += ms;
+            prof_bytes[p.kind] += p.bytes;
             prof_n[p.kind]++;
             ev_pool.push_back(p.a);
             ev_pool.push_back(p.b);
@@ -326,6 +328,10 @@ struct Sim : SimBase {
     DevBuf<double2> chi;
     DevBuf<uint16_t> detmask;
     double k_prop = 0;   // k_max * limit factor of the propagator cut
+    // column tiles holding columns inside the propagator cut (kx^2 < k_prop^2): the leading tiles_lo and
+    // trailing tiles_hi; xa = tiles_lo*COLS, xb = N - tiles_hi*COLS bound the active columns
+    int tiles_lo = 0, tiles_hi = 0, xa = 0, xb = 0;
+    double fa = 1.0;   // fraction of columns the step passes read and write
     // atoms
     size_t n_atoms = 0, atom_cap = 0;
     bool atoms_set = false, trans_built = false;
@@ -391,6 +397,24 @@ struct Sim : SimBase {
             MS_CUDA(cudaMemcpyAsync(px.p, hpx.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
             MS_CUDA(cudaMemcpyAsync(py.p, hpy.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
             MS_CUDA(cudaStreamSynchronize(st()));
+        }
+        {
+            const int C = ops.cols_per_tile, nt = N / C;
+            const double km2 = k_prop * k_prop;
+            std::vector<char> act(nt, 0);
+            for (int x = 0; x < N; x++)
+                if (H.kx[x] * H.kx[x] < km2) act[x / C] = 1;
+            tiles_lo = 0;
+            while (tiles_lo < nt && act[tiles_lo]) tiles_lo++;
+            tiles_hi = 0;
+            while (tiles_hi < nt - tiles_lo && act[nt - 1 - tiles_hi]) tiles_hi++;
+            // the active columns must be one run at each end (k_x increases away from both ends)
+            for (int i = tiles_lo; i < nt - tiles_hi; i++)
+                if (act[i]) { tiles_lo = nt; tiles_hi = 0; break; }
+            if (tiles_lo == 0 && tiles_hi == 0) tiles_lo = nt;   // degenerate cut: keep every tile
+            xa = tiles_lo * C;
+            xb = N - tiles_hi * C;
+            fa = (double)(xa + (N - xb)) / N;
         }
         // probe aberration table
         chi.ensure(ctx, NN);
@@ -544,7 +568,7 @@ struct Sim : SimBase {
     }
 
     void potentials(C *out, int slice0, int count) {
-        timed(st(), MSLICE_K_POTENTIAL, [&] {
+        timed(st(), MSLICE_K_POTENTIAL, (double)count * NN * sizeof(C), [&] {
             launch_potential<R>(st(), cfg.full3d != 0, out, count, axs.p, ays.p, azs.p, aZs.p, block_start.p, params_dev(),
                                 pot_params(slice0));
         });
@@ -554,7 +578,7 @@ struct Sim : SimBase {
     void band_limit(C *t, int count) {
         // FFT -> band_limit (k <= k_max * factor, inclusive) -> IFFT, clFFT scale s2d per transform
         const cplx<R> *tw = ctx->twiddles<R>(N);
-        timed(st(), MSLICE_K_BANDLIMIT, [&] {
+        timed(st(), MSLICE_K_BANDLIMIT, 3.0 * count * NN * 2 * sizeof(C), [&] {
             ops.row_fft(st(), t, t, count, tw, (R)1, -1);
             ops.col_bandlimit(st(), t, count, tw, kx2.p, ky2.p, H.g.k_max * cfg.inverse_limit_factor, (R)(s2d * s2d));
             ops.row_fft(st(), t, t, count, tw, (R)1, +1);
@@ -638,7 +662,7 @@ struct Sim : SimBase {
     int default_batch() const {
         if (cfg.probe_batch > 0) return cfg.probe_batch;
         size_t bytes = NN * sizeof(C);
-        int b = (int)std::max<size_t>(1, ((size_t)256 << 20) / bytes);   // ~256 MB of waves per pass
+        int b = (int)std::max<size_t>(1, ((size_t)1 << 30) / bytes);   // ~1 GiB of waves per pass (512 at 512^2 FP32)
         return std::min(b, 4096);
     }
 
@@ -672,7 +696,7 @@ struct Sim : SimBase {
         for (int i = 0; i < nb; i++) h_pos[i] = probe_pos(ids[i]);
         MS_CUDA(cudaMemcpyAsync(pos.p, h_pos.data(), nb * sizeof(double2), cudaMemcpyHostToDevice, st()));
         MS_CUDA(cudaMemcpyAsync(pix.p, h_pix.data(), nb * sizeof(int), cudaMemcpyHostToDevice, st()));
-        timed(st(), MSLICE_K_PROBE, [&] { ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N)); });
+        timed(st(), MSLICE_K_PROBE, (double)nb * NN * (sizeof(C) + sizeof(double2)), [&] { ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N)); });
         ctx->launches++;
         PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
         DetArgs det{detmask.p, cfg.n_detectors, partials.p};
@@ -680,13 +704,17 @@ struct Sim : SimBase {
         size_t oi = 0;
         const R a = (R)(1.0 / N), b = (R)(s2d * s2d * N), ds = (R)s2d;
         for (int s = 0; s < g.n_slices; s++) {
-            timed(st(), MSLICE_K_ROW_STEP, [&] { ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a); });
+            timed(st(), MSLICE_K_ROW_STEP, (double)nb * NN * sizeof(C) * ((s == 0 ? 1.0 : fa) + 1.0 + fa), [&] {
+                ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a, xa, xb, s == 0 ? 1 : 0);
+            });
             bool is_out = oi < outs.size() && outs[oi] == s;
             int mode = !is_out ? COL_STEP : (s == g.n_slices - 1 ? COL_DET_ONLY : COL_STEP_DET);
-            timed(st(), MSLICE_K_COL_STEP, [&] { ops.col_step(st(), wave.p, nb, tw, pt, b, ds, det, nullptr, mode); });
+            timed(st(), MSLICE_K_COL_STEP, (double)nb * NN * sizeof(C) * fa * (mode == COL_DET_ONLY ? 1.0 : 2.0), [&] {
+                ops.col_step(st(), wave.p, nb, tw, pt, b, ds, det, nullptr, mode, tiles_lo, tiles_hi);
+            });
             ctx->launches += 2;
             if (is_out) {
-                detector_reduce(st(), partials.p, ops.col_blocks, cfg.n_detectors, nb, pix.p, n_pix, (int)oi, out, comp);
+                detector_reduce(st(), partials.p, tiles_lo + tiles_hi, cfg.n_detectors, nb, pix.p, n_pix, (int)oi, out, comp);
                 ctx->launches++;
                 oi++;
             }
@@ -740,10 +768,12 @@ struct Sim : SimBase {
         const R a = (R)(1.0 / N), b = (R)(s2d * s2d * N), ds = (R)s2d;
         for (int s = 0; s < g.n_slices; s++) {
             check_cancel();
-            timed(st(), MSLICE_K_ROW_STEP, [&] { ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a); });
+            // single waves keep every column so the exit wave and the reciprocal copy are complete
+            timed(st(), MSLICE_K_ROW_STEP, 3.0 * NN * sizeof(C), [&] { ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1); });
             bool is_out = oi < outs.size() && outs[oi] == s;
-            timed(st(), MSLICE_K_COL_STEP, [&] {
-                ops.col_step(st(), wave.p, 1, tw, pt, b, ds, det, is_out ? recip.p : nullptr, is_out ? COL_STEP_DET : COL_STEP);
+            timed(st(), MSLICE_K_COL_STEP, (is_out ? 3.0 : 2.0) * NN * sizeof(C), [&] {
+                ops.col_step(st(), wave.p, 1, tw, pt, b, ds, det, is_out ? recip.p : nullptr, is_out ? COL_STEP_DET : COL_STEP,
+                             N / ops.cols_per_tile, 0);
             });
             ctx->launches += 2;
             if (is_out) { on_output((int)oi); oi++; }
@@ -1248,7 +1278,8 @@ int mslice_profile_enable(mslice_sim *sim, int on) {
     });
 }
 
-int mslice_profile_read(mslice_sim *sim, int kernel, double *total_ms, unsigned long long *launches, int reset) {
+int mslice_profile_read(mslice_sim *sim, int kernel, double *total_ms, unsigned long long *launches, double *bytes,
+                        int reset) {
     return guarded([&] {
         need(sim && total_ms && launches, "null argument");
         need(kernel >= 0 && kernel < MSLICE_K_COUNT, "unknown kernel kind");
@@ -1257,8 +1288,13 @@ int mslice_profile_read(mslice_sim *sim, int kernel, double *total_ms, unsigned 
         sim->impl->flush_profile();
         *total_ms = sim->impl->prof_ms[kernel];
         *launches = sim->impl->prof_n[kernel];
+        if (bytes) *bytes = sim->impl->prof_bytes[kernel];
         if (reset)
-            for (int k = 0; k < MSLICE_K_COUNT; k++) { sim->impl->prof_ms[k] = 0; sim->impl->prof_n[k] = 0; }
+            for (int k = 0; k < MSLICE_K_COUNT; k++) {
+                sim->impl->prof_ms[k] = 0;
+                sim->impl->prof_n[k] = 0;
+                sim->impl->prof_bytes[k] = 0;
+            }
     });
 }
 

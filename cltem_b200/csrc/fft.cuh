@@ -112,22 +112,42 @@ template <class R, int RAD, int SIGN> __device__ __forceinline__ void dft(cplx<R
 }
 
 // ---- shared-memory addressing of one transform's elements ---------------------------------------
-// Row transforms: one padding element per 8 keeps the stride-8 Stockham writes conflict free.
+// Row transforms (8-byte elements, 16 threads per shared-memory wavefront): an XOR swizzle inside each
+// aligned block of 16 elements, s(i) = i ^ g(i >> 4) with g(q) = (q & 7) | ((q & 4) << 1). It keeps the
+// three access patterns of the radix-8 stages distinct modulo 16: stride-1 reads (t + c), the first
+// stage's stride-8 writes (8t + m) and the second stage's grouped writes (64(t/8) + t%8 + 8m).
 struct RowAddr {
-    __device__ __forceinline__ int operator()(int i) const { return i + (i >> 3); }
-    static constexpr int size(int n) { return n + n / 8 + 1; }
+    __device__ __forceinline__ int operator()(int i) const {
+        const int q = i >> 4;
+        return i ^ ((q & 7) | ((q & 4) << 1));
+    }
+    static constexpr int size(int n) { return n; }
 };
-// Column tiles: element i of column c lives at i*COLS + c (threads of one row are consecutive).
-template <int COLS> struct ColAddr {
-    __device__ __forceinline__ int operator()(int i) const { return i * COLS; }
+// Column tiles: element i of column c at s(i)*COLS + c, threads of one row consecutive. The row swizzle
+// s(i) = i ^ ((i >> 3) & (RP - 1)), RP = rows per 128-byte wavefront, separates the rows a wavefront's
+// threads touch in the stride-8 stage writes.
+template <int COLS, int ELEM_BYTES> struct ColAddr {
+    static constexpr int RP = (128 / (COLS * ELEM_BYTES)) > 0 ? (128 / (COLS * ELEM_BYTES)) : 1;
+    __device__ __forceinline__ int operator()(int i) const { return (i ^ ((i >> 3) & (RP - 1))) * COLS; }
+};
+
+// ---- synchronisation of the threads sharing a transform's shared memory ---------------------------
+struct BlockSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+// A named barrier over the `count` threads (a multiple of 32) of one row transform.
+struct NamedSync {
+    int id, count;
+    __device__ __forceinline__ void operator()() const { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory"); }
 };
 
 // ---- the stage recursion ----------------------------------------------------------------------
 // v: E elements in "natural strided" order v[m] = x[t + m*NT] on entry and exit.
 // sm: this transform's shared memory (element 0), ad: addressing, tw: the packed twiddle table.
 // All threads of the block must call this together (it contains __syncthreads()).
-template <class R, int N, int SIGN, int S, class Addr>
-__device__ __forceinline__ void fft_stages(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm, Addr ad, int t, const cplx<R> *tw) {
+template <class R, int N, int SIGN, int S, class Addr, class Sync>
+__device__ __forceinline__ void fft_stages(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm, Addr ad, int t, const cplx<R> *tw,
+                                           Sync sync) {
     using P = Plan<N>;
     constexpr int E = P::E, NT = P::NT;
     constexpr int RAD = P::radix(S);
@@ -168,7 +188,7 @@ __device__ __forceinline__ void fft_stages(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm
 #pragma unroll
         for (int i = 0; i < E; i++) v[i] = out[i];
     } else {
-        __syncthreads();
+        sync();
 #pragma unroll
         for (int b = 0; b < NB; b++) {
             int j = t + b * NT;
@@ -177,14 +197,15 @@ __device__ __forceinline__ void fft_stages(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm
 #pragma unroll
             for (int m = 0; m < RAD; m++) sm[ad(idxD + m * Ns)] = out[b + m * NB];
         }
-        __syncthreads();
-        fft_stages<R, N, SIGN, S + 1, Addr>(v, sm, ad, t, tw);
+        sync();
+        fft_stages<R, N, SIGN, S + 1, Addr, Sync>(v, sm, ad, t, tw, sync);
     }
 }
 
-template <class R, int N, int SIGN, class Addr>
-__device__ __forceinline__ void fft(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm, Addr ad, int t, const cplx<R> *tw) {
-    fft_stages<R, N, SIGN, 0, Addr>(v, sm, ad, t, tw);
+template <class R, int N, int SIGN, class Addr, class Sync = BlockSync>
+__device__ __forceinline__ void fft(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm, Addr ad, int t, const cplx<R> *tw,
+                                    Sync sync = Sync()) {
+    fft_stages<R, N, SIGN, 0, Addr, Sync>(v, sm, ad, t, tw, sync);
 }
 
 }  // namespace ms

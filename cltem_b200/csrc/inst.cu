@@ -47,9 +47,10 @@ inline dim3 row_block() { return dim3(Plan<N>::NT, RC::ROWS); }
 inline dim3 col_grid(int batch) { return dim3(N / CC::COLS, batch); }
 inline dim3 col_block() { return dim3(CC::COLS, Plan<N>::NT); }
 
-void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a) {
+void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a, int xa, int xb,
+              int load_all) {
     ensure_attrs();
-    k_row_step<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a);
+    k_row_step<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all);
     MS_CUDA(cudaGetLastError());
 }
 void row_fft(cudaStream_t s, const cplx<R> *in, cplx<R> *out, int batch, const cplx<R> *tw, R scale, int sign) {
@@ -59,14 +60,17 @@ void row_fft(cudaStream_t s, const cplx<R> *in, cplx<R> *out, int batch, const c
     MS_CUDA(cudaGetLastError());
 }
 void col_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, PropTables<R> pt, R b, R ds, DetArgs det,
-              cplx<R> *recip, int mode) {
+              cplx<R> *recip, int mode, int tiles_lo, int tiles_hi) {
     ensure_attrs();
+    if (tiles_lo < 0 || tiles_hi < 0 || tiles_lo + tiles_hi > N / CC::COLS || tiles_lo + tiles_hi == 0)
+        throw std::runtime_error("column tile range out of bounds");
+    dim3 g(tiles_lo + tiles_hi, batch);
     if (mode == COL_STEP && recip == nullptr)
-        k_col_step<R, N, COL_STEP><<<col_grid(batch), col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip);
+        k_col_step<R, N, COL_STEP><<<g, col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip, tiles_lo);
     else if (mode == COL_DET_ONLY)
-        k_col_step<R, N, COL_DET_ONLY><<<col_grid(batch), col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip);
+        k_col_step<R, N, COL_DET_ONLY><<<g, col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip, tiles_lo);
     else
-        k_col_step<R, N, COL_STEP_DET><<<col_grid(batch), col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip);
+        k_col_step<R, N, COL_STEP_DET><<<g, col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip, tiles_lo);
     MS_CUDA(cudaGetLastError());
 }
 void col_fft(cudaStream_t s, const cplx<R> *in, cplx<R> *out, int batch, const cplx<R> *tw, R scale, int sign) {
@@ -94,6 +98,7 @@ PassOps<MS_REAL> make_pass_ops<MS_REAL, MS_N>() {
     PassOps<R> o;
     o.n = N;
     o.col_blocks = N / CC::COLS;
+    o.cols_per_tile = CC::COLS;
     o.row_step = row_step;
     o.row_fft = row_fft;
     o.col_step = col_step;

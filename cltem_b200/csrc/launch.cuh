@@ -9,9 +9,13 @@ template <class R>
 struct PassOps {
     int n = 0;
     int col_blocks = 0;   // blocks per wave of a column pass (number of detector partials per wave)
-    void (*row_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R) = nullptr;
+    // row_step(..., xa, xb, load_all): active columns x < xa or x >= xb (see k_row_step)
+    void (*row_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R, int, int, int) = nullptr;
     void (*row_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
-    void (*col_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, PropTables<R>, R, R, DetArgs, cplx<R> *, int) = nullptr;
+    // col_step(..., mode, tiles_lo, tiles_hi): the leading tiles_lo and trailing tiles_hi column tiles
+    void (*col_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, PropTables<R>, R, R, DetArgs, cplx<R> *, int, int,
+                     int) = nullptr;
+    int cols_per_tile = 0;
     void (*col_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
     void (*col_bandlimit)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const double *, const double *, double, R) = nullptr;
     void (*col_probe)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const double2 *, const double *, const double *,

@@ -38,6 +38,9 @@ template <int N, class R> struct RowCfg {
     static_assert(N % ROWS == 0, "row tile must divide the grid");
     static_assert(Plan<N>::NT * ROWS <= 1024, "row block too large");
     static constexpr int THREADS = Plan<N>::NT * ROWS;
+    static_assert(ROWS <= 15, "one named barrier per row");
+    // a row's threads are whole warps, so each row can synchronise on its own named barrier
+    static constexpr bool NAMED = (Plan<N>::NT % 32) == 0 && ROWS > 1;
     static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(N + ROWS * RowAddr::size(N)); }
 };
 // Columns per tile: a power of two dividing N. 512-thread blocks (two per SM) at the common sizes; a
@@ -59,10 +62,15 @@ __device__ __forceinline__ void load_twiddles(cplx<R> *tw, const cplx<R> *__rest
 // ------------------------------------------------------------------------------------------------
 // Row kernels: grid (res/ROWS, batch), block (NT, ROWS)
 // ------------------------------------------------------------------------------------------------
-// The multislice row pass: phi <- D_r(T * a * Dinv_r phi)
+// The multislice row pass: phi <- D_r(T * a * Dinv_r phi).
+// Band limit: the column pass multiplies by P, which is zero in every column with kx^2 >= k_cut^2, so
+// between passes only the columns x < xa or x >= xb (whole column tiles) carry data. The row pass reads
+// those (or every column when load_all is set: the first slice after probe initialisation) and writes
+// only those, since the column pass reads nothing else.
 template <class R, int N>
 __global__ void __launch_bounds__(RowCfg<N, R>::THREADS)
-k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const cplx<R> *__restrict__ twg, R a) {
+k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const cplx<R> *__restrict__ twg, R a,
+           int xa, int xb, int load_all) {
     using P = Plan<N>;
     constexpr int ROWS = RowCfg<N, R>::ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -75,14 +83,28 @@ k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const 
     const cplx<R> *trow = trans + (size_t)y * N;
     cplx<R> v[P::E];
 #pragma unroll
-    for (int m = 0; m < P::E; m++) v[m] = row[t + m * P::NT];
+    for (int m = 0; m < P::E; m++) {
+        const int x = t + m * P::NT;
+        v[m] = (load_all || x < xa || x >= xb) ? row[x] : mk<R>(0, 0);
+    }
     __syncthreads();
-    fft<R, N, +1>(v, sm, RowAddr(), t, tw);
+    if constexpr (RowCfg<N, R>::NAMED) {
+        const NamedSync sync{1 + (int)threadIdx.y, P::NT};
+        fft<R, N, +1>(v, sm, RowAddr(), t, tw, sync);
 #pragma unroll
-    for (int m = 0; m < P::E; m++) v[m] = cscale(cmul(v[m], trow[t + m * P::NT]), a);
-    fft<R, N, -1>(v, sm, RowAddr(), t, tw);
+        for (int m = 0; m < P::E; m++) v[m] = cscale(cmul(v[m], trow[t + m * P::NT]), a);
+        fft<R, N, -1>(v, sm, RowAddr(), t, tw, sync);
+    } else {
+        fft<R, N, +1>(v, sm, RowAddr(), t, tw);
 #pragma unroll
-    for (int m = 0; m < P::E; m++) row[t + m * P::NT] = v[m];
+        for (int m = 0; m < P::E; m++) v[m] = cscale(cmul(v[m], trow[t + m * P::NT]), a);
+        fft<R, N, -1>(v, sm, RowAddr(), t, tw);
+    }
+#pragma unroll
+    for (int m = 0; m < P::E; m++) {
+        const int x = t + m * P::NT;
+        if (x < xa || x >= xb) row[x] = v[m];
+    }
 }
 
 // A plain row transform (SIGN -1 forward, +1 inverse), scaled, in or out of place.
@@ -102,7 +124,8 @@ k_row_fft(const cplx<R> *in, cplx<R> *out, const cplx<R> *__restrict__ twg, R sc
 #pragma unroll
     for (int m = 0; m < P::E; m++) v[m] = in[off + t + m * P::NT];
     __syncthreads();
-    fft<R, N, SIGN>(v, sm, RowAddr(), t, tw);
+    if constexpr (RowCfg<N, R>::NAMED) fft<R, N, SIGN>(v, sm, RowAddr(), t, tw, NamedSync{1 + (int)threadIdx.y, P::NT});
+    else fft<R, N, SIGN>(v, sm, RowAddr(), t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) out[off + t + m * P::NT] = cscale(v[m], scale);
 }
@@ -139,10 +162,13 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 enum ColMode { COL_STEP = 0, COL_STEP_DET = 1, COL_DET_ONLY = 2 };
 
 // The multislice column pass: D_c, * P (strict cut), [detectors / Recip copy], * b, Dinv_c.
+// Block b works on column tile b for b < tiles_lo, else on tile N/COLS - (gridDim.x - b): the grid covers
+// the leading and trailing tiles that hold columns inside the propagator's cut (all tiles when
+// tiles_lo = N/COLS); the others would only be multiplied by zero.
 template <class R, int N, int MODE>
 __global__ void __launch_bounds__(ColCfg<N, R>::THREADS)
 k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTables<R> pt, R bscale, R det_scale,
-           DetArgs det, cplx<R> *__restrict__ recip_out) {
+           DetArgs det, cplx<R> *__restrict__ recip_out, int tiles_lo) {
     using P = Plan<N>;
     constexpr int COLS = ColCfg<N, R>::COLS;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -151,12 +177,13 @@ k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTabl
     cplx<R> *sm = tw + N + threadIdx.x;
     const int c = threadIdx.x, t = threadIdx.y;
     load_twiddles<R, N>(tw, twg, c + t * COLS, COLS * P::NT);
-    const int x = blockIdx.x * COLS + c;
+    const int tile = (int)blockIdx.x < tiles_lo ? (int)blockIdx.x : N / COLS - ((int)gridDim.x - (int)blockIdx.x);
+    const int x = tile * COLS + c;
     cplx<R> *base = wave + (size_t)blockIdx.y * N * N;
     cplx<R> v[P::E];
     col_load<R, N>(v, base, x, t);
     __syncthreads();
-    fft<R, N, -1>(v, sm, ColAddr<COLS>(), t, tw);
+    fft<R, N, -1>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
     const cplx<R> pxx = pt.px[x];
     const double kx2 = pt.kx2[x];
 #pragma unroll
@@ -193,7 +220,7 @@ k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTabl
     if constexpr (MODE != COL_DET_ONLY) {
 #pragma unroll
         for (int m = 0; m < P::E; m++) v[m] = cscale(v[m], bscale);
-        fft<R, N, +1>(v, sm, ColAddr<COLS>(), t, tw);
+        fft<R, N, +1>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
         col_store<R, N>(v, base, x, t);
     }
 }
@@ -214,7 +241,7 @@ k_col_fft(const cplx<R> *in, cplx<R> *out, const cplx<R> *__restrict__ twg, R sc
     cplx<R> v[P::E];
     col_load<R, N>(v, in + off, x, t);
     __syncthreads();
-    fft<R, N, SIGN>(v, sm, ColAddr<COLS>(), t, tw);
+    fft<R, N, SIGN>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) v[m] = cscale(v[m], scale);
     col_store<R, N>(v, out + off, x, t);
@@ -238,14 +265,14 @@ k_col_bandlimit(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, con
     cplx<R> v[P::E];
     col_load<R, N>(v, base, x, t);
     __syncthreads();
-    fft<R, N, -1>(v, sm, ColAddr<COLS>(), t, tw);
+    fft<R, N, -1>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
     const double k2x = kx2[x];
 #pragma unroll
     for (int m = 0; m < P::E; m++) {
         double k = sqrt(k2x + ky2[t + m * P::NT]);
         v[m] = cscale(v[m], (k <= lim) ? scale : (R)0);
     }
-    fft<R, N, +1>(v, sm, ColAddr<COLS>(), t, tw);
+    fft<R, N, +1>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
     col_store<R, N>(v, base, x, t);
 }
 
@@ -288,7 +315,7 @@ k_col_probe(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, const d
         }
     }
     __syncthreads();
-    fft<R, N, +1>(v, sm, ColAddr<COLS>(), t, tw);
+    fft<R, N, +1>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) v[m] = cscale(v[m], scale);
     col_store<R, N>(v, wave + (size_t)blockIdx.y * N * N, x, t);

@@ -77,7 +77,7 @@ def load_library(path=None):
         "mslice_ctx_launch_count": [C.c_void_p, C.POINTER(C.c_ulonglong)],
         "mslice_last_timing": [C.c_void_p, _dp],
         "mslice_profile_enable": [C.c_void_p, C.c_int],
-        "mslice_profile_read": [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_ulonglong), C.c_int],
+        "mslice_profile_read": [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_ulonglong), _dp, C.c_int],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -320,17 +320,15 @@ class Simulation:
         _check(self.lib.mslice_profile_enable(self.h, int(on)))
 
     def profile_read(self, reset=False):
-        """{kernel: (total device ms, launches)} accumulated while profiling was on."""
+        """{kernel: (total device ms, launches, algorithmic bytes)} accumulated while profiling was on."""
         out = {}
         for k, name in enumerate(self.KERNELS):
-            ms = C.c_double()
-            n = C.c_ulonglong()
-            _check(self.lib.mslice_profile_read(self.h, k, C.byref(ms), C.byref(n), 0))
-            out[name] = (ms.value, n.value)
+            ms, n, by = C.c_double(), C.c_ulonglong(), C.c_double()
+            _check(self.lib.mslice_profile_read(self.h, k, C.byref(ms), C.byref(n), C.byref(by), 0))
+            out[name] = (ms.value, n.value, by.value)
         if reset:
-            ms = C.c_double()
-            n = C.c_ulonglong()
-            _check(self.lib.mslice_profile_read(self.h, 0, C.byref(ms), C.byref(n), 1))
+            ms, n, by = C.c_double(), C.c_ulonglong(), C.c_double()
+            _check(self.lib.mslice_profile_read(self.h, 0, C.byref(ms), C.byref(n), C.byref(by), 1))
         return out
 
     def last_timing(self):

@@ -253,8 +253,11 @@ int mslice_last_timing(mslice_sim *sim, double *ms3);
 #define MSLICE_K_PROBE 4      /* probe generation + column inverse FFT        */
 #define MSLICE_K_COUNT 5
 int mslice_profile_enable(mslice_sim *sim, int on);
-/* Accumulated device ms and launch count of one kernel kind since the last reset; reset != 0 clears. */
-int mslice_profile_read(mslice_sim *sim, int kernel, double *total_ms, unsigned long long *launches, int reset);
+/* Accumulated device ms, launch count and algorithmic bytes (the bytes the launches must read and write
+ * in HBM by design: waves, transmission slices, tables; columns outside the propagator cut are neither
+ * read nor written) of one kernel kind since the last reset; reset != 0 clears every kind. */
+int mslice_profile_read(mslice_sim *sim, int kernel, double *total_ms, unsigned long long *launches, double *bytes,
+                        int reset);
 
 /* Atom binning without any device allocation (no counterpart in the reference).
  * For callers that cannot call cudaMalloc: a host application that manages all device memory through its
