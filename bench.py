@@ -209,6 +209,46 @@ def run_reference(args):
 # ---------------------------------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------------------------------
+def adjoint_leg(ctx, ext, warmup):
+    """Differentiable CTEM (perovskite 8x8x16, 512^2, 32 slices, FP32): device time of the image loss
+    (forward) and of loss + gradients by the adjoint with sqrt(N) checkpointing."""
+    import torch
+    from cltem_b200 import config
+    from cltem_b200.engine import Simulation
+    from cltem_b200.structure import phonon_configs
+    s, st = config.perovskite_dctem()
+    ts, _ = config.perovskite_dctem()
+    ts.cfg.C10 = s.cfg.C10 + 30.0
+    tsim = Simulation(ctx, ts.cfg)
+    tsim.set_atoms(phonon_configs(st, 1, 0.05, seed=77)[0])
+    target = tsim.ctem()[2][0]
+    tsim.close()
+    sim = Simulation(ctx, s.cfg)
+    sim.set_atoms(st)
+
+    def timed(fn, reps=3):
+        for _ in range(max(1, warmup)):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        for _ in range(reps):
+            fn()
+        b.record(ext)
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    t_fwd = timed(lambda: sim.ctem_loss(target))
+    t_adj = timed(lambda: sim.ctem_loss_grad(target, len(st), checkpoint_every=0))
+    t_adj1 = timed(lambda: sim.ctem_loss_grad(target, len(st), checkpoint_every=1))
+    sim.close()
+    return {"workload": "ctem_perovskite_8x8x16_512x512_32slices_fp32", "forward_ms": t_fwd,
+            "loss_and_grad_ms": t_adj, "ratio": t_adj / t_fwd, "checkpoint": "every ceil(sqrt(32)) = 6 slices",
+            "loss_and_grad_ms_store_all": t_adj1, "ratio_store_all": t_adj1 / t_fwd,
+            "note": "ratio = (forward + adjoint with checkpoint recomputation) / forward, both including the "
+                    "transmission build of the 32 slices"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -279,11 +319,9 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
     img = sim.staged_result()
-    # one exchange step: sum the per-rank averaged images (SimulationManager::updateImages merge)
-    timg = torch.from_numpy(np.ascontiguousarray(img)).cuda()
-    if world > 1:
-        dist.all_reduce(timg)
-        timg /= world
+    # one exchange step: merge the per-rank image sums and weights (SimulationManager::updateImages)
+    from cltem_b200.distributed import merge_average
+    img = merge_average(img * args.steps, args.steps, device=torch.device("cuda", local))
 
     probe_slices = npx * S * args.steps * world
     value = probe_slices / (ms_max / 1000.0)
@@ -348,6 +386,10 @@ def main():
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(out.numel() * 8),
                "steps": len(e2e_confs), "ms_per_step": ms_e2e / len(e2e_confs)}
 
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_baseline:
+        adjoint = adjoint_leg(ctx, ext, args.warmup)
+
     cpu = plain = None
     if rank == 0 and world == 1 and not args.no_baseline:
         # plain per-probe FP64 GPU path (the reference's unfused order with cuFFT Z2Z) on a sample
@@ -383,7 +425,8 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "plain_fp64_gpu": plain,
-            "adjoint_forward_ratio": None,
+            "adjoint_forward_ratio": adjoint["ratio"] if adjoint else None,
+            "adjoint": adjoint,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,

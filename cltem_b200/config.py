@@ -249,3 +249,31 @@ def fcc_cbed(n=(20, 20, 60), resolution=1024, double_precision=False, integrals=
     c.cbed_padding = 65.6
     s.attach_structure(st)
     return s, st
+
+
+def perovskite_dctem(n=(8, 8, 16), resolution=512, double_precision=False):
+    """Differentiable CTEM: perovskite 8x8x16 cells (5,120 atoms) over the periodic 31.24 Å field, 300 kV,
+    32 slices of 1.9525 Å, C1 = -10 nm, Cs = -15 um, objective aperture 25 mrad, no partial coherence."""
+    from .structure import perovskite
+    st = perovskite(*n)
+    s = SimulationSettings()
+    c = s.cfg
+    c.mode = abi.MODE_CTEM
+    c.double_precision = int(double_precision)
+    c.resolution = resolution
+    c.padding_xy = 0.0
+    c.padding_z = 0.0
+    c.slice_thickness = 1.9525
+    c.slice_offset = 0.97625
+    c.voltage = 300.0
+    s.maintain_area = True
+    L = n[0] * 3.905
+    c.ctem_area[:] = [0.0, L, 0.0, L]
+    c.ctem_image = 1
+    c.C10 = -100.0
+    c.C30 = -1.5e5
+    c.obj_ap = 25.0
+    c.alpha = 0.0
+    c.delta = 0.0
+    s.attach_structure(st)
+    return s, st

@@ -1,0 +1,25 @@
+// adjoint_ops.h — host entry points of the differentiable-CTEM kernels (adjoint.cu).
+#pragma once
+
+#include "misc.cuh"
+
+namespace ms {
+
+// I = |W|^2, partial[b] = block sums of (I - target)^2, gW = 4 (I - target) W; reduction_blocks() partials
+template <class R> void image_loss(cudaStream_t s, size_t n, const cplx<R> *W, const double *target, cplx<R> *gW,
+                                   double *partial);
+// gRecip = conj(H) gY and the partial sums of dL/dC10, dL/dC30 (H: ctem_image_d.cl transfer)
+template <class R> void image_backward(cudaStream_t s, int n, const cplx<R> *recip, const cplx<R> *gY, cplx<R> *gRecip,
+                                       const double *kx, const double *ky, double wavelength, const AberrD &A, double obj_ap,
+                                       double ap_smooth, double beta, double delta, double *p10, double *p30);
+// g <- conj(P) g scale inside the propagator cut
+template <class R> void mul_conj_prop(cudaStream_t s, int n, cplx<R> *g, const cplx<R> *px, const cplx<R> *py,
+                                      const double *kx2, const double *ky2, double kmax2, R scale);
+// gV = sigma Im(conj(E) gE)
+template <class R> void grad_v(cudaStream_t s, size_t count, const cplx<R> *E, const cplx<R> *gE, double sigma, double *gV);
+// per-atom gradients (x, y) of the atoms [a0, a0+count) in sorted order from gV of their slice
+void atom_grad(cudaStream_t s, int a0, int count, const double *ax, const double *ay, const int *aZ, const double *gV,
+               int n, double startx, double starty, double dx, int form, const double *prm, int i_lim, double *gxy);
+int reduction_blocks();
+
+}  // namespace ms

@@ -5,6 +5,7 @@
 // SimulationManager / SimulationCell do, binned atoms, the band-limited transmission function of every
 // slice, and a batch of waves that the fused row / column passes (passes.cuh) step through the slices.
 #include "../../include/mslice.h"
+#include "adjoint_ops.h"
 #include "fft.cuh"
 #include "launch.cuh"
 #include "misc.cuh"
@@ -312,6 +313,9 @@ struct SimBase {
     virtual void run_staged(int mode) = 0;
     virtual void staged_result(double *out, size_t cap) = 0;
     virtual void stem_plain(const int *pixels, size_t n, double *out) = 0;
+    virtual void ctem_loss_grad(const double *target, double *loss, double *gxyz, double *g10, double *g30, int ck,
+                                bool want_grad) = 0;
+    virtual void set_c10_c30(double c10, double c30) = 0;
 };
 
 template <class R>
@@ -324,7 +328,7 @@ struct Sim : SimBase {
 
     // tables
     DevBuf<double> kx, ky, kx2, ky2;
-    DevBuf<C> px, py;
+    DevBuf<C> px, py, pxc, pyc;   // propagator factors and their conjugates (adjoint)
     DevBuf<double2> chi;
     DevBuf<uint16_t> detmask;
     double k_prop = 0;   // k_max * limit factor of the propagator cut
@@ -393,9 +397,12 @@ struct Sim : SimBase {
                 hpx[i] = mk<R>((R)(f * std::cos(ax_)), (R)(f * std::sin(ax_)));
                 hpy[i] = mk<R>((R)std::cos(ay_), (R)std::sin(ay_));
             }
-            px.ensure(ctx, N); py.ensure(ctx, N);
+            px.ensure(ctx, N); py.ensure(ctx, N); pxc.ensure(ctx, N); pyc.ensure(ctx, N);
             MS_CUDA(cudaMemcpyAsync(px.p, hpx.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
             MS_CUDA(cudaMemcpyAsync(py.p, hpy.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
+            for (int i = 0; i < N; i++) { hpx[i].y = -hpx[i].y; hpy[i].y = -hpy[i].y; }
+            MS_CUDA(cudaMemcpyAsync(pxc.p, hpx.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
+            MS_CUDA(cudaMemcpyAsync(pyc.p, hpy.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
             MS_CUDA(cudaStreamSynchronize(st()));
         }
         {
@@ -904,6 +911,138 @@ struct Sim : SimBase {
         for (size_t i = 0; i < acc_n; i++) out[i] /= (double)acc_configs;
     }
 
+    void set_c10_c30(double c10, double c30) override {
+        cfg.C10 = c10;
+        cfg.C30 = c30;
+        chi_table(st(), N, kx.p, ky.p, H.g.wavelength, aberr(cfg.C10), cfg.cond_ap, cfg.cond_ap_smooth, chi.p);
+        ctx->launches++;
+    }
+
+    // ---- differentiable CTEM -------------------------------------------------------------
+    void ctem_loss_grad(const double *target, double *loss, double *gxyz, double *g10, double *g30, int ck,
+                        bool want_grad) override {
+        const mslice_geometry &g = H.g;
+        if (cfg.mode != MSLICE_MODE_CTEM) throw StateError("the image loss needs a CTEM simulation");
+        if (cfg.full3d) throw Unsupported("gradients are implemented for the projected potential");
+        if (cfg.beam_tilt != 0.0) throw Unsupported("gradients are implemented without beam tilt");
+        if (!atoms_set) throw StateError("atoms not set");
+        const int S = g.n_slices;
+        const int c = ck <= 0 ? (int)std::ceil(std::sqrt((double)S)) : std::min(ck, S);
+        const int n_ck = (S + c - 1) / c;
+        const cplx<R> *tw = ctx->twiddles<R>(N);
+        const R a = (R)(1.0 / N), b = (R)(s2d * s2d * N), ds = (R)s2d;
+        const int all_tiles = N / ops.cols_per_tile;
+        DevBuf<C> E, ck_buf, save, fw, gT, w1, w2;
+        DevBuf<double> tgt, part, gV, gxy;
+        E.ensure(ctx, (size_t)S * NN);
+        ensure_waves(1);
+        w1.ensure(ctx, NN); w2.ensure(ctx, NN);
+        tgt.ensure(ctx, NN);
+        const int nred = reduction_blocks();
+        part.ensure(ctx, 3 * (size_t)nred);
+        MS_CUDA(cudaMemcpyAsync(tgt.p, target, NN * sizeof(double), cudaMemcpyHostToDevice, st()));
+        // raw E_s = exp(i sigma V_s) for every slice, then T_s = bandlimit(E_s)
+        potentials(E.p, 0, S);
+        MS_CUDA(cudaMemcpyAsync(trans.p, E.p, (size_t)S * NN * sizeof(C), cudaMemcpyDeviceToDevice, st()));
+        band_limit(trans.p, S);
+        trans_built = true;
+        if (want_grad) {
+            ck_buf.ensure(ctx, (size_t)n_ck * NN);
+            save.ensure(ctx, (size_t)(c == 1 ? S : c) * NN);
+        }
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
+        DetArgs nodet{detmask.p, 0, partials.p};
+        // forward: plane wave through every slice, checkpoints of the row-transformed state
+        plane_wave_state<R>(st(), N, wave.p);
+        for (int s = 0; s < S; s++) {
+            if (want_grad && s % c == 0)
+                MS_CUDA(cudaMemcpyAsync(ck_buf.p + (size_t)(s / c) * NN, wave.p, NN * sizeof(C), cudaMemcpyDeviceToDevice, st()));
+            if (want_grad && c == 1) ops.row_step_save(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, save.p + (size_t)s * NN);
+            else ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1);
+            bool last = s == S - 1;
+            ops.col_step(st(), wave.p, 1, tw, pt, b, ds, nodet, last ? recip.p : nullptr, last ? COL_STEP_DET : COL_STEP,
+                         all_tiles, 0);
+            ctx->launches += 2;
+        }
+        // image W = s2d Dinv(H Recip), loss, G_W = 4 (I - target) W
+        ctem_transfer<R>(st(), N, recip.p, w1.p, kx.p, ky.p, g.wavelength, aberr(cfg.C10), cfg.obj_ap, cfg.obj_ap_smooth,
+                         cfg.alpha, cfg.delta);
+        ops.row_fft(st(), w1.p, w1.p, 1, tw, (R)1, +1);
+        ops.col_fft(st(), w1.p, w1.p, 1, tw, (R)s2d, +1);
+        image_loss<R>(st(), NN, w1.p, tgt.p, w2.p, part.p);
+        ctx->launches += 4;
+        std::vector<double> hp(3 * (size_t)nred);
+        if (!want_grad) {
+            MS_CUDA(cudaMemcpyAsync(hp.data(), part.p, nred * sizeof(double), cudaMemcpyDeviceToHost, st()));
+            MS_CUDA(cudaStreamSynchronize(st()));
+            double L = 0;
+            for (int i = 0; i < nred; i++) L += hp[i];
+            if (loss) *loss = L;
+            return;
+        }
+        // G_Y = s2d D(G_W); G_Recip = conj(H) G_Y and dL/dC10, dL/dC30
+        ops.row_fft(st(), w2.p, w2.p, 1, tw, (R)1, -1);
+        ops.col_fft(st(), w2.p, w2.p, 1, tw, (R)s2d, -1);
+        image_backward<R>(st(), N, recip.p, w2.p, w1.p, kx.p, ky.p, g.wavelength, aberr(cfg.C10), cfg.obj_ap,
+                          cfg.obj_ap_smooth, cfg.alpha, cfg.delta, part.p + nred, part.p + 2 * (size_t)nred);
+        // backward state D_r G_{u_{S-1}} = s2d N Dinv_c(conj(P) G_Recip)
+        mul_conj_prop<R>(st(), N, w1.p, px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, (R)1);
+        ops.col_fft(st(), w1.p, wave.p, 1, tw, (R)(s2d * N), +1);
+        ctx->launches += 5;
+        // sorted atoms of each slice
+        const size_t nb = (size_t)g.blocks_x * g.blocks_y;
+        std::vector<int> hbs((size_t)S * nb + 1);
+        MS_CUDA(cudaMemcpyAsync(hbs.data(), block_start.p, hbs.size() * sizeof(int), cudaMemcpyDeviceToHost, st()));
+        MS_CUDA(cudaStreamSynchronize(st()));
+        const int n_in = hbs.back();
+        gxy.ensure(ctx, 2 * (size_t)std::max(n_in, 1));
+        MS_CUDA(cudaMemsetAsync(gxy.p, 0, 2 * (size_t)std::max(n_in, 1) * sizeof(double), st()));
+        fw.ensure(ctx, NN); gT.ensure(ctx, NN); gV.ensure(ctx, NN);
+        PropTables<R> ptc{pxc.p, pyc.p, kx2.p, ky2.p, k_prop * k_prop};
+        for (int k = n_ck - 1; k >= 0; k--) {
+            const int s0 = k * c, s1 = std::min(s0 + c, S);
+            if (c > 1) {   // recompute psi_s of the segment from its checkpoint
+                MS_CUDA(cudaMemcpyAsync(fw.p, ck_buf.p + (size_t)k * NN, NN * sizeof(C), cudaMemcpyDeviceToDevice, st()));
+                for (int s = s0; s < s1; s++) {
+                    ops.row_step_save(st(), fw.p, 1, trans.p + (size_t)s * NN, tw, a, save.p + (size_t)(s - s0) * NN);
+                    if (s < s1 - 1) ops.col_step(st(), fw.p, 1, tw, pt, b, ds, nodet, nullptr, COL_STEP, all_tiles, 0);
+                    ctx->launches += 2;
+                }
+            }
+            for (int s = s1 - 1; s >= s0; s--) {
+                check_cancel();
+                if (s < S - 1) ops.col_step(st(), wave.p, 1, tw, ptc, b, ds, nodet, nullptr, COL_STEP, all_tiles, 0);
+                const C *psi = save.p + (size_t)(c == 1 ? s : s - s0) * NN;
+                ops.row_adjoint(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, psi, gT.p);
+                band_limit(gT.p, 1);   // G_E = bandlimit(G_T): the band limit is self-adjoint
+                grad_v<R>(st(), NN, E.p + (size_t)s * NN, gT.p, g.sigma, gV.p);
+                const int a0 = hbs[(size_t)s * nb], a1 = hbs[(size_t)(s + 1) * nb];
+                atom_grad(st(), a0, a1 - a0, axs.p, ays.p, aZs.p, gV.p, N, g.sim_x[0], g.sim_y[0], g.real_scale,
+                          ctx->params.form, ctx->prm_d, ctx->params.i_count, gxy.p);
+                ctx->launches += 5;
+            }
+        }
+        MS_CUDA(cudaMemcpyAsync(hp.data(), part.p, 3 * (size_t)nred * sizeof(double), cudaMemcpyDeviceToHost, st()));
+        std::vector<double> hg(2 * (size_t)std::max(n_in, 1));
+        std::vector<int> hidx(std::max<size_t>(n_atoms, 1));
+        MS_CUDA(cudaMemcpyAsync(hg.data(), gxy.p, hg.size() * sizeof(double), cudaMemcpyDeviceToHost, st()));
+        if (n_atoms) MS_CUDA(cudaMemcpyAsync(hidx.data(), idx_out.p, n_atoms * sizeof(int), cudaMemcpyDeviceToHost, st()));
+        MS_CUDA(cudaStreamSynchronize(st()));
+        double L = 0, d10 = 0, d30 = 0;
+        for (int i = 0; i < nred; i++) { L += hp[i]; d10 += hp[nred + i]; d30 += hp[2 * nred + i]; }
+        if (loss) *loss = L;
+        if (g10) *g10 = d10;
+        if (g30) *g30 = d30;
+        if (gxyz) {
+            std::fill(gxyz, gxyz + 3 * n_atoms, 0.0);
+            for (int i = 0; i < n_in; i++) {   // sorted position i holds input atom idx_out[i]
+                const int o = hidx[i];
+                gxyz[3 * (size_t)o] = hg[2 * (size_t)i];
+                gxyz[3 * (size_t)o + 1] = hg[2 * (size_t)i + 1];
+            }
+        }
+    }
+
     void stem_plain(const int *pixels, size_t n, double *out) override {
         if constexpr (sizeof(R) != 8) {
             (void)pixels; (void)n; (void)out;
@@ -952,7 +1091,11 @@ template PassOps<double> pass_ops<double>(int);
 // =================================================================================================
 // C ABI
 // =================================================================================================
-struct mslice_ctx { ms::Ctx impl; };
+struct mslice_sim;
+struct mslice_ctx {
+    ms::Ctx impl;
+    std::vector<mslice_sim *> sims;   // simulations created on this context; destroyed with it
+};
 struct mslice_sim {
     mslice_ctx *ctx;
     std::unique_ptr<ms::SimBase> impl;
@@ -960,6 +1103,8 @@ struct mslice_sim {
 
 namespace {
 template <class F> int guarded(F &&f) {
+    // clear a non-sticky error a previous call may have left in this thread's runtime state
+    cudaGetLastError();
     try {
         f();
         return MSLICE_OK;
@@ -1006,7 +1151,11 @@ int mslice_ctx_destroy(mslice_ctx *ctx) {
     return guarded([&] {
         if (!ctx) return;
         cudaSetDevice(ctx->impl.device);
+        cudaStreamSynchronize(ctx->impl.stream);
+        for (mslice_sim *s : ctx->sims) delete s;   // simulations still alive go with their context
+        ctx->sims.clear();
         delete ctx;
+        cudaGetLastError();
     });
 }
 
@@ -1064,6 +1213,7 @@ int mslice_sim_create(mslice_ctx *ctx, const mslice_config *cfg, mslice_sim **ou
         s->ctx = ctx;
         if (cfg->double_precision) s->impl = std::make_unique<ms::Sim<double>>(&ctx->impl, *cfg);
         else s->impl = std::make_unique<ms::Sim<float>>(&ctx->impl, *cfg);
+        ctx->sims.push_back(s.get());
         *out = s.release();
     });
 }
@@ -1073,6 +1223,8 @@ int mslice_sim_destroy(mslice_sim *sim) {
         if (!sim) return;
         use_device(sim->ctx);
         cudaStreamSynchronize(sim->ctx->impl.stream);
+        auto &v = sim->ctx->sims;
+        v.erase(std::remove(v.begin(), v.end(), sim), v.end());
         delete sim;
     });
 }
@@ -1169,6 +1321,31 @@ int mslice_ctem_run(mslice_sim *sim, double *ew, double *diff, double *image) {
         need(sim != nullptr, "sim is null");
         use_device(sim->ctx);
         sim->impl->ctem_run(ew, diff, image);
+    });
+}
+
+int mslice_ctem_loss_grad(mslice_sim *sim, const double *target, double *loss, double *grad_xyz, double *grad_c10,
+                          double *grad_c30, int checkpoint_every) {
+    return guarded([&] {
+        need(sim && target, "null argument");
+        use_device(sim->ctx);
+        sim->impl->ctem_loss_grad(target, loss, grad_xyz, grad_c10, grad_c30, checkpoint_every, true);
+    });
+}
+
+int mslice_set_c10_c30(mslice_sim *sim, double c10, double c30) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        use_device(sim->ctx);
+        sim->impl->set_c10_c30(c10, c30);
+    });
+}
+
+int mslice_ctem_loss(mslice_sim *sim, const double *target, double *loss) {
+    return guarded([&] {
+        need(sim && target, "null argument");
+        use_device(sim->ctx);
+        sim->impl->ctem_loss_grad(target, loss, nullptr, nullptr, nullptr, 0, false);
     });
 }
 

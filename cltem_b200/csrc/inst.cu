@@ -39,6 +39,8 @@ void ensure_attrs() {
     set_smem(k_col_fft<R, N, +1>, CC::smem());
     set_smem(k_col_bandlimit<R, N>, CC::smem());
     set_smem(k_col_probe<R, N>, CC::smem());
+    set_smem(k_row_step_save<R, N>, RC::smem());
+    set_smem(k_row_adjoint<R, N>, RC::smem());
     g_attrs_done[dev] = true;
 }
 
@@ -91,6 +93,18 @@ void col_probe(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, cons
     k_col_probe<R, N><<<col_grid(batch), col_block(), CC::smem(), s>>>(wave, tw, chi, kx, ky, pos, scale);
     MS_CUDA(cudaGetLastError());
 }
+void row_step_save(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a,
+                   cplx<R> *save) {
+    ensure_attrs();
+    k_row_step_save<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, save);
+    MS_CUDA(cudaGetLastError());
+}
+void row_adjoint(cudaStream_t s, cplx<R> *state, int batch, const cplx<R> *trans, const cplx<R> *tw, R a,
+                 const cplx<R> *psi, cplx<R> *gT) {
+    ensure_attrs();
+    k_row_adjoint<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(state, trans, tw, a, psi, gT);
+    MS_CUDA(cudaGetLastError());
+}
 }  // namespace
 
 template <>
@@ -105,6 +119,8 @@ PassOps<MS_REAL> make_pass_ops<MS_REAL, MS_N>() {
     o.col_fft = col_fft;
     o.col_bandlimit = col_bandlimit;
     o.col_probe = col_probe;
+    o.row_step_save = row_step_save;
+    o.row_adjoint = row_adjoint;
     return o;
 }
 

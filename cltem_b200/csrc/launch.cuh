@@ -1,6 +1,7 @@
 // launch.cuh — host launchers of the pass kernels, one explicit instantiation per (precision, size).
 #pragma once
 
+#include "adjoint.cuh"
 #include "passes.cuh"
 
 namespace ms {
@@ -20,6 +21,10 @@ struct PassOps {
     void (*col_bandlimit)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const double *, const double *, double, R) = nullptr;
     void (*col_probe)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const double2 *, const double *, const double *,
                       const double2 *, R) = nullptr;
+    // differentiable CTEM (adjoint.cuh)
+    void (*row_step_save)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R, cplx<R> *) = nullptr;
+    void (*row_adjoint)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R, const cplx<R> *,
+                        cplx<R> *) = nullptr;
 };
 
 // defined in inst.cu for every supported (R, N)

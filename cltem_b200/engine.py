@@ -77,6 +77,8 @@ def load_library(path=None):
         "mslice_ctx_launch_count": [C.c_void_p, C.POINTER(C.c_ulonglong)],
         "mslice_last_timing": [C.c_void_p, _dp],
         "mslice_profile_enable": [C.c_void_p, C.c_int],
+        "mslice_ctem_loss_grad": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, C.c_int],
+        "mslice_ctem_loss": [C.c_void_p, _dp, _dp],
         "mslice_profile_read": [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_ulonglong), _dp, C.c_int],
     }
     for name, args in sig.items():
@@ -127,13 +129,18 @@ class Context:
 
     def __init__(self, device: int = 0):
         self.lib = load_library()
+        import weakref
         h = C.c_void_p()
         _check(self.lib.mslice_ctx_create(device, C.byref(h)))
         self.h = h
         self.params = None
+        self._sims = weakref.WeakSet()
 
     def close(self):
+        """Destroy the context; simulations still open on it are destroyed with it."""
         if getattr(self, "h", None):
+            for sim in list(getattr(self, "_sims", ())):
+                sim.h = None   # the library frees them with the context
             self.lib.mslice_ctx_destroy(self.h)
             self.h = None
 
@@ -182,6 +189,7 @@ class Simulation:
         h = C.c_void_p()
         _check(self.lib.mslice_sim_create(ctx.h, C.byref(cfg), C.byref(h)))
         self.h = h
+        ctx._sims.add(self)
         g = abi.Geometry()
         _check(self.lib.mslice_sim_geometry(self.h, C.byref(g)))
         self.geo = g
@@ -191,7 +199,8 @@ class Simulation:
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.mslice_sim_destroy(self.h)
+            if getattr(self.ctx, "h", None):   # a closed context has already freed its simulations
+                self.lib.mslice_sim_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -272,6 +281,23 @@ class Simulation:
         _check(self.lib.mslice_ctem_run(self.h, _d(ew), _d(diff), _d(img)))
         return (_cplx(ew).reshape(no, self.res, self.res), diff.reshape(no, self.res, self.res),
                 img.reshape(no, self.res, self.res))
+
+    # ---- differentiable CTEM ----------------------------------------------------------------------
+    def ctem_loss(self, target):
+        """L = sum (I - target)^2 of the CTEM image of the current atoms (forward only)."""
+        t = np.ascontiguousarray(target, dtype=np.float64).reshape(-1)
+        L = C.c_double()
+        _check(self.lib.mslice_ctem_loss(self.h, _d(t), C.byref(L)))
+        return L.value
+
+    def ctem_loss_grad(self, target, n_atoms, checkpoint_every=0):
+        """(L, dL/dxyz [n_atoms, 3] in the order given to set_atoms, dL/dC10, dL/dC30) by the adjoint."""
+        t = np.ascontiguousarray(target, dtype=np.float64).reshape(-1)
+        L, g10, g30 = C.c_double(), C.c_double(), C.c_double()
+        gx = np.zeros(3 * max(n_atoms, 1))
+        _check(self.lib.mslice_ctem_loss_grad(self.h, _d(t), C.byref(L), _d(gx), C.byref(g10), C.byref(g30),
+                                              int(checkpoint_every)))
+        return L.value, gx[: 3 * n_atoms].reshape(n_atoms, 3), g10.value, g30.value
 
     # ---- frozen-phonon runs ---------------------------------------------------------------------
     def stage(self, configs):

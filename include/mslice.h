@@ -208,6 +208,23 @@ int mslice_cbed_run(mslice_sim *sim, double *diff);
  * Any output pointer may be NULL. */
 int mslice_ctem_run(mslice_sim *sim, double *ew, double *diff, double *image);
 
+/* ---- differentiable CTEM ---------------------------------------------- */
+/* Loss L = sum over pixels of (I - target)^2 for the CTEM objective-lens image I of the current atom
+ * configuration (simulateImagePerfect, microscope/simulationctem.cpp:114-166), and its gradients by the
+ * hand-written adjoint of the multislice: dL/d(x, y, z) of every atom passed to mslice_set_atoms (input
+ * order, 3 per atom; z is 0 in the projected model, where z only selects the slice), dL/dC10 and dL/dC30
+ * (per Å). target holds res*res doubles (x fastest). Slice waves are checkpointed every
+ * `checkpoint_every` slices (0: ceil(sqrt(n_slices)); 1: every slice, no recomputation) and recomputed
+ * segment by segment in the backward pass. Projected potentials without beam tilt only
+ * (MSLICE_ERR_UNSUPPORTED otherwise). Any output pointer may be NULL. */
+int mslice_ctem_loss_grad(mslice_sim *sim, const double *target, double *loss, double *grad_xyz, double *grad_c10,
+                          double *grad_c30, int checkpoint_every);
+/* The same loss without gradients (forward only); used to time the forward model. */
+int mslice_ctem_loss(mslice_sim *sim, const double *target, double *loss);
+/* Change the defocus C10 and spherical aberration C30 (Å) of an existing simulation (the objective lens
+ * of the CTEM image and the probe of STEM/CBED both follow). */
+int mslice_set_c10_c30(mslice_sim *sim, double c10, double c30);
+
 /* ---- frozen-phonon jobs over many configurations, one persistent call ---------------------- */
 /* Stage n_configs atom configurations on the device (concatenated host arrays, counts[c] atoms each).
  * A staged set stays resident until the next stage call or mslice_sim_destroy. */
