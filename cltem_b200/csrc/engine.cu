@@ -264,7 +264,7 @@ struct SimBase {
     double prof_ms[MSLICE_K_COUNT] = {};
     double prof_bytes[MSLICE_K_COUNT] = {};
     unsigned long long prof_n[MSLICE_K_COUNT] = {};
-    struct Pending { int kind; cudaEvent_t a, b; double bytes; };
+    struct Pending { int kind; cudaEvent_t a, b; double bytes; bool graph_owned = false; };
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> ev_pool;
     cudaEvent_t take_event() {
@@ -275,28 +275,45 @@ struct SimBase {
     }
     template <class F> void timed(cudaStream_t s, int kind, double bytes, F &&launch) {
         if (!prof) { launch(); return; }
+        // inside a stream capture a plain record only orders the capture; the external flag makes it a
+        // record node of the graph, so every replay records the event
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        MS_CUDA(cudaStreamIsCapturing(s, &cs));
+        const unsigned flags = cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
         cudaEvent_t a = take_event(), b = take_event();
-        MS_CUDA(cudaEventRecord(a, s));
+        MS_CUDA(cudaEventRecordWithFlags(a, s, flags));
         launch();
-        MS_CUDA(cudaEventRecord(b, s));
+        MS_CUDA(cudaEventRecordWithFlags(b, s, flags));
         pending.push_back({kind, a, b, bytes});
     }
-    // after a stream sync: fold the recorded launch durations into the totals
+    // after a stream sync: fold the recorded launch durations into the totals. The pending list is taken
+    // over first, so an error part-way leaves no event listed twice (the remaining ones are destroyed).
     void flush_profile() {
-        for (auto &p : pending) {
-            float ms = 0;
-            MS_CUDA(cudaEventSynchronize(p.b));
-            MS_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
-            prof_ms[p.kind] += ms;
-            prof_bytes[p.kind] += p.bytes;
-            prof_n[p.kind]++;
-            ev_pool.push_back(p.a);
-            ev_pool.push_back(p.b);
+        std::vector<Pending> todo;
+        todo.swap(pending);
+        size_t i = 0;
+        try {
+            for (; i < todo.size(); i++) {
+                const Pending &p = todo[i];
+                float ms = 0;
+                MS_CUDA(cudaEventSynchronize(p.b));
+                MS_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+                prof_ms[p.kind] += ms;
+                prof_bytes[p.kind] += p.bytes;
+                prof_n[p.kind]++;
+                if (p.graph_owned) continue;
+                ev_pool.push_back(p.a);
+                ev_pool.push_back(p.b);
+            }
+        } catch (...) {
+            for (; i < todo.size(); i++)
+                if (!todo[i].graph_owned) { cudaEventDestroy(todo[i].a); cudaEventDestroy(todo[i].b); }
+            throw;
         }
-        pending.clear();
     }
     virtual ~SimBase() {
-        for (auto &p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+        for (auto &p : pending)
+            if (!p.graph_owned) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
         for (auto e : ev_pool) cudaEventDestroy(e);
     }
     virtual void set_atoms(const int *Z, const double *x, const double *y, const double *z, size_t n, bool host) = 0;
@@ -443,6 +460,7 @@ struct Sim : SimBase {
         MS_CUDA(cudaStreamSynchronize(st()));
     }
     ~Sim() override {
+        drop_graphs();
         for (auto e : ev) if (e) cudaEventDestroy(e);
     }
 
@@ -643,6 +661,7 @@ struct Sim : SimBase {
 
     void ensure_waves(int b) {
         if (b <= batch_cap && wave.p) return;
+        drop_graphs();
         wave.ensure(ctx, (size_t)b * NN);
         recip.ensure(ctx, (size_t)b * NN);
         tmp.ensure(ctx, (size_t)b * NN);
@@ -693,16 +712,102 @@ struct Sim : SimBase {
         }
     }
 
+    // The launch sequence of one STEM batch depends only on the batch size, the output buffers and the
+    // engine's own device buffers; the probe positions and output pixel indices are device arrays that the
+    // kernels read. So the first batch of a shape runs eagerly, the second is captured into a CUDA graph and
+    // later batches replay it (a few microseconds of host time instead of 2 launches per slice). With
+    // profiling on, the graph holds its own timing events, read back after every replay.
+    struct BatchGraph {
+        cudaGraphExec_t exec = nullptr;
+        int nb = 0, n_pix = 0;
+        bool prof = false;
+        const void *key[5] = {};
+        unsigned long long nodes = 0, last_use = 0;
+        std::vector<Pending> events;   // owned by the graph
+    };
+    std::vector<BatchGraph> graphs;
+    unsigned long long graph_clock = 0;
+    static constexpr size_t kMaxGraphs = 4;
+    void release(BatchGraph &gr) {
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
+        pending.erase(std::remove_if(pending.begin(), pending.end(),
+                                     [&](const Pending &p) {
+                                         return p.graph_owned && std::any_of(gr.events.begin(), gr.events.end(),
+                                                                             [&](const Pending &q) { return q.a == p.a; });
+                                     }),
+                      pending.end());
+        for (auto &p : gr.events) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+        gr.exec = nullptr;
+        gr.events.clear();
+    }
+    void drop_graphs() {
+        for (auto &gr : graphs) release(gr);
+        graphs.clear();
+    }
+
     // Propagate `nb` STEM probes (scan pixel ids ids[0..nb)) through all slices; detector values of
     // output slice o go to out[(o*n_det + d)*n_pix + out_index[i]] (Kahan-accumulated if comp).
     void stem_batch(const int *ids, const int *out_index, int nb, int n_pix, double *out, double *comp) {
-        const mslice_geometry &g = H.g;
-        const cplx<R> *tw = ctx->twiddles<R>(N);
         h_pos.resize(nb);
         h_pix.assign(out_index, out_index + nb);
         for (int i = 0; i < nb; i++) h_pos[i] = probe_pos(ids[i]);
         MS_CUDA(cudaMemcpyAsync(pos.p, h_pos.data(), nb * sizeof(double2), cudaMemcpyHostToDevice, st()));
         MS_CUDA(cudaMemcpyAsync(pix.p, h_pix.data(), nb * sizeof(int), cudaMemcpyHostToDevice, st()));
+        const void *key[5] = {out, comp, wave.p, trans.p, partials.p};
+        BatchGraph *gr = nullptr;
+        for (auto &c : graphs)
+            if (c.nb == nb && c.n_pix == n_pix && c.prof == prof && std::equal(key, key + 5, c.key)) gr = &c;
+        if (!gr) {   // first batch of this shape: run eagerly, remember its launch count
+            unsigned long long l0 = ctx->launches;
+            enqueue_batch(nb, n_pix, out, comp);
+            if (graphs.size() == kMaxGraphs) {
+                auto lru = std::min_element(graphs.begin(), graphs.end(),
+                                            [](const BatchGraph &x, const BatchGraph &y) { return x.last_use < y.last_use; });
+                release(*lru);
+                graphs.erase(lru);
+            }
+            graphs.emplace_back();
+            BatchGraph &ng = graphs.back();
+            ng.nb = nb; ng.n_pix = n_pix; ng.prof = prof;
+            std::copy(key, key + 5, ng.key);
+            ng.nodes = ctx->launches - l0;
+            ng.last_use = ++graph_clock;
+            return;
+        }
+        gr->last_use = ++graph_clock;
+        if (!gr->exec) {   // second batch of this shape: capture
+            const size_t p0 = pending.size();
+            cudaGraph_t graph = nullptr;
+            MS_CUDA(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue_batch(nb, n_pix, out, comp);
+            } catch (...) {
+                cudaStreamEndCapture(st(), &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            MS_CUDA(cudaStreamEndCapture(st(), &graph));
+            cudaError_t e = cudaGraphInstantiate(&gr->exec, graph, 0);
+            cudaGraphDestroy(graph);
+            // the events recorded during the capture belong to the graph from now on
+            gr->events.assign(pending.begin() + p0, pending.end());
+            pending.resize(p0);
+            MS_CUDA(e);
+            ctx->launches -= gr->nodes;   // the capture only recorded the launches
+        }
+        if (!gr->events.empty()) {
+            // a replay re-records the graph's events: read the previous replay's durations first
+            const cudaEvent_t first = gr->events[0].a;
+            if (std::any_of(pending.begin(), pending.end(), [&](const Pending &p) { return p.a == first; })) flush_profile();
+        }
+        MS_CUDA(cudaGraphLaunch(gr->exec, st()));
+        ctx->launches += gr->nodes;
+        for (auto &p : gr->events) pending.push_back({p.kind, p.a, p.b, p.bytes, true});
+    }
+
+    void enqueue_batch(int nb, int n_pix, double *out, double *comp) {
+        const mslice_geometry &g = H.g;
+        const cplx<R> *tw = ctx->twiddles<R>(N);
         timed(st(), MSLICE_K_PROBE, (double)nb * NN * (sizeof(C) + sizeof(double2)), [&] { ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N)); });
         ctx->launches++;
         PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
