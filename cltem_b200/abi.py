@@ -66,6 +66,16 @@ class Config(C.Structure):
         ("intermediate_slices", C.c_int),
         ("ctem_image", C.c_int),
         ("probe_batch", C.c_int),
+        ("iterations", C.c_int),
+        ("mixed_static", C.c_int),
+        ("stem_moving_frame", C.c_int),
+        ("stem_job_pixels", C.c_int),
+        ("chromatic", C.c_int),
+        ("chromatic_cc", C.c_double),
+        ("chromatic_hwhm_neg", C.c_double), ("chromatic_hwhm_pos", C.c_double),
+        ("source_size", C.c_int),
+        ("source_fwhm", C.c_double),
+        ("seed", C.c_ulonglong),
     ]
 
 

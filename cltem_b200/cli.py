@@ -93,19 +93,23 @@ def _phonon_u2(raw_json):
     return float(ph.get("default", {}).get("value", 0.0)), bool(ph.get("force default", True))
 
 
-def _run_share(dev, settings, params, configs, out, idx, errors):
-    """Run a share of the configurations on one device; store (sum of results, count)."""
+def _run_share(dev, settings, params, configs, out, idx, errors, cfg=None, passes=None):
+    """Run a share on one device; store (sum of results, number of passes). Without `passes` the share is
+    one pass per configuration; with it, `passes` incoherent passes over all the configurations (cfg
+    carries the pass count and this device's seed)."""
     try:
         from .engine import Context, Simulation
         ctx = Context(dev)
         ctx.load_params(params)
-        sim = Simulation(ctx, settings.cfg)
-        mode = settings.cfg.mode
+        cfg = cfg if cfg is not None else settings.cfg
+        sim = Simulation(ctx, cfg)
+        mode = cfg.mode
+        weight = passes if passes is not None else len(configs)
         if mode in (abi.MODE_STEM, abi.MODE_CBED):
             sim.stage(configs)
             sim.run_staged()
-            r = sim.staged_result() * len(configs)
-            out[idx] = ({"main": r}, len(configs))
+            r = sim.staged_result() * weight
+            out[idx] = ({"main": r}, weight)
         else:
             acc = None
             for c in configs:
@@ -162,8 +166,15 @@ def main(argv=None):
     geo = geometry(settings.cfg)
     os.makedirs(a.output, exist_ok=True)
 
-    # frozen phonon configurations (incoherence iterations; PhononScattering::generateTdsFactor)
-    n_conf = settings.iterations if settings.phonon_enabled else 1
+    # frozen phonon configurations (incoherence iterations; PhononScattering::generateTdsFactor). With
+    # mixed static potentials the configurations are the sets and the iterations are passes drawing from
+    # them; without phonons, chromatic / source-size iterations are passes over the one structure.
+    iters = settings.effective_iterations()
+    mixed = settings.cfg.mixed_static > 1
+    settings.cfg.seed = a.seed
+    by_pass = mixed or (not settings.phonon_enabled and iters > 1)
+    n_conf = settings.cfg.mixed_static if mixed else (iters if settings.phonon_enabled else 1)
+    settings.cfg.iterations = iters if by_pass else 0
     u2, force_default = _phonon_u2(raw)
     if settings.phonon_enabled:
         if structure.u2 is not None and not force_default:
@@ -174,15 +185,28 @@ def main(argv=None):
         configs = [structure]
 
     devs = _devices(a.device)
-    shares = [configs[i::len(devs)] for i in range(len(devs))]
     results, errors, threads = [None] * len(devs), [], []
     t0 = time.time()
-    for i, (d, sh) in enumerate(zip(devs, shares)):
-        if not sh:
-            continue
-        th = threading.Thread(target=_run_share, args=(d, settings, params, sh, results, i, errors))
-        th.start()
-        threads.append(th)
+    if by_pass and settings.cfg.mode in (abi.MODE_STEM, abi.MODE_CBED):
+        # passes split over the devices; each device draws from its own seed
+        for i, d in enumerate(devs):
+            n_pass = iters // len(devs) + (1 if i < iters % len(devs) else 0)
+            if n_pass == 0:
+                continue
+            cfg_i = copy.deepcopy(settings.cfg)
+            cfg_i.iterations = n_pass
+            cfg_i.seed = (a.seed + 0x9E3779B97F4A7C15 * i) % (1 << 64)
+            th = threading.Thread(target=_run_share, args=(d, settings, params, configs, results, i, errors, cfg_i, n_pass))
+            th.start()
+            threads.append(th)
+    else:
+        shares = [configs[i::len(devs)] for i in range(len(devs))]
+        for i, (d, sh) in enumerate(zip(devs, shares)):
+            if not sh:
+                continue
+            th = threading.Thread(target=_run_share, args=(d, settings, params, sh, results, i, errors))
+            th.start()
+            threads.append(th)
     for th in threads:
         th.join()
     if errors:
@@ -195,7 +219,8 @@ def main(argv=None):
         imgs, _ = r
         for k, v in imgs.items():
             total[k] = v if k not in total else total[k] + v
-    total = {k: v / len(configs) for k, v in total.items()}
+    weight = sum(r[1] for r in results if r is not None)
+    total = {k: v / weight for k, v in total.items()}
 
     js = copy.deepcopy(raw)
     js["filename"] = os.path.abspath(a.structure)

@@ -43,7 +43,16 @@ class SimulationSettings:
         self.phonon_enabled = False
         self.phonon_default_u2 = 0.0
         self.parallel_pixels = 1
+        self.mixed_static_count = 1
+        self.mixed_static_enabled = False
         self.detectors = []
+
+    def effective_iterations(self) -> int:
+        """IncoherentEffects::iterations (src/simulation/incoherence/incoherenteffects.h:40-54): the stored
+        count when any effect of the mode is on (phonons; chromatic or source size outside CTEM), else 1."""
+        c = self.cfg
+        on = self.phonon_enabled or (c.mode != abi.MODE_CTEM and (c.chromatic or c.source_size))
+        return max(1, int(self.iterations)) if on else 1
 
     # -- detectors -------------------------------------------------------------------------------
     def set_detectors(self, dets):
@@ -137,6 +146,9 @@ def read_config(path_or_dict) -> SimulationSettings:
     except (KeyError, TypeError, ValueError):
         pass
     _try(j, lambda v: setattr(s, "parallel_pixels", v), "stem", "static area", "concurrent pixels", conv=int)
+    c.stem_job_pixels = max(1, int(s.parallel_pixels))
+    # "static area" off: every job simulates its own window (SimulationManager::currentAreaBase)
+    _try(j, lambda v: setattr(c, "stem_moving_frame", 0 if v else 1), "stem", "static area", "enabled", conv=bool)
     dets = []
     try:
         for name, d in _get(j, "stem", "detectors").items():
@@ -159,6 +171,20 @@ def read_config(path_or_dict) -> SimulationSettings:
     ph = ("incoherence", "inelastic scattering", "phonon")
     _try(j, lambda v: setattr(s, "phonon_enabled", v), *ph, "enabled", conv=bool)
     _try(j, lambda v: setattr(s, "phonon_default_u2", v), *ph, "default", "value", conv=float)
+    # mixed static potentials (jsonutils.cpp:319-326; SimulationManager::useParallelPotentials)
+    _try(j, lambda v: setattr(s, "mixed_static_count", v), *ph, "mixed static potentials", "count", conv=int)
+    _try(j, lambda v: setattr(s, "mixed_static_enabled", v), *ph, "mixed static potentials", "enabled", conv=bool)
+    c.mixed_static = s.mixed_static_count if (s.mixed_static_enabled and s.mixed_static_count > 1) else 0
+    # probe incoherence (jsonutils.cpp:276-308)
+    pr = ("incoherence", "probe")
+    _try(j, lambda v: setattr(c, "chromatic", int(v)), *pr, "chromatic", "enabled", conv=bool)
+    _try(j, lambda v: setattr(c, "chromatic_cc", v), *pr, "chromatic", "Cc", "val", conv=float)
+    _try(j, lambda v: setattr(c, "chromatic_hwhm_pos", v), *pr, "chromatic", "dE", "HWHM +", conv=float)
+    _try(j, lambda v: setattr(c, "chromatic_hwhm_neg", v), *pr, "chromatic", "dE", "HWHM -", conv=float)
+    _try(j, lambda v: setattr(c, "source_size", int(v)), *pr, "source size", "enabled", conv=bool)
+    _try(j, lambda v: setattr(c, "source_fwhm", v), *pr, "source size", "FWHM", "val", conv=float)
+    if c.mode != abi.MODE_STEM:
+        c.stem_moving_frame = 0   # the static-area switch is read only by STEM
     return s
 
 

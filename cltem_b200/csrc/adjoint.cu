@@ -123,116 +123,6 @@ __global__ void k_grad_v(size_t count, const cplx<R> *__restrict__ E, const cplx
     gV[i] = sigma * (ex * gy - ey * gx);
 }
 
-// d/drho of the projected potentials (projected_d.cl:104-181): K0' = -K1, K1' = -K0 - K1/x
-__device__ double k0d(double x) {   // NR 6.6 rational forms, same coefficients as the forward kernels
-    const double p0[5] = {1.0, 2.346487949187396e-1, 1.187082088663404e-2, 2.150707366040937e-4, 1.425433617130587e-6};
-    const double q0[3] = {9.847324170755358e-1, 1.518396076767770e-2, 8.362215678646257e-5};
-    const double pp0[5] = {1.159315156584126e-1, 2.770731240515333e-1, 2.066458134619875e-2, 4.574734709978264e-4, 3.454715527986737e-6};
-    const double qq0[3] = {9.836249671709183e-1, 1.627693622304549e-2, 9.809660603621949e-5};
-    const double a0[8] = {1.253314137315499, 1.475731032429900e1, 6.123767403223466e1, 1.121012633939949e2,
-                          9.285288485892228e1, 3.198289277679660e1, 3.595376024148513, 6.160228690102976e-2};
-    const double b0[8] = {1.0, 1.189963006673403e1, 5.027773590829784e1, 9.496513373427093e1,
-                          8.318077493230258e1, 3.181399777449301e1, 4.443672926432041, 1.408295601966600e-1};
-    auto poly = [](const double *c, int m, double z) { double s = c[m]; for (int i = m - 1; i >= 0; --i) s = s * z + c[i]; return s; };
-    if (x <= 1.0) {
-        double z = x * x;
-        return poly(pp0, 4, z) / poly(qq0, 2, 1.0 - z) - poly(p0, 4, z) * log(x) / poly(q0, 2, 1.0 - z);
-    }
-    double z = 1.0 / x;
-    return exp(-x) * poly(a0, 7, z) / poly(b0, 7, z) / sqrt(x);
-}
-__device__ double k1d(double x) {
-    const double p1[5] = {0.5, 5.598072040178741e-2, 1.818666382168295e-3, 2.397509908859959e-5, 1.239567816344855e-7};
-    const double q1[3] = {9.870202601341150e-1, 1.292092053534579e-2, 5.881933053917096e-5};
-    const double pp1[5] = {-3.079657578292062e-1, -8.109417631822442e-2, -3.477550948593604e-3, -5.385594871975406e-5, -3.110372465429008e-7};
-    const double qq1[3] = {9.861813171751389e-1, 1.375094061153160e-2, 6.774221332947002e-5};
-    const double a1[8] = {1.253314137315502, 1.457171340220454e1, 6.063161173098803e1, 1.147386690867892e2,
-                          1.040442011439181e2, 4.356596656837691e1, 7.265230396353690, 3.144418558991021e-1};
-    const double b1[8] = {1.0, 1.125154514806458e1, 4.427488496597630e1, 7.616113213117645e1,
-                          5.863377227890893e1, 1.850303673841586e1, 1.857244676566022, 2.538540887654872e-2};
-    auto poly = [](const double *c, int m, double z) { double s = c[m]; for (int i = m - 1; i >= 0; --i) s = s * z + c[i]; return s; };
-    if (x <= 1.0) {
-        double z = x * x;
-        return x * (poly(pp1, 4, z) / poly(qq1, 2, 1.0 - z) + poly(p1, 4, z) * log(x) / poly(q1, 2, 1.0 - z)) + 1.0 / x;
-    }
-    double z = 1.0 / x;
-    return exp(-x) * poly(a1, 7, z) / poly(b1, 7, z) / sqrt(x);
-}
-
-__device__ double dpot_drho(int form, const double *__restrict__ prm, int i_lim, int Z, double rho) {
-    if (form == 0) {   // Kirkland C.20
-        const double *p = prm + (Z - 1) * 12;
-        double s = 0;
-        for (int i = 0; i < i_lim; i++) {
-            double sb = sqrt(p[2 * i + 1]);
-            s += 300.8242834 * p[2 * i] * (-k1d(2.0 * M_PI * rho * sb)) * 2.0 * M_PI * sb;
-        }
-        for (int i = 0; i < i_lim; i++) {
-            double c = p[2 * i_lim + 2 * i], d = p[2 * i_lim + 2 * i + 1];
-            s += 150.4121417 * (c / d) * exp(-M_PI * M_PI * rho * rho / d) * (-2.0 * M_PI * M_PI * rho / d);
-        }
-        return s;
-    } else if (form == 1) {   // Peng
-        const double *p = prm + (Z - 1) * 10;
-        double s = 0;
-        for (int i = 0; i < i_lim; i++) {
-            double a = p[i], b = p[i + 5];
-            s += 150.4121417 * (a / b) * exp(-M_PI * M_PI * rho * rho / b) * (-2.0 * M_PI * M_PI * rho / b);
-        }
-        return s;
-    }
-    const double *p = prm + (Z - 1) * 10;   // Lobato eq. 16
-    double s = 0;
-    for (int i = 0; i < i_lim; i++) {
-        double a = p[i], b = p[i + 5];
-        double c = 2.0 * M_PI / sqrt(b), x = c * rho;
-        s += 945.090144399935 * a / (b * sqrt(b)) * (-c) * (k1d(x) + rho * k0d(x));
-    }
-    return s;
-}
-
-// dL/dx_a, dL/dy_a of the atoms [a0, a1) of slice k (sorted order): sum over pixels within 8 Å of
-// gV_k(r) V'(rho) d rho / d(x_a, y_a), rho = |r - r_a| clamped below at r_min (zero derivative there)
-__global__ void k_atom_grad(int a0, const double *__restrict__ ax, const double *__restrict__ ay, const int *__restrict__ aZ,
-                            const double *__restrict__ gV, int n, double startx, double starty, double dx, int form,
-                            const double *__restrict__ prm, int i_lim, double *__restrict__ gxy) {
-    __shared__ double red[32];
-    const int a = a0 + blockIdx.x;
-    const double xa = ax[a], ya = ay[a];
-    const int Z = aZ[a];
-    const double r_min = 0.25 * dx;
-    int ix0 = (int)floor((xa - 8.0 - startx) / dx), ix1 = (int)ceil((xa + 8.0 - startx) / dx);
-    int iy0 = (int)floor((ya - 8.0 - starty) / dx), iy1 = (int)ceil((ya + 8.0 - starty) / dx);
-    ix0 = max(ix0, 0); iy0 = max(iy0, 0); ix1 = min(ix1, n - 1); iy1 = min(iy1, n - 1);
-    const int w = ix1 - ix0 + 1, h = iy1 - iy0 + 1;
-    double gx = 0, gy = 0;
-    for (int i = threadIdx.x; i < w * h; i += blockDim.x) {
-        int px = ix0 + i % w, py = iy0 + i / w;
-        double rx = (startx + px * dx) - xa, ry = (starty + py * dx) - ya;
-        double rho = sqrt(rx * rx + ry * ry);
-        if (rho > r_min && rho <= 8.0) {
-            double f = gV[(size_t)py * n + px] * dpot_drho(form, prm, i_lim, Z, rho) / rho;
-            gx -= f * rx;   // d rho / d x_a = -rx / rho
-            gy -= f * ry;
-        }
-    }
-    // block sums of (gx, gy); thread 0 stores them for atom a
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        gx += __shfl_down_sync(0xffffffffu, gx, o);
-        gy += __shfl_down_sync(0xffffffffu, gy, o);
-    }
-    __shared__ double redy[32];
-    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = gx; redy[threadIdx.x >> 5] = gy; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double sx = 0, sy = 0;
-        for (int i = 0; i < (int)(blockDim.x + 31) / 32; i++) { sx += red[i]; sy += redy[i]; }
-        gxy[2 * (size_t)a] = sx;
-        gxy[2 * (size_t)a + 1] = sy;
-    }
-}
-
 // ---------------------------------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------------------------------
@@ -258,12 +148,6 @@ template <class R> void mul_conj_prop(cudaStream_t s, int n, cplx<R> *g, const c
 }
 template <class R> void grad_v(cudaStream_t s, size_t count, const cplx<R> *E, const cplx<R> *gE, double sigma, double *gV) {
     k_grad_v<R><<<(unsigned)((count + 255) / 256), 256, 0, s>>>(count, E, gE, sigma, gV);
-    MS_CUDA(cudaGetLastError());
-}
-void atom_grad(cudaStream_t s, int a0, int count, const double *ax, const double *ay, const int *aZ, const double *gV,
-               int n, double startx, double starty, double dx, int form, const double *prm, int i_lim, double *gxy) {
-    if (count <= 0) return;
-    k_atom_grad<<<count, 256, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, form, prm, i_lim, gxy);
     MS_CUDA(cudaGetLastError());
 }
 int reduction_blocks() { return kRedBlocks; }

@@ -17,9 +17,11 @@ template <class R> void mul_conj_prop(cudaStream_t s, int n, cplx<R> *g, const c
                                       const double *kx2, const double *ky2, double kmax2, R scale);
 // gV = sigma Im(conj(E) gE)
 template <class R> void grad_v(cudaStream_t s, size_t count, const cplx<R> *E, const cplx<R> *gE, double sigma, double *gV);
-// per-atom gradients (x, y) of the atoms [a0, a0+count) in sorted order from gV of their slice
+// per-atom gradients (x, y) of the atoms [a0, a0+count) in sorted order from gV of their slice (gather.cu);
+// T is the precision of the per-pixel terms and of prm (the parameterisation table)
+template <class T>
 void atom_grad(cudaStream_t s, int a0, int count, const double *ax, const double *ay, const int *aZ, const double *gV,
-               int n, double startx, double starty, double dx, int form, const double *prm, int i_lim, double *gxy);
+               int n, double startx, double starty, double dx, int form, const T *prm, int i_lim, double *gxy);
 int reduction_blocks();
 
 }  // namespace ms

@@ -6,6 +6,7 @@
 // slice, and a batch of waves that the fused row / column passes (passes.cuh) step through the slices.
 #include "../../include/mslice.h"
 #include "adjoint_ops.h"
+#include "draws.h"
 #include "fft.cuh"
 #include "launch.cuh"
 #include "misc.cuh"
@@ -14,6 +15,7 @@
 #include "potential_launch.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -71,6 +73,25 @@ struct HostGeom {
     std::vector<double> kx, ky;
 };
 
+// Moving STEM frame: paddedSimLimitsX/Y(pixel) when the static area is off
+// (SimulationManager::currentAreaBase, simulationmanager.cpp:485-505; StemArea::getPixelSimArea,
+// commonstructs.h:379-396). The window of stem_padding sits at the scan origin plus the pixel's offset
+// rounded down to the pixel size of the static frame; the SimulationCell padding is added around it.
+static void stem_frame(const mslice_config &c, int pixel, double x[2], double y[2]) {
+    double fx[2], fy[2];
+    corrected_limits(c.stem_area[0], c.stem_area[1], c.stem_area[2], c.stem_area[3], c.stem_padding, fx, fy);
+    const double pad_range = c.padding_xy - (-c.padding_xy);
+    const double rs = (pad_range + (fx[1] - fx[0])) / static_cast<double>(c.resolution);
+    const unsigned int x_px = (unsigned int)pixel % (unsigned int)c.stem_pixels_x;
+    const unsigned int y_px = (unsigned int)std::floor(pixel / c.stem_pixels_x);
+    const double pos_x = (c.stem_area[1] - c.stem_area[0]) / c.stem_pixels_x * x_px;
+    const double pos_y = (c.stem_area[3] - c.stem_area[2]) / c.stem_pixels_y * y_px;
+    const double xp = c.stem_area[0] + rs * std::floor(pos_x / rs), yp = c.stem_area[2] + rs * std::floor(pos_y / rs);
+    corrected_limits(xp, xp, yp, yp, c.stem_padding, x, y);
+    x[0] += -c.padding_xy; x[1] += c.padding_xy;
+    y[0] += -c.padding_xy; y[1] += c.padding_xy;
+}
+
 static void compute_geometry(const mslice_config &c, HostGeom &H) {
     if (c.mode != MSLICE_MODE_CTEM && c.mode != MSLICE_MODE_STEM && c.mode != MSLICE_MODE_CBED)
         throw ArgError("unknown simulation mode " + std::to_string(c.mode));
@@ -80,6 +101,12 @@ static void compute_geometry(const mslice_config &c, HostGeom &H) {
     if (c.full3d && c.full3d_integrals < 1) throw ArgError("full 3d integrals must be >= 1");
     if (c.n_detectors < 0 || c.n_detectors > MSLICE_MAX_DETECTORS) throw ArgError("too many detectors");
     if (c.mode == MSLICE_MODE_STEM && (c.stem_pixels_x < 1 || c.stem_pixels_y < 1)) throw ArgError("STEM scan needs pixels");
+    if (c.iterations < 0 || c.mixed_static < 0 || c.stem_job_pixels < 0) throw ArgError("negative incoherence count");
+    if (c.stem_moving_frame && c.mode != MSLICE_MODE_STEM) throw ArgError("the moving frame is a STEM option");
+    if (c.mixed_static > 1 && c.stem_moving_frame)
+        throw Unsupported("mixed static potentials with the moving STEM frame are not supported");
+    if (c.chromatic && !(c.chromatic_cc >= 0)) throw ArgError("chromatic Cc must be >= 0");
+    if (c.source_size && !(c.source_fwhm >= 0)) throw ArgError("source size FWHM must be >= 0");
     mslice_geometry &g = H.g;
     std::memset(&g, 0, sizeof(g));
     double fx[2], fy[2];
@@ -94,6 +121,7 @@ static void compute_geometry(const mslice_config &c, HostGeom &H) {
     fy[0] += -c.padding_xy; fy[1] += c.padding_xy;
     g.full_x[0] = g.sim_x[0] = fx[0]; g.full_x[1] = g.sim_x[1] = fx[1];
     g.full_y[0] = g.sim_y[0] = fy[0]; g.full_y[1] = g.sim_y[1] = fy[1];
+    if (c.mode == MSLICE_MODE_STEM && c.stem_moving_frame) stem_frame(c, 0, g.sim_x, g.sim_y);   // paddedSimLimitsX/Y(0)
 
     // SimulationCell::roundPaddingZ (simulationcell.cpp:43-61) and sliceCount (:75-83)
     const double dz = c.slice_thickness, off = c.slice_offset;
@@ -356,6 +384,14 @@ struct Sim : SimBase {
     // atoms
     size_t n_atoms = 0, atom_cap = 0;
     bool atoms_set = false, trans_built = false;
+    // incoherence: transmission sets (set k of slice s at trans + (k * n_slices + s) * NN), the set of each
+    // wave at each slice (tsel, [slice][wave]) and the defocus phase factor of each probe (dfac)
+    int n_sets = 1;
+    double build_x0 = 0, build_y0 = 0;   // frame start (Å) of the transmission being built
+    DevBuf<int> tsel;
+    DevBuf<double> dfac;
+    std::vector<int> h_sel;
+    std::vector<double> h_dfac;
     DevBuf<int> aZ, aZs, keys_in, keys_out, idx_in, idx_out, bid, zid, kept, counts, block_start;
     DevBuf<double> ax, ay, az, axs, ays, azs;
     DevBuf<unsigned char> cub_temp;
@@ -582,7 +618,7 @@ struct Sim : SimBase {
         p.blocks_x = g.blocks_x; p.blocks_y = g.blocks_y;
         p.max_x = g.full_x[1]; p.min_x = g.full_x[0]; p.max_y = g.full_y[1]; p.min_y = g.full_y[0];
         p.load_x = g.load_blocks_x; p.load_y = g.load_blocks_y; p.load_z = g.load_blocks_z;
-        p.sigma = g.sigma; p.startx = g.sim_x[0]; p.starty = g.sim_y[0];
+        p.sigma = g.sigma; p.startx = build_x0; p.starty = build_y0;
         p.beam_theta_mrad = cfg.beam_tilt; p.beam_phi = cfg.beam_azimuth;
         p.z0 = g.z_lims[0];
         p.integrals = cfg.full3d_integrals > 0 ? cfg.full3d_integrals : 1;
@@ -611,16 +647,40 @@ struct Sim : SimBase {
         ctx->launches += 3;
     }
 
-    void build_transmission() override {
+    // room for k transmission sets (contents are rebuilt by the caller)
+    void ensure_sets(int k) {
+        if (k <= n_sets && trans.p) return;
+        trans.ensure(ctx, (size_t)k * H.g.n_slices * NN);
+        n_sets = k;
+        trans_built = false;
+    }
+
+    // source-size shift of transmission build b (SimulationCbed::initialiseSimulation, simulationcbed.cpp:103-113)
+    void source_shift(int b, double &dx, double &dy) const {
+        dx = dy = 0;
+        if (cfg.source_size && cfg.mode != MSLICE_MODE_CTEM) draws::source_shift(cfg.seed, b, cfg.source_fwhm, dx, dy);
+    }
+
+    // the band-limited transmission of every slice into set k, frame starting at (x0, y0) Å
+    void build_set(int k, double x0, double y0) {
         if (!atoms_set) throw StateError("atoms not set (mslice_set_atoms)");
         const int S = H.g.n_slices;
-        // slices in chunks so one launch's grid stays within limits
-        const int chunk = 1024;
+        build_x0 = x0;
+        build_y0 = y0;
+        C *base = trans.p + (size_t)k * S * NN;
+        const int chunk = 1024;   // slices in chunks so one launch's grid stays within limits
         for (int s0 = 0; s0 < S; s0 += chunk) {
             int cnt = std::min(chunk, S - s0);
-            potentials(trans.p + (size_t)s0 * NN, s0, cnt);
-            band_limit(trans.p + (size_t)s0 * NN, cnt);
+            potentials(base + (size_t)s0 * NN, s0, cnt);
+            band_limit(base + (size_t)s0 * NN, cnt);
         }
+    }
+
+    // transmission of the current configuration in the frame of pixel 0 (build 0 of a run)
+    void build_transmission() override {
+        double dx, dy;
+        source_shift(0, dx, dy);
+        build_set(0, H.g.sim_x[0] + dx, H.g.sim_y[0] + dy);
         trans_built = true;
     }
 
@@ -639,6 +699,10 @@ struct Sim : SimBase {
         } else {
             if (!atoms_set) throw StateError("atoms not set");
             ensure_waves(1);
+            double dx, dy;
+            source_shift(0, dx, dy);
+            build_x0 = H.g.sim_x[0] + dx;
+            build_y0 = H.g.sim_y[0] + dy;
             potentials(tmp.p, slice, 1);
             copy_out_complex(tmp.p, NN, out);
         }
@@ -668,6 +732,8 @@ struct Sim : SimBase {
         partials.ensure(ctx, (size_t)b * std::max(1, cfg.n_detectors) * ops.col_blocks);
         pix.ensure(ctx, b);
         pos.ensure(ctx, b);
+        tsel.ensure(ctx, (size_t)b * H.g.n_slices);
+        dfac.ensure(ctx, b);
         batch_cap = b;
     }
 
@@ -679,7 +745,7 @@ struct Sim : SimBase {
         double2 p = make_double2(x - g.sim_x[0], y - g.sim_y[0]);
         MS_CUDA(cudaMemcpyAsync(pos.p, &p, sizeof(double2), cudaMemcpyHostToDevice, st()));
         const cplx<R> *tw = ctx->twiddles<R>(N);
-        ops.col_probe(st(), wave.p, 1, tw, chi.p, kx.p, ky.p, pos.p, (R)1);
+        ops.col_probe(st(), wave.p, 1, tw, chi.p, kx.p, ky.p, pos.p, (R)1, nullptr, g.wavelength);
         ops.col_fft(st(), wave.p, wave.p, 1, tw, (R)(1.0 / N), -1);
         ctx->launches += 2;
         copy_out_complex(wave.p, NN, out);
@@ -693,15 +759,16 @@ struct Sim : SimBase {
     }
 
     // STEM probe positions of scan pixels (simulationstem.cpp:152-188)
-    double2 probe_pos(int p) const {
-        const mslice_geometry &g = H.g;
+    double2 probe_pos(int p) const { return probe_pos(p, H.g.sim_x[0], H.g.sim_y[0]); }
+    // relative to the frame starting at (x0, y0) Å (initialiseProbeWave subtracts paddedSimLimits(pixel)[0])
+    double2 probe_pos(int p, double x0, double y0) const {
         int num_x = cfg.stem_pixels_x;
         double step_x = (cfg.stem_area[1] - cfg.stem_area[0]) / cfg.stem_pixels_x;
         double step_y = (cfg.stem_area[3] - cfg.stem_area[2]) / cfg.stem_pixels_y;
         int x_i = p % num_x;
         int y_i = (int)std::floor(p / num_x);
         double x_pos = cfg.stem_area[0] + x_i * step_x, y_pos = cfg.stem_area[2] + y_i * step_y;
-        return make_double2(x_pos - g.sim_x[0], y_pos - g.sim_y[0]);
+        return make_double2(x_pos - x0, y_pos - y0);
     }
 
     void check_cancel() {
@@ -721,12 +788,17 @@ struct Sim : SimBase {
         cudaGraphExec_t exec = nullptr;
         int nb = 0, n_pix = 0;
         bool prof = false;
-        const void *key[5] = {};
+        const void *key[7] = {};
         unsigned long long nodes = 0, last_use = 0;
         std::vector<Pending> events;   // owned by the graph
     };
     std::vector<BatchGraph> graphs;
     unsigned long long graph_clock = 0;
+    // MSLICE_NO_GRAPHS=1 launches every batch eagerly (for kernel profilers that filter launches by name)
+    const bool use_graphs = [] {
+        const char *e = std::getenv("MSLICE_NO_GRAPHS");
+        return !(e && e[0] == '1');
+    }();
     static constexpr size_t kMaxGraphs = 4;
     void release(BatchGraph &gr) {
         if (gr.exec) cudaGraphExecDestroy(gr.exec);
@@ -745,21 +817,31 @@ struct Sim : SimBase {
         graphs.clear();
     }
 
-    // Propagate `nb` STEM probes (scan pixel ids ids[0..nb)) through all slices; detector values of
-    // output slice o go to out[(o*n_det + d)*n_pix + out_index[i]] (Kahan-accumulated if comp).
-    void stem_batch(const int *ids, const int *out_index, int nb, int n_pix, double *out, double *comp) {
-        h_pos.resize(nb);
+    // Propagate `nb` STEM probes through all slices: probe i at hpos[i] (Å, in the frame of its transmission
+    // set); detector values of output slice o go to out[(o*n_det + d)*n_pix + out_index[i]] (Kahan-accumulated
+    // if comp). with_sel: h_sel holds the set of every wave at every slice ([slice][wave]); with_df: h_dfac
+    // holds each probe's defocus phase factor.
+    void stem_batch(const double2 *hpos, const int *out_index, int nb, int n_pix, double *out, double *comp,
+                    bool with_sel, bool with_df) {
         h_pix.assign(out_index, out_index + nb);
-        for (int i = 0; i < nb; i++) h_pos[i] = probe_pos(ids[i]);
-        MS_CUDA(cudaMemcpyAsync(pos.p, h_pos.data(), nb * sizeof(double2), cudaMemcpyHostToDevice, st()));
+        MS_CUDA(cudaMemcpyAsync(pos.p, hpos, nb * sizeof(double2), cudaMemcpyHostToDevice, st()));
         MS_CUDA(cudaMemcpyAsync(pix.p, h_pix.data(), nb * sizeof(int), cudaMemcpyHostToDevice, st()));
-        const void *key[5] = {out, comp, wave.p, trans.p, partials.p};
+        if (with_sel)
+            MS_CUDA(cudaMemcpyAsync(tsel.p, h_sel.data(), (size_t)nb * H.g.n_slices * sizeof(int), cudaMemcpyHostToDevice, st()));
+        if (with_df) MS_CUDA(cudaMemcpyAsync(dfac.p, h_dfac.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st()));
+        const int *sel = with_sel ? tsel.p : nullptr;
+        const double *df = with_df ? dfac.p : nullptr;
+        const void *key[7] = {out, comp, wave.p, trans.p, partials.p, sel, df};
         BatchGraph *gr = nullptr;
         for (auto &c : graphs)
-            if (c.nb == nb && c.n_pix == n_pix && c.prof == prof && std::equal(key, key + 5, c.key)) gr = &c;
+            if (c.nb == nb && c.n_pix == n_pix && c.prof == prof && std::equal(key, key + 7, c.key)) gr = &c;
+        if (!use_graphs) {
+            enqueue_batch(nb, n_pix, out, comp, sel, df);
+            return;
+        }
         if (!gr) {   // first batch of this shape: run eagerly, remember its launch count
             unsigned long long l0 = ctx->launches;
-            enqueue_batch(nb, n_pix, out, comp);
+            enqueue_batch(nb, n_pix, out, comp, sel, df);
             if (graphs.size() == kMaxGraphs) {
                 auto lru = std::min_element(graphs.begin(), graphs.end(),
                                             [](const BatchGraph &x, const BatchGraph &y) { return x.last_use < y.last_use; });
@@ -769,7 +851,7 @@ struct Sim : SimBase {
             graphs.emplace_back();
             BatchGraph &ng = graphs.back();
             ng.nb = nb; ng.n_pix = n_pix; ng.prof = prof;
-            std::copy(key, key + 5, ng.key);
+            std::copy(key, key + 7, ng.key);
             ng.nodes = ctx->launches - l0;
             ng.last_use = ++graph_clock;
             return;
@@ -780,7 +862,7 @@ struct Sim : SimBase {
             cudaGraph_t graph = nullptr;
             MS_CUDA(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal));
             try {
-                enqueue_batch(nb, n_pix, out, comp);
+                enqueue_batch(nb, n_pix, out, comp, sel, df);
             } catch (...) {
                 cudaStreamEndCapture(st(), &graph);
                 if (graph) cudaGraphDestroy(graph);
@@ -805,10 +887,13 @@ struct Sim : SimBase {
         for (auto &p : gr->events) pending.push_back({p.kind, p.a, p.b, p.bytes, true});
     }
 
-    void enqueue_batch(int nb, int n_pix, double *out, double *comp) {
+    void enqueue_batch(int nb, int n_pix, double *out, double *comp, const int *sel, const double *df) {
         const mslice_geometry &g = H.g;
         const cplx<R> *tw = ctx->twiddles<R>(N);
-        timed(st(), MSLICE_K_PROBE, (double)nb * NN * (sizeof(C) + sizeof(double2)), [&] { ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N)); });
+        const size_t set_stride = (size_t)g.n_slices * NN;
+        timed(st(), MSLICE_K_PROBE, (double)nb * NN * (sizeof(C) + sizeof(double2)), [&] {
+            ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N), df, g.wavelength);
+        });
         ctx->launches++;
         PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
         DetArgs det{detmask.p, cfg.n_detectors, partials.p};
@@ -817,7 +902,8 @@ struct Sim : SimBase {
         const R a = (R)(1.0 / N), b = (R)(s2d * s2d * N), ds = (R)s2d;
         for (int s = 0; s < g.n_slices; s++) {
             timed(st(), MSLICE_K_ROW_STEP, (double)nb * NN * sizeof(C) * ((s == 0 ? 1.0 : fa) + 1.0 + fa), [&] {
-                ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a, xa, xb, s == 0 ? 1 : 0);
+                ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a, xa, xb, s == 0 ? 1 : 0,
+                             sel ? sel + (size_t)s * nb : nullptr, set_stride);
             });
             bool is_out = oi < outs.size() && outs[oi] == s;
             int mode = !is_out ? COL_STEP : (s == g.n_slices - 1 ? COL_DET_ONLY : COL_STEP_DET);
@@ -833,12 +919,95 @@ struct Sim : SimBase {
         }
     }
 
+    // pi * (chromatic defocus change) / wavelength of each probe of pass `pass` (0 when chromatic is off)
+    void fill_defocus(int pass, const int *pid, int nb) {
+        h_dfac.resize(nb);
+        for (int i = 0; i < nb; i++)
+            h_dfac[i] = kPi *
+                        draws::defocus_change(cfg.seed, pass, pid[i], cfg.chromatic_cc, cfg.chromatic_hwhm_neg,
+                                              cfg.chromatic_hwhm_pos, cfg.voltage) /
+                        H.g.wavelength;
+    }
+
+    // One pass of STEM probes over scan pixels ids[0..n): `pass` numbers the random draws. Detector values
+    // go to out at out_index (stem_batch). The static frame uses the built transmission (set 0, or the
+    // mixed static sets); the moving frame splits the pixels into jobs of stem_job_pixels consecutive
+    // entries (SimulationRunner::SplitJobs, simulationrunner.cpp:52-134) and builds each job's window here,
+    // several jobs per batch, one transmission set per job.
+    void stem_pass(int pass, const int *ids, const int *out_index, size_t n, int n_pix, double *out, double *comp,
+                   bool sync_each) {
+        const mslice_geometry &g = H.g;
+        const int S = g.n_slices;
+        const int K = cfg.mixed_static > 1 ? cfg.mixed_static : 1;
+        const bool chrom = cfg.chromatic != 0;
+        auto after_batch = [&](size_t done) {
+            if (!sync_each) return;
+            MS_CUDA(cudaStreamSynchronize(st()));
+            flush_profile();
+            if (progress) progress((double)done / n, progress_user);
+        };
+        if (!cfg.stem_moving_frame) {
+            for (size_t b0 = 0; b0 < n; b0 += batch_cap) {
+                check_cancel();
+                const int nb = (int)std::min<size_t>(batch_cap, n - b0);
+                h_pos.resize(nb);
+                for (int i = 0; i < nb; i++) h_pos[i] = probe_pos(ids[b0 + i]);
+                if (K > 1) {
+                    h_sel.resize((size_t)nb * S);
+                    for (int sl = 0; sl < S; sl++)
+                        for (int i = 0; i < nb; i++) h_sel[(size_t)sl * nb + i] = draws::set_of(cfg.seed, pass, ids[b0 + i], sl, K);
+                }
+                if (chrom) fill_defocus(pass, ids + b0, nb);
+                stem_batch(h_pos.data(), out_index + b0, nb, n_pix, out, comp, K > 1, chrom);
+                after_batch(b0 + nb);
+            }
+            return;
+        }
+        const int P = std::max(1, cfg.stem_job_pixels);
+        const size_t n_jobs = (n + P - 1) / P;
+        const size_t set_bytes = (size_t)S * NN * sizeof(C);
+        size_t J = std::max(1, batch_cap / P);
+        J = std::min(J, std::max<size_t>(1, ((size_t)1 << 30) / set_bytes));   // at most ~1 GiB of job windows
+        J = std::min(J, std::max<size_t>(n_jobs, 1));
+        ensure_sets((int)J);
+        std::vector<double2> origin(J);
+        for (size_t j0 = 0; j0 < n_jobs; j0 += J) {
+            check_cancel();
+            const int nj = (int)std::min(J, n_jobs - j0);
+            for (int j = 0; j < nj; j++) {   // each job's frame: paddedSimLimitsX/Y of its first pixel
+                double fx[2], fy[2], dx, dy;
+                stem_frame(cfg, ids[(j0 + j) * P], fx, fy);
+                source_shift((int)((size_t)pass * n_jobs + j0 + j), dx, dy);
+                build_set(j, fx[0] + dx, fy[0] + dy);
+                origin[j] = make_double2(fx[0], fy[0]);
+            }
+            const size_t w0 = j0 * P, w1 = std::min(n, (j0 + nj) * P);
+            for (size_t b0 = w0; b0 < w1; b0 += batch_cap) {
+                check_cancel();
+                const int nb = (int)std::min<size_t>(batch_cap, w1 - b0);
+                h_pos.resize(nb);
+                h_sel.resize((size_t)nb * S);
+                for (int i = 0; i < nb; i++) {
+                    const int j = (int)((b0 + i) / P - j0);
+                    h_pos[i] = probe_pos(ids[b0 + i], origin[j].x, origin[j].y);
+                    for (int sl = 0; sl < S; sl++) h_sel[(size_t)sl * nb + i] = j;
+                }
+                if (chrom) fill_defocus(pass, ids + b0, nb);
+                stem_batch(h_pos.data(), out_index + b0, nb, n_pix, out, comp, true, chrom);
+                after_batch(b0 + nb);
+            }
+        }
+        trans_built = false;   // the sets now hold job windows
+    }
+
     void stem_run(const int *pixels, size_t n, double *out) override {
         if (cfg.mode != MSLICE_MODE_STEM) throw StateError("simulation is not in STEM mode");
-        if (!trans_built) build_transmission();
+        if (cfg.mixed_static > 1)
+            throw StateError("mixed static potentials draw from staged configurations (mslice_stem_run_staged)");
         const int np = cfg.stem_pixels_x * cfg.stem_pixels_y;
         for (size_t i = 0; i < n; i++)
             if (pixels[i] < 0 || pixels[i] >= np) throw ArgError("scan pixel index out of range");
+        if (!cfg.stem_moving_frame && !trans_built) build_transmission();
         const int B = default_batch();
         ensure_waves(std::min<int>(B, (int)std::max<size_t>(n, 1)));
         const mslice_geometry &g = H.g;
@@ -848,29 +1017,36 @@ struct Sim : SimBase {
         MS_CUDA(cudaMemsetAsync(dout.p, 0, std::max<size_t>(tot, 1) * sizeof(double), st()));
         std::vector<int> idx(n);
         for (size_t i = 0; i < n; i++) idx[i] = (int)i;
-        for (size_t b0 = 0; b0 < n; b0 += batch_cap) {
-            check_cancel();
-            int nb = (int)std::min<size_t>(batch_cap, n - b0);
-            stem_batch(pixels + b0, idx.data() + b0, nb, (int)n, dout.p, nullptr);
-            MS_CUDA(cudaStreamSynchronize(st()));
-            flush_profile();
-            if (progress) progress((double)(b0 + nb) / n, progress_user);
-        }
+        stem_pass(0, pixels, idx.data(), n, (int)n, dout.p, nullptr, true);
         if (tot) MS_CUDA(cudaMemcpy(out, dout.p, tot * sizeof(double), cudaMemcpyDeviceToHost));
     }
 
     // one probe (CBED) or plane wave (CTEM) through all slices with outputs at the output slices
+    // (pass numbers the random draws: the mixed static set of each slice, the chromatic defocus change)
     template <class F>
-    void single_wave(bool plane, F &&on_output) {
+    void single_wave(bool plane, int pass, F &&on_output) {
         const mslice_geometry &g = H.g;
         const cplx<R> *tw = ctx->twiddles<R>(N);
         ensure_waves(1);
+        const int K = cfg.mixed_static > 1 ? cfg.mixed_static : 1;
+        const size_t set_stride = (size_t)g.n_slices * NN;
+        if (K > 1) {
+            h_sel.resize(g.n_slices);
+            for (int sl = 0; sl < g.n_slices; sl++) h_sel[sl] = draws::set_of(cfg.seed, pass, 0, sl, K);
+            MS_CUDA(cudaMemcpyAsync(tsel.p, h_sel.data(), g.n_slices * sizeof(int), cudaMemcpyHostToDevice, st()));
+        }
         if (plane) {
             plane_wave_state<R>(st(), N, wave.p);
         } else {
             double2 p = make_double2(cfg.cbed_x - g.sim_x[0], cfg.cbed_y - g.sim_y[0]);
             MS_CUDA(cudaMemcpyAsync(pos.p, &p, sizeof(double2), cudaMemcpyHostToDevice, st()));
-            ops.col_probe(st(), wave.p, 1, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N));
+            const int pid = 0;
+            if (cfg.chromatic) {
+                fill_defocus(pass, &pid, 1);
+                MS_CUDA(cudaMemcpyAsync(dfac.p, h_dfac.data(), sizeof(double), cudaMemcpyHostToDevice, st()));
+            }
+            ops.col_probe(st(), wave.p, 1, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N), cfg.chromatic ? dfac.p : nullptr,
+                          g.wavelength);
         }
         ctx->launches++;
         PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
@@ -881,7 +1057,10 @@ struct Sim : SimBase {
         for (int s = 0; s < g.n_slices; s++) {
             check_cancel();
             // single waves keep every column so the exit wave and the reciprocal copy are complete
-            timed(st(), MSLICE_K_ROW_STEP, 3.0 * NN * sizeof(C), [&] { ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1); });
+            timed(st(), MSLICE_K_ROW_STEP, 3.0 * NN * sizeof(C), [&] {
+                ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1, K > 1 ? tsel.p + s : nullptr,
+                             set_stride);
+            });
             bool is_out = oi < outs.size() && outs[oi] == s;
             timed(st(), MSLICE_K_COL_STEP, (is_out ? 3.0 : 2.0) * NN * sizeof(C), [&] {
                 ops.col_step(st(), wave.p, 1, tw, pt, b, ds, det, is_out ? recip.p : nullptr, is_out ? COL_STEP_DET : COL_STEP,
@@ -895,10 +1074,12 @@ struct Sim : SimBase {
 
     void cbed_run(double *diff) override {
         if (cfg.mode != MSLICE_MODE_CBED) throw StateError("simulation is not in CBED mode");
+        if (cfg.mixed_static > 1)
+            throw StateError("mixed static potentials draw from staged configurations (mslice_cbed_run_staged)");
         if (!trans_built) build_transmission();
         DevBuf<double> d;
         d.ensure(ctx, (size_t)H.g.n_outputs * NN);
-        single_wave(false, [&](int o) {
+        single_wave(false, 0, [&](int o) {
             diffraction<R>(st(), N, recip.p, d.p + (size_t)o * NN, nullptr);
             ctx->launches++;
         });
@@ -908,6 +1089,7 @@ struct Sim : SimBase {
 
     void ctem_run(double *ew, double *diff, double *image) override {
         if (cfg.mode != MSLICE_MODE_CTEM) throw StateError("simulation is not in CTEM mode");
+        if (cfg.mixed_static > 1) throw Unsupported("mixed static potentials are implemented for STEM and CBED runs");
         if (!trans_built) build_transmission();
         const int no = H.g.n_outputs;
         DevBuf<double> dd, di;
@@ -917,7 +1099,7 @@ struct Sim : SimBase {
         if (image && cfg.ctem_image) di.ensure(ctx, (size_t)no * NN);
         const cplx<R> *tw = ctx->twiddles<R>(N);
         const mslice_geometry &g = H.g;
-        single_wave(true, [&](int o) {
+        single_wave(true, 0, [&](int o) {
             if (ew) {   // psi = (1/N) Dinv_r phi  (getExitWaveImage, simulationgeneral.cpp:808-830)
                 ops.row_fft(st(), wave.p, tmp.p, 1, tw, (R)(1.0 / N), +1);
                 convert_to_double<R>(st(), NN, tmp.p, de.p + (size_t)o * NN);
@@ -971,22 +1153,48 @@ struct Sim : SimBase {
         std::vector<int> ids(np);
         for (int i = 0; i < np; i++) ids[i] = i;
         if (mode == MSLICE_MODE_STEM) ensure_waves(std::min(default_batch(), np));
+        // passes: one per staged configuration, or cfg.iterations passes cycling through them; with mixed
+        // static potentials the first mixed_static configurations are built once as the sets (the reference
+        // keeps them across jobs, simulationgeneral.cpp:358) and every pass draws new sets
+        const int K = cfg.mixed_static > 1 ? cfg.mixed_static : 1;
+        if (K > 1 && n_configs < K) throw StateError("mixed static potentials need mixed_static staged configurations");
+        const int passes = K > 1 ? std::max(1, cfg.iterations) : (cfg.iterations > 0 ? cfg.iterations : n_configs);
         float t_build = 0, t_prop = 0;
         MS_CUDA(cudaEventRecord(ev[2], st()));
-        for (int c = 0; c < n_configs; c++) {
+        if (K > 1) {
+            MS_CUDA(cudaEventRecord(ev[0], st()));
+            ensure_sets(K);
+            double dx, dy;
+            source_shift(0, dx, dy);
+            for (int k = 0; k < K; k++) {
+                sort_device(sZ.p + cfg_offsets[k], sx.p + cfg_offsets[k], sy.p + cfg_offsets[k], sz.p + cfg_offsets[k],
+                            cfg_counts[k]);
+                build_set(k, g.sim_x[0] + dx, g.sim_y[0] + dy);
+            }
+            trans_built = true;
+            MS_CUDA(cudaEventRecord(ev[1], st()));
+            MS_CUDA(cudaEventSynchronize(ev[1]));
+            MS_CUDA(cudaEventElapsedTime(&t_build, ev[0], ev[1]));
+        }
+        for (int it = 0; it < passes; it++) {
             check_cancel();
             MS_CUDA(cudaEventRecord(ev[0], st()));
-            sort_device(sZ.p + cfg_offsets[c], sx.p + cfg_offsets[c], sy.p + cfg_offsets[c], sz.p + cfg_offsets[c], cfg_counts[c]);
-            build_transmission();
+            if (K == 1) {
+                const int c = it % n_configs;
+                sort_device(sZ.p + cfg_offsets[c], sx.p + cfg_offsets[c], sy.p + cfg_offsets[c], sz.p + cfg_offsets[c],
+                            cfg_counts[c]);
+                if (!(mode == MSLICE_MODE_STEM && cfg.stem_moving_frame)) {   // the moving frame builds per job
+                    double dx, dy;
+                    source_shift(it, dx, dy);
+                    build_set(0, g.sim_x[0] + dx, g.sim_y[0] + dy);
+                    trans_built = true;
+                }
+            }
             MS_CUDA(cudaEventRecord(ev[1], st()));
             if (mode == MSLICE_MODE_STEM) {
-                for (int b0 = 0; b0 < np; b0 += batch_cap) {
-                    check_cancel();
-                    int nb = std::min(batch_cap, np - b0);
-                    stem_batch(ids.data() + b0, ids.data() + b0, nb, np, acc.p, comp.p);
-                }
+                stem_pass(it, ids.data(), ids.data(), (size_t)np, np, acc.p, comp.p, false);
             } else {
-                single_wave(false, [&](int o) {
+                single_wave(false, it, [&](int o) {
                     diffraction<R>(st(), N, recip.p, acc.p + (size_t)o * NN, comp.p + (size_t)o * NN);
                     ctx->launches++;
                 });
@@ -999,12 +1207,12 @@ struct Sim : SimBase {
             MS_CUDA(cudaEventElapsedTime(&b, ev[1], ev[3]));
             t_build += a;
             t_prop += b;
-            if (progress) progress((double)(c + 1) / n_configs, progress_user);
+            if (progress) progress((double)(it + 1) / passes, progress_user);
         }
         float tot = 0;
         MS_CUDA(cudaEventElapsedTime(&tot, ev[2], ev[3]));
         timing[0] = t_build; timing[1] = t_prop; timing[2] = tot;
-        acc_configs = n_configs;
+        acc_configs = passes;
     }
 
     void staged_result(double *out, size_t cap) override {
@@ -1030,6 +1238,7 @@ struct Sim : SimBase {
         if (cfg.mode != MSLICE_MODE_CTEM) throw StateError("the image loss needs a CTEM simulation");
         if (cfg.full3d) throw Unsupported("gradients are implemented for the projected potential");
         if (cfg.beam_tilt != 0.0) throw Unsupported("gradients are implemented without beam tilt");
+        if (cfg.mixed_static > 1) throw Unsupported("gradients are implemented without mixed static potentials");
         if (!atoms_set) throw StateError("atoms not set");
         const int S = g.n_slices;
         const int c = ck <= 0 ? (int)std::ceil(std::sqrt((double)S)) : std::min(ck, S);
@@ -1063,7 +1272,7 @@ struct Sim : SimBase {
             if (want_grad && s % c == 0)
                 MS_CUDA(cudaMemcpyAsync(ck_buf.p + (size_t)(s / c) * NN, wave.p, NN * sizeof(C), cudaMemcpyDeviceToDevice, st()));
             if (want_grad && c == 1) ops.row_step_save(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, save.p + (size_t)s * NN);
-            else ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1);
+            else ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1, nullptr, 0);
             bool last = s == S - 1;
             ops.col_step(st(), wave.p, 1, tw, pt, b, ds, nodet, last ? recip.p : nullptr, last ? COL_STEP_DET : COL_STEP,
                          all_tiles, 0);
@@ -1122,8 +1331,8 @@ struct Sim : SimBase {
                 band_limit(gT.p, 1);   // G_E = bandlimit(G_T): the band limit is self-adjoint
                 grad_v<R>(st(), NN, E.p + (size_t)s * NN, gT.p, g.sigma, gV.p);
                 const int a0 = hbs[(size_t)s * nb], a1 = hbs[(size_t)(s + 1) * nb];
-                atom_grad(st(), a0, a1 - a0, axs.p, ays.p, aZs.p, gV.p, N, g.sim_x[0], g.sim_y[0], g.real_scale,
-                          ctx->params.form, ctx->prm_d, ctx->params.i_count, gxy.p);
+                atom_grad<R>(st(), a0, a1 - a0, axs.p, ays.p, aZs.p, gV.p, N, g.sim_x[0], g.sim_y[0], g.real_scale,
+                             ctx->params.form, params_dev(), ctx->params.i_count, gxy.p);
                 ctx->launches += 5;
             }
         }
@@ -1576,6 +1785,32 @@ int mslice_profile_read(mslice_sim *sim, int kernel, double *total_ms, unsigned 
                 sim->impl->prof_ms[k] = 0;
                 sim->impl->prof_n[k] = 0;
                 sim->impl->prof_bytes[k] = 0;
+            }
+    });
+}
+
+int mslice_incoherence_draws(const mslice_config *cfg, int pass, const int *pixels, size_t n_pixels, double *defocus,
+                             int *sets, int n_slices, int n_builds, double *shift) {
+    return guarded([&] {
+        need(cfg != nullptr && (pixels != nullptr || n_pixels == 0), "null argument");
+        need(n_slices >= 0 && n_builds >= 0, "negative count");
+        for (size_t i = 0; i < n_pixels; i++) {
+            if (defocus)
+                defocus[i] = cfg->chromatic ? ms::draws::defocus_change(cfg->seed, pass, pixels[i], cfg->chromatic_cc,
+                                                                          cfg->chromatic_hwhm_neg, cfg->chromatic_hwhm_pos,
+                                                                          cfg->voltage)
+                                            : 0.0;
+            if (sets)
+                for (int s = 0; s < n_slices; s++)
+                    sets[i * n_slices + s] =
+                        cfg->mixed_static > 1 ? ms::draws::set_of(cfg->seed, pass, pixels[i], s, cfg->mixed_static) : 0;
+        }
+        if (shift)
+            for (int b = 0; b < n_builds; b++) {
+                double dx = 0, dy = 0;
+                if (cfg->source_size && cfg->mode != MSLICE_MODE_CTEM) ms::draws::source_shift(cfg->seed, b, cfg->source_fwhm, dx, dy);
+                shift[2 * b] = dx;
+                shift[2 * b + 1] = dy;
             }
     });
 }

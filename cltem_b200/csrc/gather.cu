@@ -1,0 +1,107 @@
+// gather.cu — atom-position gradients of the differentiable CTEM loss.
+//
+// dL/dx_a, dL/dy_a of the atoms [a0, a0+count) of one slice (sorted order): the sum over the pixels within
+// 8 Å of atom a of gV(r) V'(rho) d rho / d(x_a, y_a), rho = |r - r_a|, with V' the derivative of the
+// projected form the forward potential kernel sums (potential.cuh; transmission_potentials_projected_d.cl)
+// and zero where the forward clamps rho to r_min = dx/4.
+//
+// One 256-thread block per atom, threads tiled 32 x 8 over the atom's pixel box. Pixel-to-atom offsets
+// are formed in FP64 (as in the forward kernel); rho, V'(rho) and the per-thread sums are in the engine's
+// precision T; the block sums are FP64. Built without -fmad=false: nothing here restates a reference
+// statement bit for bit.
+#include "adjoint_ops.h"
+#include "potential.cuh"
+
+namespace ms {
+
+// d/drho of kirkland_p / peng_p / lobato_p (potential.cuh), using K0' = -K1 and K1' = -K0 - K1/x
+template <class T>
+__device__ __forceinline__ T dpot_drho(int form, const T *__restrict__ prm, int i_lim, int Z, T rho) {
+    const T two_pi = (T)(2.0 * M_PI), pi2 = (T)(M_PI * M_PI);
+    T s = 0;
+    if (form == 0) {   // Kirkland eq. C.20: 300.82 a K0(2 pi rho sqrt b) + 150.41 (c/d) exp(-pi^2 rho^2 / d)
+        const T *p = prm + (Z - 1) * 12;
+        for (int i = 0; i < i_lim; i++) {
+            const T sb = fsqrt(p[2 * i + 1]);
+            s -= (T)300.8242834 * p[2 * i] * bessk1<T>(two_pi * rho * sb) * two_pi * sb;
+        }
+        for (int i = 0; i < i_lim; i++) {
+            const T c = p[2 * i_lim + 2 * i], d_inv = (T)1 / p[2 * i_lim + 2 * i + 1];
+            s -= (T)150.4121417 * (c * d_inv) * fexp(-pi2 * rho * rho * d_inv) * ((T)2 * pi2 * rho * d_inv);
+        }
+    } else if (form == 1) {   // Peng: 150.41 (a/b) exp(-pi^2 rho^2 / b)
+        const T *p = prm + (Z - 1) * 10;
+        for (int i = 0; i < i_lim; i++) {
+            const T a = p[i], b_inv = (T)1 / p[i + 5];
+            s -= (T)150.4121417 * (a * b_inv) * fexp(-pi2 * rho * rho * b_inv) * ((T)2 * pi2 * rho * b_inv);
+        }
+    } else {   // Lobato eq. 16: 945.09 a b^-3/2 (K0(c rho) + rho K1(c rho)), c = 2 pi / sqrt b
+        const T *p = prm + (Z - 1) * 10;
+        for (int i = 0; i < i_lim; i++) {
+            const T a = p[i], bir = (T)1 / fsqrt(p[i + 5]);
+            const T c = two_pi * bir, x = c * rho;
+            s -= (T)945.090144399935 * a * (bir * bir * bir) * c * (bessk1<T>(x) + rho * bessk0<T>(x));
+        }
+    }
+    return s;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256)
+k_atom_grad(int a0, const double *__restrict__ ax, const double *__restrict__ ay, const int *__restrict__ aZ,
+            const double *__restrict__ gV, int n, double startx, double starty, double dx, int form,
+            const T *__restrict__ prm, int i_lim, double *__restrict__ gxy) {
+    __shared__ double red[2][8];
+    const int a = a0 + blockIdx.x;
+    const double xa = ax[a], ya = ay[a];
+    const int Z = aZ[a];
+    const T r_min2 = (T)(0.0625 * dx * dx);   // (dx / 4)^2
+    int ix0 = (int)floor((xa - 8.0 - startx) / dx), ix1 = (int)ceil((xa + 8.0 - startx) / dx);
+    int iy0 = (int)floor((ya - 8.0 - starty) / dx), iy1 = (int)ceil((ya + 8.0 - starty) / dx);
+    ix0 = max(ix0, 0); iy0 = max(iy0, 0); ix1 = min(ix1, n - 1); iy1 = min(iy1, n - 1);
+    const double ox = startx - xa, oy = starty - ya;   // pixel px sits at ox + px dx from the atom
+    T gx = 0, gy = 0;
+    for (int py = iy0 + (int)threadIdx.y; py <= iy1; py += 8) {
+        const T ry = (T)(oy + py * dx);
+        const double *grow = gV + (size_t)py * n;
+        for (int px = ix0 + (int)threadIdx.x; px <= ix1; px += 32) {
+            const T rx = (T)(ox + px * dx);
+            const T rho2 = rx * rx + ry * ry;
+            if (rho2 > r_min2 && rho2 <= (T)64) {
+                const T rho = fsqrt(rho2);
+                const T f = (T)grow[px] * dpot_drho<T>(form, prm, i_lim, Z, rho) / rho;
+                gx -= f * rx;   // d rho / d x_a = -rx / rho
+                gy -= f * ry;
+            }
+        }
+    }
+    double sx = (double)gx, sy = (double)gy;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_down_sync(0xffffffffu, sx, o);
+        sy += __shfl_down_sync(0xffffffffu, sy, o);
+    }
+    const int warp = (threadIdx.y * 32 + threadIdx.x) >> 5;
+    if (threadIdx.x == 0) { red[0][warp] = sx; red[1][warp] = sy; }
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        double tx = 0, ty = 0;
+        for (int i = 0; i < 8; i++) { tx += red[0][i]; ty += red[1][i]; }
+        gxy[2 * (size_t)a] = tx;
+        gxy[2 * (size_t)a + 1] = ty;
+    }
+}
+
+template <class T>
+void atom_grad(cudaStream_t s, int a0, int count, const double *ax, const double *ay, const int *aZ, const double *gV,
+               int n, double startx, double starty, double dx, int form, const T *prm, int i_lim, double *gxy) {
+    if (count <= 0) return;
+    k_atom_grad<T><<<count, dim3(32, 8), 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, form, prm, i_lim, gxy);
+    MS_CUDA(cudaGetLastError());
+}
+template void atom_grad<float>(cudaStream_t, int, int, const double *, const double *, const int *, const double *, int,
+                               double, double, double, int, const float *, int, double *);
+template void atom_grad<double>(cudaStream_t, int, int, const double *, const double *, const int *, const double *, int,
+                                double, double, double, int, const double *, int, double *);
+
+}  // namespace ms

@@ -50,9 +50,9 @@ inline dim3 col_grid(int batch) { return dim3(N / CC::COLS, batch); }
 inline dim3 col_block() { return dim3(CC::COLS, Plan<N>::NT); }
 
 void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a, int xa, int xb,
-              int load_all) {
+              int load_all, const int *tsel, size_t tstride) {
     ensure_attrs();
-    k_row_step<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all);
+    k_row_step<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all, tsel, tstride);
     MS_CUDA(cudaGetLastError());
 }
 void row_fft(cudaStream_t s, const cplx<R> *in, cplx<R> *out, int batch, const cplx<R> *tw, R scale, int sign) {
@@ -88,9 +88,9 @@ void col_bandlimit(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, 
     MS_CUDA(cudaGetLastError());
 }
 void col_probe(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, const double2 *chi, const double *kx,
-               const double *ky, const double2 *pos, R scale) {
+               const double *ky, const double2 *pos, R scale, const double *dfac, double wavelength) {
     ensure_attrs();
-    k_col_probe<R, N><<<col_grid(batch), col_block(), CC::smem(), s>>>(wave, tw, chi, kx, ky, pos, scale);
+    k_col_probe<R, N><<<col_grid(batch), col_block(), CC::smem(), s>>>(wave, tw, chi, kx, ky, pos, scale, dfac, wavelength);
     MS_CUDA(cudaGetLastError());
 }
 void row_step_save(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a,

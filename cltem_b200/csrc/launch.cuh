@@ -10,8 +10,10 @@ template <class R>
 struct PassOps {
     int n = 0;
     int col_blocks = 0;   // blocks per wave of a column pass (number of detector partials per wave)
-    // row_step(..., xa, xb, load_all): active columns x < xa or x >= xb (see k_row_step)
-    void (*row_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R, int, int, int) = nullptr;
+    // row_step(..., xa, xb, load_all, tsel, tstride): active columns x < xa or x >= xb; tsel (or nullptr) the
+    // transmission set of each wave, sets tstride elements apart (see k_row_step)
+    void (*row_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R, int, int, int, const int *,
+                     size_t) = nullptr;
     void (*row_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
     // col_step(..., mode, tiles_lo, tiles_hi): the leading tiles_lo and trailing tiles_hi column tiles
     void (*col_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, PropTables<R>, R, R, DetArgs, cplx<R> *, int, int,
@@ -19,8 +21,9 @@ struct PassOps {
     int cols_per_tile = 0;
     void (*col_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
     void (*col_bandlimit)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const double *, const double *, double, R) = nullptr;
+    // col_probe(..., pos, scale, dfac, wavelength): dfac (or nullptr) pi * defocus change / wavelength per wave
     void (*col_probe)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const double2 *, const double *, const double *,
-                      const double2 *, R) = nullptr;
+                      const double2 *, R, const double *, double) = nullptr;
     // differentiable CTEM (adjoint.cuh)
     void (*row_step_save)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R, cplx<R> *) = nullptr;
     void (*row_adjoint)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R, const cplx<R> *,

@@ -70,7 +70,7 @@ __device__ __forceinline__ void load_twiddles(cplx<R> *tw, const cplx<R> *__rest
 template <class R, int N>
 __global__ void __launch_bounds__(RowCfg<N, R>::THREADS)
 k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const cplx<R> *__restrict__ twg, R a,
-           int xa, int xb, int load_all) {
+           int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride) {
     using P = Plan<N>;
     constexpr int ROWS = RowCfg<N, R>::ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -80,7 +80,8 @@ k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const 
     load_twiddles<R, N>(tw, twg, t + threadIdx.y * P::NT, P::NT * ROWS);
     const int y = blockIdx.x * ROWS + threadIdx.y;
     cplx<R> *row = wave + (size_t)blockIdx.y * N * N + (size_t)y * N;
-    const cplx<R> *trow = trans + (size_t)y * N;
+    // tsel (optional): transmission set of each wave; set k of this slice starts k * tstride after trans
+    const cplx<R> *trow = trans + (tsel ? (size_t)tsel[blockIdx.y] * tstride : (size_t)0) + (size_t)y * N;
     cplx<R> v[P::E];
 #pragma unroll
     for (int m = 0; m < P::E; m++) {
@@ -283,7 +284,8 @@ k_col_bandlimit(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, con
 template <class R, int N>
 __global__ void __launch_bounds__(ColCfg<N, R>::THREADS)
 k_col_probe(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, const double2 *__restrict__ chi,
-            const double *__restrict__ kx, const double *__restrict__ ky, const double2 *__restrict__ pos, R scale) {
+            const double *__restrict__ kx, const double *__restrict__ ky, const double2 *__restrict__ pos, R scale,
+            const double *__restrict__ dfac, double wl) {
     using P = Plan<N>;
     constexpr int COLS = ColCfg<N, R>::COLS;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -293,6 +295,9 @@ k_col_probe(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, const d
     load_twiddles<R, N>(tw, twg, c + t * COLS, COLS * P::NT);
     const int x = blockIdx.x * COLS + c;
     const double2 pp = pos[blockIdx.y];
+    // dfac (optional): pi * defocus change / wavelength of each wave; the aberration phase gains
+    // 2 pi / lambda * dC10 |w|^2 / 2 = dfac * |w|^2 with w = lambda k (the C10 term of init_probe_wave_d.cl:83-101)
+    const double df = dfac ? dfac[blockIdx.y] : 0.0;
     const double kxx = kx[x];
     cplx<R> v[P::E];
 #pragma unroll
@@ -302,6 +307,10 @@ k_col_probe(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, const d
         if (ch.y != 0.0) {
             double posTerm = 2.0 * M_PI * (kxx * pp.x + ky[y] * pp.y);
             double arg = -posTerm - ch.x;
+            if (dfac) {
+                const double wx = wl * kxx, wy = wl * ky[y];
+                arg -= df * (wx * wx + wy * wy);
+            }
             if constexpr (sizeof(R) == 8) {
                 v[m] = mk<R>((R)cos(arg), (R)sin(arg));
             } else {

@@ -80,6 +80,7 @@ def load_library(path=None):
         "mslice_ctem_loss_grad": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, C.c_int],
         "mslice_ctem_loss": [C.c_void_p, _dp, _dp],
         "mslice_profile_read": [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_ulonglong), _dp, C.c_int],
+        "mslice_incoherence_draws": [C.POINTER(abi.Config), C.c_int, _ip, C.c_size_t, _dp, _ip, C.c_int, C.c_int, _dp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -122,6 +123,19 @@ def geometry(cfg: abi.Config) -> abi.Geometry:
     g = abi.Geometry()
     _check(L.mslice_geometry_compute(C.byref(cfg), C.byref(g)))
     return g
+
+
+def incoherence_draws(cfg: abi.Config, pass_: int, pixels, n_slices: int, n_builds: int):
+    """The random draws of one pass (host only): defocus change per pixel (Å), transmission set per pixel and
+    slice, and the source-size frame shift (Å) of each transmission build."""
+    L = load_library()
+    pixels = np.ascontiguousarray(pixels, dtype=np.int32)
+    df = np.zeros(len(pixels))
+    sets = np.zeros((len(pixels), n_slices), np.int32)
+    shift = np.zeros((n_builds, 2))
+    _check(L.mslice_incoherence_draws(C.byref(cfg), int(pass_), _i(pixels), len(pixels), _d(df), _i(sets), int(n_slices),
+                                      int(n_builds), _d(shift)))
+    return df, sets, shift
 
 
 class Context:

@@ -115,6 +115,23 @@ typedef struct mslice_config {
     int intermediate_slices;     /* output every n slices (0 = only the exit) */
     int ctem_image;              /* CTEM: also form the objective-lens image */
     int probe_batch;             /* STEM probes propagated together (0 = engine default) */
+
+    /* ---- incoherence (IncoherentEffects, src/simulation/incoherence/; all off when zero) ---- */
+    int iterations;              /* passes of a staged run ("incoherence/iterations"); 0: one pass per staged
+                                    configuration, pass i using configuration i */
+    int mixed_static;            /* mixed static potentials: n > 1 transmission sets built from the first n staged
+                                    configurations; every probe takes a random set at every slice
+                                    (simulationgeneral.cpp:42-54,576-613,731-742) */
+    int stem_moving_frame;       /* STEM without the static area ("stem/static area/enabled" false): each job
+                                    simulates a window of +-stem_padding around its first pixel
+                                    (SimulationManager::currentAreaBase, simulationmanager.cpp:485-505) */
+    int stem_job_pixels;         /* pixels per job in the moving frame ("concurrent pixels"), >= 1 */
+    int chromatic;               /* random defocus change per probe per pass (ChromaticAberration) */
+    double chromatic_cc;         /* Cc (mm) */
+    double chromatic_hwhm_neg, chromatic_hwhm_pos;   /* energy spread half widths (eV) */
+    int source_size;             /* random shift of the transmission frame per build (ProbeSourceSize) */
+    double source_fwhm;          /* Å */
+    unsigned long long seed;     /* seed of every random draw (sets, defocus changes, frame shifts) */
 } mslice_config;
 
 /* Derived geometry (what SimulationManager / SimulationCell compute from a config). */
@@ -242,6 +259,16 @@ int mslice_staged_result(mslice_sim *sim, double *out, size_t cap);
 /* One call from host buffers to host result: stage + run + result (the end-to-end API). */
 int mslice_stem_simulate(mslice_sim *sim, int n_configs, const size_t *counts, const int *Z,
                          const double *x, const double *y, const double *z, double *out, size_t cap);
+
+/* The random draws a run makes, host only (no device needed). The reference draws from clock-seeded
+ * std::mt19937_64 engines; these are pure functions of (cfg.seed, pass, pixel, slice), so runs repeat
+ * exactly. For pass `pass` and scan pixels[i]: defocus[i] = the chromatic defocus change in Å (0 when
+ * chromatic is off), sets[i * n_slices + s] = the transmission set taken at slice s (0 unless
+ * mixed_static > 1); shift[2*b], shift[2*b+1] = the source-size frame shift in Å of transmission build
+ * b (builds are numbered per run: pass p in the static frame, p * n_jobs + j for job j in the moving
+ * frame; 0 for the mixed static sets). Any output pointer may be NULL; shift receives n_builds pairs. */
+int mslice_incoherence_draws(const mslice_config *cfg, int pass, const int *pixels, size_t n_pixels, double *defocus,
+                             int *sets, int n_slices, int n_builds, double *shift);
 
 /* ---- comparison paths and building blocks ---------------------------------------------------- */
 /* Plain per-probe STEM in the reference's unfused kernel order (simulationgeneral.cpp:736-768):

@@ -60,6 +60,8 @@ def lib():
         L.orc_k_stem_pixel.restype = C.c_double
         L.orc_k_stem_pixel.argtypes = [_dp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
         L.orc_k_ctem_image.argtypes = [C.POINTER(abi.Config), _dp, _dp, _dp, _dp]
+        L.orc_run_staged.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t), _ip, _dp, _dp, _dp, _dp]
+        L.orc_draws.argtypes = [C.POINTER(abi.Config), C.c_int, _ip, C.c_size_t, _dp, _ip, C.c_int, C.c_int, _dp]
         _lib = L
     return _lib
 
@@ -116,6 +118,16 @@ def ctem_image(cfg, recip):
     out = np.empty_like(flat)
     _chk(lib().orc_k_ctem_image(C.byref(cfg), _d(kx), _d(ky), _d(flat), _d(out)))
     return cplx(out).reshape(n, n)
+
+
+def draws(cfg, pass_, pixels, n_slices, n_builds):
+    """(defocus changes per pixel, sets [pixel, slice], frame shifts [build, 2]) of one incoherent pass."""
+    pixels = np.ascontiguousarray(pixels, dtype=np.int32)
+    df = np.zeros(len(pixels))
+    sets = np.zeros((len(pixels), n_slices), np.int32)
+    shift = np.zeros((n_builds, 2))
+    _chk(lib().orc_draws(C.byref(cfg), pass_, _i(pixels), len(pixels), _d(df), _i(sets), n_slices, n_builds, _d(shift)))
+    return df, sets, shift
 
 
 def set_threads(n):
@@ -187,6 +199,23 @@ class OracleSim:
         out = np.zeros(g.n_outputs * self.cfg.n_detectors * len(pixels))
         _chk(lib().orc_stem_run(self.h, _i(pixels), len(pixels), _d(out)))
         return out.reshape(g.n_outputs, self.cfg.n_detectors, len(pixels))
+
+    def run_staged(self, configs):
+        """Average over the passes of a staged run (STEM [o, d, pixel] or CBED [o, ky, kx]) with the config's
+        incoherence options: mixed static sets, chromatic defocus, source-size shifts, moving frame."""
+        from cltem_b200.structure import concat_configs
+        cnt, Z, x, y, z = concat_configs(configs)
+        cnt = np.ascontiguousarray(cnt, dtype=np.uint64)
+        g = self.geo
+        if self.cfg.mode == abi.MODE_STEM:
+            npx = self.cfg.stem_pixels_x * self.cfg.stem_pixels_y
+            shape = (g.n_outputs, self.cfg.n_detectors, npx)
+        else:
+            shape = (g.n_outputs, self.res, self.res)
+        out = np.zeros(int(np.prod(shape)))
+        _chk(lib().orc_run_staged(self.h, len(configs), cnt.ctypes.data_as(C.POINTER(C.c_size_t)), _i(Z), _d(x), _d(y),
+                                  _d(z), _d(out)))
+        return out.reshape(shape)
 
     def cbed(self):
         out = np.zeros(self.geo.n_outputs * self.N)

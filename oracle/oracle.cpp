@@ -87,6 +87,77 @@ static void full_area(const mslice_config &c, Lim &x, Lim &y) {
     y.lo += -c.padding_xy; y.hi += c.padding_xy;
 }
 
+// SimulationManager::currentAreaBase for STEM without the static area (simulationmanager.cpp:485-505):
+// StemArea::getPixelSimArea (commonstructs.h:379-396) with the real scale of the static frame, then the
+// SimulationCell padding (paddedSimLimitsX/Y, simulationmanager.cpp:434-440)
+static void moving_frame(const mslice_config &c, int pixel, Lim &x, Lim &y) {
+    Lim ax, ay;
+    corrected(c.stem_area[0], c.stem_area[1], c.stem_area[2], c.stem_area[3], c.stem_padding, ax, ay);
+    double pad_range = c.padding_xy - (-c.padding_xy);
+    double area_range = ax.hi - ax.lo;
+    double rs = (pad_range + area_range) / static_cast<double>(c.resolution);
+    unsigned int x_px = (unsigned int)pixel % (unsigned int)c.stem_pixels_x;
+    unsigned int y_px = (unsigned int)std::floor(pixel / c.stem_pixels_x);
+    double pos_x = ((c.stem_area[1] - c.stem_area[0]) / c.stem_pixels_x) * x_px;   // StemArea::getScaleX
+    double pos_y = ((c.stem_area[3] - c.stem_area[2]) / c.stem_pixels_y) * y_px;
+    double real_pos_x = rs * std::floor(pos_x / rs);
+    double real_pos_y = rs * std::floor(pos_y / rs);
+    double xPos = c.stem_area[0] + real_pos_x;
+    double yPos = c.stem_area[2] + real_pos_y;
+    corrected(xPos, xPos, yPos, yPos, c.stem_padding, x, y);
+    x.lo += -c.padding_xy; x.hi += c.padding_xy;
+    y.lo += -c.padding_xy; y.hi += c.padding_xy;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Random draws of the incoherence effects, restated from their definition: every draw is a function of
+// (seed, kind, pass, index): the SplitMix64 finaliser hashes the coordinates (Steele, Lea, Flood, OOPSLA
+// 2014), uniforms take the top 53 bits, normals use the Box-Muller cosine branch. They stand in for the
+// reference's clock-seeded std::mt19937_64 draws (chromaticaberration.cpp:39-56, probesourcesize.cpp:29-31,
+// simulationgeneral.cpp:740-742), which cannot be repeated.
+// ------------------------------------------------------------------------------------------------
+static uint64_t splitmix(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static uint64_t draw_key(uint64_t seed, uint64_t kind, uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t h = splitmix(seed ^ (kind << 56));
+    h = splitmix(h ^ a);
+    h = splitmix(h ^ b);
+    return splitmix(h ^ c);
+}
+static double draw_uniform(uint64_t h) { return (double)(h >> 11) * (1.0 / 9007199254740992.0); }
+static double draw_normal(uint64_t h1, uint64_t h2) {
+    double u1 = 1.0 - draw_uniform(h1), u2 = draw_uniform(h2);
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * M_PI * u2);
+}
+static int draw_set(uint64_t seed, int pass, int pixel, int slice, int n_sets) {
+    return (int)(draw_key(seed, 1, (uint64_t)pass, (uint64_t)pixel, (uint64_t)slice) % (uint64_t)n_sets);
+}
+// ChromaticAberration::getFocusChange with generateDist (chromaticaberration.cpp:39-56, 88-95); the
+// sigmas from the half widths as in setHalfWidthHalfMax* (:104-112)
+static double draw_defocus(const mslice_config &c, int pass, int pixel) {
+    double sig_pos = std::fabs(2.0 * c.chromatic_hwhm_pos / (2.0 * std::sqrt(2.0 * std::log(2.0))));
+    double sig_neg = std::fabs(2.0 * c.chromatic_hwhm_neg / (2.0 * std::sqrt(2.0 * std::log(2.0))));
+    double ratio = sig_neg / sig_pos;
+    ratio = ratio / (ratio + 1.0);
+    double selector = draw_uniform(draw_key(c.seed, 2, (uint64_t)pass, (uint64_t)pixel, 0));
+    double dist_1 = std::fabs(draw_normal(draw_key(c.seed, 2, (uint64_t)pass, (uint64_t)pixel, 1),
+                                          draw_key(c.seed, 2, (uint64_t)pass, (uint64_t)pixel, 2)));
+    double dist = selector >= ratio ? dist_1 * sig_pos : -1.0 * (dist_1 * sig_neg);
+    return 10000 * c.chromatic_cc * dist / c.voltage;
+}
+// two ProbeSourceSize::getOffset draws (simulationcbed.cpp:103-113); sigma from the FWHM (:18-20)
+static void draw_shift(const mslice_config &c, int build, double &dx, double &dy) {
+    dx = dy = 0;
+    if (!c.source_size || c.mode == MSLICE_MODE_CTEM) return;
+    double sd = c.source_fwhm / (2.0 * std::sqrt(2.0 * std::log(2.0)));
+    dx = draw_normal(draw_key(c.seed, 3, (uint64_t)build, 0, 0), draw_key(c.seed, 3, (uint64_t)build, 0, 1)) * sd;
+    dy = draw_normal(draw_key(c.seed, 3, (uint64_t)build, 1, 0), draw_key(c.seed, 3, (uint64_t)build, 1, 1)) * sd;
+}
+
 static bool resolution_valid(const mslice_config &c) {
     int r = c.resolution;
     if (c.allow_any_resolution) {
@@ -116,6 +187,11 @@ static void compute_geometry(const mslice_config &c, Geo &G) {
     // parallel STEM / CTEM / CBED: currentAreaBase == fullAreaBase (simulationmanager.cpp:485-505)
     g.sim_x[0] = fx.lo; g.sim_x[1] = fx.hi; g.sim_y[0] = fy.lo; g.sim_y[1] = fy.hi;
     g.full_x[0] = fx.lo; g.full_x[1] = fx.hi; g.full_y[0] = fy.lo; g.full_y[1] = fy.hi;
+    if (c.mode == MSLICE_MODE_STEM && c.stem_moving_frame) {   // realScale etc. use paddedSimLimitsX/Y(0)
+        Lim wx, wy;
+        moving_frame(c, 0, wx, wy);
+        g.sim_x[0] = wx.lo; g.sim_x[1] = wx.hi; g.sim_y[0] = wy.lo; g.sim_y[1] = wy.hi;
+    }
 
     // SimulationCell::roundPaddingZ (simulationcell.cpp:43-61)
     double dz = c.slice_thickness, off = c.slice_offset;
@@ -842,6 +918,8 @@ struct Sim {
     Atoms<T> atoms;
     std::vector<std::vector<std::complex<T>>> trans;   // band-limited T per slice
     std::vector<std::vector<std::complex<T>>> trans_raw;
+    std::vector<std::vector<std::vector<std::complex<T>>>> sets;   // mixed static potentials: T per set per slice
+    double frame_x = 0, frame_y = 0;   // start of the frame the next transmission build uses
     std::vector<std::complex<T>> prop;
 
     Sim(const mslice_config &cfg, int form_, int icount, const double *p, size_t np) : c(cfg), form(form_), i_count(icount) {
@@ -856,6 +934,10 @@ struct Sim {
         // propagator set up (simulationgeneral.cpp:623-637)
         propagator<T>(prop.data(), kx.data(), ky.data(), res, res, (T)g.dz, (T)g.wavenumber, (T)g.wavevector[0],
                       (T)g.wavevector[1], (T)g.wavevector[2], (T)(g.k_max * c.inverse_limit_factor));
+        double dx, dy;
+        draw_shift(c, 0, dx, dy);
+        frame_x = g.sim_x[0] + dx;
+        frame_y = g.sim_y[0] + dy;
     }
 
     PotArgs pot_args(int slice) const {
@@ -868,7 +950,7 @@ struct Sim {
         a.max_x = g.full_x[1]; a.min_x = g.full_x[0]; a.max_y = g.full_y[1]; a.min_y = g.full_y[0];
         a.block_load_x = g.load_blocks_x; a.block_load_y = g.load_blocks_y; a.slice_load_z = g.load_blocks_z;
         a.sigma = g.sigma;
-        a.startx = g.sim_x[0]; a.starty = g.sim_y[0];   // + source-size perturbation (0, not modelled)
+        a.startx = frame_x; a.starty = frame_y;   // paddedSimLimits(pixel)[0] + source-size perturbation
         a.beam_theta = c.beam_tilt; a.beam_phi = c.beam_azimuth;
         a.current_z = g.z_lims[0] + (g.n_slices - slice) * g.dz;   // simulationgeneral.cpp:590
         a.shift_x = (g.wavevector[0] / g.wavevector[2]) * g.dz / c.full3d_integrals;   // :562-563
@@ -900,10 +982,14 @@ struct Sim {
 
     // probe in reciprocal space at an absolute position (SimulationCbed::initialiseProbeWave, simulationcbed.cpp:35-91)
     void probe_k(double posx, double posy, std::complex<T> *out) const {
+        probe_k(posx, posy, out, G.g.sim_x[0], G.g.sim_y[0], 0.0);
+    }
+    // ... relative to the frame starting at (x0, y0), with C10 + delta_focus (simulationcbed.cpp:60-72)
+    void probe_k(double posx, double posy, std::complex<T> *out, double x0, double y0, double delta_focus) const {
         const mslice_geometry &g = G.g;
-        posx = posx - g.sim_x[0];
-        posy = posy - g.sim_y[0];
-        Aberr<T> A = aberrations<T>(c, c.C10);
+        posx = posx - x0;
+        posy = posy - y0;
+        Aberr<T> A = aberrations<T>(c, c.C10 + delta_focus);
         init_probe<T>(out, res, res, kx.data(), ky.data(), (T)posx, (T)posy, (T)g.wavelength, A, (T)c.cond_ap, (T)c.cond_ap_smooth);
     }
 
@@ -914,6 +1000,147 @@ struct Sim {
         fft2<T>(res, res, recip_w.data(), tmp.data(), -1);
         for (size_t i = 0; i < N; i++) recip_w[i] = cMult(tmp[i], prop[i]);
         fft2<T>(res, res, recip_w.data(), real.data(), +1);
+    }
+
+    // the same step with the transmission of slice s taken from Tset (a mixed static set or a job window)
+    void step_with(const std::vector<std::vector<std::complex<T>>> &Tset, int s, std::vector<std::complex<T>> &real,
+                   std::vector<std::complex<T>> &recip_w, std::vector<std::complex<T>> &tmp) const {
+        const auto &Ts = Tset[s];
+        for (size_t i = 0; i < N; i++) recip_w[i] = cMult(Ts[i], real[i]);
+        fft2<T>(res, res, recip_w.data(), tmp.data(), -1);
+        for (size_t i = 0; i < N; i++) recip_w[i] = cMult(tmp[i], prop[i]);
+        fft2<T>(res, res, recip_w.data(), real.data(), +1);
+    }
+
+    // transmission of slice s for probe `pixel` in pass `pass`: a random mixed static set, or `fixed`
+    const std::vector<std::vector<std::complex<T>>> &slice_set(int pass, int pixel, int s,
+                                                               const std::vector<std::vector<std::complex<T>>> &fixed) const {
+        if (c.mixed_static > 1) return sets[draw_set(c.seed, pass, pixel, s, c.mixed_static)];
+        return fixed;
+    }
+
+    // one STEM probe of an incoherent pass: probe of scan pixel p relative to the frame (x0, y0), with the
+    // chromatic defocus change of (pass, p); detector values out[o * n_det + d]
+    void stem_probe(int pass, int p, double x0, double y0, const std::vector<std::vector<std::complex<T>>> &fixed,
+                    double *out) const {
+        const mslice_geometry &g = G.g;
+        int S = g.n_slices, n_out = g.n_outputs, n_det = c.n_detectors;
+        double step_x = (c.stem_area[1] - c.stem_area[0]) / c.stem_pixels_x;
+        double step_y = (c.stem_area[3] - c.stem_area[2]) / c.stem_pixels_y;
+        int x_i = p % c.stem_pixels_x, y_i = (int)std::floor(p / c.stem_pixels_x);
+        double x_pos = c.stem_area[0] + x_i * step_x, y_pos = c.stem_area[2] + y_i * step_y;
+        double df = c.chromatic ? draw_defocus(c, pass, p) : 0.0;
+        std::vector<std::complex<T>> real(N), recip_w(N), tmp(N), sh(N);
+        probe_k(x_pos, y_pos, recip_w.data(), x0, y0, df);
+        fft2<T>(res, res, recip_w.data(), real.data(), +1);
+        int oc = 0;
+        for (int s = 0; s < S; s++) {
+            step_with(slice_set(pass, p, s, fixed), s, real, recip_w, tmp);
+            if (is_output(s)) {
+                for (int d = 0; d < n_det; d++) out[(size_t)oc * n_det + d] = stem_pixel<T>(recip_w.data(), res, res, g.angle_scale, c.detectors[d], sh);
+                oc++;
+            }
+        }
+        if (oc < n_out)
+            for (int d = 0; d < n_det; d++) out[(size_t)oc * n_det + d] = stem_pixel<T>(recip_w.data(), res, res, g.angle_scale, c.detectors[d], sh);
+    }
+
+    // one pass over scan pixels[0..n) (SimulationStem::simulate per job); adds to acc[(o*n_det + d)*n + i].
+    // Static frame: the built transmission (or the mixed static sets). Moving frame: jobs of
+    // stem_job_pixels consecutive pixels, each with its own window built here.
+    void stem_pass(int pass, const int *pixels, size_t n, double *acc) {
+        const mslice_geometry &g = G.g;
+        int n_out = g.n_outputs, n_det = c.n_detectors;
+        auto run = [&](size_t i0, size_t i1, double x0, double y0) {
+            std::vector<double> res_((i1 - i0) * n_out * n_det);
+#pragma omp parallel for schedule(dynamic)
+            for (long i = (long)i0; i < (long)i1; i++)
+                stem_probe(pass, pixels[i], x0, y0, trans, res_.data() + (size_t)(i - i0) * n_out * n_det);
+            for (size_t i = i0; i < i1; i++)
+                for (int o = 0; o < n_out; o++)
+                    for (int d = 0; d < n_det; d++)
+                        acc[((size_t)o * n_det + d) * n + i] += res_[((i - i0) * n_out + o) * n_det + d];
+        };
+        if (!c.stem_moving_frame) { run(0, n, g.sim_x[0], g.sim_y[0]); return; }
+        int P = std::max(1, c.stem_job_pixels);
+        size_t n_jobs = (n + P - 1) / P;
+        for (size_t j = 0; j < n_jobs; j++) {
+            Lim wx, wy;
+            moving_frame(c, pixels[j * P], wx, wy);
+            double dx, dy;
+            draw_shift(c, (int)((size_t)pass * n_jobs + j), dx, dy);
+            frame_x = wx.lo + dx;
+            frame_y = wy.lo + dy;
+            build_transmission();
+            run(j * P, std::min(n, (j + 1) * P), wx.lo, wy.lo);
+        }
+    }
+
+    // one CBED pass (one job): probe with the chromatic defocus change of (pass, 0); adds |psi(k)|^2
+    void cbed_pass(int pass, double *acc) const {
+        const mslice_geometry &g = G.g;
+        int S = g.n_slices;
+        double df = c.chromatic ? draw_defocus(c, pass, 0) : 0.0;
+        std::vector<std::complex<T>> real(N), recip_w(N), tmp(N);
+        std::vector<double> d(N);
+        probe_k(c.cbed_x, c.cbed_y, recip_w.data(), g.sim_x[0], g.sim_y[0], df);
+        fft2<T>(res, res, recip_w.data(), real.data(), +1);
+        int oc = 0;
+        auto out = [&]() {
+            diffraction(recip_w, d.data());
+            for (size_t i = 0; i < N; i++) acc[(size_t)oc * N + i] += d[i];
+            oc++;
+        };
+        for (int s = 0; s < S; s++) {
+            step_with(slice_set(pass, 0, s, trans), s, real, recip_w, tmp);
+            if (is_output(s)) out();
+        }
+        if (oc < g.n_outputs) out();
+    }
+
+    // staged run over configurations (the engine's mslice_*_run_staged): one pass per configuration, or
+    // cfg.iterations passes cycling through them; mixed static sets from the first mixed_static
+    // configurations, built once with the frame shift of build 0. Returns the average over passes.
+    void staged(int nc, const size_t *counts, const int *Z, const double *x, const double *y, const double *z, double *out) {
+        const mslice_geometry &g = G.g;
+        int K = c.mixed_static > 1 ? c.mixed_static : 1;
+        if (K > 1 && nc < K) throw std::invalid_argument("mixed static potentials need mixed_static configurations");
+        int passes = K > 1 ? std::max(1, c.iterations) : (c.iterations > 0 ? c.iterations : nc);
+        std::vector<size_t> off(nc + 1, 0);
+        for (int i = 0; i < nc; i++) off[i + 1] = off[i] + counts[i];
+        size_t n_pix = (size_t)c.stem_pixels_x * c.stem_pixels_y;
+        size_t tot = c.mode == MSLICE_MODE_STEM ? (size_t)g.n_outputs * c.n_detectors * n_pix : (size_t)g.n_outputs * N;
+        std::vector<double> acc(tot, 0.0);
+        std::vector<int> pix(n_pix);
+        for (size_t i = 0; i < n_pix; i++) pix[i] = (int)i;
+        if (K > 1) {
+            double dx, dy;
+            draw_shift(c, 0, dx, dy);
+            sets.clear();
+            for (int k = 0; k < K; k++) {
+                set_atoms(counts[k], Z + off[k], x + off[k], y + off[k], z + off[k]);
+                frame_x = g.sim_x[0] + dx;
+                frame_y = g.sim_y[0] + dy;
+                build_transmission();
+                sets.push_back(trans);
+            }
+        }
+        for (int it = 0; it < passes; it++) {
+            if (K == 1) {
+                int k = it % nc;
+                set_atoms(counts[k], Z + off[k], x + off[k], y + off[k], z + off[k]);
+                if (!(c.mode == MSLICE_MODE_STEM && c.stem_moving_frame)) {
+                    double dx, dy;
+                    draw_shift(c, it, dx, dy);
+                    frame_x = g.sim_x[0] + dx;
+                    frame_y = g.sim_y[0] + dy;
+                    build_transmission();
+                }
+            }
+            if (c.mode == MSLICE_MODE_STEM) stem_pass(it, pix.data(), n_pix, acc.data());
+            else cbed_pass(it, acc.data());
+        }
+        for (size_t i = 0; i < tot; i++) out[i] = acc[i] / passes;   // Image::getWeightedSlice
     }
 
     bool is_output(int s) const {
@@ -1199,6 +1426,27 @@ int orc_k_ctem_image(const mslice_config *c, const double *kx, const double *ky,
         ctem_image<double>(a.data(), b.data(), n, n, kx, ky, wavelength(c->voltage), A, c->obj_ap, c->obj_ap_smooth,
                            c->alpha, c->delta);
         for (size_t i = 0; i < b.size(); i++) { out[2 * i] = b[i].real(); out[2 * i + 1] = b[i].imag(); }
+    });
+}
+
+// staged STEM / CBED run with the incoherence options of the config (see Sim::staged)
+int orc_run_staged(OrcSim *s, int nc, const size_t *counts, const int *Z, const double *x, const double *y, const double *z,
+                   double *out) {
+    return guard([&] { if (s->dp) s->sd->staged(nc, counts, Z, x, y, z, out); else s->sf->staged(nc, counts, Z, x, y, z, out); });
+}
+
+// the random draws of one pass (mirrors the engine's mslice_incoherence_draws)
+int orc_draws(const mslice_config *c, int pass, const int *pixels, size_t n, double *defocus, int *sets_out, int n_slices,
+              int n_builds, double *shift) {
+    return guard([&] {
+        for (size_t i = 0; i < n; i++) {
+            if (defocus) defocus[i] = c->chromatic ? draw_defocus(*c, pass, pixels[i]) : 0.0;
+            if (sets_out)
+                for (int s = 0; s < n_slices; s++)
+                    sets_out[i * n_slices + s] = c->mixed_static > 1 ? draw_set(c->seed, pass, pixels[i], s, c->mixed_static) : 0;
+        }
+        if (shift)
+            for (int b = 0; b < n_builds; b++) draw_shift(*c, b, shift[2 * b], shift[2 * b + 1]);
     });
 }
 
