@@ -39,8 +39,9 @@ METRIC = "STEM probe·slices/s at 512² FP32 vs plain FP64 GPU; adjoint/forward 
 UNIT = "probe·slices/s"
 WORKLOAD = "stem_adf_perovskite_10x10x20_512x512_64x64probes_40slices_phonon_u0.08"
 # ncu: dram__bytes_read.sum + dram__bytes_write.sum per wave per launch of the step kernels at 512^2 FP32
-# (profiles/row_col_step_512_b128_ncu.md); updated when the kernels change and are re-captured
-NCU_DRAM_BYTES_PER_WAVE = {"row_step": 481.5e6 / 128, "col_step": 478.1e6 / 128}
+# (profiles/step_kernels_512_fp32_ncu.md, one launch of 256 waves); updated when the kernels change and are
+# re-captured
+NCU_DRAM_BYTES_PER_WAVE = {"row_step": 857.7e6 / 256, "col_step": 684.7e6 / 256}
 
 
 def parse():
@@ -339,7 +340,7 @@ def main():
     peak, peak_src = peaks()
     achieved = dom[1] / (dom[2] / 1000.0) / 1e9
     # DRAM bytes per wave per launch from one ncu capture of this build's step kernels
-    # (profiles/row_col_step_512_b128_ncu.md: dram__bytes_read.sum + dram__bytes_write.sum / 128 waves),
+    # (profiles/step_kernels_512_fp32_ncu.md: dram__bytes_read.sum + dram__bytes_write.sum / 256 waves),
     # scaled to this run's launches
     per_wave = NCU_DRAM_BYTES_PER_WAVE.get(dom[0])
     traffic = per_wave * (npx * S * args.steps) / max(dom[3], 1) if per_wave else None
