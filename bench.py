@@ -250,6 +250,108 @@ def adjoint_leg(ctx, ext, warmup):
                     "transmission build of the 32 slices"}
 
 
+def full3d_evaluations(sim, n_atoms, S, N):
+    """Atom-sample evaluations of one full-3D potential build (the unit the CBED full-3D throughput is quoted
+    in): for every binned atom, the pixels within 8 Å in xy times the (slice, sub-slice sample) pairs of the
+    slices that load the atom's z bin (k +- load_blocks_z) whose sample lies at most 3 Å above it (the one-sided
+    test of transmission_potentials_full_3d_f.cl:263), counted on the host from the binned atoms (no beam tilt,
+    so the xy test does not depend on the sample)."""
+    g = sim.geo
+    a = sim.sorted_atoms(n_atoms)
+    nb = g.blocks_x * g.blocks_y
+    kz_all = (np.searchsorted(a["block_start"], np.arange(len(a["x"])), side="right") - 1) // nb
+    dx, x0, y0 = g.real_scale, g.sim_x[0], g.sim_y[0]
+    rows = np.arange(-int(8 / dx) - 2, int(8 / dx) + 3)
+    I = sim.cfg.full3d_integrals
+    total = 0.0
+    for c0 in range(0, len(kz_all), 4096):
+        ax, ay, az, kz = a["x"][c0:c0 + 4096], a["y"][c0:c0 + 4096], a["z"][c0:c0 + 4096], kz_all[c0:c0 + 4096]
+        # pixels of the disk |r - r_a| <= 8 inside the grid, row by row
+        iy = np.floor((ay - y0) / dx).astype(np.int64)[:, None] + rows[None, :]
+        ry = (y0 + iy * dx) - ay[:, None]
+        h2 = 64.0 - ry * ry
+        ok = (h2 >= 0) & (iy >= 0) & (iy < N)
+        h = np.sqrt(np.where(ok, h2, 0.0))
+        lo = np.maximum(np.ceil((ax[:, None] - h - x0) / dx), 0)
+        hi = np.minimum(np.floor((ax[:, None] + h - x0) / dx), N - 1)
+        px = np.where(ok & (hi >= lo), hi - lo + 1, 0).sum(axis=1)
+        pairs = np.zeros(len(kz))
+        for off in range(-g.load_blocks_z, g.load_blocks_z + 1):
+            k = kz + off
+            valid = (k >= 0) & (k < S)
+            cz = g.z_lims[0] + (S - k) * g.dz
+            for hh in range(I + 1):
+                pairs += valid & ((cz - hh * g.dz / I) - az <= 3.0)
+        total += float((px * pairs).sum())
+    return total
+
+
+def cbed3d_leg(ctx, ext):
+    """CBED through the full-3D Lobato potential (FCC Au 20x20x60 cells, 96,000 atoms, 1024^2, 120 slices,
+    4 sub-slices, FP32): one phonon configuration (u_rms 0.09 Å) of the 50; the potential build is the bound."""
+    import torch
+    from cltem_b200 import config
+    from cltem_b200.engine import Simulation
+    from cltem_b200.params import load_default
+    from cltem_b200.structure import phonon_configs
+    s, st = config.fcc_cbed()
+    ctx.load_params(load_default("lobato"))
+    sim = Simulation(ctx, s.cfg)
+    S, N = sim.geo.n_slices, s.cfg.resolution
+    confs = phonon_configs(st, 2, 0.09, seed=90)
+    sim.stage(confs[:1])
+    sim.run_staged()                        # warm-up (sort, 120-slice build, 120 steps)
+    sim.stage(confs[1:])
+    sim.profile(True)
+    sim.profile_read(reset=True)
+    torch.cuda.synchronize()
+    sim.run_staged()
+    prof = sim.profile_read()
+    sim.profile(False)
+    t = sim.last_timing()
+    sim.set_atoms(confs[1])
+    ev = full3d_evaluations(sim, len(st), S, N)
+    pot_ms = prof["potential"][0]
+    sim.close()
+    ctx.load_params(load_default("kirkland"))
+    return {"workload": "cbed_full3d_lobato_fcc_20x20x60_1024x1024_120slices_4subslices_fp32",
+            "atom_sample_evaluations": ev, "potential_ms": pot_ms,
+            "evaluations_per_s": ev / (pot_ms * 1e-3), "config_ms": t["total_ms"],
+            "build_ms": t["build_ms"], "propagate_ms": t["propagate_ms"],
+            "projected_50_configs_s": 50 * t["total_ms"] * 1e-3,
+            "note": "one configuration of the 50; evaluations counted on the host from the binned atoms"}
+
+
+def uneven_leg(ctx, n_cells=48, n_configs=4, seed=2024):
+    """Uneven batched STEM: 48 seeded perovskite / FCC cells (4-16 cells laterally, 10-80 slices, grids
+    256-1024, 80-300 kV, 16-32 mrad, 16x16 probes, 4 phonon configurations each), FP32, each grid with the
+    autotuned probe batch. Value: probe·slices of all cells over the device time of their staged runs."""
+    from cltem_b200 import config
+    from cltem_b200.engine import Simulation
+    from cltem_b200.structure import phonon_configs
+    rng = np.random.default_rng(seed)
+    total_ps, total_ms, setup_s, batches, grids = 0.0, 0.0, 0.0, {}, {}
+    for i in range(n_cells):
+        s, st = config.uneven_stem_cell(rng)
+        t0 = time.perf_counter()
+        sim = Simulation(ctx, s.cfg)
+        if s.cfg.resolution not in batches:
+            batches[s.cfg.resolution] = sim.tune_batch()[0]
+        else:
+            sim.tune_batch()   # cached for this grid
+        sim.stage(phonon_configs(st, n_configs, 0.08, seed=seed + i))
+        setup_s += time.perf_counter() - t0
+        sim.run_staged()
+        total_ms += sim.last_timing()["total_ms"]
+        S = sim.geo.n_slices
+        total_ps += 256 * S * n_configs
+        grids[s.cfg.resolution] = grids.get(s.cfg.resolution, 0) + 1
+        sim.close()
+    return {"workload": f"uneven_stem_{n_cells}cells_16x16probes_{n_configs}configs_fp32", "value": total_ps / (total_ms * 1e-3),
+            "unit": UNIT, "probe_slices": total_ps, "device_ms": total_ms, "host_setup_s": setup_s,
+            "cells_per_grid": grids, "autotuned_batch_per_grid": batches}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -274,6 +376,9 @@ def main():
     ctx = Context(local)
     ctx.load_params(load_default("kirkland"))
     sim = Simulation(ctx, s.cfg)
+    tuned = None
+    if not args.batch:   # the probe batch from the autotuner (untimed; cached per device, grid and precision)
+        tuned = sim.tune_batch()
     S = sim.geo.n_slices
     npx = s.cfg.stem_pixels_x * s.cfg.stem_pixels_y
     N = 512 * 512
@@ -387,9 +492,11 @@ def main():
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(out.numel() * 8),
                "steps": len(e2e_confs), "ms_per_step": ms_e2e / len(e2e_confs)}
 
-    adjoint = None
+    adjoint = cbed3d = uneven = None
     if rank == 0 and world == 1 and not args.no_baseline:
         adjoint = adjoint_leg(ctx, ext, args.warmup)
+        cbed3d = cbed3d_leg(ctx, ext)
+        uneven = uneven_leg(ctx)
 
     cpu = plain = None
     if rank == 0 and world == 1 and not args.no_baseline:
@@ -419,7 +526,7 @@ def main():
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": 512, "probes": npx, "slices": S,
-                       "phonon_configs_per_gpu": args.steps, "probe_batch": sim.cfg.probe_batch or "engine default",
+                       "phonon_configs_per_gpu": args.steps, "probe_batch": sim.cfg.probe_batch or (f"{tuned[0]} (autotuned: {tuned[1]:.0f} waves/s per slice step)" if tuned else "engine default"),
                        "precision": "complex64 waves and FFTs; FP64 phase arguments, offsets and Kahan accumulation",
                        "l2": "inputs larger than L2 (per configuration: 4096 waves x 2 MiB + 40 transmission slices x 2 MiB)",
                        "parallelism": f"dp{world} (phonon configurations sharded over GPUs)"},
@@ -428,6 +535,8 @@ def main():
             "plain_fp64_gpu": plain,
             "adjoint_forward_ratio": adjoint["ratio"] if adjoint else None,
             "adjoint": adjoint,
+            "cbed_full3d": cbed3d,
+            "uneven_stem": uneven,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,

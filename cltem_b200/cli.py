@@ -42,7 +42,9 @@ def _parse(argv):
     p.add_argument("-f", "--flags", default="", help="accepted for compatibility; has no effect")
     p.add_argument("-l", "--list", action="store_true", help="list the CUDA devices and exit")
     p.add_argument("-v", "--version", action="store_true")
-    p.add_argument("--seed", type=int, default=0, help="seed of the frozen-phonon draws")
+    p.add_argument("--seed", type=int, default=0, help="seed of the frozen-phonon and incoherence draws")
+    p.add_argument("--ccds", default=None, help="directory holding the CCD tables <name>.dat named by ctem/ccd/name "
+                                                "(default: the bundled K2 and Orius tables)")
     p.add_argument("--debug", action="store_true")
     p.add_argument("-s", "--size", default=None)
     p.add_argument("-z", "--zone", default=None)
@@ -93,7 +95,19 @@ def _phonon_u2(raw_json):
     return float(ph.get("default", {}).get("value", 0.0)), bool(ph.get("force default", True))
 
 
-def _run_share(dev, settings, params, configs, out, idx, errors, cfg=None, passes=None):
+def _load_ccd(name, ccds_dir):
+    """The CCD named by ctem/ccd/name: <ccds_dir>/<name>.dat (CCDParams loaded from the executable's ccds
+    folder, src/console/main.cpp:770-778), else the bundled tables (matched by file stem or by name)."""
+    from .params import load_ccds, read_ccd
+    if ccds_dir:
+        return read_ccd(os.path.join(ccds_dir, name + ".dat"))
+    for stem, c in load_ccds().items():
+        if name in (stem, c.name):
+            return c
+    raise RuntimeError(f"unknown CCD {name!r}: give --ccds <dir> holding {name}.dat")
+
+
+def _run_share(dev, settings, params, configs, out, idx, errors, cfg=None, passes=None, ccd=None):
     """Run a share on one device; store (sum of results, number of passes). Without `passes` the share is
     one pass per configuration; with it, `passes` incoherent passes over all the configurations (cfg
     carries the pass count and this device's seed)."""
@@ -111,6 +125,8 @@ def _run_share(dev, settings, params, configs, out, idx, errors, cfg=None, passe
             r = sim.staged_result() * weight
             out[idx] = ({"main": r}, weight)
         else:
+            if ccd is not None:
+                sim.set_ccd(ccd, settings.ccd_binning, settings.ccd_dose)
             acc = None
             for c in configs:
                 sim.set_atoms(c)
@@ -184,6 +200,9 @@ def main(argv=None):
     else:
         configs = [structure]
 
+    ccd = None
+    if settings.cfg.mode == abi.MODE_CTEM and settings.ccd_name not in ("", "Perfect"):
+        ccd = _load_ccd(settings.ccd_name, a.ccds)
     devs = _devices(a.device)
     results, errors, threads = [None] * len(devs), [], []
     t0 = time.time()
@@ -204,7 +223,9 @@ def main(argv=None):
         for i, (d, sh) in enumerate(zip(devs, shares)):
             if not sh:
                 continue
-            th = threading.Thread(target=_run_share, args=(d, settings, params, sh, results, i, errors))
+            cfg_i = copy.deepcopy(settings.cfg)   # own seed per device: dose noise draws differ between devices
+            cfg_i.seed = (a.seed + 0x9E3779B97F4A7C15 * i) % (1 << 64)
+            th = threading.Thread(target=_run_share, args=(d, settings, params, sh, results, i, errors, cfg_i, None, ccd))
             th.start()
             threads.append(th)
     for th in threads:

@@ -43,6 +43,9 @@ class SimulationSettings:
         self.phonon_enabled = False
         self.phonon_default_u2 = 0.0
         self.parallel_pixels = 1
+        self.ccd_name = ""          # "ctem/ccd/name" ("" or "Perfect": no dose simulation)
+        self.ccd_dose = 10000.0     # e- per Å^2 (SimulationManager default)
+        self.ccd_binning = 1
         self.mixed_static_count = 1
         self.mixed_static_enabled = False
         self.detectors = []
@@ -185,6 +188,10 @@ def read_config(path_or_dict) -> SimulationSettings:
     _try(j, lambda v: setattr(c, "source_fwhm", v), *pr, "source size", "FWHM", "val", conv=float)
     if c.mode != abi.MODE_STEM:
         c.stem_moving_frame = 0   # the static-area switch is read only by STEM
+    # CTEM CCD (jsonutils.cpp:176-184)
+    _try(j, lambda v: setattr(s, "ccd_name", v), "ctem", "ccd", "name", conv=str)
+    _try(j, lambda v: setattr(s, "ccd_dose", v), "ctem", "ccd", "dose", "val", conv=float)
+    _try(j, lambda v: setattr(s, "ccd_binning", v), "ctem", "ccd", "binning", conv=int)
     return s
 
 
@@ -301,5 +308,47 @@ def perovskite_dctem(n=(8, 8, 16), resolution=512, double_precision=False):
     c.obj_ap = 25.0
     c.alpha = 0.0
     c.delta = 0.0
+    s.attach_structure(st)
+    return s, st
+
+
+def uneven_stem_cell(rng):
+    """One cell of the uneven batched STEM workload, drawn from `rng` (numpy Generator): a perovskite or FCC
+    supercell 4-16 cells wide and 10-80 slices thick (two slices per cell), a grid from {256, 384, 512, 768,
+    1024}, 80-300 kV, a 16-32 mrad probe (Cs = 1 um), a 16x16 raster over the whole cell, an ADF detector at
+    2-5 times the convergence angle and 8 Å xy padding."""
+    from .structure import fcc, perovskite
+    kind = rng.choice(["perovskite", "fcc"])
+    lat = int(rng.integers(4, 17))
+    slices = int(rng.integers(10, 81))
+    grid = int(rng.choice([256, 384, 512, 768, 1024]))
+    kv = float(rng.uniform(80.0, 300.0))
+    mrad = float(rng.uniform(16.0, 32.0))
+    nz = max(5, (slices + 1) // 2)
+    if kind == "perovskite":
+        a = 3.905
+        st = perovskite(lat, lat, nz)
+    else:
+        a = 4.08
+        st = fcc(lat, lat, nz)
+    s = SimulationSettings()
+    c = s.cfg
+    c.mode = abi.MODE_STEM
+    c.double_precision = 0
+    c.resolution = grid
+    c.allow_any_resolution = 1
+    c.padding_xy = 8.0
+    c.padding_z = 0.0
+    c.slice_thickness = a / 2
+    c.slice_offset = a / 4
+    c.voltage = kv
+    c.cond_ap = mrad
+    c.C10 = 0.0
+    c.C30 = 1.0e4
+    s.maintain_area = True
+    c.stem_area[:] = [0.0, lat * a, 0.0, lat * a]
+    c.stem_pixels_x = c.stem_pixels_y = 16
+    c.stem_padding = 0.0
+    s.set_detectors([("ADF", 2.0 * mrad, 5.0 * mrad, 0.0, 0.0)])
     s.attach_structure(st)
     return s, st

@@ -14,7 +14,7 @@
 namespace ms {
 namespace draws {
 
-enum Kind : uint64_t { SET = 1, DEFOCUS = 2, SOURCE = 3 };
+enum Kind : uint64_t { SET = 1, DEFOCUS = 2, SOURCE = 3, DOSE = 4 };
 
 inline uint64_t mix64(uint64_t z) {
     z += 0x9E3779B97F4A7C15ull;
@@ -65,6 +65,42 @@ inline void source_shift(uint64_t seed, int build, double fwhm, double &dx, doub
     const double sd = sigma_of_fwhm(fwhm);
     dx = normal(key(seed, SOURCE, (uint64_t)build, 0, 0), key(seed, SOURCE, (uint64_t)build, 0, 1)) * sd;
     dy = normal(key(seed, SOURCE, (uint64_t)build, 1, 0), key(seed, SOURCE, (uint64_t)build, 1, 1)) * sd;
+}
+
+// Poisson deviate of mean lam for image pixel `pixel` in dose pass `pass` (the role of
+// std::poisson_distribution in SimulationCtem::simulateImageDose, simulationctem.cpp:224-236): inversion by
+// sequential search for lam < 10, else the transformed rejection method PTRS of W. Hormann ("The
+// transformed rejection method for generating Poisson random variables", Insurance: Mathematics and
+// Economics 12 (1993) 39-45). The i-th uniform of a pixel is uniform(key(seed, DOSE, pass, pixel, i)).
+inline double poisson(uint64_t seed, int pass, uint64_t pixel, double lam) {
+    if (!(lam > 0)) return 0.0;
+    uint64_t i = 0;
+    auto U = [&]() { return uniform(key(seed, DOSE, (uint64_t)pass, pixel, i++)); };
+    if (lam < 10.0) {
+        double p = std::exp(-lam), F = p;
+        const double u = U();
+        int k = 0;
+        while (u > F && k < 1000) {
+            k++;
+            p *= lam / k;
+            F += p;
+        }
+        return (double)k;
+    }
+    const double slam = std::sqrt(lam), loglam = std::log(lam);
+    const double b = 0.931 + 2.53 * slam, a = -0.059 + 0.02483 * b;
+    const double invalpha = 1.1239 + 1.1328 / (b - 3.4), vr = 0.9277 - 3.6224 / (b - 2.0);
+    for (int it = 0; it < 1000; it++) {
+        const double u = U() - 0.5, v = U();
+        const double us = 0.5 - std::fabs(u);
+        if (!(us > 0)) continue;
+        const double k = std::floor((2.0 * a / us + b) * u + lam + 0.43);
+        if (us >= 0.07 && v <= vr) return k;
+        if (k < 0 || (us < 0.013 && v > us)) continue;
+        if (std::log(v) + std::log(invalpha) - std::log(a / (us * us) + b) <= -lam + k * loglam - std::lgamma(k + 1.0))
+            return k;
+    }
+    return std::floor(lam);
 }
 
 }  // namespace draws

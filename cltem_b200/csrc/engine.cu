@@ -23,6 +23,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 namespace ms {
@@ -361,6 +362,8 @@ struct SimBase {
     virtual void ctem_loss_grad(const double *target, double *loss, double *gxyz, double *g10, double *g30, int ck,
                                 bool want_grad) = 0;
     virtual void set_c10_c30(double c10, double c30) = 0;
+    virtual void tune_batch(const int *cands, int n, int reps, int *best, double *rate) = 0;
+    virtual void set_ccd(const double *dqe, const double *ntf, size_t n, int binning, double dose) = 0;
 };
 
 template <class R>
@@ -390,6 +393,12 @@ struct Sim : SimBase {
     double build_x0 = 0, build_y0 = 0;   // frame start (Å) of the transmission being built
     DevBuf<int> tsel;
     DevBuf<double> dfac;
+    // CTEM dose simulation (SimulationCtem::simulateImageDose): CCD tables, binning, dose (e-/Å^2) and the
+    // number of dosed images made so far (the pass of their noise draws)
+    DevBuf<double> ccd_dqe, ccd_ntf;
+    int ccd_binning = 0;
+    double ccd_dose = 0;
+    int dose_pass = 0;
     std::vector<int> h_sel;
     std::vector<double> h_dfac;
     DevBuf<int> aZ, aZs, keys_in, keys_out, idx_in, idx_out, bid, zid, kept, counts, block_start;
@@ -751,8 +760,10 @@ struct Sim : SimBase {
         copy_out_complex(wave.p, NN, out);
     }
 
+    int tuned_batch = 0;   // set by tune_batch (or the per-process cache of earlier tunings)
     int default_batch() const {
         if (cfg.probe_batch > 0) return cfg.probe_batch;
+        if (tuned_batch > 0) return tuned_batch;
         size_t bytes = NN * sizeof(C);
         int b = (int)std::max<size_t>(1, ((size_t)1 << 30) / bytes);   // ~1 GiB of waves per pass (512 at 512^2 FP32)
         return std::min(b, 4096);
@@ -1087,6 +1098,58 @@ struct Sim : SimBase {
         MS_CUDA(cudaMemcpy(diff, d.p, (size_t)H.g.n_outputs * NN * sizeof(double), cudaMemcpyDeviceToHost));
     }
 
+    // SimulationCtem::simulateImageDose (simulationctem.cpp:171-264) on the image wave `w` (real space, after
+    // the objective lens): |w|^2 -> FFT -> DQE -> IFFT -> Poisson counts of mean N_tot * value (N_tot = dose
+    // per binned pixel, conversion factor 1) -> FFT -> NTF -> IFFT; the image is the real part. Transforms use
+    // clFFT's unitary scale both ways. The counts are drawn on the host, as the reference does, from the seeded
+    // stream of pass dose_pass (one pass per dosed image).
+    void dose_image(C *w, double *out) {
+        const cplx<R> *tw = ctx->twiddles<R>(N);
+        auto fft = [&](int sign) {
+            ops.row_fft(st(), w, w, 1, tw, (R)1, sign);
+            ops.col_fft(st(), w, w, 1, tw, (R)s2d, sign);
+            ctx->launches += 2;
+        };
+        sqabs_complex<R>(st(), NN, w);
+        fft(-1);
+        ccd_filter<R>(st(), N, w, ccd_dqe.p, ccd_binning, true);
+        fft(+1);
+        ctx->launches += 2;
+        std::vector<C> h(NN);
+        MS_CUDA(cudaMemcpyAsync(h.data(), w, NN * sizeof(C), cudaMemcpyDeviceToHost, st()));
+        MS_CUDA(cudaStreamSynchronize(st()));
+        const double dose_per_pix = ccd_dose * H.g.real_scale * H.g.real_scale;
+        const double n_tot = dose_per_pix * ccd_binning * ccd_binning;
+        for (size_t i = 0; i < NN; i++)
+            h[i] = mk<R>((R)draws::poisson(cfg.seed, dose_pass, i, n_tot * (double)h[i].x), (R)0);
+        dose_pass++;
+        MS_CUDA(cudaMemcpyAsync(w, h.data(), NN * sizeof(C), cudaMemcpyHostToDevice, st()));
+        fft(-1);
+        ccd_filter<R>(st(), N, w, ccd_ntf.p, ccd_binning, false);
+        fft(+1);
+        ctx->launches++;
+        real_part_to_double<R>(st(), NN, w, out);
+        ctx->launches++;
+        MS_CUDA(cudaStreamSynchronize(st()));   // h is released on return
+    }
+
+    void set_ccd(const double *dqe, const double *ntf, size_t n, int binning, double dose) override {
+        if (n == 0) {   // back to the perfect image
+            ccd_binning = 0;
+            return;
+        }
+        if (n != 725) throw ArgError("CCD tables hold 725 values (Utils::ccdToDqeNtf)");
+        if (binning < 1) throw ArgError("CCD binning must be >= 1");
+        if (!(dose > 0)) throw ArgError("CCD dose must be positive");
+        ccd_dqe.ensure(ctx, n);
+        ccd_ntf.ensure(ctx, n);
+        MS_CUDA(cudaMemcpy(ccd_dqe.p, dqe, n * sizeof(double), cudaMemcpyHostToDevice));
+        MS_CUDA(cudaMemcpy(ccd_ntf.p, ntf, n * sizeof(double), cudaMemcpyHostToDevice));
+        ccd_binning = binning;
+        ccd_dose = dose;
+        dose_pass = 0;
+    }
+
     void ctem_run(double *ew, double *diff, double *image) override {
         if (cfg.mode != MSLICE_MODE_CTEM) throw StateError("simulation is not in CTEM mode");
         if (cfg.mixed_static > 1) throw Unsupported("mixed static potentials are implemented for STEM and CBED runs");
@@ -1111,8 +1174,13 @@ struct Sim : SimBase {
                                  cfg.obj_ap_smooth, cfg.alpha, cfg.delta);
                 ops.row_fft(st(), tmp.p, tmp.p, 1, tw, (R)1, +1);
                 ops.col_fft(st(), tmp.p, tmp.p, 1, tw, (R)s2d, +1);
-                sqabs_to_double<R>(st(), NN, tmp.p, di.p + (size_t)o * NN);
-                ctx->launches += 4;
+                ctx->launches += 3;
+                if (ccd_binning > 0) {
+                    dose_image(tmp.p, di.p + (size_t)o * NN);
+                } else {
+                    sqabs_to_double<R>(st(), NN, tmp.p, di.p + (size_t)o * NN);
+                    ctx->launches++;
+                }
             }
         });
         MS_CUDA(cudaStreamSynchronize(st()));
@@ -1222,6 +1290,79 @@ struct Sim : SimBase {
         MS_CUDA(cudaMemcpy(out, acc.p, acc_n * sizeof(double), cudaMemcpyDeviceToHost));
         // Image::getWeightedSlice: sum / weight, weight = number of configurations per pixel
         for (size_t i = 0; i < acc_n; i++) out[i] /= (double)acc_configs;
+    }
+
+    // Autotuner of the probe batch: time `reps` STEM slice steps (one row and one column pass) at each
+    // candidate batch on zeroed scratch waves with the current transmission tables, and keep the batch
+    // with the most waves per second. Results are cached per (device, grid, precision) for the process.
+    static std::map<std::tuple<int, int, int>, std::pair<int, double>> &tune_cache() {
+        static std::map<std::tuple<int, int, int>, std::pair<int, double>> m;
+        return m;
+    }
+    void tune_batch(const int *cands, int n, int reps, int *best, double *rate) override {
+        if (n < 1 || reps < 1) throw ArgError("need candidate batches and repetitions");
+        const auto key = std::make_tuple(ctx->device, N, (int)sizeof(R));
+        {
+            std::lock_guard<std::mutex> lk(ctx->mtx);
+            auto it = tune_cache().find(key);
+            if (it != tune_cache().end() && cands == nullptr) {
+                tuned_batch = it->second.first;
+                if (best) *best = it->second.first;
+                if (rate) *rate = it->second.second;
+                return;
+            }
+        }
+        std::vector<int> cs;
+        if (cands) cs.assign(cands, cands + n);
+        else cs = {64, 128, 256, 512, 1024, 2048};
+        const size_t wave_bytes = NN * sizeof(C);
+        int bmax = 0;
+        for (int b : cs) {
+            if (b < 1 || b > 65535) throw ArgError("candidate batch out of range");
+            // three wave-sized buffers per probe; stay within a quarter of the device's free memory
+            size_t fr = 0, tot = 0;
+            MS_CUDA(cudaMemGetInfo(&fr, &tot));
+            if ((size_t)b <= (size_t)batch_cap || 3 * (size_t)b * wave_bytes < fr / 4) bmax = std::max(bmax, b);
+        }
+        if (bmax == 0) throw OomError("no candidate batch fits in device memory");
+        ensure_waves(bmax);
+        MS_CUDA(cudaMemsetAsync(wave.p, 0, (size_t)bmax * wave_bytes, st()));
+        if (!trans_built) MS_CUDA(cudaMemsetAsync(trans.p, 0, NN * sizeof(C), st()));
+        const cplx<R> *tw = ctx->twiddles<R>(N);
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
+        DetArgs det{detmask.p, cfg.n_detectors, partials.p};
+        const R a = (R)(1.0 / N), b2 = (R)(s2d * s2d * N), ds = (R)s2d;
+        double best_rate = -1;
+        int best_b = cs[0];
+        for (int b : cs) {
+            if (b > bmax) continue;
+            auto step = [&] {
+                ops.row_step(st(), wave.p, b, trans.p, tw, a, xa, xb, 0, nullptr, 0);
+                ops.col_step(st(), wave.p, b, tw, pt, b2, ds, det, nullptr, COL_STEP, tiles_lo, tiles_hi);
+                ctx->launches += 2;
+            };
+            step();   // warm-up
+            MS_CUDA(cudaEventRecord(ev[0], st()));
+            for (int r = 0; r < reps; r++) step();
+            MS_CUDA(cudaEventRecord(ev[1], st()));
+            MS_CUDA(cudaEventSynchronize(ev[1]));
+            float ms = 0;
+            MS_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+            const double r_ = (double)b * reps / (ms * 1e-3);
+            if (r_ > best_rate) { best_rate = r_; best_b = b; }
+        }
+        tuned_batch = best_b;
+        if (cands == nullptr) {   // only the default candidate set is shared through the cache
+            std::lock_guard<std::mutex> lk(ctx->mtx);
+            tune_cache()[key] = {best_b, best_rate};
+        }
+        // release the scratch waves: runs allocate batches of the tuned size (batch_cap sets their size)
+        MS_CUDA(cudaStreamSynchronize(st()));
+        drop_graphs();
+        wave.free(); recip.free(); tmp.free(); partials.free(); pix.free(); pos.free(); tsel.free(); dfac.free();
+        batch_cap = 0;
+        if (best) *best = best_b;
+        if (rate) *rate = best_rate;
     }
 
     void set_c10_c30(double c10, double c30) override {
@@ -1644,6 +1785,23 @@ int mslice_ctem_loss_grad(mslice_sim *sim, const double *target, double *loss, d
         need(sim && target, "null argument");
         use_device(sim->ctx);
         sim->impl->ctem_loss_grad(target, loss, grad_xyz, grad_c10, grad_c30, checkpoint_every, true);
+    });
+}
+
+int mslice_tune_batch(mslice_sim *sim, const int *candidates, int n_candidates, int reps, int *best_batch,
+                      double *waves_per_second) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        use_device(sim->ctx);
+        sim->impl->tune_batch(candidates, candidates ? n_candidates : 1, reps, best_batch, waves_per_second);
+    });
+}
+
+int mslice_set_ccd(mslice_sim *sim, const double *dqe, const double *ntf, size_t n, int binning, double dose) {
+    return guarded([&] {
+        need(sim != nullptr && (n == 0 || (dqe != nullptr && ntf != nullptr)), "null argument");
+        use_device(sim->ctx);
+        sim->impl->set_ccd(dqe, ntf, n, binning, dose);
     });
 }
 

@@ -307,7 +307,62 @@ template <class R> void convert_from_double(cudaStream_t s, size_t count, const 
     MS_CUDA(cudaGetLastError());
 }
 
+// |z|^2 kept as a complex value with zero imaginary part (sqabs_d.cl:11-27 writes double2)
+template <class R>
+__global__ void k_sqabs_complex(size_t count, cplx<R> *__restrict__ io) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const R re = io[i].x, im = io[i].y;
+    io[i] = mk<R>(re * re + im * im, (R)0);
+}
+template <class R> void sqabs_complex(cudaStream_t s, size_t count, cplx<R> *io) {
+    if (!count) return;
+    k_sqabs_complex<R><<<(unsigned)((count + 255) / 256), 256, 0, s>>>(count, io);
+    MS_CUDA(cudaGetLastError());
+}
+
+// ccd_dqe_d / ccd_ntf_d (kernels/ccd_dqe_d.cl:13-50, ccd_ntf_d.cl:13-49): radial table lookup in unshifted
+// reciprocal pixels, linear interpolation between entries floor(r/binning) and +1 (clamped at 724), and a
+// multiply by sqrt(value) (DQE) or value (NTF)
+template <class R>
+__global__ void k_ccd_filter(cplx<R> *__restrict__ io, const double *__restrict__ table, int n, int binning, int use_sqrt) {
+    int xid = blockIdx.x * blockDim.x + threadIdx.x, yid = blockIdx.y;
+    if (xid >= n) return;
+    size_t id = (size_t)xid + (size_t)yid * n;
+    int midx = xid < n / 2 ? 0 : n;
+    int midy = yid < n / 2 ? 0 : n;
+    double xp = xid - midx, yp = yid - midy;
+    double rad = sqrt(xp * xp + yp * yp);
+    int i1 = (int)floor(rad / binning);
+    int i2 = i1 + 1;
+    double v1 = table[min(i1, 724)], v2 = table[min(i2, 724)];
+    double interp = rad / binning - floor(rad / binning);
+    double f = interp * v2 + (1 - interp) * v1;
+    double m = use_sqrt ? sqrt(f) : f;
+    double re = (double)io[id].x, im = (double)io[id].y;
+    io[id] = mk<R>((R)(re * m), (R)(im * m));
+}
+template <class R> void ccd_filter(cudaStream_t s, int n, cplx<R> *io, const double *table, int binning, bool dqe) {
+    dim3 b(128), gr((n + 127) / 128, n);
+    k_ccd_filter<R><<<gr, b, 0, s>>>(io, table, n, binning, dqe ? 1 : 0);
+    MS_CUDA(cudaGetLastError());
+}
+
+template <class R>
+__global__ void k_real_part(size_t count, const cplx<R> *__restrict__ in, double *__restrict__ out) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) out[i] = (double)in[i].x;
+}
+template <class R> void real_part_to_double(cudaStream_t s, size_t count, const cplx<R> *in, double *out) {
+    if (!count) return;
+    k_real_part<R><<<(unsigned)((count + 255) / 256), 256, 0, s>>>(count, in, out);
+    MS_CUDA(cudaGetLastError());
+}
+
 #define MS_INST(R)                                                                                                       \
+    template void real_part_to_double<R>(cudaStream_t, size_t, const cplx<R> *, double *);                            \
+    template void sqabs_complex<R>(cudaStream_t, size_t, cplx<R> *);                                                    \
+    template void ccd_filter<R>(cudaStream_t, int, cplx<R> *, const double *, int, bool);                              \
     template void diffraction<R>(cudaStream_t, int, const cplx<R> *, double *, double *);                               \
     template void sqabs_to_double<R>(cudaStream_t, size_t, const cplx<R> *, double *);                                  \
     template void ctem_transfer<R>(cudaStream_t, int, const cplx<R> *, cplx<R> *, const double *, const double *, double, \

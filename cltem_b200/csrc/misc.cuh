@@ -51,6 +51,13 @@ template <class R> void ctem_transfer(cudaStream_t s, int n, const cplx<R> *in, 
                                       double beta, double delta);
 // row-transformed plane wave: phi_0 = D_r(1) = res at kx = 0 in every row (init_plane_wave_d.cl value 1.0)
 template <class R> void plane_wave_state(cudaStream_t s, int n, cplx<R> *wave);
+// |z|^2 + 0i in place (sqabs_d.cl)
+template <class R> void sqabs_complex(cudaStream_t s, size_t count, cplx<R> *io);
+// CCD detective quantum efficiency (dqe = true: multiply by sqrt) or noise transfer function on an unshifted
+// reciprocal image (ccd_dqe_d.cl, ccd_ntf_d.cl); table of 725 radial values per binned pixel
+template <class R> void ccd_filter(cudaStream_t s, int n, cplx<R> *io, const double *table, int binning, bool dqe);
+// the real part into double (SimulationCtem::getCtemImage)
+template <class R> void real_part_to_double(cudaStream_t s, size_t count, const cplx<R> *in, double *out);
 // complex copy with conversion
 template <class R> void convert_to_double(cudaStream_t s, size_t count, const cplx<R> *in, double2 *out);
 template <class R> void convert_from_double(cudaStream_t s, size_t count, const double2 *in, cplx<R> *out);

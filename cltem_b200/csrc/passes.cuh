@@ -52,6 +52,9 @@ template <int N, class R> struct ColCfg {
     static constexpr int THREADS = Plan<N>::NT * COLS;
     static_assert(THREADS <= 1024, "column block too large");
     static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(N + N * COLS); }
+    // Blocks per SM the step pass is compiled for: 3 x 512 threads for the FP32 radix-8 plans (a 42-register
+    // budget; the 2 blocks of a 52-register build leave its global loads exposed), else what fits.
+    static constexpr int STEP_MINB = (sizeof(R) == 4 && Plan<N>::E == 8 && THREADS == 512) ? 3 : 1;
 };
 
 template <class R, int N>
@@ -167,7 +170,7 @@ enum ColMode { COL_STEP = 0, COL_STEP_DET = 1, COL_DET_ONLY = 2 };
 // the leading and trailing tiles that hold columns inside the propagator's cut (all tiles when
 // tiles_lo = N/COLS); the others would only be multiplied by zero.
 template <class R, int N, int MODE>
-__global__ void __launch_bounds__(ColCfg<N, R>::THREADS)
+__global__ void __launch_bounds__(ColCfg<N, R>::THREADS, ColCfg<N, R>::STEP_MINB)
 k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTables<R> pt, R bscale, R det_scale,
            DetArgs det, cplx<R> *__restrict__ recip_out, int tiles_lo) {
     using P = Plan<N>;

@@ -81,6 +81,8 @@ def load_library(path=None):
         "mslice_ctem_loss": [C.c_void_p, _dp, _dp],
         "mslice_profile_read": [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_ulonglong), _dp, C.c_int],
         "mslice_incoherence_draws": [C.POINTER(abi.Config), C.c_int, _ip, C.c_size_t, _dp, _ip, C.c_int, C.c_int, _dp],
+        "mslice_tune_batch": [C.c_void_p, _ip, C.c_int, C.c_int, _ip, _dp],
+        "mslice_set_ccd": [C.c_void_p, _dp, _dp, C.c_size_t, C.c_int, C.c_double],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -353,6 +355,30 @@ class Simulation:
         _check(self.lib.mslice_stem_simulate(self.h, len(configs), counts.ctypes.data_as(_szp), _i(Z), _d(x), _d(y),
                                              _d(z), _d(out), n))
         return self._shape(out)
+
+    def set_ccd(self, ccd=None, binning=1, dose=10000.0):
+        """CTEM dose simulation with a CCD (cltem_b200.params.CCD: 725-value DQE and NTF tables), `binning` and
+        `dose` electrons per Å^2 (SimulationManager defaults: binning 1, dose 10000); None restores the perfect
+        image."""
+        if ccd is None:
+            _check(self.lib.mslice_set_ccd(self.h, None, None, 0, 1, 1.0))
+            return
+        dqe = np.ascontiguousarray(ccd.dqe, dtype=np.float64)
+        ntf = np.ascontiguousarray(ccd.ntf, dtype=np.float64)
+        if dqe.size != ntf.size:
+            raise ValueError("DQE and NTF tables differ in length")
+        _check(self.lib.mslice_set_ccd(self.h, _d(dqe), _d(ntf), dqe.size, int(binning), float(dose)))
+
+    def tune_batch(self, candidates=None, reps=3):
+        """Autotune the probe batch (mslice_tune_batch); returns (batch, waves per second)."""
+        best = C.c_int()
+        rate = C.c_double()
+        if candidates is None:
+            _check(self.lib.mslice_tune_batch(self.h, None, 0, int(reps), C.byref(best), C.byref(rate)))
+        else:
+            c = np.ascontiguousarray(candidates, dtype=np.int32)
+            _check(self.lib.mslice_tune_batch(self.h, _i(c), len(c), int(reps), C.byref(best), C.byref(rate)))
+        return best.value, rate.value
 
     KERNELS = ("row_step", "col_step", "potential", "bandlimit", "probe")
 

@@ -238,6 +238,13 @@ int mslice_ctem_loss_grad(mslice_sim *sim, const double *target, double *loss, d
                           double *grad_c30, int checkpoint_every);
 /* The same loss without gradients (forward only); used to time the forward model. */
 int mslice_ctem_loss(mslice_sim *sim, const double *target, double *loss);
+/* CTEM dose simulation (SimulationCtem::simulateImageDose, microscope/simulationctem.cpp:88-108,171-264):
+ * with a CCD set, the CTEM image of mslice_ctem_run is filtered by the detective quantum efficiency, given
+ * Poisson noise for `dose` electrons per Å^2 (times realScale^2 per pixel and binning^2 per binned pixel) and
+ * filtered by the noise transfer function. dqe / ntf: the 725-value radial tables of a clTEM ccds .dat file.
+ * n = 0 clears the CCD (the perfect image). The noise is drawn from cfg.seed; the k-th dosed image after
+ * this call uses pass k (the reference draws from a clock-seeded std::mt19937_64). */
+int mslice_set_ccd(mslice_sim *sim, const double *dqe, const double *ntf, size_t n, int binning, double dose);
 /* Change the defocus C10 and spherical aberration C30 (Å) of an existing simulation (the objective lens
  * of the CTEM image and the probe of STEM/CBED both follow). */
 int mslice_set_c10_c30(mslice_sim *sim, double c10, double c30);
@@ -269,6 +276,15 @@ int mslice_stem_simulate(mslice_sim *sim, int n_configs, const size_t *counts, c
  * frame; 0 for the mixed static sets). Any output pointer may be NULL; shift receives n_builds pairs. */
 int mslice_incoherence_draws(const mslice_config *cfg, int pass, const int *pixels, size_t n_pixels, double *defocus,
                              int *sets, int n_slices, int n_builds, double *shift);
+
+/* Autotuner of the probe batch (no counterpart in the reference, which propagates `parallel pixels`
+ * probes one at a time): times `reps` slice steps (one fused row and one fused column pass) at each
+ * candidate batch size on zeroed scratch waves and makes the fastest the simulation's default batch
+ * (used when cfg.probe_batch is 0). candidates = NULL tries 64..2048 and reuses a result cached for
+ * this device, grid and precision in the process. Candidates whose waves would take more than a quarter
+ * of the free device memory are skipped. best_batch / waves_per_second may be NULL. */
+int mslice_tune_batch(mslice_sim *sim, const int *candidates, int n_candidates, int reps, int *best_batch,
+                      double *waves_per_second);
 
 /* ---- comparison paths and building blocks ---------------------------------------------------- */
 /* Plain per-probe STEM in the reference's unfused kernel order (simulationgeneral.cpp:736-768):

@@ -62,6 +62,8 @@ def lib():
         L.orc_k_ctem_image.argtypes = [C.POINTER(abi.Config), _dp, _dp, _dp, _dp]
         L.orc_run_staged.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t), _ip, _dp, _dp, _dp, _dp]
         L.orc_draws.argtypes = [C.POINTER(abi.Config), C.c_int, _ip, C.c_size_t, _dp, _ip, C.c_int, C.c_int, _dp]
+        L.orc_set_ccd.argtypes = [C.c_void_p, _dp, _dp, C.c_size_t, C.c_int, C.c_double]
+        L.orc_poisson.argtypes = [C.c_uint64, C.c_int, _dp, C.c_size_t, _dp]
         _lib = L
     return _lib
 
@@ -128,6 +130,14 @@ def draws(cfg, pass_, pixels, n_slices, n_builds):
     shift = np.zeros((n_builds, 2))
     _chk(lib().orc_draws(C.byref(cfg), pass_, _i(pixels), len(pixels), _d(df), _i(sets), n_slices, n_builds, _d(shift)))
     return df, sets, shift
+
+
+def poisson(seed, pass_, lam):
+    """The oracle's seeded Poisson deviates of means `lam` (pixel i of dose pass `pass_`)."""
+    lam = np.ascontiguousarray(lam, dtype=np.float64)
+    out = np.zeros_like(lam)
+    _chk(lib().orc_poisson(int(seed), int(pass_), _d(lam), lam.size, _d(out)))
+    return out
 
 
 def set_threads(n):
@@ -199,6 +209,11 @@ class OracleSim:
         out = np.zeros(g.n_outputs * self.cfg.n_detectors * len(pixels))
         _chk(lib().orc_stem_run(self.h, _i(pixels), len(pixels), _d(out)))
         return out.reshape(g.n_outputs, self.cfg.n_detectors, len(pixels))
+
+    def set_ccd(self, ccd, binning=1, dose=10000.0):
+        dqe = np.ascontiguousarray(ccd.dqe, dtype=np.float64)
+        ntf = np.ascontiguousarray(ccd.ntf, dtype=np.float64)
+        _chk(lib().orc_set_ccd(self.h, _d(dqe), _d(ntf), dqe.size, int(binning), float(dose)))
 
     def run_staged(self, configs):
         """Average over the passes of a staged run (STEM [o, d, pixel] or CBED [o, ky, kx]) with the config's

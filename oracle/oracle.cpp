@@ -158,6 +158,41 @@ static void draw_shift(const mslice_config &c, int build, double &dx, double &dy
     dy = draw_normal(draw_key(c.seed, 3, (uint64_t)build, 1, 0), draw_key(c.seed, 3, (uint64_t)build, 1, 1)) * sd;
 }
 
+// Poisson deviate for dose pass `pass`, pixel `pixel`: sequential-search inversion for lam < 10, else
+// Hormann's transformed rejection PTRS (Insurance: Mathematics and Economics 12 (1993) 39-45); the i-th
+// uniform of a pixel comes from draw_key(seed, 4, pass, pixel, i). Stands in for the clock-seeded
+// std::poisson_distribution of SimulationCtem::simulateImageDose (simulationctem.cpp:224-236).
+static double draw_poisson(uint64_t seed, int pass, uint64_t pixel, double lam) {
+    if (!(lam > 0)) return 0.0;
+    uint64_t i = 0;
+    auto U = [&]() { return draw_uniform(draw_key(seed, 4, (uint64_t)pass, pixel, i++)); };
+    if (lam < 10.0) {
+        double p = std::exp(-lam), F = p;
+        double u = U();
+        int k = 0;
+        while (u > F && k < 1000) {
+            k++;
+            p *= lam / k;
+            F += p;
+        }
+        return (double)k;
+    }
+    double slam = std::sqrt(lam), loglam = std::log(lam);
+    double b = 0.931 + 2.53 * slam, a = -0.059 + 0.02483 * b;
+    double invalpha = 1.1239 + 1.1328 / (b - 3.4), vr = 0.9277 - 3.6224 / (b - 2.0);
+    for (int it = 0; it < 1000; it++) {
+        double u = U() - 0.5, v = U();
+        double us = 0.5 - std::fabs(u);
+        if (!(us > 0)) continue;
+        double k = std::floor((2.0 * a / us + b) * u + lam + 0.43);
+        if (us >= 0.07 && v <= vr) return k;
+        if (k < 0 || (us < 0.013 && v > us)) continue;
+        if (std::log(v) + std::log(invalpha) - std::log(a / (us * us) + b) <= -lam + k * loglam - std::lgamma(k + 1.0))
+            return k;
+    }
+    return std::floor(lam);
+}
+
 static bool resolution_valid(const mslice_config &c) {
     int r = c.resolution;
     if (c.allow_any_resolution) {
@@ -829,6 +864,27 @@ static void init_probe(std::complex<T> *out, int W, int H, const T *k_x, const T
         }
 }
 
+// ccd_dqe_d / ccd_ntf_d (kernels/ccd_dqe_d.cl:13-50, kernels/ccd_ntf_d.cl:13-49); use_sqrt selects the DQE form
+template <class T>
+static void ccd_filter(std::complex<T> *input, const T *table, unsigned int width, unsigned int height, int binning,
+                       bool use_sqrt) {
+    for (int yid = 0; yid < (int)height; yid++)
+        for (int xid = 0; xid < (int)width; xid++) {
+            int id = xid + yid * width;
+            int midx = xid < (int)(width / 2) ? 0 : (int)width;
+            int midy = yid < (int)(height / 2) ? 0 : (int)height;
+            T xp = xid - midx, yp = yid - midy;
+            T rad = std::sqrt(xp * xp + yp * yp);
+            int i1 = (int)std::floor(rad / binning);
+            int i2 = i1 + 1;
+            T v1 = table[std::min(i1, 724)], v2 = table[std::min(i2, 724)];
+            T interp = rad / binning - std::floor(rad / binning);
+            T f = interp * v2 + (1 - interp) * v1;
+            T m = use_sqrt ? std::sqrt(f) : f;
+            input[id] = std::complex<T>(input[id].real() * m, input[id].imag() * m);
+        }
+}
+
 // ctem_image_d (kernels/ctem_image_d.cl:50-119)
 template <class T>
 static void ctem_image(const std::complex<T> *input, std::complex<T> *output, int W, int H, const T *k_x, const T *k_y,
@@ -919,6 +975,9 @@ struct Sim {
     std::vector<std::vector<std::complex<T>>> trans;   // band-limited T per slice
     std::vector<std::vector<std::complex<T>>> trans_raw;
     std::vector<std::vector<std::vector<std::complex<T>>>> sets;   // mixed static potentials: T per set per slice
+    std::vector<T> ccd_dqe, ccd_ntf;   // CTEM dose simulation (SimulationCtem::simulateImageDose)
+    int ccd_binning = 0, dose_pass = 0;
+    double ccd_dose = 0;
     double frame_x = 0, frame_y = 0;   // start of the frame the next transmission build uses
     std::vector<std::complex<T>> prop;
 
@@ -1202,7 +1261,7 @@ struct Sim {
     }
 
     void ctem_outputs(const std::vector<std::complex<T>> &real, const std::vector<std::complex<T>> &recip_w, int oc,
-                      double *ew, double *diff, double *image) const {
+                      double *ew, double *diff, double *image) {
         const mslice_geometry &g = G.g;
         if (ew) for (size_t i = 0; i < N; i++) { ew[(size_t)oc * 2 * N + 2 * i] = real[i].real(); ew[(size_t)oc * 2 * N + 2 * i + 1] = real[i].imag(); }
         if (diff) diffraction(recip_w, diff + (size_t)oc * N);
@@ -1213,11 +1272,24 @@ struct Sim {
             ctem_image<T>(recip_w.data(), im.data(), res, res, kx.data(), ky.data(), (T)g.wavelength, A, (T)c.obj_ap,
                           (T)c.obj_ap_smooth, (T)c.alpha, (T)c.delta);
             fft2<T>(res, res, im.data(), tmp.data(), +1);
-            for (size_t i = 0; i < N; i++) image[(size_t)oc * N + i] = (double)(tmp[i].real() * tmp[i].real() + tmp[i].imag() * tmp[i].imag());
+            for (size_t i = 0; i < N; i++) tmp[i] = std::complex<T>(tmp[i].real() * tmp[i].real() + tmp[i].imag() * tmp[i].imag(), 0);   // sqabs_d
+            if (ccd_binning > 0) {   // simulateImageDose (simulationctem.cpp:171-264), conversion factor 1
+                fft2<T>(res, res, tmp.data(), im.data(), -1);
+                ccd_filter<T>(im.data(), ccd_dqe.data(), res, res, ccd_binning, true);
+                fft2<T>(res, res, im.data(), tmp.data(), +1);
+                double N_tot = ccd_dose * g.real_scale * g.real_scale * ccd_binning * ccd_binning;
+                for (size_t i = 0; i < N; i++)
+                    tmp[i] = std::complex<T>((T)draw_poisson(c.seed, dose_pass, i, N_tot * (double)tmp[i].real()), 0);
+                dose_pass++;
+                fft2<T>(res, res, tmp.data(), im.data(), -1);
+                ccd_filter<T>(im.data(), ccd_ntf.data(), res, res, ccd_binning, false);
+                fft2<T>(res, res, im.data(), tmp.data(), +1);
+            }
+            for (size_t i = 0; i < N; i++) image[(size_t)oc * N + i] = (double)tmp[i].real();   // getCtemImage
         }
     }
 
-    void ctem(double *ew, double *diff, double *image) const {
+    void ctem(double *ew, double *diff, double *image) {
         const mslice_geometry &g = G.g;
         int S = g.n_slices;
         std::vector<std::complex<T>> real(N, std::complex<T>(1, 0)), recip_w(N), tmp(N);   // init_plane_wave value 1.0
@@ -1448,6 +1520,25 @@ int orc_draws(const mslice_config *c, int pass, const int *pixels, size_t n, dou
         if (shift)
             for (int b = 0; b < n_builds; b++) draw_shift(*c, b, shift[2 * b], shift[2 * b + 1]);
     });
+}
+
+int orc_set_ccd(OrcSim *s, const double *dqe, const double *ntf, size_t n, int binning, double dose) {
+    return guard([&] {
+        auto go = [&](auto *S) {
+            using T = typename std::remove_reference<decltype(S->kx)>::type::value_type;
+            S->ccd_binning = n ? binning : 0;
+            S->ccd_dose = dose;
+            S->dose_pass = 0;
+            S->ccd_dqe.assign(dqe, dqe + n);
+            S->ccd_ntf.assign(ntf, ntf + n);
+            (void)sizeof(T);
+        };
+        if (s->dp) go(s->sd); else go(s->sf);
+    });
+}
+
+int orc_poisson(uint64_t seed, int pass, const double *lam, size_t n, double *out) {
+    return guard([&] { for (size_t i = 0; i < n; i++) out[i] = draw_poisson(seed, pass, i, lam[i]); });
 }
 
 double orc_bessk0(double x) { return bessk0<double>(x); }

@@ -124,3 +124,41 @@ def test_json_incoherence_keys():
     j["incoherence"]["inelastic scattering"]["phonon"]["enabled"] = False
     s = read_config(j)
     assert s.effective_iterations() == 1 and s.cfg.stem_moving_frame == 0
+
+
+def test_ccd_tables_and_json_keys():
+    from cltem_b200.config import read_config
+    from cltem_b200.params import CCD_TABLE_SIZE, load_ccds
+    ccds = load_ccds()
+    assert set(ccds) == {"k2", "orius"}
+    for c in ccds.values():
+        assert c.dqe.shape == (CCD_TABLE_SIZE,) and c.ntf.shape == (CCD_TABLE_SIZE,)
+        assert np.all(c.dqe >= 0) and np.all(c.ntf >= 0)
+    s = read_config({"mode": {"id": 0}, "ctem": {"ccd": {"name": "K2", "dose": {"val": 50.0}, "binning": 2}}})
+    assert (s.ccd_name, s.ccd_dose, s.ccd_binning) == ("K2", 50.0, 2)
+    assert read_config({}).ccd_name == ""
+
+
+def test_ccd_reader_stream_semantics(tmp_path):
+    # the reference reads each table line with `stringstream >> double`, which splits runs like "0.70.6"
+    from cltem_b200.params import read_ccd
+    vals = " ".join(["0.5"] * 723) + " 0.70.6"
+    p = tmp_path / "cam.dat"
+    p.write_text("Cam\n\nDQE\n" + vals + "\nNTF\n" + vals + "\n")
+    c = read_ccd(str(p))
+    assert c.name == "Cam" and c.dqe.size == 725 and c.dqe[-2] == 0.7 and c.dqe[-1] == 0.6
+    p.write_text("Cam\nDQE\n0.1 0.2\nNTF\n" + vals + "\n")
+    with pytest.raises(RuntimeError):
+        read_ccd(str(p))
+
+
+@pytest.mark.parametrize("lam", [0.0, 0.3, 4.0, 9.9, 10.0, 55.0, 3000.0])
+def test_oracle_poisson_moments(oracle, lam):
+    x = oracle.poisson(7, 0, np.full(40000, lam))
+    assert np.all(x == np.floor(x)) and np.all(x >= 0)
+    if lam == 0:
+        assert not x.any()
+        return
+    se = np.sqrt(lam / x.size)
+    assert abs(x.mean() - lam) < 5 * se
+    assert abs(x.var() / lam - 1) < 0.05

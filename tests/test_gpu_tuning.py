@@ -1,0 +1,42 @@
+"""The probe-batch autotuner: it picks one of the candidates, later runs use that batch, and the results do
+not depend on the batch."""
+import numpy as np
+import pytest
+
+from cltem_b200.engine import MsliceError, Simulation
+from tests.cases import phonons, small_stem
+
+pytestmark = pytest.mark.gpu
+
+
+def test_tune_batch_picks_a_candidate_and_keeps_results(gpu_ctx, kirkland):
+    gpu_ctx.load_params(kirkland)
+    s, st = small_stem(double_precision=False, scan=5)
+    conf = phonons(st, 1)[0]
+    ref_sim = Simulation(gpu_ctx, s.cfg)
+    ref_sim.set_atoms(conf)
+    pix = np.arange(25, dtype=np.int32)
+    ref = ref_sim.stem(pix)
+    sim = Simulation(gpu_ctx, s.cfg)
+    sim.set_atoms(conf)
+    best, rate = sim.tune_batch([4, 8, 16], reps=2)
+    assert best in (4, 8, 16) and rate > 0
+    sim.build_transmission()
+    l0 = gpu_ctx.launch_count()
+    got = sim.stem(pix)
+    nbatch = -(-25 // best)
+    per_batch = 1 + 2 * sim.geo.n_slices + sim.geo.n_outputs
+    assert gpu_ctx.launch_count() - l0 == nbatch * per_batch
+    assert np.allclose(got, ref, rtol=1e-12, atol=0)   # per-probe arithmetic does not depend on the batch
+
+
+def test_tune_batch_default_candidates_are_cached(gpu_ctx, kirkland):
+    gpu_ctx.load_params(kirkland)
+    s, st = small_stem(double_precision=False, scan=2)
+    a = Simulation(gpu_ctx, s.cfg)
+    b1, r1 = a.tune_batch(reps=1)
+    b = Simulation(gpu_ctx, s.cfg)
+    b2, r2 = b.tune_batch(reps=1)   # same device, grid and precision: the cached result
+    assert (b1, r1) == (b2, r2) and b1 in (64, 128, 256, 512, 1024, 2048)
+    with pytest.raises(MsliceError):
+        a.tune_batch([0, 4])
