@@ -54,6 +54,9 @@ def parse():
     p.add_argument("--scan", type=int, default=64)
     p.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline and plain-FP64 legs")
     p.add_argument("--cpu-probes", type=int, default=32, help="probes in the bounded CPU sample")
+    p.add_argument("--only", default=None, choices=["adjoint", "cbed3d", "uneven"],
+                   help="run one extra leg alone and print its JSON (for profiling it)")
+    p.add_argument("--cbed-nz", type=int, default=60, help="FCC cells along z of the cbed3d leg (60: 120 slices)")
     return p.parse_args()
 
 
@@ -286,7 +289,7 @@ def full3d_evaluations(sim, n_atoms, S, N):
     return total
 
 
-def cbed3d_leg(ctx, ext):
+def cbed3d_leg(ctx, ext, nz=60):
     """CBED through the full-3D Lobato potential (FCC Au 20x20x60 cells, 96,000 atoms, 1024^2, 120 slices,
     4 sub-slices, FP32): one phonon configuration (u_rms 0.09 Å) of the 50; the potential build is the bound."""
     import torch
@@ -294,7 +297,7 @@ def cbed3d_leg(ctx, ext):
     from cltem_b200.engine import Simulation
     from cltem_b200.params import load_default
     from cltem_b200.structure import phonon_configs
-    s, st = config.fcc_cbed()
+    s, st = config.fcc_cbed(n=(20, 20, nz))
     ctx.load_params(load_default("lobato"))
     sim = Simulation(ctx, s.cfg)
     S, N = sim.geo.n_slices, s.cfg.resolution
@@ -314,7 +317,7 @@ def cbed3d_leg(ctx, ext):
     pot_ms = prof["potential"][0]
     sim.close()
     ctx.load_params(load_default("kirkland"))
-    return {"workload": "cbed_full3d_lobato_fcc_20x20x60_1024x1024_120slices_4subslices_fp32",
+    return {"workload": f"cbed_full3d_lobato_fcc_20x20x{nz}_1024x1024_{S}slices_4subslices_fp32",
             "atom_sample_evaluations": ev, "potential_ms": pot_ms,
             "evaluations_per_s": ev / (pot_ms * 1e-3), "config_ms": t["total_ms"],
             "build_ms": t["build_ms"], "propagate_ms": t["propagate_ms"],
@@ -362,6 +365,16 @@ def main():
     import torch
     import torch.distributed as dist
     torch.cuda.set_device(local)
+    if args.only:   # one extra leg alone (1 GPU)
+        from cltem_b200.engine import Context
+        from cltem_b200.params import load_default
+        ctx = Context(local)
+        ctx.load_params(load_default("kirkland"))
+        ext = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+        leg = {"adjoint": lambda: adjoint_leg(ctx, ext, args.warmup), "cbed3d": lambda: cbed3d_leg(ctx, ext, args.cbed_nz),
+               "uneven": lambda: uneven_leg(ctx)}[args.only]()
+        print(json.dumps({"leg": args.only, **leg}))
+        return 0
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))

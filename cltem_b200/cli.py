@@ -175,7 +175,7 @@ def main(argv=None):
     with open(a.config) as f:
         raw = json.load(f)
     settings = read_config(raw)
-    structure = read_xyz(a.structure)
+    structure = read_xyz(a.structure, seed=a.seed)
     settings.attach_structure(structure)
     params = _load_params(settings.potentials, a.params)
     from .engine import geometry

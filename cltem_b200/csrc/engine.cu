@@ -399,6 +399,9 @@ struct Sim : SimBase {
     int ccd_binning = 0;
     double ccd_dose = 0;
     int dose_pass = 0;
+    // differentiable CTEM work buffers (ctem_loss_grad)
+    DevBuf<C> E, ck_buf, save, fw, gT, w1, w2;
+    DevBuf<double> tgt, part, gV, gxy, gwork;
     std::vector<int> h_sel;
     std::vector<double> h_dfac;
     DevBuf<int> aZ, aZs, keys_in, keys_out, idx_in, idx_out, bid, zid, kept, counts, block_start;
@@ -1387,8 +1390,7 @@ struct Sim : SimBase {
         const cplx<R> *tw = ctx->twiddles<R>(N);
         const R a = (R)(1.0 / N), b = (R)(s2d * s2d * N), ds = (R)s2d;
         const int all_tiles = N / ops.cols_per_tile;
-        DevBuf<C> E, ck_buf, save, fw, gT, w1, w2;
-        DevBuf<double> tgt, part, gV, gxy;
+        // work buffers persist across calls (grow only): no allocation or implicit device sync per call
         E.ensure(ctx, (size_t)S * NN);
         ensure_waves(1);
         w1.ensure(ctx, NN); w2.ensure(ctx, NN);
@@ -1451,6 +1453,11 @@ struct Sim : SimBase {
         MS_CUDA(cudaStreamSynchronize(st()));
         const int n_in = hbs.back();
         gxy.ensure(ctx, 2 * (size_t)std::max(n_in, 1));
+        {   // scratch of the atom gather: the largest slice's atoms
+            int mx = 1;
+            for (int s = 0; s < S; s++) mx = std::max(mx, hbs[(size_t)(s + 1) * nb] - hbs[(size_t)s * nb]);
+            gwork.ensure(ctx, (size_t)atom_grad_work_doubles(mx));
+        }
         MS_CUDA(cudaMemsetAsync(gxy.p, 0, 2 * (size_t)std::max(n_in, 1) * sizeof(double), st()));
         fw.ensure(ctx, NN); gT.ensure(ctx, NN); gV.ensure(ctx, NN);
         PropTables<R> ptc{pxc.p, pyc.p, kx2.p, ky2.p, k_prop * k_prop};
@@ -1473,7 +1480,7 @@ struct Sim : SimBase {
                 grad_v<R>(st(), NN, E.p + (size_t)s * NN, gT.p, g.sigma, gV.p);
                 const int a0 = hbs[(size_t)s * nb], a1 = hbs[(size_t)(s + 1) * nb];
                 atom_grad<R>(st(), a0, a1 - a0, axs.p, ays.p, aZs.p, gV.p, N, g.sim_x[0], g.sim_y[0], g.real_scale,
-                             ctx->params.form, params_dev(), ctx->params.i_count, gxy.p);
+                             ctx->params.form, params_dev(), ctx->params.i_count, gxy.p, gwork.p);
                 ctx->launches += 5;
             }
         }

@@ -5,7 +5,7 @@
 // projected form the forward potential kernel sums (potential.cuh; transmission_potentials_projected_d.cl)
 // and zero where the forward clamps rho to r_min = dx/4.
 //
-// One 256-thread block per atom, threads tiled 32 x 8 over the atom's pixel box. Pixel-to-atom offsets
+// Threads of a block are tiled 32 x 8 over a band of the atom's pixel box. Pixel-to-atom offsets
 // are formed in FP64 (as in the forward kernel); rho, V'(rho) and the per-thread sums are in the engine's
 // precision T; the block sums are FP64. Built without -fmad=false: nothing here restates a reference
 // statement bit for bit.
@@ -46,11 +46,16 @@ __device__ __forceinline__ T dpot_drho(int form, const T *__restrict__ prm, int 
     return s;
 }
 
+// One 256-thread block per (atom, band of pixel rows): kGatherBands blocks share an atom's pixel box so a
+// slice's ~100-200 atoms still fill the GPU; each block writes its two sums to work[], and k_atom_grad_sum
+// adds the bands of every atom in a fixed order (deterministic results).
+constexpr int kGatherBands = 8;
+
 template <class T>
 __global__ void __launch_bounds__(256)
 k_atom_grad(int a0, const double *__restrict__ ax, const double *__restrict__ ay, const int *__restrict__ aZ,
             const double *__restrict__ gV, int n, double startx, double starty, double dx, int form,
-            const T *__restrict__ prm, int i_lim, double *__restrict__ gxy) {
+            const T *__restrict__ prm, int i_lim, double *__restrict__ work) {
     __shared__ double red[2][8];
     const int a = a0 + blockIdx.x;
     const double xa = ax[a], ya = ay[a];
@@ -59,9 +64,13 @@ k_atom_grad(int a0, const double *__restrict__ ax, const double *__restrict__ ay
     int ix0 = (int)floor((xa - 8.0 - startx) / dx), ix1 = (int)ceil((xa + 8.0 - startx) / dx);
     int iy0 = (int)floor((ya - 8.0 - starty) / dx), iy1 = (int)ceil((ya + 8.0 - starty) / dx);
     ix0 = max(ix0, 0); iy0 = max(iy0, 0); ix1 = min(ix1, n - 1); iy1 = min(iy1, n - 1);
+    // this block's rows: band blockIdx.y of kGatherBands equal bands of [iy0, iy1]
+    const int rows = iy1 - iy0 + 1;
+    const int r0 = iy0 + (int)(((long long)rows * blockIdx.y) / kGatherBands);
+    const int r1 = iy0 + (int)(((long long)rows * (blockIdx.y + 1)) / kGatherBands) - 1;
     const double ox = startx - xa, oy = starty - ya;   // pixel px sits at ox + px dx from the atom
     T gx = 0, gy = 0;
-    for (int py = iy0 + (int)threadIdx.y; py <= iy1; py += 8) {
+    for (int py = r0 + (int)threadIdx.y; py <= r1; py += 8) {
         const T ry = (T)(oy + py * dx);
         const double *grow = gV + (size_t)py * n;
         for (int px = ix0 + (int)threadIdx.x; px <= ix1; px += 32) {
@@ -81,27 +90,45 @@ k_atom_grad(int a0, const double *__restrict__ ax, const double *__restrict__ ay
         sx += __shfl_down_sync(0xffffffffu, sx, o);
         sy += __shfl_down_sync(0xffffffffu, sy, o);
     }
-    const int warp = (threadIdx.y * 32 + threadIdx.x) >> 5;
-    if (threadIdx.x == 0) { red[0][warp] = sx; red[1][warp] = sy; }
+    if (threadIdx.x == 0) { red[0][threadIdx.y] = sx; red[1][threadIdx.y] = sy; }
     __syncthreads();
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         double tx = 0, ty = 0;
         for (int i = 0; i < 8; i++) { tx += red[0][i]; ty += red[1][i]; }
-        gxy[2 * (size_t)a] = tx;
-        gxy[2 * (size_t)a + 1] = ty;
+        const size_t w = ((size_t)blockIdx.x * kGatherBands + blockIdx.y) * 2;
+        work[w] = tx;
+        work[w + 1] = ty;
     }
+}
+
+__global__ void k_atom_grad_sum(int a0, int count, const double *__restrict__ work, double *__restrict__ gxy) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    double tx = 0, ty = 0;
+    for (int b = 0; b < kGatherBands; b++) {
+        tx += work[((size_t)i * kGatherBands + b) * 2];
+        ty += work[((size_t)i * kGatherBands + b) * 2 + 1];
+    }
+    gxy[2 * (size_t)(a0 + i)] = tx;
+    gxy[2 * (size_t)(a0 + i) + 1] = ty;
 }
 
 template <class T>
 void atom_grad(cudaStream_t s, int a0, int count, const double *ax, const double *ay, const int *aZ, const double *gV,
-               int n, double startx, double starty, double dx, int form, const T *prm, int i_lim, double *gxy) {
+               int n, double startx, double starty, double dx, int form, const T *prm, int i_lim, double *gxy,
+               double *work) {
     if (count <= 0) return;
-    k_atom_grad<T><<<count, dim3(32, 8), 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, form, prm, i_lim, gxy);
+    k_atom_grad<T><<<dim3(count, kGatherBands), dim3(32, 8), 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, form,
+                                                                    prm, i_lim, work);
+    MS_CUDA(cudaGetLastError());
+    k_atom_grad_sum<<<(count + 127) / 128, 128, 0, s>>>(a0, count, work, gxy);
     MS_CUDA(cudaGetLastError());
 }
+int atom_grad_work_doubles(int max_count) { return 2 * kGatherBands * max_count; }
+
 template void atom_grad<float>(cudaStream_t, int, int, const double *, const double *, const int *, const double *, int,
-                               double, double, double, int, const float *, int, double *);
+                               double, double, double, int, const float *, int, double *, double *);
 template void atom_grad<double>(cudaStream_t, int, int, const double *, const double *, const int *, const double *, int,
-                                double, double, double, int, const double *, int, double *);
+                                double, double, double, int, const double *, int, double *, double *);
 
 }  // namespace ms

@@ -225,7 +225,11 @@ k_potential_projected(cplx<T> *__restrict__ out, const double *__restrict__ ax, 
                 double z_by_tan_beam_theta = z_prime / tan_beam_theta;
                 double x_prime = rad_x + z_by_tan_beam_theta * cos_beam_phi;
                 double y_prime = rad_y + z_by_tan_beam_theta * sin_beam_phi;
-                double rad_d = sqrt(z_prime * z_prime + x_prime * x_prime + y_prime * y_prime);
+                const double rad2 = z_prime * z_prime + x_prime * x_prime + y_prime * y_prime;
+                // sqrt(rad2) <= 8 needs rad2 <= 64 up to one rounding: candidates beyond 64 (1 + 1e-12) skip
+                // the square root; the test itself is the reference's (projected_d.cl:290-296)
+                if (rad2 > 64.000000000064) continue;
+                double rad_d = sqrt(rad2);
                 if (rad_d < r_min) rad_d = r_min;
                 if (rad_d <= 8.0) {
                     const T rad = (T)rad_d;
@@ -262,6 +266,7 @@ k_potential_3d(cplx<T> *__restrict__ out, const double *__restrict__ ax, const d
     const double im_pos_x = p.startx + xid * p.pixelscale;
     const double im_pos_y = p.starty + yid * p.pixelscale;
     const double r_min = 0.25 * p.pixelscale;
+    const bool no_shift = p.shift_x == 0.0 && p.shift_y == 0.0;
     T sumz = 0;
     const size_t nb = (size_t)p.blocks_x * p.blocks_y;
     for (int k = topz; k <= bottomz; k++) {
@@ -277,15 +282,21 @@ k_potential_3d(cplx<T> *__restrict__ out, const double *__restrict__ ax, const d
                 for (int l = 0; l < cn; l++) {
                     double rad_x = im_pos_x - sx[l];
                     double rad_y = im_pos_y - sy[l];
+                    // without tilt the shift is zero and the xy test is the same for every sample: an atom
+                    // beyond 8 Å adds nothing and changes no trapezoid state, so it is skipped whole
+                    const double xy0 = rad_x * rad_x + rad_y * rad_y;
+                    if (no_shift && xy0 > 64.0) continue;
                     for (int h = 0; h <= p.integrals; h++) {
                         rad_x -= p.shift_x;   // cumulative (full_3d_d.cl:244-246)
                         rad_y -= p.shift_y;
-                        double xyrad2 = rad_x * rad_x + rad_y * rad_y;
+                        double xyrad2 = no_shift ? xy0 : rad_x * rad_x + rad_y * rad_y;
                         double im_pos_z = current_z - h * p.dz * int_r;
                         double rad_z = im_pos_z - sz[l];
-                        double rad_d = sqrt(xyrad2 + rad_z * rad_z);
-                        if (rad_d < r_min) rad_d = r_min;
                         if (xyrad2 <= 64.0 && rad_z <= 3.0) {
+                            // the distance is only used by samples that pass the test: taken here instead
+                            // of for every candidate (same value as full_3d_d.cl:258-261)
+                            double rad_d = sqrt(xyrad2 + rad_z * rad_z);
+                            if (rad_d < r_min) rad_d = r_min;
                             const T rad = (T)rad_d;
                             T p1;
                             if constexpr (FORM == 0) p1 = kirkland_3<T>(prm, p.i_count, sZ[l], rad);

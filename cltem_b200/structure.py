@@ -63,7 +63,13 @@ def _stof(s: str) -> float:
     return float(np.float32(float(s)))
 
 
-def read_xyz(path: str) -> Structure:
+def read_xyz(path: str, seed: int = 0) -> Structure:
+    """Read a clTEM .xyz file (CrystalStructure::openXyz, src/simulation/structure/crystalstructure.cpp:44-173):
+    atom count, a header line of column names (A x y z [occ] [u] [u1 u2 u3], optional "nm" for nanometre units,
+    or no names for the A x y z default), then one atom per line, coordinates parsed as std::stof does.
+    With an occ column, consecutive atoms at the same position form one site; a uniform draw from a
+    generator seeded by `seed` keeps the atom whose cumulative occupancy interval holds it, or none
+    (processOccupancyList, :214-236; the reference's generator is clock-seeded)."""
     with open(path, "r") as f:
         lines = f.read().splitlines()
     try:
@@ -89,7 +95,7 @@ def read_xyz(path: str) -> Structure:
     if default:
         hocc, hu, hu1, hu2, hu3 = [h + 4 * (h != -1) for h in (hocc, hu, hu1, hu2, hu3)]
     max_header = max(hA, hx, hy, hz, hocc, hu, hu1, hu2, hu3)
-    Z, X, Y, Zc, U = [], [], [], [], []
+    Z, X, Y, Zc, U, OCC = [], [], [], [], [], []
     defined_u = hu != -1 or hu1 != -1 or hu2 != -1 or hu3 != -1
     i = 0
     for line in lines[2:]:
@@ -104,6 +110,8 @@ def read_xyz(path: str) -> Structure:
         X.append(_stof(v[hx]) * scale)
         Y.append(_stof(v[hy]) * scale)
         Zc.append(_stof(v[hz]) * scale)
+        if hocc != -1:
+            OCC.append(_stof(v[hocc]))
         if defined_u:
             u = [0.0, 0.0, 0.0]
             if hu != -1:
@@ -118,8 +126,38 @@ def read_xyz(path: str) -> Structure:
         i += 1
     if i != n:
         raise RuntimeError(f"Number of atoms does not match .xyz first line: {i} instead of {n}")
-    return Structure(np.asarray(Z, np.int32), np.asarray(X), np.asarray(Y), np.asarray(Zc),
-                     np.asarray(U) if defined_u else None, name=path)
+    keep = np.arange(len(Z))
+    if hocc != -1:
+        keep = _process_occupancy(X, Y, Zc, OCC, np.random.default_rng(seed))
+    U = np.asarray(U) if defined_u else None
+    return Structure(np.asarray(Z, np.int32)[keep], np.asarray(X)[keep], np.asarray(Y)[keep], np.asarray(Zc)[keep],
+                     U[keep] if U is not None else None, name=path)
+
+
+def _process_occupancy(X, Y, Zc, occ, rng):
+    """Indices kept by CrystalStructure::processOccupancyList over runs of consecutive atoms at one position:
+    a single fully occupied atom is kept; otherwise one uniform r in [0, 1) keeps the atom whose interval
+    [sum of earlier occupancies, + its own) holds r (or the last, when r = 1 and the sum is exactly 1), and a
+    site whose occupancies add up to more than 1 is an error."""
+    keep = []
+    i, n = 0, len(X)
+    while i < n:
+        j = i + 1
+        while j < n and X[j] == X[i] and Y[j] == Y[i] and Zc[j] == Zc[i]:
+            j += 1
+        if j - i == 1 and occ[i] == 1.0:
+            keep.append(i)
+        else:
+            r = float(rng.random())
+            total = 0.0
+            for k in range(i, j):
+                if (total <= r < total + occ[k]) or (r == 1.0 and total + occ[k] == 1.0):
+                    keep.append(k)
+                total += occ[k]
+            if total > 1.0000001:
+                raise RuntimeError(".xyz has occupancies > 1.")
+        i = j
+    return np.asarray(keep, dtype=np.int64)
 
 
 def write_xyz(s: Structure, path: str):

@@ -85,3 +85,28 @@ def test_cli_rejects_cif_and_missing_args(tmp_path, capsys):
     p.write_text(json.dumps(_cfg_json()))
     assert cli_main([str(tmp_path / "s.cif"), "-c", str(p), "-o", str(tmp_path / "o")]) == 1
     assert cli_main(["-v"]) == 0
+
+
+def test_xyz_site_occupancy(tmp_path):
+    # consecutive atoms at one position form a site; one draw keeps the atom whose cumulative occupancy
+    # interval holds it, or none (CrystalStructure::processOccupancyList)
+    lines = []
+    for k in range(400):
+        lines.append(f"Sr {k}.0 0.0 0.0 0.5")
+        lines.append(f"Ti {k}.0 0.0 0.0 0.25")   # same site: Sr 1/2, Ti 1/4, vacancy 1/4
+        lines.append(f"O {k}.5 0.0 0.0 1.0")      # a full site of its own
+    p = tmp_path / "occ.xyz"
+    p.write_text(f"{len(lines)}\nA x y z occ\n" + "\n".join(lines) + "\n")
+    s = read_xyz(str(p), seed=3)
+    z = np.asarray(s.Z)
+    assert (z == 8).sum() == 400
+    n_sr, n_ti = (z == 38).sum(), (z == 22).sum()
+    assert abs(n_sr - 200) < 45 and abs(n_ti - 100) < 35 and n_sr + n_ti < 400
+    # one atom per site at most, and the draw is repeatable
+    xs = np.asarray(s.x)[z != 8]
+    assert len(np.unique(xs)) == len(xs)
+    s2 = read_xyz(str(p), seed=3)
+    assert np.array_equal(np.asarray(s2.Z), z)
+    p.write_text("2\nA x y z occ\nSr 0 0 0 0.7\nTi 0 0 0 0.6\n")
+    with pytest.raises(RuntimeError):
+        read_xyz(str(p))
