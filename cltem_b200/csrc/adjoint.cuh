@@ -17,13 +17,14 @@ template <class R, int N>
 __global__ void __launch_bounds__(RowCfg<N, R>::THREADS)
 k_row_step_save(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const cplx<R> *__restrict__ twg, R a,
                 cplx<R> *__restrict__ save) {
-    using P = Plan<N>;
-    constexpr int ROWS = RowCfg<N, R>::ROWS;
+    using RC = RowCfg<N, R>;
+    using P = typename RC::P;
+    constexpr int ROWS = RC::ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + N + threadIdx.y * RowAddr::size(N);
+    cplx<R> *sm = tw + RC::TWN + threadIdx.y * RC::ROWSZ;
     const int t = threadIdx.x;
-    load_twiddles<R, N>(tw, twg, t + threadIdx.y * P::NT, P::NT * ROWS);
+    load_table<R>(tw, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
     const int y = blockIdx.x * ROWS + threadIdx.y;
     const size_t off = (size_t)blockIdx.y * N * N + (size_t)y * N;
     cplx<R> *row = wave + off;
@@ -32,14 +33,14 @@ k_row_step_save(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, c
 #pragma unroll
     for (int m = 0; m < P::E; m++) v[m] = row[t + m * P::NT];
     __syncthreads();
-    fft<R, N, +1>(v, sm, RowAddr(), t, tw);
+    row_transform<R, N, +1>(v, sm, t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) {
         cplx<R> psi = cscale(v[m], a);
         save[off + t + m * P::NT] = psi;
         v[m] = cmul(psi, trow[t + m * P::NT]);
     }
-    fft<R, N, -1>(v, sm, RowAddr(), t, tw);
+    row_transform<R, N, -1>(v, sm, t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) row[t + m * P::NT] = v[m];
 }
@@ -50,13 +51,14 @@ template <class R, int N>
 __global__ void __launch_bounds__(RowCfg<N, R>::THREADS)
 k_row_adjoint(cplx<R> *__restrict__ state, const cplx<R> *__restrict__ trans, const cplx<R> *__restrict__ twg, R a,
               const cplx<R> *__restrict__ psi, cplx<R> *__restrict__ gT) {
-    using P = Plan<N>;
-    constexpr int ROWS = RowCfg<N, R>::ROWS;
+    using RC = RowCfg<N, R>;
+    using P = typename RC::P;
+    constexpr int ROWS = RC::ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + N + threadIdx.y * RowAddr::size(N);
+    cplx<R> *sm = tw + RC::TWN + threadIdx.y * RC::ROWSZ;
     const int t = threadIdx.x;
-    load_twiddles<R, N>(tw, twg, t + threadIdx.y * P::NT, P::NT * ROWS);
+    load_table<R>(tw, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
     const int y = blockIdx.x * ROWS + threadIdx.y;
     const size_t off = (size_t)blockIdx.y * N * N + (size_t)y * N;
     cplx<R> *row = state + off;
@@ -65,7 +67,7 @@ k_row_adjoint(cplx<R> *__restrict__ state, const cplx<R> *__restrict__ trans, co
 #pragma unroll
     for (int m = 0; m < P::E; m++) v[m] = row[t + m * P::NT];
     __syncthreads();
-    fft<R, N, +1>(v, sm, RowAddr(), t, tw);
+    row_transform<R, N, +1>(v, sm, t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) {
         const int x = t + m * P::NT;
@@ -73,7 +75,7 @@ k_row_adjoint(cplx<R> *__restrict__ state, const cplx<R> *__restrict__ trans, co
         gT[off + x] = cmulc(g, psi[off + x]);     // conj(psi) * g
         v[m] = cmulc(g, trow[x]);                 // conj(T) * g
     }
-    fft<R, N, -1>(v, sm, RowAddr(), t, tw);
+    row_transform<R, N, -1>(v, sm, t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) row[t + m * P::NT] = v[m];
 }

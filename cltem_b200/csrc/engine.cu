@@ -8,6 +8,7 @@
 #include "adjoint_ops.h"
 #include "draws.h"
 #include "fft.cuh"
+#include "fft_wide.cuh"
 #include "launch.cuh"
 #include "misc.cuh"
 #include "plain.h"
@@ -232,19 +233,31 @@ struct Ctx {
         auto &m = sizeof(R) == 4 ? tw_f : tw_d;
         auto it = m.find(n);
         if (it != m.end()) return (const cplx<R> *)it->second;
-        // packed per-stage table (fft.cuh, plan_tw_index): W_n^(r*k*n/(Ns*R)) = exp(-2 pi i r k / (Ns*R))
-        std::vector<cplx<R>> h(n, mk<R>(0, 0));
+        // entries [0, n): the radix-8 plan's packed per-stage table (fft.cuh, plan_tw_index),
+        // W_n^(r*k*n/(Ns*R)) = exp(-2 pi i r k / (Ns*R)); for sizes whose row passes use the wide two-stage
+        // plan (fft_wide.cuh) entries [n, 2n) hold its table, W_n^(r k) at k (R2 - 1) + r - 1
+        const bool wide = wide_plan<R>(n);
+        const size_t count = (size_t)n * (wide ? 2 : 1);
+        std::vector<cplx<R>> h(count, mk<R>(0, 0));
+        const long double two_pi = 2.0L * 3.14159265358979323846264338327950288L;
         for (int s = 1; s < plan_nstages(n); s++) {
             const int Ns = plan_ns(n, s), RAD = plan_radix(n, s);
             for (int k = 0; k < Ns; k++)
                 for (int r = 1; r < RAD; r++) {
-                    long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)(r * k) /
-                                    (long double)(Ns * RAD);
+                    long double a = -two_pi * (long double)(r * k) / (long double)(Ns * RAD);
                     h[plan_tw_index(n, s, k, r)] = mk<R>((R)std::cos(a), (R)std::sin(a));
                 }
         }
-        void *d = alloc(sizeof(cplx<R>) * n);
-        MS_CUDA(cudaMemcpy(d, h.data(), sizeof(cplx<R>) * n, cudaMemcpyHostToDevice));
+        if (wide) {
+            const int E = wide_E(n), R2 = n / E;
+            for (int k = 0; k < E; k++)
+                for (int r = 1; r < R2; r++) {
+                    long double a = -two_pi * (long double)(r * k) / (long double)n;
+                    h[n + k * (R2 - 1) + (r - 1)] = mk<R>((R)std::cos(a), (R)std::sin(a));
+                }
+        }
+        void *d = alloc(sizeof(cplx<R>) * count);
+        MS_CUDA(cudaMemcpy(d, h.data(), sizeof(cplx<R>) * count, cudaMemcpyHostToDevice));
         m[n] = d;
         return (const cplx<R> *)d;
     }

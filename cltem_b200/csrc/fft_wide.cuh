@@ -1,0 +1,134 @@
+// fft_wide.cuh — two-stage Stockham FFT with wide radices for the FP32 passes at 256, 512 and 1024.
+//
+// N = E * R2 (E = 32 for N = 512 / 1024, 16 for N = 256; R2 = N / E <= E); NT = N / E threads per
+// transform hold E elements each (v[m] = x[t + m*NT] on entry and exit, the layout of fft.cuh). Stage A is a
+// radix-E DFT of each thread's elements in registers; stage B a radix-R2 DFT of E/R2 butterflies per thread
+// with twiddles W_N^(r k) (butterfly k < E, 1 <= r < R2) read from a packed table at k (R2 - 1) + r - 1.
+// One shared-memory exchange per transform instead of the radix-8 plan's two (the passes are bound by
+// shared-memory traffic, not HBM). Shared layout: element i at (i / E)(E + 1) + i % E, rows of E padded by
+// one, which keeps stage A's row writes and stage B's column reads free of bank conflicts (times COLS for
+// a column tile, columns interleaved).
+#pragma once
+
+#include "fft.cuh"
+
+namespace ms {
+
+// the pass kernels at (precision, size) use the wide plan for FP32 at 256, 512 and 1024
+template <class R> __host__ __device__ constexpr bool wide_plan(int n) {
+    return sizeof(R) == 4 && (n == 256 || n == 512 || n == 1024);
+}
+__host__ __device__ constexpr int wide_E(int n) { return n >= 512 ? 32 : 16; }
+
+template <int N> struct WidePlan {
+    static constexpr int E = wide_E(N);
+    static constexpr int R2 = N / E;
+    static constexpr int NT = N / E;
+    static constexpr int NB = R2 > 0 ? E / R2 : 1;   // stage B butterflies per thread
+    static constexpr int TW = E * (R2 - 1);          // twiddle table entries
+    static constexpr int ROWSZ = NT * (E + 1);       // padded shared elements of one transform
+};
+
+template <int E> struct WideRowAddr {
+    __device__ __forceinline__ int operator()(int i) const { return (i / E) * (E + 1) + (i % E); }
+};
+template <int E, int COLS> struct WideColAddr {
+    __device__ __forceinline__ int operator()(int i) const { return ((i / E) * (E + 1) + (i % E)) * COLS; }
+};
+
+// cos(phi pi / 16) for any integer phi
+__device__ __forceinline__ double cos_pi16(int phi) {
+    constexpr double c16[17] = {1.0, 0.98078528040323044913, 0.92387953251128675613, 0.83146961230254523708,
+                                0.70710678118654752440, 0.55557023301960222474, 0.38268343236508977173,
+                                0.19509032201612826785, 0.0, -0.19509032201612826785, -0.38268343236508977173,
+                                -0.55557023301960222474, -0.70710678118654752440, -0.83146961230254523708,
+                                -0.92387953251128675613, -0.98078528040323044913, -1.0};
+    phi &= 31;
+    return phi <= 16 ? c16[phi] : c16[32 - phi];
+}
+// exp(SIGN 2 pi i e / M) for M = 16 or 32: the angle is j pi / 16 with j = (32 / M) e; sin(x) = cos(x - pi/2)
+template <class R, int SIGN, int M> __device__ __forceinline__ cplx<R> wconst(int e) {
+    const int j = (32 / M) * e;
+    return mk<R>((R)cos_pi16(j), (R)(SIGN * cos_pi16(j - 8)));
+}
+
+// 16-point DFT in registers as 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2
+template <class R, int SIGN> __device__ __forceinline__ void dft16(cplx<R> *a) {
+    cplx<R> b[16];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) {
+        cplx<R> x0 = a[n2], x1 = a[n2 + 4], x2 = a[n2 + 8], x3 = a[n2 + 12];
+        dft4<R, SIGN>(x0, x1, x2, x3);
+        b[n2 * 4 + 0] = x0;
+        b[n2 * 4 + 1] = cmul(x1, wconst<R, SIGN, 16>(n2 * 1));
+        b[n2 * 4 + 2] = cmul(x2, wconst<R, SIGN, 16>(n2 * 2));
+        b[n2 * 4 + 3] = cmul(x3, wconst<R, SIGN, 16>(n2 * 3));
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) {
+        cplx<R> y0 = b[k1], y1 = b[4 + k1], y2 = b[8 + k1], y3 = b[12 + k1];
+        dft4<R, SIGN>(y0, y1, y2, y3);
+        a[k1] = y0;
+        a[k1 + 4] = y1;
+        a[k1 + 8] = y2;
+        a[k1 + 12] = y3;
+    }
+}
+
+// 32-point DFT in registers: two 16-point DFTs of the even and odd elements and a radix-2 combination
+template <class R, int SIGN> __device__ __forceinline__ void dft32(cplx<R> *a) {
+    cplx<R> e[16], o[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) { e[k] = a[2 * k]; o[k] = a[2 * k + 1]; }
+    dft16<R, SIGN>(e);
+    dft16<R, SIGN>(o);
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        cplx<R> w = cmul(o[k], wconst<R, SIGN, 32>(k));
+        a[k] = cadd(e[k], w);
+        a[k + 16] = csub(e[k], w);
+    }
+}
+
+template <class R, int RAD, int SIGN> __device__ __forceinline__ void dft_wide(cplx<R> *a) {
+    static_assert(RAD == 16 || RAD == 32, "wide radices are 16 and 32");
+    if constexpr (RAD == 32) dft32<R, SIGN>(a);
+    else dft16<R, SIGN>(a);
+}
+
+// threads of one transform within one warp (row tiles of the wide plan)
+struct WarpSync {
+    __device__ __forceinline__ void operator()() const { __syncwarp(); }
+};
+
+// SIGN -1 forward, +1 inverse, unnormalised; sm: this transform's shared memory, ad its addressing
+template <class R, int N, int SIGN, class Addr, class Sync>
+__device__ __forceinline__ void fft_wide(cplx<R> (&v)[WidePlan<N>::E], cplx<R> *sm, Addr ad, int t, const cplx<R> *tw,
+                                         Sync sync) {
+    using P = WidePlan<N>;
+    constexpr int E = P::E, NT = P::NT, R2 = P::R2, NB = P::NB;
+    dft_wide<R, E, SIGN>(v);   // stage A (no twiddles)
+    sync();                    // the previous transform's reads of sm are done
+#pragma unroll
+    for (int m = 0; m < E; m++) sm[ad(t * E + m)] = v[m];
+    sync();
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        const int j = t + b * NT;   // butterfly index, < E
+        cplx<R> a[R2];
+#pragma unroll
+        for (int r = 0; r < R2; r++) {
+            cplx<R> x = sm[ad(j + r * E)];
+            if (r > 0) {
+                const cplx<R> w = tw[j * (R2 - 1) + (r - 1)];
+                x = (SIGN < 0) ? cmul(x, w) : cmulc(x, w);
+            }
+            a[r] = x;
+        }
+        dft_wide<R, R2, SIGN>(a);
+#pragma unroll
+        for (int m = 0; m < R2; m++) v[b + m * NB] = a[m];
+    }
+}
+
+}  // namespace ms

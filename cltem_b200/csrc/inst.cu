@@ -45,9 +45,9 @@ void ensure_attrs() {
 }
 
 inline dim3 row_grid(int batch) { return dim3(N / RC::ROWS, batch); }
-inline dim3 row_block() { return dim3(Plan<N>::NT, RC::ROWS); }
+inline dim3 row_block() { return dim3(RC::P::NT, RC::ROWS); }
 inline dim3 col_grid(int batch) { return dim3(N / CC::COLS, batch); }
-inline dim3 col_block() { return dim3(CC::COLS, Plan<N>::NT); }
+inline dim3 col_block() { return dim3(CC::COLS, CC::P::NT); }
 
 void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a, int xa, int xb,
               int load_all, const int *tsel, size_t tstride) {

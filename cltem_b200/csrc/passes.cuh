@@ -13,6 +13,9 @@
 #pragma once
 
 #include "fft.cuh"
+#include "fft_wide.cuh"
+
+#include <type_traits>
 
 namespace ms {
 
@@ -33,33 +36,67 @@ struct DetArgs {
     double *partials;       // [batch][n_det][gridDim.x]
 };
 
+// Row tiles: ROWS rows per block, P::NT threads per row (P the FFT plan: the wide two-stage plan for FP32
+// at 256 / 512 / 1024, fft_wide.cuh; the radix-8/4/2/3 Stockham plan otherwise, fft.cuh).
 template <int N, class R> struct RowCfg {
-    static constexpr int ROWS = N <= 128 ? 8 : (N <= 256 ? 8 : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1)));
+    static constexpr bool WIDE = wide_plan<R>(N);
+    using P = std::conditional_t<WIDE, WidePlan<N>, Plan<N>>;
+    static constexpr int ROWS = WIDE ? 8 : (N <= 128 ? 8 : (N <= 256 ? 8 : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1))));
     static_assert(N % ROWS == 0, "row tile must divide the grid");
-    static_assert(Plan<N>::NT * ROWS <= 1024, "row block too large");
-    static constexpr int THREADS = Plan<N>::NT * ROWS;
+    static_assert(P::NT * ROWS <= 1024, "row block too large");
+    static constexpr int THREADS = P::NT * ROWS;
     static_assert(ROWS <= 15, "one named barrier per row");
-    // a row's threads are whole warps, so each row can synchronise on its own named barrier
-    static constexpr bool NAMED = (Plan<N>::NT % 32) == 0 && ROWS > 1;
-    static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(N + ROWS * RowAddr::size(N)); }
+    // radix-8 plan: a row's threads are whole warps, so each row synchronises on its own named barrier;
+    // wide plan: a row's threads lie inside one warp (two rows per warp at 16 threads a row)
+    static constexpr bool NAMED = !WIDE && (P::NT % 32) == 0 && ROWS > 1;
+    static_assert(!WIDE || (P::NT == 32 || (P::NT == 16 && ROWS % 2 == 0)), "wide rows must tile whole warps");
+    static constexpr int TWN = WIDE ? WidePlan<N>::TW : N;   // twiddle entries staged in shared memory
+    static constexpr int TW_OFF = WIDE ? N : 0;               // offset of the row plan's table (Ctx::twiddles)
+    static constexpr int ROWSZ = WIDE ? WidePlan<N>::ROWSZ : RowAddr::size(N);
+    static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(TWN + ROWS * ROWSZ); }
 };
-// Columns per tile: a power of two dividing N. 512-thread blocks (two per SM) at the common sizes; a
-// tile row of COLS complex values is 64 B (FP32, N <= 512), two 32 B sectors.
+// Column tiles: COLS columns per block (a power of two dividing N), P::NT threads per column. Radix-8 plan:
+// 512-thread blocks at the common sizes, a tile row of COLS complex values 64 B (FP32, N <= 512). Wide plan:
+// 128-thread blocks. Columns use the radix-8 plan at every size: measured at 512^2 FP32, the wide plan's
+// column pass (4 x 128-thread blocks per SM) took 609 us per 512-wave launch against 558 us for the radix-8
+// tiles at 3 x 512 threads per SM, while the wide row pass took 470 us against 569 us.
+constexpr bool kWideColumns = false;
 template <int N, class R> struct ColCfg {
-    static constexpr int COLS = sizeof(R) == 4 ? (N <= 512 ? 8 : (N <= 1024 ? 4 : 2))
-                                               : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1));
+    static constexpr bool WIDE = kWideColumns && wide_plan<R>(N);
+    using P = std::conditional_t<WIDE, WidePlan<N>, Plan<N>>;
+    static constexpr int COLS = WIDE ? (N <= 512 ? 8 : 4)
+                                     : (sizeof(R) == 4 ? (N <= 512 ? 8 : (N <= 1024 ? 4 : 2))
+                                                       : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1)));
     static_assert(N % COLS == 0, "column tile must divide the grid");
-    static constexpr int THREADS = Plan<N>::NT * COLS;
+    static constexpr int THREADS = P::NT * COLS;
     static_assert(THREADS <= 1024, "column block too large");
-    static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(N + N * COLS); }
+    static constexpr int TWN = WIDE ? WidePlan<N>::TW : N;
+    static constexpr int COLSZ = WIDE ? WidePlan<N>::ROWSZ : N;   // shared elements of one column
+    static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(TWN + COLSZ * COLS); }
     // Blocks per SM the step pass is compiled for: 3 x 512 threads for the FP32 radix-8 plans (a 42-register
-    // budget; the 2 blocks of a 52-register build leave its global loads exposed), else what fits.
-    static constexpr int STEP_MINB = (sizeof(R) == 4 && Plan<N>::E == 8 && THREADS == 512) ? 3 : 1;
+    // budget; the 2 blocks of a 52-register build leave its global loads exposed), 4 x 128 threads for the
+    // wide plan (128 registers), else what fits.
+    static constexpr int STEP_MINB = WIDE ? 4 : ((sizeof(R) == 4 && Plan<N>::E == 8 && THREADS == 512) ? 3 : 1);
 };
 
-template <class R, int N>
-__device__ __forceinline__ void load_twiddles(cplx<R> *tw, const cplx<R> *__restrict__ twg, int tid, int nthreads) {
-    for (int i = tid; i < N; i += nthreads) tw[i] = twg[i];
+// the pass kernels' transforms over one row / one column tile (t: the thread's index within its transform)
+template <class R, int N, int SIGN>
+__device__ __forceinline__ void row_transform(cplx<R> (&v)[RowCfg<N, R>::P::E], cplx<R> *sm, int t, const cplx<R> *tw) {
+    using RC = RowCfg<N, R>;
+    if constexpr (RC::WIDE) fft_wide<R, N, SIGN>(v, sm, WideRowAddr<RC::P::E>(), t, tw, WarpSync());
+    else if constexpr (RC::NAMED) fft<R, N, SIGN>(v, sm, RowAddr(), t, tw, NamedSync{1 + (int)threadIdx.y, RC::P::NT});
+    else fft<R, N, SIGN>(v, sm, RowAddr(), t, tw);
+}
+template <class R, int N, int SIGN>
+__device__ __forceinline__ void col_transform(cplx<R> (&v)[ColCfg<N, R>::P::E], cplx<R> *sm, int t, const cplx<R> *tw) {
+    using CC = ColCfg<N, R>;
+    if constexpr (CC::WIDE) fft_wide<R, N, SIGN>(v, sm, WideColAddr<CC::P::E, CC::COLS>(), t, tw, BlockSync());
+    else fft<R, N, SIGN>(v, sm, ColAddr<CC::COLS, (int)sizeof(cplx<R>)>(), t, tw);
+}
+
+template <class R>
+__device__ __forceinline__ void load_table(cplx<R> *tw, const cplx<R> *__restrict__ twg, int count, int tid, int nthreads) {
+    for (int i = tid; i < count; i += nthreads) tw[i] = twg[i];
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -74,13 +111,14 @@ template <class R, int N>
 __global__ void __launch_bounds__(RowCfg<N, R>::THREADS)
 k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const cplx<R> *__restrict__ twg, R a,
            int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride) {
-    using P = Plan<N>;
-    constexpr int ROWS = RowCfg<N, R>::ROWS;
+    using RC = RowCfg<N, R>;
+    using P = typename RC::P;
+    constexpr int ROWS = RC::ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + N + threadIdx.y * RowAddr::size(N);
+    cplx<R> *sm = tw + RC::TWN + threadIdx.y * RC::ROWSZ;
     const int t = threadIdx.x;
-    load_twiddles<R, N>(tw, twg, t + threadIdx.y * P::NT, P::NT * ROWS);
+    load_table<R>(tw, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
     const int y = blockIdx.x * ROWS + threadIdx.y;
     cplx<R> *row = wave + (size_t)blockIdx.y * N * N + (size_t)y * N;
     // tsel (optional): transmission set of each wave; set k of this slice starts k * tstride after trans
@@ -92,18 +130,10 @@ k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const 
         v[m] = (load_all || x < xa || x >= xb) ? row[x] : mk<R>(0, 0);
     }
     __syncthreads();
-    if constexpr (RowCfg<N, R>::NAMED) {
-        const NamedSync sync{1 + (int)threadIdx.y, P::NT};
-        fft<R, N, +1>(v, sm, RowAddr(), t, tw, sync);
+    row_transform<R, N, +1>(v, sm, t, tw);
 #pragma unroll
-        for (int m = 0; m < P::E; m++) v[m] = cscale(cmul(v[m], trow[t + m * P::NT]), a);
-        fft<R, N, -1>(v, sm, RowAddr(), t, tw, sync);
-    } else {
-        fft<R, N, +1>(v, sm, RowAddr(), t, tw);
-#pragma unroll
-        for (int m = 0; m < P::E; m++) v[m] = cscale(cmul(v[m], trow[t + m * P::NT]), a);
-        fft<R, N, -1>(v, sm, RowAddr(), t, tw);
-    }
+    for (int m = 0; m < P::E; m++) v[m] = cscale(cmul(v[m], trow[t + m * P::NT]), a);
+    row_transform<R, N, -1>(v, sm, t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) {
         const int x = t + m * P::NT;
@@ -115,21 +145,21 @@ k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const 
 template <class R, int N, int SIGN>
 __global__ void __launch_bounds__(RowCfg<N, R>::THREADS)
 k_row_fft(const cplx<R> *in, cplx<R> *out, const cplx<R> *__restrict__ twg, R scale) {
-    using P = Plan<N>;
-    constexpr int ROWS = RowCfg<N, R>::ROWS;
+    using RC = RowCfg<N, R>;
+    using P = typename RC::P;
+    constexpr int ROWS = RC::ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + N + threadIdx.y * RowAddr::size(N);
+    cplx<R> *sm = tw + RC::TWN + threadIdx.y * RC::ROWSZ;
     const int t = threadIdx.x;
-    load_twiddles<R, N>(tw, twg, t + threadIdx.y * P::NT, P::NT * ROWS);
+    load_table<R>(tw, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
     const int y = blockIdx.x * ROWS + threadIdx.y;
     const size_t off = (size_t)blockIdx.y * N * N + (size_t)y * N;
     cplx<R> v[P::E];
 #pragma unroll
     for (int m = 0; m < P::E; m++) v[m] = in[off + t + m * P::NT];
     __syncthreads();
-    if constexpr (RowCfg<N, R>::NAMED) fft<R, N, SIGN>(v, sm, RowAddr(), t, tw, NamedSync{1 + (int)threadIdx.y, P::NT});
-    else fft<R, N, SIGN>(v, sm, RowAddr(), t, tw);
+    row_transform<R, N, SIGN>(v, sm, t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) out[off + t + m * P::NT] = cscale(v[m], scale);
 }
@@ -138,14 +168,16 @@ k_row_fft(const cplx<R> *in, cplx<R> *out, const cplx<R> *__restrict__ twg, R sc
 // Column kernels: grid (res/COLS, batch), block (COLS, NT)
 // ------------------------------------------------------------------------------------------------
 template <class R, int N>
-__device__ __forceinline__ void col_load(cplx<R> (&v)[Plan<N>::E], const cplx<R> *base, int x, int t) {
+__device__ __forceinline__ void col_load(cplx<R> (&v)[ColCfg<N, R>::P::E], const cplx<R> *base, int x, int t) {
+    using P = typename ColCfg<N, R>::P;
 #pragma unroll
-    for (int m = 0; m < Plan<N>::E; m++) v[m] = base[(size_t)(t + m * Plan<N>::NT) * N + x];
+    for (int m = 0; m < P::E; m++) v[m] = base[(size_t)(t + m * P::NT) * N + x];
 }
 template <class R, int N>
-__device__ __forceinline__ void col_store(const cplx<R> (&v)[Plan<N>::E], cplx<R> *base, int x, int t) {
+__device__ __forceinline__ void col_store(const cplx<R> (&v)[ColCfg<N, R>::P::E], cplx<R> *base, int x, int t) {
+    using P = typename ColCfg<N, R>::P;
 #pragma unroll
-    for (int m = 0; m < Plan<N>::E; m++) base[(size_t)(t + m * Plan<N>::NT) * N + x] = v[m];
+    for (int m = 0; m < P::E; m++) base[(size_t)(t + m * P::NT) * N + x] = v[m];
 }
 
 // Block-wide sum of one double per thread; the result is valid in thread 0. red: >= 32 doubles.
@@ -173,21 +205,22 @@ template <class R, int N, int MODE>
 __global__ void __launch_bounds__(ColCfg<N, R>::THREADS, ColCfg<N, R>::STEP_MINB)
 k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTables<R> pt, R bscale, R det_scale,
            DetArgs det, cplx<R> *__restrict__ recip_out, int tiles_lo) {
-    using P = Plan<N>;
-    constexpr int COLS = ColCfg<N, R>::COLS;
+    using CC = ColCfg<N, R>;
+    using P = typename CC::P;
+    constexpr int COLS = CC::COLS;
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double red[32];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + N + threadIdx.x;
+    cplx<R> *sm = tw + CC::TWN + threadIdx.x;
     const int c = threadIdx.x, t = threadIdx.y;
-    load_twiddles<R, N>(tw, twg, c + t * COLS, COLS * P::NT);
+    load_table<R>(tw, twg, CC::TWN, c + t * COLS, COLS * P::NT);
     const int tile = (int)blockIdx.x < tiles_lo ? (int)blockIdx.x : N / COLS - ((int)gridDim.x - (int)blockIdx.x);
     const int x = tile * COLS + c;
     cplx<R> *base = wave + (size_t)blockIdx.y * N * N;
     cplx<R> v[P::E];
     col_load<R, N>(v, base, x, t);
     __syncthreads();
-    fft<R, N, -1>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
+    col_transform<R, N, -1>(v, sm, t, tw);
     const cplx<R> pxx = pt.px[x];
     const double kx2 = pt.kx2[x];
 #pragma unroll
@@ -224,7 +257,7 @@ k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTabl
     if constexpr (MODE != COL_DET_ONLY) {
 #pragma unroll
         for (int m = 0; m < P::E; m++) v[m] = cscale(v[m], bscale);
-        fft<R, N, +1>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
+        col_transform<R, N, +1>(v, sm, t, tw);
         col_store<R, N>(v, base, x, t);
     }
 }
@@ -233,19 +266,20 @@ k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTabl
 template <class R, int N, int SIGN>
 __global__ void __launch_bounds__(ColCfg<N, R>::THREADS)
 k_col_fft(const cplx<R> *in, cplx<R> *out, const cplx<R> *__restrict__ twg, R scale) {
-    using P = Plan<N>;
-    constexpr int COLS = ColCfg<N, R>::COLS;
+    using CC = ColCfg<N, R>;
+    using P = typename CC::P;
+    constexpr int COLS = CC::COLS;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + N + threadIdx.x;
+    cplx<R> *sm = tw + CC::TWN + threadIdx.x;
     const int c = threadIdx.x, t = threadIdx.y;
-    load_twiddles<R, N>(tw, twg, c + t * COLS, COLS * P::NT);
+    load_table<R>(tw, twg, CC::TWN, c + t * COLS, COLS * P::NT);
     const int x = blockIdx.x * COLS + c;
     const size_t off = (size_t)blockIdx.y * N * N;
     cplx<R> v[P::E];
     col_load<R, N>(v, in + off, x, t);
     __syncthreads();
-    fft<R, N, SIGN>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
+    col_transform<R, N, SIGN>(v, sm, t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) v[m] = cscale(v[m], scale);
     col_store<R, N>(v, out + off, x, t);
@@ -257,26 +291,27 @@ template <class R, int N>
 __global__ void __launch_bounds__(ColCfg<N, R>::THREADS)
 k_col_bandlimit(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, const double *__restrict__ kx2,
                 const double *__restrict__ ky2, double lim, R scale) {
-    using P = Plan<N>;
-    constexpr int COLS = ColCfg<N, R>::COLS;
+    using CC = ColCfg<N, R>;
+    using P = typename CC::P;
+    constexpr int COLS = CC::COLS;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + N + threadIdx.x;
+    cplx<R> *sm = tw + CC::TWN + threadIdx.x;
     const int c = threadIdx.x, t = threadIdx.y;
-    load_twiddles<R, N>(tw, twg, c + t * COLS, COLS * P::NT);
+    load_table<R>(tw, twg, CC::TWN, c + t * COLS, COLS * P::NT);
     const int x = blockIdx.x * COLS + c;
     cplx<R> *base = wave + (size_t)blockIdx.y * N * N;
     cplx<R> v[P::E];
     col_load<R, N>(v, base, x, t);
     __syncthreads();
-    fft<R, N, -1>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
+    col_transform<R, N, -1>(v, sm, t, tw);
     const double k2x = kx2[x];
 #pragma unroll
     for (int m = 0; m < P::E; m++) {
         double k = sqrt(k2x + ky2[t + m * P::NT]);
         v[m] = cscale(v[m], (k <= lim) ? scale : (R)0);
     }
-    fft<R, N, +1>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
+    col_transform<R, N, +1>(v, sm, t, tw);
     col_store<R, N>(v, base, x, t);
 }
 
@@ -289,13 +324,14 @@ __global__ void __launch_bounds__(ColCfg<N, R>::THREADS)
 k_col_probe(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, const double2 *__restrict__ chi,
             const double *__restrict__ kx, const double *__restrict__ ky, const double2 *__restrict__ pos, R scale,
             const double *__restrict__ dfac, double wl) {
-    using P = Plan<N>;
-    constexpr int COLS = ColCfg<N, R>::COLS;
+    using CC = ColCfg<N, R>;
+    using P = typename CC::P;
+    constexpr int COLS = CC::COLS;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + N + threadIdx.x;
+    cplx<R> *sm = tw + CC::TWN + threadIdx.x;
     const int c = threadIdx.x, t = threadIdx.y;
-    load_twiddles<R, N>(tw, twg, c + t * COLS, COLS * P::NT);
+    load_table<R>(tw, twg, CC::TWN, c + t * COLS, COLS * P::NT);
     const int x = blockIdx.x * COLS + c;
     const double2 pp = pos[blockIdx.y];
     // dfac (optional): pi * defocus change / wavelength of each wave; the aberration phase gains
@@ -327,7 +363,7 @@ k_col_probe(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, const d
         }
     }
     __syncthreads();
-    fft<R, N, +1>(v, sm, ColAddr<COLS, (int)sizeof(cplx<R>)>(), t, tw);
+    col_transform<R, N, +1>(v, sm, t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) v[m] = cscale(v[m], scale);
     col_store<R, N>(v, wave + (size_t)blockIdx.y * N * N, x, t);
