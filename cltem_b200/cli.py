@@ -8,14 +8,15 @@ for STEM one image per detector, for CBED Diff; float32 TIFFs (fileio.h:43-76) p
 each, and _NNN suffixes for intermediate-slice stacks (main.cpp:158-191).
 
 Differences from clTEM_cmd, by design: OpenCL devices and math flags (-d platform:device, -f) do not apply
-(-d takes CUDA device indices, "gpu"/"default" or "all"/"gpus"; -f is accepted and ignored); .cif input
-and its supercell options are not part of this engine; the frozen-phonon random draws take an explicit
-seed (--seed) instead of the wall clock.
+(-d takes CUDA device indices, "gpu"/"default" or "all"/"gpus"; -f is accepted and ignored); the
+frozen-phonon, occupancy and incoherence draws take an explicit seed (--seed) instead of the wall clock.
+A .cif structure takes the reference's supercell options: -s wx,wy,wz (Å) and -z u,v,w are required,
+-n u,v,w (the lattice direction along x) and -t tx,ty,tz (degrees) are optional, --fix repairs common
+file errors.
 """
 import argparse
 import copy
 import json
-import math
 import os
 import sys
 import threading
@@ -26,7 +27,7 @@ import numpy as np
 from . import abi
 from .config import read_config
 from .params import read_params, read_params_json, default_bundle_path
-from .structure import phonon_configs, read_xyz
+from .structure import frozen_phonon_configs, read_xyz
 from .tiff import write_tiff
 
 VERSION = "mslice-b200 CLI 1"
@@ -90,9 +91,34 @@ def _load_params(name, params_dir):
     return bundle[name]
 
 
-def _phonon_u2(raw_json):
-    ph = raw_json.get("incoherence", {}).get("inelastic scattering", {}).get("phonon", {})
-    return float(ph.get("default", {}).get("value", 0.0)), bool(ph.get("force default", True))
+def _three(arg, what):
+    """parseThreeCommaList (main.cpp:109-133): exactly three comma-separated numbers."""
+    try:
+        v = [float(t) for t in arg.split(",")]
+    except ValueError:
+        v = []
+    if len(v) != 3:
+        raise ValueError(f"Could not parse .cif {what} argument: {arg}")
+    return tuple(v)
+
+
+def _cif_info(a):
+    """The supercell options of a .cif input (main.cpp:416-458): -s and -z required, -n and -t optional."""
+    from .cif import SuperCellInfo
+    errs = []
+    if not a.size:
+        errs.append(".cif files require a size arg (-s, --size)")
+    if not a.zone:
+        errs.append(".cif files require a zone axis arg (-z, --zone)")
+    info = SuperCellInfo()
+    for attr, arg, what in (("widths", a.size, "size"), ("uvw", a.zone, "zone"), ("abc", a.normal, "normal"),
+                            ("tilts", a.tilts, "tilt")):
+        if arg:
+            try:
+                setattr(info, attr, _three(arg, what))
+            except ValueError as e:
+                errs.append(str(e))
+    return info, errs
 
 
 def _load_ccd(name, ccds_dir):
@@ -168,14 +194,25 @@ def main(argv=None):
     if not a.structure or not a.config or not a.output:
         print("usage: python -m cltem_b200 structure_file -c config.json -o output_dir [-d device]", file=sys.stderr)
         return 1
-    if a.structure.lower().endswith(".cif") or a.size or a.zone:
-        print("CIF input and supercell construction are not supported by this engine; give an .xyz file",
-              file=sys.stderr)
+    is_xyz, is_cif = a.structure.endswith(".xyz"), a.structure.endswith(".cif")
+    if not is_xyz and not is_cif:
+        print(f"Require a .xyz or .cif file non-option argument. Instead got: {a.structure}", file=sys.stderr)
         return 1
+    if is_cif:
+        info, errs = _cif_info(a)
+        if errs:
+            print("\n".join(errs), file=sys.stderr)
+            return 1
+    elif a.size or a.zone or a.normal or a.tilts:
+        print("WARNING: .cif options have been set for .xyz file, these will be ignored", file=sys.stderr)
     with open(a.config) as f:
         raw = json.load(f)
     settings = read_config(raw)
-    structure = read_xyz(a.structure, seed=a.seed)
+    if is_cif:
+        from .cif import read_cif_structure
+        structure = read_cif_structure(a.structure, info, fix=a.fix, seed=a.seed)
+    else:
+        structure = read_xyz(a.structure, seed=a.seed)
     settings.attach_structure(structure)
     params = _load_params(settings.potentials, a.params)
     from .engine import geometry
@@ -191,12 +228,8 @@ def main(argv=None):
     by_pass = mixed or (not settings.phonon_enabled and iters > 1)
     n_conf = settings.cfg.mixed_static if mixed else (iters if settings.phonon_enabled else 1)
     settings.cfg.iterations = iters if by_pass else 0
-    u2, force_default = _phonon_u2(raw)
     if settings.phonon_enabled:
-        if structure.u2 is not None and not force_default:
-            configs = phonon_configs(structure, n_conf, 0.0, seed=a.seed)
-        else:
-            configs = phonon_configs(structure, n_conf, math.sqrt(max(u2, 0.0)), seed=a.seed)
+        configs = frozen_phonon_configs(structure, n_conf, settings.vibrations, seed=a.seed)
     else:
         configs = [structure]
 

@@ -32,6 +32,28 @@ def _try(j, setter, *keys, conv=lambda v: v):
         return False
 
 
+def _read_vibrations(j, default):
+    """JsonToThermalVibrations (src/simulation/utilities/jsonutils.cpp:368-418): flags default to false;
+    per-element values that are not numbers (the "units" entry) are skipped."""
+    from .structure import Vibrations, symbol_to_z
+    v = Vibrations(default=float(default))
+    ph = ("incoherence", "inelastic scattering", "phonon")
+    _try(j, lambda b: setattr(v, "force_default", b), *ph, "force default", conv=bool)
+    _try(j, lambda b: setattr(v, "force_xyz", b), *ph, "force xyz displacements", conv=bool)
+    _try(j, lambda b: setattr(v, "force_defined", b), *ph, "override file", conv=bool)
+    try:
+        table = _get(j, *ph, "values")
+        for name, val in (table.items() if isinstance(table, dict) else []):
+            if isinstance(val, (int, float)) and not isinstance(val, bool):
+                try:
+                    v.values[symbol_to_z(name)] = float(val)
+                except RuntimeError:
+                    pass
+    except (KeyError, TypeError):
+        pass
+    return v
+
+
 class SimulationSettings:
     """Host-side view of a clTEM simulation (the subset of SimulationManager the path reads)."""
 
@@ -42,6 +64,7 @@ class SimulationSettings:
         self.iterations = 1
         self.phonon_enabled = False
         self.phonon_default_u2 = 0.0
+        self.vibrations = None       # structure.Vibrations, set by read_config
         self.parallel_pixels = 1
         self.ccd_name = ""          # "ctem/ccd/name" ("" or "Perfect": no dose simulation)
         self.ccd_dose = 10000.0     # e- per Å^2 (SimulationManager default)
@@ -174,6 +197,7 @@ def read_config(path_or_dict) -> SimulationSettings:
     ph = ("incoherence", "inelastic scattering", "phonon")
     _try(j, lambda v: setattr(s, "phonon_enabled", v), *ph, "enabled", conv=bool)
     _try(j, lambda v: setattr(s, "phonon_default_u2", v), *ph, "default", "value", conv=float)
+    s.vibrations = _read_vibrations(j, s.phonon_default_u2)
     # mixed static potentials (jsonutils.cpp:319-326; SimulationManager::useParallelPotentials)
     _try(j, lambda v: setattr(s, "mixed_static_count", v), *ph, "mixed static potentials", "count", conv=int)
     _try(j, lambda v: setattr(s, "mixed_static_enabled", v), *ph, "mixed static potentials", "enabled", conv=bool)

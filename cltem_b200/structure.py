@@ -44,6 +44,8 @@ class Structure:
     u2: np.ndarray = None  # optional per-atom mean-square displacement (Å^2) per axis, float64[n,3]
     name: str = ""
     extra: dict = field(default_factory=dict)
+    defined_u: np.ndarray = None  # bool[n]: u2 row given by the file (None: every row when u2 is set)
+    axes: np.ndarray = None       # float64[3,3]: rows u1, u2, u3, the displacement axes (None: x, y, z)
 
     def __len__(self):
         return int(self.Z.shape[0])
@@ -63,13 +65,12 @@ def _stof(s: str) -> float:
     return float(np.float32(float(s)))
 
 
-def read_xyz(path: str, seed: int = 0) -> Structure:
+def read_xyz(path: str, seed: int = 0, occupancy_draw: str = "normal") -> Structure:
     """Read a clTEM .xyz file (CrystalStructure::openXyz, src/simulation/structure/crystalstructure.cpp:44-173):
     atom count, a header line of column names (A x y z [occ] [u] [u1 u2 u3], optional "nm" for nanometre units,
     or no names for the A x y z default), then one atom per line, coordinates parsed as std::stof does.
-    With an occ column, consecutive atoms at the same position form one site; a uniform draw from a
-    generator seeded by `seed` keeps the atom whose cumulative occupancy interval holds it, or none
-    (processOccupancyList, :214-236; the reference's generator is clock-seeded)."""
+    With an occ column, consecutive atoms at the same position form one site resolved by one draw from a
+    generator seeded by `seed` (process_occupancy; the reference's generator is clock-seeded)."""
     with open(path, "r") as f:
         lines = f.read().splitlines()
     try:
@@ -128,17 +129,24 @@ def read_xyz(path: str, seed: int = 0) -> Structure:
         raise RuntimeError(f"Number of atoms does not match .xyz first line: {i} instead of {n}")
     keep = np.arange(len(Z))
     if hocc != -1:
-        keep = _process_occupancy(X, Y, Zc, OCC, np.random.default_rng(seed))
+        keep = process_occupancy(X, Y, Zc, OCC, np.random.default_rng(seed), occupancy_draw)
     U = np.asarray(U) if defined_u else None
     return Structure(np.asarray(Z, np.int32)[keep], np.asarray(X)[keep], np.asarray(Y)[keep], np.asarray(Zc)[keep],
                      U[keep] if U is not None else None, name=path)
 
 
-def _process_occupancy(X, Y, Zc, occ, rng):
-    """Indices kept by CrystalStructure::processOccupancyList over runs of consecutive atoms at one position:
-    a single fully occupied atom is kept; otherwise one uniform r in [0, 1) keeps the atom whose interval
-    [sum of earlier occupancies, + its own) holds r (or the last, when r = 1 and the sum is exactly 1), and a
-    site whose occupancies add up to more than 1 is an error."""
+def process_occupancy(X, Y, Zc, occ, rng, draw: str = "normal"):
+    """Indices kept by CrystalStructure::processOccupancyList (crystalstructure.cpp:214-236) over runs of
+    consecutive atoms at one position: a single fully occupied atom is kept; otherwise one draw r keeps the
+    atom whose interval [sum of earlier occupancies, + its own) holds r (or the last, when r = 1 and the sum
+    is exactly 1), and a site whose occupancies add up to more than 1 is an error.
+
+    draw="normal" takes r from a standard normal, as the reference does (its `dist` is a
+    std::normal_distribution<>(0, 1), crystalstructure.h:59), so a site keeps an atom with probability
+    Phi(total occupancy) - 1/2 at most; draw="uniform" takes r uniform on [0, 1), which keeps each atom with
+    the probability of its occupancy."""
+    if draw not in ("normal", "uniform"):
+        raise ValueError("occupancy draw must be 'normal' or 'uniform'")
     keep = []
     i, n = 0, len(X)
     while i < n:
@@ -148,7 +156,7 @@ def _process_occupancy(X, Y, Zc, occ, rng):
         if j - i == 1 and occ[i] == 1.0:
             keep.append(i)
         else:
-            r = float(rng.random())
+            r = float(rng.standard_normal()) if draw == "normal" else float(rng.random())
             total = 0.0
             for k in range(i, j):
                 if (total <= r < total + occ[k]) or (r == 1.0 and total + occ[k] == 1.0):
@@ -192,19 +200,71 @@ def _tile(basis, a, nx, ny, nz, name):
                      np.asarray(W, np.float64), name=f"{name}_{nx}x{ny}x{nz}")
 
 
-def phonon_configs(s: Structure, n_configs: int, u_rms: float, seed: int = 0):
-    """n_configs frozen-phonon configurations: each atom displaced by N(0, u_rms^2) per axis, FP64,
-    configuration c drawn from numpy's PCG64 seeded with (seed, c)."""
+def _displaced(s: Structure, sd: np.ndarray, n_configs: int, seed: int, axes=None):
     out = []
     for c in range(n_configs):
         rng = np.random.Generator(np.random.PCG64([seed, c]))
-        if s.u2 is not None:
-            sd = np.sqrt(s.u2)
-        else:
-            sd = np.full((len(s), 3), float(u_rms))
         d = rng.standard_normal((len(s), 3)) * sd
-        out.append(Structure(s.Z.copy(), s.x + d[:, 0], s.y + d[:, 1], s.z + d[:, 2], name=f"{s.name}#ph{c}"))
+        if axes is None:
+            x, y, z = s.x + d[:, 0], s.y + d[:, 1], s.z + d[:, 2]
+        else:   # x + d1 u1 + d2 u2 + d3 u3 (simulationgeneral.cpp:196-202)
+            u1, u2, u3 = (np.asarray(a, dtype=np.float64) for a in axes)
+            x = s.x + d[:, 0] * u1[0] + d[:, 1] * u2[0] + d[:, 2] * u3[0]
+            y = s.y + d[:, 0] * u1[1] + d[:, 1] * u2[1] + d[:, 2] * u3[1]
+            z = s.z + d[:, 0] * u1[2] + d[:, 1] * u2[2] + d[:, 2] * u3[2]
+        out.append(Structure(s.Z.copy(), x, y, z, name=f"{s.name}#ph{c}"))
     return out
+
+
+def phonon_configs(s: Structure, n_configs: int, u_rms: float, seed: int = 0):
+    """n_configs frozen-phonon configurations: each atom displaced by N(0, u_rms^2) per axis (or by the
+    structure's own u2 when it has one), FP64, configuration c drawn from numpy's PCG64 seeded with
+    (seed, c)."""
+    sd = np.sqrt(s.u2) if s.u2 is not None else np.full((len(s), 3), float(u_rms))
+    return _displaced(s, sd, n_configs, seed)
+
+
+@dataclass
+class Vibrations:
+    """Thermal-vibration settings of PhononScattering (src/simulation/incoherence/inelastic/phonon.cpp,
+    read by JsonToThermalVibrations, src/simulation/utilities/jsonutils.cpp:368-418)."""
+    default: float = 0.0          # Å^2, "default"/"value": every element not in `values`
+    values: dict = field(default_factory=dict)   # atomic number -> Å^2 ("values")
+    force_default: bool = False   # "force default"
+    force_defined: bool = False   # "override file": the element table over the file's values
+    force_xyz: bool = False       # "force xyz displacements": x, y, z axes over the structure's
+
+    def vibration(self, Z: np.ndarray) -> np.ndarray:
+        """PhononScattering::getVibrations for each atomic number."""
+        table = np.full(max(int(np.max(Z, initial=0)), max(self.values, default=0)) + 1, float(self.default))
+        for k, v in self.values.items():
+            table[int(k)] = float(v)
+        return table[np.asarray(Z, dtype=np.int64)]
+
+    def mean_square(self, s: Structure) -> np.ndarray:
+        """Per atom and axis the u^2 PhononScattering::generateTdsFactor (phonon.cpp:98-128) takes: the
+        default when forced, else the element table when the file is overridden, else the file's value for
+        atoms that define one, else the element table."""
+        n = len(s)
+        if self.force_default:
+            return np.full((n, 3), float(self.default))
+        table = np.repeat(self.vibration(s.Z)[:, None], 3, axis=1)
+        if self.force_defined or s.u2 is None:
+            return table
+        defined = np.ones(n, dtype=bool) if s.defined_u is None else np.asarray(s.defined_u, dtype=bool)
+        return np.where(defined[:, None], np.asarray(s.u2, dtype=np.float64), table)
+
+
+def frozen_phonon_configs(s: Structure, n_configs: int, vib: Vibrations, seed: int = 0):
+    """n_configs frozen-phonon configurations as SimulationGeneral::sortAtoms makes one
+    (simulationgeneral.cpp:177-205): per atom three deviates sqrt(u^2) N(0, 1) along the structure's
+    displacement axes (its rotated cell vectors for a CIF supercell; x, y, z for .xyz input or when
+    forced), with u^2 from Vibrations.mean_square. Configuration c draws from numpy's PCG64 seeded with
+    (seed, c); the reference's generator is clock-seeded."""
+    with np.errstate(invalid="ignore"):
+        sd = np.sqrt(vib.mean_square(s))
+    axes = None if (vib.force_xyz or s.axes is None) else s.axes
+    return _displaced(s, sd, n_configs, seed, axes)
 
 
 def concat_configs(configs):

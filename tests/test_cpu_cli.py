@@ -97,11 +97,16 @@ def test_xyz_site_occupancy(tmp_path):
         lines.append(f"O {k}.5 0.0 0.0 1.0")      # a full site of its own
     p = tmp_path / "occ.xyz"
     p.write_text(f"{len(lines)}\nA x y z occ\n" + "\n".join(lines) + "\n")
-    s = read_xyz(str(p), seed=3)
+    s = read_xyz(str(p), seed=3, occupancy_draw="uniform")
     z = np.asarray(s.Z)
     assert (z == 8).sum() == 400
     n_sr, n_ti = (z == 38).sum(), (z == 22).sum()
     assert abs(n_sr - 200) < 45 and abs(n_ti - 100) < 35 and n_sr + n_ti < 400
+    # the reference's draw is a standard normal: Sr kept with P(0 <= r < 1/2) = 0.191, Ti with 0.082
+    s = read_xyz(str(p), seed=3)
+    z = np.asarray(s.Z)
+    n_sr, n_ti = (z == 38).sum(), (z == 22).sum()
+    assert abs(n_sr - 76.6) < 28 and abs(n_ti - 32.8) < 19 and (z == 8).sum() == 400
     # one atom per site at most, and the draw is repeatable
     xs = np.asarray(s.x)[z != 8]
     assert len(np.unique(xs)) == len(xs)

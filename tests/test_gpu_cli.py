@@ -65,3 +65,35 @@ def test_cli_ctem_outputs(tmp_path):
         assert nm + ".tif" in files and nm + ".json" in files
     amp, _ = read_tiff(str(out / "EW_amplitude.tif"))
     assert amp.shape == (256, 256) and np.all(np.isfinite(amp))
+
+
+def test_cli_cif_supercell_ctem_matches_engine(tmp_path):
+    from cltem_b200.cif import SuperCellInfo, read_cif_structure
+    from tests.test_cpu_cif import PEROVSKITE
+    cif = tmp_path / "sto.cif"
+    cif.write_text(PEROVSKITE)
+    cfg = _cfg_json()
+    cfg["mode"] = {"id": 1, "name": "CTEM"}
+    cfg["maintain areas"] = False
+    cfg["ctem"] = {"simulate image": False}
+    cfg["intermediate output"] = {"enabled": False, "slice interval": 0}
+    cfg["incoherence"]["inelastic scattering"]["phonon"]["enabled"] = False
+    cj = tmp_path / "c.json"
+    cj.write_text(json.dumps(cfg))
+    out = tmp_path / "out"
+    args = [str(cif), "-c", str(cj), "-o", str(out), "-s", "15.5,15.5,8", "-z", "0,0,1", "-n", "1,0,0"]
+    assert cli_main(args) == 0
+    amp, _ = read_tiff(str(out / "EW_amplitude.tif"))
+    st = read_cif_structure(str(cif), SuperCellInfo(uvw=(0, 0, 1), abc=(1, 0, 0), widths=(15.5, 15.5, 8)))
+    # Sr on 4 x 4 x 3 lattice points (z = 8 is inside [0, 8] by rounding), Ti 4 x 4 x 2, O 48 + 32 + 32
+    assert [(st.Z == z).sum() for z in (38, 22, 8)] == [48, 32, 112]
+    s = read_config(cfg)
+    s.attach_structure(st)
+    ctx = Context(0)
+    ctx.load_params(load_default("kirkland"))
+    sim = Simulation(ctx, s.cfg)
+    sim.set_atoms(st)
+    ew, _, _ = sim.ctem()
+    assert np.allclose(amp, np.abs(ew[-1]).astype(np.float32), rtol=1e-6, atol=1e-6)
+    sim.close()
+    ctx.close()
