@@ -11,6 +11,7 @@ attach_structure mirrors SimulationManager::setStructure (simulationmanager.cpp:
 centre.
 """
 import json
+from dataclasses import dataclass
 import math
 
 from . import abi
@@ -30,6 +31,37 @@ def _try(j, setter, *keys, conv=lambda v: v):
         return True
     except (KeyError, TypeError, ValueError):
         return False
+
+
+@dataclass
+class PlasmonSettings:
+    """PlasmonScattering's settings (src/simulation/incoherence/inelastic/plasmon.h, read by
+    jsonutils.cpp:331-360; mean free path converted from nm to Å).
+
+    Enabling plasmons changes no result in the reference: its scattering depths are never generated
+    (PlasmonScattering::initDepthVectors and generateScatteringDepths have no callers), so
+    getGeneratedDepth always returns +inf and modifyBeamTilt is never reached
+    (simulationstem.cpp:191-232, simulationcbed.cpp:145-187, simulationctem.cpp:316-357). What enabling
+    them does change is reproduced here: the incoherence iterations count (IncoherentEffects::enabled) and
+    mixed static potentials are off (precalculateTransmission is false, so parallelPotentialsCount is 1)."""
+    enabled: bool = False
+    kind: str = "full"             # "full" or "individual"
+    individual: int = 1
+    mean_free_path: float = 100.0  # Å (10 nm)
+    characteristic_angle: float = 1.0   # mrad
+    critical_angle: float = 0.1         # mrad
+
+
+def _read_plasmon(j):
+    p = PlasmonSettings()
+    pl = ("incoherence", "inelastic scattering", "plasmon")
+    _try(j, lambda v: setattr(p, "enabled", v), *pl, "enabled", conv=bool)
+    _try(j, lambda v: setattr(p, "kind", v if v in ("full", "individual") else p.kind), *pl, "type", conv=str)
+    _try(j, lambda v: setattr(p, "individual", v), *pl, "individual", conv=int)
+    _try(j, lambda v: setattr(p, "mean_free_path", v * 10.0), *pl, "mean free path", "value", conv=float)
+    _try(j, lambda v: setattr(p, "characteristic_angle", v), *pl, "characteristic angle", "value", conv=float)
+    _try(j, lambda v: setattr(p, "critical_angle", v), *pl, "critical angle", "value", conv=float)
+    return p
 
 
 def _read_vibrations(j, default):
@@ -71,14 +103,32 @@ class SimulationSettings:
         self.ccd_binning = 1
         self.mixed_static_count = 1
         self.mixed_static_enabled = False
+        self.precalculate_transmission = True   # "precalculate transmission" (SimulationManager default)
+        self.plasmon = PlasmonSettings()
         self.detectors = []
 
     def effective_iterations(self) -> int:
         """IncoherentEffects::iterations (src/simulation/incoherence/incoherenteffects.h:40-54): the stored
-        count when any effect of the mode is on (phonons; chromatic or source size outside CTEM), else 1."""
+        count when any effect of the mode is on (phonons or plasmons; chromatic or source size outside
+        CTEM), else 1."""
         c = self.cfg
-        on = self.phonon_enabled or (c.mode != abi.MODE_CTEM and (c.chromatic or c.source_size))
+        on = self.phonon_enabled or self.plasmon.enabled or (c.mode != abi.MODE_CTEM and (c.chromatic or c.source_size))
         return max(1, int(self.iterations)) if on else 1
+
+    def mixed_static_sets(self) -> int:
+        """SimulationManager::useParallelPotentials / parallelPotentialsCount (simulationmanager.h:185-232):
+        mixed static potentials need frozen phonons and precalculated transmissions (which plasmons turn
+        off); STEM uses them only with the static frame, the other modes only when there are fewer sets
+        than iterations. Returns the set count, or 0 when the reference would not use them."""
+        c = self.cfg
+        precalc = self.precalculate_transmission and not self.plasmon.enabled
+        do_parallel = self.phonon_enabled and precalc and self.mixed_static_enabled
+        n = int(self.mixed_static_count)
+        if c.mode == abi.MODE_STEM:
+            count = n if (do_parallel and not c.stem_moving_frame) else 1
+        else:
+            count = n if (do_parallel and n < self.effective_iterations()) else 1
+        return count if (self.mixed_static_enabled and count > 1) else 0
 
     # -- detectors -------------------------------------------------------------------------------
     def set_detectors(self, dets):
@@ -201,7 +251,8 @@ def read_config(path_or_dict) -> SimulationSettings:
     # mixed static potentials (jsonutils.cpp:319-326; SimulationManager::useParallelPotentials)
     _try(j, lambda v: setattr(s, "mixed_static_count", v), *ph, "mixed static potentials", "count", conv=int)
     _try(j, lambda v: setattr(s, "mixed_static_enabled", v), *ph, "mixed static potentials", "enabled", conv=bool)
-    c.mixed_static = s.mixed_static_count if (s.mixed_static_enabled and s.mixed_static_count > 1) else 0
+    _try(j, lambda v: setattr(s, "precalculate_transmission", v), "precalculate transmission", conv=bool)
+    s.plasmon = _read_plasmon(j)
     # probe incoherence (jsonutils.cpp:276-308)
     pr = ("incoherence", "probe")
     _try(j, lambda v: setattr(c, "chromatic", int(v)), *pr, "chromatic", "enabled", conv=bool)
@@ -212,6 +263,7 @@ def read_config(path_or_dict) -> SimulationSettings:
     _try(j, lambda v: setattr(c, "source_fwhm", v), *pr, "source size", "FWHM", "val", conv=float)
     if c.mode != abi.MODE_STEM:
         c.stem_moving_frame = 0   # the static-area switch is read only by STEM
+    c.mixed_static = s.mixed_static_sets()
     # CTEM CCD (jsonutils.cpp:176-184)
     _try(j, lambda v: setattr(s, "ccd_name", v), "ctem", "ccd", "name", conv=str)
     _try(j, lambda v: setattr(s, "ccd_dose", v), "ctem", "ccd", "dose", "val", conv=float)

@@ -111,13 +111,48 @@ def test_json_incoherence_keys():
                                                              "mixed static potentials": {"enabled": True, "count": 4}}}}}
     s = read_config(j)
     c = s.cfg
-    assert (c.stem_moving_frame, c.stem_job_pixels, c.mixed_static) == (1, 5, 4)
+    # STEM uses mixed static potentials only with the static frame (parallelPotentialsCount)
+    assert (c.stem_moving_frame, c.stem_job_pixels, c.mixed_static) == (1, 5, 0)
     assert (c.chromatic, c.chromatic_cc, c.chromatic_hwhm_pos, c.chromatic_hwhm_neg) == (1, 1.3, 0.9, 0.4)
     assert (c.source_size, c.source_fwhm) == (1, 0.8)
     assert s.effective_iterations() == 7
-    # mixed static potentials need count > 1 (SimulationManager::useParallelPotentials)
-    j["incoherence"]["inelastic scattering"]["phonon"]["mixed static potentials"]["count"] = 1
+    j["stem"]["static area"]["enabled"] = True
+    assert read_config(j).cfg.mixed_static == 4
+    # they need count > 1, frozen phonons and precalculated transmissions, which plasmons turn off
+    ph = j["incoherence"]["inelastic scattering"]
+    ph["phonon"]["mixed static potentials"]["count"] = 1
     assert read_config(j).cfg.mixed_static == 0
+    ph["phonon"]["mixed static potentials"]["count"] = 4
+    ph["plasmon"] = {"enabled": True, "mean free path": {"value": 12.0}, "type": "individual", "individual": 2}
+    s = read_config(j)
+    assert s.cfg.mixed_static == 0 and s.plasmon.enabled and s.plasmon.mean_free_path == 120.0
+    assert s.plasmon.kind == "individual" and s.plasmon.individual == 2
+    ph["plasmon"]["enabled"] = False
+    j["precalculate transmission"] = False
+    assert read_config(j).cfg.mixed_static == 0
+    j["precalculate transmission"] = True
+    ph["phonon"]["enabled"] = False
+    assert read_config(j).cfg.mixed_static == 0
+    ph["phonon"]["enabled"] = True
+    # CBED: only with fewer sets than iterations
+    j["mode"]["id"] = 3
+    assert read_config(j).cfg.mixed_static == 4
+    j["incoherence"]["iterations"] = 4
+    assert read_config(j).cfg.mixed_static == 0
+    j["incoherence"]["iterations"] = 7
+    j["mode"]["id"] = 2
+    j["stem"]["static area"]["enabled"] = False
+    # plasmons alone switch the incoherence iterations on
+    ph["phonon"]["enabled"] = False
+    j["incoherence"]["probe"]["chromatic"]["enabled"] = False
+    j["incoherence"]["probe"]["source size"]["enabled"] = False
+    assert read_config(j).effective_iterations() == 1
+    ph["plasmon"]["enabled"] = True
+    assert read_config(j).effective_iterations() == 7
+    ph["plasmon"]["enabled"] = False
+    ph["phonon"]["enabled"] = True
+    j["incoherence"]["probe"]["chromatic"]["enabled"] = True
+    j["incoherence"]["probe"]["source size"]["enabled"] = True
     # CTEM: chromatic / source size do not count as incoherence (IncoherentEffects::enabled), the moving
     # frame is a STEM switch
     j["mode"]["id"] = 0
