@@ -389,6 +389,8 @@ struct Sim : SimBase {
 
     // tables
     DevBuf<double> kx, ky, kx2, ky2;
+    DevBuf<int2> ycut;   // per column, the band of rows the propagator's cut keeps
+    PlainWork plain_work;   // buffers and plan of the plain FP64 path (stem_plain)
     DevBuf<C> px, py, pxc, pyc;   // propagator factors and their conjugates (adjoint)
     DevBuf<double2> chi;
     DevBuf<uint16_t> detmask;
@@ -464,6 +466,22 @@ struct Sim : SimBase {
         MS_CUDA(cudaMemcpyAsync(ky2.p, hy2.data(), N * sizeof(double), cudaMemcpyHostToDevice, st()));
         // separable propagator (propagator_d.cl:18-52): phase pi dz s, s = (k^2 - kz^2 - (kx+bx)^2 - (ky+by)^2)/kz
         k_prop = g.k_max * cfg.inverse_limit_factor;
+        {   // the strict cut kx^2 + ky^2 < kp^2 per column as rows [0, a) and [b, N): ky^2 rises from row 0 to the
+            // middle row and falls after it, so the kept rows are such a band; the test is the kernels' FP64 one
+            const double kp2 = k_prop * k_prop;
+            std::vector<int2> hc(N);
+            for (int x = 0; x < N; x++) {
+                int a = 0;
+                while (a < N && hx2[x] + hy2[a] < kp2) a++;
+                int b = N;
+                while (b > a && hx2[x] + hy2[b - 1] < kp2) b--;
+                for (int y = a; y < b; y++)
+                    if (hx2[x] + hy2[y] < kp2) throw StateError("propagator cut is not a band of rows");
+                hc[x] = make_int2(a, b);
+            }
+            ycut.ensure(ctx, N);
+            MS_CUDA(cudaMemcpyAsync(ycut.p, hc.data(), N * sizeof(int2), cudaMemcpyHostToDevice, st()));
+        }
         {
             const double bk = g.wavenumber, bx = g.wavevector[0], by = g.wavevector[1], bz = g.wavevector[2];
             const double f = bz / bk;
@@ -922,7 +940,7 @@ struct Sim : SimBase {
             ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N), df, g.wavelength);
         });
         ctx->launches++;
-        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p};
         DetArgs det{detmask.p, cfg.n_detectors, partials.p};
         std::vector<int> outs = output_slices(cfg, g);
         size_t oi = 0;
@@ -1076,7 +1094,7 @@ struct Sim : SimBase {
                           g.wavelength);
         }
         ctx->launches++;
-        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p};
         DetArgs det{detmask.p, 0, partials.p};
         std::vector<int> outs = output_slices(cfg, g);
         size_t oi = 0;
@@ -1345,7 +1363,7 @@ struct Sim : SimBase {
         MS_CUDA(cudaMemsetAsync(wave.p, 0, (size_t)bmax * wave_bytes, st()));
         if (!trans_built) MS_CUDA(cudaMemsetAsync(trans.p, 0, NN * sizeof(C), st()));
         const cplx<R> *tw = ctx->twiddles<R>(N);
-        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p};
         DetArgs det{detmask.p, cfg.n_detectors, partials.p};
         const R a = (R)(1.0 / N), b2 = (R)(s2d * s2d * N), ds = (R)s2d;
         double best_rate = -1;
@@ -1420,7 +1438,7 @@ struct Sim : SimBase {
             ck_buf.ensure(ctx, (size_t)n_ck * NN);
             save.ensure(ctx, (size_t)(c == 1 ? S : c) * NN);
         }
-        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop};
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p};
         DetArgs nodet{detmask.p, 0, partials.p};
         // forward: plane wave through every slice, checkpoints of the row-transformed state
         plane_wave_state<R>(st(), N, wave.p);
@@ -1473,7 +1491,7 @@ struct Sim : SimBase {
         }
         MS_CUDA(cudaMemsetAsync(gxy.p, 0, 2 * (size_t)std::max(n_in, 1) * sizeof(double), st()));
         fw.ensure(ctx, NN); gT.ensure(ctx, NN); gV.ensure(ctx, NN);
-        PropTables<R> ptc{pxc.p, pyc.p, kx2.p, ky2.p, k_prop * k_prop};
+        PropTables<R> ptc{pxc.p, pyc.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p};
         for (int k = n_ck - 1; k >= 0; k--) {
             const int s0 = k * c, s1 = std::min(s0 + c, S);
             if (c > 1) {   // recompute psi_s of the segment from its checkpoint
@@ -1545,7 +1563,7 @@ struct Sim : SimBase {
                 a.ycPx[d] = cfg.detectors[d].ycentre / g.angle_scale;
             }
             a.launches = &ctx->launches;
-            plain_stem(st(), a, pixels, n, out);
+            plain_stem(st(), a, plain_work, pixels, n, out);
         }
     }
 };

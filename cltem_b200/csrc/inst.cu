@@ -2,6 +2,8 @@
 // Compiled once per (MS_REAL, MS_N) pair by the build (e.g. -DMS_REAL=float -DMS_N=512).
 #include "launch.cuh"
 
+#include <type_traits>
+
 #ifndef MS_REAL
 #error "MS_REAL must be defined"
 #endif
@@ -23,6 +25,21 @@ template <class K> void set_smem(K kernel, size_t bytes) {
     MS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
 }
 
+// the two-column step kernel of the FP32 radix-8 plans (templates, so that the FP64 build discards them)
+template <class RR> void pair_attrs() {
+    if constexpr (std::is_same<RR, float>::value && pair_columns<N>()) set_smem(k_col_step_pair<N>, PairCfg<N>::smem());
+}
+template <class RR>
+bool pair_step(cudaStream_t s, dim3 g, cplx<RR> *wave, const cplx<RR> *tw, PropTables<RR> pt, RR b, int tiles_lo) {
+    if constexpr (std::is_same<RR, float>::value && pair_columns<N>()) {
+        k_col_step_pair<N><<<g, dim3(PairCfg<N>::PAIRS, Plan<N>::NT), PairCfg<N>::smem(), s>>>(wave, tw, pt, b, tiles_lo);
+        MS_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        return false;
+    }
+}
+
 // kernel attributes are per device: set once for each device this process launches on
 bool g_attrs_done[64] = {};
 void ensure_attrs() {
@@ -33,6 +50,7 @@ void ensure_attrs() {
     set_smem(k_row_fft<R, N, -1>, RC::smem());
     set_smem(k_row_fft<R, N, +1>, RC::smem());
     set_smem(k_col_step<R, N, COL_STEP>, CC::smem());
+    pair_attrs<R>();
     set_smem(k_col_step<R, N, COL_STEP_DET>, CC::smem());
     set_smem(k_col_step<R, N, COL_DET_ONLY>, CC::smem());
     set_smem(k_col_fft<R, N, -1>, CC::smem());
@@ -67,6 +85,7 @@ void col_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, PropT
     if (tiles_lo < 0 || tiles_hi < 0 || tiles_lo + tiles_hi > N / CC::COLS || tiles_lo + tiles_hi == 0)
         throw std::runtime_error("column tile range out of bounds");
     dim3 g(tiles_lo + tiles_hi, batch);
+    if (mode == COL_STEP && recip == nullptr && pt.ycut && pair_step<R>(s, g, wave, tw, pt, b, tiles_lo)) return;
     if (mode == COL_STEP && recip == nullptr)
         k_col_step<R, N, COL_STEP><<<g, col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip, tiles_lo);
     else if (mode == COL_DET_ONLY)

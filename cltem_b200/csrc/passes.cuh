@@ -14,6 +14,7 @@
 
 #include "fft.cuh"
 #include "fft_wide.cuh"
+#include "fft_pair.cuh"
 
 #include <type_traits>
 
@@ -28,6 +29,7 @@ struct PropTables {
     const double *kx2;   // res: kx*kx (FP64, the reference's k0x)
     const double *ky2;   // res: ky*ky
     double kmax2;        // (k_max * limit_factor)^2 of the propagator's strict cut (propagator_d.cl:34-36)
+    const int2 *ycut;    // res: column x keeps rows y < ycut[x].x and y >= ycut[x].y, the same cut tabulated
 };
 
 struct DetArgs {
@@ -260,6 +262,62 @@ k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTabl
         col_transform<R, N, +1>(v, sm, t, tw);
         col_store<R, N>(v, base, x, t);
     }
+}
+
+// The plain step (COL_STEP) of the FP32 radix-8 plans with each thread carrying two adjacent columns of
+// the tile: 16-byte loads, stores and shared-memory exchanges (fft_pair.cuh), and the propagator's cut
+// read as a row band per column (PropTables::ycut) instead of an FP64 test per element. Same arithmetic
+// per element as k_col_step<float, N, COL_STEP>. 256 threads at 64 registers: 4 blocks per SM.
+template <int N> struct PairCfg {
+    using P = Plan<N>;
+    static constexpr int COLS = ColCfg<N, float>::COLS;
+    static constexpr int PAIRS = COLS / 2;
+    static constexpr int THREADS = PAIRS * P::NT;
+    static constexpr size_t smem() { return sizeof(float2) * (size_t)N + sizeof(float4) * (size_t)N * PAIRS; }
+};
+template <int N> constexpr bool pair_columns() {
+    return Plan<N>::E == 8 && !ColCfg<N, float>::WIDE && ColCfg<N, float>::COLS >= 2;
+}
+
+template <int N>
+__global__ void __launch_bounds__(PairCfg<N>::THREADS, 4)
+k_col_step_pair(float2 *__restrict__ wave, const float2 *__restrict__ twg, PropTables<float> pt, float bscale,
+                int tiles_lo) {
+    using PC = PairCfg<N>;
+    using P = typename PC::P;
+    constexpr int PAIRS = PC::PAIRS, E = P::E, NT = P::NT;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    float2 *tw = reinterpret_cast<float2 *>(smraw);
+    float4 *sm = reinterpret_cast<float4 *>(tw + N) + threadIdx.x;
+    const int p = threadIdx.x, t = threadIdx.y;
+    load_table<float>(tw, twg, N, p + t * PAIRS, PAIRS * NT);
+    const int tile = (int)blockIdx.x < tiles_lo ? (int)blockIdx.x : N / PC::COLS - ((int)gridDim.x - (int)blockIdx.x);
+    const int x = tile * PC::COLS + 2 * p;
+    float4 *base = reinterpret_cast<float4 *>(wave + (size_t)blockIdx.y * N * N + x);
+    float2 va[E], vb[E];
+#pragma unroll
+    for (int m = 0; m < E; m++) {
+        const float4 q = base[(size_t)(t + m * NT) * (N / 2)];
+        va[m] = make_float2(q.x, q.y);
+        vb[m] = make_float2(q.z, q.w);
+    }
+    __syncthreads();
+    fft_pair<N, -1>(va, vb, sm, ColAddr<PAIRS, 16>(), t, tw);
+    const float2 pxa = pt.px[x], pxb = pt.px[x + 1];
+    const int2 ca = pt.ycut[x], cb = pt.ycut[x + 1];
+#pragma unroll
+    for (int m = 0; m < E; m++) {
+        const int y = t + m * NT;
+        const float2 py = pt.py[y];
+        const float2 pa = (y < ca.x || y >= ca.y) ? cmul(pxa, py) : mk<float>(0, 0);
+        const float2 pb = (y < cb.x || y >= cb.y) ? cmul(pxb, py) : mk<float>(0, 0);
+        va[m] = cscale(cmul(va[m], pa), bscale);
+        vb[m] = cscale(cmul(vb[m], pb), bscale);
+    }
+    fft_pair<N, +1>(va, vb, sm, ColAddr<PAIRS, 16>(), t, tw);
+#pragma unroll
+    for (int m = 0; m < E; m++)
+        base[(size_t)(t + m * NT) * (N / 2)] = make_float4(va[m].x, va[m].y, vb[m].x, vb[m].y);
 }
 
 // A plain column transform, scaled, in or out of place.

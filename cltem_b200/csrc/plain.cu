@@ -99,26 +99,38 @@ static void cufft_check(cufftResult r, const char *what) {
     if (r != CUFFT_SUCCESS) throw CudaError(std::string(what) + " failed (cufft status " + std::to_string((int)r) + ")");
 }
 
-void plain_stem(cudaStream_t s, const PlainArgs &a, const int *pixels, size_t n_pix, double *out) {
+void PlainWork::release() {
+    if (has_plan) cufftDestroy((cufftHandle)plan);
+    has_plan = false;
+    cudaFree(real); cudaFree(recip); cudaFree(tmp); cudaFree(prop); cudaFree(t2); cudaFree(t3); cudaFree(red);
+    real = recip = tmp = prop = nullptr;
+    t2 = t3 = red = nullptr;
+    n = 0;
+}
+
+void plain_stem(cudaStream_t s, const PlainArgs &a, PlainWork &w, const int *pixels, size_t n_pix, double *out) {
     const int n = a.n;
     const size_t NN = (size_t)n * n;
-    double2 *real = nullptr, *recip = nullptr, *tmp = nullptr, *prop = nullptr;
-    double *t2 = nullptr, *t3 = nullptr, *red = nullptr;
-    cufftHandle plan = 0;
-    auto release = [&]() {
-        if (plan) cufftDestroy(plan);
-        cudaFree(real); cudaFree(recip); cudaFree(tmp); cudaFree(prop); cudaFree(t2); cudaFree(t3); cudaFree(red);
-    };
+    const unsigned nGroups = (unsigned)(NN / 256);
     try {
-        MS_CUDA(cudaMalloc(&real, NN * sizeof(double2)));
-        MS_CUDA(cudaMalloc(&recip, NN * sizeof(double2)));
-        MS_CUDA(cudaMalloc(&tmp, NN * sizeof(double2)));
-        MS_CUDA(cudaMalloc(&prop, NN * sizeof(double2)));
-        MS_CUDA(cudaMalloc(&t2, NN * sizeof(double)));
-        MS_CUDA(cudaMalloc(&t3, NN * sizeof(double)));
-        const unsigned nGroups = (unsigned)(NN / 256);
-        MS_CUDA(cudaMalloc(&red, nGroups * sizeof(double)));
-        cufft_check(cufftPlan2d(&plan, n, n, CUFFT_Z2Z), "cufftPlan2d");
+        if (w.n != n) {
+            w.release();
+            MS_CUDA(cudaMalloc(&w.real, NN * sizeof(double2)));
+            MS_CUDA(cudaMalloc(&w.recip, NN * sizeof(double2)));
+            MS_CUDA(cudaMalloc(&w.tmp, NN * sizeof(double2)));
+            MS_CUDA(cudaMalloc(&w.prop, NN * sizeof(double2)));
+            MS_CUDA(cudaMalloc(&w.t2, NN * sizeof(double)));
+            MS_CUDA(cudaMalloc(&w.t3, NN * sizeof(double)));
+            MS_CUDA(cudaMalloc(&w.red, nGroups * sizeof(double)));
+            cufftHandle plan = 0;
+            cufft_check(cufftPlan2d(&plan, n, n, CUFFT_Z2Z), "cufftPlan2d");
+            w.plan = (int)plan;
+            w.has_plan = true;
+            w.n = n;
+        }
+        double2 *real = w.real, *recip = w.recip, *tmp = w.tmp, *prop = w.prop;
+        double *t2 = w.t2, *t3 = w.t3, *red = w.red;
+        const cufftHandle plan = (cufftHandle)w.plan;
         cufft_check(cufftSetStream(plan, s), "cufftSetStream");
         dim3 b(128), g((n + 127) / 128, n);
         k_plain_propagator<<<g, b, 0, s>>>(prop, a.kx, a.ky, n, a.dz, a.beam_k, a.beam_kx, a.beam_ky, a.beam_kz, a.k_max_prop);
@@ -167,10 +179,9 @@ void plain_stem(cudaStream_t s, const PlainArgs &a, const int *pixels, size_t n_
             }
         }
     } catch (...) {
-        release();
+        w.release();
         throw;
     }
-    release();
 }
 
 }  // namespace ms

@@ -17,6 +17,18 @@ struct PlainArgs {
     unsigned long long *launches; // kernel launch counter (may be null)
 };
 
-void plain_stem(cudaStream_t s, const PlainArgs &a, const int *pixels, size_t n_pix, double *out);
+// Buffers and cuFFT plan of the plain path, kept between calls as the reference keeps its buffers between
+// jobs (SimulationGeneral::initialiseBuffers reallocates only when the resolution changes).
+struct PlainWork {
+    int n = 0;
+    double2 *real = nullptr, *recip = nullptr, *tmp = nullptr, *prop = nullptr;
+    double *t2 = nullptr, *t3 = nullptr, *red = nullptr;
+    int plan = 0;            // cufftHandle
+    bool has_plan = false;
+    void release();
+    ~PlainWork() { release(); }
+};
+
+void plain_stem(cudaStream_t s, const PlainArgs &a, PlainWork &w, const int *pixels, size_t n_pix, double *out);
 
 }  // namespace ms
