@@ -267,12 +267,14 @@ k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTabl
 // The plain step (COL_STEP) of the FP32 radix-8 plans with each thread carrying two adjacent columns of
 // the tile: 16-byte loads, stores and shared-memory exchanges (fft_pair.cuh), and the propagator's cut
 // read as a row band per column (PropTables::ycut) instead of an FP64 test per element. Same arithmetic
-// per element as k_col_step<float, N, COL_STEP>. 256 threads at 64 registers: 4 blocks per SM.
+// per element as k_col_step<float, N, COL_STEP>. Up to 256 threads a block: 4 blocks per SM (64 registers
+// at 256 threads); 512 threads (4096²): 2 blocks.
 template <int N> struct PairCfg {
     using P = Plan<N>;
     static constexpr int COLS = ColCfg<N, float>::COLS;
     static constexpr int PAIRS = COLS / 2;
     static constexpr int THREADS = PAIRS * P::NT;
+    static constexpr int MINB = THREADS <= 256 ? 4 : 2;
     static constexpr size_t smem() { return sizeof(float2) * (size_t)N + sizeof(float4) * (size_t)N * PAIRS; }
 };
 template <int N> constexpr bool pair_columns() {
@@ -280,7 +282,7 @@ template <int N> constexpr bool pair_columns() {
 }
 
 template <int N>
-__global__ void __launch_bounds__(PairCfg<N>::THREADS, 4)
+__global__ void __launch_bounds__(PairCfg<N>::THREADS, PairCfg<N>::MINB)
 k_col_step_pair(float2 *__restrict__ wave, const float2 *__restrict__ twg, PropTables<float> pt, float bscale,
                 int tiles_lo) {
     using PC = PairCfg<N>;
