@@ -202,6 +202,44 @@ struct Params {
     int max_z = 0;
 };
 
+// The per-element term table of the FP32 full-3D kernel (potential.cuh, k_potential_3d_f): for each element
+// Z = 1..max_z and term, float4 at (Z - 1) * kPot3Terms + term, formed in FP64 from the parameterisation
+// table `v` (12 values per element for Kirkland, 10 for Peng / Lobato) and rounded once.
+std::vector<float4> pot3_table(int form, int i_count, const std::vector<double> &v, int max_z) {
+    constexpr double kLog2e = 1.44269504088896340736;
+    std::vector<float4> t((size_t)std::max(max_z, 0) * kPot3Terms, make_float4(0, 0, 0, 0));
+    const int stride = form == 0 ? 12 : 10;
+    for (int Z = 1; Z <= max_z; Z++) {
+        const double *q = v.data() + (size_t)(Z - 1) * stride;
+        float4 *o = t.data() + (size_t)(Z - 1) * kPot3Terms;
+        for (int i = 0; i < i_count; i++) {
+            if (form == 2) {   // Lobato
+                const double b = q[i + 5];
+                if (!(b > 0)) continue;
+                const double bir = 1.0 / std::sqrt(b);
+                o[i] = make_float4((float)(472.545072199968 * q[i] * (bir * bir * bir)), (float)(-2.0 * M_PI * bir * kLog2e),
+                                   (float)(std::sqrt(b) / M_PI), 0.0f);
+            } else if (form == 1) {   // Peng
+                const double b = q[i + 5];
+                if (!(b > 0)) continue;
+                const double bir = 1.0 / std::sqrt(b);
+                o[i] = make_float4((float)(266.5157269 * q[i] * (bir * bir * bir)), 0.0f, 0.0f,
+                                   (float)(-M_PI * M_PI / b * kLog2e));
+            } else {   // Kirkland: Lorentzian terms, then Gaussian terms
+                const double a = q[2 * i], b = q[2 * i + 1];
+                if (b >= 0) o[i] = make_float4((float)(150.4121417 * a), (float)(-2.0 * M_PI * std::sqrt(b) * kLog2e), 0.0f, 0.0f);
+                const double c = q[2 * i_count + 2 * i], d = q[2 * i_count + 2 * i + 1];
+                if (d > 0) {
+                    const double dir = 1.0 / std::sqrt(d);
+                    o[i_count + i] = make_float4((float)(266.5157269 * c * (dir * dir * dir)), 0.0f, 0.0f,
+                                                 (float)(-M_PI * M_PI / d * kLog2e));
+                }
+            }
+        }
+    }
+    return t;
+}
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -211,6 +249,8 @@ struct Ctx {
     double *prm_d = nullptr;
     float *prm_f = nullptr;
     size_t prm_n = 0;
+    float4 *pot3_tab = nullptr;   // pot3_table of the loaded parameterisation (FP32 full-3D kernel)
+    size_t pot3_n = 0;
     std::map<int, void *> tw_f, tw_d;   // twiddle tables per size
     std::mutex mtx;
 
@@ -267,6 +307,7 @@ struct Ctx {
         for (auto &kv : tw_d) cudaFree(kv.second);
         cudaFree(prm_d);
         cudaFree(prm_f);
+        cudaFree(pot3_tab);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -674,7 +715,7 @@ struct Sim : SimBase {
     void potentials(C *out, int slice0, int count) {
         timed(st(), MSLICE_K_POTENTIAL, (double)count * NN * sizeof(C), [&] {
             launch_potential<R>(st(), cfg.full3d != 0, out, count, axs.p, ays.p, azs.p, aZs.p, block_start.p, params_dev(),
-                                pot_params(slice0));
+                                ctx->pot3_tab, pot_params(slice0));
         });
         ctx->launches++;
     }
@@ -1686,6 +1727,11 @@ int mslice_params_load(mslice_ctx *ctx, int form, int i_per_atom, const double *
         std::vector<float> pf(p, p + n);
         MS_CUDA(cudaMemcpy(c.prm_d, p, n * sizeof(double), cudaMemcpyHostToDevice));
         MS_CUDA(cudaMemcpy(c.prm_f, pf.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+        if (c.pot3_tab) { c.release(c.pot3_tab, c.pot3_n * sizeof(float4)); c.pot3_tab = nullptr; }
+        const std::vector<float4> t3 = ms::pot3_table(form, i_per_atom, c.params.values, c.params.max_z);
+        c.pot3_n = t3.size();
+        c.pot3_tab = (float4 *)c.alloc(t3.size() * sizeof(float4));
+        MS_CUDA(cudaMemcpy(c.pot3_tab, t3.data(), t3.size() * sizeof(float4), cudaMemcpyHostToDevice));
     });
 }
 

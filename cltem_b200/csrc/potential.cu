@@ -3,20 +3,38 @@
 #include "potential.cuh"
 #include "potential_launch.h"
 
+#include <type_traits>
+
 #ifndef MS_REAL
 #error "MS_REAL must be defined"
 #endif
 
 namespace ms {
 
+// the FP32 full-3D kernel (a template, so that the FP64 build discards it)
+template <class T>
+bool potential_3d_f(cudaStream_t s, dim3 grd, dim3 blk, cplx<T> *out, const double *ax, const double *ay,
+                    const double *az, const int *aZ, const int *block_start, const float4 *tab3, const PotParams &p) {
+    if constexpr (std::is_same<T, float>::value) {
+        if (p.form == 0) k_potential_3d_f<0><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, tab3, p);
+        else if (p.form == 1) k_potential_3d_f<1><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, tab3, p);
+        else k_potential_3d_f<2><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, tab3, p);
+        MS_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        return false;
+    }
+}
+
 template <>
 void launch_potential<MS_REAL>(cudaStream_t s, bool full3d, cplx<MS_REAL> *out, int n_slices, const double *ax,
                                const double *ay, const double *az, const int *aZ, const int *block_start,
-                               const MS_REAL *prm, const PotParams &p) {
+                               const MS_REAL *prm, const float4 *tab3, const PotParams &p) {
     using T = MS_REAL;
     if (p.width % 16 || p.height % 16) throw std::runtime_error("potential grid must be a multiple of 16");
     dim3 blk(16, 16), grd(p.width / 16, p.height / 16, n_slices);
     if (n_slices <= 0) return;
+    if (full3d && tab3 && potential_3d_f<T>(s, grd, blk, out, ax, ay, az, aZ, block_start, tab3, p)) return;
     if (full3d) {
         if (p.form == 0) k_potential_3d<T, 0><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
         else if (p.form == 1) k_potential_3d<T, 1><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
@@ -28,5 +46,6 @@ void launch_potential<MS_REAL>(cudaStream_t s, bool full3d, cplx<MS_REAL> *out, 
     }
     MS_CUDA(cudaGetLastError());
 }
+
 
 }  // namespace ms

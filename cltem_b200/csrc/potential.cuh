@@ -315,4 +315,150 @@ k_potential_3d(cplx<T> *__restrict__ out, const double *__restrict__ ax, const d
                        (T)(sub_slice_thickness * p.sigma) * sumz);
 }
 
+// ---- FP32 full 3-D potentials -------------------------------------------------------------------
+// The FP32 engine's full-3D build is bound by instruction issue. This kernel makes the same geometric
+// decisions as k_potential_3d:
+// - the same FP64 offsets and FP64 tests (8 Å in xy, the one-sided 3 Å in z);
+// - the same atom and sample order;
+// - the same trapezoid pairing.
+// It cuts the instructions per sample:
+// - The distance is rounded once to FP32 and its square root taken in FP32.
+// - Each form is a sum of exponentials whose per-element constants come from a table built on the host
+//   in FP64 and rounded once (pot3_table). exp is taken as exp2f of a pre-scaled exponent.
+// - The atoms of all bin rows a tile reads are staged through shared memory as one list, instead of one
+//   load (and two barriers) per bin row. A flag on the first atom of each bin row resets the trapezoid's
+//   previous sample there, as the reference's per-row `p2 = 0` does (full_3d_d.cl:238).
+// Table, per element Z and term i, float4 at (Z - 1) * kPot3Terms + i:
+// - Lobato (full_3d_d.cl:102-118): (472.545·a·b^-3/2, -2π·log2(e)/√b, √b/π, 0);
+//   term = x·exp2(y·r)·(z/r + 1).
+// - Peng: (266.516·a·b^-3/2, 0, 0, -π²·log2(e)/b); term = x·exp2(w·r²).
+// - Kirkland, Lorentzian terms i < n: (150.412·a, -2π·log2(e)·√b, 0, 0); the term x·exp2(y·r)/r.
+//   Gaussian terms i = n + j: (266.516·c·d^-3/2, 0, 0, -π²·log2(e)/d); the term x·exp2(w·r²).
+constexpr int kPot3Terms = 6;
+constexpr int kPot3Rows = 64;            // bin rows staged per pass of the row list
+constexpr int kPot3First = 1 << 30;     // flag on the first atom of a bin row in the staged Z
+
+template <int FORM>
+__device__ __forceinline__ float pot3_eval(const float4 *__restrict__ tab, int i_count, int Z, float rad) {
+    const float4 *t = tab + (Z - 1) * kPot3Terms;
+    const float inv = __fdividef(1.0f, rad);
+    if constexpr (FORM == 2) {
+        float sum = 0.0f;
+        for (int i = 0; i < i_count; i++) {
+            const float4 c = __ldg(t + i);
+            sum += c.x * exp2f(c.y * rad) * fmaf(c.z, inv, 1.0f);
+        }
+        return sum;
+    } else if constexpr (FORM == 1) {
+        const float r2 = rad * rad;
+        float sum = 0.0f;
+        for (int i = 0; i < i_count; i++) {
+            const float4 c = __ldg(t + i);
+            sum += c.x * exp2f(c.w * r2);
+        }
+        return sum;
+    } else {
+        const float r2 = rad * rad;
+        float suml = 0.0f, sumg = 0.0f;
+        for (int i = 0; i < i_count; i++) {
+            const float4 c = __ldg(t + i);
+            suml += c.x * exp2f(c.y * rad);
+        }
+        for (int i = 0; i < i_count; i++) {
+            const float4 c = __ldg(t + i_count + i);
+            sumg += c.x * exp2f(c.w * r2);
+        }
+        return suml * inv + sumg;
+    }
+}
+
+// grid (W/16, H/16, n_slices), block (16, 16)
+template <int FORM>
+__global__ void __launch_bounds__(256)
+k_potential_3d_f(float2 *__restrict__ out, const double *__restrict__ ax, const double *__restrict__ ay,
+                 const double *__restrict__ az, const int *__restrict__ aZ, const int *__restrict__ block_start,
+                 const float4 *__restrict__ tab, PotParams p) {
+    __shared__ double sx[kAtomChunk], sy[kAtomChunk], sz[kAtomChunk];
+    __shared__ int sZ[kAtomChunk];
+    __shared__ int row_start[kPot3Rows], row_off[kPot3Rows + 1];
+    const int lid = threadIdx.x + 16 * threadIdx.y;
+    const int xid = blockIdx.x * 16 + threadIdx.x, yid = blockIdx.y * 16 + threadIdx.y;
+    const int slice = blockIdx.z + p.slice0;
+    int si, ei, sj, ej;
+    tile_bins(p, blockIdx.x, blockIdx.y, si, ei, sj, ej);
+    int topz = slice - p.load_z, bottomz = slice + p.load_z;
+    const double int_r = 1.0 / p.integrals;
+    const double sub_slice_thickness = p.dz * int_r;
+    if (topz < 0) topz = 0;
+    if (bottomz >= p.total_slices) bottomz = p.total_slices - 1;
+    const double current_z = p.z0 + (p.total_slices - slice) * p.dz;
+    const double im_pos_x = p.startx + xid * p.pixelscale;
+    const double im_pos_y = p.starty + yid * p.pixelscale;
+    const float r_min = (float)(0.25 * p.pixelscale);
+    const bool no_shift = p.shift_x == 0.0 && p.shift_y == 0.0;
+    const size_t nb = (size_t)p.blocks_x * p.blocks_y;
+    const int nj = ej - sj + 1;
+    const int n_rows = (bottomz >= topz && nj > 0) ? (bottomz - topz + 1) * nj : 0;
+    float sumz = 0.0f, p2 = 0.0f;
+    for (int r0 = 0; r0 < n_rows; r0 += kPot3Rows) {
+        const int nr = min(kPot3Rows, n_rows - r0);
+        __syncthreads();   // the previous pass's readers of the row tables and the chunk are done
+        if (lid < nr) {
+            const int r = r0 + lid, k = topz + r / nj, j = sj + r % nj;
+            const int start = block_start[k * nb + p.blocks_x * j + si];
+            row_start[lid] = start;
+            row_off[lid + 1] = block_start[k * nb + p.blocks_x * j + ei + 1] - start;   // count, summed below
+        }
+        __syncthreads();
+        if (lid == 0) {
+            row_off[0] = 0;
+            for (int r = 0; r < nr; r++) row_off[r + 1] += row_off[r];
+        }
+        __syncthreads();
+        const int total = row_off[nr];
+        for (int c0 = 0; c0 < total; c0 += kAtomChunk) {
+            const int cn = min(kAtomChunk, total - c0);
+            __syncthreads();
+            if (lid < cn) {
+                const int f = c0 + lid;
+                int lo = 0, hi = nr - 1;   // the last row whose offset is <= f (a non-empty row holds f)
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (row_off[mid] <= f) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int a = row_start[lo] + (f - row_off[lo]);
+                sx[lid] = ax[a]; sy[lid] = ay[a]; sz[lid] = az[a];
+                sZ[lid] = aZ[a] | (f == row_off[lo] ? kPot3First : 0);
+            }
+            __syncthreads();
+            for (int l = 0; l < cn; l++) {
+                const int zf = sZ[l];
+                if (zf & kPot3First) p2 = 0.0f;   // a new bin row
+                const int Z = zf & (kPot3First - 1);
+                double rad_x = im_pos_x - sx[l];
+                double rad_y = im_pos_y - sy[l];
+                const double xy0 = rad_x * rad_x + rad_y * rad_y;
+                if (no_shift && xy0 > 64.0) continue;
+                for (int h = 0; h <= p.integrals; h++) {
+                    rad_x -= p.shift_x;
+                    rad_y -= p.shift_y;
+                    const double xyrad2 = no_shift ? xy0 : rad_x * rad_x + rad_y * rad_y;
+                    const double im_pos_z = current_z - h * p.dz * int_r;
+                    const double rad_z = im_pos_z - sz[l];
+                    if (xyrad2 <= 64.0 && rad_z <= 3.0) {
+                        const float rad = fmaxf(sqrtf((float)(xyrad2 + rad_z * rad_z)), r_min);
+                        const float p1 = pot3_eval<FORM>(tab, p.i_count, Z, rad);
+                        sumz += (h != 0) * (p1 + p2) * 0.5f;
+                        p2 = p1;
+                    }
+                }
+            }
+        }
+    }
+    if (xid < p.width && yid < p.height)
+        write_trans<float>(out + (size_t)blockIdx.z * p.width * p.height + (size_t)yid * p.width + xid,
+                           (float)(sub_slice_thickness * p.sigma) * sumz);
+}
+
 }  // namespace ms

@@ -135,9 +135,12 @@ def test_transmission_projected(gpu_ctx, oracle, params_all, dp, form):
 
 
 @pytest.mark.parametrize("dp", [True, False])
-@pytest.mark.parametrize("form", ["lobato", "kirkland"])
-def test_transmission_full3d(gpu_ctx, oracle, params_all, dp, form):
+@pytest.mark.parametrize("form", ["lobato", "kirkland", "peng"])
+@pytest.mark.parametrize("tilt", [0.0, 12.0])
+def test_transmission_full3d(gpu_ctx, oracle, params_all, dp, form, tilt):
+    # tilt (mrad): the per-sub-slice shift moves the xy offsets between samples (full_3d_d.cl:244-246)
     s, st = small_cbed(double_precision=dp, form=form)
+    s.cfg.beam_tilt, s.cfg.beam_azimuth = tilt, 0.7
     p = params_all[form]
     sim = _sim(gpu_ctx, p, s)
     osim = _osim(oracle, p, s)
