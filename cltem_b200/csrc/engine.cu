@@ -225,14 +225,14 @@ std::vector<float4> pot3_table(int form, int i_count, const std::vector<double> 
                 const double bir = 1.0 / std::sqrt(b);
                 o[i] = make_float4((float)(266.5157269 * q[i] * (bir * bir * bir)), 0.0f, 0.0f,
                                    (float)(-M_PI * M_PI / b * kLog2e));
-            } else {   // Kirkland: Lorentzian terms, then Gaussian terms
+            } else {   // Kirkland: Lorentzian terms at 0..2, Gaussian terms at 3..5
                 const double a = q[2 * i], b = q[2 * i + 1];
                 if (b >= 0) o[i] = make_float4((float)(150.4121417 * a), (float)(-2.0 * M_PI * std::sqrt(b) * kLog2e), 0.0f, 0.0f);
                 const double c = q[2 * i_count + 2 * i], d = q[2 * i_count + 2 * i + 1];
                 if (d > 0) {
                     const double dir = 1.0 / std::sqrt(d);
-                    o[i_count + i] = make_float4((float)(266.5157269 * c * (dir * dir * dir)), 0.0f, 0.0f,
-                                                 (float)(-M_PI * M_PI / d * kLog2e));
+                    o[3 + i] = make_float4((float)(266.5157269 * c * (dir * dir * dir)), 0.0f, 0.0f,
+                                           (float)(-M_PI * M_PI / d * kLog2e));
                 }
             }
         }

@@ -16,9 +16,11 @@ template <class T>
 bool potential_3d_f(cudaStream_t s, dim3 grd, dim3 blk, cplx<T> *out, const double *ax, const double *ay,
                     const double *az, const int *aZ, const int *block_start, const float4 *tab3, const PotParams &p) {
     if constexpr (std::is_same<T, float>::value) {
-        if (p.form == 0) k_potential_3d_f<0><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, tab3, p);
-        else if (p.form == 1) k_potential_3d_f<1><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, tab3, p);
-        else k_potential_3d_f<2><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, tab3, p);
+        constexpr int PX = kPot3Px;
+        const dim3 b2(16 / PX, 16);   // PX pixels a thread
+        if (p.form == 0) k_potential_3d_f<0, PX><<<grd, b2, 0, s>>>(out, ax, ay, az, aZ, block_start, tab3, p);
+        else if (p.form == 1) k_potential_3d_f<1, PX><<<grd, b2, 0, s>>>(out, ax, ay, az, aZ, block_start, tab3, p);
+        else k_potential_3d_f<2, PX><<<grd, b2, 0, s>>>(out, ax, ay, az, aZ, block_start, tab3, p);
         MS_CUDA(cudaGetLastError());
         return true;
     } else {

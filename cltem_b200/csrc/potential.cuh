@@ -322,67 +322,81 @@ k_potential_3d(cplx<T> *__restrict__ out, const double *__restrict__ ax, const d
 // - the same atom and sample order;
 // - the same trapezoid pairing.
 // It cuts the instructions per sample:
+// - Each thread computes kPot3Px pixels of its tile row. The atom loads, the per-atom table reads and the
+//   FP64 z tests are shared by its pixels.
 // - The distance is rounded once to FP32 and its square root taken in FP32.
 // - Each form is a sum of exponentials whose per-element constants come from a table built on the host
-//   in FP64 and rounded once (pot3_table). exp is taken as exp2f of a pre-scaled exponent.
+//   in FP64 and rounded once (pot3_table). A thread reads an atom's terms once into registers, and takes
+//   exp as ex2.approx.ftz.f32 (relative error below 2^-22) of a pre-scaled exponent.
 // - The atoms of all bin rows a tile reads are staged through shared memory as one list, instead of one
 //   load (and two barriers) per bin row. A flag on the first atom of each bin row resets the trapezoid's
 //   previous sample there, as the reference's per-row `p2 = 0` does (full_3d_d.cl:238).
-// Table, per element Z and term i, float4 at (Z - 1) * kPot3Terms + i:
-// - Lobato (full_3d_d.cl:102-118): (472.545·a·b^-3/2, -2π·log2(e)/√b, √b/π, 0);
+// Table, per element Z and term i, float4 at (Z - 1) * kPot3Terms + i (terms beyond the parameterisation's
+// count are zero):
+// - Lobato (full_3d_d.cl:102-118), i < 5: (472.545·a·b^-3/2, -2π·log2(e)/√b, √b/π, 0);
 //   term = x·exp2(y·r)·(z/r + 1).
-// - Peng: (266.516·a·b^-3/2, 0, 0, -π²·log2(e)/b); term = x·exp2(w·r²).
-// - Kirkland, Lorentzian terms i < n: (150.412·a, -2π·log2(e)·√b, 0, 0); the term x·exp2(y·r)/r.
-//   Gaussian terms i = n + j: (266.516·c·d^-3/2, 0, 0, -π²·log2(e)/d); the term x·exp2(w·r²).
+// - Peng, i < 5: (266.516·a·b^-3/2, 0, 0, -π²·log2(e)/b); term = x·exp2(w·r²).
+// - Kirkland, Lorentzian terms i < 3: (150.412·a, -2π·log2(e)·√b, 0, 0); the term x·exp2(y·r)/r.
+//   Gaussian terms i = 3 + j: (266.516·c·d^-3/2, 0, 0, -π²·log2(e)/d); the term x·exp2(w·r²).
 constexpr int kPot3Terms = 6;
 constexpr int kPot3Rows = 64;            // bin rows staged per pass of the row list
 constexpr int kPot3First = 1 << 30;     // flag on the first atom of a bin row in the staged Z
 
+// 2^x by the special-function unit (hand-written PTX; flushes subnormal results to zero)
+__device__ __forceinline__ float ex2a(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+// terms of each kind per element: Kirkland 3 Lorentzian + 3 Gaussian, Peng / Lobato 5
+template <int FORM> struct Pot3N {
+    static constexpr int L = FORM == 0 ? 3 : 5;
+    static constexpr int G = FORM == 0 ? 3 : 0;
+};
 template <int FORM>
-__device__ __forceinline__ float pot3_eval(const float4 *__restrict__ tab, int i_count, int Z, float rad) {
-    const float4 *t = tab + (Z - 1) * kPot3Terms;
+__device__ __forceinline__ float pot3_eval_r(const float4 (&c)[Pot3N<FORM>::L + Pot3N<FORM>::G], float rad) {
     const float inv = __fdividef(1.0f, rad);
     if constexpr (FORM == 2) {
         float sum = 0.0f;
-        for (int i = 0; i < i_count; i++) {
-            const float4 c = __ldg(t + i);
-            sum += c.x * exp2f(c.y * rad) * fmaf(c.z, inv, 1.0f);
-        }
+#pragma unroll
+        for (int i = 0; i < 5; i++) sum += c[i].x * ex2a(c[i].y * rad) * fmaf(c[i].z, inv, 1.0f);
         return sum;
     } else if constexpr (FORM == 1) {
         const float r2 = rad * rad;
         float sum = 0.0f;
-        for (int i = 0; i < i_count; i++) {
-            const float4 c = __ldg(t + i);
-            sum += c.x * exp2f(c.w * r2);
-        }
+#pragma unroll
+        for (int i = 0; i < 5; i++) sum += c[i].x * ex2a(c[i].w * r2);
         return sum;
     } else {
         const float r2 = rad * rad;
         float suml = 0.0f, sumg = 0.0f;
-        for (int i = 0; i < i_count; i++) {
-            const float4 c = __ldg(t + i);
-            suml += c.x * exp2f(c.y * rad);
-        }
-        for (int i = 0; i < i_count; i++) {
-            const float4 c = __ldg(t + i_count + i);
-            sumg += c.x * exp2f(c.w * r2);
-        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) suml += c[i].x * ex2a(c[i].y * rad);
+#pragma unroll
+        for (int i = 0; i < 3; i++) sumg += c[3 + i].x * ex2a(c[3 + i].w * r2);
         return suml * inv + sumg;
     }
 }
 
-// grid (W/16, H/16, n_slices), block (16, 16)
-template <int FORM>
-__global__ void __launch_bounds__(256)
+// Pixels a thread computes in the FP32 full-3D kernel (x, x + 16/PX, ... of its tile row)
+#ifndef MS_POT3_PX
+#define MS_POT3_PX 4
+#endif
+constexpr int kPot3Px = MS_POT3_PX;
+
+// grid (W/16, H/16, n_slices), block (16/PX, 16): each thread the pixels x + m·16/PX, m < PX, of its tile row
+template <int FORM, int PX>
+__global__ void __launch_bounds__(256 / PX)
 k_potential_3d_f(float2 *__restrict__ out, const double *__restrict__ ax, const double *__restrict__ ay,
                  const double *__restrict__ az, const int *__restrict__ aZ, const int *__restrict__ block_start,
                  const float4 *__restrict__ tab, PotParams p) {
+    constexpr int NTERM = Pot3N<FORM>::L + Pot3N<FORM>::G;
+    constexpr int TX = 16 / PX, NTH = 256 / PX;
     __shared__ double sx[kAtomChunk], sy[kAtomChunk], sz[kAtomChunk];
     __shared__ int sZ[kAtomChunk];
     __shared__ int row_start[kPot3Rows], row_off[kPot3Rows + 1];
-    const int lid = threadIdx.x + 16 * threadIdx.y;
-    const int xid = blockIdx.x * 16 + threadIdx.x, yid = blockIdx.y * 16 + threadIdx.y;
+    const int lid = threadIdx.x + TX * threadIdx.y;
+    const int xid0 = blockIdx.x * 16 + threadIdx.x, yid = blockIdx.y * 16 + threadIdx.y;
     const int slice = blockIdx.z + p.slice0;
     int si, ei, sj, ej;
     tile_bins(p, blockIdx.x, blockIdx.y, si, ei, sj, ej);
@@ -392,14 +406,18 @@ k_potential_3d_f(float2 *__restrict__ out, const double *__restrict__ ax, const 
     if (topz < 0) topz = 0;
     if (bottomz >= p.total_slices) bottomz = p.total_slices - 1;
     const double current_z = p.z0 + (p.total_slices - slice) * p.dz;
-    const double im_pos_x = p.startx + xid * p.pixelscale;
+    double pos_x[PX];
+#pragma unroll
+    for (int m = 0; m < PX; m++) pos_x[m] = p.startx + (xid0 + m * TX) * p.pixelscale;
     const double im_pos_y = p.starty + yid * p.pixelscale;
     const float r_min = (float)(0.25 * p.pixelscale);
     const bool no_shift = p.shift_x == 0.0 && p.shift_y == 0.0;
     const size_t nb = (size_t)p.blocks_x * p.blocks_y;
     const int nj = ej - sj + 1;
     const int n_rows = (bottomz >= topz && nj > 0) ? (bottomz - topz + 1) * nj : 0;
-    float sumz = 0.0f, p2 = 0.0f;
+    float sum[PX], q[PX];
+#pragma unroll
+    for (int m = 0; m < PX; m++) { sum[m] = 0.0f; q[m] = 0.0f; }
     for (int r0 = 0; r0 < n_rows; r0 += kPot3Rows) {
         const int nr = min(kPot3Rows, n_rows - r0);
         __syncthreads();   // the previous pass's readers of the row tables and the chunk are done
@@ -419,8 +437,8 @@ k_potential_3d_f(float2 *__restrict__ out, const double *__restrict__ ax, const 
         for (int c0 = 0; c0 < total; c0 += kAtomChunk) {
             const int cn = min(kAtomChunk, total - c0);
             __syncthreads();
-            if (lid < cn) {
-                const int f = c0 + lid;
+            for (int w = lid; w < cn; w += NTH) {
+                const int f = c0 + w;
                 int lo = 0, hi = nr - 1;   // the last row whose offset is <= f (a non-empty row holds f)
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) >> 1;
@@ -428,37 +446,67 @@ k_potential_3d_f(float2 *__restrict__ out, const double *__restrict__ ax, const 
                     else hi = mid - 1;
                 }
                 const int a = row_start[lo] + (f - row_off[lo]);
-                sx[lid] = ax[a]; sy[lid] = ay[a]; sz[lid] = az[a];
-                sZ[lid] = aZ[a] | (f == row_off[lo] ? kPot3First : 0);
+                sx[w] = ax[a]; sy[w] = ay[a]; sz[w] = az[a];
+                sZ[w] = aZ[a] | (f == row_off[lo] ? kPot3First : 0);
             }
             __syncthreads();
             for (int l = 0; l < cn; l++) {
                 const int zf = sZ[l];
-                if (zf & kPot3First) p2 = 0.0f;   // a new bin row
+                if (zf & kPot3First) {   // a new bin row
+#pragma unroll
+                    for (int m = 0; m < PX; m++) q[m] = 0.0f;
+                }
+                const double xl = sx[l];
+                const double ry = im_pos_y - sy[l];
+                const double yy = ry * ry;
+                double rx[PX], xy0[PX];
+                bool in[PX], any = false;
+#pragma unroll
+                for (int m = 0; m < PX; m++) {
+                    rx[m] = pos_x[m] - xl;
+                    xy0[m] = rx[m] * rx[m] + yy;
+                    // without tilt the xy test is the same for every sample: beyond 8 Å the atom adds nothing
+                    in[m] = !(no_shift && xy0[m] > 64.0);
+                    any = any || in[m];
+                }
+                if (!any) continue;
                 const int Z = zf & (kPot3First - 1);
-                double rad_x = im_pos_x - sx[l];
-                double rad_y = im_pos_y - sy[l];
-                const double xy0 = rad_x * rad_x + rad_y * rad_y;
-                if (no_shift && xy0 > 64.0) continue;
+                float4 c[NTERM];
+                const float4 *t = tab + (Z - 1) * kPot3Terms;
+#pragma unroll
+                for (int i = 0; i < NTERM; i++) c[i] = __ldg(t + i);
+                const double zl = sz[l];
+                double ry_s = ry;
                 for (int h = 0; h <= p.integrals; h++) {
-                    rad_x -= p.shift_x;
-                    rad_y -= p.shift_y;
-                    const double xyrad2 = no_shift ? xy0 : rad_x * rad_x + rad_y * rad_y;
-                    const double im_pos_z = current_z - h * p.dz * int_r;
-                    const double rad_z = im_pos_z - sz[l];
-                    if (xyrad2 <= 64.0 && rad_z <= 3.0) {
-                        const float rad = fmaxf(sqrtf((float)(xyrad2 + rad_z * rad_z)), r_min);
-                        const float p1 = pot3_eval<FORM>(tab, p.i_count, Z, rad);
-                        sumz += (h != 0) * (p1 + p2) * 0.5f;
-                        p2 = p1;
+#pragma unroll
+                    for (int m = 0; m < PX; m++) rx[m] -= p.shift_x;   // cumulative (full_3d_d.cl:244-246)
+                    ry_s -= p.shift_y;
+                    const double rad_z = (current_z - h * p.dz * int_r) - zl;
+                    if (rad_z <= 3.0) {
+                        const double yys = no_shift ? yy : ry_s * ry_s;
+                        const double zz = rad_z * rad_z;
+#pragma unroll
+                        for (int m = 0; m < PX; m++) {
+                            const double xyr = no_shift ? xy0[m] : rx[m] * rx[m] + yys;
+                            if (in[m] && xyr <= 64.0) {
+                                const float rad = fmaxf(sqrtf((float)(xyr + zz)), r_min);
+                                const float p1 = pot3_eval_r<FORM>(c, rad);
+                                sum[m] += (h != 0) * (p1 + q[m]) * 0.5f;
+                                q[m] = p1;
+                            }
+                        }
                     }
                 }
             }
         }
     }
-    if (xid < p.width && yid < p.height)
-        write_trans<float>(out + (size_t)blockIdx.z * p.width * p.height + (size_t)yid * p.width + xid,
-                           (float)(sub_slice_thickness * p.sigma) * sumz);
+    const float sc = (float)(sub_slice_thickness * p.sigma);
+    if (yid < p.height) {
+        float2 *o = out + (size_t)blockIdx.z * p.width * p.height + (size_t)yid * p.width;
+#pragma unroll
+        for (int m = 0; m < PX; m++)
+            if (xid0 + m * TX < p.width) write_trans<float>(o + xid0 + m * TX, sc * sum[m]);
+    }
 }
 
 }  // namespace ms
