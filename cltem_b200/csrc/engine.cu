@@ -240,6 +240,36 @@ std::vector<float4> pot3_table(int form, int i_count, const std::vector<double> 
     return t;
 }
 
+// The per-element term table of the FP32 projected kernel (potential.cuh, k_potential_projected_f): for each
+// element Z = 1..max_z and term, float2 at (Z - 1) * kPotPTerms + term, formed in FP64 and rounded once.
+std::vector<float2> potp_table(int form, int i_count, const std::vector<double> &v, int max_z) {
+    constexpr double kLog2e = 1.44269504088896340736;
+    std::vector<float2> t((size_t)std::max(max_z, 0) * kPotPTerms, make_float2(0, 0));
+    const int stride = form == 0 ? 12 : 10;
+    for (int Z = 1; Z <= max_z; Z++) {
+        const double *q = v.data() + (size_t)(Z - 1) * stride;
+        float2 *o = t.data() + (size_t)(Z - 1) * kPotPTerms;
+        for (int i = 0; i < i_count; i++) {
+            if (form == 2) {   // Lobato
+                const double b = q[i + 5];
+                if (!(b > 0)) continue;
+                const double bir = 1.0 / std::sqrt(b);
+                o[i] = make_float2((float)(945.090144399935 * q[i] * (bir * bir * bir)), (float)(2.0 * M_PI * bir));
+            } else if (form == 1) {   // Peng
+                const double b = q[i + 5];
+                if (!(b > 0)) continue;
+                o[i] = make_float2((float)(150.4121417 * q[i] / b), (float)(-M_PI * M_PI / b * kLog2e));
+            } else {   // Kirkland: K0 terms at 0..2, Gaussian terms at 3..5
+                const double a = q[2 * i], b = q[2 * i + 1];
+                if (b >= 0) o[i] = make_float2((float)(300.8242834 * a), (float)(2.0 * M_PI * std::sqrt(b)));
+                const double c = q[2 * i_count + 2 * i], d = q[2 * i_count + 2 * i + 1];
+                if (d > 0) o[3 + i] = make_float2((float)(150.4121417 * c / d), (float)(-M_PI * M_PI / d * kLog2e));
+            }
+        }
+    }
+    return t;
+}
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -251,6 +281,8 @@ struct Ctx {
     size_t prm_n = 0;
     float4 *pot3_tab = nullptr;   // pot3_table of the loaded parameterisation (FP32 full-3D kernel)
     size_t pot3_n = 0;
+    float2 *potp_tab = nullptr;   // potp_table of the loaded parameterisation (FP32 projected kernel)
+    size_t potp_n = 0;
     std::map<int, void *> tw_f, tw_d;   // twiddle tables per size
     std::mutex mtx;
 
@@ -308,6 +340,7 @@ struct Ctx {
         cudaFree(prm_d);
         cudaFree(prm_f);
         cudaFree(pot3_tab);
+        cudaFree(potp_tab);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -715,7 +748,7 @@ struct Sim : SimBase {
     void potentials(C *out, int slice0, int count) {
         timed(st(), MSLICE_K_POTENTIAL, (double)count * NN * sizeof(C), [&] {
             launch_potential<R>(st(), cfg.full3d != 0, out, count, axs.p, ays.p, azs.p, aZs.p, block_start.p, params_dev(),
-                                ctx->pot3_tab, pot_params(slice0));
+                                ctx->pot3_tab, ctx->potp_tab, pot_params(slice0));
         });
         ctx->launches++;
     }
@@ -1552,7 +1585,7 @@ struct Sim : SimBase {
                 grad_v<R>(st(), NN, E.p + (size_t)s * NN, gT.p, g.sigma, gV.p);
                 const int a0 = hbs[(size_t)s * nb], a1 = hbs[(size_t)(s + 1) * nb];
                 atom_grad<R>(st(), a0, a1 - a0, axs.p, ays.p, aZs.p, gV.p, N, g.sim_x[0], g.sim_y[0], g.real_scale,
-                             ctx->params.form, params_dev(), ctx->params.i_count, gxy.p, gwork.p);
+                             ctx->params.form, params_dev(), ctx->params.i_count, ctx->potp_tab, gxy.p, gwork.p);
                 ctx->launches += 5;
             }
         }
@@ -1732,6 +1765,11 @@ int mslice_params_load(mslice_ctx *ctx, int form, int i_per_atom, const double *
         c.pot3_n = t3.size();
         c.pot3_tab = (float4 *)c.alloc(t3.size() * sizeof(float4));
         MS_CUDA(cudaMemcpy(c.pot3_tab, t3.data(), t3.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        if (c.potp_tab) { c.release(c.potp_tab, c.potp_n * sizeof(float2)); c.potp_tab = nullptr; }
+        const std::vector<float2> tp = ms::potp_table(form, i_per_atom, c.params.values, c.params.max_z);
+        c.potp_n = tp.size();
+        c.potp_tab = (float2 *)c.alloc(tp.size() * sizeof(float2));
+        MS_CUDA(cudaMemcpy(c.potp_tab, tp.data(), tp.size() * sizeof(float2), cudaMemcpyHostToDevice));
     });
 }
 

@@ -12,6 +12,8 @@
 #include "adjoint_ops.h"
 #include "potential.cuh"
 
+#include <type_traits>
+
 namespace ms {
 
 // d/drho of kirkland_p / peng_p / lobato_p (potential.cuh), using K0' = -K1 and K1' = -K0 - K1/x
@@ -101,6 +103,90 @@ k_atom_grad(int a0, const double *__restrict__ ax, const double *__restrict__ ay
     }
 }
 
+// The FP32 gradient of the FP32 projected kernel's evaluation (k_potential_projected_f): the terms of the
+// table (potential.cuh, potp_table) differentiated with K0' = -K1 and K1' = -K0 - K1/x, evaluated by the same
+// FP32 K0 / K1. Same blocks, bands, pixel offsets, r_min and 8 Å limits as k_atom_grad.
+template <int FORM>
+__device__ __forceinline__ float dpotp_drho(const float2 (&c)[FORM == 0 ? 6 : 5], float rho) {
+    constexpr float kLn2x2 = 1.38629436111989061883f;   // 2 ln 2
+    if constexpr (FORM == 0) {
+        const float r2 = rho * rho;
+        float s = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 3; i++) s -= c[i].x * c[i].y * k1f(c[i].y * rho);
+#pragma unroll
+        for (int i = 0; i < 3; i++) s += c[3 + i].x * ex2a(c[3 + i].y * r2) * (kLn2x2 * c[3 + i].y * rho);
+        return s;
+    } else if constexpr (FORM == 1) {
+        const float r2 = rho * rho;
+        float s = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 5; i++) s += c[i].x * ex2a(c[i].y * r2) * (kLn2x2 * c[i].y * rho);
+        return s;
+    } else {
+        float s = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 5; i++) {
+            const float x = c[i].y * rho;
+            s -= c[i].x * c[i].y * (k1f(x) + rho * k0f(x));
+        }
+        return s;
+    }
+}
+
+template <int FORM>
+__global__ void __launch_bounds__(256)
+k_atom_grad_f(int a0, const double *__restrict__ ax, const double *__restrict__ ay, const int *__restrict__ aZ,
+              const double *__restrict__ gV, int n, double startx, double starty, double dx,
+              const float2 *__restrict__ tab, double *__restrict__ work) {
+    constexpr int NTERM = FORM == 0 ? 6 : 5;
+    __shared__ double red[2][8];
+    const int a = a0 + blockIdx.x;
+    const double xa = ax[a], ya = ay[a];
+    float2 c[NTERM];
+    const float2 *t = tab + (aZ[a] - 1) * kPotPTerms;
+#pragma unroll
+    for (int i = 0; i < NTERM; i++) c[i] = __ldg(t + i);
+    const float r_min2 = (float)(0.0625 * dx * dx);   // (dx / 4)^2
+    int ix0 = (int)floor((xa - 8.0 - startx) / dx), ix1 = (int)ceil((xa + 8.0 - startx) / dx);
+    int iy0 = (int)floor((ya - 8.0 - starty) / dx), iy1 = (int)ceil((ya + 8.0 - starty) / dx);
+    ix0 = max(ix0, 0); iy0 = max(iy0, 0); ix1 = min(ix1, n - 1); iy1 = min(iy1, n - 1);
+    const int rows = iy1 - iy0 + 1;
+    const int r0 = iy0 + (int)(((long long)rows * blockIdx.y) / kGatherBands);
+    const int r1 = iy0 + (int)(((long long)rows * (blockIdx.y + 1)) / kGatherBands) - 1;
+    const double ox = startx - xa, oy = starty - ya;
+    float gx = 0, gy = 0;
+    for (int py = r0 + (int)threadIdx.y; py <= r1; py += 8) {
+        const float ry = (float)(oy + py * dx);
+        const double *grow = gV + (size_t)py * n;
+        for (int px = ix0 + (int)threadIdx.x; px <= ix1; px += 32) {
+            const float rx = (float)(ox + px * dx);
+            const float rho2 = rx * rx + ry * ry;
+            if (rho2 > r_min2 && rho2 <= 64.0f) {
+                const float rho = sqrtf(rho2);
+                const float f = (float)grow[px] * __fdividef(dpotp_drho<FORM>(c, rho), rho);
+                gx -= f * rx;   // d rho / d x_a = -rx / rho
+                gy -= f * ry;
+            }
+        }
+    }
+    double sx = (double)gx, sy = (double)gy;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_down_sync(0xffffffffu, sx, o);
+        sy += __shfl_down_sync(0xffffffffu, sy, o);
+    }
+    if (threadIdx.x == 0) { red[0][threadIdx.y] = sx; red[1][threadIdx.y] = sy; }
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        double tx = 0, ty = 0;
+        for (int i = 0; i < 8; i++) { tx += red[0][i]; ty += red[1][i]; }
+        const size_t w = ((size_t)blockIdx.x * kGatherBands + blockIdx.y) * 2;
+        work[w] = tx;
+        work[w + 1] = ty;
+    }
+}
+
 __global__ void k_atom_grad_sum(int a0, int count, const double *__restrict__ work, double *__restrict__ gxy) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
@@ -115,11 +201,17 @@ __global__ void k_atom_grad_sum(int a0, int count, const double *__restrict__ wo
 
 template <class T>
 void atom_grad(cudaStream_t s, int a0, int count, const double *ax, const double *ay, const int *aZ, const double *gV,
-               int n, double startx, double starty, double dx, int form, const T *prm, int i_lim, double *gxy,
-               double *work) {
+               int n, double startx, double starty, double dx, int form, const T *prm, int i_lim, const float2 *tabp,
+               double *gxy, double *work) {
     if (count <= 0) return;
-    k_atom_grad<T><<<dim3(count, kGatherBands), dim3(32, 8), 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, form,
-                                                                    prm, i_lim, work);
+    const dim3 grd(count, kGatherBands), blk(32, 8);
+    if (std::is_same<T, float>::value && tabp) {
+        if (form == 0) k_atom_grad_f<0><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
+        else if (form == 1) k_atom_grad_f<1><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
+        else k_atom_grad_f<2><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
+    } else {
+        k_atom_grad<T><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, form, prm, i_lim, work);
+    }
     MS_CUDA(cudaGetLastError());
     k_atom_grad_sum<<<(count + 127) / 128, 128, 0, s>>>(a0, count, work, gxy);
     MS_CUDA(cudaGetLastError());
@@ -127,8 +219,8 @@ void atom_grad(cudaStream_t s, int a0, int count, const double *ax, const double
 int atom_grad_work_doubles(int max_count) { return 2 * kGatherBands * max_count; }
 
 template void atom_grad<float>(cudaStream_t, int, int, const double *, const double *, const int *, const double *, int,
-                               double, double, double, int, const float *, int, double *, double *);
+                               double, double, double, int, const float *, int, const float2 *, double *, double *);
 template void atom_grad<double>(cudaStream_t, int, int, const double *, const double *, const int *, const double *, int,
-                                double, double, double, int, const double *, int, double *, double *);
+                                double, double, double, int, const double *, int, const float2 *, double *, double *);
 
 }  // namespace ms

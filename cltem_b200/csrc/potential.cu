@@ -28,15 +28,33 @@ bool potential_3d_f(cudaStream_t s, dim3 grd, dim3 blk, cplx<T> *out, const doub
     }
 }
 
+// the FP32 projected kernel (a template, so that the FP64 build discards it)
+template <class T>
+bool potential_projected_f(cudaStream_t s, dim3 grd, cplx<T> *out, const double *ax, const double *ay, const int *aZ,
+                           const int *block_start, const float2 *tabp, const PotParams &p) {
+    if constexpr (std::is_same<T, float>::value) {
+        constexpr int PX = kPotPPx;
+        const dim3 b(16 / PX, 16);   // PX pixels a thread
+        if (p.form == 0) k_potential_projected_f<0, PX><<<grd, b, 0, s>>>(out, ax, ay, aZ, block_start, tabp, p);
+        else if (p.form == 1) k_potential_projected_f<1, PX><<<grd, b, 0, s>>>(out, ax, ay, aZ, block_start, tabp, p);
+        else k_potential_projected_f<2, PX><<<grd, b, 0, s>>>(out, ax, ay, aZ, block_start, tabp, p);
+        MS_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        return false;
+    }
+}
+
 template <>
 void launch_potential<MS_REAL>(cudaStream_t s, bool full3d, cplx<MS_REAL> *out, int n_slices, const double *ax,
                                const double *ay, const double *az, const int *aZ, const int *block_start,
-                               const MS_REAL *prm, const float4 *tab3, const PotParams &p) {
+                               const MS_REAL *prm, const float4 *tab3, const float2 *tabp, const PotParams &p) {
     using T = MS_REAL;
     if (p.width % 16 || p.height % 16) throw std::runtime_error("potential grid must be a multiple of 16");
     dim3 blk(16, 16), grd(p.width / 16, p.height / 16, n_slices);
     if (n_slices <= 0) return;
     if (full3d && tab3 && potential_3d_f<T>(s, grd, blk, out, ax, ay, az, aZ, block_start, tab3, p)) return;
+    if (!full3d && tabp && potential_projected_f<T>(s, grd, out, ax, ay, aZ, block_start, tabp, p)) return;
     if (full3d) {
         if (p.form == 0) k_potential_3d<T, 0><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
         else if (p.form == 1) k_potential_3d<T, 1><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);

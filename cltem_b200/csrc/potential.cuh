@@ -509,4 +509,211 @@ k_potential_3d_f(float2 *__restrict__ out, const double *__restrict__ ax, const 
     }
 }
 
+// ---- FP32 projected potentials ---------------------------------------------------------------------
+// K0 / K1 by the same rational approximations as bessk0 / bessk1 (projected_d.cl:57-102), in FP32: the
+// coefficients are the FP64 ones rounded to float at compile time (bessk0<float> rounds them at run
+// time); exp is ex2.approx.ftz, the divisions __fdividef and 1/sqrt rsqrtf (errors of a few ulp).
+template <class... C> __device__ __forceinline__ float hornerf(float, float c0) { return c0; }
+template <class... C> __device__ __forceinline__ float hornerf(float x, float c0, C... c) {
+    return fmaf(hornerf(x, c...), x, c0);   // c0 + x (c1 + x (c2 + ...))
+}
+#define F(v) ((float)(v))
+__device__ __forceinline__ float k0f(float x) {
+    if (x <= 1.0f) {
+        const float z = x * x, w = 1.0f - z;
+        const float term = hornerf(z, F(1.0), F(2.346487949187396e-1), F(1.187082088663404e-2),
+                                 F(2.150707366040937e-4), F(1.425433617130587e-6)) * logf(x) *
+                           __fdividef(1.0f, hornerf(w, F(9.847324170755358e-1), F(1.518396076767770e-2),
+                                                    F(8.362215678646257e-5)));
+        return hornerf(z, F(1.159315156584126e-1), F(2.770731240515333e-1), F(2.066458134619875e-2),
+                       F(4.574734709978264e-4), F(3.454715527986737e-6)) *
+               __fdividef(1.0f, hornerf(w, F(9.836249671709183e-1), F(1.627693622304549e-2), F(9.809660603621949e-5))) -
+               term;
+    }
+    const float z = __fdividef(1.0f, x);
+    return ex2a(-1.44269504088896341f * x) *
+           hornerf(z, F(1.253314137315499), F(1.475731032429900e1), F(6.123767403223466e1),
+                   F(1.121012633939949e2), F(9.285288485892228e1), F(3.198289277679660e1),
+                   F(3.595376024148513), F(6.160228690102976e-2)) *
+           __fdividef(1.0f, hornerf(z, F(1.0), F(1.189963006673403e1), F(5.027773590829784e1),
+                                   F(9.496513373427093e1),
+                   F(8.318077493230258e1), F(3.181399777449301e1), F(4.443672926432041),
+                   F(1.408295601966600e-1))) * rsqrtf(x);
+}
+__device__ __forceinline__ float k1f(float x) {
+    if (x <= 1.0f) {
+        const float z = x * x, w = 1.0f - z;
+        const float term = hornerf(z, F(0.5), F(5.598072040178741e-2), F(1.818666382168295e-3),
+                                 F(2.397509908859959e-5), F(1.239567816344855e-7)) * logf(x) *
+                           __fdividef(1.0f, hornerf(w, F(9.870202601341150e-1), F(1.292092053534579e-2),
+                                                    F(5.881933053917096e-5)));
+        return x * (hornerf(z, F(-3.079657578292062e-1), F(-8.109417631822442e-2), F(-3.477550948593604e-3),
+                            F(-5.385594871975406e-5), F(-3.110372465429008e-7)) *
+                    __fdividef(1.0f, hornerf(w, F(9.861813171751389e-1), F(1.375094061153160e-2),
+                                             F(6.774221332947002e-5))) +
+                    term) +
+               __fdividef(1.0f, x);
+    }
+    const float z = __fdividef(1.0f, x);
+    return ex2a(-1.44269504088896341f * x) *
+           hornerf(z, F(1.253314137315502), F(1.457171340220454e1), F(6.063161173098803e1),
+                   F(1.147386690867892e2), F(1.040442011439181e2), F(4.356596656837691e1),
+                   F(7.265230396353690), F(3.144418558991021e-1)) *
+           __fdividef(1.0f, hornerf(z, F(1.0), F(1.125154514806458e1), F(4.427488496597630e1),
+                                   F(7.616113213117645e1),
+                   F(5.863377227890893e1), F(1.850303673841586e1), F(1.857244676566022),
+                   F(2.538540887654872e-2))) * rsqrtf(x);
+}
+#undef F
+
+// Table of the FP32 projected kernel, per element Z and term i, float2 at (Z - 1) * kPotPTerms + i (terms
+// beyond the parameterisation's count are zero; projected_d.cl:104-181):
+// - Kirkland, i < 3: (300.824·a, 2π√b), the term x·K0(y·r); i = 3 + j: (150.412·c/d, -π²·log2(e)/d), the
+//   term x·exp2(y·r²).
+// - Lobato, i < 5: (945.090·a·b^-3/2, 2π/√b), the term x·(K0(y·r) + r·K1(y·r)).
+// - Peng, i < 5: (150.412·a/b, -π²·log2(e)/b), the term x·exp2(y·r²).
+constexpr int kPotPTerms = 6;
+#ifndef MS_POTP_PX
+#define MS_POTP_PX 4
+#endif
+constexpr int kPotPPx = MS_POTP_PX;   // pixels a thread in the FP32 projected kernel
+
+template <int FORM>
+__device__ __forceinline__ float potp_eval(const float2 (&c)[FORM == 0 ? 6 : 5], float rad) {
+    if constexpr (FORM == 0) {
+        const float r2 = rad * rad;
+        float suml = 0.0f, sumg = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 3; i++) suml += c[i].x * k0f(c[i].y * rad);
+#pragma unroll
+        for (int i = 0; i < 3; i++) sumg += c[3 + i].x * ex2a(c[3 + i].y * r2);
+        return suml + sumg;
+    } else if constexpr (FORM == 1) {
+        const float r2 = rad * rad;
+        float sum = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 5; i++) sum += c[i].x * ex2a(c[i].y * r2);
+        return sum;
+    } else {
+        float sum = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 5; i++) {
+            const float x = c[i].y * rad;
+            sum += c[i].x * (k0f(x) + rad * k1f(x));
+        }
+        return sum;
+    }
+}
+
+// The FP32 projected potential: the bins, atoms and 8 Å test of k_potential_projected, with
+// - PX pixels a thread (x + m·16/PX of its tile row), sharing the atom loads and the per-atom table reads;
+// - the tilt geometry in FP64 with z' / tan θ taken as z' · (1 / tan θ), and without tilt (θ = 0) the plain
+//   distance, which the tilt terms change by under 1e-32 Å² there;
+// - the form from the per-element table and the FP32 Bessel functions above.
+// grid (W/16, H/16, n_slices), block (16/PX, 16)
+template <int FORM, int PX>
+__global__ void __launch_bounds__(256 / PX)
+k_potential_projected_f(float2 *__restrict__ out, const double *__restrict__ ax, const double *__restrict__ ay,
+                        const int *__restrict__ aZ, const int *__restrict__ block_start, const float2 *__restrict__ tab,
+                        PotParams p) {
+    constexpr int NTERM = FORM == 0 ? 6 : 5;
+    constexpr int TX = 16 / PX, NTH = 256 / PX;
+    __shared__ double sx[kAtomChunk], sy[kAtomChunk];
+    __shared__ int sZ[kAtomChunk];
+    __shared__ int row_start[kPot3Rows], row_off[kPot3Rows + 1];
+    const int lid = threadIdx.x + TX * threadIdx.y;
+    const int xid0 = blockIdx.x * 16 + threadIdx.x, yid = blockIdx.y * 16 + threadIdx.y;
+    const int slice = blockIdx.z + p.slice0;
+    int si, ei, sj, ej;
+    tile_bins(p, blockIdx.x, blockIdx.y, si, ei, sj, ej);
+    int k = slice;
+    if (k < 0) k = 0;
+    if (k >= p.total_slices) k = p.total_slices - 1;
+    const bool tilt = p.beam_theta_mrad != 0.0;
+    const double beam_theta = M_PI_2 - p.beam_theta_mrad * 0.001;
+    const double cos_beam_phi = cos(p.beam_phi), sin_beam_phi = sin(p.beam_phi);
+    const double sin_beam_2theta = sin(2.0 * beam_theta);
+    const double inv_tan_beam_theta = 1.0 / tan(beam_theta);
+    double pos_x[PX];
+#pragma unroll
+    for (int m = 0; m < PX; m++) pos_x[m] = p.startx + (xid0 + m * TX) * p.pixelscale;
+    const double im_pos_y = p.starty + yid * p.pixelscale;
+    const float r_min = (float)(0.25 * p.pixelscale);
+    float sum[PX];
+#pragma unroll
+    for (int m = 0; m < PX; m++) sum[m] = 0.0f;
+    const size_t nb = (size_t)p.blocks_x * p.blocks_y;
+    const int n_rows = ej - sj + 1;
+    for (int r0 = 0; r0 < n_rows; r0 += kPot3Rows) {
+        const int nr = min(kPot3Rows, n_rows - r0);
+        __syncthreads();   // the previous pass's readers of the row tables and the chunk are done
+        if (lid < nr) {
+            const int j = sj + r0 + lid;
+            const int start = block_start[k * nb + p.blocks_x * j + si];
+            row_start[lid] = start;
+            row_off[lid + 1] = block_start[k * nb + p.blocks_x * j + ei + 1] - start;   // count, summed below
+        }
+        __syncthreads();
+        if (lid == 0) {
+            row_off[0] = 0;
+            for (int r = 0; r < nr; r++) row_off[r + 1] += row_off[r];
+        }
+        __syncthreads();
+        const int total = row_off[nr];
+        for (int c0 = 0; c0 < total; c0 += kAtomChunk) {
+            const int cn = min(kAtomChunk, total - c0);
+            __syncthreads();
+            for (int w = lid; w < cn; w += NTH) {
+                const int f = c0 + w;
+                int lo = 0, hi = nr - 1;   // the last row whose offset is <= f (a non-empty row holds f)
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (row_off[mid] <= f) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int a = row_start[lo] + (f - row_off[lo]);
+                sx[w] = ax[a]; sy[w] = ay[a]; sZ[w] = aZ[a];
+            }
+            __syncthreads();
+            for (int l = 0; l < cn; l++) {
+                const double xl = sx[l];
+                const double rad_y = im_pos_y - sy[l];
+                double rad2[PX];
+                bool any = false;
+#pragma unroll
+                for (int m = 0; m < PX; m++) {
+                    const double rad_x = pos_x[m] - xl;
+                    if (tilt) {
+                        const double zp = -0.5 * (rad_x * cos_beam_phi + rad_y * sin_beam_phi) * sin_beam_2theta;
+                        const double zt = zp * inv_tan_beam_theta;
+                        const double xp = rad_x + zt * cos_beam_phi, yp = rad_y + zt * sin_beam_phi;
+                        rad2[m] = zp * zp + xp * xp + yp * yp;
+                    } else {
+                        rad2[m] = rad_x * rad_x + rad_y * rad_y;
+                    }
+                    any = any || rad2[m] <= 64.0;
+                }
+                if (!any) continue;
+                float2 c[NTERM];
+                const float2 *t = tab + (sZ[l] - 1) * kPotPTerms;
+#pragma unroll
+                for (int i = 0; i < NTERM; i++) c[i] = __ldg(t + i);
+#pragma unroll
+                for (int m = 0; m < PX; m++) {
+                    if (rad2[m] <= 64.0) {
+                        const float rad = fmaxf(sqrtf((float)rad2[m]), r_min);
+                        sum[m] += potp_eval<FORM>(c, rad);
+                    }
+                }
+            }
+        }
+    }
+    if (yid < p.height) {
+        float2 *o = out + (size_t)blockIdx.z * p.width * p.height + (size_t)yid * p.width;
+#pragma unroll
+        for (int m = 0; m < PX; m++)
+            if (xid0 + m * TX < p.width) write_trans<float>(o + xid0 + m * TX, (float)p.sigma * sum[m]);
+    }
+}
+
 }  // namespace ms

@@ -8,11 +8,11 @@ namespace ms {
 struct PotParams;
 
 // Launch the projected (full3d = false) or full 3-D potential kernel for `n_slices` consecutive slices
-// starting at p.slice0; out holds n_slices res*res complex transmission values. tab3: the FP32 full-3D
-// term table (pot3_table), used by the FP32 build's full-3D kernel; may be null otherwise.
+// starting at p.slice0; out holds n_slices res*res complex transmission values. tab3 / tabp: the FP32
+// full-3D and projected term tables (pot3_table, potp_table), used by the FP32 build's kernels when set.
 template <class T>
 void launch_potential(cudaStream_t s, bool full3d, cplx<T> *out, int n_slices, const double *ax, const double *ay,
                       const double *az, const int *aZ, const int *block_start, const T *prm, const float4 *tab3,
-                      const PotParams &p);
+                      const float2 *tabp, const PotParams &p);
 
 }  // namespace ms
