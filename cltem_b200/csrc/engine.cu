@@ -242,9 +242,11 @@ std::vector<float4> pot3_table(int form, int i_count, const std::vector<double> 
 
 // The per-element term table of the FP32 projected kernel (potential.cuh, k_potential_projected_f): for each
 // element Z = 1..max_z and term, float2 at (Z - 1) * kPotPTerms + term, formed in FP64 and rounded once.
+// Terms the parameterisation does not use are (0, 1): a zero weight on a finite K0(r), K1(r) or exp2(r²)
+// (a zero argument would make K0 infinite and the zero term NaN).
 std::vector<float2> potp_table(int form, int i_count, const std::vector<double> &v, int max_z) {
     constexpr double kLog2e = 1.44269504088896340736;
-    std::vector<float2> t((size_t)std::max(max_z, 0) * kPotPTerms, make_float2(0, 0));
+    std::vector<float2> t((size_t)std::max(max_z, 0) * kPotPTerms, make_float2(0, 1));
     const int stride = form == 0 ? 12 : 10;
     for (int Z = 1; Z <= max_z; Z++) {
         const double *q = v.data() + (size_t)(Z - 1) * stride;
@@ -261,7 +263,7 @@ std::vector<float2> potp_table(int form, int i_count, const std::vector<double> 
                 o[i] = make_float2((float)(150.4121417 * q[i] / b), (float)(-M_PI * M_PI / b * kLog2e));
             } else {   // Kirkland: K0 terms at 0..2, Gaussian terms at 3..5
                 const double a = q[2 * i], b = q[2 * i + 1];
-                if (b >= 0) o[i] = make_float2((float)(300.8242834 * a), (float)(2.0 * M_PI * std::sqrt(b)));
+                if (b > 0) o[i] = make_float2((float)(300.8242834 * a), (float)(2.0 * M_PI * std::sqrt(b)));
                 const double c = q[2 * i_count + 2 * i], d = q[2 * i_count + 2 * i + 1];
                 if (d > 0) o[3 + i] = make_float2((float)(150.4121417 * c / d), (float)(-M_PI * M_PI / d * kLog2e));
             }

@@ -156,6 +156,29 @@ def test_transmission_full3d(gpu_ctx, oracle, params_all, dp, form, tilt):
         assert rel_l2(sim.transmission(sl, True), osim.transmission(sl, True)) < TOL[dp]
 
 
+@pytest.mark.parametrize("dp", [True, False])
+@pytest.mark.parametrize("form", ["kirkland", "peng", "lobato"])
+@pytest.mark.parametrize("full3d", [False, True])
+def test_transmission_one_term(gpu_ctx, oracle, params_all, dp, form, full3d):
+    # a parameterisation that uses only the first term of each kind (i_per_atom = 1): the kernels index the
+    # table with the full per-element stride and sum fewer terms
+    from cltem_b200.params import Parameterisation
+    full = params_all[form]
+    p = Parameterisation(full.name + "_1", full.form, 1, full.values)
+    s, st = small_cbed(double_precision=dp, form=form) if full3d else small_stem(double_precision=dp)
+    sim = _sim(gpu_ctx, p, s)
+    osim = _osim(oracle, p, s)
+    sim.set_atoms(st)
+    osim.set_atoms(st)
+    sim.build_transmission()
+    osim.build_transmission()
+    for sl in range(sim.geo.n_slices):
+        t = sim.transmission(sl, False)
+        assert np.all(np.isfinite(t))
+        assert rel_l2(t, osim.transmission(sl, False)) < TOL[dp]
+    gpu_ctx.load_params(params_all["kirkland"])
+
+
 # ---------------------------------------------------------------------------------------------------
 # Propagator and probe
 # ---------------------------------------------------------------------------------------------------
