@@ -528,8 +528,20 @@ def main():
         g1.synchronize()
         pms = g0.elapsed_time(g1)
         pv = len(pix) * S / (pms / 1000.0)
+        # the fused FP64 engine on the same configuration (one batch of 512 probes): the design's gain at the
+        # reference's own precision
+        fpix = np.arange(512, dtype=np.int32)
+        simd.stem(fpix[:64])   # untimed warm-up (batch buffers)
+        torch.cuda.synchronize()
+        g0.record(ext)
+        simd.stem(fpix)
+        g1.record(ext)
+        g1.synchronize()
+        fv = len(fpix) * S / (g0.elapsed_time(g1) / 1000.0)
         plain = {"value": pv, "unit": UNIT, "sample": f"{len(pix)} probes x {S} slices, FP64, one probe at a time",
-                 "fused_fp32_over_plain_fp64": value / pv}
+                 "fused_fp32_over_plain_fp64": value / pv,
+                 "fused_fp64": {"value": fv, "unit": UNIT, "sample": f"{len(fpix)} probes x {S} slices in one batch",
+                                "fused_fp64_over_plain_fp64": fv / pv}}
         simd.close()
         cpu = cpu_baseline_leg(args.cpu_probes)
 
