@@ -181,12 +181,13 @@ def run_reference(args):
     ob.lib()
     threads = ob.num_threads()
     n_probes = max(4, args.cpu_probes // 4)
+    # the workload's precision (FP32, the reference's _f path), as the GPU arm
     for w in range(args.warmup):   # untimed: a tiny sample
-        cpu_sample(1, double_precision=True, seed=100 + w)
+        cpu_sample(1, double_precision=False, seed=100 + w)
     vals, infos = [], []
     t0 = time.perf_counter()
     for k in range(args.steps):
-        v, info = cpu_sample(n_probes, double_precision=True, seed=k)
+        v, info = cpu_sample(n_probes, double_precision=False, seed=k)
         vals.append(v)
         infos.append(info)
     wall = time.perf_counter() - t0
@@ -196,12 +197,12 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "grid": 512, "probes": 4096, "slices": S,
                    "parallelism": "host threads (OpenMP)", "sample_wall_s": wall},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": (f"per step: transmission build of {S} slices + {n_probes} of 4096 probes "
-                                    f"through all slices of one phonon configuration, FP64 (the reference's _d path), "
+                                    f"through all slices of one phonon configuration, FP32 (the reference's _f path), "
                                     f"scaled to a 4096-probe configuration; the reference's OpenCL CPU-device build "
                                     f"needs OpenCL headers/ICD and clFFT, absent here")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
