@@ -216,6 +216,25 @@ def test_stem_parity(gpu_ctx, oracle, kirkland, dp, interval):
         assert rel_l2(got[:, d], ref[:, d]) < TOL[dp], (d, got[:, d], ref[:, d])
 
 
+@pytest.mark.parametrize("dp", [True, False])
+@pytest.mark.parametrize("res", [64, 96, 128, 384, 512, 768, 1024])
+def test_stem_parity_sizes(gpu_ctx, oracle, kirkland, dp, res):
+    # the fused step kernels at every plan the engine picks: radix-8 and 3 * 2^k columns, the two-column
+    # FP32 step, the wide FP32 rows at 512 and 1024, the radix-8 rows elsewhere
+    s, st = small_stem(double_precision=dp, res=res, n=(2, 2, 2), scan=2)
+    s.cfg.allow_any_resolution = 1   # 64, 96, 128 and 384 are not in the reference's resolution list
+    sim = _sim(gpu_ctx, kirkland, s)
+    osim = _osim(oracle, kirkland, s)
+    sim.set_atoms(st)
+    osim.set_atoms(st)
+    osim.build_transmission()
+    pixels = np.arange(s.cfg.stem_pixels_x * s.cfg.stem_pixels_y, dtype=np.int32)
+    got = sim.stem(pixels)
+    ref = osim.stem(pixels)
+    for d in range(s.cfg.n_detectors):
+        assert rel_l2(got[:, d], ref[:, d]) < TOL[dp], (res, d)
+
+
 def test_stem_staged_phonon_average(gpu_ctx, oracle, kirkland):
     s, st = small_stem(double_precision=True)
     confs = phonons(st, 3)
