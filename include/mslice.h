@@ -225,7 +225,7 @@ int mslice_cbed_run(mslice_sim *sim, double *diff);
  * Any output pointer may be NULL. */
 int mslice_ctem_run(mslice_sim *sim, double *ew, double *diff, double *image);
 
-/* ---- differentiable CTEM ---------------------------------------------- */
+/* ---- differentiable CTEM (image loss and its gradients) ------------------------------------------- */
 /* Loss L = sum over pixels of (I - target)^2 for the CTEM objective-lens image I of the current atom
  * configuration (simulateImagePerfect, microscope/simulationctem.cpp:114-166), and its gradients by the
  * hand-written adjoint of the multislice: dL/d(x, y, z) of every atom passed to mslice_set_atoms (input
