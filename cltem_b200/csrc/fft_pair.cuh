@@ -1,4 +1,4 @@
-// fft_pair.cuh — the radix-8 Stockham plan of fft.cuh applied to two adjacent columns at once (FP32).
+// fft_pair.cuh — the Stockham plans of fft.cuh (2^k and 3·2^k) applied to two adjacent columns at once (FP32).
 //
 // A thread holds element m of its two columns in va[m], vb[m] (v[m] = x[t + m*NT] as in fft.cuh). Both
 // columns go through the same butterflies and twiddles in the same order as fft.cuh, so each column's

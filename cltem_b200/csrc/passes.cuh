@@ -264,11 +264,13 @@ k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTabl
     }
 }
 
-// The plain step (COL_STEP) of the FP32 radix-8 plans with each thread carrying two adjacent columns of
-// the tile: 16-byte loads, stores and shared-memory exchanges (fft_pair.cuh), and the propagator's cut
-// read as a row band per column (PropTables::ycut) instead of an FP64 test per element. Same arithmetic
-// per element as k_col_step<float, N, COL_STEP>. Up to 256 threads a block: 4 blocks per SM (64 registers
-// at 256 threads); 512 threads (4096²): 2 blocks.
+// The plain step (COL_STEP) of the FP32 column plans (2^k and 3·2^k) with each thread carrying two adjacent
+// columns of the tile: 16-byte loads, stores and shared-memory exchanges (fft_pair.cuh), and the
+// propagator's cut read as a row band per column (PropTables::ycut) instead of an FP64 test per element.
+// Same arithmetic per element as k_col_step<float, N, COL_STEP>. Up to 256 threads a block: 4 blocks per
+// SM (64 registers at 256 threads, 128 at 128); 512 threads (4096²): 2 blocks. Measured against the
+// one-column kernel in a 256-probe STEM run: 256² −12%, 384² −11%, 512² −5%, 768² −32%, 1024² −5%, 1536² −25%,
+// 2048² ±0, 3072² −13%, 4096² −18%, with bit-identical results.
 template <int N> struct PairCfg {
     using P = Plan<N>;
     static constexpr int COLS = ColCfg<N, float>::COLS;
@@ -278,7 +280,7 @@ template <int N> struct PairCfg {
     static constexpr size_t smem() { return sizeof(float2) * (size_t)N + sizeof(float4) * (size_t)N * PAIRS; }
 };
 template <int N> constexpr bool pair_columns() {
-    return Plan<N>::E == 8 && !ColCfg<N, float>::WIDE && ColCfg<N, float>::COLS >= 2;
+    return !ColCfg<N, float>::WIDE && ColCfg<N, float>::COLS >= 2;
 }
 
 template <int N>
