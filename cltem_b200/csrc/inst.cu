@@ -40,6 +40,24 @@ bool pair_step(cudaStream_t s, dim3 g, cplx<RR> *wave, const cplx<RR> *tw, PropT
     }
 }
 
+// the two-row step kernel of the FP32 non-wide row plans
+template <class RR> void rowpair_attrs() {
+    if constexpr (std::is_same<RR, float>::value && pair_rows<N>()) set_smem(k_row_step_pair<N>, RowPairCfg<N>::smem());
+}
+template <class RR>
+bool rowpair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans, const cplx<RR> *tw, RR a, int xa,
+                  int xb, int load_all, const int *tsel, size_t tstride) {
+    if constexpr (std::is_same<RR, float>::value && pair_rows<N>()) {
+        using PC = RowPairCfg<N>;
+        k_row_step_pair<N><<<dim3(N / (2 * PC::PAIRS), batch), dim3(Plan<N>::NT, PC::PAIRS), PC::smem(), s>>>(
+            wave, trans, tw, a, xa, xb, load_all, tsel, tstride);
+        MS_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        return false;
+    }
+}
+
 // kernel attributes are per device: set once for each device this process launches on
 bool g_attrs_done[64] = {};
 void ensure_attrs() {
@@ -51,6 +69,7 @@ void ensure_attrs() {
     set_smem(k_row_fft<R, N, +1>, RC::smem());
     set_smem(k_col_step<R, N, COL_STEP>, CC::smem());
     pair_attrs<R>();
+    rowpair_attrs<R>();
     set_smem(k_col_step<R, N, COL_STEP_DET>, CC::smem());
     set_smem(k_col_step<R, N, COL_DET_ONLY>, CC::smem());
     set_smem(k_col_fft<R, N, -1>, CC::smem());
@@ -70,6 +89,7 @@ inline dim3 col_block() { return dim3(CC::COLS, CC::P::NT); }
 void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a, int xa, int xb,
               int load_all, const int *tsel, size_t tstride) {
     ensure_attrs();
+    if (rowpair_step<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride)) return;
     k_row_step<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all, tsel, tstride);
     MS_CUDA(cudaGetLastError());
 }
