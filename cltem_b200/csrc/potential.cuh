@@ -324,7 +324,7 @@ k_potential_3d(cplx<T> *__restrict__ out, const double *__restrict__ ax, const d
 // It cuts the instructions per sample:
 // - Each thread computes kPot3Px pixels of its tile row. The atom loads, the per-atom table reads and the
 //   FP64 z tests are shared by its pixels.
-// - The distance is rounded once to FP32 and its square root taken in FP32.
+// - The squared distance is rounded once to FP32; one rsqrtf gives both the distance and its reciprocal.
 // - Each form is a sum of exponentials whose per-element constants come from a table built on the host
 //   in FP64 and rounded once (pot3_table). A thread reads an atom's terms once into registers, and takes
 //   exp as ex2.approx.ftz.f32 (relative error below 2^-22) of a pre-scaled exponent.
@@ -354,8 +354,7 @@ template <int FORM> struct Pot3N {
     static constexpr int G = FORM == 0 ? 3 : 0;
 };
 template <int FORM>
-__device__ __forceinline__ float pot3_eval_r(const float4 (&c)[Pot3N<FORM>::L + Pot3N<FORM>::G], float rad) {
-    const float inv = __fdividef(1.0f, rad);
+__device__ __forceinline__ float pot3_eval_r(const float4 (&c)[Pot3N<FORM>::L + Pot3N<FORM>::G], float rad, float inv) {
     if constexpr (FORM == 2) {
         float sum = 0.0f;
 #pragma unroll
@@ -411,6 +410,7 @@ k_potential_3d_f(float2 *__restrict__ out, const double *__restrict__ ax, const 
     for (int m = 0; m < PX; m++) pos_x[m] = p.startx + (xid0 + m * TX) * p.pixelscale;
     const double im_pos_y = p.starty + yid * p.pixelscale;
     const float r_min = (float)(0.25 * p.pixelscale);
+    const float inv_r_min = 1.0f / r_min;
     const bool no_shift = p.shift_x == 0.0 && p.shift_y == 0.0;
     const size_t nb = (size_t)p.blocks_x * p.blocks_y;
     const int nj = ej - sj + 1;
@@ -489,8 +489,10 @@ k_potential_3d_f(float2 *__restrict__ out, const double *__restrict__ ax, const 
                         for (int m = 0; m < PX; m++) {
                             const double xyr = no_shift ? xy0[m] : rx[m] * rx[m] + yys;
                             if (in[m] && xyr <= 64.0) {
-                                const float rad = fmaxf(sqrtf((float)(xyr + zz)), r_min);
-                                const float p1 = pot3_eval_r<FORM>(c, rad);
+                                const float r2f = (float)(xyr + zz);
+                                float inv = rsqrtf(r2f), rad = r2f * inv;
+                                if (!(rad >= r_min)) { rad = r_min; inv = inv_r_min; }   // also r2f = 0 (NaN)
+                                const float p1 = pot3_eval_r<FORM>(c, rad, inv);
                                 sum[m] += (h != 0) * (p1 + q[m]) * 0.5f;
                                 q[m] = p1;
                             }
