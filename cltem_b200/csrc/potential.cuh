@@ -514,57 +514,54 @@ k_potential_3d_f(float2 *__restrict__ out, const double *__restrict__ ax, const 
 // ---- FP32 projected potentials ---------------------------------------------------------------------
 // K0 / K1 by the same rational approximations as bessk0 / bessk1 (projected_d.cl:57-102), in FP32: the
 // coefficients are the FP64 ones rounded to float at compile time (bessk0<float> rounds them at run
-// time); exp is ex2.approx.ftz, the divisions __fdividef and 1/sqrt rsqrtf (errors of a few ulp).
+// time). exp is ex2.approx.ftz and log __logf (absolute error near 2^-21 on (0, 1], where the log term
+// stays below the rational part); each branch's quotients share one __fdividef, and for x > 1 one rsqrtf
+// gives both 1/sqrt(x) and 1/x. Errors of a few ulp of the result.
 template <class... C> __device__ __forceinline__ float hornerf(float, float c0) { return c0; }
 template <class... C> __device__ __forceinline__ float hornerf(float x, float c0, C... c) {
     return fmaf(hornerf(x, c...), x, c0);   // c0 + x (c1 + x (c2 + ...))
 }
 #define F(v) ((float)(v))
 __device__ __forceinline__ float k0f(float x) {
-    if (x <= 1.0f) {
+    if (x <= 1.0f) {   // (P2 Q1 - P1 log(x) Q2) / (Q1 Q2): one reciprocal for the two quotients
         const float z = x * x, w = 1.0f - z;
-        const float term = hornerf(z, F(1.0), F(2.346487949187396e-1), F(1.187082088663404e-2),
-                                 F(2.150707366040937e-4), F(1.425433617130587e-6)) * logf(x) *
-                           __fdividef(1.0f, hornerf(w, F(9.847324170755358e-1), F(1.518396076767770e-2),
-                                                    F(8.362215678646257e-5)));
-        return hornerf(z, F(1.159315156584126e-1), F(2.770731240515333e-1), F(2.066458134619875e-2),
-                       F(4.574734709978264e-4), F(3.454715527986737e-6)) *
-               __fdividef(1.0f, hornerf(w, F(9.836249671709183e-1), F(1.627693622304549e-2), F(9.809660603621949e-5))) -
-               term;
+        const float p1 = hornerf(z, F(1.0), F(2.346487949187396e-1), F(1.187082088663404e-2),
+                                 F(2.150707366040937e-4), F(1.425433617130587e-6));
+        const float q1 = hornerf(w, F(9.847324170755358e-1), F(1.518396076767770e-2), F(8.362215678646257e-5));
+        const float p2 = hornerf(z, F(1.159315156584126e-1), F(2.770731240515333e-1), F(2.066458134619875e-2),
+                                 F(4.574734709978264e-4), F(3.454715527986737e-6));
+        const float q2 = hornerf(w, F(9.836249671709183e-1), F(1.627693622304549e-2), F(9.809660603621949e-5));
+        return __fdividef(p2 * q1 - p1 * __logf(x) * q2, q1 * q2);
     }
-    const float z = __fdividef(1.0f, x);
-    return ex2a(-1.44269504088896341f * x) *
-           hornerf(z, F(1.253314137315499), F(1.475731032429900e1), F(6.123767403223466e1),
-                   F(1.121012633939949e2), F(9.285288485892228e1), F(3.198289277679660e1),
-                   F(3.595376024148513), F(6.160228690102976e-2)) *
-           __fdividef(1.0f, hornerf(z, F(1.0), F(1.189963006673403e1), F(5.027773590829784e1),
-                                   F(9.496513373427093e1),
-                   F(8.318077493230258e1), F(3.181399777449301e1), F(4.443672926432041),
-                   F(1.408295601966600e-1))) * rsqrtf(x);
+    const float rs = rsqrtf(x), z = rs * rs;   // 1/sqrt(x) and 1/x from one reciprocal square root
+    const float p = hornerf(z, F(1.253314137315499), F(1.475731032429900e1), F(6.123767403223466e1),
+                            F(1.121012633939949e2), F(9.285288485892228e1), F(3.198289277679660e1),
+                            F(3.595376024148513), F(6.160228690102976e-2));
+    const float q = hornerf(z, F(1.0), F(1.189963006673403e1), F(5.027773590829784e1), F(9.496513373427093e1),
+                            F(8.318077493230258e1), F(3.181399777449301e1), F(4.443672926432041),
+                            F(1.408295601966600e-1));
+    return ex2a(-1.44269504088896341f * x) * __fdividef(p * rs, q);
 }
 __device__ __forceinline__ float k1f(float x) {
-    if (x <= 1.0f) {
+    if (x <= 1.0f) {   // (x^2 (P2 Q1 + P1 log(x) Q2) + Q1 Q2) / (x Q1 Q2): one reciprocal
         const float z = x * x, w = 1.0f - z;
-        const float term = hornerf(z, F(0.5), F(5.598072040178741e-2), F(1.818666382168295e-3),
-                                 F(2.397509908859959e-5), F(1.239567816344855e-7)) * logf(x) *
-                           __fdividef(1.0f, hornerf(w, F(9.870202601341150e-1), F(1.292092053534579e-2),
-                                                    F(5.881933053917096e-5)));
-        return x * (hornerf(z, F(-3.079657578292062e-1), F(-8.109417631822442e-2), F(-3.477550948593604e-3),
-                            F(-5.385594871975406e-5), F(-3.110372465429008e-7)) *
-                    __fdividef(1.0f, hornerf(w, F(9.861813171751389e-1), F(1.375094061153160e-2),
-                                             F(6.774221332947002e-5))) +
-                    term) +
-               __fdividef(1.0f, x);
+        const float p1 = hornerf(z, F(0.5), F(5.598072040178741e-2), F(1.818666382168295e-3),
+                                 F(2.397509908859959e-5), F(1.239567816344855e-7));
+        const float q1 = hornerf(w, F(9.870202601341150e-1), F(1.292092053534579e-2), F(5.881933053917096e-5));
+        const float p2 = hornerf(z, F(-3.079657578292062e-1), F(-8.109417631822442e-2), F(-3.477550948593604e-3),
+                                 F(-5.385594871975406e-5), F(-3.110372465429008e-7));
+        const float q2 = hornerf(w, F(9.861813171751389e-1), F(1.375094061153160e-2), F(6.774221332947002e-5));
+        const float qq = q1 * q2;
+        return __fdividef(z * (p2 * q1 + p1 * __logf(x) * q2) + qq, x * qq);
     }
-    const float z = __fdividef(1.0f, x);
-    return ex2a(-1.44269504088896341f * x) *
-           hornerf(z, F(1.253314137315502), F(1.457171340220454e1), F(6.063161173098803e1),
-                   F(1.147386690867892e2), F(1.040442011439181e2), F(4.356596656837691e1),
-                   F(7.265230396353690), F(3.144418558991021e-1)) *
-           __fdividef(1.0f, hornerf(z, F(1.0), F(1.125154514806458e1), F(4.427488496597630e1),
-                                   F(7.616113213117645e1),
-                   F(5.863377227890893e1), F(1.850303673841586e1), F(1.857244676566022),
-                   F(2.538540887654872e-2))) * rsqrtf(x);
+    const float rs = rsqrtf(x), z = rs * rs;
+    const float p = hornerf(z, F(1.253314137315502), F(1.457171340220454e1), F(6.063161173098803e1),
+                            F(1.147386690867892e2), F(1.040442011439181e2), F(4.356596656837691e1),
+                            F(7.265230396353690), F(3.144418558991021e-1));
+    const float q = hornerf(z, F(1.0), F(1.125154514806458e1), F(4.427488496597630e1), F(7.616113213117645e1),
+                            F(5.863377227890893e1), F(1.850303673841586e1), F(1.857244676566022),
+                            F(2.538540887654872e-2));
+    return ex2a(-1.44269504088896341f * x) * __fdividef(p * rs, q);
 }
 #undef F
 
