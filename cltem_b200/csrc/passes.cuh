@@ -109,8 +109,14 @@ __device__ __forceinline__ void load_table(cplx<R> *tw, const cplx<R> *__restric
 // between passes only the columns x < xa or x >= xb (whole column tiles) carry data. The row pass reads
 // those (or every column when load_all is set: the first slice after probe initialisation) and writes
 // only those, since the column pass reads nothing else.
+// FP64 radix-8 step kernels at 256 threads are compiled for 3 blocks per SM (80 registers). Measured against
+// the compiler's 86-122 registers at 2 blocks, in a 256-probe STEM run: row pass 256² −11%, 512² −20%, 2048²
+// −4%; column pass 1024² −5%, 2048² −26%; bit-identical results.
+template <class R, int N, int THREADS, int OTHER> constexpr int fp64_step_minb() {
+    return (sizeof(R) == 8 && THREADS == 256 && Plan<N>::E == 8) ? 3 : OTHER;
+}
 template <class R, int N>
-__global__ void __launch_bounds__(RowCfg<N, R>::THREADS)
+__global__ void __launch_bounds__(RowCfg<N, R>::THREADS, fp64_step_minb<R, N, RowCfg<N, R>::THREADS, 1>())
 k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const cplx<R> *__restrict__ twg, R a,
            int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride) {
     using RC = RowCfg<N, R>;
@@ -263,7 +269,8 @@ enum ColMode { COL_STEP = 0, COL_STEP_DET = 1, COL_DET_ONLY = 2 };
 // the leading and trailing tiles that hold columns inside the propagator's cut (all tiles when
 // tiles_lo = N/COLS); the others would only be multiplied by zero.
 template <class R, int N, int MODE>
-__global__ void __launch_bounds__(ColCfg<N, R>::THREADS, ColCfg<N, R>::STEP_MINB)
+__global__ void __launch_bounds__(ColCfg<N, R>::THREADS,
+                                  fp64_step_minb<R, N, ColCfg<N, R>::THREADS, ColCfg<N, R>::STEP_MINB>())
 k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTables<R> pt, R bscale, R det_scale,
            DetArgs det, cplx<R> *__restrict__ recip_out, int tiles_lo) {
     using CC = ColCfg<N, R>;
