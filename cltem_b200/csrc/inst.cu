@@ -65,6 +65,7 @@ void ensure_attrs() {
     MS_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64 || g_attrs_done[dev]) return;
     set_smem(k_row_step<R, N>, RC::smem());
+    if constexpr (std::is_same<R, double>::value && fp64_row_bounded<N>()) set_smem(k_row_step_d<N>, RC::smem());
     set_smem(k_row_fft<R, N, -1>, RC::smem());
     set_smem(k_row_fft<R, N, +1>, RC::smem());
     set_smem(k_col_step<R, N, COL_STEP>, CC::smem());
@@ -83,6 +84,20 @@ void ensure_attrs() {
 
 inline dim3 row_grid(int batch) { return dim3(N / RC::ROWS, batch); }
 inline dim3 row_block() { return dim3(RC::P::NT, RC::ROWS); }
+
+// the FP64 row step built for 3 blocks per SM where that is set (fp64_step_minb)
+template <class RR>
+bool row_step_d(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans, const cplx<RR> *tw, RR a, int xa,
+                int xb, int load_all, const int *tsel, size_t tstride) {
+    if constexpr (std::is_same<RR, double>::value && fp64_row_bounded<N>()) {
+        k_row_step_d<N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all, tsel,
+                                                                       tstride);
+        MS_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        return false;
+    }
+}
 inline dim3 col_grid(int batch) { return dim3(N / CC::COLS, batch); }
 inline dim3 col_block() { return dim3(CC::COLS, CC::P::NT); }
 
@@ -90,6 +105,7 @@ void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, co
               int load_all, const int *tsel, size_t tstride) {
     ensure_attrs();
     if (rowpair_step<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride)) return;
+    if (row_step_d<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride)) return;
     k_row_step<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all, tsel, tstride);
     MS_CUDA(cudaGetLastError());
 }

@@ -109,16 +109,20 @@ __device__ __forceinline__ void load_table(cplx<R> *tw, const cplx<R> *__restric
 // between passes only the columns x < xa or x >= xb (whole column tiles) carry data. The row pass reads
 // those (or every column when load_all is set: the first slice after probe initialisation) and writes
 // only those, since the column pass reads nothing else.
-// FP64 radix-8 step kernels at 256 threads are compiled for 3 blocks per SM (80 registers). Measured against
-// the compiler's 86-122 registers at 2 blocks, in a 256-probe STEM run: row pass 256² −11%, 512² −20%, 2048²
-// −4%; column pass 1024² −5%, 2048² −26%; bit-identical results.
+// FP64 step kernels: the radix-8 plans at 256 threads are compiled for 3 blocks per SM (80 registers), the
+// 3·2^k plans for a 128-register budget (the compiler otherwise takes 186-234). Measured against the
+// compiler's choice, in a 256-probe STEM run, with bit-identical results: row pass 256² −11%, 384² −4%,
+// 512² −20%, 768² −4%, 1536² −12%, 2048² −4%, 3072² −19%; column pass 384² −7%, 768² −9%, 1024² −5%,
+// 1536² −6%, 2048² −26%, 3072² −14%.
 template <class R, int N, int THREADS, int OTHER> constexpr int fp64_step_minb() {
-    return (sizeof(R) == 8 && THREADS == 256 && Plan<N>::E == 8) ? 3 : OTHER;
+    return (sizeof(R) == 8 && THREADS == 256 && Plan<N>::E == 8) ? 3
+         : (sizeof(R) == 8 && Plan<N>::E == 12 && THREADS * 128 < 65536) ? 65536 / (THREADS * 128) : OTHER;
 }
+// the row step's body, shared by k_row_step and its FP64 3-blocks-per-SM build k_row_step_d
 template <class R, int N>
-__global__ void __launch_bounds__(RowCfg<N, R>::THREADS, fp64_step_minb<R, N, RowCfg<N, R>::THREADS, 1>())
-k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const cplx<R> *__restrict__ twg, R a,
-           int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride) {
+__device__ __forceinline__ void row_step_body(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans,
+                                              const cplx<R> *__restrict__ twg, R a, int xa, int xb, int load_all,
+                                              const int *__restrict__ tsel, size_t tstride) {
     using RC = RowCfg<N, R>;
     using P = typename RC::P;
     constexpr int ROWS = RC::ROWS;
@@ -147,6 +151,24 @@ k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const 
         const int x = t + m * P::NT;
         if (x < xa || x >= xb) row[x] = v[m];
     }
+}
+
+// No minimum-blocks hint: an explicit 1 lets the FP32 wide row pass take 170 registers instead of 128 (37%
+// slower at 512²).
+template <class R, int N>
+__global__ void __launch_bounds__(RowCfg<N, R>::THREADS)
+k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const cplx<R> *__restrict__ twg, R a,
+           int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride) {
+    row_step_body<R, N>(wave, trans, twg, a, xa, xb, load_all, tsel, tstride);
+}
+template <int N> constexpr bool fp64_row_bounded() {
+    return fp64_step_minb<double, N, RowCfg<N, double>::THREADS, 1>() > 1;
+}
+template <int N>
+__global__ void __launch_bounds__(RowCfg<N, double>::THREADS, fp64_step_minb<double, N, RowCfg<N, double>::THREADS, 1>())
+k_row_step_d(double2 *__restrict__ wave, const double2 *__restrict__ trans, const double2 *__restrict__ twg, double a,
+             int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride) {
+    row_step_body<double, N>(wave, trans, twg, a, xa, xb, load_all, tsel, tstride);
 }
 
 // The row step of the FP32 radix-8 / 3·2^k row plans (sizes without the wide plan) with each thread carrying
