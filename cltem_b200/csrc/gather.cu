@@ -7,8 +7,9 @@
 //
 // Threads of a block are tiled 32 x 8 over a band of the atom's pixel box. Pixel-to-atom offsets
 // are formed in FP64 (as in the forward kernel); rho, V'(rho) and the per-thread sums are in the engine's
-// precision T; the block sums are FP64. Built without -fmad=false: nothing here restates a reference
-// statement bit for bit.
+// precision; the block sums are FP64. The FP64 engine differentiates the restated forms (k_atom_grad); the
+// FP32 engine differentiates the table form its forward kernel evaluates (k_atom_grad_f). Built without
+// -fmad=false: nothing here restates a reference statement bit for bit.
 #include "adjoint_ops.h"
 #include "potential.cuh"
 
@@ -205,11 +206,14 @@ void atom_grad(cudaStream_t s, int a0, int count, const double *ax, const double
                double *gxy, double *work) {
     if (count <= 0) return;
     const dim3 grd(count, kGatherBands), blk(32, 8);
-    if (std::is_same<T, float>::value && tabp) {
+    if constexpr (std::is_same<T, float>::value) {   // the FP32 engine differentiates its table kernel
+        if (tabp == nullptr) throw std::runtime_error("the FP32 gradient needs the term table of the parameterisation");
+        (void)prm; (void)i_lim;
         if (form == 0) k_atom_grad_f<0><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
         else if (form == 1) k_atom_grad_f<1><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
         else k_atom_grad_f<2><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
-    } else {
+    } else {   // the FP64 engine: the FP64 derivative of the restated forms
+        (void)tabp;
         k_atom_grad<T><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, form, prm, i_lim, work);
     }
     MS_CUDA(cudaGetLastError());

@@ -45,6 +45,24 @@ bool potential_projected_f(cudaStream_t s, dim3 grd, cplx<T> *out, const double 
     }
 }
 
+// the FP64 kernels (a template, so that the FP32 build discards them)
+template <class T>
+void potential_d(cudaStream_t s, bool full3d, dim3 grd, dim3 blk, cplx<T> *out, const double *ax, const double *ay,
+                 const double *az, const int *aZ, const int *block_start, const T *prm, const PotParams &p) {
+    if constexpr (std::is_same<T, double>::value) {
+        if (full3d) {
+            if (p.form == 0) k_potential_3d<T, 0><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
+            else if (p.form == 1) k_potential_3d<T, 1><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
+            else k_potential_3d<T, 2><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
+        } else {
+            if (p.form == 0) k_potential_projected<T, 0><<<grd, blk, 0, s>>>(out, ax, ay, aZ, block_start, prm, p);
+            else if (p.form == 1) k_potential_projected<T, 1><<<grd, blk, 0, s>>>(out, ax, ay, aZ, block_start, prm, p);
+            else k_potential_projected<T, 2><<<grd, blk, 0, s>>>(out, ax, ay, aZ, block_start, prm, p);
+        }
+        MS_CUDA(cudaGetLastError());
+    }
+}
+
 template <>
 void launch_potential<MS_REAL>(cudaStream_t s, bool full3d, cplx<MS_REAL> *out, int n_slices, const double *ax,
                                const double *ay, const double *az, const int *aZ, const int *block_start,
@@ -53,18 +71,15 @@ void launch_potential<MS_REAL>(cudaStream_t s, bool full3d, cplx<MS_REAL> *out, 
     if (p.width % 16 || p.height % 16) throw std::runtime_error("potential grid must be a multiple of 16");
     dim3 blk(16, 16), grd(p.width / 16, p.height / 16, n_slices);
     if (n_slices <= 0) return;
-    if (full3d && tab3 && potential_3d_f<T>(s, grd, blk, out, ax, ay, az, aZ, block_start, tab3, p)) return;
-    if (!full3d && tabp && potential_projected_f<T>(s, grd, out, ax, ay, aZ, block_start, tabp, p)) return;
-    if (full3d) {
-        if (p.form == 0) k_potential_3d<T, 0><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
-        else if (p.form == 1) k_potential_3d<T, 1><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
-        else k_potential_3d<T, 2><<<grd, blk, 0, s>>>(out, ax, ay, az, aZ, block_start, prm, p);
-    } else {
-        if (p.form == 0) k_potential_projected<T, 0><<<grd, blk, 0, s>>>(out, ax, ay, aZ, block_start, prm, p);
-        else if (p.form == 1) k_potential_projected<T, 1><<<grd, blk, 0, s>>>(out, ax, ay, aZ, block_start, prm, p);
-        else k_potential_projected<T, 2><<<grd, blk, 0, s>>>(out, ax, ay, aZ, block_start, prm, p);
+    if constexpr (std::is_same<T, float>::value) {   // the FP32 engine: the table kernels
+        if (full3d ? tab3 == nullptr : tabp == nullptr)
+            throw std::runtime_error("the FP32 potentials need the term tables of the loaded parameterisation");
+        (void)prm;
+        if (full3d) potential_3d_f<T>(s, grd, blk, out, ax, ay, az, aZ, block_start, tab3, p);
+        else potential_projected_f<T>(s, grd, out, ax, ay, aZ, block_start, tabp, p);
+    } else {   // the FP64 engine: the reference's _d statements
+        potential_d<T>(s, full3d, grd, blk, out, ax, ay, az, aZ, block_start, prm, p);
     }
-    MS_CUDA(cudaGetLastError());
 }
 
 
