@@ -217,10 +217,11 @@ def test_stem_parity(gpu_ctx, oracle, kirkland, dp, interval):
 
 
 @pytest.mark.parametrize("dp", [True, False])
-@pytest.mark.parametrize("res", [64, 96, 128, 384, 512, 768, 1024])
+@pytest.mark.parametrize("res", [64, 96, 128, 384, 512, 768, 1024, 1536, 2048])
 def test_stem_parity_sizes(gpu_ctx, oracle, kirkland, dp, res):
     # the fused step kernels at every plan the engine picks: radix-8 and 3 * 2^k columns, the two-column
-    # FP32 step, the wide FP32 rows at 512 and 1024, the radix-8 rows elsewhere
+    # FP32 step, the wide FP32 rows at 512 and 1024, the two-row FP32 step elsewhere (one row pair a block
+    # from 1536), the FP64 steps with their register budgets
     s, st = small_stem(double_precision=dp, res=res, n=(2, 2, 2), scan=2)
     s.cfg.allow_any_resolution = 1   # 64, 96, 128 and 384 are not in the reference's resolution list
     sim = _sim(gpu_ctx, kirkland, s)
