@@ -157,6 +157,24 @@ def test_transmission_full3d(gpu_ctx, oracle, params_all, dp, form, tilt):
 
 
 @pytest.mark.parametrize("dp", [True, False])
+def test_transmission_full3d_many_rows(gpu_ctx, oracle, params_all, dp):
+    # 0.25 Å slices: each slice reads ±12 z bins, so a tile's list of bin rows (up to 25 x 3) is staged in
+    # more than one pass of 64 rows, with the trapezoid's row resets across the passes
+    s, st = small_cbed(double_precision=dp, n=(2, 2, 2))
+    s.cfg.slice_thickness, s.cfg.slice_offset = 0.25, 0.125
+    p = params_all["lobato"]
+    sim = _sim(gpu_ctx, p, s)
+    osim = _osim(oracle, p, s)
+    assert sim.geo.load_blocks_z == 12 and sim.geo.n_slices == 25
+    sim.set_atoms(st)
+    osim.set_atoms(st)
+    sim.build_transmission()
+    osim.build_transmission()
+    for sl in range(sim.geo.n_slices):
+        assert rel_l2(sim.transmission(sl, False), osim.transmission(sl, False)) < TOL[dp], sl
+
+
+@pytest.mark.parametrize("dp", [True, False])
 @pytest.mark.parametrize("form", ["kirkland", "peng", "lobato"])
 @pytest.mark.parametrize("full3d", [False, True])
 def test_transmission_one_term(gpu_ctx, oracle, params_all, dp, form, full3d):
