@@ -321,6 +321,22 @@ def test_ctem_parity(gpu_ctx, oracle, kirkland, dp):
     assert rel_l2(img, oimg) < TOL[dp]
 
 
+@pytest.mark.parametrize("dp", [True, False])
+@pytest.mark.parametrize("res", [384, 768, 1024])
+def test_ctem_parity_sizes(gpu_ctx, oracle, kirkland, dp, res):
+    # one plane wave through the step kernels of each plan (single-wave launches)
+    s, st = small_ctem(double_precision=dp, res=res, n=(3, 3, 2))
+    s.cfg.allow_any_resolution = 1
+    sim = _sim(gpu_ctx, kirkland, s)
+    osim = _osim(oracle, kirkland, s)
+    sim.set_atoms(st)
+    osim.set_atoms(st)
+    osim.build_transmission()
+    ew, diff, img = sim.ctem()
+    oew, odiff, oimg = osim.ctem()
+    assert rel_l2(ew, oew) < TOL[dp] and rel_l2(diff, odiff) < TOL[dp] and rel_l2(img, oimg) < TOL[dp]
+
+
 def test_ctem_vacuum_is_unchanged(gpu_ctx, kirkland):
     s, st = small_ctem(double_precision=True)
     sim = _sim(gpu_ctx, kirkland, s)
