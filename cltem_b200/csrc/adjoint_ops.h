@@ -17,13 +17,21 @@ template <class R> void mul_conj_prop(cudaStream_t s, int n, cplx<R> *g, const c
                                       const double *kx2, const double *ky2, double kmax2, R scale);
 // gV = sigma Im(conj(E) gE)
 template <class R> void grad_v(cudaStream_t s, size_t count, const cplx<R> *E, const cplx<R> *gE, double sigma, double *gV);
-// per-atom gradients (x, y) of the atoms [a0, a0+count) in sorted order from gV of their slice (gather.cu);
+// The atoms of up to kGradMaxSlices consecutive slices for one atom_grad launch: slice t holds the sorted
+// atoms [start[t], start[t+1]) and reads gV + t * stride (the slices' gV stored one after the other).
+constexpr int kGradMaxSlices = 32;
+struct GradSlices {
+    int start[kGradMaxSlices + 1];
+    int n;
+    size_t stride;
+};
+// per-atom gradients (x, y) of the atoms of the slices in sl (sorted order) from gV of their slice (gather.cu);
 // T is the precision of the per-pixel terms and of prm (the parameterisation table). tabp (FP32 only, may be
 // null): the projected term table the FP32 forward kernel evaluates (potp_table); when set, the FP32
 // gradient differentiates that same evaluation.
-// work: atom_grad_work_doubles(count) doubles of scratch (per-band partial sums)
+// work: atom_grad_work_doubles(atoms of sl) doubles of scratch (per-band partial sums)
 template <class T>
-void atom_grad(cudaStream_t s, int a0, int count, const double *ax, const double *ay, const int *aZ, const double *gV,
+void atom_grad(cudaStream_t s, const GradSlices &sl, const double *ax, const double *ay, const int *aZ, const double *gV,
                int n, double startx, double starty, double dx, int form, const T *prm, int i_lim, const float2 *tabp,
                double *gxy, double *work);
 int atom_grad_work_doubles(int max_count);

@@ -1560,35 +1560,48 @@ struct Sim : SimBase {
         MS_CUDA(cudaStreamSynchronize(st()));
         const int n_in = hbs.back();
         gxy.ensure(ctx, 2 * (size_t)std::max(n_in, 1));
-        {   // scratch of the atom gather: the largest slice's atoms
+        {   // scratch of the atom gather: the atoms of the largest checkpoint segment
             int mx = 1;
-            for (int s = 0; s < S; s++) mx = std::max(mx, hbs[(size_t)(s + 1) * nb] - hbs[(size_t)s * nb]);
+            for (int s0 = 0; s0 < S; s0 += c) {
+                const int s1 = std::min(s0 + c, S);
+                mx = std::max(mx, hbs[(size_t)s1 * nb] - hbs[(size_t)s0 * nb]);
+            }
             gwork.ensure(ctx, (size_t)atom_grad_work_doubles(mx));
         }
         MS_CUDA(cudaMemsetAsync(gxy.p, 0, 2 * (size_t)std::max(n_in, 1) * sizeof(double), st()));
-        fw.ensure(ctx, NN); gT.ensure(ctx, NN); gV.ensure(ctx, NN);
+        // gT and gV of every slice of a segment, so that the band limit, gV and the atom gather run once per
+        // segment over all its slices (batch-1 launches of those kernels leave most of the GPU idle)
+        fw.ensure(ctx, NN); gT.ensure(ctx, (size_t)c * NN); gV.ensure(ctx, (size_t)c * NN);
         PropTables<R> ptc{pxc.p, pyc.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p};
         for (int k = n_ck - 1; k >= 0; k--) {
-            const int s0 = k * c, s1 = std::min(s0 + c, S);
+            const int s0 = k * c, s1 = std::min(s0 + c, S), m = s1 - s0;
             if (c > 1) {   // recompute psi_s of the segment from its checkpoint
                 MS_CUDA(cudaMemcpyAsync(fw.p, ck_buf.p + (size_t)k * NN, NN * sizeof(C), cudaMemcpyDeviceToDevice, st()));
                 for (int s = s0; s < s1; s++) {
                     ops.row_step_save(st(), fw.p, 1, trans.p + (size_t)s * NN, tw, a, save.p + (size_t)(s - s0) * NN);
                     if (s < s1 - 1) ops.col_step(st(), fw.p, 1, tw, pt, b, ds, nodet, nullptr, COL_STEP, all_tiles, 0);
-                    ctx->launches += 2;
+                    ctx->launches += s < s1 - 1 ? 2 : 1;
                 }
             }
             for (int s = s1 - 1; s >= s0; s--) {
                 check_cancel();
                 if (s < S - 1) ops.col_step(st(), wave.p, 1, tw, ptc, b, ds, nodet, nullptr, COL_STEP, all_tiles, 0);
                 const C *psi = save.p + (size_t)(c == 1 ? s : s - s0) * NN;
-                ops.row_adjoint(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, psi, gT.p);
-                band_limit(gT.p, 1);   // G_E = bandlimit(G_T): the band limit is self-adjoint
-                grad_v<R>(st(), NN, E.p + (size_t)s * NN, gT.p, g.sigma, gV.p);
-                const int a0 = hbs[(size_t)s * nb], a1 = hbs[(size_t)(s + 1) * nb];
-                atom_grad<R>(st(), a0, a1 - a0, axs.p, ays.p, aZs.p, gV.p, N, g.sim_x[0], g.sim_y[0], g.real_scale,
-                             ctx->params.form, params_dev(), ctx->params.i_count, ctx->potp_tab, gxy.p, gwork.p);
-                ctx->launches += 5;
+                ops.row_adjoint(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, psi, gT.p + (size_t)(s - s0) * NN);
+                ctx->launches += s < S - 1 ? 2 : 1;
+            }
+            band_limit(gT.p, m);   // G_E = bandlimit(G_T): the band limit is self-adjoint
+            grad_v<R>(st(), (size_t)m * NN, E.p + (size_t)s0 * NN, gT.p, g.sigma, gV.p);
+            ctx->launches++;
+            for (int t0 = 0; t0 < m; t0 += kGradMaxSlices) {
+                GradSlices gs{};
+                gs.n = std::min(kGradMaxSlices, m - t0);
+                gs.stride = NN;
+                for (int i = 0; i <= gs.n; i++) gs.start[i] = hbs[(size_t)(s0 + t0 + i) * nb];
+                atom_grad<R>(st(), gs, axs.p, ays.p, aZs.p, gV.p + (size_t)t0 * NN, N, g.sim_x[0], g.sim_y[0],
+                             g.real_scale, ctx->params.form, params_dev(), ctx->params.i_count, ctx->potp_tab, gxy.p,
+                             gwork.p);
+                ctx->launches += 2;
             }
         }
         MS_CUDA(cudaMemcpyAsync(hp.data(), part.p, 3 * (size_t)nred * sizeof(double), cudaMemcpyDeviceToHost, st()));

@@ -1,6 +1,7 @@
 // gather.cu — atom-position gradients of the differentiable CTEM loss.
 //
-// dL/dx_a, dL/dy_a of the atoms [a0, a0+count) of one slice (sorted order): the sum over the pixels within
+// dL/dx_a, dL/dy_a of the atoms of one or more consecutive slices (sorted order; one launch per checkpoint
+// segment of the adjoint, so the grid holds several slices' atoms): the sum over the pixels within
 // 8 Å of atom a of gV(r) V'(rho) d rho / d(x_a, y_a), rho = |r - r_a|, with V' the derivative of the
 // projected form the forward potential kernel sums (potential.cuh; transmission_potentials_projected_d.cl)
 // and zero where the forward clamps rho to r_min = dx/4.
@@ -54,13 +55,21 @@ __device__ __forceinline__ T dpot_drho(int form, const T *__restrict__ prm, int 
 // adds the bands of every atom in a fixed order (deterministic results).
 constexpr int kGatherBands = 8;
 
+// the slice t of sl holding sorted atom a: start[t] <= a < start[t+1] (empty slices are passed over)
+__device__ __forceinline__ int slice_of(const GradSlices &sl, int a) {
+    int t = 0;
+    while (t + 1 < sl.n && a >= sl.start[t + 1]) t++;
+    return t;
+}
+
 template <class T>
 __global__ void __launch_bounds__(256)
-k_atom_grad(int a0, const double *__restrict__ ax, const double *__restrict__ ay, const int *__restrict__ aZ,
-            const double *__restrict__ gV, int n, double startx, double starty, double dx, int form,
+k_atom_grad(const GradSlices sl, const double *__restrict__ ax, const double *__restrict__ ay,
+            const int *__restrict__ aZ, const double *__restrict__ gV, int n, double startx, double starty, double dx, int form,
             const T *__restrict__ prm, int i_lim, double *__restrict__ work) {
     __shared__ double red[2][8];
-    const int a = a0 + blockIdx.x;
+    const int a = sl.start[0] + blockIdx.x;
+    const double *gVs = gV + (size_t)slice_of(sl, a) * sl.stride;
     const double xa = ax[a], ya = ay[a];
     const int Z = aZ[a];
     const T r_min2 = (T)(0.0625 * dx * dx);   // (dx / 4)^2
@@ -75,7 +84,7 @@ k_atom_grad(int a0, const double *__restrict__ ax, const double *__restrict__ ay
     T gx = 0, gy = 0;
     for (int py = r0 + (int)threadIdx.y; py <= r1; py += 8) {
         const T ry = (T)(oy + py * dx);
-        const double *grow = gV + (size_t)py * n;
+        const double *grow = gVs + (size_t)py * n;
         for (int px = ix0 + (int)threadIdx.x; px <= ix1; px += 32) {
             const T rx = (T)(ox + px * dx);
             const T rho2 = rx * rx + ry * ry;
@@ -137,12 +146,13 @@ __device__ __forceinline__ float dpotp_drho(const float2 (&c)[FORM == 0 ? 6 : 5]
 
 template <int FORM>
 __global__ void __launch_bounds__(256)
-k_atom_grad_f(int a0, const double *__restrict__ ax, const double *__restrict__ ay, const int *__restrict__ aZ,
-              const double *__restrict__ gV, int n, double startx, double starty, double dx,
+k_atom_grad_f(const GradSlices sl, const double *__restrict__ ax, const double *__restrict__ ay,
+              const int *__restrict__ aZ, const double *__restrict__ gV, int n, double startx, double starty, double dx,
               const float2 *__restrict__ tab, double *__restrict__ work) {
     constexpr int NTERM = FORM == 0 ? 6 : 5;
     __shared__ double red[2][8];
-    const int a = a0 + blockIdx.x;
+    const int a = sl.start[0] + blockIdx.x;
+    const double *gVs = gV + (size_t)slice_of(sl, a) * sl.stride;
     const double xa = ax[a], ya = ay[a];
     float2 c[NTERM];
     const float2 *t = tab + (aZ[a] - 1) * kPotPTerms;
@@ -159,7 +169,7 @@ k_atom_grad_f(int a0, const double *__restrict__ ax, const double *__restrict__ 
     float gx = 0, gy = 0;
     for (int py = r0 + (int)threadIdx.y; py <= r1; py += 8) {
         const float ry = (float)(oy + py * dx);
-        const double *grow = gV + (size_t)py * n;
+        const double *grow = gVs + (size_t)py * n;
         for (int px = ix0 + (int)threadIdx.x; px <= ix1; px += 32) {
             const float rx = (float)(ox + px * dx);
             const float rho2 = rx * rx + ry * ry;
@@ -201,20 +211,22 @@ __global__ void k_atom_grad_sum(int a0, int count, const double *__restrict__ wo
 }
 
 template <class T>
-void atom_grad(cudaStream_t s, int a0, int count, const double *ax, const double *ay, const int *aZ, const double *gV,
+void atom_grad(cudaStream_t s, const GradSlices &sl, const double *ax, const double *ay, const int *aZ, const double *gV,
                int n, double startx, double starty, double dx, int form, const T *prm, int i_lim, const float2 *tabp,
                double *gxy, double *work) {
+    if (sl.n < 1 || sl.n > kGradMaxSlices) throw std::runtime_error("atom_grad: 1 to kGradMaxSlices slices a launch");
+    const int a0 = sl.start[0], count = sl.start[sl.n] - a0;
     if (count <= 0) return;
     const dim3 grd(count, kGatherBands), blk(32, 8);
     if constexpr (std::is_same<T, float>::value) {   // the FP32 engine differentiates its table kernel
         if (tabp == nullptr) throw std::runtime_error("the FP32 gradient needs the term table of the parameterisation");
         (void)prm; (void)i_lim;
-        if (form == 0) k_atom_grad_f<0><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
-        else if (form == 1) k_atom_grad_f<1><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
-        else k_atom_grad_f<2><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
+        if (form == 0) k_atom_grad_f<0><<<grd, blk, 0, s>>>(sl, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
+        else if (form == 1) k_atom_grad_f<1><<<grd, blk, 0, s>>>(sl, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
+        else k_atom_grad_f<2><<<grd, blk, 0, s>>>(sl, ax, ay, aZ, gV, n, startx, starty, dx, tabp, work);
     } else {   // the FP64 engine: the FP64 derivative of the restated forms
         (void)tabp;
-        k_atom_grad<T><<<grd, blk, 0, s>>>(a0, ax, ay, aZ, gV, n, startx, starty, dx, form, prm, i_lim, work);
+        k_atom_grad<T><<<grd, blk, 0, s>>>(sl, ax, ay, aZ, gV, n, startx, starty, dx, form, prm, i_lim, work);
     }
     MS_CUDA(cudaGetLastError());
     k_atom_grad_sum<<<(count + 127) / 128, 128, 0, s>>>(a0, count, work, gxy);
@@ -222,9 +234,11 @@ void atom_grad(cudaStream_t s, int a0, int count, const double *ax, const double
 }
 int atom_grad_work_doubles(int max_count) { return 2 * kGatherBands * max_count; }
 
-template void atom_grad<float>(cudaStream_t, int, int, const double *, const double *, const int *, const double *, int,
-                               double, double, double, int, const float *, int, const float2 *, double *, double *);
-template void atom_grad<double>(cudaStream_t, int, int, const double *, const double *, const int *, const double *, int,
-                                double, double, double, int, const double *, int, const float2 *, double *, double *);
+template void atom_grad<float>(cudaStream_t, const GradSlices &, const double *, const double *, const int *,
+                               const double *, int, double, double, double, int, const float *, int, const float2 *,
+                               double *, double *);
+template void atom_grad<double>(cudaStream_t, const GradSlices &, const double *, const double *, const int *,
+                                const double *, int, double, double, double, int, const double *, int, const float2 *,
+                                double *, double *);
 
 }  // namespace ms

@@ -110,3 +110,23 @@ def test_torch_autograd_function(kirkland):
     assert abs(loss.item() - L) <= 1e-12 * L
     assert np.allclose(xyz.grad.numpy(), g, rtol=0, atol=1e-12 * np.abs(g).max())
     assert np.allclose(lens.grad.numpy(), [g10, g30], rtol=1e-12)
+
+
+@pytest.mark.parametrize("dp", [True, False])
+def test_gradient_independent_of_checkpoint_segments(kirkland, dp):
+    """The adjoint band-limits gT, forms gV and gathers the atom gradients once per checkpoint segment (up to
+    32 slices a launch): thin slices (0.2 Å, ~40 slices, most of them empty) give the same loss and gradients
+    for one slice a segment, 5 slices a segment and every slice in one segment (two atom launches)."""
+    ctx, s, st, target = _setup(dp, kirkland)
+    s.cfg.slice_thickness = 0.2
+    s.cfg.slice_offset = 0.1
+    sim = Simulation(ctx, s.cfg)
+    sim.set_atoms(st)
+    runs = [sim.ctem_loss_grad(target, len(st), checkpoint_every=ck) for ck in (1, 5, 10000)]
+    L1, g1, c10, c30 = runs[0]
+    assert np.abs(g1).max() > 0
+    tol = 1e-12 if dp else 1e-6
+    for L, g, d10, d30 in runs[1:]:
+        assert abs(L - L1) <= tol * L1
+        assert np.abs(g - g1).max() <= tol * np.abs(g1).max()
+        assert abs(d10 - c10) <= tol * abs(c10) and abs(d30 - c30) <= tol * abs(c30)
