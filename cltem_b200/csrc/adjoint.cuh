@@ -21,10 +21,11 @@ k_row_step_save(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, c
     using P = typename RC::P;
     constexpr int ROWS = RC::ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + RC::TWN + threadIdx.y * RC::ROWSZ;
+    cplx<R> *tws = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tws + RC::TWS + threadIdx.y * RC::ROWSZ;
     const int t = threadIdx.x;
-    load_table<R>(tw, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
+    const cplx<R> *tw =
+        twiddles_for<RC::TWG, R>(tws, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
     const int y = blockIdx.x * ROWS + threadIdx.y;
     const size_t off = (size_t)blockIdx.y * N * N + (size_t)y * N;
     cplx<R> *row = wave + off;
@@ -55,10 +56,11 @@ k_row_adjoint(cplx<R> *__restrict__ state, const cplx<R> *__restrict__ trans, co
     using P = typename RC::P;
     constexpr int ROWS = RC::ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + RC::TWN + threadIdx.y * RC::ROWSZ;
+    cplx<R> *tws = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tws + RC::TWS + threadIdx.y * RC::ROWSZ;
     const int t = threadIdx.x;
-    load_table<R>(tw, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
+    const cplx<R> *tw =
+        twiddles_for<RC::TWG, R>(tws, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
     const int y = blockIdx.x * ROWS + threadIdx.y;
     const size_t off = (size_t)blockIdx.y * N * N + (size_t)y * N;
     cplx<R> *row = state + off;

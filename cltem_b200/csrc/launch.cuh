@@ -35,6 +35,6 @@ template <class R, int N> PassOps<R> make_pass_ops();
 // switch over the supported sizes; throws for an unsupported one
 template <class R> PassOps<R> pass_ops(int n);
 
-#define MS_SIZES(X) X(64) X(96) X(128) X(256) X(384) X(512) X(768) X(1024) X(1536) X(2048) X(3072) X(4096)
+#define MS_SIZES(X) X(64) X(96) X(128) X(256) X(384) X(512) X(768) X(1024) X(1536) X(2048) X(3072) X(4096) X(8192)
 
 }  // namespace ms

@@ -21,6 +21,7 @@
 namespace ms {
 
 constexpr int kMaxDetectors = 16;
+constexpr size_t kMaxBlockSmem = 227 * 1024;   // dynamic shared memory one block may opt in to (sm_100)
 
 template <class R>
 struct PropTables {
@@ -55,7 +56,11 @@ template <int N, class R> struct RowCfg {
     static constexpr int TWN = WIDE ? WidePlan<N>::TW : N;   // twiddle entries staged in shared memory
     static constexpr int TW_OFF = WIDE ? N : 0;               // offset of the row plan's table (Ctx::twiddles)
     static constexpr int ROWSZ = WIDE ? WidePlan<N>::ROWSZ : RowAddr::size(N);
-    static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(TWN + ROWS * ROWSZ); }
+    // the table is read from global memory (L1 / L2) when it and the rows do not both fit (FP64 8192)
+    static constexpr bool TWG = sizeof(cplx<R>) * (size_t)(TWN + ROWS * ROWSZ) > kMaxBlockSmem;
+    static constexpr int TWS = TWG ? 0 : TWN;   // twiddle entries staged in shared memory
+    static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(TWS + ROWS * ROWSZ); }
+    static_assert(smem() <= kMaxBlockSmem, "row tile exceeds shared memory");
 };
 // Column tiles: COLS columns per block (a power of two dividing N), P::NT threads per column. Radix-8 plan:
 // 512-thread blocks at the common sizes, a tile row of COLS complex values 64 B (FP32, N <= 512). Wide plan:
@@ -67,14 +72,17 @@ template <int N, class R> struct ColCfg {
     static constexpr bool WIDE = kWideColumns && wide_plan<R>(N);
     using P = std::conditional_t<WIDE, WidePlan<N>, Plan<N>>;
     static constexpr int COLS = WIDE ? (N <= 512 ? 8 : 4)
-                                     : (sizeof(R) == 4 ? (N <= 512 ? 8 : (N <= 1024 ? 4 : 2))
+                                     : (sizeof(R) == 4 ? (N <= 512 ? 8 : (N <= 1024 ? 4 : (N <= 4096 ? 2 : 1)))
                                                        : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1)));
     static_assert(N % COLS == 0, "column tile must divide the grid");
     static constexpr int THREADS = P::NT * COLS;
     static_assert(THREADS <= 1024, "column block too large");
     static constexpr int TWN = WIDE ? WidePlan<N>::TW : N;
     static constexpr int COLSZ = WIDE ? WidePlan<N>::ROWSZ : N;   // shared elements of one column
-    static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(TWN + COLSZ * COLS); }
+    static constexpr bool TWG = sizeof(cplx<R>) * (size_t)(TWN + COLSZ * COLS) > kMaxBlockSmem;   // as RowCfg
+    static constexpr int TWS = TWG ? 0 : TWN;
+    static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(TWS + COLSZ * COLS); }
+    static_assert(smem() <= kMaxBlockSmem, "column tile exceeds shared memory");
     // Blocks per SM the step pass is compiled for: 3 x 512 threads for the FP32 radix-8 plans (a 42-register
     // budget; the 2 blocks of a 52-register build leave its global loads exposed), 4 x 128 threads for the
     // wide plan (128 registers), else what fits.
@@ -99,6 +107,19 @@ __device__ __forceinline__ void col_transform(cplx<R> (&v)[ColCfg<N, R>::P::E], 
 template <class R>
 __device__ __forceinline__ void load_table(cplx<R> *tw, const cplx<R> *__restrict__ twg, int count, int tid, int nthreads) {
     for (int i = tid; i < count; i += nthreads) tw[i] = twg[i];
+}
+// the twiddle table a pass reads: count entries staged in shared memory at tws, or, when the Cfg's TWG is
+// set, the global table itself (read through L1 / L2)
+template <bool TWG, class R>
+__device__ __forceinline__ const cplx<R> *twiddles_for(cplx<R> *tws, const cplx<R> *__restrict__ twg, int count,
+                                                       int tid, int nthreads) {
+    if constexpr (TWG) {
+        (void)tws; (void)count; (void)tid; (void)nthreads;
+        return twg;
+    } else {
+        load_table<R>(tws, twg, count, tid, nthreads);
+        return tws;
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -127,10 +148,11 @@ __device__ __forceinline__ void row_step_body(cplx<R> *__restrict__ wave, const 
     using P = typename RC::P;
     constexpr int ROWS = RC::ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + RC::TWN + threadIdx.y * RC::ROWSZ;
+    cplx<R> *tws = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tws + RC::TWS + threadIdx.y * RC::ROWSZ;
     const int t = threadIdx.x;
-    load_table<R>(tw, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
+    const cplx<R> *tw =
+        twiddles_for<RC::TWG, R>(tws, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
     const int y = blockIdx.x * ROWS + threadIdx.y;
     cplx<R> *row = wave + (size_t)blockIdx.y * N * N + (size_t)y * N;
     // tsel (optional): transmission set of each wave; set k of this slice starts k * tstride after trans
@@ -238,10 +260,11 @@ k_row_fft(const cplx<R> *in, cplx<R> *out, const cplx<R> *__restrict__ twg, R sc
     using P = typename RC::P;
     constexpr int ROWS = RC::ROWS;
     extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + RC::TWN + threadIdx.y * RC::ROWSZ;
+    cplx<R> *tws = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tws + RC::TWS + threadIdx.y * RC::ROWSZ;
     const int t = threadIdx.x;
-    load_table<R>(tw, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
+    const cplx<R> *tw =
+        twiddles_for<RC::TWG, R>(tws, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
     const int y = blockIdx.x * ROWS + threadIdx.y;
     const size_t off = (size_t)blockIdx.y * N * N + (size_t)y * N;
     cplx<R> v[P::E];
@@ -300,10 +323,10 @@ k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTabl
     constexpr int COLS = CC::COLS;
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double red[32];
-    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + CC::TWN + threadIdx.x;
+    cplx<R> *tws = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tws + CC::TWS + threadIdx.x;
     const int c = threadIdx.x, t = threadIdx.y;
-    load_table<R>(tw, twg, CC::TWN, c + t * COLS, COLS * P::NT);
+    const cplx<R> *tw = twiddles_for<CC::TWG, R>(tws, twg, CC::TWN, c + t * COLS, COLS * P::NT);
     const int tile = (int)blockIdx.x < tiles_lo ? (int)blockIdx.x : N / COLS - ((int)gridDim.x - (int)blockIdx.x);
     const int x = tile * COLS + c;
     cplx<R> *base = wave + (size_t)blockIdx.y * N * N;
@@ -420,10 +443,10 @@ k_col_fft(const cplx<R> *in, cplx<R> *out, const cplx<R> *__restrict__ twg, R sc
     using P = typename CC::P;
     constexpr int COLS = CC::COLS;
     extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + CC::TWN + threadIdx.x;
+    cplx<R> *tws = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tws + CC::TWS + threadIdx.x;
     const int c = threadIdx.x, t = threadIdx.y;
-    load_table<R>(tw, twg, CC::TWN, c + t * COLS, COLS * P::NT);
+    const cplx<R> *tw = twiddles_for<CC::TWG, R>(tws, twg, CC::TWN, c + t * COLS, COLS * P::NT);
     const int x = blockIdx.x * COLS + c;
     const size_t off = (size_t)blockIdx.y * N * N;
     cplx<R> v[P::E];
@@ -445,10 +468,10 @@ k_col_bandlimit(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, con
     using P = typename CC::P;
     constexpr int COLS = CC::COLS;
     extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + CC::TWN + threadIdx.x;
+    cplx<R> *tws = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tws + CC::TWS + threadIdx.x;
     const int c = threadIdx.x, t = threadIdx.y;
-    load_table<R>(tw, twg, CC::TWN, c + t * COLS, COLS * P::NT);
+    const cplx<R> *tw = twiddles_for<CC::TWG, R>(tws, twg, CC::TWN, c + t * COLS, COLS * P::NT);
     const int x = blockIdx.x * COLS + c;
     cplx<R> *base = wave + (size_t)blockIdx.y * N * N;
     cplx<R> v[P::E];
@@ -478,10 +501,10 @@ k_col_probe(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, const d
     using P = typename CC::P;
     constexpr int COLS = CC::COLS;
     extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *sm = tw + CC::TWN + threadIdx.x;
+    cplx<R> *tws = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *sm = tws + CC::TWS + threadIdx.x;
     const int c = threadIdx.x, t = threadIdx.y;
-    load_table<R>(tw, twg, CC::TWN, c + t * COLS, COLS * P::NT);
+    const cplx<R> *tw = twiddles_for<CC::TWG, R>(tws, twg, CC::TWN, c + t * COLS, COLS * P::NT);
     const int x = blockIdx.x * COLS + c;
     const double2 pp = pos[blockIdx.y];
     // dfac (optional): pi * defocus change / wavelength of each wave; the aberration phase gains

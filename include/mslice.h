@@ -78,8 +78,8 @@ typedef struct mslice_detector {
 typedef struct mslice_config {
     int mode;                    /* MSLICE_MODE_* */
     int double_precision;        /* 0: FP32 complex64 engine, 1: FP64 complex128 engine */
-    int resolution;              /* grid side; clTEM allows {256,512,768,1024,1536,2048,3072,4096,8192};
-                                    8192 is rejected with MSLICE_ERR_UNSUPPORTED (not built) */
+    int resolution;              /* grid side; clTEM allows {256,512,768,1024,1536,2048,3072,4096,8192},
+                                    all built; with allow_any_resolution also 64, 96, 128 and 384 */
     int allow_any_resolution;    /* extension: accept other sizes of the form 2^a or 3*2^a (e.g. 384) */
     double slice_thickness;      /* Å */
     double slice_offset;         /* Å */
