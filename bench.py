@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--scan", type=int, default=64)
     p.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline and plain-FP64 legs")
     p.add_argument("--cpu-probes", type=int, default=32, help="probes in the bounded CPU sample")
-    p.add_argument("--only", default=None, choices=["adjoint", "cbed3d", "uneven"],
+    p.add_argument("--only", default=None, choices=["adjoint", "cbed3d", "uneven", "cufft"],
                    help="run one extra leg alone and print its JSON (for profiling it)")
     p.add_argument("--cbed-nz", type=int, default=60, help="FCC cells along z of the cbed3d leg (60: 120 slices)")
     return p.parse_args()
@@ -159,6 +159,41 @@ def cpu_sample(n_probes, double_precision, seed=0):
     S = osim.geo.n_slices
     full = npx * S / ((t1 - t0) + (t2 - t1) * npx / n_probes)
     return full, {"build_s": t1 - t0, "propagate_s": t2 - t1, "probes": n_probes, "slices": S, "configs": 1}
+
+
+def cufft_leg(batch=512, steps=20, warmup=3, n=512):
+    """The same multislice step built from cuFFT (through torch.fft) and elementwise kernels, timed for
+    comparison with the fused passes: per probe·slice, psi <- IFFT2(P * FFT2(T * psi)) on a batch of n² complex64
+    waves (1 GiB at 512 waves of 512², larger than L2); neither transform scales, as the fused passes fold the
+    scale into P. Device time with CUDA events after warm-up."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(7)
+    w = torch.randn(batch, n, n, dtype=torch.complex64, device="cuda", generator=g)
+    T = torch.exp(1j * torch.rand(n, n, device="cuda", generator=g)).to(torch.complex64)
+    P = (torch.exp(1j * torch.rand(n, n, device="cuda", generator=g)) / (n * n)).to(torch.complex64)
+    buf = torch.empty_like(w)
+
+    def step():
+        w.mul_(T)
+        torch.fft.fft2(w, out=buf)
+        buf.mul_(P)
+        torch.fft.ifft2(buf, norm="forward", out=w)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        step()
+    b.record()
+    b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    del w, buf
+    torch.cuda.empty_cache()
+    return {"value": batch / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms,
+            "sample": f"{steps} steps of {batch} waves of {n}² complex64 after {warmup} untimed",
+            "kernels": "torch.fft.fft2 / ifft2 (cuFFT C2C) + 2 elementwise multiplies per step"}
 
 
 def cpu_baseline_leg(n_probes):
@@ -373,7 +408,7 @@ def main():
         ctx.load_params(load_default("kirkland"))
         ext = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
         leg = {"adjoint": lambda: adjoint_leg(ctx, ext, args.warmup), "cbed3d": lambda: cbed3d_leg(ctx, ext, args.cbed_nz),
-               "uneven": lambda: uneven_leg(ctx)}[args.only]()
+               "uneven": lambda: uneven_leg(ctx), "cufft": lambda: cufft_leg()}[args.only]()
         print(json.dumps({"leg": args.only, **leg}))
         return 0
     if world > 1:
@@ -512,7 +547,7 @@ def main():
         cbed3d = cbed3d_leg(ctx, ext)
         uneven = uneven_leg(ctx)
 
-    cpu = plain = None
+    cpu = plain = cufft = None
     if rank == 0 and world == 1 and not args.no_baseline:
         # plain per-probe FP64 GPU path (the reference's unfused order with cuFFT Z2Z) on a sample
         sd, std_ = workload(double_precision=True)
@@ -546,6 +581,8 @@ def main():
                  "fused_fp64": {"value": fv, "unit": UNIT, "sample": f"3 runs of {len(fpix)} probes x {S} slices after 2 untimed",
                                 "fused_fp64_over_plain_fp64": fv / pv}}
         simd.close()
+        cufft = cufft_leg()
+        cufft["fused_fp32_over_cufft"] = value / cufft["value"]
         cpu = cpu_baseline_leg(args.cpu_probes)
 
     if rank == 0:
@@ -561,6 +598,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "plain_fp64_gpu": plain,
+            "cufft_fp32_step": cufft,
             "adjoint_forward_ratio": adjoint["ratio"] if adjoint else None,
             "adjoint": adjoint,
             "cbed_full3d": cbed3d,

@@ -25,14 +25,27 @@ template <class K> void set_smem(K kernel, size_t bytes) {
     MS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
 }
 
-// the two-column step kernel of the FP32 radix-8 plans (templates, so that the FP64 build discards them)
+// the two-column step kernel of the FP32 plans (templates, so that the FP64 build discards them)
 template <class RR> void pair_attrs() {
-    if constexpr (std::is_same<RR, float>::value && pair_columns<N>()) set_smem(k_col_step_pair<N>, PairCfg<N>::smem());
+    if constexpr (std::is_same<RR, float>::value && pair_columns<N>()) {
+        using PC = PairStepCfg<N>;
+        set_smem(k_col_step_pair<N, PC::COLS, pair_loose<N>()>, PC::smem());
+    }
 }
 template <class RR>
-bool pair_step(cudaStream_t s, dim3 g, cplx<RR> *wave, const cplx<RR> *tw, PropTables<RR> pt, RR b, int tiles_lo) {
+bool pair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw, PropTables<RR> pt, RR b, int tiles_lo,
+               int tiles_hi) {
     if constexpr (std::is_same<RR, float>::value && pair_columns<N>()) {
-        k_col_step_pair<N><<<g, dim3(PairCfg<N>::PAIRS, Plan<N>::NT), PairCfg<N>::smem(), s>>>(wave, tw, pt, b, tiles_lo);
+        using PC = PairStepCfg<N>;
+        // the engine's tiles are CC::COLS wide and the step's tile covers k of them; the extra columns of a
+        // partly active tile lie outside the propagator's cut and come out zero, and the row pass never
+        // reads them
+        constexpr int k = PC::COLS / CC::COLS, total = N / PC::COLS;
+        static_assert(PC::COLS % CC::COLS == 0, "the step's tile must cover whole engine tiles");
+        int lo = (tiles_lo + k - 1) / k, hi = (tiles_hi + k - 1) / k;
+        if (lo + hi > total) { lo = total; hi = 0; }
+        k_col_step_pair<N, PC::COLS, pair_loose<N>()><<<dim3(lo + hi, batch), dim3(PC::PAIRS, Plan<N>::NT), PC::smem(),
+                                                       s>>>(wave, tw, pt, b, lo);
         MS_CUDA(cudaGetLastError());
         return true;
     } else {
@@ -121,7 +134,8 @@ void col_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, PropT
     if (tiles_lo < 0 || tiles_hi < 0 || tiles_lo + tiles_hi > N / CC::COLS || tiles_lo + tiles_hi == 0)
         throw std::runtime_error("column tile range out of bounds");
     dim3 g(tiles_lo + tiles_hi, batch);
-    if (mode == COL_STEP && recip == nullptr && pt.ycut && pair_step<R>(s, g, wave, tw, pt, b, tiles_lo)) return;
+    if (mode == COL_STEP && recip == nullptr && pt.ycut && pair_step<R>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi))
+        return;
     if (mode == COL_STEP && recip == nullptr)
         k_col_step<R, N, COL_STEP><<<g, col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip, tiles_lo);
     else if (mode == COL_DET_ONLY)

@@ -378,27 +378,40 @@ k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTabl
 // The plain step (COL_STEP) of the FP32 column plans (2^k and 3·2^k) with each thread carrying two adjacent
 // columns of the tile: 16-byte loads, stores and shared-memory exchanges (fft_pair.cuh), and the
 // propagator's cut read as a row band per column (PropTables::ycut) instead of an FP64 test per element.
-// Same arithmetic per element as k_col_step<float, N, COL_STEP>. Up to 256 threads a block: 4 blocks per
-// SM (64 registers at 256 threads, 128 at 128); 512 threads (4096²): 2 blocks. Measured against the
-// one-column kernel in a 256-probe STEM run: 256² −12%, 384² −11%, 512² −5%, 768² −32%, 1024² −5%, 1536² −25%,
-// 2048² ±0, 3072² −13%, 4096² −18%, with bit-identical results.
-template <int N> struct PairCfg {
+// Same arithmetic per element as k_col_step<float, N, COL_STEP>. At the engine's column tile it measured,
+// against the one-column kernel in a 256-probe STEM run: 256² −12%, 384² −11%, 512² −5%, 768² −32%,
+// 1024² −5%, 1536² −25%, 2048² ±0, 3072² −13%, 4096² −18%, with bit-identical results. Its tile is now wider
+// than the engine's (PairStepCfg below).
+template <int N, int COLS_, bool LOOSE = false> struct PairCfg {
     using P = Plan<N>;
-    static constexpr int COLS = ColCfg<N, float>::COLS;
+    static constexpr int COLS = COLS_;
     static constexpr int PAIRS = COLS / 2;
     static constexpr int THREADS = PAIRS * P::NT;
-    static constexpr int MINB = THREADS <= 256 ? 4 : 2;
+    // 64 registers a thread, or (LOOSE) 128
+    static constexpr int MINB = LOOSE ? (THREADS * 128 >= 65536 ? 1 : 65536 / (THREADS * 128))
+                                      : (THREADS <= 256 ? 4 : (THREADS <= 512 ? 2 : 1));
     static constexpr size_t smem() { return sizeof(float2) * (size_t)N + sizeof(float4) * (size_t)N * PAIRS; }
+    static constexpr bool ok = !ColCfg<N, float>::WIDE && COLS >= 2 && N % COLS == 0 && THREADS <= 1024 &&
+                               smem() <= kMaxBlockSmem;
 };
-template <int N> constexpr bool pair_columns() {
-    return !ColCfg<N, float>::WIDE && ColCfg<N, float>::COLS >= 2;
+// The step's tile: k times the engine's column tile (ColCfg::COLS), 64 or (LOOSE) 128 registers a thread.
+// Measured in a STEM run at each size (batch of ~1 GiB of waves, column-pass device time per probe·slice),
+// against the engine's tile at 64 registers:
+//   256² 2x loose −7%, 384² 2x loose −9%, 512² 2x −2.5%, 768² 4x −19%, 1024² 2x −8%, 1536² 4x −25%,
+//   2048² 4x −22%, 3072² 4x −22%, 4096² 2x −17%, 8192² 2x (two columns where the engine's tile has one) −33%.
+// Wider tiles put whole 32-byte sectors (and more of each 128-byte line) behind every row a block loads.
+template <int N> constexpr int pair_mult() {
+    return (N == 768 || N == 1536 || N == 2048 || N == 3072) ? 4 : (N >= 256 ? 2 : 1);
 }
+template <int N> constexpr bool pair_loose() { return N == 256 || N == 384; }
+template <int N> using PairStepCfg = PairCfg<N, pair_mult<N>() * ColCfg<N, float>::COLS, pair_loose<N>()>;
+template <int N> constexpr bool pair_columns() { return PairStepCfg<N>::ok; }
 
-template <int N>
-__global__ void __launch_bounds__(PairCfg<N>::THREADS, PairCfg<N>::MINB)
+template <int N, int COLS, bool LOOSE>
+__global__ void __launch_bounds__(PairCfg<N, COLS, LOOSE>::THREADS, PairCfg<N, COLS, LOOSE>::MINB)
 k_col_step_pair(float2 *__restrict__ wave, const float2 *__restrict__ twg, PropTables<float> pt, float bscale,
                 int tiles_lo) {
-    using PC = PairCfg<N>;
+    using PC = PairCfg<N, COLS, LOOSE>;
     using P = typename PC::P;
     constexpr int PAIRS = PC::PAIRS, E = P::E, NT = P::NT;
     extern __shared__ __align__(16) unsigned char smraw[];
