@@ -41,7 +41,7 @@ WORKLOAD = "stem_adf_perovskite_10x10x20_512x512_64x64probes_40slices_phonon_u0.
 # ncu: dram__bytes_read.sum + dram__bytes_write.sum per wave per launch of the step kernels at 512^2 FP32
 # (profiles/step_kernels_512_fp32_ncu.md, one launch of 256 waves); updated when the kernels change and are
 # re-captured
-NCU_DRAM_BYTES_PER_WAVE = {"row_step": 856.5e6 / 256, "col_step": 710.0e6 / 256}
+NCU_DRAM_BYTES_PER_WAVE = {"row_step": 856.5e6 / 256, "col_step": 679.5e6 / 256}
 
 
 def parse():
