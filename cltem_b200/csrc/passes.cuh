@@ -62,7 +62,10 @@ template <int N, class R> struct RowCfg {
     static constexpr size_t smem() { return sizeof(cplx<R>) * (size_t)(TWS + ROWS * ROWSZ); }
     static_assert(smem() <= kMaxBlockSmem, "row tile exceeds shared memory");
 };
-// Column tiles: COLS columns per block (a power of two dividing N), P::NT threads per column. Radix-8 plan:
+// Column tiles: COLS columns per block (a power of two dividing N), P::NT threads per column. FP64: wider
+// tiles than one 16-byte column measured faster per probe·slice in a STEM run (768²: 4 against 2 columns
+// −15%; 1536², 2048², 3072²: 2 against 1 −25%, −19%, −25%) and slower at 512² (8 against 4: +25%) and
+// 1024² (4 against 2: +1%); at 4096² and 8192² two columns need more than 1,024 threads. Radix-8 plan:
 // 512-thread blocks at the common sizes, a tile row of COLS complex values 64 B (FP32, N <= 512). Wide plan:
 // 128-thread blocks. Columns use the radix-8 plan at every size: measured at 512^2 FP32, the wide plan's
 // column pass (4 x 128-thread blocks per SM) took 609 us per 512-wave launch against 558 us for the radix-8
@@ -73,7 +76,7 @@ template <int N, class R> struct ColCfg {
     using P = std::conditional_t<WIDE, WidePlan<N>, Plan<N>>;
     static constexpr int COLS = WIDE ? (N <= 512 ? 8 : 4)
                                      : (sizeof(R) == 4 ? (N <= 512 ? 8 : (N <= 1024 ? 4 : (N <= 4096 ? 2 : 1)))
-                                                       : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1)));
+                                                       : (N <= 768 ? 4 : (N <= 3072 ? 2 : 1)));
     static_assert(N % COLS == 0, "column tile must divide the grid");
     static constexpr int THREADS = P::NT * COLS;
     static_assert(THREADS <= 1024, "column block too large");
