@@ -55,14 +55,15 @@ bool pair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw, Pr
 
 // the two-row step kernel of the FP32 non-wide row plans
 template <class RR> void rowpair_attrs() {
-    if constexpr (std::is_same<RR, float>::value && pair_rows<N>()) set_smem(k_row_step_pair<N>, RowPairCfg<N>::smem());
+    if constexpr (std::is_same<RR, float>::value && pair_rows<N>())
+        set_smem(k_row_step_pair<N, rowpair_pairs<N>()>, RowPairStepCfg<N>::smem());
 }
 template <class RR>
 bool rowpair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans, const cplx<RR> *tw, RR a, int xa,
                   int xb, int load_all, const int *tsel, size_t tstride) {
     if constexpr (std::is_same<RR, float>::value && pair_rows<N>()) {
-        using PC = RowPairCfg<N>;
-        k_row_step_pair<N><<<dim3(N / (2 * PC::PAIRS), batch), dim3(Plan<N>::NT, PC::PAIRS), PC::smem(), s>>>(
+        constexpr int PR = rowpair_pairs<N>();
+        k_row_step_pair<N, PR><<<dim3(N / (2 * PR), batch), dim3(Plan<N>::NT, PR), RowPairStepCfg<N>::smem(), s>>>(
             wave, trans, tw, a, xa, xb, load_all, tsel, tstride);
         MS_CUDA(cudaGetLastError());
         return true;

@@ -201,27 +201,33 @@ k_row_step_d(double2 *__restrict__ wave, const double2 *__restrict__ trans, cons
 // twiddle serves both rows (fft_pair.cuh; ColAddr<1, 16> keeps the stage writes conflict-free). Same
 // arithmetic per element as k_row_step<float, N>. Measured against the one-row kernel in a 256-probe STEM
 // run: 384² −10%, 768² −11%, 1536² −14%, 2048² −9%, 3072² −17%, 4096² −33%, with bit-identical results.
-template <int N> struct RowPairCfg {
+template <int N> constexpr int rowpair_base() { return RowCfg<N, float>::ROWS >= 2 ? RowCfg<N, float>::ROWS / 2 : 1; }
+template <int N, int PAIRS_ = rowpair_base<N>()> struct RowPairCfg {
     using P = Plan<N>;
-    static constexpr int PAIRS = RowCfg<N, float>::ROWS >= 2 ? RowCfg<N, float>::ROWS / 2 : 1;   // row pairs a block
+    static constexpr int PAIRS = PAIRS_;   // row pairs a block
     static constexpr int THREADS = P::NT * PAIRS;
     static constexpr size_t smem() { return sizeof(float2) * (size_t)N + sizeof(float4) * (size_t)N * PAIRS; }
+    static constexpr bool ok = !RowCfg<N, float>::WIDE && THREADS <= 1024 && N % (2 * PAIRS) == 0 &&
+                               smem() <= kMaxBlockSmem;
 };
-template <int N> constexpr bool pair_rows() {
-    return !RowCfg<N, float>::WIDE && RowPairCfg<N>::THREADS <= 1024;
-}
+// Row pairs a block of the step: twice the base at 384² and 768² (measured in a STEM run per size, row-pass
+// device time per probe·slice: −2.3% and −3.3%; 1536² to 4096² were 10-39% slower with 2 or 4 times the
+// base, 8192² has no room)
+template <int N> constexpr int rowpair_pairs() { return (N == 384 || N == 768 ? 2 : 1) * rowpair_base<N>(); }
+template <int N> using RowPairStepCfg = RowPairCfg<N, rowpair_pairs<N>()>;
+template <int N> constexpr bool pair_rows() { return RowPairStepCfg<N>::ok; }
 // blocks per SM the two-row step is compiled for: a 128-register budget (measured against no cap: 2048² and
 // 4096² the same, 384² to 3072² 6-21% faster at the cap)
-template <int N> constexpr int rowpair_minb() {
-    return RowPairCfg<N>::THREADS * 128 >= 65536 ? 1 : 65536 / (RowPairCfg<N>::THREADS * 128);
+template <int N, int PAIRS = rowpair_base<N>()> constexpr int rowpair_minb() {
+    return RowPairCfg<N, PAIRS>::THREADS * 128 >= 65536 ? 1 : 65536 / (RowPairCfg<N, PAIRS>::THREADS * 128);
 }
 
 // grid (N / (2 PAIRS), batch), block (NT, PAIRS)
-template <int N>
-__global__ void __launch_bounds__(RowPairCfg<N>::THREADS, rowpair_minb<N>())
+template <int N, int PAIRS_>
+__global__ void __launch_bounds__(RowPairCfg<N, PAIRS_>::THREADS, rowpair_minb<N, PAIRS_>())
 k_row_step_pair(float2 *__restrict__ wave, const float2 *__restrict__ trans, const float2 *__restrict__ twg, float a,
                 int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride) {
-    using PC = RowPairCfg<N>;
+    using PC = RowPairCfg<N, PAIRS_>;
     using P = typename PC::P;
     constexpr int E = P::E, NT = P::NT;
     extern __shared__ __align__(16) unsigned char smraw[];
