@@ -54,7 +54,9 @@ def parse():
     p.add_argument("--scan", type=int, default=64)
     p.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline and plain-FP64 legs")
     p.add_argument("--cpu-probes", type=int, default=32, help="probes in the bounded CPU sample")
-    p.add_argument("--only", default=None, choices=["adjoint", "cbed3d", "uneven", "cufft"],
+    p.add_argument("--sizes", default="256,384,512,768,1024,1536,2048,3072,4096,8192",
+                   help="grids of the sizes leg (comma-separated)")
+    p.add_argument("--only", default=None, choices=["adjoint", "cbed3d", "uneven", "cufft", "sizes"],
                    help="run one extra leg alone and print its JSON (for profiling it)")
     p.add_argument("--cbed-nz", type=int, default=60, help="FCC cells along z of the cbed3d leg (60: 120 slices)")
     return p.parse_args()
@@ -361,6 +363,50 @@ def cbed3d_leg(ctx, ext, nz=60):
             "note": "one configuration of the 50; evaluations counted on the host from the binned atoms"}
 
 
+def sizes_leg(ctx, sizes, dp=False, n_atoms=30, seed=11):
+    """The step kernels at each grid: FP32 (or FP64) STEM of a batch of about 1 GiB of waves (at most 1024
+    probes) through 7 slices of 0.25 Å over a 400 Å field holding a few seeded atoms; device time per
+    probe·slice of the row and column passes (the column figure includes the last step of each batch, which
+    carries the detector reduction), from the engine's per-kernel event timing of the third of three runs."""
+    import torch
+    from cltem_b200 import config
+    from cltem_b200.engine import Simulation
+    from cltem_b200.structure import Structure
+    rng = np.random.default_rng(seed)
+    st = Structure(rng.choice([8, 22, 38], n_atoms).astype(np.int32), rng.uniform(-40, 40, n_atoms),
+                   rng.uniform(-40, 40, n_atoms), rng.uniform(0.2, 1.7, n_atoms))
+    out = {}
+    for res in sizes:
+        s, _ = config.perovskite_stem(n=(1, 1, 1), resolution=res, scan=1, double_precision=dp)
+        c = s.cfg
+        c.allow_any_resolution = 1
+        c.stem_area[:] = [0.0, 0.2, 0.0, 0.2]
+        c.padding_xy = 192.0
+        c.slice_thickness, c.slice_offset = 0.25, 0.125
+        npr = min(1024, max(4, (1 << 30) // (res * res * (16 if dp else 8))))
+        k = int(np.ceil(np.sqrt(npr)))
+        c.stem_pixels_x = c.stem_pixels_y = k
+        s.attach_structure(st)
+        sim = Simulation(ctx, c)
+        sim.set_atoms(st)
+        pix = np.arange(npr, dtype=np.int32)
+        sim.stem(pix)
+        sim.stem(pix)
+        torch.cuda.synchronize()
+        sim.profile(True)
+        sim.profile_read(reset=True)
+        sim.stem(pix)
+        torch.cuda.synchronize()
+        p = sim.profile_read()
+        sim.profile(False)
+        S = sim.geo.n_slices
+        out[str(res)] = {"probes": npr, "slices": S,
+                         "row_us_per_probe_slice": 1e3 * p["row_step"][0] / (npr * S),
+                         "col_us_per_probe_slice": 1e3 * p["col_step"][0] / (npr * S)}
+        sim.close()
+    return {"workload": f"stem_sparse_400A_{'fp64' if dp else 'fp32'}", "sizes": out}
+
+
 def uneven_leg(ctx, n_cells=48, n_configs=4, seed=2024):
     """Uneven batched STEM: 48 seeded perovskite / FCC cells (4-16 cells laterally, 10-80 slices, grids
     256-1024, 80-300 kV, 16-32 mrad, 16x16 probes, 4 phonon configurations each), FP32, each grid with the
@@ -408,7 +454,8 @@ def main():
         ctx.load_params(load_default("kirkland"))
         ext = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
         leg = {"adjoint": lambda: adjoint_leg(ctx, ext, args.warmup), "cbed3d": lambda: cbed3d_leg(ctx, ext, args.cbed_nz),
-               "uneven": lambda: uneven_leg(ctx), "cufft": lambda: cufft_leg()}[args.only]()
+               "uneven": lambda: uneven_leg(ctx), "cufft": lambda: cufft_leg(),
+               "sizes": lambda: sizes_leg(ctx, [int(v) for v in args.sizes.split(",")])}[args.only]()
         print(json.dumps({"leg": args.only, **leg}))
         return 0
     if world > 1:
