@@ -38,9 +38,9 @@ sys.path.insert(0, ROOT)
 METRIC = "STEM probe·slices/s at 512² FP32 vs plain FP64 GPU; adjoint/forward time ratio"
 UNIT = "probe·slices/s"
 WORKLOAD = "stem_adf_perovskite_10x10x20_512x512_64x64probes_40slices_phonon_u0.08"
-# ncu: dram__bytes_read.sum + dram__bytes_write.sum per wave per launch of the step kernels at 512^2 FP32
-# (profiles/step_kernels_512_fp32_ncu.md, one launch of 256 waves); updated when the kernels change and are
-# re-captured
+# DRAM bytes per wave of one launch of each step kernel at 512^2 FP32 (ncu dram__bytes_read.sum +
+# dram__bytes_write.sum over one launch, divided by its waves), measured on this build's kernels; a kernel
+# change needs a new capture
 NCU_DRAM_BYTES_PER_WAVE = {"row_step": 856.5e6 / 256, "col_step": 679.5e6 / 256}
 
 
@@ -291,6 +291,40 @@ def adjoint_leg(ctx, ext, warmup):
                     "transmission build of the 32 slices"}
 
 
+def parity_leg(ctx, sim, confs, avg_image, n_pixels=8, seed=31):
+    """Correctness of the headline run, outside the timed region, on n_pixels seeded scan pixels: the FP32
+    engine's image of the first timed configuration (staged and run again through the same batches and
+    graphs) against the FP64 CPU oracle, and the FP32 image averaged over every timed configuration against
+    the FP64 engine averaged over the same configurations (relative L2 over the pixels)."""
+    from oracle import bind as ob
+    from cltem_b200.engine import Simulation
+    from cltem_b200.params import load_default
+    avg32 = np.asarray(avg_image).reshape(-1)
+    npx = sim.cfg.stem_pixels_x * sim.cfg.stem_pixels_y
+    pix = np.sort(np.random.default_rng(seed).choice(npx, n_pixels, replace=False)).astype(np.int32)
+    sim.stage(confs[:1])
+    sim.run_staged()
+    one32 = sim.staged_result().reshape(-1)
+    t0 = time.perf_counter()
+    o = ob.OracleSim(sim.cfg, load_default("kirkland"), double_precision=True)
+    o.set_atoms(confs[0])
+    o.build_transmission()
+    ref = o.stem(pix).reshape(-1)
+    t_oracle = time.perf_counter() - t0
+    s64, _ = workload(double_precision=True)
+    sim64 = Simulation(ctx, s64.cfg)
+    acc = np.zeros(n_pixels)
+    for c in confs:
+        sim64.set_atoms(c)
+        acc += sim64.stem(pix).reshape(-1)
+    sim64.close()
+    acc /= len(confs)
+    rl2 = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    return {"pixels": pix.tolist(), "fp32_vs_fp64_oracle_config0": rl2(one32[pix], ref),
+            "fp32_avg_vs_fp64_engine_avg": rl2(avg32[pix], acc), "configs_averaged": len(confs),
+            "tolerance": 1e-5, "oracle_s": t_oracle}
+
+
 def full3d_evaluations(sim, n_atoms, S, N):
     """Atom-sample evaluations of one full-3D potential build (the unit the CBED full-3D throughput is quoted
     in): for every binned atom, the pixels within 8 Å in xy times the (slice, sub-slice sample) pairs of the
@@ -521,6 +555,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
     img = sim.staged_result()
+    img_local = img.copy()   # this rank's average (the parity leg checks it)
     # one exchange step: merge the per-rank image sums and weights (SimulationManager::updateImages)
     from cltem_b200.distributed import merge_average
     img = merge_average(img * args.steps, args.steps, device=torch.device("cuda", local))
@@ -540,9 +575,7 @@ def main():
     dom = ("row_step", row_bytes, row_ms, row_n) if row_ms >= col_ms else ("col_step", col_bytes, col_ms, col_n)
     peak, peak_src = peaks()
     achieved = dom[1] / (dom[2] / 1000.0) / 1e9
-    # DRAM bytes per wave per launch from one ncu capture of this build's step kernels
-    # (profiles/step_kernels_512_fp32_ncu.md: dram__bytes_read.sum + dram__bytes_write.sum / 256 waves),
-    # scaled to this run's launches
+    # DRAM bytes per wave from one ncu capture of this build's step kernels, scaled to this run's launches
     per_wave = NCU_DRAM_BYTES_PER_WAVE.get(dom[0])
     traffic = per_wave * (npx * S * args.steps) / max(dom[3], 1) if per_wave else None
     roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -587,6 +620,10 @@ def main():
         e2e = {"value": npx * S * len(e2e_confs) * world / (ms_e2e / 1000.0), "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(out.numel() * 8),
                "steps": len(e2e_confs), "ms_per_step": ms_e2e / len(e2e_confs)}
+
+    parity = None
+    if rank == 0 and not args.no_baseline:
+        parity = parity_leg(ctx, sim, confs, img_local)
 
     adjoint = cbed3d = uneven = None
     if rank == 0 and world == 1 and not args.no_baseline:
@@ -651,6 +688,7 @@ def main():
             "cbed_full3d": cbed3d,
             "uneven_stem": uneven,
             "e2e": e2e,
+            "parity": parity,
             "gpu_launches": launches,
             "clocks": clk,
         }

@@ -33,7 +33,9 @@ __global__ void k_atom_keys(int n, const double *__restrict__ x, const double *_
             bidy -= (bidy == g.blocks_y);
             bid = bidx + g.blocks_x * bidy;
         }
-        if (bid >= 0 && zid >= 0) key = zid * g.blocks_x * g.blocks_y + bid;
+        // zid < n_slices holds for a geometry whose slice count covers z_lims (mslice_geometry_compute); the test
+        // keeps a caller-filled geometry that does not from forming keys beyond the bins
+        if (bid >= 0 && zid >= 0 && zid < g.n_slices) key = zid * g.blocks_x * g.blocks_y + bid;
     }
     keys[i] = key;
     idx[i] = i;
@@ -57,8 +59,8 @@ __global__ void k_atom_gather(int n, const int *__restrict__ idx, const int *__r
 __global__ void k_atom_hist(int n, const int *__restrict__ keys, int n_bins, int *__restrict__ counts) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int k = keys[i];
-    if (k < n_bins) atomicAdd(&counts[k], 1);
+    const int k = keys[i];
+    if ((unsigned)k < (unsigned)n_bins) atomicAdd(&counts[k], 1);
 }
 
 static int key_bits(int n_bins) {

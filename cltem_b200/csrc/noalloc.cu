@@ -9,7 +9,7 @@
 #include "../../include/mslice.h"
 #include "misc.cuh"
 
-#include <mutex>
+#include <cmath>
 #include <string>
 
 namespace ms {
@@ -27,23 +27,14 @@ constexpr size_t kMaxAtoms = 131072;
 constexpr size_t kMaxBins = 65535;
 __device__ __align__(256) unsigned char g_bin_scratch[kScratchBytes];
 
-std::mutex g_scratch_mtx;
-void *g_scratch_addr[64] = {};
-
-// Device address of g_bin_scratch on the current device, looked up once per device.
+// Device address of g_bin_scratch on the current device. It is looked up on every call (the lookup is
+// cheap), so an address cached before a device reset or a primary-context teardown is never reused.
 void *scratch_address() {
-    int dev = 0;
-    MS_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) throw ms::CudaError("device ordinal out of range for the binning scratch");
-    std::lock_guard<std::mutex> lk(g_scratch_mtx);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_bin_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            throw ms::CudaError(std::string("cudaGetSymbolAddress of the binning scratch failed: ") + cudaGetErrorString(e));
-        g_scratch_addr[dev] = p;
-    }
-    return g_scratch_addr[dev];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_bin_scratch);
+    if (e != cudaSuccess || p == nullptr)
+        throw ms::CudaError(std::string("cudaGetSymbolAddress of the binning scratch failed: ") + cudaGetErrorString(e));
+    return p;
 }
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
@@ -58,6 +49,12 @@ extern "C" int mslice_bin_atoms_noalloc(const mslice_geometry *geo, const int *Z
             throw std::invalid_argument("null argument");
         if (geo->n_slices < 1 || geo->blocks_x < 1 || geo->blocks_y < 1 || !(geo->dz > 0))
             throw std::invalid_argument("geometry is not initialised (use mslice_geometry_compute)");
+        // the limits must be ordered and the slice count must cover z_lims as mslice_geometry_compute makes it
+        // (sliceCount, simulationcell.cpp:75-83), so every kept atom's slice index lies below n_slices
+        if (!(geo->full_x[1] > geo->full_x[0]) || !(geo->full_y[1] > geo->full_y[0]) || !(geo->z_lims[1] > geo->z_lims[0]))
+            throw std::invalid_argument("geometry limits are empty or reversed");
+        if ((double)geo->n_slices < std::ceil((geo->z_lims[1] - geo->z_lims[0]) / geo->dz - 0.000001))
+            throw std::invalid_argument("geometry: n_slices does not cover z_lims at slice thickness dz");
         const size_t n_bins = (size_t)geo->n_slices * geo->blocks_x * geo->blocks_y;
         if (n > kMaxAtoms)
             throw std::invalid_argument("mslice_bin_atoms_noalloc: " + std::to_string(n) + " atoms exceed its limit of " +

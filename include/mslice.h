@@ -329,7 +329,9 @@ int mslice_profile_read(mslice_sim *sim, int kernel, double *total_ms, unsigned 
  * the caller — on `stream` (a cudaStream_t, NULL for the default stream); it returns once the work is
  * queued. Its working memory is one fixed 8 MiB device array inside the library, held on every device that
  * loads the library until the process exits; the limits are 131072 atoms and 65535 bins, and larger
- * requests fail with MSLICE_ERR_ARG. The first call on a device looks the array up (cudaGetSymbolAddress),
+ * requests fail with MSLICE_ERR_ARG, as does a geometry whose limits are empty or whose n_slices does not
+ * cover z_lims at thickness dz. Every call looks the array's device address up (cudaGetSymbolAddress, so no
+ * address outlives a device reset); the first call on a device also loads the library's device code there,
  * so make that first call before any stream capture. Every call reuses the same array: calls whose work
  * overlaps on the GPU (two streams, two host threads) race on it, so serialise them. */
 int mslice_bin_atoms_noalloc(const mslice_geometry *geo, const int *Z, const double *x, const double *y, const double *z,

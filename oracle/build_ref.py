@@ -3,7 +3,8 @@
 TEST INFRASTRUCTURE ONLY. The reference (clTEM) cannot be built here: its host code needs the OpenCL
 C++ bindings, an OpenCL platform, clFFT, libtiff, Eigen and easylogging++. Its kernels, though, are
 OpenCL C, close enough to C++ that g++ compiles them with a small shim. This script
-  1. reads kernels/<name>_d.cl from the reference tree (default /root/reference, or argv[1]),
+  1. reads kernels/<name>_d.cl from the reference tree (argv[1], else $CLTEM_REFERENCE, else the build
+     container's mount point below),
   2. applies clTEM's own source transform for the default math mode: delete "native_"
      (KernelSource::BuildToKernel, src/simulation/kernels.h:37-45),
   3. applies two syntax shims that OpenCL C needs and C++ lacks: the vector literal
@@ -25,6 +26,18 @@ KERNELS = ["atom_sort", "band_limit", "band_pass", "complex_multiply", "complex_
            "transmission_potentials_projected", "transmission_potentials_full_3d", "ctem_image"]
 
 
+# Where the build container mounts the reference tree (read-only). This recipe is the one place that names
+# it; the fixture scripts and the package build ask reference_root().
+_CONTAINER_MOUNT = "/root/reference"
+
+
+def reference_root(arg=None):
+    """The clTEM source tree to read: `arg`, else $CLTEM_REFERENCE, else the build container's mount point;
+    None when that directory holds no kernels/ (machines without the reference, such as the GPU box)."""
+    root = arg or os.environ.get("CLTEM_REFERENCE") or _CONTAINER_MOUNT
+    return root if os.path.isdir(os.path.join(root, "kernels")) else None
+
+
 def transform(src: str) -> str:
     src = src.replace("native_", "")
     src = re.sub(r"\(double2\)\s*\(", "make_double2(", src)
@@ -32,7 +45,10 @@ def transform(src: str) -> str:
     return src
 
 
-def build(ref_root="/root/reference", quiet=False):
+def build(ref_root=None, quiet=False):
+    ref_root = reference_root(ref_root)
+    if ref_root is None:
+        raise FileNotFoundError("reference tree not found: pass its path or set CLTEM_REFERENCE")
     kdir = os.path.join(ref_root, "kernels")
     if not os.path.isdir(kdir):
         raise FileNotFoundError(f"reference kernels not found under {kdir}")
@@ -55,4 +71,4 @@ def build(ref_root="/root/reference", quiet=False):
 
 
 if __name__ == "__main__":
-    build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    build(sys.argv[1] if len(sys.argv) > 1 else None)

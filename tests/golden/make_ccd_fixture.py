@@ -1,6 +1,6 @@
 """Make tests/golden/ccds.json from the reference's CCD tables.
 
-Run in a container where the clTEM sources are mounted (default /root/reference):
+Run where the clTEM sources are present (the path as the argument, else as oracle/build_ref.py finds it):
     python tests/golden/make_ccd_fixture.py [reference_root]
 The tables (DQE and NTF of the K2 and Orius cameras, ccds/*.dat) are the inputs of clTEM's CTEM dose
 simulation (src/simulation/microscope/simulationctem.cpp:88-108, 171-264); bundling them lets the tests
@@ -17,7 +17,10 @@ from cltem_b200.params import read_ccd  # noqa: E402
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    from oracle.build_ref import reference_root
+    root = reference_root(sys.argv[1] if len(sys.argv) > 1 else None)
+    if root is None:
+        raise SystemExit("reference tree not found: pass its path or set CLTEM_REFERENCE")
     out = {}
     for fn in sorted(os.listdir(os.path.join(root, "ccds"))):
         if fn.endswith(".dat"):

@@ -1,6 +1,6 @@
 """Make tests/golden/params.json from the reference's parameter tables.
 
-Run in a container where the clTEM sources are mounted (default /root/reference):
+Run where the clTEM sources are present (the path as the argument, else as oracle/build_ref.py finds it):
     python tests/golden/make_params_fixture.py [reference_root]
 The tables (Kirkland, Peng, Lobato scattering-factor parameterisations) are the inputs the
 multislice path reads at run time (src/simulation/utilities/stringutils.cpp:149-184); bundling them
@@ -19,7 +19,10 @@ FORM_NAMES = {0: "kirkland", 1: "peng", 2: "lobato"}
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    from oracle.build_ref import reference_root
+    root = reference_root(sys.argv[1] if len(sys.argv) > 1 else None)
+    if root is None:
+        raise SystemExit("reference tree not found: pass its path or set CLTEM_REFERENCE")
     out = {}
     for fn in ("kirkland.dat", "peng.dat", "lobato.dat"):
         p = read_params(os.path.join(root, "params", fn))

@@ -2,7 +2,7 @@
 seeded inputs, for parity checks where the reference tree is absent (the GPU box).
 
 Needs oracle/_ref/libref.so, built from the reference's kernels/*_d.cl by oracle/build_ref.py:
-    python oracle/build_ref.py /root/reference && python tests/golden/make_ref_golden.py
+    python oracle/build_ref.py [reference_root] && python tests/golden/make_ref_golden.py
 Inputs come from the seeded workloads of tests/cases.py; the binned atoms the potential kernels read are
 produced by the reference's atom_sort kernel plus the host binning (restated in the oracle, whose ids this
 script checks against atom_sort first).
@@ -38,7 +38,7 @@ def pot_args(g, cfg, form, icount, k, full3d):
 
 def main():
     if not rb.available():
-        raise SystemExit("build the reference kernels first: python oracle/build_ref.py /root/reference")
+        raise SystemExit("build the reference kernels first: python oracle/build_ref.py [reference_root]")
     P = read_params_json(default_bundle_path())
     L = rb.lib()
     out = {}

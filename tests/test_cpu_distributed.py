@@ -1,6 +1,7 @@
-"""The N>1 path on CPU: world-size-2 gloo processes shard frozen-phonon configurations and merge the
-images with one all-reduce; the result equals the single-process average. (The images here come from the
-CPU oracle so the test needs no GPU; the GPU ranks run the same sharding and merge in bench.py.)"""
+"""The N>1 path on CPU: world-size-2 gloo processes shard frozen-phonon configurations (or scan pixels)
+and merge the images with one all-reduce; the result equals the single-process average. (The images here
+come from the CPU oracle so the test needs no GPU; tests/test_gpu_distributed.py merges the engine's own
+images the same way.)"""
 import os
 import socket
 
@@ -27,7 +28,7 @@ def _free_port():
     return p
 
 
-def _worker(rank, world, port, out_path):
+def _worker(rank, world, port, out_path, mode="configs"):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -41,23 +42,34 @@ def _worker(rank, world, port, out_path):
     osim = ob.OracleSim(s.cfg, load_default("kirkland"))
     pix = np.arange(4, dtype=np.int32)
     acc = np.zeros((1, 2, 4))
-    mine = shard_configs(len(confs), rank, world)
-    for c in mine:
-        osim.set_atoms(confs[c])
-        osim.build_transmission()
-        acc += osim.stem(pix)
-    avg = merge_average(acc, len(mine))
+    if mode == "configs":        # whole configurations per rank, one weight per rank
+        mine = shard_configs(len(confs), rank, world)
+        for c in mine:
+            osim.set_atoms(confs[c])
+            osim.build_transmission()
+            acc += osim.stem(pix)
+        avg = merge_average(acc, len(mine))
+    else:                        # every configuration over this rank's scan pixels, per-pixel weights
+        mine = np.array(shard_pixels(len(pix), rank, world), dtype=np.int32)
+        w = np.zeros_like(acc)
+        for c in confs:
+            osim.set_atoms(c)
+            osim.build_transmission()
+            acc[..., mine] += osim.stem(pix[mine])
+            w[..., mine] += 1
+        avg = merge_average(acc, w)
     if rank == 0:
         np.save(out_path, avg)
     dist.barrier()
     dist.destroy_process_group()
 
 
-def test_two_rank_gloo_merge_equals_single_process(tmp_path):
+@pytest.mark.parametrize("mode", ["configs", "pixels"])
+def test_two_rank_gloo_merge_equals_single_process(tmp_path, mode):
     out = str(tmp_path / "avg.npy")
     ctx = mp.get_context("spawn")
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, out)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, out, mode)) for r in range(2)]
     for p in procs:
         p.start()
     for p in procs:
