@@ -272,6 +272,30 @@ std::vector<float2> potp_table(int form, int i_count, const std::vector<double> 
     return t;
 }
 
+// A twiddle (cos a, sin a) rounded to R. FP32: of the roundings down and up of its two parts, the pair whose
+// squared modulus is closest to 1 (then the nearest): an FFT round trip multiplies by |w|^2, and a modulus
+// error would repeat at every slice and add up with thickness, while a phase error of up to an ulp does not
+// (the inverse transform's conjugate twiddle undoes it). FP64: the nearest doubles.
+template <class R> cplx<R> round_unit(long double c, long double s) {
+    if constexpr (sizeof(R) == 8) {
+        return mk<R>((R)c, (R)s);
+    } else {
+        auto down = [](long double v) { float f = (float)v; return (long double)f > v ? std::nextafter(f, -2.0f) : f; };
+        auto up = [](long double v) { float f = (float)v; return (long double)f < v ? std::nextafter(f, 2.0f) : f; };
+        const float cs[2] = {down(c), up(c)}, ss[2] = {down(s), up(s)};
+        float bc = (float)c, bs = (float)s;
+        long double best_m = std::fabs((long double)bc * bc + (long double)bs * bs - 1.0L);
+        long double best_d = std::fabs((long double)bc - c) + std::fabs((long double)bs - s);
+        for (float cc : cs)
+            for (float sc : ss) {
+                const long double m = std::fabs((long double)cc * cc + (long double)sc * sc - 1.0L);
+                const long double d = std::fabs((long double)cc - c) + std::fabs((long double)sc - s);
+                if (m < best_m || (m == best_m && d < best_d)) { best_m = m; best_d = d; bc = cc; bs = sc; }
+            }
+        return mk<R>(bc, bs);
+    }
+}
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -287,6 +311,7 @@ struct Ctx {
     size_t potp_n = 0;
     std::map<int, void *> tw_f, tw_d;   // twiddle tables per size
     std::mutex mtx;
+    int *step_err = nullptr;   // error word of the persistent step passes (tma.cuh StepError; 0 = none)
 
     void *alloc(size_t bytes) {
         if (bytes == 0) return nullptr;
@@ -319,7 +344,7 @@ struct Ctx {
             for (int k = 0; k < Ns; k++)
                 for (int r = 1; r < RAD; r++) {
                     long double a = -two_pi * (long double)(r * k) / (long double)(Ns * RAD);
-                    h[plan_tw_index(n, s, k, r)] = mk<R>((R)std::cos(a), (R)std::sin(a));
+                    h[plan_tw_index(n, s, k, r)] = round_unit<R>(std::cos(a), std::sin(a));
                 }
         }
         if (wide) {
@@ -327,7 +352,7 @@ struct Ctx {
             for (int k = 0; k < E; k++)
                 for (int r = 1; r < R2; r++) {
                     long double a = -two_pi * (long double)(r * k) / (long double)n;
-                    h[n + k * (R2 - 1) + (r - 1)] = mk<R>((R)std::cos(a), (R)std::sin(a));
+                    h[n + k * (R2 - 1) + (r - 1)] = round_unit<R>(std::cos(a), std::sin(a));
                 }
         }
         void *d = alloc(sizeof(cplx<R>) * count);
@@ -337,6 +362,7 @@ struct Ctx {
     }
     ~Ctx() {
         cudaSetDevice(device);
+        cudaFree(step_err);
         for (auto &kv : tw_f) cudaFree(kv.second);
         for (auto &kv : tw_d) cudaFree(kv.second);
         cudaFree(prm_d);
@@ -452,6 +478,8 @@ struct SimBase {
                                 bool want_grad) = 0;
     virtual void set_c10_c30(double c10, double c30) = 0;
     virtual void tune_batch(const int *cands, int n, int reps, int *best, double *rate) = 0;
+    virtual void set_step_variant(int col, int row) = 0;
+    virtual void get_tuning(int *batch, int *col, int *n_col, int *row, int *n_row) = 0;
     virtual void set_ccd(const double *dqe, const double *ntf, size_t n, int binning, double dose) = 0;
 };
 
@@ -468,6 +496,7 @@ struct Sim : SimBase {
     DevBuf<int2> ycut;   // per column, the band of rows the propagator's cut keeps
     PlainWork plain_work;   // buffers and plan of the plain FP64 path (stem_plain)
     DevBuf<C> px, py, pxc, pyc;   // propagator factors and their conjugates (adjoint)
+    DevBuf<C> pxe, pye, pxec, pyec;   // FP32: relative representation errors of px, py and of their conjugates
     DevBuf<double2> chi;
     DevBuf<uint16_t> detmask;
     double k_prop = 0;   // k_max * limit factor of the propagator cut
@@ -562,19 +591,35 @@ struct Sim : SimBase {
             const double bk = g.wavenumber, bx = g.wavevector[0], by = g.wavevector[1], bz = g.wavevector[2];
             const double f = bz / bk;
             const double c0 = kPi * g.dz * (bk * bk - bz * bz) / bz;
-            std::vector<C> hpx(N), hpy(N);
+            std::vector<C> hpx(N), hpy(N), hex(N), hey(N);
+            // relative error (p64 - p) / p of a factor rounded to R, in FP64 (zero in the FP64 engine)
+            auto rel_err = [](double re, double im, C r) {
+                const double dr = re - (double)r.x, di = im - (double)r.y, n2 = (double)r.x * r.x + (double)r.y * r.y;
+                return mk<R>((R)((dr * r.x + di * r.y) / n2), (R)((di * r.x - dr * r.y) / n2));
+            };
             for (int i = 0; i < N; i++) {
                 double ax_ = -kPi * g.dz * (bx + H.kx[i]) * (bx + H.kx[i]) / bz + c0;
                 double ay_ = -kPi * g.dz * (by + H.ky[i]) * (by + H.ky[i]) / bz;
                 hpx[i] = mk<R>((R)(f * std::cos(ax_)), (R)(f * std::sin(ax_)));
                 hpy[i] = mk<R>((R)std::cos(ay_), (R)std::sin(ay_));
+                hex[i] = rel_err(f * std::cos(ax_), f * std::sin(ax_), hpx[i]);
+                hey[i] = rel_err(std::cos(ay_), std::sin(ay_), hpy[i]);
             }
             px.ensure(ctx, N); py.ensure(ctx, N); pxc.ensure(ctx, N); pyc.ensure(ctx, N);
+            pxe.ensure(ctx, N); pye.ensure(ctx, N); pxec.ensure(ctx, N); pyec.ensure(ctx, N);
             MS_CUDA(cudaMemcpyAsync(px.p, hpx.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
             MS_CUDA(cudaMemcpyAsync(py.p, hpy.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
-            for (int i = 0; i < N; i++) { hpx[i].y = -hpx[i].y; hpy[i].y = -hpy[i].y; }
+            MS_CUDA(cudaMemcpyAsync(pxe.p, hex.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
+            MS_CUDA(cudaMemcpyAsync(pye.p, hey.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
+            MS_CUDA(cudaStreamSynchronize(st()));   // the host vectors are rewritten below
+            for (int i = 0; i < N; i++) {
+                hpx[i].y = -hpx[i].y; hpy[i].y = -hpy[i].y;
+                hex[i].y = -hex[i].y; hey[i].y = -hey[i].y;   // conj(p (1 + e)) = conj(p) (1 + conj(e))
+            }
             MS_CUDA(cudaMemcpyAsync(pxc.p, hpx.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
             MS_CUDA(cudaMemcpyAsync(pyc.p, hpy.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
+            MS_CUDA(cudaMemcpyAsync(pxec.p, hex.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
+            MS_CUDA(cudaMemcpyAsync(pyec.p, hey.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
             MS_CUDA(cudaStreamSynchronize(st()));
         }
         {
@@ -871,6 +916,19 @@ struct Sim : SimBase {
     }
 
     int tuned_batch = 0;   // set by tune_batch (or the per-process cache of earlier tunings)
+    int col_variant = 0;   // kernel of the batched column step (PassOps::col_step), set by tune_batch
+    int row_variant = 0;   // L2 prefetch distance of the batched row step (PassOps::row_step), set by tune_batch
+
+    // the error word of the persistent passes: read after the stream's work is done, reset, reported
+    void check_step_err() {
+        int e = 0;
+        MS_CUDA(cudaMemcpyAsync(&e, ctx->step_err, sizeof(int), cudaMemcpyDeviceToHost, st()));
+        MS_CUDA(cudaStreamSynchronize(st()));
+        if (e != 0) {
+            MS_CUDA(cudaMemsetAsync(ctx->step_err, 0, sizeof(int), st()));
+            throw CudaError("a persistent step pass abandoned a wait (code " + std::to_string(e) + "); results are invalid");
+        }
+    }
     int default_batch() const {
         if (cfg.probe_batch > 0) return cfg.probe_batch;
         if (tuned_batch > 0) return tuned_batch;
@@ -1016,7 +1074,7 @@ struct Sim : SimBase {
             ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N), df, g.wavelength);
         });
         ctx->launches++;
-        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p};
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p, ctx->step_err, pxe.p, pye.p};
         DetArgs det{detmask.p, cfg.n_detectors, partials.p};
         std::vector<int> outs = output_slices(cfg, g);
         size_t oi = 0;
@@ -1024,12 +1082,12 @@ struct Sim : SimBase {
         for (int s = 0; s < g.n_slices; s++) {
             timed(st(), MSLICE_K_ROW_STEP, (double)nb * NN * sizeof(C) * ((s == 0 ? 1.0 : fa) + 1.0 + fa), [&] {
                 ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a, xa, xb, s == 0 ? 1 : 0,
-                             sel ? sel + (size_t)s * nb : nullptr, set_stride);
+                             sel ? sel + (size_t)s * nb : nullptr, set_stride, row_variant);
             });
             bool is_out = oi < outs.size() && outs[oi] == s;
             int mode = !is_out ? COL_STEP : (s == g.n_slices - 1 ? COL_DET_ONLY : COL_STEP_DET);
             timed(st(), MSLICE_K_COL_STEP, (double)nb * NN * sizeof(C) * fa * (mode == COL_DET_ONLY ? 1.0 : 2.0), [&] {
-                ops.col_step(st(), wave.p, nb, tw, pt, b, ds, det, nullptr, mode, tiles_lo, tiles_hi);
+                ops.col_step(st(), wave.p, nb, tw, pt, b, ds, det, nullptr, mode, tiles_lo, tiles_hi, col_variant);
             });
             ctx->launches += 2;
             if (is_out) {
@@ -1064,6 +1122,7 @@ struct Sim : SimBase {
         auto after_batch = [&](size_t done) {
             if (!sync_each) return;
             MS_CUDA(cudaStreamSynchronize(st()));
+            check_step_err();
             flush_profile();
             if (progress) progress((double)done / n, progress_user);
         };
@@ -1170,7 +1229,7 @@ struct Sim : SimBase {
                           g.wavelength);
         }
         ctx->launches++;
-        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p};
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p, ctx->step_err, pxe.p, pye.p};
         DetArgs det{detmask.p, 0, partials.p};
         std::vector<int> outs = output_slices(cfg, g);
         size_t oi = 0;
@@ -1180,12 +1239,12 @@ struct Sim : SimBase {
             // single waves keep every column so the exit wave and the reciprocal copy are complete
             timed(st(), MSLICE_K_ROW_STEP, 3.0 * NN * sizeof(C), [&] {
                 ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1, K > 1 ? tsel.p + s : nullptr,
-                             set_stride);
+                             set_stride, 0);
             });
             bool is_out = oi < outs.size() && outs[oi] == s;
             timed(st(), MSLICE_K_COL_STEP, (is_out ? 3.0 : 2.0) * NN * sizeof(C), [&] {
                 ops.col_step(st(), wave.p, 1, tw, pt, b, ds, det, is_out ? recip.p : nullptr, is_out ? COL_STEP_DET : COL_STEP,
-                             N / ops.cols_per_tile, 0);
+                             N / ops.cols_per_tile, 0, 0);
             });
             ctx->launches += 2;
             if (is_out) { on_output((int)oi); oi++; }
@@ -1379,6 +1438,7 @@ struct Sim : SimBase {
             }
             MS_CUDA(cudaEventRecord(ev[3], st()));
             MS_CUDA(cudaEventSynchronize(ev[3]));
+            check_step_err();
             flush_profile();
             float a = 0, b = 0;
             MS_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
@@ -1402,11 +1462,14 @@ struct Sim : SimBase {
         for (size_t i = 0; i < acc_n; i++) out[i] /= (double)acc_configs;
     }
 
-    // Autotuner of the probe batch: time `reps` STEM slice steps (one row and one column pass) at each
-    // candidate batch on zeroed scratch waves with the current transmission tables, and keep the batch
-    // with the most waves per second. Results are cached per (device, grid, precision) for the process.
-    static std::map<std::tuple<int, int, int>, std::pair<int, double>> &tune_cache() {
-        static std::map<std::tuple<int, int, int>, std::pair<int, double>> m;
+    // Autotuner of the probe batch and of the column step's kernel: time `reps` STEM slice steps (one row and
+    // one column pass) for each candidate batch and each column-pass variant (PassOps::col_variants: the
+    // one-launch-per-tile kernel and the persistent TMA-fed passes) on zeroed scratch waves with the current
+    // transmission tables, and keep the pair with the most waves per second. Results are cached per
+    // (device, grid, precision) for the process.
+    struct Tuning { int batch; double rate; int col_variant; int row_variant; };
+    static std::map<std::tuple<int, int, int>, Tuning> &tune_cache() {
+        static std::map<std::tuple<int, int, int>, Tuning> m;
         return m;
     }
     void tune_batch(const int *cands, int n, int reps, int *best, double *rate) override {
@@ -1416,9 +1479,11 @@ struct Sim : SimBase {
             std::lock_guard<std::mutex> lk(ctx->mtx);
             auto it = tune_cache().find(key);
             if (it != tune_cache().end() && cands == nullptr) {
-                tuned_batch = it->second.first;
-                if (best) *best = it->second.first;
-                if (rate) *rate = it->second.second;
+                tuned_batch = it->second.batch;
+                col_variant = it->second.col_variant;
+                row_variant = it->second.row_variant;
+                if (best) *best = it->second.batch;
+                if (rate) *rate = it->second.rate;
                 return;
             }
         }
@@ -1439,16 +1504,14 @@ struct Sim : SimBase {
         MS_CUDA(cudaMemsetAsync(wave.p, 0, (size_t)bmax * wave_bytes, st()));
         if (!trans_built) MS_CUDA(cudaMemsetAsync(trans.p, 0, NN * sizeof(C), st()));
         const cplx<R> *tw = ctx->twiddles<R>(N);
-        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p};
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p, ctx->step_err, pxe.p, pye.p};
         DetArgs det{detmask.p, cfg.n_detectors, partials.p};
         const R a = (R)(1.0 / N), b2 = (R)(s2d * s2d * N), ds = (R)s2d;
-        double best_rate = -1;
-        int best_b = cs[0];
-        for (int b : cs) {
-            if (b > bmax) continue;
+        // time one slice step of each (batch, row variant, column variant)
+        auto rate_of = [&](int b, int row_v, int col_v) {
             auto step = [&] {
-                ops.row_step(st(), wave.p, b, trans.p, tw, a, xa, xb, 0, nullptr, 0);
-                ops.col_step(st(), wave.p, b, tw, pt, b2, ds, det, nullptr, COL_STEP, tiles_lo, tiles_hi);
+                ops.row_step(st(), wave.p, b, trans.p, tw, a, xa, xb, 0, nullptr, 0, row_v);
+                ops.col_step(st(), wave.p, b, tw, pt, b2, ds, det, nullptr, COL_STEP, tiles_lo, tiles_hi, col_v);
                 ctx->launches += 2;
             };
             step();   // warm-up
@@ -1458,13 +1521,27 @@ struct Sim : SimBase {
             MS_CUDA(cudaEventSynchronize(ev[1]));
             float ms = 0;
             MS_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
-            const double r_ = (double)b * reps / (ms * 1e-3);
-            if (r_ > best_rate) { best_rate = r_; best_b = b; }
+            return (double)b * reps / (ms * 1e-3);
+        };
+        double best_rate = -1;
+        int best_b = cs[0], best_v = 0, best_rv = 0;
+        for (int variant = 0; variant < ops.col_variants; variant++)   // batch and column kernel
+            for (int b : cs) {
+                if (b > bmax) continue;
+                const double r_ = rate_of(b, 0, variant);
+                if (r_ > best_rate) { best_rate = r_; best_b = b; best_v = variant; }
+            }
+        for (int rv = 1; rv < ops.row_variants; rv++) {   // then the row pass's prefetch at that pair
+            const double r_ = rate_of(best_b, rv, best_v);
+            if (r_ > best_rate) { best_rate = r_; best_rv = rv; }
         }
+        check_step_err();
         tuned_batch = best_b;
+        col_variant = best_v;
+        row_variant = best_rv;
         if (cands == nullptr) {   // only the default candidate set is shared through the cache
             std::lock_guard<std::mutex> lk(ctx->mtx);
-            tune_cache()[key] = {best_b, best_rate};
+            tune_cache()[key] = {best_b, best_rate, best_v, best_rv};
         }
         // release the scratch waves: runs allocate batches of the tuned size (batch_cap sets their size)
         MS_CUDA(cudaStreamSynchronize(st()));
@@ -1473,6 +1550,25 @@ struct Sim : SimBase {
         batch_cap = 0;
         if (best) *best = best_b;
         if (rate) *rate = best_rate;
+    }
+
+    void set_step_variant(int col, int row) override {
+        if (col < 0 || col >= ops.col_variants)
+            throw ArgError("column step variant " + std::to_string(col) + " out of range [0, " +
+                           std::to_string(ops.col_variants) + ")");
+        if (row < 0 || row >= ops.row_variants)
+            throw ArgError("row step variant " + std::to_string(row) + " out of range [0, " +
+                           std::to_string(ops.row_variants) + ")");
+        if (col != col_variant || row != row_variant) drop_graphs();   // captured batches hold the previous kernels
+        col_variant = col;
+        row_variant = row;
+    }
+    void get_tuning(int *batch, int *col, int *n_col, int *row, int *n_row) override {
+        if (batch) *batch = default_batch();
+        if (col) *col = col_variant;
+        if (n_col) *n_col = ops.col_variants;
+        if (row) *row = row_variant;
+        if (n_row) *n_row = ops.row_variants;
     }
 
     void set_c10_c30(double c10, double c30) override {
@@ -1514,7 +1610,7 @@ struct Sim : SimBase {
             ck_buf.ensure(ctx, (size_t)n_ck * NN);
             save.ensure(ctx, (size_t)(c == 1 ? S : c) * NN);
         }
-        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p};
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p, ctx->step_err, pxe.p, pye.p};
         DetArgs nodet{detmask.p, 0, partials.p};
         // forward: plane wave through every slice, checkpoints of the row-transformed state
         plane_wave_state<R>(st(), N, wave.p);
@@ -1522,10 +1618,10 @@ struct Sim : SimBase {
             if (want_grad && s % c == 0)
                 MS_CUDA(cudaMemcpyAsync(ck_buf.p + (size_t)(s / c) * NN, wave.p, NN * sizeof(C), cudaMemcpyDeviceToDevice, st()));
             if (want_grad && c == 1) ops.row_step_save(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, save.p + (size_t)s * NN);
-            else ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1, nullptr, 0);
+            else ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1, nullptr, 0, 0);
             bool last = s == S - 1;
             ops.col_step(st(), wave.p, 1, tw, pt, b, ds, nodet, last ? recip.p : nullptr, last ? COL_STEP_DET : COL_STEP,
-                         all_tiles, 0);
+                         all_tiles, 0, 0);
             ctx->launches += 2;
         }
         // image W = s2d Dinv(H Recip), loss, G_W = 4 (I - target) W
@@ -1572,20 +1668,20 @@ struct Sim : SimBase {
         // gT and gV of every slice of a segment, so that the band limit, gV and the atom gather run once per
         // segment over all its slices (batch-1 launches of those kernels leave most of the GPU idle)
         fw.ensure(ctx, NN); gT.ensure(ctx, (size_t)c * NN); gV.ensure(ctx, (size_t)c * NN);
-        PropTables<R> ptc{pxc.p, pyc.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p};
+        PropTables<R> ptc{pxc.p, pyc.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p, ctx->step_err, pxec.p, pyec.p};
         for (int k = n_ck - 1; k >= 0; k--) {
             const int s0 = k * c, s1 = std::min(s0 + c, S), m = s1 - s0;
             if (c > 1) {   // recompute psi_s of the segment from its checkpoint
                 MS_CUDA(cudaMemcpyAsync(fw.p, ck_buf.p + (size_t)k * NN, NN * sizeof(C), cudaMemcpyDeviceToDevice, st()));
                 for (int s = s0; s < s1; s++) {
                     ops.row_step_save(st(), fw.p, 1, trans.p + (size_t)s * NN, tw, a, save.p + (size_t)(s - s0) * NN);
-                    if (s < s1 - 1) ops.col_step(st(), fw.p, 1, tw, pt, b, ds, nodet, nullptr, COL_STEP, all_tiles, 0);
+                    if (s < s1 - 1) ops.col_step(st(), fw.p, 1, tw, pt, b, ds, nodet, nullptr, COL_STEP, all_tiles, 0, 0);
                     ctx->launches += s < s1 - 1 ? 2 : 1;
                 }
             }
             for (int s = s1 - 1; s >= s0; s--) {
                 check_cancel();
-                if (s < S - 1) ops.col_step(st(), wave.p, 1, tw, ptc, b, ds, nodet, nullptr, COL_STEP, all_tiles, 0);
+                if (s < S - 1) ops.col_step(st(), wave.p, 1, tw, ptc, b, ds, nodet, nullptr, COL_STEP, all_tiles, 0, 0);
                 const C *psi = save.p + (size_t)(c == 1 ? s : s - s0) * NN;
                 ops.row_adjoint(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, psi, gT.p + (size_t)(s - s0) * NN);
                 ctx->launches += s < S - 1 ? 2 : 1;
@@ -1725,6 +1821,8 @@ int mslice_ctx_create(int device, mslice_ctx **out) {
         auto c = std::make_unique<mslice_ctx>();
         c->impl.device = device;
         MS_CUDA(cudaStreamCreateWithFlags(&c->impl.stream, cudaStreamNonBlocking));
+        MS_CUDA(cudaMalloc(&c->impl.step_err, sizeof(int)));
+        MS_CUDA(cudaMemset(c->impl.step_err, 0, sizeof(int)));
         *out = c.release();
     });
 }
@@ -1931,6 +2029,22 @@ int mslice_tune_batch(mslice_sim *sim, const int *candidates, int n_candidates, 
         need(sim != nullptr, "sim is null");
         use_device(sim->ctx);
         sim->impl->tune_batch(candidates, candidates ? n_candidates : 1, reps, best_batch, waves_per_second);
+    });
+}
+
+int mslice_set_step_variant(mslice_sim *sim, int col_variant, int row_variant) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        use_device(sim->ctx);
+        sim->impl->set_step_variant(col_variant, row_variant);
+    });
+}
+
+int mslice_get_tuning(mslice_sim *sim, int *batch, int *col_variant, int *n_col_variants, int *row_variant,
+                      int *n_row_variants) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        sim->impl->get_tuning(batch, col_variant, n_col_variants, row_variant, n_row_variants);
     });
 }
 

@@ -69,17 +69,33 @@ template <class R, int SIGN> __device__ __forceinline__ void dft4(cplx<R> &a0, c
     a1 = cadd(A1, A3);
     a3 = csub(A1, A3);
 }
+// a sqrt(3)/2: FP32 as the FP32 value plus its remainder (as mul_rsqrt2 below), FP64 the FP64 value
+template <class R> __device__ __forceinline__ R mul_sqrt3_2(R a) {
+    if constexpr (sizeof(R) == 8) {
+        return a * (R)0.86602540378443864676;
+    } else {
+        return fmaf(a, 0.8660253882408142f, a * 1.5543625053737742e-08f);
+    }
+}
 template <class R, int SIGN> __device__ __forceinline__ void dft3(cplx<R> &a0, cplx<R> &a1, cplx<R> &a2) {
-    const R h = (R)0.86602540378443864676;   // sqrt(3)/2
     cplx<R> t1 = cadd(a1, a2), t2 = csub(a1, a2);
     cplx<R> m = mk<R>(a0.x - (R)0.5 * t1.x, a0.y - (R)0.5 * t1.y);
-    cplx<R> s = mul_i(cscale(t2, h), SIGN);
+    cplx<R> s = mul_i(mk<R>(mul_sqrt3_2<R>(t2.x), mul_sqrt3_2<R>(t2.y)), SIGN);
     a0 = cadd(a0, t1);
     a1 = cadd(m, s);
     a2 = csub(m, s);
 }
+// a / sqrt(2). FP32: times the FP32 value of 1/sqrt(2) plus its remainder, so the radix-8 twiddles keep
+// modulus 1 to second order (an FFT round trip multiplies by |w|^2, and a modulus error would repeat at every
+// slice and add up with thickness); FP64: times the FP64 value.
+template <class R> __device__ __forceinline__ R mul_rsqrt2(R a) {
+    if constexpr (sizeof(R) == 8) {
+        return a * (R)0.70710678118654752440;
+    } else {
+        return fmaf(a, 0.7071067690849304f, a * 1.2101617485882343e-08f);
+    }
+}
 template <class R, int SIGN> __device__ __forceinline__ void dft8(cplx<R> *a) {
-    const R q = (R)0.70710678118654752440;   // 1/sqrt(2)
     cplx<R> e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6];
     cplx<R> o0 = a[1], o1 = a[3], o2 = a[5], o3 = a[7];
     dft4<R, SIGN>(e0, e1, e2, e3);
@@ -87,11 +103,11 @@ template <class R, int SIGN> __device__ __forceinline__ void dft8(cplx<R> *a) {
     // W8^1 = (1 + SIGN i)/sqrt2, W8^2 = SIGN i, W8^3 = (-1 + SIGN i)/sqrt2
     cplx<R> w1o1, w2o2, w3o3;
     if (SIGN < 0) {
-        w1o1 = mk<R>((o1.x + o1.y) * q, (o1.y - o1.x) * q);
-        w3o3 = mk<R>((o3.y - o3.x) * q, (-o3.x - o3.y) * q);
+        w1o1 = mk<R>(mul_rsqrt2<R>(o1.x + o1.y), mul_rsqrt2<R>(o1.y - o1.x));
+        w3o3 = mk<R>(mul_rsqrt2<R>(o3.y - o3.x), mul_rsqrt2<R>(-o3.x - o3.y));
     } else {
-        w1o1 = mk<R>((o1.x - o1.y) * q, (o1.y + o1.x) * q);
-        w3o3 = mk<R>((-o3.x - o3.y) * q, (o3.x - o3.y) * q);
+        w1o1 = mk<R>(mul_rsqrt2<R>(o1.x - o1.y), mul_rsqrt2<R>(o1.y + o1.x));
+        w3o3 = mk<R>(mul_rsqrt2<R>(-o3.x - o3.y), mul_rsqrt2<R>(o3.x - o3.y));
     }
     w2o2 = mul_i(o2, SIGN);
     a[0] = cadd(e0, o0);

@@ -11,9 +11,9 @@
 
 namespace ms {
 
-template <int N, int SIGN, int S, class Addr>
+template <int N, int SIGN, int S, class Addr, class Sync>
 __device__ __forceinline__ void fftp_stages(float2 (&va)[Plan<N>::E], float2 (&vb)[Plan<N>::E], float4 *sm, Addr ad,
-                                            int t, const float2 *tw) {
+                                            int t, const float2 *tw, Sync sync) {
     using P = Plan<N>;
     constexpr int E = P::E, NT = P::NT;
     constexpr int RAD = P::radix(S);
@@ -64,7 +64,7 @@ __device__ __forceinline__ void fftp_stages(float2 (&va)[Plan<N>::E], float2 (&v
 #pragma unroll
         for (int i = 0; i < E; i++) { va[i] = oa[i]; vb[i] = ob[i]; }
     } else {
-        __syncthreads();
+        sync();
 #pragma unroll
         for (int b = 0; b < NB; b++) {
             const int j = t + b * NT;
@@ -74,15 +74,16 @@ __device__ __forceinline__ void fftp_stages(float2 (&va)[Plan<N>::E], float2 (&v
             for (int m = 0; m < RAD; m++)
                 sm[ad(idxD + m * Ns)] = make_float4(oa[b + m * NB].x, oa[b + m * NB].y, ob[b + m * NB].x, ob[b + m * NB].y);
         }
-        __syncthreads();
-        fftp_stages<N, SIGN, S + 1, Addr>(va, vb, sm, ad, t, tw);
+        sync();
+        fftp_stages<N, SIGN, S + 1, Addr, Sync>(va, vb, sm, ad, t, tw, sync);
     }
 }
 
-template <int N, int SIGN, class Addr>
+// sync: the barrier over the threads sharing sm (the whole block by default)
+template <int N, int SIGN, class Addr, class Sync = BlockSync>
 __device__ __forceinline__ void fft_pair(float2 (&va)[Plan<N>::E], float2 (&vb)[Plan<N>::E], float4 *sm, Addr ad, int t,
-                                         const float2 *tw) {
-    fftp_stages<N, SIGN, 0, Addr>(va, vb, sm, ad, t, tw);
+                                         const float2 *tw, Sync sync = Sync()) {
+    fftp_stages<N, SIGN, 0, Addr, Sync>(va, vb, sm, ad, t, tw, sync);
 }
 
 }  // namespace ms

@@ -46,10 +46,34 @@ __device__ __forceinline__ double cos_pi16(int phi) {
     phi &= 31;
     return phi <= 16 ? c16[phi] : c16[32 - phi];
 }
-// exp(SIGN 2 pi i e / M) for M = 16 or 32: the angle is j pi / 16 with j = (32 / M) e; sin(x) = cos(x - pi/2)
-template <class R, int SIGN, int M> __device__ __forceinline__ cplx<R> wconst(int e) {
+// FP32 values of cos(m pi / 16), m = 0..8, each (cos, sin) pair (c[m], c[8 - m]) picked among the roundings of
+// its two parts for the squared modulus closest to 1: an FFT round trip multiplies by |w|^2, and a modulus error
+// repeats at every slice. cos(pi/4) = 0.70710677 leaves 2 c^2 - 1 = -3.4e-8; kC4Lo carries its remainder.
+__device__ __forceinline__ float cos_pi16_f(int phi) {
+    constexpr float c16[9] = {1.0f, 0.9807852506637573f, 0.9238795638084412f, 0.8314695954322815f, 0.7071067690849304f,
+                              0.5555702447891235f, 0.3826833963394165f, 0.19509033858776093f, 0.0f};
+    phi &= 31;
+    const int m = phi <= 16 ? phi : 32 - phi;        // cos(phi pi/16) = cos((32 - phi) pi/16)
+    return m <= 8 ? c16[m] : -c16[16 - m];             // cos((16 - m) pi/16) = -cos(m pi/16)
+}
+constexpr float kC4Lo = 1.2101617485882343e-08f;      // cos(pi/4) - 0.70710677f
+
+// x times exp(SIGN 2 pi i e / M) for M = 16 or 32: the angle is j pi / 16 with j = (32 / M) e; sin(x) = cos(x - pi/2).
+// FP32: the constants above, and at odd multiples of pi/4 the remainder of cos(pi/4) is added, so those
+// twiddles are exact to second order.
+template <class R, int SIGN, int M> __device__ __forceinline__ cplx<R> cmul_wconst(cplx<R> x, int e) {
     const int j = (32 / M) * e;
-    return mk<R>((R)cos_pi16(j), (R)(SIGN * cos_pi16(j - 8)));
+    if constexpr (sizeof(R) == 8) {
+        return cmul(x, mk<R>((R)cos_pi16(j), (R)(SIGN * cos_pi16(j - 8))));
+    } else {
+        const cplx<R> w = mk<R>(cos_pi16_f(j), (R)SIGN * cos_pi16_f(j - 8));
+        cplx<R> r = cmul(x, w);
+        if ((j & 7) == 4) {   // both parts are +-cos(pi/4)
+            const cplx<R> wl = mk<R>(w.x > 0 ? kC4Lo : -kC4Lo, w.y > 0 ? kC4Lo : -kC4Lo);
+            r = cadd(r, cmul(x, wl));
+        }
+        return r;
+    }
 }
 
 // 16-point DFT in registers as 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2
@@ -60,9 +84,9 @@ template <class R, int SIGN> __device__ __forceinline__ void dft16(cplx<R> *a) {
         cplx<R> x0 = a[n2], x1 = a[n2 + 4], x2 = a[n2 + 8], x3 = a[n2 + 12];
         dft4<R, SIGN>(x0, x1, x2, x3);
         b[n2 * 4 + 0] = x0;
-        b[n2 * 4 + 1] = cmul(x1, wconst<R, SIGN, 16>(n2 * 1));
-        b[n2 * 4 + 2] = cmul(x2, wconst<R, SIGN, 16>(n2 * 2));
-        b[n2 * 4 + 3] = cmul(x3, wconst<R, SIGN, 16>(n2 * 3));
+        b[n2 * 4 + 1] = cmul_wconst<R, SIGN, 16>(x1, n2 * 1);
+        b[n2 * 4 + 2] = cmul_wconst<R, SIGN, 16>(x2, n2 * 2);
+        b[n2 * 4 + 3] = cmul_wconst<R, SIGN, 16>(x3, n2 * 3);
     }
 #pragma unroll
     for (int k1 = 0; k1 < 4; k1++) {
@@ -84,7 +108,7 @@ template <class R, int SIGN> __device__ __forceinline__ void dft32(cplx<R> *a) {
     dft16<R, SIGN>(o);
 #pragma unroll
     for (int k = 0; k < 16; k++) {
-        cplx<R> w = cmul(o[k], wconst<R, SIGN, 32>(k));
+        cplx<R> w = cmul_wconst<R, SIGN, 32>(o[k], k);
         a[k] = cadd(e[k], w);
         a[k + 16] = csub(e[k], w);
     }

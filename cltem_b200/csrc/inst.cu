@@ -53,18 +53,85 @@ bool pair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw, Pr
     }
 }
 
+// The persistent TMA-fed column passes of the FP32 power-of-two plans (passes_tma.cuh), by variant, where
+// their stages and tables fit in shared memory (256^2: both; 512^2: variant 1):
+//   1: the step's tile (PairStepCfg::COLS columns), 3 stages, one block per SM
+//   2: half that tile, 3 stages, two blocks per SM
+template <int V> struct TmaVariant;
+template <> struct TmaVariant<1> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS, 3, 1>; };
+template <> struct TmaVariant<2> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, 3, 2>; };
+template <class RR, int V> constexpr bool tma_col_ok() {
+    if constexpr (std::is_same<RR, float>::value && pair_columns<N>()) {
+        using TC = typename TmaVariant<V>::template Cfg<N>;
+        return TC::ok && TC::COLS % CC::COLS == 0;   // the tile covers whole engine tiles
+    } else {
+        return false;
+    }
+}
+template <class RR> constexpr int tma_col_variants() {
+    return tma_col_ok<RR, 1>() ? (tma_col_ok<RR, 2>() ? 3 : 2) : 1;
+}
+int g_sms[64] = {};
+int sm_count() {
+    int dev = 0;
+    MS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw std::runtime_error("device ordinal out of range");
+    if (!g_sms[dev]) MS_CUDA(cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev));
+    return g_sms[dev];
+}
+template <class RR, int V> void tma_col_attrs() {
+    if constexpr (tma_col_ok<RR, V>()) {
+        using TC = typename TmaVariant<V>::template Cfg<N>;
+        set_smem(k_col_step_tma<N, TC::COLS, TC::STAGES, TC::MINB>, TC::smem());
+    }
+}
+template <class RR, int V>
+bool tma_col_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw, PropTables<RR> pt, RR b, int tiles_lo,
+                  int tiles_hi) {
+    if constexpr (tma_col_ok<RR, V>()) {
+        using TC = typename TmaVariant<V>::template Cfg<N>;
+        if (!pt.err) throw std::runtime_error("persistent column pass without an error word");
+        constexpr int k = TC::COLS / CC::COLS, total = N / TC::COLS;
+        static_assert(TC::COLS % CC::COLS == 0, "the step's tile must cover whole engine tiles");
+        int lo = (tiles_lo + k - 1) / k, hi = (tiles_hi + k - 1) / k;
+        if (lo + hi > total) { lo = total; hi = 0; }
+        const long long items = (long long)(lo + hi) * batch;
+        if (items > 0x7fffffffLL || (long long)batch * N > 0x7fffffffLL) throw std::runtime_error("batch too large");
+        const CUtensorMap tm = wave_tensor_map(wave, 2ull * N, (unsigned long long)batch * N, TC::BOX_FLOATS, TC::BOX_ROWS);
+        const int grid = (int)std::min<long long>(items, (long long)TC::MINB * sm_count());
+        k_col_step_tma<N, TC::COLS, TC::STAGES, TC::MINB><<<grid, TC::THREADS, TC::smem(), s>>>(
+            tm, wave, tw, pt, b, lo, lo + hi, (int)items, pt.err);
+        MS_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        return false;
+    }
+}
+
 // the two-row step kernel of the FP32 non-wide row plans
 template <class RR> void rowpair_attrs() {
     if constexpr (std::is_same<RR, float>::value && pair_rows<N>())
         set_smem(k_row_step_pair<N, rowpair_pairs<N>()>, RowPairStepCfg<N>::smem());
 }
+// blocks of kernel k (block size threads, dynamic smem bytes) resident on the whole device
+template <class K> int resident_blocks(K k, int threads, size_t smem) {
+    int per_sm = 0;
+    MS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem));
+    return std::max(1, per_sm) * sm_count();
+}
 template <class RR>
 bool rowpair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans, const cplx<RR> *tw, RR a, int xa,
-                  int xb, int load_all, const int *tsel, size_t tstride) {
+                  int xb, int load_all, const int *tsel, size_t tstride, int variant) {
     if constexpr (std::is_same<RR, float>::value && pair_rows<N>()) {
         constexpr int PR = rowpair_pairs<N>();
+        static int res[64] = {};
+        int dev = 0;
+        MS_CUDA(cudaGetDevice(&dev));
+        if (variant > 0 && !res[dev])
+            res[dev] = resident_blocks(k_row_step_pair<N, PR>, Plan<N>::NT * PR, RowPairStepCfg<N>::smem());
+        const int pf = variant > 0 ? variant * res[dev] : 0;
         k_row_step_pair<N, PR><<<dim3(N / (2 * PR), batch), dim3(Plan<N>::NT, PR), RowPairStepCfg<N>::smem(), s>>>(
-            wave, trans, tw, a, xa, xb, load_all, tsel, tstride);
+            wave, trans, tw, a, xa, xb, load_all, tsel, tstride, pf);
         MS_CUDA(cudaGetLastError());
         return true;
     } else {
@@ -84,6 +151,8 @@ void ensure_attrs() {
     set_smem(k_row_fft<R, N, +1>, RC::smem());
     set_smem(k_col_step<R, N, COL_STEP>, CC::smem());
     pair_attrs<R>();
+    tma_col_attrs<R, 1>();
+    tma_col_attrs<R, 2>();
     rowpair_attrs<R>();
     set_smem(k_col_step<R, N, COL_STEP_DET>, CC::smem());
     set_smem(k_col_step<R, N, COL_DET_ONLY>, CC::smem());
@@ -102,10 +171,10 @@ inline dim3 row_block() { return dim3(RC::P::NT, RC::ROWS); }
 // the FP64 row step built for 3 blocks per SM where that is set (fp64_step_minb)
 template <class RR>
 bool row_step_d(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans, const cplx<RR> *tw, RR a, int xa,
-                int xb, int load_all, const int *tsel, size_t tstride) {
+                int xb, int load_all, const int *tsel, size_t tstride, int pf) {
     if constexpr (std::is_same<RR, double>::value && fp64_row_bounded<N>()) {
         k_row_step_d<N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all, tsel,
-                                                                       tstride);
+                                                                       tstride, pf);
         MS_CUDA(cudaGetLastError());
         return true;
     } else {
@@ -116,11 +185,18 @@ inline dim3 col_grid(int batch) { return dim3(N / CC::COLS, batch); }
 inline dim3 col_block() { return dim3(CC::COLS, CC::P::NT); }
 
 void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a, int xa, int xb,
-              int load_all, const int *tsel, size_t tstride) {
+              int load_all, const int *tsel, size_t tstride, int variant) {
     ensure_attrs();
-    if (rowpair_step<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride)) return;
-    if (row_step_d<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride)) return;
-    k_row_step<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all, tsel, tstride);
+    if (variant < 0 || variant > 2) throw std::runtime_error("row pass variant out of range");
+    if (rowpair_step<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride, variant)) return;
+    static int res[64] = {};
+    int dev = 0;
+    MS_CUDA(cudaGetDevice(&dev));
+    if (variant > 0 && !res[dev]) res[dev] = resident_blocks(k_row_step<R, N>, RC::THREADS, RC::smem());
+    const int pf = variant > 0 ? variant * res[dev] : 0;
+    if (row_step_d<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride, pf)) return;
+    k_row_step<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all, tsel, tstride,
+                                                                   pf);
     MS_CUDA(cudaGetLastError());
 }
 void row_fft(cudaStream_t s, const cplx<R> *in, cplx<R> *out, int batch, const cplx<R> *tw, R scale, int sign) {
@@ -130,13 +206,17 @@ void row_fft(cudaStream_t s, const cplx<R> *in, cplx<R> *out, int batch, const c
     MS_CUDA(cudaGetLastError());
 }
 void col_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, PropTables<R> pt, R b, R ds, DetArgs det,
-              cplx<R> *recip, int mode, int tiles_lo, int tiles_hi) {
+              cplx<R> *recip, int mode, int tiles_lo, int tiles_hi, int variant) {
     ensure_attrs();
     if (tiles_lo < 0 || tiles_hi < 0 || tiles_lo + tiles_hi > N / CC::COLS || tiles_lo + tiles_hi == 0)
         throw std::runtime_error("column tile range out of bounds");
+    if (variant < 0 || variant >= tma_col_variants<R>()) throw std::runtime_error("column pass variant out of range");
     dim3 g(tiles_lo + tiles_hi, batch);
-    if (mode == COL_STEP && recip == nullptr && pt.ycut && pair_step<R>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi))
-        return;
+    if (mode == COL_STEP && recip == nullptr && pt.ycut) {
+        if (variant == 1 && tma_col_step<R, 1>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (variant == 2 && tma_col_step<R, 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (pair_step<R>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+    }
     if (mode == COL_STEP && recip == nullptr)
         k_col_step<R, N, COL_STEP><<<g, col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip, tiles_lo);
     else if (mode == COL_DET_ONLY)
@@ -183,6 +263,7 @@ PassOps<MS_REAL> make_pass_ops<MS_REAL, MS_N>() {
     o.n = N;
     o.col_blocks = N / CC::COLS;
     o.cols_per_tile = CC::COLS;
+    o.col_variants = tma_col_variants<R>();
     o.row_step = row_step;
     o.row_fft = row_fft;
     o.col_step = col_step;

@@ -3,6 +3,7 @@
 
 #include "adjoint.cuh"
 #include "passes.cuh"
+#include "passes_tma.cuh"
 
 namespace ms {
 
@@ -12,12 +13,18 @@ struct PassOps {
     int col_blocks = 0;   // blocks per wave of a column pass (number of detector partials per wave)
     // row_step(..., xa, xb, load_all, tsel, tstride): active columns x < xa or x >= xb; tsel (or nullptr) the
     // transmission set of each wave, sets tstride elements apart (see k_row_step)
+    // ..., variant): 0 plain; 1, 2 each block also prefetches into L2 the rows of the block one (two) residencies
+    // of the grid later (row_variants of them)
     void (*row_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R, int, int, int, const int *,
-                     size_t) = nullptr;
+                     size_t, int) = nullptr;
+    int row_variants = 3;
     void (*row_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
-    // col_step(..., mode, tiles_lo, tiles_hi): the leading tiles_lo and trailing tiles_hi column tiles
+    // col_step(..., mode, tiles_lo, tiles_hi, variant): the leading tiles_lo and trailing tiles_hi column tiles;
+    // variant picks the kernel of the plain step (COL_STEP without a reciprocal copy), 0 <= variant <
+    // col_variants: 0 the one-launch-per-tile kernels, 1.. the persistent TMA-fed column passes
     void (*col_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, PropTables<R>, R, R, DetArgs, cplx<R> *, int, int,
-                     int) = nullptr;
+                     int, int) = nullptr;
+    int col_variants = 1;
     int cols_per_tile = 0;
     void (*col_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
     void (*col_bandlimit)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const double *, const double *, double, R) = nullptr;

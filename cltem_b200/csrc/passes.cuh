@@ -31,7 +31,28 @@ struct PropTables {
     const double *ky2;   // res: ky*ky
     double kmax2;        // (k_max * limit_factor)^2 of the propagator's strict cut (propagator_d.cl:34-36)
     const int2 *ycut;    // res: column x keeps rows y < ycut[x].x and y >= ycut[x].y, the same cut tabulated
+    int *err = nullptr;  // error word of the persistent passes (passes_tma.cuh), or nullptr
+    // FP32: the relative representation errors of px and py, (p64 - p32) / p32 formed in FP64 and rounded
+    const cplx<R> *pxe = nullptr;
+    const cplx<R> *pye = nullptr;
 };
+
+// v times the propagator factor px * py of its k (inside the strict cut; the caller zeroes the rest).
+// FP64: v (px py), the reference's product. FP32: a factor rounded to FP32 carries a representation error
+// that is the same at every slice, so it would add up linearly with thickness (tens of slices reach the
+// 1e-5 tolerance). Here v is multiplied by px and then by py, whose roundings depend on v and do not repeat,
+// and the product is then corrected by (1 + ex + ey), the relative errors of the FP32 factors against
+// their FP64 values: the factor applied matches the FP64 propagator to second order in those errors.
+template <class R>
+__device__ __forceinline__ cplx<R> prop_mul(cplx<R> v, cplx<R> px, cplx<R> py, cplx<R> ex, cplx<R> ey) {
+    if constexpr (sizeof(R) == 8) {
+        (void)ex; (void)ey;
+        return cmul(v, cmul(px, py));
+    } else {
+        const cplx<R> u = cmul(cmul(v, px), py);
+        return cadd(u, cmul(u, cadd(ex, ey)));
+    }
+}
 
 struct DetArgs {
     const uint16_t *mask;   // res*res bit masks of the detectors, unshifted k-space pixel order
@@ -125,6 +146,33 @@ __device__ __forceinline__ const cplx<R> *twiddles_for(cplx<R> *tws, const cplx<
     }
 }
 
+// L2 prefetch of [p, p + bytes) by the copy engine (cp.async.bulk.prefetch; a hint, no data returned):
+// the part aligned to 16 bytes at both ends
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
+    const uintptr_t a = (reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15);
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + bytes) & ~uintptr_t(15);
+    if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
+}
+// Row passes with pf > 0: the block with linear index L asks the copy engine to bring the rows that block
+// L + pf reads (its wave rows' active columns) into L2, so that a block launched a residency later finds
+// them there rather than in HBM. rows: the rows this thread prefetches for (first row y0, count n).
+template <class C>
+__device__ __forceinline__ void prefetch_rows(const C *wave, int N, int rows_per_block, int pf, int xa, int xb,
+                                             int load_all) {
+    const long long L = (long long)blockIdx.x + (long long)blockIdx.y * gridDim.x + pf;
+    if (L >= (long long)gridDim.x * gridDim.y) return;
+    const int bx = (int)(L % gridDim.x), by = (int)(L / gridDim.x);
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    if (tid >= rows_per_block) return;
+    const C *r = wave + (size_t)by * N * N + ((size_t)bx * rows_per_block + tid) * N;
+    if (load_all) {
+        prefetch_l2(r, (size_t)N * sizeof(C));
+    } else {
+        if (xa > 0) prefetch_l2(r, (size_t)xa * sizeof(C));
+        if (xb < N) prefetch_l2(r + xb, (size_t)(N - xb) * sizeof(C));
+    }
+}
+
 // ------------------------------------------------------------------------------------------------
 // Row kernels: grid (res/ROWS, batch), block (NT, ROWS)
 // ------------------------------------------------------------------------------------------------
@@ -146,10 +194,11 @@ template <class R, int N, int THREADS, int OTHER> constexpr int fp64_step_minb()
 template <class R, int N>
 __device__ __forceinline__ void row_step_body(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans,
                                               const cplx<R> *__restrict__ twg, R a, int xa, int xb, int load_all,
-                                              const int *__restrict__ tsel, size_t tstride) {
+                                              const int *__restrict__ tsel, size_t tstride, int pf) {
     using RC = RowCfg<N, R>;
     using P = typename RC::P;
     constexpr int ROWS = RC::ROWS;
+    if (pf > 0) prefetch_rows(wave, N, ROWS, pf, xa, xb, load_all);
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tws = reinterpret_cast<cplx<R> *>(smraw);
     cplx<R> *sm = tws + RC::TWS + threadIdx.y * RC::ROWSZ;
@@ -183,8 +232,8 @@ __device__ __forceinline__ void row_step_body(cplx<R> *__restrict__ wave, const 
 template <class R, int N>
 __global__ void __launch_bounds__(RowCfg<N, R>::THREADS)
 k_row_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans, const cplx<R> *__restrict__ twg, R a,
-           int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride) {
-    row_step_body<R, N>(wave, trans, twg, a, xa, xb, load_all, tsel, tstride);
+           int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride, int pf) {
+    row_step_body<R, N>(wave, trans, twg, a, xa, xb, load_all, tsel, tstride, pf);
 }
 template <int N> constexpr bool fp64_row_bounded() {
     return fp64_step_minb<double, N, RowCfg<N, double>::THREADS, 1>() > 1;
@@ -192,8 +241,8 @@ template <int N> constexpr bool fp64_row_bounded() {
 template <int N>
 __global__ void __launch_bounds__(RowCfg<N, double>::THREADS, fp64_step_minb<double, N, RowCfg<N, double>::THREADS, 1>())
 k_row_step_d(double2 *__restrict__ wave, const double2 *__restrict__ trans, const double2 *__restrict__ twg, double a,
-             int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride) {
-    row_step_body<double, N>(wave, trans, twg, a, xa, xb, load_all, tsel, tstride);
+             int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride, int pf) {
+    row_step_body<double, N>(wave, trans, twg, a, xa, xb, load_all, tsel, tstride, pf);
 }
 
 // The row step of the FP32 radix-8 / 3·2^k row plans (sizes without the wide plan) with each thread carrying
@@ -226,10 +275,11 @@ template <int N, int PAIRS = rowpair_base<N>()> constexpr int rowpair_minb() {
 template <int N, int PAIRS_>
 __global__ void __launch_bounds__(RowPairCfg<N, PAIRS_>::THREADS, rowpair_minb<N, PAIRS_>())
 k_row_step_pair(float2 *__restrict__ wave, const float2 *__restrict__ trans, const float2 *__restrict__ twg, float a,
-                int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride) {
+                int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride, int pf) {
     using PC = RowPairCfg<N, PAIRS_>;
     using P = typename PC::P;
     constexpr int E = P::E, NT = P::NT;
+    if (pf > 0) prefetch_rows(wave, N, 2 * PC::PAIRS, pf, xa, xb, load_all);
     extern __shared__ __align__(16) unsigned char smraw[];
     float2 *tw = reinterpret_cast<float2 *>(smraw);
     float4 *sm = reinterpret_cast<float4 *>(tw + N) + (size_t)threadIdx.y * N;
@@ -344,12 +394,14 @@ k_col_step(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ twg, PropTabl
     __syncthreads();
     col_transform<R, N, -1>(v, sm, t, tw);
     const cplx<R> pxx = pt.px[x];
+    const cplx<R> exx = sizeof(R) == 4 ? pt.pxe[x] : mk<R>(0, 0);
     const double kx2 = pt.kx2[x];
 #pragma unroll
     for (int m = 0; m < P::E; m++) {
         const int y = t + m * P::NT;
-        cplx<R> p = (kx2 + pt.ky2[y] < pt.kmax2) ? cmul(pxx, pt.py[y]) : mk<R>(0, 0);
-        v[m] = cmul(v[m], p);
+        v[m] = (kx2 + pt.ky2[y] < pt.kmax2)
+                   ? prop_mul<R>(v[m], pxx, pt.py[y], exx, sizeof(R) == 4 ? pt.pye[y] : mk<R>(0, 0))
+                   : mk<R>(0, 0);
     }
     if constexpr (MODE == COL_STEP_DET || MODE == COL_DET_ONLY) {
         if (det.n_det > 0) {
@@ -416,6 +468,23 @@ template <int N> constexpr bool pair_loose() { return N == 256 || N == 384; }
 template <int N> using PairStepCfg = PairCfg<N, pair_mult<N>() * ColCfg<N, float>::COLS, pair_loose<N>()>;
 template <int N> constexpr bool pair_columns() { return PairStepCfg<N>::ok; }
 
+// The propagator and scale b on the two columns x, x + 1 a thread holds (elements t + m NT), zero outside the
+// cut (the row band of PropTables::ycut): shared by the two-column step kernels.
+template <int N>
+__device__ __forceinline__ void prop_pair(float2 (&va)[Plan<N>::E], float2 (&vb)[Plan<N>::E], const PropTables<float> &pt,
+                                          int x, int t, float bscale) {
+    constexpr int E = Plan<N>::E, NT = Plan<N>::NT;
+    const float2 pxa = pt.px[x], pxb = pt.px[x + 1], exa = pt.pxe[x], exb = pt.pxe[x + 1];
+    const int2 ca = pt.ycut[x], cb = pt.ycut[x + 1];
+#pragma unroll
+    for (int m = 0; m < E; m++) {
+        const int y = t + m * NT;
+        const float2 py = pt.py[y], ey = pt.pye[y];
+        va[m] = (y < ca.x || y >= ca.y) ? cscale(prop_mul<float>(va[m], pxa, py, exa, ey), bscale) : mk<float>(0, 0);
+        vb[m] = (y < cb.x || y >= cb.y) ? cscale(prop_mul<float>(vb[m], pxb, py, exb, ey), bscale) : mk<float>(0, 0);
+    }
+}
+
 template <int N, int COLS, bool LOOSE>
 __global__ void __launch_bounds__(PairCfg<N, COLS, LOOSE>::THREADS, PairCfg<N, COLS, LOOSE>::MINB)
 k_col_step_pair(float2 *__restrict__ wave, const float2 *__restrict__ twg, PropTables<float> pt, float bscale,
@@ -440,17 +509,7 @@ k_col_step_pair(float2 *__restrict__ wave, const float2 *__restrict__ twg, PropT
     }
     __syncthreads();
     fft_pair<N, -1>(va, vb, sm, ColAddr<PAIRS, 16>(), t, tw);
-    const float2 pxa = pt.px[x], pxb = pt.px[x + 1];
-    const int2 ca = pt.ycut[x], cb = pt.ycut[x + 1];
-#pragma unroll
-    for (int m = 0; m < E; m++) {
-        const int y = t + m * NT;
-        const float2 py = pt.py[y];
-        const float2 pa = (y < ca.x || y >= ca.y) ? cmul(pxa, py) : mk<float>(0, 0);
-        const float2 pb = (y < cb.x || y >= cb.y) ? cmul(pxb, py) : mk<float>(0, 0);
-        va[m] = cscale(cmul(va[m], pa), bscale);
-        vb[m] = cscale(cmul(vb[m], pb), bscale);
-    }
+    prop_pair<N>(va, vb, pt, x, t, bscale);
     fft_pair<N, +1>(va, vb, sm, ColAddr<PAIRS, 16>(), t, tw);
 #pragma unroll
     for (int m = 0; m < E; m++)

@@ -82,6 +82,8 @@ def load_library(path=None):
         "mslice_profile_read": [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_ulonglong), _dp, C.c_int],
         "mslice_incoherence_draws": [C.POINTER(abi.Config), C.c_int, _ip, C.c_size_t, _dp, _ip, C.c_int, C.c_int, _dp],
         "mslice_tune_batch": [C.c_void_p, _ip, C.c_int, C.c_int, _ip, _dp],
+        "mslice_set_step_variant": [C.c_void_p, C.c_int, C.c_int],
+        "mslice_get_tuning": [C.c_void_p, _ip, _ip, _ip, _ip, _ip],
         "mslice_set_ccd": [C.c_void_p, _dp, _dp, C.c_size_t, C.c_int, C.c_double],
     }
     for name, args in sig.items():
@@ -379,6 +381,22 @@ class Simulation:
             c = np.ascontiguousarray(candidates, dtype=np.int32)
             _check(self.lib.mslice_tune_batch(self.h, _i(c), len(c), int(reps), C.byref(best), C.byref(rate)))
         return best.value, rate.value
+
+    def set_step_variant(self, col_variant, row_variant=None):
+        """Kernels of the batched STEM step (mslice_set_step_variant): column 0 one block per tile, 1 / 2 the
+        persistent TMA-fed passes; row 0 plain, 1 / 2 with an L2 prefetch one / two grid residencies ahead. The
+        row variant is kept when not given."""
+        if row_variant is None:
+            row_variant = self.tuning()["row_variant"]
+        _check(self.lib.mslice_set_step_variant(self.h, int(col_variant), int(row_variant)))
+
+    def tuning(self):
+        """{"batch", "col_variant", "col_variants", "row_variant", "row_variants"} the next STEM run uses
+        (mslice_get_tuning)."""
+        b, v, n, rv, rn = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(self.lib.mslice_get_tuning(self.h, C.byref(b), C.byref(v), C.byref(n), C.byref(rv), C.byref(rn)))
+        return {"batch": b.value, "col_variant": v.value, "col_variants": n.value, "row_variant": rv.value,
+                "row_variants": rn.value}
 
     KERNELS = ("row_step", "col_step", "potential", "bandlimit", "probe")
 

@@ -278,14 +278,27 @@ int mslice_stem_simulate(mslice_sim *sim, int n_configs, const size_t *counts, c
 int mslice_incoherence_draws(const mslice_config *cfg, int pass, const int *pixels, size_t n_pixels, double *defocus,
                              int *sets, int n_slices, int n_builds, double *shift);
 
-/* Autotuner of the probe batch (no counterpart in the reference, which propagates `parallel pixels`
- * probes one at a time): times `reps` slice steps (one fused row and one fused column pass) at each
- * candidate batch size on zeroed scratch waves and makes the fastest the simulation's default batch
- * (used when cfg.probe_batch is 0). candidates = NULL tries 64..2048 and reuses a result cached for
- * this device, grid and precision in the process. Candidates whose waves would take more than a quarter
- * of the free device memory are skipped. best_batch / waves_per_second may be NULL. */
+/* Autotuner of the probe batch and of the column step's kernel (no counterpart in the reference, which
+ * propagates `parallel pixels` probes one at a time): times `reps` slice steps (one fused row and one
+ * fused column pass) for each candidate batch size and each column-pass variant (see
+ * mslice_set_step_variant) on zeroed scratch waves and makes the fastest pair the simulation's default
+ * (the batch is used when cfg.probe_batch is 0). candidates = NULL tries 64..2048 and reuses a result
+ * cached for this device, grid and precision in the process. Candidates whose waves would take more than
+ * a quarter of the free device memory are skipped. best_batch / waves_per_second may be NULL. */
 int mslice_tune_batch(mslice_sim *sim, const int *candidates, int n_candidates, int reps, int *best_batch,
                       double *waves_per_second);
+/* The kernels of the batched STEM step (no counterpart in the reference). Column step: 0 = one block per
+ * column tile and wave; 1, 2 (FP32 power-of-two grids where their shared memory fits) = persistent passes,
+ * one or two blocks per SM, whose producer warp streams tiles into a ring of shared-memory stages with TMA
+ * (1: the step's tile, 3 stages; 2: half that tile, two blocks per SM). Row step: 0 = plain; 1, 2 = each
+ * block also asks the copy engine to prefetch into L2 the rows that the blocks one or two residencies of the
+ * grid later will read. All variants give bit-identical results. Out-of-range values fail with
+ * MSLICE_ERR_ARG. */
+int mslice_set_step_variant(mslice_sim *sim, int col_variant, int row_variant);
+/* The batch the next STEM run uses, the column- and row-step variants and their counts for this grid and
+ * precision (any pointer may be NULL). */
+int mslice_get_tuning(mslice_sim *sim, int *batch, int *col_variant, int *n_col_variants, int *row_variant,
+                      int *n_row_variants);
 
 /* ---- comparison paths and building blocks ---------------------------------------------------- */
 /* Plain per-probe STEM in the reference's unfused kernel order (simulationgeneral.cpp:736-768):

@@ -40,3 +40,45 @@ def test_tune_batch_default_candidates_are_cached(gpu_ctx, kirkland):
     assert (b1, r1) == (b2, r2) and b1 in (64, 128, 256, 512, 1024, 2048)
     with pytest.raises(MsliceError):
         a.tune_batch([0, 4])
+
+
+@pytest.mark.parametrize("res", [256, 512, 1024])
+def test_column_step_variants_are_bit_identical(gpu_ctx, kirkland, res):
+    """The persistent TMA-fed column passes (variants 1, 2) do the one-launch-per-tile kernel's arithmetic in
+    the same order: identical detector values over a batch large enough that every block loops over many
+    (wave, tile) items and reuses each shared-memory stage many times."""
+    gpu_ctx.load_params(kirkland)
+    s, st = small_stem(double_precision=False, res=res, n=(3, 3, 3), scan=12)
+    s.cfg.probe_batch = 144
+    conf = phonons(st, 1)[0]
+    sim = Simulation(gpu_ctx, s.cfg)
+    sim.set_atoms(conf)
+    t = sim.tuning()
+    nv = t["col_variants"]
+    assert t["row_variants"] == 3
+    assert nv >= (2 if res <= 512 else 1)   # the persistent passes where their stages and tables fit
+    pix = np.arange(144, dtype=np.int32)
+    out = []
+    for v in range(nv):
+        for rv in range(3):   # the row pass with and without its L2 prefetch
+            sim.set_step_variant(v, rv)
+            assert sim.tuning()["col_variant"] == v and sim.tuning()["row_variant"] == rv
+            out.append(sim.stem(pix))
+            out.append(sim.stem(pix))   # a second run replays the batch's CUDA graph
+    for r in out[1:]:
+        assert np.array_equal(r, out[0])
+    with pytest.raises(MsliceError):
+        sim.set_step_variant(nv, 0)
+    with pytest.raises(MsliceError):
+        sim.set_step_variant(0, 3)
+    sim.close()
+
+
+def test_tuner_reports_its_column_variant(gpu_ctx, kirkland):
+    gpu_ctx.load_params(kirkland)
+    s, st = small_stem(double_precision=False, res=512, scan=2)
+    sim = Simulation(gpu_ctx, s.cfg)
+    best, rate = sim.tune_batch([64, 256], reps=2)
+    t = sim.tuning()
+    assert t["batch"] == best and 0 <= t["col_variant"] < t["col_variants"] and 0 <= t["row_variant"] < t["row_variants"]
+    sim.close()
