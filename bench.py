@@ -39,9 +39,10 @@ METRIC = "STEM probe·slices/s at 512² FP32 vs plain FP64 GPU; adjoint/forward 
 UNIT = "probe·slices/s"
 WORKLOAD = "stem_adf_perovskite_10x10x20_512x512_64x64probes_40slices_phonon_u0.08"
 # DRAM bytes per wave of one launch of each step kernel at 512^2 FP32 (ncu dram__bytes_read.sum +
-# dram__bytes_write.sum over one launch, divided by its waves), measured on this build's kernels; a kernel
-# change needs a new capture
-NCU_DRAM_BYTES_PER_WAVE = {"row_step": 856.5e6 / 256, "col_step": 679.5e6 / 256}
+# dram__bytes_write.sum over one launch of the timed configuration, divided by its waves), measured at this
+# workload's autotuned batch of 2048 waves on this build's kernels (row pass with its L2 prefetch, persistent
+# TMA-fed column pass); a kernel change needs a new capture
+NCU_DRAM_BYTES_PER_WAVE = {"row_step": (2956389120 + 2893711616) / 2048, "col_step": (3087454464 + 2890425600) / 2048}
 
 
 def parse():
@@ -140,9 +141,10 @@ class ClockSampler:
 # CPU legs (oracle): the baseline beside our line, and the whole reference arm
 # ---------------------------------------------------------------------------------------------------
 def cpu_sample(n_probes, double_precision, seed=0):
-    """Time the CPU restatement on a bounded sample of one configuration of the workload: the
-    transmission build of all 40 slices plus n_probes probes through all slices; return the implied
-    probe·slices/s for a full 4096-probe configuration."""
+    """Time the CPU restatement on a bounded sample of one configuration of the workload: the transmission
+    build of all 40 slices, then n_probes probes through all slices (OpenMP over the probes). Both parts are
+    measured; `value` combines them into the rate of a whole 4096-probe configuration (one build, 4096 probes),
+    the unit the GPU arm's step is quoted in, and `sample_rate` is the sample's own probe·slices per second."""
     from oracle import bind as ob
     from cltem_b200.params import load_default
     from cltem_b200.structure import phonon_configs
@@ -159,8 +161,47 @@ def cpu_sample(n_probes, double_precision, seed=0):
     osim.stem(pix)
     t2 = time.perf_counter()
     S = osim.geo.n_slices
-    full = npx * S / ((t1 - t0) + (t2 - t1) * npx / n_probes)
-    return full, {"build_s": t1 - t0, "propagate_s": t2 - t1, "probes": n_probes, "slices": S, "configs": 1}
+    per_probe = (t2 - t1) / n_probes
+    return {"value": npx * S / ((t1 - t0) + per_probe * npx), "sample_rate": n_probes * S / (t2 - t0),
+            "build_s": t1 - t0, "propagate_s": t2 - t1, "per_probe_s": per_probe, "sample_s": t2 - t0,
+            "probes": n_probes, "slices": S, "configs": 1}
+
+
+def ref_kernel_leg(seed=0):
+    """The reference's own compiled double-precision kernels (oracle/_ref/libref.so, its kernels/*_d.cl built
+    for the CPU) beside the restatement, on one slice of the workload's projected potential (the one kernel of
+    the path that is not an FFT): seconds per slice for each. The reference kernel runs each 16x16 work group
+    as a team of 256 threads, one group after another, as its OpenCL CPU device would; the restatement uses
+    OpenMP over pixels. None where the reference kernels were not built."""
+    from oracle import bind as ob
+    from oracle import ref_bind as rb
+    if not rb.available():
+        return None
+    from cltem_b200.params import load_default
+    from cltem_b200.structure import phonon_configs
+    s, st = workload(double_precision=True)
+    p = load_default("kirkland")
+    conf = phonon_configs(st, 1, 0.08, seed=1000 + seed)[0]
+    o = ob.OracleSim(s.cfg, p, double_precision=True)
+    o.set_atoms(conf)
+    g = o.geo
+    a = o.sorted_atoms(len(conf))
+    k = g.n_slices // 2
+    ia = np.array([p.form, p.i_per_atom, s.cfg.resolution, s.cfg.resolution, k, g.n_slices, g.blocks_x, g.blocks_y,
+                   g.load_blocks_x, g.load_blocks_y, g.load_blocks_z, s.cfg.full3d_integrals], np.int32)
+    da = np.array([g.dz, g.real_scale, g.full_x[1], g.full_x[0], g.full_y[1], g.full_y[0], g.sigma, g.sim_x[0],
+                   g.sim_y[0], s.cfg.beam_tilt, s.cfg.beam_azimuth], np.float64)
+    out = np.zeros(2 * s.cfg.resolution ** 2)
+    vals = np.ascontiguousarray(p.values)
+    t0 = time.perf_counter()
+    rb.lib().ref_transmission_projected_d(rb.d(out), rb.d(a["x"]), rb.d(a["y"]), rb.d(a["z"]), rb.i(a["Z"]), rb.d(vals),
+                                          rb.i(ia), rb.d(da), rb.i(a["block_start"]))
+    t1 = time.perf_counter()
+    mine = o.transmission(k, band_limited=False)   # the oracle's own potential of the same slice
+    t2 = time.perf_counter()
+    same = bool(np.array_equal(rb.cplx(out, mine.shape), mine))
+    return {"kernel": "transmission_potentials_projected_d, one 512x512 slice of the workload", "reference_s": t1 - t0,
+            "restatement_s": t2 - t1, "identical_output": same}
 
 
 def cufft_leg(batch=512, steps=20, warmup=3, n=512):
@@ -201,13 +242,15 @@ def cufft_leg(batch=512, steps=20, warmup=3, n=512):
 def cpu_baseline_leg(n_probes):
     from oracle import bind as ob
     threads = ob.num_threads()
-    v, info = cpu_sample(n_probes, double_precision=False)
-    return {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": (f"CPU oracle (C++/OpenMP restatement of the reference path, FP32 instantiation) on one "
-                       f"phonon configuration: transmission build of {info['slices']} slices "
-                       f"({info['build_s']:.1f} s) + {n_probes} of 4096 probes through all slices "
-                       f"({info['propagate_s']:.1f} s), scaled to a 4096-probe configuration"),
-            "threads": threads}
+    r = cpu_sample(n_probes, double_precision=False)
+    return {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"CPU oracle (C++/OpenMP restatement of the reference path, FP32 instantiation) on one phonon "
+                       f"configuration: transmission build of {r['slices']} slices ({r['build_s']:.2f} s, measured) + "
+                       f"{n_probes} of 4096 probes through all slices ({r['propagate_s']:.2f} s, measured, "
+                       f"{r['per_probe_s']:.3f} s a probe), combined into the rate of a whole 4096-probe configuration; "
+                       f"the same sample the reference arm times per step"),
+            "build_s": r["build_s"], "per_probe_s": r["per_probe_s"], "sample_s": r["sample_s"],
+            "sample_rate": r["sample_rate"], "threads": threads, "reference_kernels": ref_kernel_leg()}
 
 
 def run_reference(args):
@@ -217,31 +260,33 @@ def run_reference(args):
     from oracle import bind as ob
     ob.lib()
     threads = ob.num_threads()
-    n_probes = max(4, args.cpu_probes // 4)
+    n_probes = args.cpu_probes
     # the workload's precision (FP32, the reference's _f path), as the GPU arm
     for w in range(args.warmup):   # untimed: a tiny sample
         cpu_sample(1, double_precision=False, seed=100 + w)
-    vals, infos = [], []
+    runs = []
     t0 = time.perf_counter()
     for k in range(args.steps):
-        v, info = cpu_sample(n_probes, double_precision=False, seed=k)
-        vals.append(v)
-        infos.append(info)
+        runs.append(cpu_sample(n_probes, double_precision=False, seed=k))
     wall = time.perf_counter() - t0
-    value = statistics.mean(vals)
-    S = infos[0]["slices"]
-    ms_per_step = 4096 * S / value * 1000.0
+    value = statistics.mean(r["value"] for r in runs)
+    S = runs[0]["slices"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "grid": 512, "probes": 4096, "slices": S,
-                   "parallelism": "host threads (OpenMP)", "sample_wall_s": wall},
+                   "parallelism": "host threads (OpenMP over probes)", "sample_wall_s": wall},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": (f"per step: transmission build of {S} slices + {n_probes} of 4096 probes "
-                                    f"through all slices of one phonon configuration, FP32 (the reference's _f path), "
-                                    f"scaled to a 4096-probe configuration; the reference's OpenCL CPU-device build "
-                                    f"needs OpenCL headers/ICD and clFFT, absent here")},
+                         "sample": (f"per step (timed): transmission build of {S} slices + {n_probes} of 4096 probes "
+                                    f"through all slices of one phonon configuration, FP32 (the reference's _f path); "
+                                    f"value = the measured build and per-probe times combined into the rate of a whole "
+                                    f"4096-probe configuration; the reference's OpenCL CPU-device build needs OpenCL "
+                                    f"headers/ICD and clFFT, absent here"),
+                         "build_s": statistics.mean(r["build_s"] for r in runs),
+                         "per_probe_s": statistics.mean(r["per_probe_s"] for r in runs),
+                         "sample_rate": statistics.mean(r["sample_rate"] for r in runs),
+                         "reference_kernels": ref_kernel_leg()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -509,6 +554,12 @@ def main():
     tuned = None
     if not args.batch:   # the probe batch from the autotuner (untimed; cached per device, grid and precision)
         tuned = sim.tune_batch()
+    tn = sim.tuning()
+    step_kernels = {
+        "column": ["one block per column tile and wave", "persistent, TMA-fed, step tile, 3 stages",
+                   "persistent, TMA-fed, half tile, 2 blocks per SM"][tn["col_variant"]],
+        "row": ["plain", "L2 prefetch one grid residency ahead", "L2 prefetch two grid residencies ahead"][tn["row_variant"]],
+        "chosen_by": "autotuner (mslice_tune_batch)" if not args.batch else "defaults"}
     S = sim.geo.n_slices
     npx = s.cfg.stem_pixels_x * s.cfg.stem_pixels_y
     N = 512 * 512
@@ -676,6 +727,7 @@ def main():
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": 512, "probes": npx, "slices": S,
                        "phonon_configs_per_gpu": args.steps, "probe_batch": sim.cfg.probe_batch or (f"{tuned[0]} (autotuned: {tuned[1]:.0f} waves/s per slice step)" if tuned else "engine default"),
+                       "step_kernels": step_kernels,
                        "precision": "complex64 waves and FFTs; FP64 phase arguments, offsets and Kahan accumulation",
                        "l2": "inputs larger than L2 (per configuration: 4096 waves x 2 MiB + 40 transmission slices x 2 MiB)",
                        "parallelism": f"dp{world} (phonon configurations sharded over GPUs)"},

@@ -76,6 +76,11 @@ class Config(C.Structure):
         ("source_size", C.c_int),
         ("source_fwhm", C.c_double),
         ("seed", C.c_ulonglong),
+        ("plasmon", C.c_int),
+        ("plasmon_individual", C.c_int),
+        ("plasmon_mfp", C.c_double),
+        ("plasmon_char_angle", C.c_double),
+        ("plasmon_crit_angle", C.c_double),
     ]
 
 
@@ -129,4 +134,8 @@ def config_defaults() -> Config:
     c.stem_area[:] = [0.0, 10.0, 0.0, 10.0]
     c.stem_pixels_x = 64
     c.stem_pixels_y = 64
+    # PlasmonScattering defaults (plasmon.h: 10 nm, 1 mrad, 0.1 mrad, type full)
+    c.plasmon_mfp = 100.0
+    c.plasmon_char_angle = 1.0
+    c.plasmon_crit_angle = 0.1
     return c

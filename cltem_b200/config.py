@@ -38,18 +38,29 @@ class PlasmonSettings:
     """PlasmonScattering's settings (src/simulation/incoherence/inelastic/plasmon.h, read by
     jsonutils.cpp:331-360; mean free path converted from nm to Å).
 
-    Enabling plasmons changes no result in the reference: its scattering depths are never generated
-    (PlasmonScattering::initDepthVectors and generateScatteringDepths have no callers), so
-    getGeneratedDepth always returns +inf and modifyBeamTilt is never reached
-    (simulationstem.cpp:191-232, simulationcbed.cpp:145-187, simulationctem.cpp:316-357). What enabling
-    them does change is reproduced here: the incoherence iterations count (IncoherentEffects::enabled) and
-    mixed static potentials are off (precalculateTransmission is false, so parallelPotentialsCount is 1)."""
+    With plasmons on, clTEM_cmd draws a table of scattering depths per job before the run
+    (src/console/main.cpp:710-727: initDepthVectors, generateScatteringDepths over the crystal's
+    thickness), and each job's slice loop tilts its beam at every depth it reaches
+    (simulationstem.cpp:191-232, simulationcbed.cpp:145-187, simulationctem.cpp:316-357). apply() copies
+    these settings into the engine's config, where the same events are made from seeded draws. Enabling
+    them also sets the incoherence iterations count (IncoherentEffects::enabled) and turns mixed static
+    potentials off (precalculateTransmission is false, so parallelPotentialsCount is 1)."""
     enabled: bool = False
     kind: str = "full"             # "full" or "individual"
     individual: int = 1
     mean_free_path: float = 100.0  # Å (10 nm)
     characteristic_angle: float = 1.0   # mrad
     critical_angle: float = 0.1         # mrad
+
+
+def apply_plasmon(cfg, p: "PlasmonSettings"):
+    """The plasmon fields of the engine's config (include/mslice.h) from the settings: "individual" n is
+    passed as n, "full" as 0."""
+    cfg.plasmon = int(bool(p.enabled))
+    cfg.plasmon_individual = max(1, int(p.individual)) if p.kind == "individual" else 0
+    cfg.plasmon_mfp = float(p.mean_free_path)
+    cfg.plasmon_char_angle = float(p.characteristic_angle)
+    cfg.plasmon_crit_angle = float(p.critical_angle)
 
 
 def _read_plasmon(j):
@@ -253,6 +264,7 @@ def read_config(path_or_dict) -> SimulationSettings:
     _try(j, lambda v: setattr(s, "mixed_static_enabled", v), *ph, "mixed static potentials", "enabled", conv=bool)
     _try(j, lambda v: setattr(s, "precalculate_transmission", v), "precalculate transmission", conv=bool)
     s.plasmon = _read_plasmon(j)
+    apply_plasmon(c, s.plasmon)
     # probe incoherence (jsonutils.cpp:276-308)
     pr = ("incoherence", "probe")
     _try(j, lambda v: setattr(c, "chromatic", int(v)), *pr, "chromatic", "enabled", conv=bool)

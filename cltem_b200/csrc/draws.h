@@ -10,11 +10,13 @@
 #pragma once
 #include <cmath>
 #include <cstdint>
+#include <limits>
+#include <vector>
 
 namespace ms {
 namespace draws {
 
-enum Kind : uint64_t { SET = 1, DEFOCUS = 2, SOURCE = 3, DOSE = 4 };
+enum Kind : uint64_t { SET = 1, DEFOCUS = 2, SOURCE = 3, DOSE = 4, PLASMON_DEPTH = 5, PLASMON_ANGLE = 6 };
 
 inline uint64_t mix64(uint64_t z) {
     z += 0x9E3779B97F4A7C15ull;
@@ -101,6 +103,82 @@ inline double poisson(uint64_t seed, int pass, uint64_t pixel, double lam) {
             return k;
     }
     return std::floor(lam);
+}
+
+// ---- plasmon scattering (PlasmonScattering, src/simulation/incoherence/inelastic/plasmon.cpp) ----------------
+// The reference draws every plasmon number from one clock-seeded std::uniform_real_distribution<>(0, 1) stream in
+// call order: the depth tables of all jobs at set-up (clTEM_cmd main.cpp:710-727), the angles of each event
+// while the jobs run. Here each draw is a function of (seed, job, attempt or event, index).
+
+// Scattering depths (Å) of job `job` for a crystal `thickness` Å thick: getDistancesforCombined
+// (plasmon.cpp:93-120), cumulative distances -mfp ln(u) while they stay <= thickness, then +inf. With
+// `individual` > 0 it is getDistancesForIndividual (:69-91): whole tables are drawn again (attempt 0, 1, ...)
+// until one has exactly `individual` entries counting the closing +inf, i.e. individual - 1 scattering
+// events, as the reference compares the table's size with the requested number. Returns false where the
+// reference gives up (more than 1e10 events in a table; or, for `individual`, no table of the asked size
+// within max_attempts attempts).
+inline bool plasmon_depths(uint64_t seed, uint64_t job, double mfp, double thickness, int individual,
+                           std::vector<double> &out, uint64_t max_attempts = 10000000ull) {
+    auto table = [&](uint64_t attempt, std::vector<double> &d) {
+        d.clear();
+        uint64_t i = 0;
+        auto distance = [&]() { return -1.0 * mfp * std::log(uniform(key(seed, PLASMON_DEPTH, job, attempt, i++))); };
+        double t = distance();
+        double c = 0;
+        while (t <= thickness && c < 1e10) {
+            d.push_back(t);
+            t += distance();
+            c++;
+        }
+        if (c >= 1e10) { d.clear(); return false; }
+        d.push_back(std::numeric_limits<double>::infinity());
+        return true;
+    };
+    if (individual <= 0) return table(0, out) && !out.empty();
+    for (uint64_t a = 0; a < max_attempts; a++) {
+        if (table(a, out) && out.size() == (size_t)individual) return true;
+    }
+    out.clear();
+    return false;
+}
+
+// Polar angle (mrad) and azimuth (rad) of scattering event `event` of job `job` (getScatteringPolar,
+// plasmon.cpp:22-31, then getScatteringAzimuth, :17-20, in the order simulate() asks for them).
+inline void plasmon_angles(uint64_t seed, uint64_t job, uint64_t event, double char_angle, double crit_angle,
+                           double &polar_mrad, double &azimuth) {
+    const double crit_2 = crit_angle * crit_angle, char_2 = char_angle * char_angle;
+    const double u1 = uniform(key(seed, PLASMON_ANGLE, job, event, 0));
+    const double ang_2 = char_2 * (std::pow((crit_2 + char_2) / char_2, u1) - 1);
+    polar_mrad = std::sqrt(ang_2);
+    azimuth = 2.0 * 3.14159265358979323846 * uniform(key(seed, PLASMON_ANGLE, job, event, 1));
+}
+
+// Utils::generateRotationAroundVector (vectorutils.cpp:8-19): Rodrigues' rotation by `angle` about `ax`
+// (normalised first), applied to v.
+inline void rotate_about(const double ax_in[3], double angle, double v[3]) {
+    const double n = std::sqrt(ax_in[0] * ax_in[0] + ax_in[1] * ax_in[1] + ax_in[2] * ax_in[2]);
+    const double a[3] = {ax_in[0] / n, ax_in[1] / n, ax_in[2] / n};
+    const double s = std::sin(angle), c1 = 1 - std::cos(angle);
+    // R = I + s [a]x + (1 - cos) [a]x^2, [a]x = ((0, -a2, a1), (a2, 0, -a0), (-a1, a0, 0))
+    const double K[3][3] = {{0.0, -a[2], a[1]}, {a[2], 0.0, -a[0]}, {-a[1], a[0], 0.0}};
+    double K2[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) K2[i][j] = K[i][0] * K[0][j] + K[i][1] * K[1][j] + K[i][2] * K[2][j];
+    double r[3];
+    for (int i = 0; i < 3; i++) {
+        double acc = 0;
+        for (int j = 0; j < 3; j++) acc += ((i == j ? 1.0 : 0.0) + K[i][j] * s + K2[i][j] * c1) * v[j];
+        r[i] = acc;
+    }
+    v[0] = r[0]; v[1] = r[1]; v[2] = r[2];
+}
+// Utils::rotateVectorSpherical (vectorutils.cpp:21-31): both rotations are formed from the incoming axes,
+// z is turned by theta about y and then by phi about the old z, y by phi about the old z.
+inline void rotate_spherical(double z[3], double y[3], double theta, double phi) {
+    const double z0[3] = {z[0], z[1], z[2]}, y0[3] = {y[0], y[1], y[2]};
+    rotate_about(y0, theta, z);
+    rotate_about(z0, phi, z);
+    rotate_about(z0, phi, y);
 }
 
 }  // namespace draws

@@ -108,6 +108,13 @@ static void compute_geometry(const mslice_config &c, HostGeom &H) {
     if (c.mixed_static > 1 && c.stem_moving_frame)
         throw Unsupported("mixed static potentials with the moving STEM frame are not supported");
     if (c.chromatic && !(c.chromatic_cc >= 0)) throw ArgError("chromatic Cc must be >= 0");
+    if (c.plasmon) {
+        if (!(c.plasmon_mfp > 0) || !(c.plasmon_char_angle > 0) || !(c.plasmon_crit_angle >= 0) || c.plasmon_individual < 0)
+            throw ArgError("plasmon settings need a positive mean free path and characteristic angle");
+        // plasmons turn precalculated transmissions off, and with them mixed static potentials
+        // (SimulationManager::parallelPotentialsCount, simulationmanager.h:185-232)
+        if (c.mixed_static > 1) throw Unsupported("mixed static potentials are off when plasmons are on");
+    }
     if (c.source_size && !(c.source_fwhm >= 0)) throw ArgError("source size FWHM must be >= 0");
     mslice_geometry &g = H.g;
     std::memset(&g, 0, sizeof(g));
@@ -587,41 +594,7 @@ struct Sim : SimBase {
             ycut.ensure(ctx, N);
             MS_CUDA(cudaMemcpyAsync(ycut.p, hc.data(), N * sizeof(int2), cudaMemcpyHostToDevice, st()));
         }
-        {
-            const double bk = g.wavenumber, bx = g.wavevector[0], by = g.wavevector[1], bz = g.wavevector[2];
-            const double f = bz / bk;
-            const double c0 = kPi * g.dz * (bk * bk - bz * bz) / bz;
-            std::vector<C> hpx(N), hpy(N), hex(N), hey(N);
-            // relative error (p64 - p) / p of a factor rounded to R, in FP64 (zero in the FP64 engine)
-            auto rel_err = [](double re, double im, C r) {
-                const double dr = re - (double)r.x, di = im - (double)r.y, n2 = (double)r.x * r.x + (double)r.y * r.y;
-                return mk<R>((R)((dr * r.x + di * r.y) / n2), (R)((di * r.x - dr * r.y) / n2));
-            };
-            for (int i = 0; i < N; i++) {
-                double ax_ = -kPi * g.dz * (bx + H.kx[i]) * (bx + H.kx[i]) / bz + c0;
-                double ay_ = -kPi * g.dz * (by + H.ky[i]) * (by + H.ky[i]) / bz;
-                hpx[i] = mk<R>((R)(f * std::cos(ax_)), (R)(f * std::sin(ax_)));
-                hpy[i] = mk<R>((R)std::cos(ay_), (R)std::sin(ay_));
-                hex[i] = rel_err(f * std::cos(ax_), f * std::sin(ax_), hpx[i]);
-                hey[i] = rel_err(std::cos(ay_), std::sin(ay_), hpy[i]);
-            }
-            px.ensure(ctx, N); py.ensure(ctx, N); pxc.ensure(ctx, N); pyc.ensure(ctx, N);
-            pxe.ensure(ctx, N); pye.ensure(ctx, N); pxec.ensure(ctx, N); pyec.ensure(ctx, N);
-            MS_CUDA(cudaMemcpyAsync(px.p, hpx.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
-            MS_CUDA(cudaMemcpyAsync(py.p, hpy.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
-            MS_CUDA(cudaMemcpyAsync(pxe.p, hex.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
-            MS_CUDA(cudaMemcpyAsync(pye.p, hey.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
-            MS_CUDA(cudaStreamSynchronize(st()));   // the host vectors are rewritten below
-            for (int i = 0; i < N; i++) {
-                hpx[i].y = -hpx[i].y; hpy[i].y = -hpy[i].y;
-                hex[i].y = -hex[i].y; hey[i].y = -hey[i].y;   // conj(p (1 + e)) = conj(p) (1 + conj(e))
-            }
-            MS_CUDA(cudaMemcpyAsync(pxc.p, hpx.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
-            MS_CUDA(cudaMemcpyAsync(pyc.p, hpy.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
-            MS_CUDA(cudaMemcpyAsync(pxec.p, hex.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
-            MS_CUDA(cudaMemcpyAsync(pyec.p, hey.data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
-            MS_CUDA(cudaStreamSynchronize(st()));
-        }
+        set_propagator(g.wavevector[0], g.wavevector[1], g.wavevector[2]);
         {
             const int C = ops.cols_per_tile, nt = N / C;
             const double km2 = k_prop * k_prop;
@@ -662,6 +635,126 @@ struct Sim : SimBase {
     ~Sim() override {
         drop_graphs();
         for (auto e : ev) if (e) cudaEventDestroy(e);
+    }
+
+    // The separable propagator (propagator_d.cl:18-52) for the beam wavevector (bx, by, bz): phase pi dz s,
+    // s = (k^2 - kz^2 - (kx+bx)^2 - (ky+by)^2)/kz with k the wavenumber, as px[x] * py[y]; the FP32 tables'
+    // relative representation errors; the conjugates for the adjoint. Copied in stream order and waited for.
+    void set_propagator(double bx, double by, double bz) {
+        const mslice_geometry &g = H.g;
+        const double bk = g.wavenumber;
+        const double f = bz / bk;
+        const double c0 = kPi * g.dz * (bk * bk - bz * bz) / bz;
+        std::vector<C> hpx(N), hpy(N), hex(N), hey(N);
+        // relative error (p64 - p) / p of a factor rounded to R, in FP64 (zero in the FP64 engine)
+        auto rel_err = [](double re, double im, C r) {
+            const double dr = re - (double)r.x, di = im - (double)r.y, n2 = (double)r.x * r.x + (double)r.y * r.y;
+            return mk<R>((R)((dr * r.x + di * r.y) / n2), (R)((di * r.x - dr * r.y) / n2));
+        };
+        for (int i = 0; i < N; i++) {
+            double ax_ = -kPi * g.dz * (bx + H.kx[i]) * (bx + H.kx[i]) / bz + c0;
+            double ay_ = -kPi * g.dz * (by + H.ky[i]) * (by + H.ky[i]) / bz;
+            hpx[i] = mk<R>((R)(f * std::cos(ax_)), (R)(f * std::sin(ax_)));
+            hpy[i] = mk<R>((R)std::cos(ay_), (R)std::sin(ay_));
+            hex[i] = rel_err(f * std::cos(ax_), f * std::sin(ax_), hpx[i]);
+            hey[i] = rel_err(std::cos(ay_), std::sin(ay_), hpy[i]);
+        }
+        px.ensure(ctx, N); py.ensure(ctx, N); pxc.ensure(ctx, N); pyc.ensure(ctx, N);
+        pxe.ensure(ctx, N); pye.ensure(ctx, N); pxec.ensure(ctx, N); pyec.ensure(ctx, N);
+        std::vector<C> cpx(hpx), cpy(hpy), cex(hex), cey(hey);
+        for (int i = 0; i < N; i++) {
+            cpx[i].y = -cpx[i].y; cpy[i].y = -cpy[i].y;
+            cex[i].y = -cex[i].y; cey[i].y = -cey[i].y;   // conj(p (1 + e)) = conj(p) (1 + conj(e))
+        }
+        const std::pair<C *, const std::vector<C> *> up[8] = {{px.p, &hpx},  {py.p, &hpy},  {pxe.p, &hex},  {pye.p, &hey},
+                                                              {pxc.p, &cpx}, {pyc.p, &cpy}, {pxec.p, &cex}, {pyec.p, &cey}};
+        for (const auto &u : up)
+            MS_CUDA(cudaMemcpyAsync(u.first, u.second->data(), N * sizeof(C), cudaMemcpyHostToDevice, st()));
+        MS_CUDA(cudaStreamSynchronize(st()));   // the host vectors go out of scope on return
+    }
+
+    // ---- plasmon scattering: the slice loops of SimulationStem/Cbed/Ctem::simulate with plasmons on -------------
+    // (simulationstem.cpp:190-232, simulationcbed.cpp:145-187, simulationctem.cpp:316-357). A job's beam starts
+    // as (0, 0, k) turned by the beam tilt and azimuth; after each slice whose exit depth (below the padding
+    // slices) reaches the job's next scattering depth, it turns by a drawn polar angle about the current azimuth
+    // axis and a drawn azimuth about the old beam, and modifyBeamTilt rebuilds the propagator (and, in the full
+    // 3-D model, the sub-slice shifts of the transmissions that follow).
+    struct Beam {
+        double k[3], y[3];            // wavevector and the axis the polar rotation turns about
+        std::vector<double> depths;   // scattering depths (Å), the last +inf
+        int count = 0;                // events so far
+        uint64_t job = 0;
+        bool tilted = false;          // an event has changed the propagator
+    };
+    bool shift_override = false;      // the full 3-D sub-slice shifts of the current beam (pot_params)
+    double ov_shift_x = 0, ov_shift_y = 0;
+    Beam beam_of_job(uint64_t job) const {
+        Beam b;
+        b.job = job;
+        b.k[0] = 0; b.k[1] = 0; b.k[2] = H.g.wavenumber;
+        b.y[0] = 0; b.y[1] = 1; b.y[2] = 0;
+        draws::rotate_spherical(b.k, b.y, cfg.beam_tilt / 1000.0, cfg.beam_azimuth);
+        // the crystal's thickness (CrystalStructure::limitsZ, clTEM_cmd main.cpp:712-714)
+        const double thk = cfg.struct_limits[5] - cfg.struct_limits[4];
+        if (!draws::plasmon_depths(cfg.seed, job, cfg.plasmon_mfp, thk, cfg.plasmon_individual, b.depths))
+            throw ArgError("Could not generate valid plasmon configuration (job " + std::to_string(job) + ")");
+        return b;
+    }
+    // after slice s of job b: a scattering event when the exit depth reaches the next depth
+    // (PlasmonScattering::getGeneratedDepth, plasmon.cpp:122-141); true when one happened
+    bool plasmon_step(Beam &b, int s) {
+        const mslice_geometry &g = H.g;
+        const double depth = (s + 1 - g.pre_slices) * g.dz;
+        const double next = b.count < (int)b.depths.size() ? b.depths[b.count] : std::numeric_limits<double>::infinity();
+        if (!(depth >= next)) return false;
+        double polar, az;
+        draws::plasmon_angles(cfg.seed, b.job, (uint64_t)b.count, cfg.plasmon_char_angle, cfg.plasmon_crit_angle, polar, az);
+        draws::rotate_spherical(b.k, b.y, polar / 1000.0, az);
+        b.count++;
+        modify_beam(b.k, s);
+        b.tilted = true;
+        return true;
+    }
+    // SimulationGeneral::modifyBeamTilt (simulationgeneral.cpp:649-679) after slice s
+    void modify_beam(const double k[3], int s) {
+        if (!cfg.full3d)   // the reference stops here: see below
+            throw Unsupported("plasmon scattering event with the projected potential: the reference's modifyBeamTilt "
+                              "sets argument 29 of transmission_potentials_projected, which has 29 arguments (0-28), so "
+                              "clSetKernelArg fails and the simulation stops (simulationgeneral.cpp:662-668)");
+        const mslice_geometry &g = H.g;
+        const int ints = cfg.full3d_integrals > 0 ? cfg.full3d_integrals : 1;
+        // both sub-slice shifts from kx, as the reference writes them (:657-661)
+        ov_shift_x = (k[0] / k[2]) * g.dz / ints;
+        ov_shift_y = (k[0] / k[2]) * g.dz / ints;
+        shift_override = true;
+        set_propagator(k[0], k[1], k[2]);
+        // the transmissions of the slices still to come, with the new shifts (the reference builds every slice's
+        // transmission as it reaches it when plasmons are on, simulationgeneral.cpp:697-729)
+        const int S = g.n_slices;
+        if (s + 1 < S) {
+            potentials(trans.p + (size_t)(s + 1) * NN, s + 1, S - s - 1);
+            band_limit(trans.p + (size_t)(s + 1) * NN, S - s - 1);
+        }
+    }
+    // back to the configuration's beam after a tilted job: propagator and transmissions of the frame in use
+    void restore_beam() {
+        const mslice_geometry &g = H.g;
+        shift_override = false;
+        set_propagator(g.wavevector[0], g.wavevector[1], g.wavevector[2]);
+        potentials(trans.p, 0, g.n_slices);
+        band_limit(trans.p, g.n_slices);
+    }
+    // the translation of diffraction outputs after tilts (getDiffractionImage / getStemPixel with d_k =
+    // k_vec - orig_k, translateDiffImage simulationgeneral.cpp:832-853)
+    Shift2 out_shift(const Beam &b) const {
+        const mslice_geometry &g = H.g;
+        const double shx = (b.k[0] - g.wavevector[0]) / g.inverse_scale, shy = (b.k[1] - g.wavevector[1]) / g.inverse_scale;
+        Shift2 sh;
+        sh.ix = (int)std::floor(shx);
+        sh.iy = (int)std::floor(shy);
+        sh.sx = shx - sh.ix;
+        sh.sy = shy - sh.iy;
+        return sh;
     }
 
     AberrD aberr(double c10) const {
@@ -788,6 +881,10 @@ struct Sim : SimBase {
         p.integrals = cfg.full3d_integrals > 0 ? cfg.full3d_integrals : 1;
         p.shift_x = (g.wavevector[0] / g.wavevector[2]) * g.dz / p.integrals;   // simulationgeneral.cpp:562-563
         p.shift_y = (g.wavevector[1] / g.wavevector[2]) * g.dz / p.integrals;
+        if (shift_override) {   // after a plasmon event (modify_beam)
+            p.shift_x = ov_shift_x;
+            p.shift_y = ov_shift_y;
+        }
         p.form = ctx->params.form; p.i_count = ctx->params.i_count;
         return p;
     }
@@ -1117,6 +1214,10 @@ struct Sim : SimBase {
                    bool sync_each) {
         const mslice_geometry &g = H.g;
         const int S = g.n_slices;
+        if (cfg.plasmon) {
+            stem_pass_plasmon(pass, ids, out_index, n, n_pix, out, comp);
+            return;
+        }
         const int K = cfg.mixed_static > 1 ? cfg.mixed_static : 1;
         const bool chrom = cfg.chromatic != 0;
         auto after_batch = [&](size_t done) {
@@ -1180,6 +1281,75 @@ struct Sim : SimBase {
         trans_built = false;   // the sets now hold job windows
     }
 
+    // STEM with plasmons (SimulationStem::simulate, simulationstem.cpp:143-278): jobs of stem_job_pixels consecutive
+    // pixels, job `pass * n_jobs + j` (SimulationRunner::SplitJobs numbers the jobs of pass after pass; the
+    // reference's pixel shuffle is clock-seeded and not reproduced), each one batch with its own tilt history,
+    // launched slice by slice. At an output slice the column pass keeps the reciprocal wave and, after the
+    // event check, the detectors read its translated pattern (the identity while the beam is untilted).
+    DevBuf<double> tpart;   // detector partials of the translated readout
+    void stem_pass_plasmon(int pass, const int *ids, const int *out_index, size_t n, int n_pix, double *out, double *comp) {
+        const mslice_geometry &g = H.g;
+        if (cfg.stem_moving_frame) throw Unsupported("plasmon scattering with the moving STEM frame is not supported");
+        const int P = std::max(1, cfg.stem_job_pixels);
+        const size_t n_jobs = (n + P - 1) / P;
+        ensure_waves((int)std::min<size_t>((size_t)P, std::max<size_t>(n, 1)));
+        const int nd = cfg.n_detectors;
+        double in[16] = {}, outr[16] = {}, xc[16] = {}, yc[16] = {};
+        for (int d = 0; d < nd; d++) {
+            in[d] = cfg.detectors[d].inner / g.angle_scale;
+            outr[d] = cfg.detectors[d].outer / g.angle_scale;
+            xc[d] = cfg.detectors[d].xcentre / g.angle_scale;
+            yc[d] = cfg.detectors[d].ycentre / g.angle_scale;
+        }
+        const int det_blocks = (int)((NN + 255) / 256);
+        tpart.ensure(ctx, (size_t)batch_cap * std::max(1, nd) * det_blocks);
+        const cplx<R> *tw = ctx->twiddles<R>(N);
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p, ctx->step_err, pxe.p, pye.p};
+        DetArgs nodet{detmask.p, 0, partials.p};
+        const std::vector<int> outs = output_slices(cfg, g);
+        const R a = (R)(1.0 / N), b = (R)(s2d * s2d * N), ds = (R)s2d;
+        const bool chrom = cfg.chromatic != 0;
+        for (size_t j = 0; j < n_jobs; j++) {
+            check_cancel();
+            const size_t i0 = j * P, i1 = std::min(n, i0 + P);
+            const int nb = (int)(i1 - i0);
+            Beam beam = beam_of_job((uint64_t)pass * n_jobs + j);
+            BeamScope scope{this};
+            plasmon_beam = &beam;
+            h_pos.resize(nb);
+            for (int i = 0; i < nb; i++) h_pos[i] = probe_pos(ids[i0 + i]);
+            h_pix.assign(out_index + i0, out_index + i1);
+            MS_CUDA(cudaMemcpyAsync(pos.p, h_pos.data(), nb * sizeof(double2), cudaMemcpyHostToDevice, st()));
+            MS_CUDA(cudaMemcpyAsync(pix.p, h_pix.data(), nb * sizeof(int), cudaMemcpyHostToDevice, st()));
+            if (chrom) {
+                fill_defocus(pass, ids + i0, nb);
+                MS_CUDA(cudaMemcpyAsync(dfac.p, h_dfac.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st()));
+            }
+            // columns outside the propagator's cut are never written by the column pass: zero there
+            MS_CUDA(cudaMemsetAsync(recip.p, 0, (size_t)nb * NN * sizeof(C), st()));
+            ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N), chrom ? dfac.p : nullptr,
+                          g.wavelength);
+            ctx->launches++;
+            size_t oi = 0;
+            for (int s = 0; s < g.n_slices; s++) {
+                ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a, xa, xb, s == 0 ? 1 : 0, nullptr, 0, 0);
+                const bool is_out = oi < outs.size() && outs[oi] == s;
+                const int mode = !is_out ? COL_STEP : (s == g.n_slices - 1 ? COL_DET_ONLY : COL_STEP_DET);
+                pt.px = px.p; pt.py = py.p; pt.pxe = pxe.p; pt.pye = pye.p;   // set_propagator keeps the buffers
+                ops.col_step(st(), wave.p, nb, tw, pt, b, ds, nodet, is_out ? recip.p : nullptr, mode, tiles_lo, tiles_hi, 0);
+                ctx->launches += 2;
+                plasmon_step(beam, s);
+                if (is_out) {
+                    const int blocks = detectors_shifted<R>(st(), N, nb, recip.p, out_shift(beam), nd, in, outr, xc, yc, tpart.p);
+                    detector_reduce(st(), tpart.p, blocks, nd, nb, pix.p, n_pix, (int)oi, out, comp);
+                    ctx->launches += 2;
+                    oi++;
+                }
+            }
+            MS_CUDA(cudaStreamSynchronize(st()));
+        }
+    }
+
     void stem_run(const int *pixels, size_t n, double *out) override {
         if (cfg.mode != MSLICE_MODE_STEM) throw StateError("simulation is not in STEM mode");
         if (cfg.mixed_static > 1)
@@ -1210,6 +1380,13 @@ struct Sim : SimBase {
         ensure_waves(1);
         const int K = cfg.mixed_static > 1 ? cfg.mixed_static : 1;
         const size_t set_stride = (size_t)g.n_slices * NN;
+        // plasmons: the job of a CTEM / CBED pass is the pass (SimulationRunner::SplitJobs, simulationrunner.cpp:62-67)
+        Beam beam;
+        BeamScope scope{this};
+        if (cfg.plasmon) {
+            beam = beam_of_job((uint64_t)pass);
+            plasmon_beam = &beam;
+        }
         if (K > 1) {
             h_sel.resize(g.n_slices);
             for (int sl = 0; sl < g.n_slices; sl++) h_sel[sl] = draws::set_of(cfg.seed, pass, 0, sl, K);
@@ -1247,9 +1424,34 @@ struct Sim : SimBase {
                              N / ops.cols_per_tile, 0, 0);
             });
             ctx->launches += 2;
+            if (plasmon_beam) plasmon_step(*plasmon_beam, s);   // the event check comes before the slice's outputs
             if (is_out) { on_output((int)oi); oi++; }
             if (progress) progress((double)(s + 1) / g.n_slices, progress_user);
         }
+    }
+
+    // ends a plasmon job on every exit path: the configuration's beam back if an event tilted it
+    struct BeamScope {
+        Sim *sim;
+        ~BeamScope() {
+            if (!sim->plasmon_beam) return;
+            if (sim->plasmon_beam->tilted) {
+                try {
+                    sim->restore_beam();
+                } catch (...) {   // a failing restore leaves the tables of the tilted beam: rebuilt by the next run
+                    sim->trans_built = false;
+                }
+            }
+            sim->plasmon_beam = nullptr;
+        }
+    };
+
+    // the diffraction output of the single wave in recip: translated while a plasmon event has tilted the beam
+    Beam *plasmon_beam = nullptr;   // the beam of the job single_wave is running (plasmons on), else nullptr
+    void diff_out(double *out, double *comp) {
+        if (plasmon_beam && plasmon_beam->tilted) diffraction_shifted<R>(st(), N, recip.p, out_shift(*plasmon_beam), out, comp);
+        else diffraction<R>(st(), N, recip.p, out, comp);
+        ctx->launches++;
     }
 
     void cbed_run(double *diff) override {
@@ -1260,8 +1462,7 @@ struct Sim : SimBase {
         DevBuf<double> d;
         d.ensure(ctx, (size_t)H.g.n_outputs * NN);
         single_wave(false, 0, [&](int o) {
-            diffraction<R>(st(), N, recip.p, d.p + (size_t)o * NN, nullptr);
-            ctx->launches++;
+            diff_out(d.p + (size_t)o * NN, nullptr);
         });
         MS_CUDA(cudaStreamSynchronize(st()));
         MS_CUDA(cudaMemcpy(diff, d.p, (size_t)H.g.n_outputs * NN * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1337,7 +1538,7 @@ struct Sim : SimBase {
                 convert_to_double<R>(st(), NN, tmp.p, de.p + (size_t)o * NN);
                 ctx->launches += 2;
             }
-            if (diff) { diffraction<R>(st(), N, recip.p, dd.p + (size_t)o * NN, nullptr); ctx->launches++; }
+            if (diff) diff_out(dd.p + (size_t)o * NN, nullptr);
             if (image && cfg.ctem_image) {   // simulateImagePerfect (simulationctem.cpp:114-166)
                 ctem_transfer<R>(st(), N, recip.p, tmp.p, kx.p, ky.p, g.wavelength, aberr(cfg.C10), cfg.obj_ap,
                                  cfg.obj_ap_smooth, cfg.alpha, cfg.delta);
@@ -1432,8 +1633,7 @@ struct Sim : SimBase {
                 stem_pass(it, ids.data(), ids.data(), (size_t)np, np, acc.p, comp.p, false);
             } else {
                 single_wave(false, it, [&](int o) {
-                    diffraction<R>(st(), N, recip.p, acc.p + (size_t)o * NN, comp.p + (size_t)o * NN);
-                    ctx->launches++;
+                    diff_out(acc.p + (size_t)o * NN, comp.p + (size_t)o * NN);
                 });
             }
             MS_CUDA(cudaEventRecord(ev[3], st()));
@@ -2221,6 +2421,26 @@ int mslice_incoherence_draws(const mslice_config *cfg, int pass, const int *pixe
                 shift[2 * b] = dx;
                 shift[2 * b + 1] = dy;
             }
+    });
+}
+
+int mslice_plasmon_draws(const mslice_config *cfg, unsigned long long job, double thickness, double *depths, size_t cap,
+                         size_t *n_depths, int n_events, double *angles) {
+    return guarded([&] {
+        need(cfg != nullptr, "null argument");
+        if (depths || n_depths) {
+            need(depths != nullptr && n_depths != nullptr, "depths and n_depths go together");
+            std::vector<double> d;
+            if (!ms::draws::plasmon_depths(cfg->seed, job, cfg->plasmon_mfp, thickness, cfg->plasmon_individual, d))
+                throw ms::ArgError("Could not generate valid plasmon configuration");
+            need(d.size() <= cap, "depth capacity too small");
+            std::copy(d.begin(), d.end(), depths);
+            *n_depths = d.size();
+        }
+        if (angles)
+            for (int e = 0; e < n_events; e++)
+                ms::draws::plasmon_angles(cfg->seed, job, (uint64_t)e, cfg->plasmon_char_angle, cfg->plasmon_crit_angle,
+                                          angles[2 * e], angles[2 * e + 1]);
     });
 }
 

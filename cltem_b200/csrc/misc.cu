@@ -222,6 +222,92 @@ template <class R> void diffraction(cudaStream_t s, int n, const cplx<R> *recip,
     MS_CUDA(cudaGetLastError());
 }
 
+// ---- the diffraction pattern translated after a plasmon tilt ---------------------------------------------
+// Pixel (X, Y) of |fftshift(recip)|^2 translated by bilinear_translate_d (kernels/bilinear_translate_d.cl:18-77):
+// the source pixel (X - ix, Y - iy), wrapped once, and its left, upper and upper-left neighbours (wrapped),
+// weighted by the sub-pixel shift (sx, sy); 0 where one wrap does not bring the source into the grid. The
+// shifted image at (X', Y') is |recip| ^2 at ((X' + n/2) % n, (Y' + n/2) % n) (fft_shift_d.cl:12-48, even n).
+template <class R>
+__device__ __forceinline__ double translated_intensity(const cplx<R> *__restrict__ recip, int n, int X, int Y, Shift2 sh) {
+    int nx = X - sh.ix, ny = Y - sh.iy;
+    if (nx < 0) nx += n; else if (nx >= n) nx -= n;
+    if (ny < 0) ny += n; else if (ny >= n) ny -= n;
+    if (nx < 0 || nx >= n || ny < 0 || ny >= n) return 0.0;
+    const int xl = nx == 0 ? n - 1 : nx - 1, yu = ny == 0 ? n - 1 : ny - 1;   // left and upper neighbours
+    auto I = [&](int xs, int ys) {
+        const cplx<R> v = recip[(size_t)((ys + n / 2) % n) * n + (xs + n / 2) % n];
+        const double re = (double)v.x, im = (double)v.y;
+        return re * re + im * im;
+    };
+    const double f_br = sh.sx * sh.sy, f_bl = (1.0 - sh.sx) * sh.sy;
+    const double f_tr = sh.sx * (1.0 - sh.sy), f_tl = (1.0 - sh.sx) * (1.0 - sh.sy);
+    return f_tl * I(nx, ny) + f_tr * I(xl, ny) + f_bl * I(nx, yu) + f_br * I(xl, yu);
+}
+
+template <class R>
+__global__ void k_diffraction_shifted(int n, const cplx<R> *__restrict__ recip, Shift2 sh, double *__restrict__ out,
+                                      double *__restrict__ comp) {
+    const int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y;
+    if (X >= n) return;
+    const double e = translated_intensity<R>(recip, n, X, Y, sh);
+    const size_t oi = (size_t)Y * n + X;
+    if (comp) {
+        double sum = out[oi], c = comp[oi];
+        kahan_add(sum, c, e);
+        out[oi] = sum;
+        comp[oi] = c;
+    } else {
+        out[oi] = e;
+    }
+}
+template <class R> void diffraction_shifted(cudaStream_t s, int n, const cplx<R> *recip, Shift2 sh, double *out, double *comp) {
+    dim3 b(128), gr((n + 127) / 128, n);
+    k_diffraction_shifted<R><<<gr, b, 0, s>>>(n, recip, sh, out, comp);
+    MS_CUDA(cudaGetLastError());
+}
+
+// STEM detectors on the translated pattern (getStemPixel with d_kx, d_ky != 0, simulationstem.cpp:74-132):
+// band_pass_d's annulus on the translated |fftshift(recip)|^2 of every wave of a batch (waves n*n apart);
+// per block and detector an FP64 partial sum at partials[(wave * n_det + d) * gridDim.x + block]
+template <class R>
+__global__ void __launch_bounds__(256) k_det_shifted(int n, const cplx<R> *__restrict__ recip, Shift2 sh, int n_det, DetDesc D,
+                                                     double *__restrict__ partials) {
+    __shared__ double red[8];
+    const size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int X = (int)(id % n), Y = (int)(id / n);
+    const bool in = id < (size_t)n * n;
+    const double e = in ? translated_intensity<R>(recip + (size_t)blockIdx.y * n * n, n, X, Y, sh) : 0.0;
+    for (int d = 0; d < n_det; d++) {
+        const double centX = n / 2.0 + D.xc[d], centY = n / 2.0 + D.yc[d];
+        const double radius = sqrt((X - centX) * (X - centX) + (Y - centY) * (Y - centY));
+        double v = (in && radius <= D.out[d] && radius >= D.in[d]) ? e : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int w = 0; w < (int)(blockDim.x / 32); w++) t += red[w];
+            partials[((size_t)blockIdx.y * n_det + d) * gridDim.x + blockIdx.x] = t;
+        }
+    }
+}
+template <class R>
+int detectors_shifted(cudaStream_t s, int n, int batch, const cplx<R> *recip, Shift2 sh, int n_det, const double *innerPx,
+                      const double *outerPx, const double *xcPx, const double *ycPx, double *partials) {
+    DetDesc D;
+    for (int d = 0; d < 16; d++) {
+        D.in[d] = d < n_det ? innerPx[d] : 0;
+        D.out[d] = d < n_det ? outerPx[d] : 0;
+        D.xc[d] = d < n_det ? xcPx[d] : 0;
+        D.yc[d] = d < n_det ? ycPx[d] : 0;
+    }
+    const int blocks = (int)(((size_t)n * n + 255) / 256);
+    k_det_shifted<R><<<dim3(blocks, batch), 256, 0, s>>>(n, recip, sh, n_det, D, partials);
+    MS_CUDA(cudaGetLastError());
+    return blocks;
+}
+
 template <class R>
 __global__ void k_sqabs(size_t count, const cplx<R> *__restrict__ in, double *__restrict__ out) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -366,6 +452,9 @@ template <class R> void real_part_to_double(cudaStream_t s, size_t count, const 
     template void sqabs_complex<R>(cudaStream_t, size_t, cplx<R> *);                                                    \
     template void ccd_filter<R>(cudaStream_t, int, cplx<R> *, const double *, int, bool);                              \
     template void diffraction<R>(cudaStream_t, int, const cplx<R> *, double *, double *);                               \
+    template void diffraction_shifted<R>(cudaStream_t, int, const cplx<R> *, Shift2, double *, double *);               \
+    template int detectors_shifted<R>(cudaStream_t, int, int, const cplx<R> *, Shift2, int, const double *,             \
+                                      const double *, const double *, const double *, double *);                        \
     template void sqabs_to_double<R>(cudaStream_t, size_t, const cplx<R> *, double *);                                  \
     template void ctem_transfer<R>(cudaStream_t, int, const cplx<R> *, cplx<R> *, const double *, const double *, double, \
                                    const AberrD &, double, double, double, double);                                    \

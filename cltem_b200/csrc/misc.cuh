@@ -43,6 +43,20 @@ void detector_reduce(cudaStream_t s, const double *partials, int n_blocks, int n
 // Diffraction |fftshift(recip)|^2 (getDiffractionImage, simulationgeneral.cpp:772-806) into out (double);
 // Kahan-accumulated when comp != nullptr.
 template <class R> void diffraction(cudaStream_t s, int n, const cplx<R> *recip, double *out, double *comp);
+// A translation of the diffraction pattern by (ix + sx, iy + sy) pixels, 0 <= sx, sy < 1
+// (SimulationGeneral::translateDiffImage, simulationgeneral.cpp:832-853)
+struct Shift2 {
+    int ix, iy;
+    double sx, sy;
+};
+// The diffraction pattern translated by sh (bilinear_translate_d.cl:18-77) into out, Kahan-accumulated when
+// comp != nullptr (getDiffractionImage with d_kx, d_ky != 0, simulationgeneral.cpp:772-806)
+template <class R> void diffraction_shifted(cudaStream_t s, int n, const cplx<R> *recip, Shift2 sh, double *out, double *comp);
+// STEM detectors on each wave's translated pattern (getStemPixel with d_kx, d_ky != 0): FP64 block partials at
+// partials[(wave * n_det + d) * blocks + block]; returns blocks (the n_blocks of detector_reduce)
+template <class R> int detectors_shifted(cudaStream_t s, int n, int batch, const cplx<R> *recip, Shift2 sh, int n_det,
+                                         const double *innerPx, const double *outerPx, const double *xcPx,
+                                         const double *ycPx, double *partials);
 // |psi|^2 into double
 template <class R> void sqabs_to_double(cudaStream_t s, size_t count, const cplx<R> *in, double *out);
 // ctem_image_d (kernels/ctem_image_d.cl:50-119) on the reciprocal exit wave

@@ -81,6 +81,7 @@ def load_library(path=None):
         "mslice_ctem_loss": [C.c_void_p, _dp, _dp],
         "mslice_profile_read": [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_ulonglong), _dp, C.c_int],
         "mslice_incoherence_draws": [C.POINTER(abi.Config), C.c_int, _ip, C.c_size_t, _dp, _ip, C.c_int, C.c_int, _dp],
+        "mslice_plasmon_draws": [C.POINTER(abi.Config), C.c_ulonglong, C.c_double, _dp, C.c_size_t, _szp, C.c_int, _dp],
         "mslice_tune_batch": [C.c_void_p, _ip, C.c_int, C.c_int, _ip, _dp],
         "mslice_set_step_variant": [C.c_void_p, C.c_int, C.c_int],
         "mslice_get_tuning": [C.c_void_p, _ip, _ip, _ip, _ip, _ip],
@@ -140,6 +141,17 @@ def incoherence_draws(cfg: abi.Config, pass_: int, pixels, n_slices: int, n_buil
     _check(L.mslice_incoherence_draws(C.byref(cfg), int(pass_), _i(pixels), len(pixels), _d(df), _i(sets), int(n_slices),
                                       int(n_builds), _d(shift)))
     return df, sets, shift
+
+
+def plasmon_draws(cfg: abi.Config, job: int, thickness: float, n_events: int = 0, cap: int = 4096):
+    """The seeded plasmon draws of one job (host only): scattering depths (Å, the last +inf) and the
+    (polar mrad, azimuth rad) of its first n_events events."""
+    L = load_library()
+    d = np.zeros(cap)
+    n = C.c_size_t()
+    ang = np.zeros(2 * max(n_events, 1))
+    _check(L.mslice_plasmon_draws(C.byref(cfg), int(job), float(thickness), _d(d), cap, C.byref(n), int(n_events), _d(ang)))
+    return d[: n.value], ang[: 2 * n_events].reshape(n_events, 2)
 
 
 class Context:

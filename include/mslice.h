@@ -132,7 +132,15 @@ typedef struct mslice_config {
     double chromatic_hwhm_neg, chromatic_hwhm_pos;   /* energy spread half widths (eV) */
     int source_size;             /* random shift of the transmission frame per build (ProbeSourceSize) */
     double source_fwhm;          /* Å */
-    unsigned long long seed;     /* seed of every random draw (sets, defocus changes, frame shifts) */
+    unsigned long long seed;     /* seed of every random draw (sets, defocus changes, frame shifts, plasmons) */
+
+    /* ---- plasmon scattering (PlasmonScattering, src/simulation/incoherence/inelastic/plasmon.h) ---------- */
+    int plasmon;                 /* 1: scattering events tilt the beam of each job ("inelastic scattering/plasmon") */
+    int plasmon_individual;      /* 0: type "full"; n >= 1: type "individual" with "individual" n, which the reference
+                                    meets with tables of n entries counting the closing +inf: n - 1 events */
+    double plasmon_mfp;          /* mean free path (Å; the JSON's nm x 10) */
+    double plasmon_char_angle;   /* characteristic angle (mrad) */
+    double plasmon_crit_angle;   /* critical angle (mrad) */
 } mslice_config;
 
 /* Derived geometry (what SimulationManager / SimulationCell compute from a config). */
@@ -277,6 +285,14 @@ int mslice_stem_simulate(mslice_sim *sim, int n_configs, const size_t *counts, c
  * frame; 0 for the mixed static sets). Any output pointer may be NULL; shift receives n_builds pairs. */
 int mslice_incoherence_draws(const mslice_config *cfg, int pass, const int *pixels, size_t n_pixels, double *defocus,
                              int *sets, int n_slices, int n_builds, double *shift);
+/* The seeded plasmon draws of job `job` (host only; replaces the clock-seeded stream of PlasmonScattering,
+ * src/simulation/incoherence/inelastic/plasmon.cpp): the scattering depths (Å) of generateScatteringDepths for a
+ * crystal `thickness` Å thick, closed by +inf (n_depths entries into depths[cap]; MSLICE_ERR_ARG where the
+ * reference could not make a valid table), and the (polar mrad, azimuth rad) pairs of events 0..n_events-1 into
+ * angles[2 * n_events]. Jobs are numbered as the runs number them: the pass for CTEM / CBED, pass * n_jobs + j
+ * for STEM job j of stem_job_pixels consecutive pixels. Any output may be NULL. */
+int mslice_plasmon_draws(const mslice_config *cfg, unsigned long long job, double thickness, double *depths, size_t cap,
+                         size_t *n_depths, int n_events, double *angles);
 
 /* Autotuner of the probe batch and of the column step's kernel (no counterpart in the reference, which
  * propagates `parallel pixels` probes one at a time): times `reps` slice steps (one fused row and one

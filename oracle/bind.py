@@ -64,6 +64,9 @@ def lib():
         L.orc_draws.argtypes = [C.POINTER(abi.Config), C.c_int, _ip, C.c_size_t, _dp, _ip, C.c_int, C.c_int, _dp]
         L.orc_set_ccd.argtypes = [C.c_void_p, _dp, _dp, C.c_size_t, C.c_int, C.c_double]
         L.orc_poisson.argtypes = [C.c_uint64, C.c_int, _dp, C.c_size_t, _dp]
+        L.orc_k_bilinear_translate.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int]
+        L.orc_plasmon_depths.argtypes = [C.POINTER(abi.Config), C.c_ulonglong, C.c_double, _dp, C.c_size_t,
+                                         C.POINTER(C.c_size_t)]
         _lib = L
     return _lib
 
@@ -138,6 +141,21 @@ def poisson(seed, pass_, lam):
     out = np.zeros_like(lam)
     _chk(lib().orc_poisson(int(seed), int(pass_), _d(lam), lam.size, _d(out)))
     return out
+
+
+def bilinear_translate(img, ix, iy, sx, sy):
+    """bilinear_translate_d restated (FP64) on a real image [h, w]."""
+    a = np.ascontiguousarray(img, dtype=np.float64)
+    out = np.empty_like(a)
+    _chk(lib().orc_k_bilinear_translate(_d(a), _d(out), int(ix), int(iy), float(sx), float(sy), a.shape[1], a.shape[0]))
+    return out
+
+
+def plasmon_depths(cfg, job, thickness, cap=4096):
+    out = np.zeros(cap)
+    n = C.c_size_t()
+    _chk(lib().orc_plasmon_depths(C.byref(cfg), int(job), float(thickness), _d(out), cap, C.byref(n)))
+    return out[: n.value]
 
 
 def set_threads(n):

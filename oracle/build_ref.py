@@ -21,7 +21,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-KERNELS = ["atom_sort", "band_limit", "band_pass", "complex_multiply", "complex_to_real", "fft_shift",
+KERNELS = ["atom_sort", "band_limit", "band_pass", "bilinear_translate", "complex_multiply", "complex_to_real", "fft_shift",
            "init_plane_wave", "init_probe_wave", "propagator", "sqabs", "sum_reduction",
            "transmission_potentials_projected", "transmission_potentials_full_3d", "ctem_image"]
 

@@ -28,11 +28,13 @@
 #include "../include/mslice.h"
 
 #include <algorithm>
+#include <array>
 #include <cfloat>
 #include <cmath>
 #include <complex>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -156,6 +158,68 @@ static void draw_shift(const mslice_config &c, int build, double &dx, double &dy
     double sd = c.source_fwhm / (2.0 * std::sqrt(2.0 * std::log(2.0)));
     dx = draw_normal(draw_key(c.seed, 3, (uint64_t)build, 0, 0), draw_key(c.seed, 3, (uint64_t)build, 0, 1)) * sd;
     dy = draw_normal(draw_key(c.seed, 3, (uint64_t)build, 1, 0), draw_key(c.seed, 3, (uint64_t)build, 1, 1)) * sd;
+}
+
+// ---- plasmon scattering (PlasmonScattering, src/simulation/incoherence/inelastic/plasmon.cpp), seeded ----
+// getScatteringDistance (plasmon.cpp:11-14) is -mfp ln(u); getDistancesforCombined (:93-120) adds distances
+// while they stay <= thickness and closes the table with +inf; getDistancesForIndividual (:69-91) draws whole
+// tables again until one has `individual` entries, the closing +inf included. The i-th uniform of table
+// `attempt` of job `job` is draw_uniform(draw_key(seed, 5, job, attempt, i)).
+static bool draw_plasmon_depths(const mslice_config &c, uint64_t job, double thickness, std::vector<double> &out) {
+    auto table = [&](uint64_t attempt, std::vector<double> &d) {
+        d.clear();
+        uint64_t i = 0;
+        auto dist = [&]() { return -1.0 * c.plasmon_mfp * std::log(draw_uniform(draw_key(c.seed, 5, job, attempt, i++))); };
+        double current_t = dist();
+        double cnt = 0;
+        while (current_t <= thickness && cnt < 1e10) {
+            d.push_back(current_t);
+            current_t += dist();
+            cnt++;
+        }
+        if (cnt >= 1e10) { d.clear(); return false; }
+        d.push_back(std::numeric_limits<double>::infinity());
+        return true;
+    };
+    if (c.plasmon_individual <= 0) return table(0, out) && !out.empty();
+    for (uint64_t a = 0; a < 10000000ull; a++)
+        if (table(a, out) && out.size() == (size_t)c.plasmon_individual) return true;
+    out.clear();
+    return false;
+}
+// getScatteringPolar (plasmon.cpp:22-31) then getScatteringAzimuth (:17-20) of event `ev` of job `job`
+static void draw_plasmon_angles(const mslice_config &c, uint64_t job, uint64_t ev, double &polar, double &azimuth) {
+    double rnd = draw_uniform(draw_key(c.seed, 6, job, ev, 0));
+    double crit_2 = c.plasmon_crit_angle * c.plasmon_crit_angle;
+    double char_2 = c.plasmon_char_angle * c.plasmon_char_angle;
+    double ang_2 = char_2 * (std::pow((crit_2 + char_2) / char_2, rnd) - 1);
+    polar = std::sqrt(ang_2);
+    azimuth = 2.0 * M_PI * draw_uniform(draw_key(c.seed, 6, job, ev, 1));
+}
+// Utils::generateRotationAroundVector (vectorutils.cpp:8-19): I + sin a [ax]x + (1 - cos a) [ax]x^2, ax normalised
+static void rotation_about(const double axis[3], double angle, double R[3][3]) {
+    double n = std::sqrt(axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2]);
+    double ax[3] = {axis[0] / n, axis[1] / n, axis[2] / n};
+    double cm[3][3] = {{0.0, -ax[2], ax[1]}, {ax[2], 0.0, -ax[0]}, {-ax[1], ax[0], 0.0}};
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            double cc = cm[i][0] * cm[0][j] + cm[i][1] * cm[1][j] + cm[i][2] * cm[2][j];
+            R[i][j] = (i == j ? 1.0 : 0.0) + cm[i][j] * std::sin(angle) + cc * (1 - std::cos(angle));
+        }
+}
+static void mat_vec(const double R[3][3], double v[3]) {
+    double r[3];
+    for (int i = 0; i < 3; i++) r[i] = R[i][0] * v[0] + R[i][1] * v[1] + R[i][2] * v[2];
+    v[0] = r[0]; v[1] = r[1]; v[2] = r[2];
+}
+// Utils::rotateVectorSpherical (vectorutils.cpp:21-31)
+static void rotate_spherical(double z[3], double y[3], double theta, double phi) {
+    double r_theta[3][3], r_phi[3][3];
+    rotation_about(y, theta, r_theta);
+    rotation_about(z, phi, r_phi);
+    mat_vec(r_theta, z);
+    mat_vec(r_phi, z);
+    mat_vec(r_phi, y);
 }
 
 // Poisson deviate for dose pass `pass`, pixel `pixel`: sequential-search inversion for lam < 10, else
@@ -933,6 +997,84 @@ static void fft_shift(const std::complex<T> *input, std::complex<T> *output, int
         }
 }
 
+// bilinear_translate_d (kernels/bilinear_translate_d.cl:18-77)
+template <class T>
+static void bilinear_translate(const T *input, T *output, int pixel_shift_x, int pixel_shift_y, T subpixel_shift_x,
+                               T subpixel_shift_y, int width, int height) {
+    for (int yid = 0; yid < height; yid++)
+        for (int xid = 0; xid < width; xid++) {
+            int id = xid + width * yid;
+            int new_xid = xid - pixel_shift_x;
+            int new_yid = yid - pixel_shift_y;
+            if (new_xid < 0) new_xid = width + new_xid;
+            else if (new_xid >= width) new_xid = new_xid - width;
+            if (new_yid < 0) new_yid = height + new_yid;
+            else if (new_yid >= height) new_yid = new_yid - height;
+            int new_id = new_xid + width * new_yid;
+            int br_px = new_id;
+            int bl_px = new_id - 1;
+            int tr_px = new_id - width;
+            int tl_px = new_id - width - 1;
+            if (new_xid == 0) { bl_px += width; tl_px += width; }
+            if (new_yid == 0) { tr_px += width * height; tl_px += width * height; }
+            if (new_xid >= 0 && new_xid < width && new_yid >= 0 && new_yid < height) {
+                T f_br = subpixel_shift_x * subpixel_shift_y;
+                T f_bl = ((T)1.0 - subpixel_shift_x) * subpixel_shift_y;
+                T f_tr = subpixel_shift_x * ((T)1.0 - subpixel_shift_y);
+                T f_tl = ((T)1.0 - subpixel_shift_x) * ((T)1.0 - subpixel_shift_y);
+                output[id] = f_tl * input[br_px] + f_tr * input[bl_px] + f_bl * input[tr_px] + f_br * input[tl_px];
+            } else {
+                output[id] = (T)0.0;
+            }
+        }
+}
+
+// |fftshift(recip)|^2 in T (complex_to_real method 4), translated when d_kx or d_ky is nonzero
+// (getDiffractionImage simulationgeneral.cpp:772-806 / getStemPixel simulationstem.cpp:74-103, with
+// translateDiffImage :832-853: shift = d_k / inverseScale pixels, floor and remainder)
+template <class T>
+static void shifted_intensity(const std::complex<T> *recip_wave, int W, int H, double d_kx, double d_ky, double inverse_scale,
+                              std::vector<T> &out) {
+    std::vector<std::complex<T>> sh((size_t)W * H);
+    fft_shift(recip_wave, sh.data(), W, H);
+    std::vector<T> I((size_t)W * H);
+    for (size_t i = 0; i < I.size(); i++) I[i] = sh[i].real() * sh[i].real() + sh[i].imag() * sh[i].imag();
+    out.resize(I.size());
+    if (d_kx != 0.0 || d_ky != 0.0) {
+        double shift_x = d_kx / inverse_scale, shift_y = d_ky / inverse_scale;
+        int int_shift_x = (int)std::floor(shift_x), int_shift_y = (int)std::floor(shift_y);
+        double sub_shift_x = shift_x - int_shift_x, sub_shift_y = shift_y - int_shift_y;
+        bilinear_translate<T>(I.data(), out.data(), int_shift_x, int_shift_y, (T)sub_shift_x, (T)sub_shift_y, W, H);
+    } else {
+        out = I;
+    }
+}
+// getStemPixel on the (translated) pattern: band_pass -> sum_reduction -> host sum (as stem_pixel below)
+template <class T>
+static double stem_pixel_shifted(const std::complex<T> *recip_wave, int W, int H, double angle_scale, const mslice_detector &d,
+                                 double d_kx, double d_ky, double inverse_scale) {
+    std::vector<T> I;
+    shifted_intensity<T>(recip_wave, W, H, d_kx, d_ky, inverse_scale, I);
+    T innerPx = (T)(d.inner / angle_scale), outerPx = (T)(d.outer / angle_scale);
+    T xcPx = (T)(d.xcentre / angle_scale), ycPx = (T)(d.ycentre / angle_scale);
+    unsigned int total = (unsigned int)W * H;
+    unsigned int nGroups = total / 256;
+    double sum = 0;
+    for (unsigned int g = 0; g < nGroups; g++) {
+        T gsum = 0;
+        for (unsigned int i = 0; i < 256; i++) {
+            unsigned int id = g * 256 + i;
+            int xid = (int)(id % W), yid = (int)(id / W);
+            T centX = W / (T)2.0 + xcPx, centY = H / (T)2.0 + ycPx;
+            T radius = std::sqrt((xid - centX) * (xid - centX) + (yid - centY) * (yid - centY));
+            T o = (radius <= outerPx && radius >= innerPx) ? I[id] : (T)0.0;
+            gsum += std::fabs(o);
+        }
+        sum += (double)(gsum * (T)M_SQRT2);
+    }
+    return sum;
+}
+
 // getStemPixel -> complex_to_real(4) -> band_pass -> sum_reduction -> host sum
 // (simulationstem.cpp:42-132, complex_to_real_d.cl:12-37, band_pass_d.cl:15-38, sum_reduction_d.cl:13-35)
 template <class T>
@@ -997,6 +1139,139 @@ struct Sim {
         draw_shift(c, 0, dx, dy);
         frame_x = g.sim_x[0] + dx;
         frame_y = g.sim_y[0] + dy;
+    }
+
+    // ---- plasmon scattering: one job's slice loop (simulationstem.cpp:190-232, simulationcbed.cpp:145-187,
+    // simulationctem.cpp:316-357). The events depend only on the job, so the transmission, propagator and beam of
+    // every slice are planned first, then the job's waves run through them.
+    struct JobPlan {
+        std::vector<const std::vector<std::complex<T>> *> trans;   // the transmission each slice uses
+        std::vector<std::vector<std::complex<T>>> owned;          // those built after an event
+        std::vector<const std::vector<std::complex<T>> *> prop;    // the propagator each slice uses
+        std::vector<std::vector<std::complex<T>>> props;
+        std::vector<std::array<double, 3>> k_out;                 // the beam after slice s's event check
+    };
+    void plan_job(uint64_t job, JobPlan &P) const {
+        const mslice_geometry &g = G.g;
+        const int S = g.n_slices;
+        double k_vec[3] = {0.0, 0.0, g.wavenumber}, y_axis[3] = {0.0, 1.0, 0.0};
+        rotate_spherical(k_vec, y_axis, c.beam_tilt / 1000.0, c.beam_azimuth);
+        std::vector<double> depths;
+        double thk = c.struct_limits[5] - c.struct_limits[4];   // crystalStructure()->limitsZ (main.cpp:712-714)
+        if (!draw_plasmon_depths(c, job, thk, depths)) throw std::runtime_error("Could not generate valid plasmon configuration.");
+        P.trans.assign(S, nullptr);
+        P.prop.assign(S, &prop);
+        P.owned.clear();
+        P.owned.reserve(S);
+        P.props.clear();
+        P.props.reserve(S);
+        P.k_out.assign(S, {0, 0, 0});
+        unsigned int count = 0;
+        bool modified = false;
+        double sx = 0, sy = 0;   // the sub-slice shifts modifyBeamTilt sets (full 3-D)
+        const std::vector<std::complex<T>> *cur_prop = &prop;
+        for (int i = 0; i < S; i++) {
+            if (!modified) {
+                P.trans[i] = &trans[i];
+            } else {   // doMultiSliceStep builds the slice with the arguments set so far (simulationgeneral.cpp:697-729)
+                PotArgs a = pot_args(i);
+                a.shift_x = sx;
+                a.shift_y = sy;
+                std::vector<std::complex<T>> raw(N), tmp(N);
+                P.owned.emplace_back(N);
+                potential_full3d<T>(a, atoms, params.data(), raw.data());
+                fft2<T>(res, res, raw.data(), tmp.data(), -1);
+                band_limit<T>(tmp.data(), res, res, (T)g.k_max, (T)c.inverse_limit_factor, kx.data(), ky.data());
+                fft2<T>(res, res, tmp.data(), P.owned.back().data(), +1);
+                P.trans[i] = &P.owned.back();
+            }
+            P.prop[i] = cur_prop;
+            double current_depth = (i + 1 - g.pre_slices) * g.dz;
+            double next = count < depths.size() ? depths[count] : std::numeric_limits<double>::infinity();
+            if (current_depth >= next) {
+                double p_tilt, p_azimuth;
+                draw_plasmon_angles(c, job, count, p_tilt, p_azimuth);
+                rotate_spherical(k_vec, y_axis, p_tilt / 1000.0, p_azimuth);
+                // modifyBeamTilt (simulationgeneral.cpp:649-679)
+                if (!c.full3d)
+                    throw std::runtime_error("plasmon scattering event with the projected potential: modifyBeamTilt sets "
+                                             "argument 29 of transmission_potentials_projected, which has none");
+                sx = (k_vec[0] / k_vec[2]) * g.dz / c.full3d_integrals;
+                sy = (k_vec[0] / k_vec[2]) * g.dz / c.full3d_integrals;   // kx, as the reference writes it
+                P.props.emplace_back(N);
+                propagator<T>(P.props.back().data(), kx.data(), ky.data(), res, res, (T)g.dz, (T)g.wavenumber, (T)k_vec[0],
+                              (T)k_vec[1], (T)k_vec[2], (T)(g.k_max * c.inverse_limit_factor));
+                cur_prop = &P.props.back();
+                modified = true;
+                count++;
+            }
+            P.k_out[i] = {k_vec[0], k_vec[1], k_vec[2]};
+        }
+    }
+    // the doMultiSliceStep of slice s under a job plan
+    void step_plan(const JobPlan &P, int s, std::vector<std::complex<T>> &real, std::vector<std::complex<T>> &recip_w,
+                   std::vector<std::complex<T>> &tmp) const {
+        const auto &Ts = *P.trans[s];
+        const auto &Ps = *P.prop[s];
+        for (size_t i = 0; i < N; i++) recip_w[i] = cMult(Ts[i], real[i]);
+        fft2<T>(res, res, recip_w.data(), tmp.data(), -1);
+        for (size_t i = 0; i < N; i++) recip_w[i] = cMult(tmp[i], Ps[i]);
+        fft2<T>(res, res, recip_w.data(), real.data(), +1);
+    }
+    // the diffraction image under a plan, after slice s (getDiffractionImage(0, k_vec - orig_k))
+    void diffraction_plan(const JobPlan &P, int s, const std::vector<std::complex<T>> &recip_w, double *out) const {
+        const mslice_geometry &g = G.g;
+        std::vector<T> I;
+        shifted_intensity<T>(recip_w.data(), res, res, P.k_out[s][0] - g.wavevector[0], P.k_out[s][1] - g.wavevector[1],
+                             g.inverse_scale, I);
+        for (size_t i = 0; i < N; i++) out[i] = (double)I[i];
+    }
+    // one STEM probe of job plan P (SimulationStem::simulate's per-pixel work with plasmons)
+    void stem_probe_plan(int pass, int p, const JobPlan &P, double *out) const {
+        const mslice_geometry &g = G.g;
+        int S = g.n_slices, n_out = g.n_outputs, n_det = c.n_detectors;
+        double step_x = (c.stem_area[1] - c.stem_area[0]) / c.stem_pixels_x;
+        double step_y = (c.stem_area[3] - c.stem_area[2]) / c.stem_pixels_y;
+        int x_i = p % c.stem_pixels_x, y_i = (int)std::floor(p / c.stem_pixels_x);
+        double x_pos = c.stem_area[0] + x_i * step_x, y_pos = c.stem_area[2] + y_i * step_y;
+        double df = c.chromatic ? draw_defocus(c, pass, p) : 0.0;
+        std::vector<std::complex<T>> real(N), recip_w(N), tmp(N);
+        probe_k(x_pos, y_pos, recip_w.data(), frame_x0(), frame_y0(), df);
+        fft2<T>(res, res, recip_w.data(), real.data(), +1);
+        int oc = 0;
+        auto out_at = [&](int s) {
+            for (int d = 0; d < n_det; d++)
+                out[(size_t)oc * n_det + d] = stem_pixel_shifted<T>(recip_w.data(), res, res, g.angle_scale, c.detectors[d],
+                                                                    P.k_out[s][0] - g.wavevector[0], P.k_out[s][1] - g.wavevector[1],
+                                                                    g.inverse_scale);
+            oc++;
+        };
+        for (int s = 0; s < S; s++) {
+            step_plan(P, s, real, recip_w, tmp);
+            if (is_output(s)) out_at(s);
+        }
+        if (oc < n_out) out_at(S - 1);
+    }
+    double frame_x0() const { return G.g.sim_x[0]; }
+    double frame_y0() const { return G.g.sim_y[0]; }
+    // STEM with plasmons over pixels[0..n) of pass `pass`: jobs of stem_job_pixels consecutive entries, job
+    // pass * n_jobs + j; adds to acc[(o*n_det + d)*n + i]
+    void stem_pass_plasmon(int pass, const int *pixels, size_t n, double *acc) const {
+        const mslice_geometry &g = G.g;
+        int n_out = g.n_outputs, n_det = c.n_detectors;
+        size_t P_ = (size_t)std::max(1, c.stem_job_pixels);
+        size_t n_jobs = (n + P_ - 1) / P_;
+        for (size_t j = 0; j < n_jobs; j++) {
+            JobPlan P;
+            plan_job((uint64_t)pass * n_jobs + j, P);
+            size_t i0 = j * P_, i1 = std::min(n, i0 + P_);
+            std::vector<double> r((i1 - i0) * n_out * n_det);
+#pragma omp parallel for schedule(dynamic)
+            for (long i = (long)i0; i < (long)i1; i++) stem_probe_plan(pass, pixels[i], P, r.data() + (size_t)(i - i0) * n_out * n_det);
+            for (size_t i = i0; i < i1; i++)
+                for (int o = 0; o < n_out; o++)
+                    for (int d = 0; d < n_det; d++) acc[((size_t)o * n_det + d) * n + i] += r[((i - i0) * n_out + o) * n_det + d];
+        }
     }
 
     PotArgs pot_args(int slice) const {
@@ -1144,17 +1419,21 @@ struct Sim {
         std::vector<double> d(N);
         probe_k(c.cbed_x, c.cbed_y, recip_w.data(), g.sim_x[0], g.sim_y[0], df);
         fft2<T>(res, res, recip_w.data(), real.data(), +1);
+        JobPlan P;
+        if (c.plasmon) plan_job((uint64_t)pass, P);   // a CBED job is one pass (SimulationRunner::SplitJobs)
         int oc = 0;
-        auto out = [&]() {
-            diffraction(recip_w, d.data());
+        auto out = [&](int s) {
+            if (c.plasmon) diffraction_plan(P, s, recip_w, d.data());
+            else diffraction(recip_w, d.data());
             for (size_t i = 0; i < N; i++) acc[(size_t)oc * N + i] += d[i];
             oc++;
         };
         for (int s = 0; s < S; s++) {
-            step_with(slice_set(pass, 0, s, trans), s, real, recip_w, tmp);
-            if (is_output(s)) out();
+            if (c.plasmon) step_plan(P, s, real, recip_w, tmp);
+            else step_with(slice_set(pass, 0, s, trans), s, real, recip_w, tmp);
+            if (is_output(s)) out(s);
         }
-        if (oc < g.n_outputs) out();
+        if (oc < g.n_outputs) out(S - 1);
     }
 
     // staged run over configurations (the engine's mslice_*_run_staged): one pass per configuration, or
@@ -1196,7 +1475,8 @@ struct Sim {
                     build_transmission();
                 }
             }
-            if (c.mode == MSLICE_MODE_STEM) stem_pass(it, pix.data(), n_pix, acc.data());
+            if (c.mode == MSLICE_MODE_STEM && c.plasmon) stem_pass_plasmon(it, pix.data(), n_pix, acc.data());
+            else if (c.mode == MSLICE_MODE_STEM) stem_pass(it, pix.data(), n_pix, acc.data());
             else cbed_pass(it, acc.data());
         }
         for (size_t i = 0; i < tot; i++) out[i] = acc[i] / passes;   // Image::getWeightedSlice
@@ -1252,19 +1532,28 @@ struct Sim {
         std::vector<std::complex<T>> real(N), recip_w(N), tmp(N);
         probe_k(c.cbed_x, c.cbed_y, recip_w.data());
         fft2<T>(res, res, recip_w.data(), real.data(), +1);
+        JobPlan P;
+        if (c.plasmon) plan_job(0, P);
         int oc = 0;
+        auto out = [&](int s) {
+            if (c.plasmon) diffraction_plan(P, s, recip_w, diff + (size_t)oc * N);
+            else diffraction(recip_w, diff + (size_t)oc * N);
+            oc++;
+        };
         for (int s = 0; s < S; s++) {
-            step(s, real, recip_w, tmp);
-            if (is_output(s)) { diffraction(recip_w, diff + (size_t)oc * N); oc++; }
+            if (c.plasmon) step_plan(P, s, real, recip_w, tmp);
+            else step(s, real, recip_w, tmp);
+            if (is_output(s)) out(s);
         }
-        if (oc < g.n_outputs) diffraction(recip_w, diff + (size_t)oc * N);
+        if (oc < g.n_outputs) out(S - 1);
     }
 
     void ctem_outputs(const std::vector<std::complex<T>> &real, const std::vector<std::complex<T>> &recip_w, int oc,
-                      double *ew, double *diff, double *image) {
+                      double *ew, double *diff, double *image, const JobPlan *P = nullptr, int s = 0) {
         const mslice_geometry &g = G.g;
         if (ew) for (size_t i = 0; i < N; i++) { ew[(size_t)oc * 2 * N + 2 * i] = real[i].real(); ew[(size_t)oc * 2 * N + 2 * i + 1] = real[i].imag(); }
-        if (diff) diffraction(recip_w, diff + (size_t)oc * N);
+        if (diff && P) diffraction_plan(*P, s, recip_w, diff + (size_t)oc * N);
+        else if (diff) diffraction(recip_w, diff + (size_t)oc * N);
         if (image && c.ctem_image) {
             // simulateImagePerfect (simulationctem.cpp:114-166)
             std::vector<std::complex<T>> im(N), tmp(N);
@@ -1293,12 +1582,16 @@ struct Sim {
         const mslice_geometry &g = G.g;
         int S = g.n_slices;
         std::vector<std::complex<T>> real(N, std::complex<T>(1, 0)), recip_w(N), tmp(N);   // init_plane_wave value 1.0
+        JobPlan P;
+        if (c.plasmon) plan_job(0, P);
+        const JobPlan *pp = c.plasmon ? &P : nullptr;
         int oc = 0;
         for (int s = 0; s < S; s++) {
-            step(s, real, recip_w, tmp);
-            if (is_output(s)) { ctem_outputs(real, recip_w, oc, ew, diff, image); oc++; }
+            if (c.plasmon) step_plan(P, s, real, recip_w, tmp);
+            else step(s, real, recip_w, tmp);
+            if (is_output(s)) { ctem_outputs(real, recip_w, oc, ew, diff, image, pp, s); oc++; }
         }
-        if (oc < g.n_outputs) ctem_outputs(real, recip_w, oc, ew, diff, image);
+        if (oc < g.n_outputs) ctem_outputs(real, recip_w, oc, ew, diff, image, pp, S - 1);
     }
 };
 
@@ -1434,6 +1727,11 @@ int orc_stem_run(OrcSim *s, const int *pixels, size_t n_pix, double *out) {
             int n_out = S->G.g.n_outputs, n_det = S->c.n_detectors;
             std::vector<double> tmp((size_t)n_out * n_det);
             std::vector<double> res((size_t)n_out * n_det * n_pix, 0.0);
+            if (S->c.plasmon) {   // jobs of consecutive entries of the pixel list, pass 0
+                S->stem_pass_plasmon(0, pixels, n_pix, res.data());
+                std::copy(res.begin(), res.end(), out);
+                return;
+            }
 #pragma omp parallel for schedule(dynamic)
             for (long i = 0; i < (long)n_pix; i++) {
                 std::vector<double> one((size_t)n_out * n_det);
@@ -1453,6 +1751,23 @@ int orc_cbed_run(OrcSim *s, double *diff) {
 
 int orc_ctem_run(OrcSim *s, double *ew, double *diff, double *image) {
     return guard([&] { if (s->dp) s->sd->ctem(ew, diff, image); else s->sf->ctem(ew, diff, image); });
+}
+
+// bilinear_translate_d restated (FP64), for the pin against the reference's kernel
+int orc_k_bilinear_translate(const double *in, double *out, int ix, int iy, double sx, double sy, int w, int h) {
+    return guard([&] { bilinear_translate<double>(in, out, ix, iy, sx, sy, w, h); });
+}
+
+// the seeded plasmon depths of job `job` (NaN-free; +inf closes the table): n_out entries written, at most cap
+int orc_plasmon_depths(const mslice_config *c, unsigned long long job, double thickness, double *out, size_t cap,
+                       size_t *n_out) {
+    return guard([&] {
+        std::vector<double> d;
+        if (!draw_plasmon_depths(*c, job, thickness, d)) throw std::runtime_error("Could not generate valid plasmon configuration.");
+        if (d.size() > cap) throw std::invalid_argument("depth capacity too small");
+        std::copy(d.begin(), d.end(), out);
+        *n_out = d.size();
+    });
 }
 
 // standalone building blocks for KATs

@@ -21,7 +21,8 @@ def lib():
     global _lib
     if _lib is None:
         _lib = C.CDLL(LIB_PATH)
-        for name in ("ref_atom_sort_d", "ref_band_limit_d", "ref_band_pass_d", "ref_complex_multiply_d",
+        for name in ("ref_atom_sort_d", "ref_band_limit_d", "ref_band_pass_d", "ref_bilinear_translate_d",
+                     "ref_complex_multiply_d",
                      "ref_complex_to_real_d", "ref_fft_shift_d", "ref_init_plane_wave_d", "ref_init_probe_wave_d",
                      "ref_ctem_image_d", "ref_propagator_d", "ref_sqabs_d", "ref_sum_reduction_d",
                      "ref_transmission_projected_d", "ref_transmission_full3d_d"):
@@ -30,6 +31,7 @@ def lib():
                                                                                         C.c_double, C.c_int]
         _lib.ref_band_limit_d.argtypes = [_dp, C.c_uint, C.c_uint, C.c_double, C.c_double, _dp, _dp]
         _lib.ref_band_pass_d.argtypes = [_dp, _dp, C.c_uint, C.c_uint] + [C.c_double] * 4
+        _lib.ref_bilinear_translate_d.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_uint, C.c_uint]
         _lib.ref_fft_shift_d.argtypes = [_dp, _dp, C.c_uint, C.c_uint]
         _lib.ref_complex_to_real_d.argtypes = [_dp, _dp, C.c_int, C.c_uint, C.c_uint]
         _lib.ref_sum_reduction_d.argtypes = [_dp, _dp, C.c_uint]

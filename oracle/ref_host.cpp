@@ -22,6 +22,9 @@ namespace ref_band_limit {
 namespace ref_band_pass {
 #include "band_pass_d.inc"
 }
+namespace ref_bilinear_translate {
+#include "bilinear_translate_d.inc"
+}
 namespace ref_complex_multiply {
 #include "complex_multiply_d.inc"
 }
@@ -115,6 +118,10 @@ void ref_band_limit_d(double *io, unsigned w, unsigned h, double k_max, double f
 
 void ref_band_pass_d(const double *in, double *out, unsigned w, unsigned h, double inner, double outer, double xc, double yc) {
     ndrange(w, h, [&] { ref_band_pass::band_pass_d(in, out, w, h, inner, outer, xc, yc); });
+}
+
+void ref_bilinear_translate_d(const double *in, double *out, int ix, int iy, double sx, double sy, unsigned w, unsigned h) {
+    ndrange(w, h, [&] { ref_bilinear_translate::bilinear_translate_d((double *)in, out, ix, iy, sx, sy, w, h); });
 }
 
 void ref_complex_multiply_d(double *a, double *b, double *out, unsigned w, unsigned h) {
