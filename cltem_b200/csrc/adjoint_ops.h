@@ -24,6 +24,8 @@ struct GradSlices {
     int start[kGradMaxSlices + 1];
     int n;
     size_t stride;
+    // beam tilt of the projected potential: rho^2 = r^2 - tilt_s2 (r . (cphi, sphi))^2 (0: untilted)
+    double tilt_s2 = 0, cphi = 1, sphi = 0;
 };
 // per-atom gradients (x, y) of the atoms of the slices in sl (sorted order) from gV of their slice (gather.cu);
 // T is the precision of the per-pixel terms and of prm (the parameterisation table). tabp (FP32 only, may be

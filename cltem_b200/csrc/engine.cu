@@ -405,6 +405,7 @@ template <class T> struct DevBuf {
 struct SimBase {
     Ctx *ctx;
     mslice_config cfg;
+    bool adj_valid = false;   // the state of the last adjoint forward is intact (Sim::ctem_forward)
     HostGeom H;
     std::atomic<bool> cancel{false};
     mslice_progress_cb progress = nullptr;
@@ -479,13 +480,18 @@ struct SimBase {
     virtual void ctem_run(double *ew, double *diff, double *image) = 0;
     virtual void stage(int n_configs, const size_t *counts, const int *Z, const double *x, const double *y, const double *z) = 0;
     virtual void run_staged(int mode) = 0;
+    virtual void run_staged_async() = 0;
+    virtual void wait_run() = 0;
     virtual void staged_result(double *out, size_t cap) = 0;
     virtual void stem_plain(const int *pixels, size_t n, double *out) = 0;
     virtual void ctem_loss_grad(const double *target, double *loss, double *gxyz, double *g10, double *g30, int ck,
                                 bool want_grad) = 0;
+    virtual void ctem_loss_forward(const double *target, double *loss, int ck, unsigned long long *token) = 0;
+    virtual void ctem_loss_backward(unsigned long long token, double *gxyz, double *g10, double *g30) = 0;
     virtual void set_c10_c30(double c10, double c30) = 0;
     virtual void tune_batch(const int *cands, int n, int reps, int *best, double *rate) = 0;
     virtual void set_step_variant(int col, int row) = 0;
+    virtual std::string step_variant_name(int which, int index) = 0;
     virtual void get_tuning(int *batch, int *col, int *n_col, int *row, int *n_row) = 0;
     virtual void set_ccd(const double *dqe, const double *ntf, size_t n, int binning, double dose) = 0;
 };
@@ -633,6 +639,8 @@ struct Sim : SimBase {
         MS_CUDA(cudaStreamSynchronize(st()));
     }
     ~Sim() override {
+        if (run_in_flight) cudaStreamSynchronize(st());
+        release_run_graph();
         drop_graphs();
         for (auto e : ev) if (e) cudaEventDestroy(e);
     }
@@ -1091,6 +1099,8 @@ struct Sim : SimBase {
     void drop_graphs() {
         for (auto &gr : graphs) release(gr);
         graphs.clear();
+        if (run_in_flight) cudaStreamSynchronize(st());
+        release_run_graph();
     }
 
     // Propagate `nb` STEM probes through all slices: probe i at hpos[i] (Å, in the frame of its transmission
@@ -1163,12 +1173,16 @@ struct Sim : SimBase {
         for (auto &p : gr->events) pending.push_back({p.kind, p.a, p.b, p.bytes, true});
     }
 
-    void enqueue_batch(int nb, int n_pix, double *out, double *comp, const int *sel, const double *df) {
+    // positions (pos_d) and output pixel indices (pix_d) of the batch's waves: the batch arrays unless given
+    void enqueue_batch(int nb, int n_pix, double *out, double *comp, const int *sel, const double *df,
+                       const double2 *pos_d = nullptr, const int *pix_d = nullptr) {
         const mslice_geometry &g = H.g;
         const cplx<R> *tw = ctx->twiddles<R>(N);
         const size_t set_stride = (size_t)g.n_slices * NN;
+        if (!pos_d) pos_d = pos.p;
+        if (!pix_d) pix_d = pix.p;
         timed(st(), MSLICE_K_PROBE, (double)nb * NN * (sizeof(C) + sizeof(double2)), [&] {
-            ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos.p, (R)(s2d * N), df, g.wavelength);
+            ops.col_probe(st(), wave.p, nb, tw, chi.p, kx.p, ky.p, pos_d, (R)(s2d * N), df, g.wavelength);
         });
         ctx->launches++;
         PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p, ctx->step_err, pxe.p, pye.p};
@@ -1188,7 +1202,7 @@ struct Sim : SimBase {
             });
             ctx->launches += 2;
             if (is_out) {
-                detector_reduce(st(), partials.p, tiles_lo + tiles_hi, cfg.n_detectors, nb, pix.p, n_pix, (int)oi, out, comp);
+                detector_reduce(st(), partials.p, tiles_lo + tiles_hi, cfg.n_detectors, nb, pix_d, n_pix, (int)oi, out, comp);
                 ctx->launches++;
                 oi++;
             }
@@ -1578,8 +1592,163 @@ struct Sim : SimBase {
         n_configs = nc;
     }
 
+    // ---- a whole staged STEM run as one CUDA graph -------------------------------------------------------
+    // With the static frame, one transmission set, no plasmons and no progress callback, the launch sequence of
+    // a staged run (per pass: binning of the pass's configuration, its transmission build, then every probe
+    // batch) depends only on the staged layout and the buffers: the positions of all scan pixels (and the
+    // chromatic defocus of every pass) are uploaded first, the run is captured once into a graph, and every run
+    // of the same layout is one cudaGraphLaunch. The graph keeps its own timing events when profiling is on.
+    struct RunGraph {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<uintptr_t> key;
+        std::vector<Pending> events;   // owned by the graph
+        unsigned long long nodes = 0;
+    } run_graph;
+    DevBuf<double2> run_pos;   // probe position of every scan pixel (static frame)
+    DevBuf<int> run_pix;       // 0..n_pix-1
+    DevBuf<double> run_dfac;   // chromatic defocus factor of every (pass, pixel)
+    bool async_run = false;    // mslice_stem_run_staged_async: launch and return
+    bool run_in_flight = false;
+    int run_passes = 0;
+    bool run_graph_ok() const {
+        return use_graphs && cfg.mode == MSLICE_MODE_STEM && cfg.mixed_static <= 1 && !cfg.stem_moving_frame &&
+               !cfg.plasmon && progress == nullptr;
+    }
+    void release_run_graph() {
+        if (run_graph.exec) cudaGraphExecDestroy(run_graph.exec);
+        pending.erase(std::remove_if(pending.begin(), pending.end(),
+                                     [&](const Pending &p) {
+                                         return p.graph_owned &&
+                                                std::any_of(run_graph.events.begin(), run_graph.events.end(),
+                                                            [&](const Pending &q) { return q.a == p.a; });
+                                     }),
+                      pending.end());
+        for (auto &p : run_graph.events) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+        run_graph = RunGraph();
+    }
+    // the whole run's launches (pass = binning + build + every batch), for capture
+    void enqueue_run(int passes, int np) {
+        const mslice_geometry &g = H.g;
+        const bool chrom = cfg.chromatic != 0;
+        for (int it = 0; it < passes; it++) {
+            const int c = it % n_configs;
+            sort_device(sZ.p + cfg_offsets[c], sx.p + cfg_offsets[c], sy.p + cfg_offsets[c], sz.p + cfg_offsets[c],
+                        cfg_counts[c]);
+            double dx, dy;
+            source_shift(it, dx, dy);
+            build_set(0, g.sim_x[0] + dx, g.sim_y[0] + dy);
+            for (int b0 = 0; b0 < np; b0 += batch_cap) {
+                const int nb = std::min(batch_cap, np - b0);
+                enqueue_batch(nb, np, acc.p, comp.p, nullptr, chrom ? run_dfac.p + (size_t)it * np + b0 : nullptr,
+                              run_pos.p + b0, run_pix.p + b0);
+            }
+        }
+    }
+    void launch_run_graph(int passes, int np) {
+        const bool chrom = cfg.chromatic != 0;
+        // per-pixel (and per-pass) inputs of every batch, uploaded before the capture
+        run_pos.ensure(ctx, np);
+        run_pix.ensure(ctx, np);
+        std::vector<double2> hp(np);
+        std::vector<int> hi(np);
+        for (int i = 0; i < np; i++) { hp[i] = probe_pos(i); hi[i] = i; }
+        MS_CUDA(cudaMemcpyAsync(run_pos.p, hp.data(), np * sizeof(double2), cudaMemcpyHostToDevice, st()));
+        MS_CUDA(cudaMemcpyAsync(run_pix.p, hi.data(), np * sizeof(int), cudaMemcpyHostToDevice, st()));
+        std::vector<double> hd;
+        if (chrom) {
+            run_dfac.ensure(ctx, (size_t)passes * np);
+            hd.resize((size_t)passes * np);
+            for (int it = 0; it < passes; it++) {
+                fill_defocus(it, hi.data(), np);
+                std::copy(h_dfac.begin(), h_dfac.end(), hd.begin() + (size_t)it * np);
+            }
+            MS_CUDA(cudaMemcpyAsync(run_dfac.p, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice, st()));
+        }
+        MS_CUDA(cudaStreamSynchronize(st()));   // the host staging vectors go out of scope
+        std::vector<uintptr_t> key = {(uintptr_t)acc.p, (uintptr_t)comp.p, (uintptr_t)wave.p, (uintptr_t)trans.p,
+                                      (uintptr_t)partials.p, (uintptr_t)sZ.p, (uintptr_t)sx.p, (uintptr_t)sy.p,
+                                      (uintptr_t)sz.p, (uintptr_t)run_pos.p, (uintptr_t)run_pix.p,
+                                      (uintptr_t)(chrom ? run_dfac.p : nullptr), (uintptr_t)passes, (uintptr_t)np,
+                                      (uintptr_t)n_configs, (uintptr_t)batch_cap, (uintptr_t)prof,
+                                      (uintptr_t)col_variant, (uintptr_t)row_variant};
+        for (int c = 0; c < n_configs; c++) { key.push_back(cfg_offsets[c]); key.push_back(cfg_counts[c]); }
+        if (!run_graph.exec || key != run_graph.key) {
+            release_run_graph();
+            (void)ctx->twiddles<R>(N);   // allocated on first use: never inside the capture
+            const size_t p0 = pending.size();
+            const unsigned long long l0 = ctx->launches;
+            cudaGraph_t graph = nullptr;
+            MS_CUDA(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue_run(passes, np);
+            } catch (...) {
+                cudaStreamEndCapture(st(), &graph);
+                if (graph) cudaGraphDestroy(graph);
+                for (size_t i = p0; i < pending.size(); i++) { cudaEventDestroy(pending[i].a); cudaEventDestroy(pending[i].b); }
+                pending.resize(p0);
+                ctx->launches = l0;
+                throw;
+            }
+            MS_CUDA(cudaStreamEndCapture(st(), &graph));
+            cudaError_t e = cudaGraphInstantiate(&run_graph.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            run_graph.events.assign(pending.begin() + p0, pending.end());
+            pending.resize(p0);
+            if (e != cudaSuccess) {
+                for (auto &p : run_graph.events) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+                run_graph = RunGraph();
+                MS_CUDA(e);
+            }
+            run_graph.nodes = ctx->launches - l0;
+            ctx->launches = l0;
+            run_graph.key = key;
+        }
+        if (!run_graph.events.empty()) {   // a replay re-records the graph's events: read the previous replay first
+            const cudaEvent_t first = run_graph.events[0].a;
+            if (std::any_of(pending.begin(), pending.end(), [&](const Pending &p) { return p.a == first; })) {
+                MS_CUDA(cudaStreamSynchronize(st()));
+                flush_profile();
+            }
+        }
+        MS_CUDA(cudaEventRecord(ev[2], st()));
+        MS_CUDA(cudaGraphLaunch(run_graph.exec, st()));
+        MS_CUDA(cudaEventRecord(ev[3], st()));
+        ctx->launches += run_graph.nodes;
+        for (auto &p : run_graph.events) pending.push_back({p.kind, p.a, p.b, p.bytes, true});
+        trans_built = true;
+        run_in_flight = true;
+    }
+    // wait for a graph run, then its timing, error word, profile and pass count
+    void finish_run() {
+        if (!run_in_flight) return;
+        run_in_flight = false;
+        MS_CUDA(cudaEventSynchronize(ev[3]));
+        check_step_err();
+        flush_profile();
+        float tot = 0;
+        MS_CUDA(cudaEventElapsedTime(&tot, ev[2], ev[3]));
+        timing[0] = -1.0;   // one graph: the build / propagation split is not timed
+        timing[1] = -1.0;
+        timing[2] = tot;
+        acc_configs = run_passes;
+    }
+
+    // launch a staged STEM run and return: one graph launch when run_graph_ok(), else the synchronous run
+    void run_staged_async() override {
+        async_run = true;
+        try {
+            run_staged(MSLICE_MODE_STEM);
+        } catch (...) {
+            async_run = false;
+            throw;
+        }
+        async_run = false;
+    }
+    void wait_run() override { finish_run(); }
+
     void run_staged(int mode) override {
         if (n_configs < 1) throw StateError("no configurations staged (mslice_stage_configs)");
+        finish_run();   // a run still in flight owns the accumulators
         if (mode != cfg.mode) throw StateError("staged run of the wrong mode");
         const mslice_geometry &g = H.g;
         const int np = cfg.stem_pixels_x * cfg.stem_pixels_y;
@@ -1597,6 +1766,13 @@ struct Sim : SimBase {
         const int K = cfg.mixed_static > 1 ? cfg.mixed_static : 1;
         if (K > 1 && n_configs < K) throw StateError("mixed static potentials need mixed_static staged configurations");
         const int passes = K > 1 ? std::max(1, cfg.iterations) : (cfg.iterations > 0 ? cfg.iterations : n_configs);
+        if (mode == MSLICE_MODE_STEM && run_graph_ok()) {   // every pass and batch in one graph launch
+            check_cancel();
+            launch_run_graph(passes, np);
+            run_passes = passes;
+            if (!async_run) finish_run();
+            return;
+        }
         float t_build = 0, t_prop = 0;
         MS_CUDA(cudaEventRecord(ev[2], st()));
         if (K > 1) {
@@ -1654,6 +1830,7 @@ struct Sim : SimBase {
     }
 
     void staged_result(double *out, size_t cap) override {
+        finish_run();
         if (acc_configs < 1) throw StateError("no staged run");
         if (cap < acc_n) throw ArgError("output capacity too small");
         MS_CUDA(cudaStreamSynchronize(st()));
@@ -1763,6 +1940,16 @@ struct Sim : SimBase {
         col_variant = col;
         row_variant = row;
     }
+    std::string step_variant_name(int which, int index) override {
+        if (which == 0) {
+            if (index < 0 || index >= ops.col_variants) throw ArgError("column step variant out of range");
+            return ops.col_variant_name ? ops.col_variant_name(index) : std::string();
+        }
+        if (which != 1 || index < 0 || index >= ops.row_variants) throw ArgError("row step variant out of range");
+        static const char *names[3] = {"plain", "L2 prefetch of the rows one grid residency ahead",
+                                       "L2 prefetch of the rows two grid residencies ahead"};
+        return names[index];
+    }
     void get_tuning(int *batch, int *col, int *n_col, int *row, int *n_row) override {
         if (batch) *batch = default_batch();
         if (col) *col = col_variant;
@@ -1779,13 +1966,17 @@ struct Sim : SimBase {
     }
 
     // ---- differentiable CTEM -------------------------------------------------------------
-    void ctem_loss_grad(const double *target, double *loss, double *gxyz, double *g10, double *g30, int ck,
-                        bool want_grad) override {
+    // The adjoint's forward half: the loss and, with want_grad, the checkpoints and state its backward half
+    // reads. Any other call on the simulation in between invalidates that state (adj_valid).
+    unsigned long long adj_token = 0;
+    int adj_c = 1, adj_nck = 1, adj_nred = 0;
+    void ctem_forward(const double *target, double *loss, int ck, bool want_grad) {
+        adj_valid = false;
         const mslice_geometry &g = H.g;
         if (cfg.mode != MSLICE_MODE_CTEM) throw StateError("the image loss needs a CTEM simulation");
         if (cfg.full3d) throw Unsupported("gradients are implemented for the projected potential");
-        if (cfg.beam_tilt != 0.0) throw Unsupported("gradients are implemented without beam tilt");
         if (cfg.mixed_static > 1) throw Unsupported("gradients are implemented without mixed static potentials");
+        if (cfg.plasmon) throw Unsupported("gradients are implemented without plasmon scattering");
         if (!atoms_set) throw StateError("atoms not set");
         const int S = g.n_slices;
         const int c = ck <= 0 ? (int)std::ceil(std::sqrt((double)S)) : std::min(ck, S);
@@ -1831,15 +2022,35 @@ struct Sim : SimBase {
         ops.col_fft(st(), w1.p, w1.p, 1, tw, (R)s2d, +1);
         image_loss<R>(st(), NN, w1.p, tgt.p, w2.p, part.p);
         ctx->launches += 4;
-        std::vector<double> hp(3 * (size_t)nred);
-        if (!want_grad) {
-            MS_CUDA(cudaMemcpyAsync(hp.data(), part.p, nred * sizeof(double), cudaMemcpyDeviceToHost, st()));
-            MS_CUDA(cudaStreamSynchronize(st()));
-            double L = 0;
-            for (int i = 0; i < nred; i++) L += hp[i];
-            if (loss) *loss = L;
-            return;
+        std::vector<double> hp((size_t)nred);
+        MS_CUDA(cudaMemcpyAsync(hp.data(), part.p, nred * sizeof(double), cudaMemcpyDeviceToHost, st()));
+        MS_CUDA(cudaStreamSynchronize(st()));
+        double L = 0;
+        for (int i = 0; i < nred; i++) L += hp[i];
+        if (loss) *loss = L;
+        if (want_grad) {
+            adj_c = c;
+            adj_nck = n_ck;
+            adj_nred = nred;
+            adj_token++;
+            adj_valid = true;
         }
+    }
+
+    // The backward half: dL/dxyz, dL/dC10, dL/dC30 from the state of the last ctem_forward with want_grad.
+    void ctem_backward(double *gxyz, double *g10, double *g30) {
+        if (!adj_valid) throw StateError("no forward state for the adjoint (run mslice_ctem_loss_forward; any other call on "
+                                         "the simulation in between invalidates it)");
+        adj_valid = false;
+        const mslice_geometry &g = H.g;
+        const int S = g.n_slices;
+        const int c = adj_c, n_ck = adj_nck, nred = adj_nred;
+        const cplx<R> *tw = ctx->twiddles<R>(N);
+        const R a = (R)(1.0 / N), b = (R)(s2d * s2d * N), ds = (R)s2d;
+        const int all_tiles = N / ops.cols_per_tile;
+        PropTables<R> pt{px.p, py.p, kx2.p, ky2.p, k_prop * k_prop, ycut.p, ctx->step_err, pxe.p, pye.p};
+        DetArgs nodet{detmask.p, 0, partials.p};
+        std::vector<double> hp(3 * (size_t)nred);
         // G_Y = s2d D(G_W); G_Recip = conj(H) G_Y and dL/dC10, dL/dC30
         ops.row_fft(st(), w2.p, w2.p, 1, tw, (R)1, -1);
         ops.col_fft(st(), w2.p, w2.p, 1, tw, (R)s2d, -1);
@@ -1893,6 +2104,10 @@ struct Sim : SimBase {
                 GradSlices gs{};
                 gs.n = std::min(kGradMaxSlices, m - t0);
                 gs.stride = NN;
+                // the projected kernel's tilt-corrected radius: rho^2 = r^2 - sin^2(tilt) (r . e_phi)^2
+                gs.tilt_s2 = std::sin(cfg.beam_tilt / 1000.0) * std::sin(cfg.beam_tilt / 1000.0);
+                gs.cphi = std::cos(cfg.beam_azimuth);
+                gs.sphi = std::sin(cfg.beam_azimuth);
                 for (int i = 0; i <= gs.n; i++) gs.start[i] = hbs[(size_t)(s0 + t0 + i) * nb];
                 atom_grad<R>(st(), gs, axs.p, ays.p, aZs.p, gV.p + (size_t)t0 * NN, N, g.sim_x[0], g.sim_y[0],
                              g.real_scale, ctx->params.form, params_dev(), ctx->params.i_count, ctx->potp_tab, gxy.p,
@@ -1906,9 +2121,8 @@ struct Sim : SimBase {
         MS_CUDA(cudaMemcpyAsync(hg.data(), gxy.p, hg.size() * sizeof(double), cudaMemcpyDeviceToHost, st()));
         if (n_atoms) MS_CUDA(cudaMemcpyAsync(hidx.data(), idx_out.p, n_atoms * sizeof(int), cudaMemcpyDeviceToHost, st()));
         MS_CUDA(cudaStreamSynchronize(st()));
-        double L = 0, d10 = 0, d30 = 0;
-        for (int i = 0; i < nred; i++) { L += hp[i]; d10 += hp[nred + i]; d30 += hp[2 * nred + i]; }
-        if (loss) *loss = L;
+        double d10 = 0, d30 = 0;
+        for (int i = 0; i < nred; i++) { d10 += hp[nred + i]; d30 += hp[2 * nred + i]; }
         if (g10) *g10 = d10;
         if (g30) *g30 = d30;
         if (gxyz) {
@@ -1919,6 +2133,21 @@ struct Sim : SimBase {
                 gxyz[3 * (size_t)o + 1] = hg[2 * (size_t)i + 1];
             }
         }
+    }
+
+    void ctem_loss_grad(const double *target, double *loss, double *gxyz, double *g10, double *g30, int ck,
+                        bool want_grad) override {
+        ctem_forward(target, loss, ck, want_grad);
+        if (want_grad) ctem_backward(gxyz, g10, g30);
+    }
+    void ctem_loss_forward(const double *target, double *loss, int ck, unsigned long long *token) override {
+        ctem_forward(target, loss, ck, true);
+        if (token) *token = adj_token;
+    }
+    void ctem_loss_backward(unsigned long long token, double *gxyz, double *g10, double *g30) override {
+        if (!adj_valid || token != adj_token)
+            throw StateError("the forward state of this adjoint is gone: another forward or run used the simulation since");
+        ctem_backward(gxyz, g10, g30);
     }
 
     void stem_plain(const int *pixels, size_t n, double *out) override {
@@ -2144,6 +2373,7 @@ int mslice_set_atoms(mslice_sim *sim, const int *Z, const double *x, const doubl
     return guarded([&] {
         need(sim && (n == 0 || (Z && x && y && z)), "null argument");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->set_atoms(Z, x, y, z, n, true);
     });
 }
@@ -2161,6 +2391,7 @@ int mslice_build_transmission(mslice_sim *sim) {
     return guarded([&] {
         need(sim != nullptr, "sim is null");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->build_transmission();
         MS_CUDA(cudaStreamSynchronize(sim->ctx->impl.stream));
     });
@@ -2170,6 +2401,7 @@ int mslice_get_transmission(mslice_sim *sim, int slice, int band_limited, double
     return guarded([&] {
         need(sim && out, "null argument");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->get_transmission(slice, band_limited, out);
     });
 }
@@ -2186,6 +2418,7 @@ int mslice_get_probe(mslice_sim *sim, double x, double y, double *out) {
     return guarded([&] {
         need(sim && out, "null argument");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->get_probe(x, y, out);
     });
 }
@@ -2194,6 +2427,7 @@ int mslice_stem_run(mslice_sim *sim, const int *pixels, size_t n_pixels, double 
     return guarded([&] {
         need(sim && (n_pixels == 0 || (pixels && out)), "null argument");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->stem_run(pixels, n_pixels, out);
     });
 }
@@ -2202,6 +2436,7 @@ int mslice_cbed_run(mslice_sim *sim, double *diff) {
     return guarded([&] {
         need(sim && diff, "null argument");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->cbed_run(diff);
     });
 }
@@ -2210,6 +2445,7 @@ int mslice_ctem_run(mslice_sim *sim, double *ew, double *diff, double *image) {
     return guarded([&] {
         need(sim != nullptr, "sim is null");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->ctem_run(ew, diff, image);
     });
 }
@@ -2228,6 +2464,7 @@ int mslice_tune_batch(mslice_sim *sim, const int *candidates, int n_candidates, 
     return guarded([&] {
         need(sim != nullptr, "sim is null");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->tune_batch(candidates, candidates ? n_candidates : 1, reps, best_batch, waves_per_second);
     });
 }
@@ -2236,7 +2473,18 @@ int mslice_set_step_variant(mslice_sim *sim, int col_variant, int row_variant) {
     return guarded([&] {
         need(sim != nullptr, "sim is null");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->set_step_variant(col_variant, row_variant);
+    });
+}
+
+int mslice_step_variant_name(mslice_sim *sim, int which, int index, char *buf, size_t cap) {
+    return guarded([&] {
+        need(sim && buf && cap > 0, "null argument");
+        const std::string nm = sim->impl->step_variant_name(which, index);
+        const size_t n = std::min(nm.size(), cap - 1);
+        std::memcpy(buf, nm.data(), n);
+        buf[n] = 0;
     });
 }
 
@@ -2252,6 +2500,7 @@ int mslice_set_ccd(mslice_sim *sim, const double *dqe, const double *ntf, size_t
     return guarded([&] {
         need(sim != nullptr && (n == 0 || (dqe != nullptr && ntf != nullptr)), "null argument");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->set_ccd(dqe, ntf, n, binning, dose);
     });
 }
@@ -2260,7 +2509,26 @@ int mslice_set_c10_c30(mslice_sim *sim, double c10, double c30) {
     return guarded([&] {
         need(sim != nullptr, "sim is null");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->set_c10_c30(c10, c30);
+    });
+}
+
+int mslice_ctem_loss_forward(mslice_sim *sim, const double *target, double *loss, int checkpoint_every,
+                             unsigned long long *token) {
+    return guarded([&] {
+        need(sim && target, "null argument");
+        use_device(sim->ctx);
+        sim->impl->ctem_loss_forward(target, loss, checkpoint_every, token);
+    });
+}
+
+int mslice_ctem_loss_backward(mslice_sim *sim, unsigned long long token, double *grad_xyz, double *grad_c10,
+                              double *grad_c30) {
+    return guarded([&] {
+        need(sim != nullptr, "null argument");
+        use_device(sim->ctx);
+        sim->impl->ctem_loss_backward(token, grad_xyz, grad_c10, grad_c30);
     });
 }
 
@@ -2268,6 +2536,7 @@ int mslice_ctem_loss(mslice_sim *sim, const double *target, double *loss) {
     return guarded([&] {
         need(sim && target, "null argument");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->ctem_loss_grad(target, loss, nullptr, nullptr, nullptr, 0, false);
     });
 }
@@ -2277,6 +2546,7 @@ int mslice_stage_configs(mslice_sim *sim, int n_configs, const size_t *counts, c
     return guarded([&] {
         need(sim && counts && n_configs > 0, "null argument");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->stage(n_configs, counts, Z, x, y, z);
     });
 }
@@ -2285,6 +2555,7 @@ int mslice_stem_run_staged(mslice_sim *sim) {
     return guarded([&] {
         need(sim != nullptr, "sim is null");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->run_staged(MSLICE_MODE_STEM);
     });
 }
@@ -2293,7 +2564,26 @@ int mslice_cbed_run_staged(mslice_sim *sim) {
     return guarded([&] {
         need(sim != nullptr, "sim is null");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->run_staged(MSLICE_MODE_CBED);
+    });
+}
+
+int mslice_stem_run_staged_async(mslice_sim *sim) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
+        if (sim->impl->cfg.mode != MSLICE_MODE_STEM) throw ms::StateError("simulation is not in STEM mode");
+        sim->impl->run_staged_async();
+    });
+}
+
+int mslice_sim_wait(mslice_sim *sim) {
+    return guarded([&] {
+        need(sim != nullptr, "sim is null");
+        use_device(sim->ctx);
+        sim->impl->wait_run();
     });
 }
 
@@ -2310,6 +2600,7 @@ int mslice_stem_simulate(mslice_sim *sim, int n_configs, const size_t *counts, c
     return guarded([&] {
         need(sim && counts && out && n_configs > 0, "null argument");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->stage(n_configs, counts, Z, x, y, z);
         sim->impl->run_staged(MSLICE_MODE_STEM);
         sim->impl->staged_result(out, cap);
@@ -2320,6 +2611,7 @@ int mslice_stem_run_plain(mslice_sim *sim, const int *pixels, size_t n_pixels, d
     return guarded([&] {
         need(sim && (n_pixels == 0 || (pixels && out)), "null argument");
         use_device(sim->ctx);
+        sim->impl->adj_valid = false;   // the adjoint's forward state is gone
         sim->impl->stem_plain(pixels, n_pixels, out);
     });
 }

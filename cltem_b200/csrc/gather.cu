@@ -2,7 +2,8 @@
 //
 // dL/dx_a, dL/dy_a of the atoms of one or more consecutive slices (sorted order; one launch per checkpoint
 // segment of the adjoint, so the grid holds several slices' atoms): the sum over the pixels within
-// 8 Å of atom a of gV(r) V'(rho) d rho / d(x_a, y_a), rho = |r - r_a|, with V' the derivative of the
+// 8 Å of atom a of gV(r) V'(rho) d rho / d(x_a, y_a), rho = |r - r_a| (tilt-corrected under a beam tilt, TiltT),
+// with V' the derivative of the
 // projected form the forward potential kernel sums (potential.cuh; transmission_potentials_projected_d.cl)
 // and zero where the forward clamps rho to r_min = dx/4.
 //
@@ -50,6 +51,13 @@ __device__ __forceinline__ T dpot_drho(int form, const T *__restrict__ prm, int 
     return s;
 }
 
+// The beam tilt of the projected kernel (transmission_potentials_projected_d.cl:283-297, theta = pi/2 - tilt):
+// z' = -u sin t cos t, x' = rx - u sin^2 t cos phi, y' = ry - u sin^2 t sin phi with u = rx cos phi + ry sin phi,
+// so its radius is rho^2 = rx^2 + ry^2 - sin^2(t) u^2, and d rho / d rx = (rx - sin^2(t) u cos phi) / rho.
+template <class T> struct TiltT {
+    T s2, c, s;   // sin^2(tilt), cos(phi), sin(phi)
+};
+
 // One 256-thread block per (atom, band of pixel rows): kGatherBands blocks share an atom's pixel box so a
 // slice's ~100-200 atoms still fill the GPU; each block writes its two sums to work[], and k_atom_grad_sum
 // adds the bands of every atom in a fixed order (deterministic results).
@@ -81,18 +89,20 @@ k_atom_grad(const GradSlices sl, const double *__restrict__ ax, const double *__
     const int r0 = iy0 + (int)(((long long)rows * blockIdx.y) / kGatherBands);
     const int r1 = iy0 + (int)(((long long)rows * (blockIdx.y + 1)) / kGatherBands) - 1;
     const double ox = startx - xa, oy = starty - ya;   // pixel px sits at ox + px dx from the atom
+    const TiltT<T> ts{(T)sl.tilt_s2, (T)sl.cphi, (T)sl.sphi};
     T gx = 0, gy = 0;
     for (int py = r0 + (int)threadIdx.y; py <= r1; py += 8) {
         const T ry = (T)(oy + py * dx);
         const double *grow = gVs + (size_t)py * n;
         for (int px = ix0 + (int)threadIdx.x; px <= ix1; px += 32) {
             const T rx = (T)(ox + px * dx);
-            const T rho2 = rx * rx + ry * ry;
+            const T u = rx * ts.c + ry * ts.s;
+            const T rho2 = rx * rx + ry * ry - ts.s2 * u * u;
             if (rho2 > r_min2 && rho2 <= (T)64) {
                 const T rho = fsqrt(rho2);
                 const T f = (T)grow[px] * dpot_drho<T>(form, prm, i_lim, Z, rho) / rho;
-                gx -= f * rx;   // d rho / d x_a = -rx / rho
-                gy -= f * ry;
+                gx -= f * (rx - ts.s2 * u * ts.c);   // d rho / d x_a = -(rx - s2 u cos phi) / rho
+                gy -= f * (ry - ts.s2 * u * ts.s);
             }
         }
     }
@@ -166,18 +176,20 @@ k_atom_grad_f(const GradSlices sl, const double *__restrict__ ax, const double *
     const int r0 = iy0 + (int)(((long long)rows * blockIdx.y) / kGatherBands);
     const int r1 = iy0 + (int)(((long long)rows * (blockIdx.y + 1)) / kGatherBands) - 1;
     const double ox = startx - xa, oy = starty - ya;
+    const TiltT<float> ts{(float)sl.tilt_s2, (float)sl.cphi, (float)sl.sphi};
     float gx = 0, gy = 0;
     for (int py = r0 + (int)threadIdx.y; py <= r1; py += 8) {
         const float ry = (float)(oy + py * dx);
         const double *grow = gVs + (size_t)py * n;
         for (int px = ix0 + (int)threadIdx.x; px <= ix1; px += 32) {
             const float rx = (float)(ox + px * dx);
-            const float rho2 = rx * rx + ry * ry;
+            const float u = rx * ts.c + ry * ts.s;
+            const float rho2 = rx * rx + ry * ry - ts.s2 * u * u;
             if (rho2 > r_min2 && rho2 <= 64.0f) {
                 const float rho = sqrtf(rho2);
                 const float f = (float)grow[px] * __fdividef(dpotp_drho<FORM>(c, rho), rho);
-                gx -= f * rx;   // d rho / d x_a = -rx / rho
-                gy -= f * ry;
+                gx -= f * (rx - ts.s2 * u * ts.c);   // d rho / d x_a = -(rx - s2 u cos phi) / rho
+                gy -= f * (ry - ts.s2 * u * ts.s);
             }
         }
     }

@@ -25,33 +25,43 @@ template <class K> void set_smem(K kernel, size_t bytes) {
     MS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
 }
 
-// the two-column step kernel of the FP32 plans (templates, so that the FP64 build discards them)
-template <class RR> void pair_attrs() {
-    if constexpr (std::is_same<RR, float>::value && pair_columns<N>()) {
-        using PC = PairStepCfg<N>;
-        set_smem(k_col_step_pair<N, PC::COLS, pair_loose<N>()>, PC::smem());
+// the two-column step kernel of the FP32 plans (templates, so that the FP64 build discards them) with a tile of
+// C columns: C = PairStepCfg::COLS (the measured default), half or twice that where the tile is valid
+template <class RR, int C> constexpr bool pair_tile_ok() {
+    if constexpr (std::is_same<RR, float>::value && pair_columns<N>() && C >= 2 && C <= N) {
+        return PairCfg<N, C, pair_loose<N>()>::ok && C % CC::COLS == 0 && N % C == 0;
+    } else {
+        return false;
     }
 }
-template <class RR>
+template <class RR, int C> void pair_attrs() {
+    if constexpr (pair_tile_ok<RR, C>()) {
+        using PC = PairCfg<N, C, pair_loose<N>()>;
+        set_smem(k_col_step_pair<N, C, pair_loose<N>()>, PC::smem());
+    }
+}
+template <class RR, int C>
 bool pair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw, PropTables<RR> pt, RR b, int tiles_lo,
                int tiles_hi) {
-    if constexpr (std::is_same<RR, float>::value && pair_columns<N>()) {
-        using PC = PairStepCfg<N>;
+    if constexpr (pair_tile_ok<RR, C>()) {
+        using PC = PairCfg<N, C, pair_loose<N>()>;
         // the engine's tiles are CC::COLS wide and the step's tile covers k of them; the extra columns of a
         // partly active tile lie outside the propagator's cut and come out zero, and the row pass never
         // reads them
-        constexpr int k = PC::COLS / CC::COLS, total = N / PC::COLS;
-        static_assert(PC::COLS % CC::COLS == 0, "the step's tile must cover whole engine tiles");
+        constexpr int k = C / CC::COLS, total = N / C;
+        static_assert(C % CC::COLS == 0, "the step's tile must cover whole engine tiles");
         int lo = (tiles_lo + k - 1) / k, hi = (tiles_hi + k - 1) / k;
         if (lo + hi > total) { lo = total; hi = 0; }
-        k_col_step_pair<N, PC::COLS, pair_loose<N>()><<<dim3(lo + hi, batch), dim3(PC::PAIRS, Plan<N>::NT), PC::smem(),
-                                                       s>>>(wave, tw, pt, b, lo);
+        k_col_step_pair<N, C, pair_loose<N>()><<<dim3(lo + hi, batch), dim3(PC::PAIRS, Plan<N>::NT), PC::smem(), s>>>(
+            wave, tw, pt, b, lo);
         MS_CUDA(cudaGetLastError());
         return true;
     } else {
         return false;
     }
 }
+// C of the default two-column step (a valid value for the FP64 build too, where nothing uses it)
+constexpr int kPairC = pair_columns<N>() ? PairStepCfg<N>::COLS : 2;
 
 // The persistent TMA-fed column passes of the FP32 power-of-two plans (passes_tma.cuh), by variant, where
 // their stages and tables fit in shared memory (256^2: both; 512^2: variant 1):
@@ -68,8 +78,34 @@ template <class RR, int V> constexpr bool tma_col_ok() {
         return false;
     }
 }
-template <class RR> constexpr int tma_col_variants() {
-    return tma_col_ok<RR, 1>() ? (tma_col_ok<RR, 2>() ? 3 : 2) : 1;
+// The column-step kernels of this size, by kind: 0 the two-column step at its default tile, 1 / 2 the
+// persistent TMA-fed passes, 3 / 4 the two-column step at half / twice the default tile. A variant index of
+// PassOps::col_step is a position in the list of the kinds valid here (kind 0 always first).
+struct KindList {
+    int kind[5];
+    int n;
+};
+template <class RR> constexpr KindList col_kinds() {
+    KindList k{{0, -1, -1, -1, -1}, 1};
+    if (tma_col_ok<RR, 1>()) k.kind[k.n++] = 1;
+    if (tma_col_ok<RR, 2>()) k.kind[k.n++] = 2;
+    if (pair_tile_ok<RR, kPairC / 2>()) k.kind[k.n++] = 3;
+    if (pair_tile_ok<RR, kPairC * 2>()) k.kind[k.n++] = 4;
+    return k;
+}
+template <class RR> constexpr int tma_col_variants() { return col_kinds<RR>().n; }
+// the name of column-step variant v of this size
+std::string col_variant_name(int v) {
+    constexpr KindList k = col_kinds<R>();
+    if (v < 0 || v >= k.n) return "";
+    const int kind = k.kind[v];
+    auto cols = [](int c) { return std::to_string(c) + "-column tiles"; };
+    if (kind == 0 && !std::is_same<R, float>::value) return "one block per column tile and wave";
+    if (kind == 0) return "one block per (" + cols(kPairC) + ", wave), two columns a thread";
+    if (kind == 3) return "one block per (" + cols(kPairC / 2) + ", wave), two columns a thread";
+    if (kind == 4) return "one block per (" + cols(kPairC * 2) + ", wave), two columns a thread";
+    if (kind == 1) return "persistent, TMA-fed, " + cols(kPairC) + ", 3 stages, 1 block per SM";
+    return "persistent, TMA-fed, " + cols(kPairC / 2) + ", 3 stages, 2 blocks per SM";
 }
 int g_sms[64] = {};
 int sm_count() {
@@ -150,7 +186,9 @@ void ensure_attrs() {
     set_smem(k_row_fft<R, N, -1>, RC::smem());
     set_smem(k_row_fft<R, N, +1>, RC::smem());
     set_smem(k_col_step<R, N, COL_STEP>, CC::smem());
-    pair_attrs<R>();
+    pair_attrs<R, kPairC>();
+    pair_attrs<R, kPairC / 2>();
+    pair_attrs<R, kPairC * 2>();
     tma_col_attrs<R, 1>();
     tma_col_attrs<R, 2>();
     rowpair_attrs<R>();
@@ -213,9 +251,13 @@ void col_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, PropT
     if (variant < 0 || variant >= tma_col_variants<R>()) throw std::runtime_error("column pass variant out of range");
     dim3 g(tiles_lo + tiles_hi, batch);
     if (mode == COL_STEP && recip == nullptr && pt.ycut) {
-        if (variant == 1 && tma_col_step<R, 1>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
-        if (variant == 2 && tma_col_step<R, 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
-        if (pair_step<R>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        constexpr KindList kinds = col_kinds<R>();
+        const int kind = kinds.kind[variant];
+        if (kind == 1 && tma_col_step<R, 1>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 2 && tma_col_step<R, 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 3 && pair_step<R, kPairC / 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 4 && pair_step<R, kPairC * 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (pair_step<R, kPairC>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
     }
     if (mode == COL_STEP && recip == nullptr)
         k_col_step<R, N, COL_STEP><<<g, col_block(), CC::smem(), s>>>(wave, tw, pt, b, ds, det, recip, tiles_lo);
@@ -264,6 +306,7 @@ PassOps<MS_REAL> make_pass_ops<MS_REAL, MS_N>() {
     o.col_blocks = N / CC::COLS;
     o.cols_per_tile = CC::COLS;
     o.col_variants = tma_col_variants<R>();
+    o.col_variant_name = col_variant_name;
     o.row_step = row_step;
     o.row_fft = row_fft;
     o.col_step = col_step;

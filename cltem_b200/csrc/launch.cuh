@@ -5,6 +5,8 @@
 #include "passes.cuh"
 #include "passes_tma.cuh"
 
+#include <string>
+
 namespace ms {
 
 template <class R>
@@ -21,10 +23,12 @@ struct PassOps {
     void (*row_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
     // col_step(..., mode, tiles_lo, tiles_hi, variant): the leading tiles_lo and trailing tiles_hi column tiles;
     // variant picks the kernel of the plain step (COL_STEP without a reciprocal copy), 0 <= variant <
-    // col_variants: 0 the one-launch-per-tile kernels, 1.. the persistent TMA-fed column passes
+    // col_variants: 0 the one-block-per-tile kernel at its default tile, then (where valid for the size) the
+    // persistent TMA-fed passes and the one-block-per-tile kernel at other tile widths (col_variant_name)
     void (*col_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, PropTables<R>, R, R, DetArgs, cplx<R> *, int, int,
                      int, int) = nullptr;
     int col_variants = 1;
+    std::string (*col_variant_name)(int) = nullptr;   // a description of column variant v
     int cols_per_tile = 0;
     void (*col_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
     void (*col_bandlimit)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const double *, const double *, double, R) = nullptr;

@@ -68,6 +68,8 @@ def load_library(path=None):
         "mslice_ctem_run": [C.c_void_p, _dp, _dp, _dp],
         "mslice_stage_configs": [C.c_void_p, C.c_int, _szp, _ip, _dp, _dp, _dp],
         "mslice_stem_run_staged": [C.c_void_p],
+        "mslice_stem_run_staged_async": [C.c_void_p],
+        "mslice_sim_wait": [C.c_void_p],
         "mslice_cbed_run_staged": [C.c_void_p],
         "mslice_staged_result": [C.c_void_p, _dp, C.c_size_t],
         "mslice_stem_simulate": [C.c_void_p, C.c_int, _szp, _ip, _dp, _dp, _dp, _dp, C.c_size_t],
@@ -79,11 +81,14 @@ def load_library(path=None):
         "mslice_profile_enable": [C.c_void_p, C.c_int],
         "mslice_ctem_loss_grad": [C.c_void_p, _dp, _dp, _dp, _dp, _dp, C.c_int],
         "mslice_ctem_loss": [C.c_void_p, _dp, _dp],
+        "mslice_ctem_loss_forward": [C.c_void_p, _dp, _dp, C.c_int, C.POINTER(C.c_ulonglong)],
+        "mslice_ctem_loss_backward": [C.c_void_p, C.c_ulonglong, _dp, _dp, _dp],
         "mslice_profile_read": [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_ulonglong), _dp, C.c_int],
         "mslice_incoherence_draws": [C.POINTER(abi.Config), C.c_int, _ip, C.c_size_t, _dp, _ip, C.c_int, C.c_int, _dp],
         "mslice_plasmon_draws": [C.POINTER(abi.Config), C.c_ulonglong, C.c_double, _dp, C.c_size_t, _szp, C.c_int, _dp],
         "mslice_tune_batch": [C.c_void_p, _ip, C.c_int, C.c_int, _ip, _dp],
         "mslice_set_step_variant": [C.c_void_p, C.c_int, C.c_int],
+        "mslice_step_variant_name": [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_size_t],
         "mslice_get_tuning": [C.c_void_p, _ip, _ip, _ip, _ip, _ip],
         "mslice_set_ccd": [C.c_void_p, _dp, _dp, C.c_size_t, C.c_int, C.c_double],
     }
@@ -163,6 +168,7 @@ class Context:
         h = C.c_void_p()
         _check(self.lib.mslice_ctx_create(device, C.byref(h)))
         self.h = h
+        self.device = device
         self.params = None
         self._sims = weakref.WeakSet()
 
@@ -329,6 +335,20 @@ class Simulation:
                                               int(checkpoint_every)))
         return L.value, gx[: 3 * n_atoms].reshape(n_atoms, 3), g10.value, g30.value
 
+    def ctem_loss_forward(self, target, checkpoint_every=0):
+        """The loss, keeping the adjoint's state: (L, token) for ctem_loss_backward."""
+        t = np.ascontiguousarray(target, dtype=np.float64).reshape(-1)
+        L, tok = C.c_double(), C.c_ulonglong()
+        _check(self.lib.mslice_ctem_loss_forward(self.h, _d(t), C.byref(L), int(checkpoint_every), C.byref(tok)))
+        return L.value, tok.value
+
+    def ctem_loss_backward(self, token, n_atoms):
+        """(dL/dxyz [n_atoms, 3], dL/dC10, dL/dC30) from the state of forward `token`."""
+        g10, g30 = C.c_double(), C.c_double()
+        gx = np.zeros(3 * max(n_atoms, 1))
+        _check(self.lib.mslice_ctem_loss_backward(self.h, int(token), _d(gx), C.byref(g10), C.byref(g30)))
+        return gx[: 3 * n_atoms].reshape(n_atoms, 3), g10.value, g30.value
+
     # ---- frozen-phonon runs ---------------------------------------------------------------------
     def stage(self, configs):
         from .structure import concat_configs
@@ -341,6 +361,13 @@ class Simulation:
             _check(self.lib.mslice_stem_run_staged(self.h))
         else:
             _check(self.lib.mslice_cbed_run_staged(self.h))
+
+    def run_staged_async(self):
+        """Queue a staged STEM run and return (mslice_stem_run_staged_async); wait() or staged_result() waits."""
+        _check(self.lib.mslice_stem_run_staged_async(self.h))
+
+    def wait(self):
+        _check(self.lib.mslice_sim_wait(self.h))
 
     def result_size(self):
         if self.cfg.mode == abi.MODE_STEM:
@@ -401,6 +428,12 @@ class Simulation:
         if row_variant is None:
             row_variant = self.tuning()["row_variant"]
         _check(self.lib.mslice_set_step_variant(self.h, int(col_variant), int(row_variant)))
+
+    def step_variant_name(self, which, index):
+        """A description of column (which = 0) or row (1) step variant `index` (mslice_step_variant_name)."""
+        buf = C.create_string_buffer(256)
+        _check(self.lib.mslice_step_variant_name(self.h, int(which), int(index), buf, 256))
+        return buf.value.decode()
 
     def tuning(self):
         """{"batch", "col_variant", "col_variants", "row_variant", "row_variants"} the next STEM run uses

@@ -1,8 +1,9 @@
 // ctem_loss_op.cpp — the differentiable CTEM image loss as a libtorch autograd Function.
 //
 // forward(xyz [n,3] float64, lens [2] float64 = (C10, C30) in Å) -> loss (0-d float64): sets the atoms and the
-// lens of an mslice simulation and runs mslice_ctem_loss_grad (include/mslice.h), keeping the gradients
-// for backward. backward returns grad_output * dL/dxyz and grad_output * dL/d(C10, C30).
+// lens of an mslice simulation and runs the adjoint's forward half, mslice_ctem_loss_forward (include/mslice.h),
+// which keeps the checkpoints the backward half needs. backward runs mslice_ctem_loss_backward and returns
+// grad_output * dL/dxyz and grad_output * dL/d(C10, C30); a forward with no backward costs only the forward.
 // The simulation handle, the atomic numbers and the target image are fixed per op instance.
 #include <torch/extension.h>
 
@@ -34,19 +35,25 @@ struct CtemImageLoss : public torch::autograd::Function<CtemImageLoss> {
         for (int64_t i = 0; i < n; i++) { x[i] = pp[3 * i]; y[i] = pp[3 * i + 1]; w[i] = pp[3 * i + 2]; }
         check(mslice_set_c10_c30(sim, l.data_ptr<double>()[0], l.data_ptr<double>()[1]));
         check(mslice_set_atoms(sim, z.data_ptr<int>(), x.data(), y.data(), w.data(), (size_t)n));
-        double loss = 0, g10 = 0, g30 = 0;
-        auto gxyz = torch::zeros({n, 3}, torch::kFloat64);
-        check(mslice_ctem_loss_grad(sim, t.data_ptr<double>(), &loss, gxyz.data_ptr<double>(), &g10, &g30,
-                                    (int)checkpoint_every));
-        auto glens = torch::tensor({g10, g30}, torch::kFloat64);
-        ctx->save_for_backward({gxyz, glens});
+        double loss = 0;
+        unsigned long long token = 0;
+        check(mslice_ctem_loss_forward(sim, t.data_ptr<double>(), &loss, (int)checkpoint_every, &token));
+        ctx->saved_data["sim"] = sim_handle;
+        ctx->saved_data["token"] = (int64_t)token;
+        ctx->saved_data["n"] = n;
         return torch::tensor(loss, torch::kFloat64).to(xyz.device());
     }
 
     static tensor_list backward(AutogradContext *ctx, tensor_list grad_outputs) {
-        auto saved = ctx->get_saved_variables();
+        auto sim = reinterpret_cast<mslice_sim *>(ctx->saved_data["sim"].toInt());
+        const auto token = (unsigned long long)ctx->saved_data["token"].toInt();
+        const int64_t n = ctx->saved_data["n"].toInt();
+        double g10 = 0, g30 = 0;
+        auto gxyz = torch::zeros({n, 3}, torch::kFloat64);
+        check(mslice_ctem_loss_backward(sim, token, gxyz.data_ptr<double>(), &g10, &g30));
+        auto glens = torch::tensor({g10, g30}, torch::kFloat64);
         auto go = grad_outputs[0].to(torch::kCPU);
-        return {saved[0] * go, saved[1] * go, torch::Tensor(), torch::Tensor(), torch::Tensor(), torch::Tensor()};
+        return {gxyz * go, glens * go, torch::Tensor(), torch::Tensor(), torch::Tensor(), torch::Tensor()};
     }
 };
 

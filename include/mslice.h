@@ -241,10 +241,19 @@ int mslice_ctem_run(mslice_sim *sim, double *ew, double *diff, double *image);
  * order, 3 per atom; z is 0 in the projected model, where z only selects the slice), dL/dC10 and dL/dC30
  * (per Å). target holds res*res doubles (x fastest). Slice waves are checkpointed every
  * `checkpoint_every` slices (0: ceil(sqrt(n_slices)); 1: every slice, no recomputation) and recomputed
- * segment by segment in the backward pass. Projected potentials without beam tilt only
- * (MSLICE_ERR_UNSUPPORTED otherwise). Any output pointer may be NULL. */
+ * segment by segment in the backward pass. Projected potentials (with or without beam tilt) only; the
+ * full 3-D model, mixed static potentials and plasmons fail with MSLICE_ERR_UNSUPPORTED. Any output
+ * pointer may be NULL. The same as mslice_ctem_loss_forward followed by mslice_ctem_loss_backward. */
 int mslice_ctem_loss_grad(mslice_sim *sim, const double *target, double *loss, double *grad_xyz, double *grad_c10,
                           double *grad_c30, int checkpoint_every);
+/* The two halves of mslice_ctem_loss_grad, for autograd frameworks that run the backward pass later: the
+ * forward computes the loss and keeps the checkpoints and state the adjoint needs, returning a token; the
+ * backward turns that state into the gradients. Any other call on the simulation in between (a run, new
+ * atoms or lens, another forward) invalidates the state and the backward fails with MSLICE_ERR_STATE. */
+int mslice_ctem_loss_forward(mslice_sim *sim, const double *target, double *loss, int checkpoint_every,
+                             unsigned long long *token);
+int mslice_ctem_loss_backward(mslice_sim *sim, unsigned long long token, double *grad_xyz, double *grad_c10,
+                              double *grad_c30);
 /* The same loss without gradients (forward only); used to time the forward model. */
 int mslice_ctem_loss(mslice_sim *sim, const double *target, double *loss);
 /* CTEM dose simulation (SimulationCtem::simulateImageDose, microscope/simulationctem.cpp:88-108,171-264):
@@ -264,8 +273,18 @@ int mslice_set_c10_c30(mslice_sim *sim, double c10, double c30);
 int mslice_stage_configs(mslice_sim *sim, int n_configs, const size_t *counts, const int *Z,
                          const double *x, const double *y, const double *z);
 /* Run every staged configuration and every STEM scan pixel (all px*py in scan order), accumulating
- * the detector values over configurations in FP64 with Kahan compensation on the device. */
+ * the detector values over configurations in FP64 with Kahan compensation on the device. With the static
+ * frame, one transmission set, no plasmons and no progress callback, the whole run (every pass's binning,
+ * transmission build and probe batches) is captured once into a CUDA graph and each run of the same staged
+ * layout is a single graph launch (MSLICE_NO_GRAPHS=1 launches eagerly); mslice_last_timing then reports
+ * the whole run only (build and propagation -1). */
 int mslice_stem_run_staged(mslice_sim *sim);
+/* The same run, returning once it is queued (no counterpart in the reference): with the single-launch path
+ * above the call enqueues the graph on the context's stream and returns, so runs on different contexts
+ * (streams) overlap; otherwise it runs synchronously. mslice_sim_wait waits for it (and reports a failed
+ * wait of the step kernels); mslice_staged_result and the next run wait as well. */
+int mslice_stem_run_staged_async(mslice_sim *sim);
+int mslice_sim_wait(mslice_sim *sim);
 /* Same for CBED: accumulates |psi(k)|^2 over configurations. */
 int mslice_cbed_run_staged(mslice_sim *sim);
 /* Averaged result of the last *_run_staged call: STEM out[(o*n_det + d)*px*py + p], CBED
@@ -304,13 +323,17 @@ int mslice_plasmon_draws(const mslice_config *cfg, unsigned long long job, doubl
 int mslice_tune_batch(mslice_sim *sim, const int *candidates, int n_candidates, int reps, int *best_batch,
                       double *waves_per_second);
 /* The kernels of the batched STEM step (no counterpart in the reference). Column step: 0 = one block per
- * column tile and wave; 1, 2 (FP32 power-of-two grids where their shared memory fits) = persistent passes,
- * one or two blocks per SM, whose producer warp streams tiles into a ring of shared-memory stages with TMA
- * (1: the step's tile, 3 stages; 2: half that tile, two blocks per SM). Row step: 0 = plain; 1, 2 = each
- * block also asks the copy engine to prefetch into L2 the rows that the blocks one or two residencies of the
- * grid later will read. All variants give bit-identical results. Out-of-range values fail with
- * MSLICE_ERR_ARG. */
+ * column tile and wave at the default tile width; the further variants of the grid and precision (FP32) are
+ * the persistent passes, one or two blocks per SM, whose producer warp streams tiles into a ring of
+ * shared-memory stages with TMA (power-of-two grids where their shared memory fits), and the one-block-per-tile
+ * kernel at half and twice the default tile width (mslice_step_variant_name describes each). Row step: 0 =
+ * plain; 1, 2 = each block also asks the copy engine to prefetch into L2 the rows that the blocks one or two
+ * residencies of the grid later will read. All variants give bit-identical results. Out-of-range values fail
+ * with MSLICE_ERR_ARG. */
 int mslice_set_step_variant(mslice_sim *sim, int col_variant, int row_variant);
+/* A description of step-kernel variant `index` (which: 0 column, 1 row) of this simulation's grid and
+ * precision into buf (NUL-terminated, at most cap bytes). */
+int mslice_step_variant_name(mslice_sim *sim, int which, int index, char *buf, size_t cap);
 /* The batch the next STEM run uses, the column- and row-step variants and their counts for this grid and
  * precision (any pointer may be NULL). */
 int mslice_get_tuning(mslice_sim *sim, int *batch, int *col_variant, int *n_col_variants, int *row_variant,

@@ -130,3 +130,62 @@ def test_gradient_independent_of_checkpoint_segments(kirkland, dp):
         assert abs(L - L1) <= tol * L1
         assert np.abs(g - g1).max() <= tol * np.abs(g1).max()
         assert abs(d10 - c10) <= tol * abs(c10) and abs(d30 - c30) <= tol * abs(c30)
+
+
+def test_forward_backward_halves_equal_loss_grad(kirkland):
+    """mslice_ctem_loss_forward + mslice_ctem_loss_backward give mslice_ctem_loss_grad's numbers; a run in
+    between invalidates the forward state."""
+    from cltem_b200 import abi
+    from cltem_b200.engine import MsliceError
+    ctx, s, st, target = _setup(True, kirkland)
+    sim = Simulation(ctx, s.cfg)
+    sim.set_atoms(st)
+    L, g, g10, g30 = sim.ctem_loss_grad(target, len(st))
+    L2, tok = sim.ctem_loss_forward(target)
+    g2, h10, h30 = sim.ctem_loss_backward(tok, len(st))
+    assert L2 == L and np.array_equal(g2, g) and h10 == g10 and h30 == g30
+    L3, tok3 = sim.ctem_loss_forward(target)
+    sim.ctem()                                          # another run: the forward state is gone
+    with pytest.raises(MsliceError) as e:
+        sim.ctem_loss_backward(tok3, len(st))
+    assert e.value.code == abi.ERR_STATE
+    _, tok4 = sim.ctem_loss_forward(target)
+    with pytest.raises(MsliceError):
+        sim.ctem_loss_backward(tok4 - 1, len(st))       # a stale token
+
+
+@pytest.mark.parametrize("dp", [True, False])
+def test_adjoint_with_beam_tilt_matches_finite_differences(kirkland, dp):
+    """Beam tilt (6 mrad at azimuth 0.7 rad): the projected kernel's tilt-corrected radius in the atom gradient,
+    the tilted propagator in the adjoint; FP64 against FP64 central differences, FP32 against FP64."""
+    ctx, s, st, target = _setup(True, kirkland)
+    s.cfg.beam_tilt, s.cfg.beam_azimuth = 6.0, 0.7
+    sim = Simulation(ctx, s.cfg)
+    sim.set_atoms(st)
+    L, g, g10, g30 = sim.ctem_loss_grad(target, len(st))
+    L_ = s.cfg.ctem_area[1]
+    inner = np.where((st.x > 0.5) & (st.y > 0.5) & (st.x < L_ - 0.5) & (st.y < L_ - 0.5))[0]
+    h = 1e-4
+    if dp:
+        for i in np.random.default_rng(3).choice(inner, 4, replace=False):
+            for axis in (0, 1):
+                lp = _loss64(ctx, s, st, (i, axis, +h)).ctem_loss(target)
+                lm = _loss64(ctx, s, st, (i, axis, -h)).ctem_loss(target)
+                fd = (lp - lm) / (2 * h)
+                assert abs(g[i, axis] - fd) <= 2e-5 * max(abs(fd), 1e-3 * np.abs(g).max()), (i, axis, g[i, axis], fd)
+        fd10 = (_loss64(ctx, s, st, dc10=1e-2).ctem_loss(target) - _loss64(ctx, s, st, dc10=-1e-2).ctem_loss(target)) / 2e-2
+        assert abs(g10 - fd10) <= 1e-5 * abs(fd10)
+    else:
+        from copy import deepcopy
+        c32 = deepcopy(s.cfg)
+        c32.double_precision = 0
+        s32 = Simulation(ctx, c32)
+        s32.set_atoms(st)
+        c64 = deepcopy(s.cfg)
+        c64.double_precision = 1
+        s64 = Simulation(ctx, c64)
+        s64.set_atoms(st)
+        L64, g64, c10_64, c30_64 = s64.ctem_loss_grad(target, len(st))
+        L32, g32, c10_32, c30_32 = s32.ctem_loss_grad(target, len(st))
+        assert abs(L32 - L64) <= 1e-4 * L64
+        assert np.linalg.norm(g32 - g64) <= 1e-3 * np.linalg.norm(g64)

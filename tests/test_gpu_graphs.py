@@ -56,3 +56,64 @@ def test_graph_profile_counts_every_replay(gpu_ctx, kirkland):
     other.stage(phonons(st, 2))
     other.run_staged()
     assert np.array_equal(sim.staged_result(), other.staged_result())
+
+
+def _staged_case(kirkland, chromatic=False):
+    from tests.cases import phonons, small_stem
+    s, st = small_stem(double_precision=False, scan=8)
+    s.cfg.probe_batch = 24   # several batches a pass, the last one short
+    if chromatic:
+        s.cfg.chromatic = 1
+        s.cfg.chromatic_cc = 1.5
+        s.cfg.chromatic_hwhm_neg = s.cfg.chromatic_hwhm_pos = 0.4
+    return s, phonons(st, 3, seed=21)
+
+
+@pytest.mark.parametrize("chromatic", [False, True])
+def test_whole_staged_run_graph_matches_eager(gpu_ctx, kirkland, chromatic, monkeypatch):
+    """A staged STEM run captured as one graph (every pass's binning, build and batches) gives the eager run's
+    bits, on its first launch (captured) and on replays."""
+    from cltem_b200.engine import Simulation
+    gpu_ctx.load_params(kirkland)
+    s, confs = _staged_case(kirkland, chromatic)
+    monkeypatch.setenv("MSLICE_NO_GRAPHS", "1")
+    eager = Simulation(gpu_ctx, s.cfg)
+    monkeypatch.delenv("MSLICE_NO_GRAPHS")
+    eager.stage(confs)
+    eager.run_staged()
+    ref = eager.staged_result()
+    sim = Simulation(gpu_ctx, s.cfg)
+    sim.stage(confs)
+    for _ in range(3):
+        sim.run_staged()
+        assert np.array_equal(sim.staged_result(), ref)
+    assert sim.last_timing()["total_ms"] > 0 and sim.last_timing()["build_ms"] == -1
+    eager.close()
+    sim.close()
+
+
+def test_async_runs_on_two_contexts_overlap_and_match(kirkland):
+    """Queued staged runs on two contexts (two streams): each result equals its synchronous run."""
+    from cltem_b200.engine import Context, Simulation
+    from tests.cases import phonons, small_stem
+    ctxs = [Context(0), Context(0)]
+    sims, refs = [], []
+    for k, c in enumerate(ctxs):
+        c.load_params(kirkland)
+        s, st = small_stem(double_precision=False, scan=6, res=256 if k == 0 else 128)
+        s.cfg.allow_any_resolution = 1
+        confs = phonons(st, 2, seed=30 + k)
+        sim = Simulation(c, s.cfg)
+        sim.stage(confs)
+        sim.run_staged()
+        refs.append(sim.staged_result().copy())
+        sims.append(sim)
+    for sim in sims:
+        sim.run_staged_async()
+    for sim, ref in zip(sims, refs):
+        sim.wait()
+        assert np.array_equal(sim.staged_result(), ref)
+    for sim in sims:
+        sim.close()
+    for c in ctxs:
+        c.close()

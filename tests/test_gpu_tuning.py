@@ -42,11 +42,12 @@ def test_tune_batch_default_candidates_are_cached(gpu_ctx, kirkland):
         a.tune_batch([0, 4])
 
 
-@pytest.mark.parametrize("res", [256, 512, 1024])
+@pytest.mark.parametrize("res", [256, 512, 768, 1024, 2048])
 def test_column_step_variants_are_bit_identical(gpu_ctx, kirkland, res):
-    """The persistent TMA-fed column passes (variants 1, 2) do the one-launch-per-tile kernel's arithmetic in
-    the same order: identical detector values over a batch large enough that every block loops over many
-    (wave, tile) items and reuses each shared-memory stage many times."""
+    """Every column-step kernel the tuner may pick (the persistent TMA-fed passes, the one-block-per-tile kernel
+    at other tile widths) does the default kernel's arithmetic in the same order: identical detector values
+    over a batch large enough that every persistent block loops over many (wave, tile) items and reuses each
+    shared-memory stage many times."""
     gpu_ctx.load_params(kirkland)
     s, st = small_stem(double_precision=False, res=res, n=(3, 3, 3), scan=12)
     s.cfg.probe_batch = 144
@@ -57,6 +58,11 @@ def test_column_step_variants_are_bit_identical(gpu_ctx, kirkland, res):
     nv = t["col_variants"]
     assert t["row_variants"] == 3
     assert nv >= (2 if res <= 512 else 1)   # the persistent passes where their stages and tables fit
+    names = [sim.step_variant_name(0, v) for v in range(nv)]
+    assert len(set(names)) == nv and all(names)
+    assert len({sim.step_variant_name(1, v) for v in range(3)}) == 3
+    with pytest.raises(MsliceError):
+        sim.step_variant_name(0, nv)
     pix = np.arange(144, dtype=np.int32)
     out = []
     for v in range(nv):
