@@ -446,11 +446,13 @@ def cbed3d_leg(ctx, ext, nz=60):
             "note": "one configuration of the 50; evaluations counted on the host from the binned atoms"}
 
 
-def sizes_leg(ctx, sizes, dp=False, n_atoms=30, seed=11):
-    """The step kernels at each grid: FP32 (or FP64) STEM of a batch of about 1 GiB of waves (at most 1024
-    probes) through 7 slices of 0.25 Å over a 400 Å field holding a few seeded atoms; device time per
-    probe·slice of the row and column passes (the column figure includes the last step of each batch, which
-    carries the detector reduction), from the engine's per-kernel event timing of the third of three runs."""
+def sizes_leg(ctx, sizes, dp=False, n_atoms=30, seed=11, tune=True):
+    """The step kernels at each grid: FP32 (or FP64) STEM of about 1 GiB of waves (at most 1024 probes)
+    through 7 slices of 0.25 Å over a 400 Å field holding a few seeded atoms; device time per probe·slice of
+    the row and column passes (the column figure includes the last step of each batch, which carries the
+    detector reduction), from the engine's per-kernel event timing of the third of three runs. With `tune` the
+    autotuner picks each grid's probe batch and step kernels first (as a STEM run of that grid would), and
+    the figures are also given per pixel, relative to 512²."""
     import torch
     from cltem_b200 import config
     from cltem_b200.engine import Simulation
@@ -472,6 +474,10 @@ def sizes_leg(ctx, sizes, dp=False, n_atoms=30, seed=11):
         s.attach_structure(st)
         sim = Simulation(ctx, c)
         sim.set_atoms(st)
+        tuned = None
+        if tune:
+            cands = [b for b in (2, 4, 8, 16, 32, 64, 128, 256, 512, 1024) if b <= npr]
+            tuned = sim.tune_batch(cands)
         pix = np.arange(npr, dtype=np.int32)
         sim.stem(pix)
         sim.stem(pix)
@@ -483,10 +489,17 @@ def sizes_leg(ctx, sizes, dp=False, n_atoms=30, seed=11):
         p = sim.profile_read()
         sim.profile(False)
         S = sim.geo.n_slices
-        out[str(res)] = {"probes": npr, "slices": S,
-                         "row_us_per_probe_slice": 1e3 * p["row_step"][0] / (npr * S),
-                         "col_us_per_probe_slice": 1e3 * p["col_step"][0] / (npr * S)}
+        row_us, col_us = 1e3 * p["row_step"][0] / (npr * S), 1e3 * p["col_step"][0] / (npr * S)
+        out[str(res)] = {"probes": npr, "slices": S, "row_us_per_probe_slice": row_us,
+                         "col_us_per_probe_slice": col_us, "ps_per_pixel": 1e6 * (row_us + col_us) / (res * res)}
+        if tuned:
+            tn = sim.tuning()
+            out[str(res)].update({"batch": tuned[0], "column": sim.step_variant_name(0, tn["col_variant"]),
+                                  "row": sim.step_variant_name(1, tn["row_variant"])})
         sim.close()
+    if "512" in out:
+        for v in out.values():
+            v["per_pixel_vs_512"] = v["ps_per_pixel"] / out["512"]["ps_per_pixel"]
     return {"workload": f"stem_sparse_400A_{'fp64' if dp else 'fp32'}", "sizes": out}
 
 

@@ -64,12 +64,19 @@ bool pair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw, Pr
 constexpr int kPairC = pair_columns<N>() ? PairStepCfg<N>::COLS : 2;
 
 // The persistent TMA-fed column passes of the FP32 power-of-two plans (passes_tma.cuh), by variant, where
-// their stages and tables fit in shared memory (256^2: both; 512^2: variant 1):
+// their stages and tables fit in shared memory:
 //   1: the step's tile (PairStepCfg::COLS columns), 3 stages, one block per SM
 //   2: half that tile, 3 stages, two blocks per SM
+//   3, 4: as 1, 2, with the results stored from the stage by TMA instead of from the consumers' registers
+//   5, 6: half the step's tile, 2 stages, one block per SM, stores from registers / by TMA (the grids whose
+//         tile column of N rows is too tall for three stages, e.g. 2048^2)
 template <int V> struct TmaVariant;
 template <> struct TmaVariant<1> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS, 3, 1>; };
 template <> struct TmaVariant<2> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, 3, 2>; };
+template <> struct TmaVariant<3> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS, 3, 1, true>; };
+template <> struct TmaVariant<4> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, 3, 2, true>; };
+template <> struct TmaVariant<5> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, 2, 1>; };
+template <> struct TmaVariant<6> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, 2, 1, true>; };
 template <class RR, int V> constexpr bool tma_col_ok() {
     if constexpr (std::is_same<RR, float>::value && pair_columns<N>()) {
         using TC = typename TmaVariant<V>::template Cfg<N>;
@@ -79,18 +86,23 @@ template <class RR, int V> constexpr bool tma_col_ok() {
     }
 }
 // The column-step kernels of this size, by kind: 0 the two-column step at its default tile, 1 / 2 the
-// persistent TMA-fed passes, 3 / 4 the two-column step at half / twice the default tile. A variant index of
+// persistent TMA-fed passes, 3 / 4 the two-column step at half / twice the default tile, 5 / 6 the persistent
+// passes 1 / 2 storing through TMA, 7 / 8 the two-stage persistent passes 5 / 6. A variant index of
 // PassOps::col_step is a position in the list of the kinds valid here (kind 0 always first).
 struct KindList {
-    int kind[5];
+    int kind[9];
     int n;
 };
 template <class RR> constexpr KindList col_kinds() {
-    KindList k{{0, -1, -1, -1, -1}, 1};
+    KindList k{{0, -1, -1, -1, -1, -1, -1, -1, -1}, 1};
     if (tma_col_ok<RR, 1>()) k.kind[k.n++] = 1;
     if (tma_col_ok<RR, 2>()) k.kind[k.n++] = 2;
     if (pair_tile_ok<RR, kPairC / 2>()) k.kind[k.n++] = 3;
     if (pair_tile_ok<RR, kPairC * 2>()) k.kind[k.n++] = 4;
+    if (tma_col_ok<RR, 3>()) k.kind[k.n++] = 5;
+    if (tma_col_ok<RR, 4>()) k.kind[k.n++] = 6;
+    if (tma_col_ok<RR, 5>()) k.kind[k.n++] = 7;
+    if (tma_col_ok<RR, 6>()) k.kind[k.n++] = 8;
     return k;
 }
 template <class RR> constexpr int tma_col_variants() { return col_kinds<RR>().n; }
@@ -105,7 +117,11 @@ std::string col_variant_name(int v) {
     if (kind == 3) return "one block per (" + cols(kPairC / 2) + ", wave), two columns a thread";
     if (kind == 4) return "one block per (" + cols(kPairC * 2) + ", wave), two columns a thread";
     if (kind == 1) return "persistent, TMA-fed, " + cols(kPairC) + ", 3 stages, 1 block per SM";
-    return "persistent, TMA-fed, " + cols(kPairC / 2) + ", 3 stages, 2 blocks per SM";
+    if (kind == 2) return "persistent, TMA-fed, " + cols(kPairC / 2) + ", 3 stages, 2 blocks per SM";
+    if (kind == 5) return "persistent, TMA loads and stores, " + cols(kPairC) + ", 3 stages, 1 block per SM";
+    if (kind == 6) return "persistent, TMA loads and stores, " + cols(kPairC / 2) + ", 3 stages, 2 blocks per SM";
+    if (kind == 7) return "persistent, TMA-fed, " + cols(kPairC / 2) + ", 2 stages, 1 block per SM";
+    return "persistent, TMA loads and stores, " + cols(kPairC / 2) + ", 2 stages, 1 block per SM";
 }
 int g_sms[64] = {};
 int sm_count() {
@@ -118,7 +134,7 @@ int sm_count() {
 template <class RR, int V> void tma_col_attrs() {
     if constexpr (tma_col_ok<RR, V>()) {
         using TC = typename TmaVariant<V>::template Cfg<N>;
-        set_smem(k_col_step_tma<N, TC::COLS, TC::STAGES, TC::MINB>, TC::smem());
+        set_smem(k_col_step_tma<N, TC::COLS, TC::STAGES, TC::MINB, TC::TS>, TC::smem());
     }
 }
 template <class RR, int V>
@@ -135,7 +151,7 @@ bool tma_col_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw,
         if (items > 0x7fffffffLL || (long long)batch * N > 0x7fffffffLL) throw std::runtime_error("batch too large");
         const CUtensorMap tm = wave_tensor_map(wave, 2ull * N, (unsigned long long)batch * N, TC::BOX_FLOATS, TC::BOX_ROWS);
         const int grid = (int)std::min<long long>(items, (long long)TC::MINB * sm_count());
-        k_col_step_tma<N, TC::COLS, TC::STAGES, TC::MINB><<<grid, TC::THREADS, TC::smem(), s>>>(
+        k_col_step_tma<N, TC::COLS, TC::STAGES, TC::MINB, TC::TS><<<grid, TC::THREADS, TC::smem(), s>>>(
             tm, wave, tw, pt, b, lo, lo + hi, (int)items, pt.err);
         MS_CUDA(cudaGetLastError());
         return true;
@@ -191,6 +207,10 @@ void ensure_attrs() {
     pair_attrs<R, kPairC * 2>();
     tma_col_attrs<R, 1>();
     tma_col_attrs<R, 2>();
+    tma_col_attrs<R, 3>();
+    tma_col_attrs<R, 4>();
+    tma_col_attrs<R, 5>();
+    tma_col_attrs<R, 6>();
     rowpair_attrs<R>();
     set_smem(k_col_step<R, N, COL_STEP_DET>, CC::smem());
     set_smem(k_col_step<R, N, COL_DET_ONLY>, CC::smem());
@@ -255,6 +275,10 @@ void col_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, PropT
         const int kind = kinds.kind[variant];
         if (kind == 1 && tma_col_step<R, 1>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 2 && tma_col_step<R, 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 5 && tma_col_step<R, 3>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 6 && tma_col_step<R, 4>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 7 && tma_col_step<R, 5>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 8 && tma_col_step<R, 6>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 3 && pair_step<R, kPairC / 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 4 && pair_step<R, kPairC * 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (pair_step<R, kPairC>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;

@@ -9,9 +9,11 @@
 //   - the consumer threads read a stage into registers, run the transforms using the same stage as their
 //     exchange space (the tile's row-major layout is the exchange layout of ColAddr<PAIRS, 16> when a tile
 //     row is 128 bytes), hand the stage back (one mbarrier arrive per warp) and store the tile to HBM
-//     straight from registers.
+//     straight from registers;
+//   - or (TS) the consumers write the transformed tile back into its stage and the producer thread stores it
+//     to HBM with cp.async.bulk.tensor before it refills the stage, so no consumer issues a global store.
 // So a tile's global loads overlap the transforms of the tiles before it, and no consumer waits on a
-// global load. Only this GPU's own wave buffer is read; no load uses cluster multicast.
+// global load. Only this GPU's own wave buffer is read and written; no load uses cluster multicast.
 #pragma once
 
 #include "passes.cuh"
@@ -21,9 +23,10 @@ namespace ms {
 
 // Tile of COLS columns (two a consumer thread) of an N-row wave; the stage is the whole tile, loaded as
 // N / BOX_ROWS boxes of at most 256 rows (a tensor-map box dimension is at most 256).
-template <int N, int COLS_, int STAGES_ = 3, int MINB_ = 1> struct TmaColCfg {
+template <int N, int COLS_, int STAGES_ = 3, int MINB_ = 1, bool TS_ = false> struct TmaColCfg {
     using P = Plan<N>;
     static constexpr int COLS = COLS_;
+    static constexpr bool TS = TS_;                    // results leave through the stage and a TMA store
     static constexpr int MINB = MINB_;                 // blocks per SM (the grid is MINB x the SM count)
     static constexpr int PAIRS = COLS / 2;
     static constexpr int NCONS = PAIRS * P::NT;        // consumer threads
@@ -33,9 +36,9 @@ template <int N, int COLS_, int STAGES_ = 3, int MINB_ = 1> struct TmaColCfg {
     static constexpr int BOX_ROWS = N < 256 ? N : 256;
     static constexpr int LOADS = N / BOX_ROWS;
     static constexpr int BOX_FLOATS = 2 * COLS;        // inner box extent in FP32 elements
-    // stages (128-byte aligned), twiddle table, the propagator tables (px, px errors, py, py errors, the cut
-    // rows of each column), 2 mbarriers per stage, alignment slack
-    static constexpr size_t smem() { return 128 + (size_t)STAGES * STAGE_BYTES + 6 * sizeof(float2) * N + 16 * STAGES; }
+    // stages (128-byte aligned), twiddle table, the propagator's row tables (py and its errors, read at every
+    // element; the column tables are read once per item from global memory), 2 mbarriers per stage
+    static constexpr size_t smem() { return 128 + (size_t)STAGES * STAGE_BYTES + 3 * sizeof(float2) * N + 16 * STAGES; }
     // one SM holds 228 KB of shared memory, 1 KB of it reserved per block
     static constexpr bool ok = P::pow2 && N % BOX_ROWS == 0 && COLS >= 2 && (BOX_FLOATS * 4) % 16 == 0 &&
                                BOX_FLOATS <= 256 && NCONS % 32 == 0 && THREADS <= 1024 && smem() <= kMaxBlockSmem &&
@@ -45,21 +48,21 @@ template <int N, int COLS_, int STAGES_ = 3, int MINB_ = 1> struct TmaColCfg {
 // Work item i (0 <= i < n_items = batch * n_active): wave i / n_active, active tile j = i % n_active, which is
 // column tile j for j < tiles_lo and tile N/COLS - (n_active - j) otherwise (the tiles holding columns inside
 // the propagator's cut). err: the error word (tma.cuh StepError), written only when a wait is abandoned.
-template <int N, int COLS, int STAGES, int MINB>
-__global__ void __launch_bounds__(TmaColCfg<N, COLS, STAGES, MINB>::THREADS, MINB)
+template <int N, int COLS, int STAGES, int MINB, bool TS>
+__global__ void __launch_bounds__(TmaColCfg<N, COLS, STAGES, MINB, TS>::THREADS, MINB)
 k_col_step_tma(const __grid_constant__ CUtensorMap tm, float2 *__restrict__ wave, const float2 *__restrict__ twg,
                PropTables<float> pt, float bscale, int tiles_lo, int n_active, int n_items, int *err) {
-    using TC = TmaColCfg<N, COLS, STAGES, MINB>;
+    using TC = TmaColCfg<N, COLS, STAGES, MINB, TS>;
     using P = Plan<N>;
     constexpr int PAIRS = TC::PAIRS, E = P::E, NT = P::NT, K = TC::STAGES, NCONS = TC::NCONS;
     extern __shared__ unsigned char smraw[];
     unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
     float4 *stages = reinterpret_cast<float4 *>(base);
     float2 *tw = reinterpret_cast<float2 *>(base + (size_t)K * TC::STAGE_BYTES);
-    // the propagator tables, read at every element: staged once per block, so no consumer waits on L1 for them
-    float2 *s_px = tw + N, *s_pxe = s_px + N, *s_py = s_pxe + N, *s_pye = s_py + N;
-    int2 *s_cut = reinterpret_cast<int2 *>(s_pye + N);
-    uint64_t *full = reinterpret_cast<uint64_t *>(s_cut + N);
+    // the propagator's row tables, read at every element: staged once per block, so no consumer waits on L1
+    // for them (the column tables px, pxe and ycut are read once per item)
+    float2 *s_py = tw + N, *s_pye = s_py + N;
+    uint64_t *full = reinterpret_cast<uint64_t *>(s_pye + N);
     uint64_t *empty = full + K;
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -71,33 +74,62 @@ k_col_step_tma(const __grid_constant__ CUtensorMap tm, float2 *__restrict__ wave
     }
     for (int i = tid; i < N; i += TC::THREADS) {
         tw[i] = twg[i];
-        s_px[i] = pt.px[i];
-        s_pxe[i] = pt.pxe[i];
         s_py[i] = pt.py[i];
         s_pye[i] = pt.pye[i];
-        s_cut[i] = pt.ycut[i];
     }
     __syncthreads();
     PropTables<float> spt = pt;
-    spt.px = s_px; spt.pxe = s_pxe; spt.py = s_py; spt.pye = s_pye; spt.ycut = s_cut;
+    spt.py = s_py;
+    spt.pye = s_pye;
 
-    if (tid >= NCONS) {   // producer warp: one elected thread issues the tile loads
+    if (tid >= NCONS) {   // producer warp: one elected thread issues the tile loads (and, with TS, stores)
         if (tid == NCONS) {
             tma_prefetch_desc(&tm);
+            // wave and column tile of this block's k-th item
+            auto item_of = [&](int kk, int &w, int &tile) {
+                const int item = blockIdx.x + kk * gridDim.x;
+                w = item / n_active;
+                const int j = item - w * n_active;
+                tile = j < tiles_lo ? j : N / COLS - (n_active - j);
+            };
+            // store the results of item kk, which the consumers left in its stage (TS)
+            auto store = [&](int kk) {
+                int w, tile;
+                item_of(kk, w, tile);
+                const unsigned char *src = base + (size_t)(kk % K) * TC::STAGE_BYTES;
+#pragma unroll
+                for (int l = 0; l < TC::LOADS; l++)
+                    tma_store_2d(&tm, tile * TC::BOX_FLOATS, w * N + l * TC::BOX_ROWS,
+                                 src + (size_t)l * TC::BOX_ROWS * COLS * 8);
+                bulk_commit();
+            };
             int k = 0;
             bool ok = true;
             for (int item = blockIdx.x; item < n_items; item += gridDim.x, k++) {
                 const int s = k % K;
                 const unsigned use = (unsigned)(k / K);
                 if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, err, STEP_WAIT_EMPTY)) { ok = false; break; }
-                const int w = item / n_active, j = item - w * n_active;
-                const int tile = j < tiles_lo ? j : N / COLS - (n_active - j);
+                if constexpr (TS) {
+                    if (use > 0) {   // the stage holds item k - K's results: store them, then wait until read
+                        store(k - K);
+                        bulk_wait_read_all();
+                    }
+                }
+                int w, tile;
+                item_of(k, w, tile);
                 unsigned char *dst = base + (size_t)s * TC::STAGE_BYTES;
                 mbar_arrive_expect_tx(&full[s], TC::STAGE_BYTES);
 #pragma unroll
                 for (int l = 0; l < TC::LOADS; l++)
                     tma_load_2d(dst + (size_t)l * TC::BOX_ROWS * COLS * 8, &tm, tile * TC::BOX_FLOATS,
                                 w * N + l * TC::BOX_ROWS, &full[s]);
+            }
+            if constexpr (TS) {   // the last (up to K) items: store each once its consumers are done
+                for (int kk = k - K < 0 ? 0 : k - K; ok && kk < k; kk++) {
+                    if (!mbar_wait(&empty[kk % K], (unsigned)(kk / K) & 1, err, STEP_WAIT_EMPTY)) { ok = false; break; }
+                    store(kk);
+                }
+                bulk_wait_all();   // every store issued has written HBM and read its stage
             }
             if (!ok) {   // a wait was abandoned: let the loads already issued land before the block exits
                 for (int d = 1; d <= K && k - d >= 0; d++) {
@@ -129,14 +161,26 @@ k_col_step_tma(const __grid_constant__ CUtensorMap tm, float2 *__restrict__ wave
         fft_pair<N, -1>(va, vb, sm + p, ColAddr<PAIRS, 16>(), t, tw, cbar);
         prop_pair<N>(va, vb, spt, x, t, bscale);
         fft_pair<N, +1>(va, vb, sm + p, ColAddr<PAIRS, 16>(), t, tw, cbar);
-        // the stage's last reads are done: hand it back to the producer (the copy engine writes it next)
-        fence_proxy_async_smem();
-        __syncwarp();
-        if ((tid & 31) == 0) mbar_arrive(&empty[s]);
-        float4 *gb = reinterpret_cast<float4 *>(wave + (size_t)w * N * N + x);
+        if constexpr (TS) {
+            // every consumer has read its last exchange values: the stage takes the results, which the
+            // producer's TMA store then reads (the writes are ordered before it by the proxy fence and the
+            // release of the arrive)
+            cbar();
 #pragma unroll
-        for (int m = 0; m < E; m++)
-            gb[(size_t)(t + m * NT) * (N / 2)] = make_float4(va[m].x, va[m].y, vb[m].x, vb[m].y);
+            for (int m = 0; m < E; m++) sm[(t + m * NT) * PAIRS + p] = make_float4(va[m].x, va[m].y, vb[m].x, vb[m].y);
+            fence_proxy_async_smem();
+            __syncwarp();
+            if ((tid & 31) == 0) mbar_arrive(&empty[s]);
+        } else {
+            // the stage's last reads are done: hand it back to the producer (the copy engine writes it next)
+            fence_proxy_async_smem();
+            __syncwarp();
+            if ((tid & 31) == 0) mbar_arrive(&empty[s]);
+            float4 *gb = reinterpret_cast<float4 *>(wave + (size_t)w * N * N + x);
+#pragma unroll
+            for (int m = 0; m < E; m++)
+                gb[(size_t)(t + m * NT) * (N / 2)] = make_float4(va[m].x, va[m].y, vb[m].x, vb[m].y);
+        }
     }
 }
 

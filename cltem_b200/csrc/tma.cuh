@@ -4,8 +4,9 @@
 // shared-memory stages with cp.async.bulk.tensor (one elected thread; the copy engine moves the tile while
 // the consumer warps transform the previous one), and two mbarriers per stage hand each stage over:
 //   full[s]  : the producer arms it with the tile's byte count; the copy engine completes it
-//   empty[s] : each consumer warp arrives once it has read the stage for the last time
-// All loads are plain (no cluster multicast) and read this GPU's own wave buffer.
+//   empty[s] : each consumer warp arrives once it has read the stage for the last time (or, in the passes that
+//              store through TMA, once it has written its results into the stage)
+// All loads are plain (no cluster multicast) and read this GPU's own wave buffer; stores write only it.
 //
 // Every wait is bounded: a wait that does not complete within kWaitSpins polls records an error code in a
 // device word the host reads after the launch and reports, and the kernel winds down instead of hanging.
@@ -75,6 +76,21 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *m, int
         "l"(reinterpret_cast<uint64_t>(m)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
 }
+
+// 2-D tiled store of the box at element coordinates (x, y) of tensor map `m` from shared memory at src, in
+// this thread's current bulk async-group; same alignment rule as the load. The source must have been written
+// before a fence.proxy.async by its writers and a barrier that orders them before this thread.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *m, int x, int y, const void *src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<uint64_t>(m)),
+                 "r"(x), "r"(y), "r"(smem_u32(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// wait until this thread's bulk groups have finished reading their shared-memory sources (the stage may be
+// overwritten), or have completed entirely (their global writes are done)
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // named barrier over `count` threads (a multiple of 32) of the block
 struct NamedBar {
