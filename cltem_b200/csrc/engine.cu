@@ -1908,7 +1908,7 @@ struct Sim : SimBase {
                 const double r_ = rate_of(b, 0, variant);
                 if (r_ > best_rate) { best_rate = r_; best_b = b; best_v = variant; }
             }
-        for (int rv = 1; rv < ops.row_variants; rv++) {   // then the row pass's prefetch at that pair
+        for (int rv = 1; rv < ops.row_variants; rv++) {   // then the row pass's prefetch / order at that pair
             const double r_ = rate_of(best_b, rv, best_v);
             if (r_ > best_rate) { best_rate = r_; best_rv = rv; }
         }
@@ -1946,8 +1946,9 @@ struct Sim : SimBase {
             return ops.col_variant_name ? ops.col_variant_name(index) : std::string();
         }
         if (which != 1 || index < 0 || index >= ops.row_variants) throw ArgError("row step variant out of range");
-        static const char *names[3] = {"plain", "L2 prefetch of the rows one grid residency ahead",
-                                       "L2 prefetch of the rows two grid residencies ahead"};
+        static const char *names[4] = {"plain", "L2 prefetch of the rows one grid residency ahead",
+                                       "L2 prefetch of the rows two grid residencies ahead",
+                                       "wave-fastest grid order (the same rows of consecutive waves together)"};
         return names[index];
     }
     void get_tuning(int *batch, int *col, int *n_col, int *row, int *n_row) override {

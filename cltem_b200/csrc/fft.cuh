@@ -9,8 +9,8 @@
 // t + m*NT a thread loads from global memory, and the last stage writes exactly the elements
 // t + m*NT it stores, so only the inner stage boundaries go through shared memory.
 //
-// Sizes: N = 2^k (E = 8, radix-8 stages plus one radix-2/4 stage) and N = 3*2^k (E = 12, radix-4
-// stages, an optional radix-2 stage and one radix-3 stage). Unnormalised transforms; callers scale.
+// Sizes: N = 2^k (E = 8, radix-8 stages plus one radix-2/4 stage) and N = 3*2^k (E = 12, one radix-12
+// stage, radix-4 stages and an optional radix-2 stage). Unnormalised transforms; callers scale.
 #pragma once
 
 #include "common.cuh"
@@ -22,14 +22,16 @@ __host__ __device__ constexpr bool is_pow2(int n) { return n > 0 && (n & (n - 1)
 
 // The radix plan of a length, shared by the device stages and the host twiddle-table builder:
 // 2^k: k/3 radix-8 stages, then one radix-2 or radix-4 stage if k%3 != 0;
-// 3*2^k: k/2 radix-4 stages, a radix-2 stage if k is odd, then a radix-3 stage.
+// 3*2^k (k >= 2): one radix-12 stage (a prime-factor 3 x 4 DFT: no twiddles inside, dft12), (k-2)/2 radix-4
+// stages, then a radix-2 stage if k is odd. One exchange fewer than radix-3 and radix-4 stages apart (768: 4
+// stages instead of 5).
 __host__ __device__ constexpr int plan_k(int n) { return is_pow2(n) ? ilog2c(n) : ilog2c(n / 3); }
 __host__ __device__ constexpr int plan_nstages(int n) {
-    return is_pow2(n) ? (plan_k(n) / 3 + (plan_k(n) % 3 ? 1 : 0)) : (plan_k(n) / 2 + (plan_k(n) % 2) + 1);
+    return is_pow2(n) ? (plan_k(n) / 3 + (plan_k(n) % 3 ? 1 : 0)) : (1 + (plan_k(n) - 2) / 2 + (plan_k(n) % 2));
 }
 __host__ __device__ constexpr int plan_radix(int n, int s) {
     return is_pow2(n) ? (s < plan_k(n) / 3 ? 8 : (plan_k(n) % 3 == 1 ? 2 : 4))
-                      : (s < plan_k(n) / 2 ? 4 : ((plan_k(n) % 2 && s == plan_k(n) / 2) ? 2 : 3));
+                      : (s == 0 ? 12 : (s <= (plan_k(n) - 2) / 2 ? 4 : 2));
 }
 __host__ __device__ constexpr int plan_ns(int n, int s) { return s == 0 ? 1 : plan_ns(n, s - 1) * plan_radix(n, s - 1); }
 // Twiddle table layout: stage s >= 1 stores W_n^(r*k*n/(Ns*R)) for k < Ns, 1 <= r < R at
@@ -42,7 +44,7 @@ __host__ __device__ constexpr int plan_tw_index(int n, int s, int k, int r) {
 template <int N>
 struct Plan {
     static constexpr bool pow2 = is_pow2(N);
-    static_assert(pow2 || (N % 3 == 0 && is_pow2(N / 3)), "FFT length must be 2^k or 3*2^k");
+    static_assert(pow2 || (N % 3 == 0 && is_pow2(N / 3) && N >= 12), "FFT length must be 2^k or 3*2^k, k >= 2");
     static constexpr int E = pow2 ? 8 : 12;
     static constexpr int NT = N / E;
     static constexpr int nstages = plan_nstages(N);
@@ -120,10 +122,32 @@ template <class R, int SIGN> __device__ __forceinline__ void dft8(cplx<R> *a) {
     a[7] = csub(e3, w3o3);
 }
 
+// 12-point DFT as a prime-factor (Good-Thomas) 3 x 4 transform: with n = (4 n1 + 3 n2) mod 12 and
+// k = (4 k1 + 9 k2) mod 12, W12^(nk) = W3^(n1 k1) W4^(n2 k2), so four 3-point DFTs over n1 and three 4-point
+// DFTs over n2 give the transform with no twiddle products; the index maps cost nothing in registers.
+template <class R, int SIGN> __device__ __forceinline__ void dft12(cplx<R> *a) {
+    cplx<R> y[3][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) {
+        cplx<R> x0 = a[(3 * n2) % 12], x1 = a[(4 + 3 * n2) % 12], x2 = a[(8 + 3 * n2) % 12];
+        dft3<R, SIGN>(x0, x1, x2);
+        y[0][n2] = x0;
+        y[1][n2] = x1;
+        y[2][n2] = x2;
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 3; k1++) {
+        dft4<R, SIGN>(y[k1][0], y[k1][1], y[k1][2], y[k1][3]);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; k2++) a[(4 * k1 + 9 * k2) % 12] = y[k1][k2];
+    }
+}
+
 template <class R, int RAD, int SIGN> __device__ __forceinline__ void dft(cplx<R> *a) {
     if constexpr (RAD == 2) dft2<R, SIGN>(a[0], a[1]);
     else if constexpr (RAD == 3) dft3<R, SIGN>(a[0], a[1], a[2]);
     else if constexpr (RAD == 4) dft4<R, SIGN>(a[0], a[1], a[2], a[3]);
+    else if constexpr (RAD == 12) dft12<R, SIGN>(a);
     else dft8<R, SIGN>(a);
 }
 

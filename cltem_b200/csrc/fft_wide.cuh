@@ -48,7 +48,8 @@ __device__ __forceinline__ double cos_pi16(int phi) {
 }
 // FP32 values of cos(m pi / 16), m = 0..8, each (cos, sin) pair (c[m], c[8 - m]) picked among the roundings of
 // its two parts for the squared modulus closest to 1: an FFT round trip multiplies by |w|^2, and a modulus error
-// repeats at every slice. cos(pi/4) = 0.70710677 leaves 2 c^2 - 1 = -3.4e-8; kC4Lo carries its remainder.
+// repeats at every slice. cos(pi/4) = 0.70710677 leaves 2 c^2 - 1 = -3.4e-8, so cmul_wconst applies that one
+// through mul_rsqrt2, which carries its remainder.
 __device__ __forceinline__ float cos_pi16_f(int phi) {
     constexpr float c16[9] = {1.0f, 0.9807852506637573f, 0.9238795638084412f, 0.8314695954322815f, 0.7071067690849304f,
                               0.5555702447891235f, 0.3826833963394165f, 0.19509033858776093f, 0.0f};
@@ -56,23 +57,29 @@ __device__ __forceinline__ float cos_pi16_f(int phi) {
     const int m = phi <= 16 ? phi : 32 - phi;        // cos(phi pi/16) = cos((32 - phi) pi/16)
     return m <= 8 ? c16[m] : -c16[16 - m];             // cos((16 - m) pi/16) = -cos(m pi/16)
 }
-constexpr float kC4Lo = 1.2101617485882343e-08f;      // cos(pi/4) - 0.70710677f
 
 // x times exp(SIGN 2 pi i e / M) for M = 16 or 32: the angle is j pi / 16 with j = (32 / M) e; sin(x) = cos(x - pi/2).
-// FP32: the constants above, and at odd multiples of pi/4 the remainder of cos(pi/4) is added, so those
-// twiddles are exact to second order.
+// e is a compile-time constant at every call (unrolled loops), so the branches below fold away. FP32: the
+// multiples of pi/2 are exact sign swaps (a product with 0 or 1 is not folded by the compiler under IEEE rules,
+// so cmul would spend 2 instructions on them); the odd multiples of pi/4 scale the sum and difference of the
+// parts by cos(pi/4) plus its remainder (mul_rsqrt2), 6 instructions where a compensated cmul takes 10 and
+// exact to second order; the rest are one cmul with the constants above.
 template <class R, int SIGN, int M> __device__ __forceinline__ cplx<R> cmul_wconst(cplx<R> x, int e) {
-    const int j = (32 / M) * e;
+    const int j = ((32 / M) * e) & 31;
     if constexpr (sizeof(R) == 8) {
         return cmul(x, mk<R>((R)cos_pi16(j), (R)(SIGN * cos_pi16(j - 8))));
     } else {
-        const cplx<R> w = mk<R>(cos_pi16_f(j), (R)SIGN * cos_pi16_f(j - 8));
-        cplx<R> r = cmul(x, w);
-        if ((j & 7) == 4) {   // both parts are +-cos(pi/4)
-            const cplx<R> wl = mk<R>(w.x > 0 ? kC4Lo : -kC4Lo, w.y > 0 ? kC4Lo : -kC4Lo);
-            r = cadd(r, cmul(x, wl));
+        if (j == 0) return x;
+        if (j == 16) return mk<R>(-x.x, -x.y);
+        if (j == 8) return mul_i(x, SIGN);       // exp(SIGN i pi/2) = SIGN i
+        if (j == 24) return mul_i(x, -SIGN);
+        if ((j & 7) == 4) {                      // w = cos(pi/4) (sx, sy)
+            const R sx = cos_pi16_f(j) > 0 ? (R)1 : (R)-1;
+            const R sy = (R)SIGN * cos_pi16_f(j - 8) > 0 ? (R)1 : (R)-1;
+            // x w = cos(pi/4) (sx x.x - sy x.y, sy x.x + sx x.y)
+            return mk<R>(mul_rsqrt2<R>(sx * x.x - sy * x.y), mul_rsqrt2<R>(sy * x.x + sx * x.y));
         }
-        return r;
+        return cmul(x, mk<R>(cos_pi16_f(j), (R)SIGN * cos_pi16_f(j - 8)));
     }
 }
 

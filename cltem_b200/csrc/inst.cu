@@ -26,25 +26,26 @@ template <class K> void set_smem(K kernel, size_t bytes) {
 }
 
 // the two-column step kernel of the FP32 plans (templates, so that the FP64 build discards them) with a tile of
-// C columns: C = PairStepCfg::COLS (the measured default), half or twice that where the tile is valid
-template <class RR, int C> constexpr bool pair_tile_ok() {
+// C columns: C = PairStepCfg::COLS (the measured default), half or twice that where the tile is valid; L the
+// register budget (false: 64 registers a thread, true: 128; pair_loose is the measured default)
+template <class RR, int C, bool L = pair_loose<N>()> constexpr bool pair_tile_ok() {
     if constexpr (std::is_same<RR, float>::value && pair_columns<N>() && C >= 2 && C <= N) {
-        return PairCfg<N, C, pair_loose<N>()>::ok && C % CC::COLS == 0 && N % C == 0;
+        return PairCfg<N, C, L>::ok && C % CC::COLS == 0 && N % C == 0;
     } else {
         return false;
     }
 }
-template <class RR, int C> void pair_attrs() {
-    if constexpr (pair_tile_ok<RR, C>()) {
-        using PC = PairCfg<N, C, pair_loose<N>()>;
-        set_smem(k_col_step_pair<N, C, pair_loose<N>()>, PC::smem());
+template <class RR, int C, bool L = pair_loose<N>()> void pair_attrs() {
+    if constexpr (pair_tile_ok<RR, C, L>()) {
+        using PC = PairCfg<N, C, L>;
+        set_smem(k_col_step_pair<N, C, L>, PC::smem());
     }
 }
-template <class RR, int C>
+template <class RR, int C, bool L = pair_loose<N>()>
 bool pair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw, PropTables<RR> pt, RR b, int tiles_lo,
                int tiles_hi) {
-    if constexpr (pair_tile_ok<RR, C>()) {
-        using PC = PairCfg<N, C, pair_loose<N>()>;
+    if constexpr (pair_tile_ok<RR, C, L>()) {
+        using PC = PairCfg<N, C, L>;
         // the engine's tiles are CC::COLS wide and the step's tile covers k of them; the extra columns of a
         // partly active tile lie outside the propagator's cut and come out zero, and the row pass never
         // reads them
@@ -52,8 +53,8 @@ bool pair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw, Pr
         static_assert(C % CC::COLS == 0, "the step's tile must cover whole engine tiles");
         int lo = (tiles_lo + k - 1) / k, hi = (tiles_hi + k - 1) / k;
         if (lo + hi > total) { lo = total; hi = 0; }
-        k_col_step_pair<N, C, pair_loose<N>()><<<dim3(lo + hi, batch), dim3(PC::PAIRS, Plan<N>::NT), PC::smem(), s>>>(
-            wave, tw, pt, b, lo);
+        k_col_step_pair<N, C, L><<<dim3(lo + hi, batch), dim3(PC::PAIRS, Plan<N>::NT), PC::smem(), s>>>(wave, tw, pt, b,
+                                                                                                        lo);
         MS_CUDA(cudaGetLastError());
         return true;
     } else {
@@ -87,14 +88,15 @@ template <class RR, int V> constexpr bool tma_col_ok() {
 }
 // The column-step kernels of this size, by kind: 0 the two-column step at its default tile, 1 / 2 the
 // persistent TMA-fed passes, 3 / 4 the two-column step at half / twice the default tile, 5 / 6 the persistent
-// passes 1 / 2 storing through TMA, 7 / 8 the two-stage persistent passes 5 / 6. A variant index of
-// PassOps::col_step is a position in the list of the kinds valid here (kind 0 always first).
+// passes 1 / 2 storing through TMA, 7 / 8 the two-stage persistent passes 5 / 6, 9 the two-column step at its
+// default tile with the other register budget. A variant index of PassOps::col_step is a position in the list
+// of the kinds valid here (kind 0 always first).
 struct KindList {
-    int kind[9];
+    int kind[10];
     int n;
 };
 template <class RR> constexpr KindList col_kinds() {
-    KindList k{{0, -1, -1, -1, -1, -1, -1, -1, -1}, 1};
+    KindList k{{0, -1, -1, -1, -1, -1, -1, -1, -1, -1}, 1};
     if (tma_col_ok<RR, 1>()) k.kind[k.n++] = 1;
     if (tma_col_ok<RR, 2>()) k.kind[k.n++] = 2;
     if (pair_tile_ok<RR, kPairC / 2>()) k.kind[k.n++] = 3;
@@ -103,6 +105,7 @@ template <class RR> constexpr KindList col_kinds() {
     if (tma_col_ok<RR, 4>()) k.kind[k.n++] = 6;
     if (tma_col_ok<RR, 5>()) k.kind[k.n++] = 7;
     if (tma_col_ok<RR, 6>()) k.kind[k.n++] = 8;
+    if (pair_tile_ok<RR, kPairC, !pair_loose<N>()>()) k.kind[k.n++] = 9;
     return k;
 }
 template <class RR> constexpr int tma_col_variants() { return col_kinds<RR>().n; }
@@ -121,6 +124,9 @@ std::string col_variant_name(int v) {
     if (kind == 5) return "persistent, TMA loads and stores, " + cols(kPairC) + ", 3 stages, 1 block per SM";
     if (kind == 6) return "persistent, TMA loads and stores, " + cols(kPairC / 2) + ", 3 stages, 2 blocks per SM";
     if (kind == 7) return "persistent, TMA-fed, " + cols(kPairC / 2) + ", 2 stages, 1 block per SM";
+    if (kind == 9)
+        return "one block per (" + cols(kPairC) + ", wave), two columns a thread, " +
+               (pair_loose<N>() ? "64" : "128") + "-register budget";
     return "persistent, TMA loads and stores, " + cols(kPairC / 2) + ", 2 stages, 1 block per SM";
 }
 int g_sms[64] = {};
@@ -179,11 +185,12 @@ bool rowpair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tra
         static int res[64] = {};
         int dev = 0;
         MS_CUDA(cudaGetDevice(&dev));
-        if (variant > 0 && !res[dev])
+        if (variant > 0 && variant < 3 && !res[dev])
             res[dev] = resident_blocks(k_row_step_pair<N, PR>, Plan<N>::NT * PR, RowPairStepCfg<N>::smem());
-        const int pf = variant > 0 ? variant * res[dev] : 0;
-        k_row_step_pair<N, PR><<<dim3(N / (2 * PR), batch), dim3(Plan<N>::NT, PR), RowPairStepCfg<N>::smem(), s>>>(
-            wave, trans, tw, a, xa, xb, load_all, tsel, tstride, pf);
+        const int pf = variant == 3 ? kWaveFastRows : (variant > 0 ? variant * res[dev] : 0);
+        const dim3 g = variant == 3 ? dim3(batch, N / (2 * PR)) : dim3(N / (2 * PR), batch);
+        k_row_step_pair<N, PR><<<g, dim3(Plan<N>::NT, PR), RowPairStepCfg<N>::smem(), s>>>(wave, trans, tw, a, xa, xb,
+                                                                                         load_all, tsel, tstride, pf);
         MS_CUDA(cudaGetLastError());
         return true;
     } else {
@@ -205,6 +212,7 @@ void ensure_attrs() {
     pair_attrs<R, kPairC>();
     pair_attrs<R, kPairC / 2>();
     pair_attrs<R, kPairC * 2>();
+    pair_attrs<R, kPairC, !pair_loose<N>()>();
     tma_col_attrs<R, 1>();
     tma_col_attrs<R, 2>();
     tma_col_attrs<R, 3>();
@@ -224,6 +232,7 @@ void ensure_attrs() {
 }
 
 inline dim3 row_grid(int batch) { return dim3(N / RC::ROWS, batch); }
+inline dim3 row_grid_wave_fast(int batch) { return dim3(batch, N / RC::ROWS); }
 inline dim3 row_block() { return dim3(RC::P::NT, RC::ROWS); }
 
 // the FP64 row step built for 3 blocks per SM where that is set (fp64_step_minb)
@@ -231,8 +240,8 @@ template <class RR>
 bool row_step_d(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans, const cplx<RR> *tw, RR a, int xa,
                 int xb, int load_all, const int *tsel, size_t tstride, int pf) {
     if constexpr (std::is_same<RR, double>::value && fp64_row_bounded<N>()) {
-        k_row_step_d<N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all, tsel,
-                                                                       tstride, pf);
+        k_row_step_d<N><<<pf == kWaveFastRows ? row_grid_wave_fast(batch) : row_grid(batch), row_block(), RC::smem(),
+                          s>>>(wave, trans, tw, a, xa, xb, load_all, tsel, tstride, pf);
         MS_CUDA(cudaGetLastError());
         return true;
     } else {
@@ -245,16 +254,17 @@ inline dim3 col_block() { return dim3(CC::COLS, CC::P::NT); }
 void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a, int xa, int xb,
               int load_all, const int *tsel, size_t tstride, int variant) {
     ensure_attrs();
-    if (variant < 0 || variant > 2) throw std::runtime_error("row pass variant out of range");
+    if (variant < 0 || variant > 3) throw std::runtime_error("row pass variant out of range");
+    if (batch > 65535 && variant != 3) throw std::runtime_error("batch too large for the row grid");
     if (rowpair_step<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride, variant)) return;
     static int res[64] = {};
     int dev = 0;
     MS_CUDA(cudaGetDevice(&dev));
-    if (variant > 0 && !res[dev]) res[dev] = resident_blocks(k_row_step<R, N>, RC::THREADS, RC::smem());
-    const int pf = variant > 0 ? variant * res[dev] : 0;
+    if (variant > 0 && variant < 3 && !res[dev]) res[dev] = resident_blocks(k_row_step<R, N>, RC::THREADS, RC::smem());
+    const int pf = variant == 3 ? kWaveFastRows : (variant > 0 ? variant * res[dev] : 0);
     if (row_step_d<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride, pf)) return;
-    k_row_step<R, N><<<row_grid(batch), row_block(), RC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all, tsel, tstride,
-                                                                   pf);
+    k_row_step<R, N><<<pf == kWaveFastRows ? row_grid_wave_fast(batch) : row_grid(batch), row_block(), RC::smem(), s>>>(
+        wave, trans, tw, a, xa, xb, load_all, tsel, tstride, pf);
     MS_CUDA(cudaGetLastError());
 }
 void row_fft(cudaStream_t s, const cplx<R> *in, cplx<R> *out, int batch, const cplx<R> *tw, R scale, int sign) {
@@ -279,6 +289,7 @@ void col_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, PropT
         if (kind == 6 && tma_col_step<R, 4>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 7 && tma_col_step<R, 5>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 8 && tma_col_step<R, 6>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 9 && pair_step<R, kPairC, !pair_loose<N>()>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 3 && pair_step<R, kPairC / 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 4 && pair_step<R, kPairC * 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (pair_step<R, kPairC>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;

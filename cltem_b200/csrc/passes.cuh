@@ -174,8 +174,12 @@ __device__ __forceinline__ void prefetch_rows(const C *wave, int N, int rows_per
 }
 
 // ------------------------------------------------------------------------------------------------
-// Row kernels: grid (res/ROWS, batch), block (NT, ROWS)
+// Row kernels: grid (res/ROWS, batch), block (NT, ROWS); with pf == kWaveFastRows the grid is (batch,
+// res/ROWS) instead, so the blocks the scheduler issues together hold the same rows of consecutive waves and
+// read the same transmission rows (from L2 after the first), where the usual order reads a whole wave's
+// worth of wave rows between two reads of a transmission row (at 2048² a slice of T is 32 MB).
 // ------------------------------------------------------------------------------------------------
+constexpr int kWaveFastRows = -1;
 // The multislice row pass: phi <- D_r(T * a * Dinv_r phi).
 // Band limit: the column pass multiplies by P, which is zero in every column with kx^2 >= k_cut^2, so
 // between passes only the columns x < xa or x >= xb (whole column tiles) carry data. The row pass reads
@@ -205,10 +209,11 @@ __device__ __forceinline__ void row_step_body(cplx<R> *__restrict__ wave, const 
     const int t = threadIdx.x;
     const cplx<R> *tw =
         twiddles_for<RC::TWG, R>(tws, twg + RC::TW_OFF, RC::TWN, t + threadIdx.y * P::NT, P::NT * ROWS);
-    const int y = blockIdx.x * ROWS + threadIdx.y;
-    cplx<R> *row = wave + (size_t)blockIdx.y * N * N + (size_t)y * N;
+    const int rblk = pf == kWaveFastRows ? blockIdx.y : blockIdx.x, w = pf == kWaveFastRows ? blockIdx.x : blockIdx.y;
+    const int y = rblk * ROWS + threadIdx.y;
+    cplx<R> *row = wave + (size_t)w * N * N + (size_t)y * N;
     // tsel (optional): transmission set of each wave; set k of this slice starts k * tstride after trans
-    const cplx<R> *trow = trans + (tsel ? (size_t)tsel[blockIdx.y] * tstride : (size_t)0) + (size_t)y * N;
+    const cplx<R> *trow = trans + (tsel ? (size_t)tsel[w] * tstride : (size_t)0) + (size_t)y * N;
     cplx<R> v[P::E];
 #pragma unroll
     for (int m = 0; m < P::E; m++) {
@@ -285,9 +290,10 @@ k_row_step_pair(float2 *__restrict__ wave, const float2 *__restrict__ trans, con
     float4 *sm = reinterpret_cast<float4 *>(tw + N) + (size_t)threadIdx.y * N;
     const int t = threadIdx.x;
     load_table<float>(tw, twg, N, t + threadIdx.y * NT, NT * PC::PAIRS);
-    const int y = (blockIdx.x * PC::PAIRS + threadIdx.y) * 2;
-    float2 *ra = wave + (size_t)blockIdx.y * N * N + (size_t)y * N, *rb = ra + N;
-    const float2 *ta = trans + (tsel ? (size_t)tsel[blockIdx.y] * tstride : (size_t)0) + (size_t)y * N, *tb = ta + N;
+    const int rblk = pf == kWaveFastRows ? blockIdx.y : blockIdx.x, w = pf == kWaveFastRows ? blockIdx.x : blockIdx.y;
+    const int y = (rblk * PC::PAIRS + threadIdx.y) * 2;
+    float2 *ra = wave + (size_t)w * N * N + (size_t)y * N, *rb = ra + N;
+    const float2 *ta = trans + (tsel ? (size_t)tsel[w] * tstride : (size_t)0) + (size_t)y * N, *tb = ta + N;
     float2 va[E], vb[E];
 #pragma unroll
     for (int m = 0; m < E; m++) {

@@ -328,7 +328,8 @@ int mslice_tune_batch(mslice_sim *sim, const int *candidates, int n_candidates, 
  * shared-memory stages with TMA (power-of-two grids where their shared memory fits), and the one-block-per-tile
  * kernel at half and twice the default tile width (mslice_step_variant_name describes each). Row step: 0 =
  * plain; 1, 2 = each block also asks the copy engine to prefetch into L2 the rows that the blocks one or two
- * residencies of the grid later will read. All variants give bit-identical results. Out-of-range values fail
+ * residencies of the grid later will read; 3 = the grid in wave-fastest order, so blocks issued together read
+ * the same transmission rows. All variants give bit-identical results. Out-of-range values fail
  * with MSLICE_ERR_ARG. */
 int mslice_set_step_variant(mslice_sim *sim, int col_variant, int row_variant);
 /* A description of step-kernel variant `index` (which: 0 column, 1 row) of this simulation's grid and

@@ -56,17 +56,17 @@ def test_column_step_variants_are_bit_identical(gpu_ctx, kirkland, res):
     sim.set_atoms(conf)
     t = sim.tuning()
     nv = t["col_variants"]
-    assert t["row_variants"] == 3
+    assert t["row_variants"] == 4
     assert nv >= (2 if res <= 512 else 1)   # the persistent passes where their stages and tables fit
     names = [sim.step_variant_name(0, v) for v in range(nv)]
     assert len(set(names)) == nv and all(names)
-    assert len({sim.step_variant_name(1, v) for v in range(3)}) == 3
+    assert len({sim.step_variant_name(1, v) for v in range(4)}) == 4
     with pytest.raises(MsliceError):
         sim.step_variant_name(0, nv)
     pix = np.arange(144, dtype=np.int32)
     out = []
     for v in range(nv):
-        for rv in range(3):   # the row pass with and without its L2 prefetch
+        for rv in range(4):   # the row pass with and without its L2 prefetch, and in wave-fastest order
             sim.set_step_variant(v, rv)
             assert sim.tuning()["col_variant"] == v and sim.tuning()["row_variant"] == rv
             out.append(sim.stem(pix))
@@ -76,7 +76,7 @@ def test_column_step_variants_are_bit_identical(gpu_ctx, kirkland, res):
     with pytest.raises(MsliceError):
         sim.set_step_variant(nv, 0)
     with pytest.raises(MsliceError):
-        sim.set_step_variant(0, 3)
+        sim.set_step_variant(0, 4)
     sim.close()
 
 
