@@ -446,13 +446,14 @@ def cbed3d_leg(ctx, ext, nz=60):
             "note": "one configuration of the 50; evaluations counted on the host from the binned atoms"}
 
 
-def sizes_leg(ctx, sizes, dp=False, n_atoms=30, seed=11, tune=True):
+def sizes_leg(ctx, sizes, dp=False, n_atoms=30, seed=11, tune=True, variants=None):
     """The step kernels at each grid: FP32 (or FP64) STEM of about 1 GiB of waves (at most 1024 probes)
     through 7 slices of 0.25 Å over a 400 Å field holding a few seeded atoms; device time per probe·slice of
     the row and column passes (the column figure includes the last step of each batch, which carries the
     detector reduction), from the engine's per-kernel event timing of the third of three runs. With `tune` the
     autotuner picks each grid's probe batch and step kernels first (as a STEM run of that grid would), and
-    the figures are also given per pixel, relative to 512²."""
+    the figures are also given per pixel, relative to 512². `variants` = (column, row) fixes the step kernels
+    instead (mslice_set_step_variant; the indices are per grid), with the engine's default batch."""
     import torch
     from cltem_b200 import config
     from cltem_b200.engine import Simulation
@@ -475,7 +476,9 @@ def sizes_leg(ctx, sizes, dp=False, n_atoms=30, seed=11, tune=True):
         sim = Simulation(ctx, c)
         sim.set_atoms(st)
         tuned = None
-        if tune:
+        if variants is not None:
+            sim.set_step_variant(*variants)
+        elif tune:
             cands = [b for b in (2, 4, 8, 16, 32, 64, 128, 256, 512, 1024) if b <= npr]
             tuned = sim.tune_batch(cands)
         pix = np.arange(npr, dtype=np.int32)
@@ -492,9 +495,9 @@ def sizes_leg(ctx, sizes, dp=False, n_atoms=30, seed=11, tune=True):
         row_us, col_us = 1e3 * p["row_step"][0] / (npr * S), 1e3 * p["col_step"][0] / (npr * S)
         out[str(res)] = {"probes": npr, "slices": S, "row_us_per_probe_slice": row_us,
                          "col_us_per_probe_slice": col_us, "ps_per_pixel": 1e6 * (row_us + col_us) / (res * res)}
-        if tuned:
+        if tuned or variants is not None:
             tn = sim.tuning()
-            out[str(res)].update({"batch": tuned[0], "column": sim.step_variant_name(0, tn["col_variant"]),
+            out[str(res)].update({"batch": tuned[0] if tuned else tn["batch"], "column": sim.step_variant_name(0, tn["col_variant"]),
                                   "row": sim.step_variant_name(1, tn["row_variant"])})
         sim.close()
     if "512" in out:
@@ -580,7 +583,8 @@ def main():
         ext = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
         leg = {"adjoint": lambda: adjoint_leg(ctx, ext, args.warmup), "cbed3d": lambda: cbed3d_leg(ctx, ext, args.cbed_nz),
                "uneven": lambda: uneven_leg(ctx), "cufft": lambda: cufft_leg(),
-               "sizes": lambda: sizes_leg(ctx, [int(v) for v in args.sizes.split(",")])}[args.only]()
+               "sizes": lambda: sizes_leg(ctx, [int(v) for v in args.sizes.split(",")],
+                                          variants=tuple(int(v) for v in args.variants.split(":")) if args.variants else None)}[args.only]()
         print(json.dumps({"leg": args.only, **leg}))
         return 0
     if world > 1:

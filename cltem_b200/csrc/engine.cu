@@ -341,9 +341,10 @@ struct Ctx {
         if (it != m.end()) return (const cplx<R> *)it->second;
         // entries [0, n): the radix-8 plan's packed per-stage table (fft.cuh, plan_tw_index),
         // W_n^(r*k*n/(Ns*R)) = exp(-2 pi i r k / (Ns*R)); for sizes whose row passes use the wide two-stage
-        // plan (fft_wide.cuh) entries [n, 2n) hold its table, W_n^(r k) at k (R2 - 1) + r - 1
-        const bool wide = wide_plan<R>(n);
-        const size_t count = (size_t)n * (wide ? 2 : 1);
+        // plan (fft_wide.cuh) entries [n, 2n) hold its table, W_n^(r k) at k (R2 - 1) + r - 1; for the
+        // three-stage wide plan they hold its stages' tables in the packed layout (Wide3Plan::tw_base)
+        const bool wide = wide_plan<R>(n), wide3 = !wide && wide3_plan<R>(n);
+        const size_t count = (size_t)n * ((wide || wide3) ? 2 : 1);
         std::vector<cplx<R>> h(count, mk<R>(0, 0));
         const long double two_pi = 2.0L * 3.14159265358979323846264338327950288L;
         for (int s = 1; s < plan_nstages(n); s++) {
@@ -353,6 +354,22 @@ struct Ctx {
                     long double a = -two_pi * (long double)(r * k) / (long double)(Ns * RAD);
                     h[plan_tw_index(n, s, k, r)] = round_unit<R>(std::cos(a), std::sin(a));
                 }
+        }
+        if (wide3) {
+            auto fill = [&](auto plan) {
+                using P = decltype(plan);
+                for (int st = 1; st < P::nstages; st++) {
+                    const int Ns = P::ns(st), RAD = P::radix(st);
+                    for (int k = 0; k < Ns; k++)
+                        for (int r = 1; r < RAD; r++) {
+                            long double a = -two_pi * (long double)(r * k) / (long double)(Ns * RAD);
+                            h[n + P::tw_base(st) + k * (RAD - 1) + (r - 1)] = round_unit<R>(std::cos(a), std::sin(a));
+                        }
+                }
+            };
+            if (n == 2048) fill(Wide3Plan<2048>());
+            else if (n == 4096) fill(Wide3Plan<4096>());
+            else fill(Wide3Plan<8192>());
         }
         if (wide) {
             const int E = wide_E(n), R2 = n / E;

@@ -50,6 +50,8 @@ struct Plan {
     static constexpr int nstages = plan_nstages(N);
     __host__ __device__ static constexpr int radix(int s) { return plan_radix(N, s); }
     __host__ __device__ static constexpr int ns(int s) { return plan_ns(N, s); }
+    // first entry of stage s's twiddles (s >= 1) in the packed table
+    __host__ __device__ static constexpr int tw_base(int s) { return plan_tw_index(N, s, 0, 1); }
 };
 
 // ---- small DFTs in registers; SIGN = -1 forward, +1 inverse --------------------------------------
@@ -143,11 +145,17 @@ template <class R, int SIGN> __device__ __forceinline__ void dft12(cplx<R> *a) {
     }
 }
 
+// the wide radices (fft_wide.cuh), for plans that mix them with the radix-8 stages
+template <class R, int SIGN> __device__ __forceinline__ void dft16(cplx<R> *a);
+template <class R, int SIGN> __device__ __forceinline__ void dft32(cplx<R> *a);
+
 template <class R, int RAD, int SIGN> __device__ __forceinline__ void dft(cplx<R> *a) {
     if constexpr (RAD == 2) dft2<R, SIGN>(a[0], a[1]);
     else if constexpr (RAD == 3) dft3<R, SIGN>(a[0], a[1], a[2]);
     else if constexpr (RAD == 4) dft4<R, SIGN>(a[0], a[1], a[2], a[3]);
     else if constexpr (RAD == 12) dft12<R, SIGN>(a);
+    else if constexpr (RAD == 16) dft16<R, SIGN>(a);
+    else if constexpr (RAD == 32) dft32<R, SIGN>(a);
     else dft8<R, SIGN>(a);
 }
 
@@ -185,16 +193,16 @@ struct NamedSync {
 // v: E elements in "natural strided" order v[m] = x[t + m*NT] on entry and exit.
 // sm: this transform's shared memory (element 0), ad: addressing, tw: the packed twiddle table.
 // All threads of the block must call this together (it contains __syncthreads()).
-template <class R, int N, int SIGN, int S, class Addr, class Sync>
-__device__ __forceinline__ void fft_stages(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm, Addr ad, int t, const cplx<R> *tw,
+// P: the radix plan (Plan<N>, or another with the same members: E, NT, nstages, radix, ns, tw_base).
+template <class R, int N, int SIGN, int S, class Addr, class Sync, class P = Plan<N>>
+__device__ __forceinline__ void fft_stages(cplx<R> (&v)[P::E], cplx<R> *sm, Addr ad, int t, const cplx<R> *tw,
                                            Sync sync) {
-    using P = Plan<N>;
     constexpr int E = P::E, NT = P::NT;
     constexpr int RAD = P::radix(S);
     constexpr int Ns = P::ns(S);
     constexpr int NB = E / RAD;          // butterflies per thread
     constexpr bool last = (S == P::nstages - 1);
-    constexpr int TWB = plan_tw_index(N, S > 0 ? S : 1, 0, 1);   // this stage's block of the twiddle table
+    constexpr int TWB = P::tw_base(S > 0 ? S : 1);   // this stage's block of the twiddle table
     if constexpr (S > 0) {
 #pragma unroll
         for (int b = 0; b < NB; b++) {
@@ -238,7 +246,7 @@ __device__ __forceinline__ void fft_stages(cplx<R> (&v)[Plan<N>::E], cplx<R> *sm
             for (int m = 0; m < RAD; m++) sm[ad(idxD + m * Ns)] = out[b + m * NB];
         }
         sync();
-        fft_stages<R, N, SIGN, S + 1, Addr, Sync>(v, sm, ad, t, tw, sync);
+        fft_stages<R, N, SIGN, S + 1, Addr, Sync, P>(v, sm, ad, t, tw, sync);
     }
 }
 

@@ -127,6 +127,30 @@ template <class R, int RAD, int SIGN> __device__ __forceinline__ void dft_wide(c
     else dft16<R, SIGN>(a);
 }
 
+// The three-stage wide plan of the FP32 rows at 2048, 4096 and 8192: stage A a radix-32 DFT of each thread's
+// 32 elements in registers (no twiddles), then two Stockham stages of radix R1 x R2 (8 x 8 at 2048, 16 x 8 at
+// 4096, 16 x 16 at 8192) through fft_stages, so a transform makes two shared-memory exchanges where the
+// radix-8 plan makes three (four at 8192), with NT = N / 32 threads (2, 4 or 8 warps) a row. Rows of 32 elements are padded by one in shared
+// memory (WideRowAddr<32>), which keeps stage A's row writes and the later strided reads conflict-free.
+template <class R> __host__ __device__ constexpr bool wide3_plan(int n) {
+    return sizeof(R) == 4 && (n == 2048 || n == 4096 || n == 8192);
+}
+template <int N> struct Wide3Plan {
+    static constexpr int E = 32;
+    static constexpr int NT = N / E;
+    static constexpr int R1 = N == 2048 ? 8 : 16;
+    static constexpr int R2 = N / (E * R1);
+    static constexpr int nstages = 3;
+    __host__ __device__ static constexpr int radix(int s) { return s == 0 ? E : (s == 1 ? R1 : R2); }
+    __host__ __device__ static constexpr int ns(int s) { return s == 0 ? 1 : (s == 1 ? E : E * R1); }
+    // the packed table (W_{Ns RAD}^(r k) of stage s >= 1 at tw_base(s) + k (RAD - 1) + r - 1, k < Ns)
+    __host__ __device__ static constexpr int tw_base(int s) { return s <= 1 ? 0 : E * (R1 - 1); }
+    static constexpr int TW = E * (R1 - 1) + E * R1 * (R2 - 1);   // = N - 32
+    static constexpr int ROWSZ = NT * (E + 1);                     // padded shared elements of one transform
+    static_assert((N != 2048 && N != 4096 && N != 8192) || (E * R1 * R2 == N && E % R1 == 0 && E % R2 == 0),
+                  "three-stage wide plan");
+};
+
 // threads of one transform within one warp (row tiles of the wide plan)
 struct WarpSync {
     __device__ __forceinline__ void operator()() const { __syncwarp(); }

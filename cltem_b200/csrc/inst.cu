@@ -64,20 +64,30 @@ bool pair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw, Pr
 // C of the default two-column step (a valid value for the FP64 build too, where nothing uses it)
 constexpr int kPairC = pair_columns<N>() ? PairStepCfg<N>::COLS : 2;
 
-// The persistent TMA-fed column passes of the FP32 power-of-two plans (passes_tma.cuh), by variant, where
+// The persistent TMA-fed column passes of the FP32 plans (passes_tma.cuh), by variant, where
 // their stages and tables fit in shared memory:
 //   1: the step's tile (PairStepCfg::COLS columns), 3 stages, one block per SM
 //   2: half that tile, 3 stages, two blocks per SM
 //   3, 4: as 1, 2, with the results stored from the stage by TMA instead of from the consumers' registers
-//   5, 6: half the step's tile, 2 stages, one block per SM, stores from registers / by TMA (the grids whose
-//         tile column of N rows is too tall for three stages, e.g. 2048^2)
+//   5, 6: half the step's tile, as many stages as fit (at most 6), one block per SM, stores from registers /
+//         by TMA (the grids whose default tile is too tall for three stages, 1024^2 and up)
+//   7: as 6 with the twiddles read from global memory, which frees room for one more stage (2048^2)
 template <int V> struct TmaVariant;
 template <> struct TmaVariant<1> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS, 3, 1>; };
 template <> struct TmaVariant<2> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, 3, 2>; };
 template <> struct TmaVariant<3> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS, 3, 1, true>; };
 template <> struct TmaVariant<4> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, 3, 2, true>; };
-template <> struct TmaVariant<5> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, 2, 1>; };
-template <> struct TmaVariant<6> { template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, 2, 1, true>; };
+template <> struct TmaVariant<5> {
+    template <int NN> using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, tma_fit_stages<NN, PairStepCfg<NN>::COLS / 2, false>(), 1>;
+};
+template <> struct TmaVariant<6> {
+    template <int NN>
+    using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, tma_fit_stages<NN, PairStepCfg<NN>::COLS / 2, false>(), 1, true>;
+};
+template <> struct TmaVariant<7> {
+    template <int NN>
+    using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, tma_fit_stages<NN, PairStepCfg<NN>::COLS / 2, true>(), 1, true, true>;
+};
 template <class RR, int V> constexpr bool tma_col_ok() {
     if constexpr (std::is_same<RR, float>::value && pair_columns<N>()) {
         using TC = typename TmaVariant<V>::template Cfg<N>;
@@ -88,15 +98,15 @@ template <class RR, int V> constexpr bool tma_col_ok() {
 }
 // The column-step kernels of this size, by kind: 0 the two-column step at its default tile, 1 / 2 the
 // persistent TMA-fed passes, 3 / 4 the two-column step at half / twice the default tile, 5 / 6 the persistent
-// passes 1 / 2 storing through TMA, 7 / 8 the two-stage persistent passes 5 / 6, 9 the two-column step at its
-// default tile with the other register budget. A variant index of PassOps::col_step is a position in the list
-// of the kinds valid here (kind 0 always first).
+// passes 1 / 2 storing through TMA, 7 / 8 / 10 the deep-ring persistent passes 5 / 6 / 7, 9 the two-column step
+// at its default tile with the other register budget. A variant index of PassOps::col_step is a position in the
+// list of the kinds valid here (kind 0 always first).
 struct KindList {
-    int kind[10];
+    int kind[11];
     int n;
 };
 template <class RR> constexpr KindList col_kinds() {
-    KindList k{{0, -1, -1, -1, -1, -1, -1, -1, -1, -1}, 1};
+    KindList k{{0, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1}, 1};
     if (tma_col_ok<RR, 1>()) k.kind[k.n++] = 1;
     if (tma_col_ok<RR, 2>()) k.kind[k.n++] = 2;
     if (pair_tile_ok<RR, kPairC / 2>()) k.kind[k.n++] = 3;
@@ -106,6 +116,7 @@ template <class RR> constexpr KindList col_kinds() {
     if (tma_col_ok<RR, 5>()) k.kind[k.n++] = 7;
     if (tma_col_ok<RR, 6>()) k.kind[k.n++] = 8;
     if (pair_tile_ok<RR, kPairC, !pair_loose<N>()>()) k.kind[k.n++] = 9;
+    if (tma_col_ok<RR, 7>()) k.kind[k.n++] = 10;
     return k;
 }
 template <class RR> constexpr int tma_col_variants() { return col_kinds<RR>().n; }
@@ -123,11 +134,18 @@ std::string col_variant_name(int v) {
     if (kind == 2) return "persistent, TMA-fed, " + cols(kPairC / 2) + ", 3 stages, 2 blocks per SM";
     if (kind == 5) return "persistent, TMA loads and stores, " + cols(kPairC) + ", 3 stages, 1 block per SM";
     if (kind == 6) return "persistent, TMA loads and stores, " + cols(kPairC / 2) + ", 3 stages, 2 blocks per SM";
-    if (kind == 7) return "persistent, TMA-fed, " + cols(kPairC / 2) + ", 2 stages, 1 block per SM";
+    auto stages = [](int n) { return std::to_string(n) + " stages"; };
+    if (kind == 7)
+        return "persistent, TMA-fed, " + cols(kPairC / 2) + ", " + stages(TmaVariant<5>::Cfg<N>::STAGES) +
+               ", 1 block per SM";
+    if (kind == 10)
+        return "persistent, TMA loads and stores, " + cols(kPairC / 2) + ", " + stages(TmaVariant<7>::Cfg<N>::STAGES) +
+               ", twiddles from L1, 1 block per SM";
     if (kind == 9)
         return "one block per (" + cols(kPairC) + ", wave), two columns a thread, " +
                (pair_loose<N>() ? "64" : "128") + "-register budget";
-    return "persistent, TMA loads and stores, " + cols(kPairC / 2) + ", 2 stages, 1 block per SM";
+    return "persistent, TMA loads and stores, " + cols(kPairC / 2) + ", " + stages(TmaVariant<6>::Cfg<N>::STAGES) +
+           ", 1 block per SM";
 }
 int g_sms[64] = {};
 int sm_count() {
@@ -140,7 +158,7 @@ int sm_count() {
 template <class RR, int V> void tma_col_attrs() {
     if constexpr (tma_col_ok<RR, V>()) {
         using TC = typename TmaVariant<V>::template Cfg<N>;
-        set_smem(k_col_step_tma<N, TC::COLS, TC::STAGES, TC::MINB, TC::TS>, TC::smem());
+        set_smem(k_col_step_tma<N, TC::COLS, TC::STAGES, TC::MINB, TC::TS, TC::TWG>, TC::smem());
     }
 }
 template <class RR, int V>
@@ -157,7 +175,7 @@ bool tma_col_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw,
         if (items > 0x7fffffffLL || (long long)batch * N > 0x7fffffffLL) throw std::runtime_error("batch too large");
         const CUtensorMap tm = wave_tensor_map(wave, 2ull * N, (unsigned long long)batch * N, TC::BOX_FLOATS, TC::BOX_ROWS);
         const int grid = (int)std::min<long long>(items, (long long)TC::MINB * sm_count());
-        k_col_step_tma<N, TC::COLS, TC::STAGES, TC::MINB, TC::TS><<<grid, TC::THREADS, TC::smem(), s>>>(
+        k_col_step_tma<N, TC::COLS, TC::STAGES, TC::MINB, TC::TS, TC::TWG><<<grid, TC::THREADS, TC::smem(), s>>>(
             tm, wave, tw, pt, b, lo, lo + hi, (int)items, pt.err);
         MS_CUDA(cudaGetLastError());
         return true;
@@ -198,6 +216,9 @@ bool rowpair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tra
     }
 }
 
+template <class RR> void row_w3_attrs() {
+    if constexpr (std::is_same<RR, float>::value && RowCfg<N, RR>::WIDE3) set_smem(k_row_step_w3<N>, RC::smem());
+}
 // kernel attributes are per device: set once for each device this process launches on
 bool g_attrs_done[64] = {};
 void ensure_attrs() {
@@ -205,6 +226,7 @@ void ensure_attrs() {
     MS_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64 || g_attrs_done[dev]) return;
     set_smem(k_row_step<R, N>, RC::smem());
+    row_w3_attrs<R>();
     if constexpr (std::is_same<R, double>::value && fp64_row_bounded<N>()) set_smem(k_row_step_d<N>, RC::smem());
     set_smem(k_row_fft<R, N, -1>, RC::smem());
     set_smem(k_row_fft<R, N, +1>, RC::smem());
@@ -219,6 +241,7 @@ void ensure_attrs() {
     tma_col_attrs<R, 4>();
     tma_col_attrs<R, 5>();
     tma_col_attrs<R, 6>();
+    tma_col_attrs<R, 7>();
     rowpair_attrs<R>();
     set_smem(k_col_step<R, N, COL_STEP_DET>, CC::smem());
     set_smem(k_col_step<R, N, COL_DET_ONLY>, CC::smem());
@@ -248,6 +271,26 @@ bool row_step_d(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans
         return false;
     }
 }
+// the FP32 row step with the three-stage wide plan (RowCfg::WIDE3), compiled for its blocks per SM
+template <class RR>
+bool row_step_w3(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans, const cplx<RR> *tw, RR a, int xa,
+                 int xb, int load_all, const int *tsel, size_t tstride, int pf) {
+    if constexpr (std::is_same<RR, float>::value && RowCfg<N, RR>::WIDE3) {
+        k_row_step_w3<N><<<pf == kWaveFastRows ? row_grid_wave_fast(batch) : row_grid(batch), row_block(), RC::smem(),
+                           s>>>(wave, trans, tw, a, xa, xb, load_all, tsel, tstride, pf);
+        MS_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        return false;
+    }
+}
+// blocks of the row step resident on the whole device
+template <class RR> int row_resident() {
+    if constexpr (std::is_same<RR, float>::value && RowCfg<N, RR>::WIDE3)
+        return resident_blocks(k_row_step_w3<N>, RC::THREADS, RC::smem());
+    else
+        return resident_blocks(k_row_step<RR, N>, RC::THREADS, RC::smem());
+}
 inline dim3 col_grid(int batch) { return dim3(N / CC::COLS, batch); }
 inline dim3 col_block() { return dim3(CC::COLS, CC::P::NT); }
 
@@ -260,9 +303,10 @@ void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, co
     static int res[64] = {};
     int dev = 0;
     MS_CUDA(cudaGetDevice(&dev));
-    if (variant > 0 && variant < 3 && !res[dev]) res[dev] = resident_blocks(k_row_step<R, N>, RC::THREADS, RC::smem());
+    if (variant > 0 && variant < 3 && !res[dev]) res[dev] = row_resident<R>();
     const int pf = variant == 3 ? kWaveFastRows : (variant > 0 ? variant * res[dev] : 0);
     if (row_step_d<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride, pf)) return;
+    if (row_step_w3<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride, pf)) return;
     k_row_step<R, N><<<pf == kWaveFastRows ? row_grid_wave_fast(batch) : row_grid(batch), row_block(), RC::smem(), s>>>(
         wave, trans, tw, a, xa, xb, load_all, tsel, tstride, pf);
     MS_CUDA(cudaGetLastError());
@@ -290,6 +334,7 @@ void col_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, PropT
         if (kind == 7 && tma_col_step<R, 5>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 8 && tma_col_step<R, 6>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 9 && pair_step<R, kPairC, !pair_loose<N>()>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 10 && tma_col_step<R, 7>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 3 && pair_step<R, kPairC / 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 4 && pair_step<R, kPairC * 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (pair_step<R, kPairC>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;

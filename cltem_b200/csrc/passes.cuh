@@ -64,8 +64,10 @@ struct DetArgs {
 // at 256 / 512 / 1024, fft_wide.cuh; the radix-8/4/2/3 Stockham plan otherwise, fft.cuh).
 template <int N, class R> struct RowCfg {
     static constexpr bool WIDE = wide_plan<R>(N);
-    using P = std::conditional_t<WIDE, WidePlan<N>, Plan<N>>;
-    static constexpr int ROWS = WIDE ? 8 : (N <= 128 ? 8 : (N <= 256 ? 8 : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1))));
+    static constexpr bool WIDE3 = !WIDE && wide3_plan<R>(N);   // the three-stage wide plan (FP32 2048, 4096)
+    using P = std::conditional_t<WIDE, WidePlan<N>, std::conditional_t<WIDE3, Wide3Plan<N>, Plan<N>>>;
+    static constexpr int ROWS = WIDE ? 8 : (WIDE3 ? (N == 2048 ? 2 : 1)
+                                                   : (N <= 128 ? 8 : (N <= 256 ? 8 : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1)))));
     static_assert(N % ROWS == 0, "row tile must divide the grid");
     static_assert(P::NT * ROWS <= 1024, "row block too large");
     static constexpr int THREADS = P::NT * ROWS;
@@ -74,9 +76,10 @@ template <int N, class R> struct RowCfg {
     // wide plan: a row's threads lie inside one warp (two rows per warp at 16 threads a row)
     static constexpr bool NAMED = !WIDE && (P::NT % 32) == 0 && ROWS > 1;
     static_assert(!WIDE || (P::NT == 32 || (P::NT == 16 && ROWS % 2 == 0)), "wide rows must tile whole warps");
-    static constexpr int TWN = WIDE ? WidePlan<N>::TW : N;   // twiddle entries staged in shared memory
-    static constexpr int TW_OFF = WIDE ? N : 0;               // offset of the row plan's table (Ctx::twiddles)
-    static constexpr int ROWSZ = WIDE ? WidePlan<N>::ROWSZ : RowAddr::size(N);
+    // twiddle entries staged in shared memory, and the offset of the row plan's table (Ctx::twiddles)
+    static constexpr int TWN = WIDE ? WidePlan<N>::TW : (WIDE3 ? Wide3Plan<N>::TW : N);
+    static constexpr int TW_OFF = (WIDE || WIDE3) ? N : 0;
+    static constexpr int ROWSZ = WIDE ? WidePlan<N>::ROWSZ : (WIDE3 ? Wide3Plan<N>::ROWSZ : RowAddr::size(N));
     // the table is read from global memory (L1 / L2) when it and the rows do not both fit (FP64 8192)
     static constexpr bool TWG = sizeof(cplx<R>) * (size_t)(TWN + ROWS * ROWSZ) > kMaxBlockSmem;
     static constexpr int TWS = TWG ? 0 : TWN;   // twiddle entries staged in shared memory
@@ -118,6 +121,11 @@ template <class R, int N, int SIGN>
 __device__ __forceinline__ void row_transform(cplx<R> (&v)[RowCfg<N, R>::P::E], cplx<R> *sm, int t, const cplx<R> *tw) {
     using RC = RowCfg<N, R>;
     if constexpr (RC::WIDE) fft_wide<R, N, SIGN>(v, sm, WideRowAddr<RC::P::E>(), t, tw, WarpSync());
+    else if constexpr (RC::WIDE3 && RC::NAMED)
+        fft_stages<R, N, SIGN, 0, WideRowAddr<32>, NamedSync, Wide3Plan<N>>(v, sm, WideRowAddr<32>(), t, tw,
+                                                                            NamedSync{1 + (int)threadIdx.y, RC::P::NT});
+    else if constexpr (RC::WIDE3)
+        fft_stages<R, N, SIGN, 0, WideRowAddr<32>, BlockSync, Wide3Plan<N>>(v, sm, WideRowAddr<32>(), t, tw, BlockSync());
     else if constexpr (RC::NAMED) fft<R, N, SIGN>(v, sm, RowAddr(), t, tw, NamedSync{1 + (int)threadIdx.y, RC::P::NT});
     else fft<R, N, SIGN>(v, sm, RowAddr(), t, tw);
 }
@@ -249,6 +257,16 @@ k_row_step_d(double2 *__restrict__ wave, const double2 *__restrict__ trans, cons
              int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride, int pf) {
     row_step_body<double, N>(wave, trans, twg, a, xa, xb, load_all, tsel, tstride, pf);
 }
+// The FP32 row step with the three-stage wide plan (2048, 4096, 8192), compiled for the blocks per SM its
+// shared memory allows (4 x 128 threads at 2048, 3 x 128 at 4096, 1 x 256 at 8192): without the hint the
+// compiler takes 175-185 registers a thread at 2048 and 4096, which leaves 2 blocks (8 warps) per SM.
+template <int N> constexpr int wide3_minb() { return N == 2048 ? 4 : (N == 4096 ? 3 : 1); }
+template <int N>
+__global__ void __launch_bounds__(RowCfg<N, float>::THREADS, wide3_minb<N>())
+k_row_step_w3(float2 *__restrict__ wave, const float2 *__restrict__ trans, const float2 *__restrict__ twg, float a,
+              int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride, int pf) {
+    row_step_body<float, N>(wave, trans, twg, a, xa, xb, load_all, tsel, tstride, pf);
+}
 
 // The row step of the FP32 radix-8 / 3·2^k row plans (sizes without the wide plan) with each thread carrying
 // the same element of two adjacent rows of a wave: the shared-memory exchanges move 16-byte pairs and each
@@ -261,8 +279,8 @@ template <int N, int PAIRS_ = rowpair_base<N>()> struct RowPairCfg {
     static constexpr int PAIRS = PAIRS_;   // row pairs a block
     static constexpr int THREADS = P::NT * PAIRS;
     static constexpr size_t smem() { return sizeof(float2) * (size_t)N + sizeof(float4) * (size_t)N * PAIRS; }
-    static constexpr bool ok = !RowCfg<N, float>::WIDE && THREADS <= 1024 && N % (2 * PAIRS) == 0 &&
-                               smem() <= kMaxBlockSmem;
+    static constexpr bool ok = !RowCfg<N, float>::WIDE && !RowCfg<N, float>::WIDE3 && THREADS <= 1024 &&
+                               N % (2 * PAIRS) == 0 && smem() <= kMaxBlockSmem;
 };
 // Row pairs a block of the step: twice the base at 384² and 768² (measured in a STEM run per size, row-pass
 // device time per probe·slice: −2.3% and −3.3%; 1536² to 4096² were 10-39% slower with 2 or 4 times the

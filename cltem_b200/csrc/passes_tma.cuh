@@ -21,47 +21,62 @@
 
 namespace ms {
 
+// the largest divisor of n that is at most 256 (a tensor-map box dimension is at most 256)
+constexpr int tma_box_rows(int n, int d = 256) { return d <= 1 ? 1 : (n % d == 0 ? d : tma_box_rows(n, d - 1)); }
+
 // Tile of COLS columns (two a consumer thread) of an N-row wave; the stage is the whole tile, loaded as
-// N / BOX_ROWS boxes of at most 256 rows (a tensor-map box dimension is at most 256).
-template <int N, int COLS_, int STAGES_ = 3, int MINB_ = 1, bool TS_ = false> struct TmaColCfg {
+// N / BOX_ROWS boxes of BOX_ROWS rows. TWG: the FFT reads its twiddles from global memory (through L1)
+// instead of a staged copy, which leaves room for one more stage where the tile column is tall (2048).
+template <int N, int COLS_, int STAGES_ = 3, int MINB_ = 1, bool TS_ = false, bool TWG_ = false> struct TmaColCfg {
     using P = Plan<N>;
     static constexpr int COLS = COLS_;
     static constexpr bool TS = TS_;                    // results leave through the stage and a TMA store
+    static constexpr bool TWG = TWG_;
     static constexpr int MINB = MINB_;                 // blocks per SM (the grid is MINB x the SM count)
     static constexpr int PAIRS = COLS / 2;
     static constexpr int NCONS = PAIRS * P::NT;        // consumer threads
     static constexpr int THREADS = NCONS + 32;         // + the producer warp
     static constexpr int STAGES = STAGES_;
     static constexpr int STAGE_BYTES = N * COLS * 8;
-    static constexpr int BOX_ROWS = N < 256 ? N : 256;
+    static constexpr int BOX_ROWS = tma_box_rows(N);
     static constexpr int LOADS = N / BOX_ROWS;
     static constexpr int BOX_FLOATS = 2 * COLS;        // inner box extent in FP32 elements
+    static constexpr int TABLES = (TWG ? 2 : 3) * N;   // staged float2 entries: twiddles (unless TWG), py, py errors
     // stages (128-byte aligned), twiddle table, the propagator's row tables (py and its errors, read at every
     // element; the column tables are read once per item from global memory), 2 mbarriers per stage
-    static constexpr size_t smem() { return 128 + (size_t)STAGES * STAGE_BYTES + 3 * sizeof(float2) * N + 16 * STAGES; }
+    static constexpr size_t smem() { return 128 + (size_t)STAGES * STAGE_BYTES + sizeof(float2) * TABLES + 16 * STAGES; }
     // one SM holds 228 KB of shared memory, 1 KB of it reserved per block
-    static constexpr bool ok = P::pow2 && N % BOX_ROWS == 0 && COLS >= 2 && (BOX_FLOATS * 4) % 16 == 0 &&
-                               BOX_FLOATS <= 256 && NCONS % 32 == 0 && THREADS <= 1024 && smem() <= kMaxBlockSmem &&
-                               MINB * (smem() + 1024) <= 228 * 1024 && (size_t)MINB * THREADS * 64 <= 65536;
+    static constexpr bool ok = STAGES >= 2 && N % BOX_ROWS == 0 && BOX_ROWS >= 16 && COLS >= 2 &&
+                               (BOX_FLOATS * 4) % 16 == 0 && BOX_FLOATS <= 256 && NCONS % 32 == 0 &&
+                               THREADS <= 1024 && smem() <= kMaxBlockSmem && MINB * (smem() + 1024) <= 228 * 1024 &&
+                               (size_t)MINB * THREADS * 64 <= 65536;
 };
+// the most stages (at most 6) of a COLS-column tile that fit beside the tables in one block's shared memory
+template <int N, int COLS, bool TWG> constexpr int tma_fit_stages() {
+    constexpr size_t fixed = 128 + sizeof(float2) * (size_t)(TWG ? 2 : 3) * N;
+    constexpr size_t per = (size_t)N * COLS * 8 + 16;
+    constexpr int s = fixed < kMaxBlockSmem ? (int)((kMaxBlockSmem - fixed) / per) : 0;
+    return s > 6 ? 6 : s;
+}
 
 // Work item i (0 <= i < n_items = batch * n_active): wave i / n_active, active tile j = i % n_active, which is
 // column tile j for j < tiles_lo and tile N/COLS - (n_active - j) otherwise (the tiles holding columns inside
 // the propagator's cut). err: the error word (tma.cuh StepError), written only when a wait is abandoned.
-template <int N, int COLS, int STAGES, int MINB, bool TS>
-__global__ void __launch_bounds__(TmaColCfg<N, COLS, STAGES, MINB, TS>::THREADS, MINB)
+template <int N, int COLS, int STAGES, int MINB, bool TS, bool TWG>
+__global__ void __launch_bounds__(TmaColCfg<N, COLS, STAGES, MINB, TS, TWG>::THREADS, MINB)
 k_col_step_tma(const __grid_constant__ CUtensorMap tm, float2 *__restrict__ wave, const float2 *__restrict__ twg,
                PropTables<float> pt, float bscale, int tiles_lo, int n_active, int n_items, int *err) {
-    using TC = TmaColCfg<N, COLS, STAGES, MINB, TS>;
+    using TC = TmaColCfg<N, COLS, STAGES, MINB, TS, TWG>;
     using P = Plan<N>;
     constexpr int PAIRS = TC::PAIRS, E = P::E, NT = P::NT, K = TC::STAGES, NCONS = TC::NCONS;
     extern __shared__ unsigned char smraw[];
     unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
     float4 *stages = reinterpret_cast<float4 *>(base);
-    float2 *tw = reinterpret_cast<float2 *>(base + (size_t)K * TC::STAGE_BYTES);
+    float2 *tabs = reinterpret_cast<float2 *>(base + (size_t)K * TC::STAGE_BYTES);
     // the propagator's row tables, read at every element: staged once per block, so no consumer waits on L1
     // for them (the column tables px, pxe and ycut are read once per item)
-    float2 *s_py = tw + N, *s_pye = s_py + N;
+    float2 *s_tw = tabs, *s_py = TWG ? tabs : tabs + N, *s_pye = s_py + N;
+    const float2 *tw = TWG ? twg : s_tw;
     uint64_t *full = reinterpret_cast<uint64_t *>(s_pye + N);
     uint64_t *empty = full + K;
     const int tid = threadIdx.x;
@@ -73,7 +88,7 @@ k_col_step_tma(const __grid_constant__ CUtensorMap tm, float2 *__restrict__ wave
         mbar_fence_init();
     }
     for (int i = tid; i < N; i += TC::THREADS) {
-        tw[i] = twg[i];
+        if constexpr (!TWG) s_tw[i] = twg[i];
         s_py[i] = pt.py[i];
         s_pye[i] = pt.pye[i];
     }
