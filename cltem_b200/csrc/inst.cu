@@ -88,6 +88,20 @@ template <> struct TmaVariant<7> {
     template <int NN>
     using Cfg = TmaColCfg<NN, PairStepCfg<NN>::COLS / 2, tma_fit_stages<NN, PairStepCfg<NN>::COLS / 2, true>(), 1, true, true>;
 };
+// The persistent passes with one barrier domain per column pair (passes_tmx.cuh), 3 stages, TMA loads and
+// stores, no producer warp: 11 a tile of 8192 / N columns (512 threads, one block per SM), 12 half that tile
+// (256 threads, two blocks per SM)
+template <int V> struct TmxVariant;
+template <> struct TmxVariant<11> { template <int NN> using Cfg = TmxColCfg<NN, (8192 / NN > 1 ? 8192 / NN : 2), 3, 1>; };
+template <> struct TmxVariant<12> { template <int NN> using Cfg = TmxColCfg<NN, (4096 / NN > 1 ? 4096 / NN : 2), 3, 2>; };
+template <class RR, int V> constexpr bool tmx_col_ok() {
+    if constexpr (std::is_same<RR, float>::value && pair_columns<N>() && N >= 512) {
+        using TC = typename TmxVariant<V>::template Cfg<N>;
+        return TC::ok && TC::COLS % CC::COLS == 0 && N % TC::COLS == 0;
+    } else {
+        return false;
+    }
+}
 template <class RR, int V> constexpr bool tma_col_ok() {
     if constexpr (std::is_same<RR, float>::value && pair_columns<N>()) {
         using TC = typename TmaVariant<V>::template Cfg<N>;
@@ -99,14 +113,14 @@ template <class RR, int V> constexpr bool tma_col_ok() {
 // The column-step kernels of this size, by kind: 0 the two-column step at its default tile, 1 / 2 the
 // persistent TMA-fed passes, 3 / 4 the two-column step at half / twice the default tile, 5 / 6 the persistent
 // passes 1 / 2 storing through TMA, 7 / 8 / 10 the deep-ring persistent passes 5 / 6 / 7, 9 the two-column step
-// at its default tile with the other register budget. A variant index of PassOps::col_step is a position in the
+// at its default tile with the other register budget, 11 / 12 the per-pair-barrier passes. A variant index of PassOps::col_step is a position in the
 // list of the kinds valid here (kind 0 always first).
 struct KindList {
-    int kind[11];
+    int kind[13];
     int n;
 };
 template <class RR> constexpr KindList col_kinds() {
-    KindList k{{0, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1}, 1};
+    KindList k{{0, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1}, 1};
     if (tma_col_ok<RR, 1>()) k.kind[k.n++] = 1;
     if (tma_col_ok<RR, 2>()) k.kind[k.n++] = 2;
     if (pair_tile_ok<RR, kPairC / 2>()) k.kind[k.n++] = 3;
@@ -117,6 +131,8 @@ template <class RR> constexpr KindList col_kinds() {
     if (tma_col_ok<RR, 6>()) k.kind[k.n++] = 8;
     if (pair_tile_ok<RR, kPairC, !pair_loose<N>()>()) k.kind[k.n++] = 9;
     if (tma_col_ok<RR, 7>()) k.kind[k.n++] = 10;
+    if (tmx_col_ok<RR, 11>()) k.kind[k.n++] = 11;
+    if (tmx_col_ok<RR, 12>()) k.kind[k.n++] = 12;
     return k;
 }
 template <class RR> constexpr int tma_col_variants() { return col_kinds<RR>().n; }
@@ -141,6 +157,11 @@ std::string col_variant_name(int v) {
     if (kind == 10)
         return "persistent, TMA loads and stores, " + cols(kPairC / 2) + ", " + stages(TmaVariant<7>::Cfg<N>::STAGES) +
                ", twiddles from L1, 1 block per SM";
+    if (kind == 11 || kind == 12) {
+        constexpr int c11 = TmxVariant<11>::Cfg<N>::COLS, c12 = TmxVariant<12>::Cfg<N>::COLS;
+        return "persistent, per-pair barriers, TMA loads and stores, " + cols(kind == 11 ? c11 : c12) +
+               ", 3 stages, " + (kind == 11 ? "1 block" : "2 blocks") + " per SM";
+    }
     if (kind == 9)
         return "one block per (" + cols(kPairC) + ", wave), two columns a thread, " +
                (pair_loose<N>() ? "64" : "128") + "-register budget";
@@ -177,6 +198,35 @@ bool tma_col_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw,
         const int grid = (int)std::min<long long>(items, (long long)TC::MINB * sm_count());
         k_col_step_tma<N, TC::COLS, TC::STAGES, TC::MINB, TC::TS, TC::TWG><<<grid, TC::THREADS, TC::smem(), s>>>(
             tm, wave, tw, pt, b, lo, lo + hi, (int)items, pt.err);
+        MS_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        return false;
+    }
+}
+
+template <class RR, int V> void tmx_col_attrs() {
+    if constexpr (tmx_col_ok<RR, V>()) {
+        using TC = typename TmxVariant<V>::template Cfg<N>;
+        set_smem(k_col_step_tmx<N, TC::COLS, TC::STAGES, TC::MINB>, TC::smem());
+    }
+}
+template <class RR, int V>
+bool tmx_col_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw, PropTables<RR> pt, RR b, int tiles_lo,
+                  int tiles_hi) {
+    if constexpr (tmx_col_ok<RR, V>()) {
+        using TC = typename TmxVariant<V>::template Cfg<N>;
+        if (!pt.err) throw std::runtime_error("persistent column pass without an error word");
+        constexpr int k = TC::COLS / CC::COLS, total = N / TC::COLS;
+        int lo = (tiles_lo + k - 1) / k, hi = (tiles_hi + k - 1) / k;
+        if (lo + hi > total) { lo = total; hi = 0; }
+        const long long items = (long long)(lo + hi) * batch;
+        if (items > 0x7fffffffLL || (long long)batch * N > 0x7fffffffLL) throw std::runtime_error("batch too large");
+        const CUtensorMap tm =
+            wave_tensor_map(wave, 2ull * N, (unsigned long long)batch * N, TC::BOX_FLOATS, TC::BOX_ROWS, TC::SWIZZLE);
+        const int grid = (int)std::min<long long>(items, (long long)TC::MINB * sm_count());
+        k_col_step_tmx<N, TC::COLS, TC::STAGES, TC::MINB><<<grid, TC::THREADS, TC::smem(), s>>>(tm, tw, pt, b, lo, lo + hi,
+                                                                                              (int)items, pt.err);
         MS_CUDA(cudaGetLastError());
         return true;
     } else {
@@ -242,6 +292,8 @@ void ensure_attrs() {
     tma_col_attrs<R, 5>();
     tma_col_attrs<R, 6>();
     tma_col_attrs<R, 7>();
+    tmx_col_attrs<R, 11>();
+    tmx_col_attrs<R, 12>();
     rowpair_attrs<R>();
     set_smem(k_col_step<R, N, COL_STEP_DET>, CC::smem());
     set_smem(k_col_step<R, N, COL_DET_ONLY>, CC::smem());
@@ -335,6 +387,8 @@ void col_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, PropT
         if (kind == 8 && tma_col_step<R, 6>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 9 && pair_step<R, kPairC, !pair_loose<N>()>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 10 && tma_col_step<R, 7>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 11 && tmx_col_step<R, 11>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 12 && tmx_col_step<R, 12>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 3 && pair_step<R, kPairC / 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 4 && pair_step<R, kPairC * 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (pair_step<R, kPairC>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;

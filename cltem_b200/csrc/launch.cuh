@@ -4,6 +4,7 @@
 #include "adjoint.cuh"
 #include "passes.cuh"
 #include "passes_tma.cuh"
+#include "passes_tmx.cuh"
 
 #include <string>
 

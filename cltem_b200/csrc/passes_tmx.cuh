@@ -1,0 +1,317 @@
+// passes_tmx.cuh — persistent column pass with one barrier domain per column pair (FP32, 2^k plans).
+//
+// Same arithmetic per element, in the same order, as k_col_step_pair / k_col_step_tma (column FFT of two
+// adjacent columns a thread, times the propagator inside its cut and the scale b, inverse column FFT), so
+// the results are bit-identical. What changes is who waits for whom:
+//   - the NT threads of one column pair are whole warps (thread t of pair p is thread p * NT + t), and each
+//     pair synchronises its FFT exchanges on its own named barrier, so a pair that waits on shared memory
+//     does not hold up the other pairs of the block (k_col_step_tma makes all 16 consumer warps meet at
+//     every exchange);
+//   - there is no producer warp: one thread of the first pair issues the tile loads and stores at item
+//     boundaries, so the block is 16 warps of 128 registers instead of 17 of 96;
+//   - each thread keeps the twiddles of its butterflies in registers (they depend only on its position in
+//     the transform), so the exchanges are the only shared-memory traffic of the FFTs.
+// Tile layout in a stage: element (row y, pair p), 16 bytes, at slot PAIRS * y + (p ^ h(y)), h(y) =
+// (y * PAIRS >> 3) mod PAIRS: the copy engine's 128B / 64B / 32B swizzle for 8 / 4 / 2 pairs (16-byte chunks
+// of a 1024-byte atom XORed with the row's position in it), none for one pair. The FFT exchanges store
+// logical row i at physical row g(i) = i ^ ((i >> 3) & 7) with the same swizzle. Both layouts give every pair
+// the same slots (each pair only ever touches its own), and every access pattern of the radix-8/4/2 stages
+// meets 8 distinct 16-byte bank groups per quarter warp. Both maps are linear over GF(2) in the bits of the
+// row, so an address is a per-thread base combined with a constant: an add folded into the instruction where
+// the constant's bits lie outside the base's, one XOR otherwise.
+// Only this GPU's own wave buffer is read and written; no load uses cluster multicast.
+#pragma once
+
+#include "passes_tma.cuh"
+
+namespace ms {
+
+template <int PAIRS> __host__ __device__ constexpr int tmx_swz(int row) {
+    return PAIRS == 1 ? 0 : ((row * PAIRS) >> 3) & (PAIRS - 1);
+}
+// 16-byte slot of logical row i of pair 0 in the copy engine's layout / in the exchange layout
+template <int PAIRS> __host__ __device__ constexpr int tmx_tlay(int i) { return PAIRS * i ^ tmx_swz<PAIRS>(i); }
+template <int PAIRS> __host__ __device__ constexpr int tmx_lay(int i) { return tmx_tlay<PAIRS>(i ^ ((i >> 3) & 7)); }
+// the exchange write position of butterfly j's output 0 at stage S (fft.cuh: (j / Ns) Ns RAD + j mod Ns)
+template <int N, int S> __host__ __device__ constexpr int tmx_wrow(int j) {
+    return (j / Plan<N>::ns(S)) * Plan<N>::ns(S) * Plan<N>::radix(S) + j % Plan<N>::ns(S);
+}
+// every bit a per-thread base f(t) ^ p can have (t < NT, p < PAIRS)
+template <int PAIRS, int NT> __host__ __device__ constexpr int tmx_mask_tlay() {
+    int m = PAIRS - 1;
+    for (int b = 1; b < NT; b <<= 1) m |= tmx_tlay<PAIRS>(b);
+    return m;
+}
+template <int PAIRS, int NT> __host__ __device__ constexpr int tmx_mask_lay() {
+    int m = PAIRS - 1;
+    for (int b = 1; b < NT; b <<= 1) m |= tmx_lay<PAIRS>(b);
+    return m;
+}
+template <int N, int PAIRS, int S> __host__ __device__ constexpr int tmx_mask_w() {
+    int m = PAIRS - 1;
+    for (int b = 1; b < Plan<N>::NT; b <<= 1) m |= tmx_lay<PAIRS>(tmx_wrow<N, S>(b));
+    return m;
+}
+// base combined with the constant c: the two share no bit when (c & mask) == 0, and then the sum is the XOR
+__device__ __forceinline__ int tmx_at(int base, int c, int mask) { return (c & mask) == 0 ? base + c : base ^ c; }
+
+// twiddles a thread holds: stage S >= 1 keeps NB (RAD - 1) of them, in stage order
+template <int N> __host__ __device__ constexpr int tmx_tw_off(int S) {
+    int o = 0;
+    for (int s = 1; s < S; s++) o += (Plan<N>::E / Plan<N>::radix(s)) * (Plan<N>::radix(s) - 1);
+    return o;
+}
+template <int N> constexpr int tmx_tw_count() { return tmx_tw_off<N>(Plan<N>::nstages); }
+
+template <int N, int COLS_, int STAGES_, int MINB_ = 1> struct TmxColCfg {
+    using P = Plan<N>;
+    static constexpr int COLS = COLS_;
+    static constexpr int PAIRS = COLS / 2;
+    static constexpr int NT = P::NT;
+    static constexpr int THREADS = PAIRS * NT;
+    static constexpr int STAGES = STAGES_;
+    static constexpr int MINB = MINB_;
+    static constexpr int STAGE_BYTES = N * COLS * 8;
+    static constexpr int BOX_ROWS = tma_box_rows(N);
+    static constexpr int LOADS = N / BOX_ROWS;
+    static constexpr int BOX_FLOATS = 2 * COLS;
+    static constexpr int TWR = tmx_tw_count<N>();
+    // 1024-byte alignment slack (the swizzle atom), stages, the propagator's row tables (py and its errors),
+    // two mbarriers per stage
+    static constexpr size_t smem() { return 1024 + (size_t)STAGES * STAGE_BYTES + sizeof(float2) * 2 * N + 16 * STAGES; }
+    static constexpr bool ok = is_pow2(N) && P::E == 8 && (PAIRS == 1 || PAIRS == 2 || PAIRS == 4 || PAIRS == 8) &&
+                               NT % 32 == 0 && THREADS <= 1024 && PAIRS <= 15 && STAGES >= 3 && N % BOX_ROWS == 0 &&
+                               BOX_ROWS >= 16 && smem() <= kMaxBlockSmem && MINB * (smem() + 1024) <= 228 * 1024 &&
+                               (size_t)MINB * THREADS * 128 <= 65536;
+    // the copy engine's swizzle span in bytes (a tile row), 0 for none
+    static constexpr int SWIZZLE = PAIRS == 1 ? 0 : COLS * 8;
+};
+
+// Stage S of the pair FFT (fft_pair.cuh's fftp_stages with the layouts above and register twiddles).
+// rbase: tmx_lay(t) ^ p; wb[S]: tmx_lay(tmx_wrow<N, S>(t)) ^ p.
+template <int N, int PAIRS, int SIGN, int S, int TWR>
+__device__ __forceinline__ void tmx_stages(float2 (&va)[Plan<N>::E], float2 (&vb)[Plan<N>::E], float4 *sm, int rbase,
+                                           const int (&wb)[Plan<N>::nstages], const float2 (&twr)[TWR], NamedBar bar) {
+    using P = Plan<N>;
+    constexpr int E = P::E, NT = P::NT;
+    constexpr int RAD = P::radix(S);
+    constexpr int Ns = P::ns(S);
+    constexpr int NB = E / RAD;
+    constexpr bool last = (S == P::nstages - 1);
+    constexpr int TWO = tmx_tw_off<N>(S > 0 ? S : 1);
+    if constexpr (S > 0) {
+        constexpr int RM = tmx_mask_lay<PAIRS, NT>();
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+#pragma unroll
+            for (int r = 0; r < RAD; r++) {
+                const float4 q = sm[tmx_at(rbase, tmx_lay<PAIRS>(b * NT + r * (N / RAD)), RM)];
+                va[b + r * NB] = make_float2(q.x, q.y);
+                vb[b + r * NB] = make_float2(q.z, q.w);
+            }
+        }
+    }
+    float2 oa[E], ob[E];
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        float2 a[RAD], c[RAD];
+#pragma unroll
+        for (int r = 0; r < RAD; r++) {
+            float2 x = va[b + r * NB], y = vb[b + r * NB];
+            if constexpr (S > 0) {
+                if (r > 0) {
+                    const float2 w = twr[TWO + b * (RAD - 1) + (r - 1)];
+                    x = (SIGN < 0) ? cmul(x, w) : cmulc(x, w);
+                    y = (SIGN < 0) ? cmul(y, w) : cmulc(y, w);
+                }
+            }
+            a[r] = x;
+            c[r] = y;
+        }
+        dft<float, RAD, SIGN>(a);
+        dft<float, RAD, SIGN>(c);
+#pragma unroll
+        for (int m = 0; m < RAD; m++) {
+            oa[b + m * NB] = a[m];
+            ob[b + m * NB] = c[m];
+        }
+    }
+    if constexpr (last) {
+#pragma unroll
+        for (int i = 0; i < E; i++) { va[i] = oa[i]; vb[i] = ob[i]; }
+    } else {
+        constexpr int WM = tmx_mask_w<N, PAIRS, S>();
+        bar();   // the pair's reads of the previous layout are done
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+#pragma unroll
+            for (int m = 0; m < RAD; m++)
+                sm[tmx_at(wb[S], tmx_lay<PAIRS>(tmx_wrow<N, S>(b * NT) | (m * Ns)), WM)] =
+                    make_float4(oa[b + m * NB].x, oa[b + m * NB].y, ob[b + m * NB].x, ob[b + m * NB].y);
+        }
+        bar();
+        tmx_stages<N, PAIRS, SIGN, S + 1, TWR>(va, vb, sm, rbase, wb, twr, bar);
+    }
+}
+
+// thread t's twiddles: stage S, butterfly j = t + b NT, k = j mod Ns, entries r = 1..RAD-1 of the packed table
+template <int N, int S, int TWR> __device__ __forceinline__ void tmx_load_twiddles(float2 (&twr)[TWR], const float2 *twg, int t) {
+    if constexpr (S < Plan<N>::nstages) {
+        using P = Plan<N>;
+        constexpr int RAD = P::radix(S), Ns = P::ns(S), NB = P::E / RAD, NT = P::NT;
+        constexpr int TWB = plan_tw_index(N, S, 0, 1);
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            const int k = (t + b * NT) % Ns;
+#pragma unroll
+            for (int r = 1; r < RAD; r++) twr[tmx_tw_off<N>(S) + b * (RAD - 1) + (r - 1)] = twg[TWB + k * (RAD - 1) + (r - 1)];
+        }
+        tmx_load_twiddles<N, S + 1, TWR>(twr, twg, t);
+    }
+}
+template <int N, int PAIRS, int S> __device__ __forceinline__ void tmx_write_bases(int (&wb)[Plan<N>::nstages], int t, int p) {
+    if constexpr (S < Plan<N>::nstages) {
+        wb[S] = tmx_lay<PAIRS>(tmx_wrow<N, S>(t)) ^ p;
+        tmx_write_bases<N, PAIRS, S + 1>(wb, t, p);
+    }
+}
+
+// Work item i (0 <= i < n_items = batch * n_active): wave i / n_active, active tile j = i % n_active (column
+// tile j for j < tiles_lo, tile N/COLS - (n_active - j) otherwise), as k_col_step_tma. The block's items are
+// blockIdx.x + k gridDim.x. Thread 0 keeps the ring: before item k it stores item k - 1 (once every warp has
+// written its results into that stage) and loads item k + STAGES - 2 into the stage of item k - 2 (once
+// that stage's store has read it). err: the error word (tma.cuh StepError), written only when a wait is
+// abandoned; a producer that gives up stops loading, and the consumers then give up at the first item that
+// was never loaded (no pair is left waiting at a barrier for a warp that left).
+template <int N, int COLS, int STAGES, int MINB>
+__global__ void __launch_bounds__(TmxColCfg<N, COLS, STAGES, MINB>::THREADS, MINB)
+k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict__ twg, PropTables<float> pt, float bscale,
+               int tiles_lo, int n_active, int n_items, int *err) {
+    using TC = TmxColCfg<N, COLS, STAGES, MINB>;
+    using P = Plan<N>;
+    constexpr int PAIRS = TC::PAIRS, E = P::E, NT = P::NT, K = TC::STAGES, THREADS = TC::THREADS;
+    extern __shared__ unsigned char smraw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
+    float4 *stages = reinterpret_cast<float4 *>(base);
+    float2 *s_py = reinterpret_cast<float2 *>(base + (size_t)K * TC::STAGE_BYTES), *s_pye = s_py + N;
+    uint64_t *full = reinterpret_cast<uint64_t *>(s_pye + N);
+    uint64_t *empty = full + K;
+    const int tid = threadIdx.x;
+    const int p = tid / NT, t = tid % NT;
+    if (tid == 0) {
+        for (int s = 0; s < K; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], THREADS / 32);
+        }
+        mbar_fence_init();
+    }
+    for (int i = tid; i < N; i += THREADS) {
+        s_py[i] = pt.py[i];
+        s_pye[i] = pt.pye[i];
+    }
+    float2 twr[TC::TWR];
+    tmx_load_twiddles<N, 1, TC::TWR>(twr, twg, t);
+    int wb[P::nstages];
+    tmx_write_bases<N, PAIRS, 0>(wb, t, p);
+    const int rbase = tmx_lay<PAIRS>(t) ^ p, tbase = tmx_tlay<PAIRS>(t) ^ p;
+    constexpr int TM = tmx_mask_tlay<PAIRS, NT>();
+    const NamedBar bar{1 + p, NT};
+    __syncthreads();
+
+    const int n_mine = n_items > (int)blockIdx.x ? (n_items - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    // (producer, thread 0) wave and column tile of this block's k-th item
+    auto item_of = [&](int kk, int &w, int &tile) {
+        const int item = (int)blockIdx.x + kk * (int)gridDim.x;
+        w = item / n_active;
+        const int j = item - w * n_active;
+        tile = j < tiles_lo ? j : N / COLS - (n_active - j);
+    };
+    auto load = [&](int kk) {
+        int w, tile;
+        item_of(kk, w, tile);
+        unsigned char *dst = base + (size_t)(kk % K) * TC::STAGE_BYTES;
+        mbar_arrive_expect_tx(&full[kk % K], TC::STAGE_BYTES);
+#pragma unroll
+        for (int l = 0; l < TC::LOADS; l++)
+            tma_load_2d(dst + (size_t)l * TC::BOX_ROWS * COLS * 8, &tm, tile * TC::BOX_FLOATS, w * N + l * TC::BOX_ROWS,
+                        &full[kk % K]);
+    };
+    auto store = [&](int kk) {
+        int w, tile;
+        item_of(kk, w, tile);
+        const unsigned char *src = base + (size_t)(kk % K) * TC::STAGE_BYTES;
+#pragma unroll
+        for (int l = 0; l < TC::LOADS; l++)
+            tma_store_2d(&tm, tile * TC::BOX_FLOATS, w * N + l * TC::BOX_ROWS, src + (size_t)l * TC::BOX_ROWS * COLS * 8);
+        bulk_commit();
+    };
+    bool prod_ok = true;   // thread 0: false once a producer wait was abandoned (no more loads or stores)
+    int issued = 0;        // thread 0: items whose loads were issued
+    if (tid == 0) {
+        tma_prefetch_desc(&tm);
+        for (; issued < K - 2 && issued < n_mine; issued++) load(issued);
+    }
+
+    for (int k = 0; k < n_mine; k++) {
+        if (tid == 0 && prod_ok) {
+            if (k >= 1) {
+                if (mbar_wait(&empty[(k - 1) % K], (unsigned)((k - 1) / K) & 1, err, STEP_WAIT_EMPTY)) store(k - 1);
+                else prod_ok = false;
+            }
+            if (prod_ok && issued < n_mine) {   // issued == k + K - 2
+                if (issued >= K) bulk_wait_read<1>();   // the store of item issued - K has read its stage
+                load(issued++);
+            }
+        }
+        __syncwarp();
+        const int s = k % K;
+        const int item = (int)blockIdx.x + k * (int)gridDim.x;
+        const int w = item / n_active, j = item - w * n_active;
+        const int tile = j < tiles_lo ? j : N / COLS - (n_active - j);
+        const int x = tile * COLS + 2 * p;
+        const float2 pxa = pt.px[x], pxb = pt.px[x + 1], exa = pt.pxe[x], exb = pt.pxe[x + 1];
+        const int2 ca = pt.ycut[x], cb = pt.ycut[x + 1];
+        if (!mbar_wait(&full[s], (unsigned)(k / K) & 1, err, STEP_WAIT_FULL)) break;
+        float4 *sm = stages + (size_t)s * (TC::STAGE_BYTES / 16);
+        float2 va[E], vb[E];
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            const float4 q = sm[tmx_at(tbase, tmx_tlay<PAIRS>(m * NT), TM)];
+            va[m] = make_float2(q.x, q.y);
+            vb[m] = make_float2(q.z, q.w);
+        }
+        tmx_stages<N, PAIRS, -1, 0, TC::TWR>(va, vb, sm, rbase, wb, twr, bar);
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            const int y = t + m * NT;
+            const float2 py = s_py[y], ey = s_pye[y];
+            va[m] = (y < ca.x || y >= ca.y) ? cscale(prop_mul<float>(va[m], pxa, py, exa, ey), bscale) : mk<float>(0, 0);
+            vb[m] = (y < cb.x || y >= cb.y) ? cscale(prop_mul<float>(vb[m], pxb, py, exb, ey), bscale) : mk<float>(0, 0);
+        }
+        tmx_stages<N, PAIRS, +1, 0, TC::TWR>(va, vb, sm, rbase, wb, twr, bar);
+        bar();   // the pair's last exchange reads are done: the stage takes its results
+#pragma unroll
+        for (int m = 0; m < E; m++)
+            sm[tmx_at(tbase, tmx_tlay<PAIRS>(m * NT), TM)] = make_float4(va[m].x, va[m].y, vb[m].x, vb[m].y);
+        fence_proxy_async_smem();
+        __syncwarp();
+        if ((tid & 31) == 0) mbar_arrive(&empty[s]);
+    }
+
+    if (tid == 0) {
+        if (prod_ok && n_mine > 0) {   // the last item's results
+            const int kk = n_mine - 1;
+            if (mbar_wait(&empty[kk % K], (unsigned)(kk / K) & 1, err, STEP_WAIT_EMPTY)) store(kk);
+            else prod_ok = false;
+        }
+        if (!prod_ok) {   // let the loads already issued land before the block exits
+            for (int d = 1; d <= K && issued - d >= 0; d++) {
+                const int kk = issued - d;
+                mbar_wait(&full[kk % K], (unsigned)(kk / K) & 1, err, STEP_WAIT_DRAIN);
+            }
+        }
+        bulk_wait_all();   // every store issued has read its stage and written HBM
+    }
+}
+
+}  // namespace ms

@@ -91,6 +91,10 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 // overwritten), or have completed entirely (their global writes are done)
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// wait until at most PENDING of this thread's most recent bulk groups are still reading their sources
+template <int PENDING> __device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(PENDING) : "memory");
+}
 
 // named barrier over `count` threads (a multiple of 32) of the block
 struct NamedBar {
@@ -99,11 +103,13 @@ struct NamedBar {
 };
 
 // Host: a 2-D tensor map over `rows` rows of `row_floats` FP32 values (row stride row_floats * 4 bytes) at
-// `base`, with boxes of box_floats x box_rows, no swizzle, no interleave. cuTensorMapEncodeTiled checks the
+// `base`, with boxes of box_floats x box_rows, no interleave, and the shared-memory swizzle of swizzle_bytes
+// (0: none; 32, 64 or 128: 16-byte chunks XORed with the row's position in a 256 / 512 / 1024-byte atom, which
+// needs a box row of at most that many bytes and stage addresses aligned to 1024 bytes). cuTensorMapEncodeTiled checks the
 // base (16-byte aligned), the stride and the box's inner extent (multiples of 16 bytes); the kernels keep
 // every box's x coordinate a multiple of box_floats, so each copy starts on a 16-byte boundary.
 inline CUtensorMap wave_tensor_map(const void *base, unsigned long long row_floats, unsigned long long rows,
-                                   unsigned box_floats, unsigned box_rows) {
+                                   unsigned box_floats, unsigned box_rows, int swizzle_bytes = 0) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
         void *fn = nullptr;
         cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
@@ -115,13 +121,20 @@ inline CUtensorMap wave_tensor_map(const void *base, unsigned long long row_floa
     if ((box_floats * 4) % 16 != 0 || box_floats > 256 || box_rows > 256 || box_rows == 0 ||
         (reinterpret_cast<uintptr_t>(base) & 15) != 0 || (row_floats * 4) % 16 != 0)
         throw std::runtime_error("tensor map: misaligned base, stride or box");
+    CUtensorMapSwizzle sw = CU_TENSOR_MAP_SWIZZLE_NONE;
+    if (swizzle_bytes == 32) sw = CU_TENSOR_MAP_SWIZZLE_32B;
+    else if (swizzle_bytes == 64) sw = CU_TENSOR_MAP_SWIZZLE_64B;
+    else if (swizzle_bytes == 128) sw = CU_TENSOR_MAP_SWIZZLE_128B;
+    else if (swizzle_bytes != 0) throw std::runtime_error("tensor map: swizzle must be 0, 32, 64 or 128 bytes");
+    if (swizzle_bytes && box_floats * 4 > (unsigned)swizzle_bytes)
+        throw std::runtime_error("tensor map: box row wider than the swizzle span");
     CUtensorMap m;
     const cuuint64_t dims[2] = {row_floats, rows};
     const cuuint64_t strides[1] = {row_floats * 4};
     const cuuint32_t box[2] = {box_floats, box_rows};
     const cuuint32_t estr[2] = {1, 1};
     CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
     return m;
