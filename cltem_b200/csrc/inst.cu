@@ -95,7 +95,7 @@ template <int V> struct TmxVariant;
 template <> struct TmxVariant<11> { template <int NN> using Cfg = TmxColCfg<NN, (8192 / NN > 1 ? 8192 / NN : 2), 3, 1>; };
 template <> struct TmxVariant<12> { template <int NN> using Cfg = TmxColCfg<NN, (4096 / NN > 1 ? 4096 / NN : 2), 3, 2>; };
 template <class RR, int V> constexpr bool tmx_col_ok() {
-    if constexpr (std::is_same<RR, float>::value && pair_columns<N>() && N >= 512) {
+    if constexpr (std::is_same<RR, float>::value && pair_columns<N>() && N >= 256) {
         using TC = typename TmxVariant<V>::template Cfg<N>;
         return TC::ok && TC::COLS % CC::COLS == 0 && N % TC::COLS == 0;
     } else {
