@@ -342,9 +342,10 @@ struct Ctx {
         // entries [0, n): the radix-8 plan's packed per-stage table (fft.cuh, plan_tw_index),
         // W_n^(r*k*n/(Ns*R)) = exp(-2 pi i r k / (Ns*R)); for sizes whose row passes use the wide two-stage
         // plan (fft_wide.cuh) entries [n, 2n) hold its table, W_n^(r k) at k (R2 - 1) + r - 1; for the
-        // three-stage wide plan they hold its stages' tables in the packed layout (Wide3Plan::tw_base)
-        const bool wide = wide_plan<R>(n), wide3 = !wide && wide3_plan<R>(n);
-        const size_t count = (size_t)n * ((wide || wide3) ? 2 : 1);
+        // three-stage wide plan and the radix-24 plans they hold their stages' tables in the packed layout
+        // (Wide3Plan::tw_base, Wide24Plan::tw_base)
+        const bool wide = wide_plan<R>(n), wide3 = !wide && wide3_plan<R>(n), wide24 = wide24_plan<R>(n);
+        const size_t count = (size_t)n * ((wide || wide3 || wide24) ? 2 : 1);
         std::vector<cplx<R>> h(count, mk<R>(0, 0));
         const long double two_pi = 2.0L * 3.14159265358979323846264338327950288L;
         for (int s = 1; s < plan_nstages(n); s++) {
@@ -355,7 +356,7 @@ struct Ctx {
                     h[plan_tw_index(n, s, k, r)] = round_unit<R>(std::cos(a), std::sin(a));
                 }
         }
-        if (wide3) {
+        if (wide3 || wide24) {
             auto fill = [&](auto plan) {
                 using P = decltype(plan);
                 for (int st = 1; st < P::nstages; st++) {
@@ -369,7 +370,11 @@ struct Ctx {
             };
             if (n == 2048) fill(Wide3Plan<2048>());
             else if (n == 4096) fill(Wide3Plan<4096>());
-            else fill(Wide3Plan<8192>());
+            else if (n == 8192) fill(Wide3Plan<8192>());
+            else if (n == 384) fill(Wide24Plan<384>());
+            else if (n == 768) fill(Wide24Plan<768>());
+            else if (n == 1536) fill(Wide24Plan<1536>());
+            else fill(Wide24Plan<3072>());
         }
         if (wide) {
             const int E = wide_E(n), R2 = n / E;

@@ -145,6 +145,27 @@ template <class R, int SIGN> __device__ __forceinline__ void dft12(cplx<R> *a) {
     }
 }
 
+// 24-point DFT as a prime-factor (Good-Thomas) 3 x 8 transform: n = (8 n1 + 3 n2) mod 24 and
+// k = (16 k1 + 9 k2) mod 24, so W24^(nk) = W3^(n1 k1) W8^(n2 k2): eight 3-point DFTs over n1, three 8-point
+// DFTs over n2, no twiddle products
+template <class R, int SIGN> __device__ __forceinline__ void dft24(cplx<R> *a) {
+    cplx<R> y[3][8];
+#pragma unroll
+    for (int n2 = 0; n2 < 8; n2++) {
+        cplx<R> x0 = a[(3 * n2) % 24], x1 = a[(8 + 3 * n2) % 24], x2 = a[(16 + 3 * n2) % 24];
+        dft3<R, SIGN>(x0, x1, x2);
+        y[0][n2] = x0;
+        y[1][n2] = x1;
+        y[2][n2] = x2;
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 3; k1++) {
+        dft8<R, SIGN>(y[k1]);
+#pragma unroll
+        for (int k2 = 0; k2 < 8; k2++) a[(16 * k1 + 9 * k2) % 24] = y[k1][k2];
+    }
+}
+
 // the wide radices (fft_wide.cuh), for plans that mix them with the radix-8 stages
 template <class R, int SIGN> __device__ __forceinline__ void dft16(cplx<R> *a);
 template <class R, int SIGN> __device__ __forceinline__ void dft32(cplx<R> *a);
@@ -154,6 +175,7 @@ template <class R, int RAD, int SIGN> __device__ __forceinline__ void dft(cplx<R
     else if constexpr (RAD == 3) dft3<R, SIGN>(a[0], a[1], a[2]);
     else if constexpr (RAD == 4) dft4<R, SIGN>(a[0], a[1], a[2], a[3]);
     else if constexpr (RAD == 12) dft12<R, SIGN>(a);
+    else if constexpr (RAD == 24) dft24<R, SIGN>(a);
     else if constexpr (RAD == 16) dft16<R, SIGN>(a);
     else if constexpr (RAD == 32) dft32<R, SIGN>(a);
     else dft8<R, SIGN>(a);

@@ -151,6 +151,33 @@ template <int N> struct Wide3Plan {
                   "three-stage wide plan");
 };
 
+// The radix-24 plans of the FP32 rows at 3·2^k: stage A a 24-point prime-factor DFT of each thread's 24
+// elements in registers (no twiddles), then Stockham stages through fft_stages: 384 = 24·4·4, 768 = 24·8·4,
+// 1536 = 24·8·8, 3072 = 24·8·8·2. Two shared-memory exchanges a transform (three at 3072) where the radix-12
+// plan makes three (four at 1536, five stages at 3072), with NT = N / 24 threads a row (16, 32, 64, 128). The
+// exchanges address element i at i ^ ((i / 24) & 15) (at 384, i ^ ((i >> 3) & 15)): a permutation of
+// [0, N) that meets 2 wavefronts, the minimum, for every stage's reads and writes (checked exhaustively on
+// the host for the four sizes), with no padding.
+template <class R> __host__ __device__ constexpr bool wide24_plan(int n) {
+    return sizeof(R) == 4 && (n == 384 || n == 768 || n == 1536 || n == 3072);
+}
+template <int N> struct Wide24Plan {
+    static constexpr int E = 24;
+    static constexpr int NT = N / E;
+    static constexpr int nstages = N == 3072 ? 4 : 3;
+    __host__ __device__ static constexpr int radix(int s) {
+        return s == 0 ? 24 : (N == 384 ? 4 : (N == 768 ? (s == 1 ? 8 : 4) : (s <= 2 ? 8 : 2)));
+    }
+    __host__ __device__ static constexpr int ns(int s) { return s == 0 ? 1 : ns(s - 1) * radix(s - 1); }
+    // the packed table (W_{Ns RAD}^(r k) of stage s >= 1 at tw_base(s) + k (RAD - 1) + r - 1, k < Ns)
+    __host__ __device__ static constexpr int tw_base(int s) { return s <= 1 ? 0 : tw_base(s - 1) + ns(s - 1) * (radix(s - 1) - 1); }
+    static constexpr int TW = tw_base(nstages);
+    static constexpr int ROWSZ = N;   // shared elements of one transform (swizzled, unpadded)
+};
+template <int N> struct Wide24Addr {
+    __device__ __forceinline__ int operator()(int i) const { return N == 384 ? i ^ ((i >> 3) & 15) : i ^ ((i / 24) & 15); }
+};
+
 // threads of one transform within one warp (row tiles of the wide plan)
 struct WarpSync {
     __device__ __forceinline__ void operator()() const { __syncwarp(); }

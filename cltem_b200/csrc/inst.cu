@@ -267,7 +267,7 @@ bool rowpair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tra
 }
 
 template <class RR> void row_w3_attrs() {
-    if constexpr (std::is_same<RR, float>::value && RowCfg<N, RR>::WIDE3) set_smem(k_row_step_w3<N>, RC::smem());
+    if constexpr (std::is_same<RR, float>::value && (RowCfg<N, RR>::WIDE3 || RowCfg<N, RR>::WIDE24)) set_smem(k_row_step_w3<N>, RC::smem());
 }
 // kernel attributes are per device: set once for each device this process launches on
 bool g_attrs_done[64] = {};
@@ -323,11 +323,12 @@ bool row_step_d(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans
         return false;
     }
 }
-// the FP32 row step with the three-stage wide plan (RowCfg::WIDE3), compiled for its blocks per SM
+// the FP32 row step with the three-stage wide plan or a radix-24 plan (RowCfg::WIDE3 / WIDE24), compiled for
+// its blocks per SM
 template <class RR>
 bool row_step_w3(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans, const cplx<RR> *tw, RR a, int xa,
                  int xb, int load_all, const int *tsel, size_t tstride, int pf) {
-    if constexpr (std::is_same<RR, float>::value && RowCfg<N, RR>::WIDE3) {
+    if constexpr (std::is_same<RR, float>::value && (RowCfg<N, RR>::WIDE3 || RowCfg<N, RR>::WIDE24)) {
         k_row_step_w3<N><<<pf == kWaveFastRows ? row_grid_wave_fast(batch) : row_grid(batch), row_block(), RC::smem(),
                            s>>>(wave, trans, tw, a, xa, xb, load_all, tsel, tstride, pf);
         MS_CUDA(cudaGetLastError());
@@ -338,7 +339,7 @@ bool row_step_w3(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tran
 }
 // blocks of the row step resident on the whole device
 template <class RR> int row_resident() {
-    if constexpr (std::is_same<RR, float>::value && RowCfg<N, RR>::WIDE3)
+    if constexpr (std::is_same<RR, float>::value && (RowCfg<N, RR>::WIDE3 || RowCfg<N, RR>::WIDE24))
         return resident_blocks(k_row_step_w3<N>, RC::THREADS, RC::smem());
     else
         return resident_blocks(k_row_step<RR, N>, RC::THREADS, RC::smem());

@@ -61,25 +61,31 @@ struct DetArgs {
 };
 
 // Row tiles: ROWS rows per block, P::NT threads per row (P the FFT plan: the wide two-stage plan for FP32
-// at 256 / 512 / 1024, fft_wide.cuh; the radix-8/4/2/3 Stockham plan otherwise, fft.cuh).
+// at 256 / 512 / 1024, the three-stage wide plan at 2048 to 8192 and the radix-24 plans at 384 to 3072,
+// fft_wide.cuh; the radix-8/4/2/3 Stockham plan otherwise, fft.cuh).
 template <int N, class R> struct RowCfg {
     static constexpr bool WIDE = wide_plan<R>(N);
     static constexpr bool WIDE3 = !WIDE && wide3_plan<R>(N);   // the three-stage wide plan (FP32 2048, 4096)
-    using P = std::conditional_t<WIDE, WidePlan<N>, std::conditional_t<WIDE3, Wide3Plan<N>, Plan<N>>>;
-    static constexpr int ROWS = WIDE ? 8 : (WIDE3 ? (N == 2048 ? 2 : 1)
-                                                   : (N <= 128 ? 8 : (N <= 256 ? 8 : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1)))));
+    static constexpr bool WIDE24 = wide24_plan<R>(N);            // the radix-24 plans (FP32 384 to 3072)
+    using P = std::conditional_t<WIDE, WidePlan<N>,
+                                 std::conditional_t<WIDE3, Wide3Plan<N>, std::conditional_t<WIDE24, Wide24Plan<N>, Plan<N>>>>;
+    static constexpr int ROWS = WIDE ? 8 : (WIDE3 ? (N == 2048 ? 2 : 1) : (WIDE24 ? 128 / (N / 24)
+                                                   : (N <= 128 ? 8 : (N <= 256 ? 8 : (N <= 512 ? 4 : (N <= 1024 ? 2 : 1))))));
     static_assert(N % ROWS == 0, "row tile must divide the grid");
     static_assert(P::NT * ROWS <= 1024, "row block too large");
     static constexpr int THREADS = P::NT * ROWS;
     static_assert(ROWS <= 15, "one named barrier per row");
     // radix-8 plan: a row's threads are whole warps, so each row synchronises on its own named barrier;
-    // wide plan: a row's threads lie inside one warp (two rows per warp at 16 threads a row)
-    static constexpr bool NAMED = !WIDE && (P::NT % 32) == 0 && ROWS > 1;
+    // wide plan (and radix-24 plans of at most 32 threads a row): a row's threads lie inside one warp (two rows
+    // per warp at 16 threads a row)
+    static constexpr bool WARP = WIDE || (WIDE24 && P::NT <= 32);
+    static constexpr bool NAMED = !WARP && (P::NT % 32) == 0 && ROWS > 1;
     static_assert(!WIDE || (P::NT == 32 || (P::NT == 16 && ROWS % 2 == 0)), "wide rows must tile whole warps");
     // twiddle entries staged in shared memory, and the offset of the row plan's table (Ctx::twiddles)
-    static constexpr int TWN = WIDE ? WidePlan<N>::TW : (WIDE3 ? Wide3Plan<N>::TW : N);
-    static constexpr int TW_OFF = (WIDE || WIDE3) ? N : 0;
-    static constexpr int ROWSZ = WIDE ? WidePlan<N>::ROWSZ : (WIDE3 ? Wide3Plan<N>::ROWSZ : RowAddr::size(N));
+    static constexpr int TWN = WIDE ? WidePlan<N>::TW : (WIDE3 ? Wide3Plan<N>::TW : (WIDE24 ? Wide24Plan<N>::TW : N));
+    static constexpr int TW_OFF = (WIDE || WIDE3 || WIDE24) ? N : 0;
+    static constexpr int ROWSZ =
+        WIDE ? WidePlan<N>::ROWSZ : (WIDE3 ? Wide3Plan<N>::ROWSZ : (WIDE24 ? Wide24Plan<N>::ROWSZ : RowAddr::size(N)));
     // the table is read from global memory (L1 / L2) when it and the rows do not both fit (FP64 8192)
     static constexpr bool TWG = sizeof(cplx<R>) * (size_t)(TWN + ROWS * ROWSZ) > kMaxBlockSmem;
     static constexpr int TWS = TWG ? 0 : TWN;   // twiddle entries staged in shared memory
@@ -126,6 +132,13 @@ __device__ __forceinline__ void row_transform(cplx<R> (&v)[RowCfg<N, R>::P::E], 
                                                                             NamedSync{1 + (int)threadIdx.y, RC::P::NT});
     else if constexpr (RC::WIDE3)
         fft_stages<R, N, SIGN, 0, WideRowAddr<32>, BlockSync, Wide3Plan<N>>(v, sm, WideRowAddr<32>(), t, tw, BlockSync());
+    else if constexpr (RC::WIDE24 && RC::WARP)
+        fft_stages<R, N, SIGN, 0, Wide24Addr<N>, WarpSync, Wide24Plan<N>>(v, sm, Wide24Addr<N>(), t, tw, WarpSync());
+    else if constexpr (RC::WIDE24 && RC::NAMED)
+        fft_stages<R, N, SIGN, 0, Wide24Addr<N>, NamedSync, Wide24Plan<N>>(v, sm, Wide24Addr<N>(), t, tw,
+                                                                          NamedSync{1 + (int)threadIdx.y, RC::P::NT});
+    else if constexpr (RC::WIDE24)
+        fft_stages<R, N, SIGN, 0, Wide24Addr<N>, BlockSync, Wide24Plan<N>>(v, sm, Wide24Addr<N>(), t, tw, BlockSync());
     else if constexpr (RC::NAMED) fft<R, N, SIGN>(v, sm, RowAddr(), t, tw, NamedSync{1 + (int)threadIdx.y, RC::P::NT});
     else fft<R, N, SIGN>(v, sm, RowAddr(), t, tw);
 }
@@ -260,7 +273,9 @@ k_row_step_d(double2 *__restrict__ wave, const double2 *__restrict__ trans, cons
 // The FP32 row step with the three-stage wide plan (2048, 4096, 8192), compiled for the blocks per SM its
 // shared memory allows (4 x 128 threads at 2048, 3 x 128 at 4096, 1 x 256 at 8192): without the hint the
 // compiler takes 175-185 registers a thread at 2048 and 4096, which leaves 2 blocks (8 warps) per SM.
-template <int N> constexpr int wide3_minb() { return N == 2048 ? 4 : (N == 4096 ? 3 : 1); }
+// blocks per SM the FP32 row step of the three-stage wide plans and the radix-24 plans is compiled for (the
+// radix-24 rows take 168 registers without a bound: 4 blocks of 128 threads give them 128)
+template <int N> constexpr int wide3_minb() { return wide24_plan<float>(N) ? 4 : (N == 2048 ? 4 : (N == 4096 ? 3 : 1)); }
 template <int N>
 __global__ void __launch_bounds__(RowCfg<N, float>::THREADS, wide3_minb<N>())
 k_row_step_w3(float2 *__restrict__ wave, const float2 *__restrict__ trans, const float2 *__restrict__ twg, float a,
@@ -279,7 +294,8 @@ template <int N, int PAIRS_ = rowpair_base<N>()> struct RowPairCfg {
     static constexpr int PAIRS = PAIRS_;   // row pairs a block
     static constexpr int THREADS = P::NT * PAIRS;
     static constexpr size_t smem() { return sizeof(float2) * (size_t)N + sizeof(float4) * (size_t)N * PAIRS; }
-    static constexpr bool ok = !RowCfg<N, float>::WIDE && !RowCfg<N, float>::WIDE3 && THREADS <= 1024 &&
+    static constexpr bool ok = !RowCfg<N, float>::WIDE && !RowCfg<N, float>::WIDE3 && !RowCfg<N, float>::WIDE24 &&
+                               THREADS <= 1024 &&
                                N % (2 * PAIRS) == 0 && smem() <= kMaxBlockSmem;
 };
 // Row pairs a block of the step: twice the base at 384² and 768² (measured in a STEM run per size, row-pass
