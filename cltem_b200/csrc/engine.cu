@@ -1968,10 +1968,7 @@ struct Sim : SimBase {
             return ops.col_variant_name ? ops.col_variant_name(index) : std::string();
         }
         if (which != 1 || index < 0 || index >= ops.row_variants) throw ArgError("row step variant out of range");
-        static const char *names[4] = {"plain", "L2 prefetch of the rows one grid residency ahead",
-                                       "L2 prefetch of the rows two grid residencies ahead",
-                                       "wave-fastest grid order (the same rows of consecutive waves together)"};
-        return names[index];
+        return ops.row_variant_name ? ops.row_variant_name(index) : std::string();
     }
     void get_tuning(int *batch, int *col, int *n_col, int *row, int *n_row) override {
         if (batch) *batch = default_batch();

@@ -238,7 +238,10 @@ bool tmx_col_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw,
 template <class RR> void rowpair_attrs() {
     if constexpr (std::is_same<RR, float>::value && pair_rows<N>())
         set_smem(k_row_step_pair<N, rowpair_pairs<N>()>, RowPairStepCfg<N>::smem());
+    if constexpr (std::is_same<RR, float>::value && alt_pair_rows<N>())
+        set_smem(k_row_step_pair<N, altrow_pairs<N>()>, RowPairCfg<N, altrow_pairs<N>()>::smem());
 }
+
 // blocks of kernel k (block size threads, dynamic smem bytes) resident on the whole device
 template <class K> int resident_blocks(K k, int threads, size_t smem) {
     int per_sm = 0;
@@ -264,6 +267,43 @@ bool rowpair_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tra
     } else {
         return false;
     }
+}
+
+// the two-row step of the plain plan as the alternative row plan (variants 4-7: prefetch / order mode v - 4)
+template <class RR>
+bool altrow_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans, const cplx<RR> *tw, RR a, int xa,
+                 int xb, int load_all, const int *tsel, size_t tstride, int variant) {
+    if constexpr (std::is_same<RR, float>::value && alt_pair_rows<N>()) {
+        constexpr int PR = altrow_pairs<N>();
+        using PC = RowPairCfg<N, PR>;
+        static int res[64] = {};
+        int dev = 0;
+        MS_CUDA(cudaGetDevice(&dev));
+        const int mode = variant - 4;
+        if (mode > 0 && mode < 3 && !res[dev]) res[dev] = resident_blocks(k_row_step_pair<N, PR>, PC::THREADS, PC::smem());
+        const int pf = mode == 3 ? kWaveFastRows : (mode > 0 ? mode * res[dev] : 0);
+        if (mode != 3 && batch > 65535) throw std::runtime_error("batch too large for the row grid");
+        const dim3 g = mode == 3 ? dim3(batch, N / (2 * PR)) : dim3(N / (2 * PR), batch);
+        k_row_step_pair<N, PR><<<g, dim3(Plan<N>::NT, PR), PC::smem(), s>>>(wave, trans, tw, a, xa, xb, load_all, tsel,
+                                                                          tstride, pf);
+        MS_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        return false;
+    }
+}
+template <class RR> constexpr int row_variant_count() {
+    if constexpr (std::is_same<RR, float>::value) return alt_pair_rows<N>() ? 8 : 4;
+    else return 4;
+}
+std::string row_variant_name(int v) {
+    static const char *modes[4] = {"plain", "L2 prefetch of the rows one grid residency ahead",
+                                   "L2 prefetch of the rows two grid residencies ahead",
+                                   "wave-fastest grid order (the same rows of consecutive waves together)"};
+    if (v < 0 || v >= row_variant_count<R>()) return "";
+    if (v < 4) return modes[v];
+    return std::string("plain Stockham plan (radix ") + (is_pow2(N) ? "8" : "12 then 4") + "), two rows a thread; " +
+           modes[v - 4];
 }
 
 template <class RR> void row_w3_attrs() {
@@ -350,7 +390,11 @@ inline dim3 col_block() { return dim3(CC::COLS, CC::P::NT); }
 void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a, int xa, int xb,
               int load_all, const int *tsel, size_t tstride, int variant) {
     ensure_attrs();
-    if (variant < 0 || variant > 3) throw std::runtime_error("row pass variant out of range");
+    if (variant < 0 || variant >= row_variant_count<R>()) throw std::runtime_error("row pass variant out of range");
+    if (variant >= 4) {
+        if (altrow_step<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride, variant)) return;
+        throw std::runtime_error("row pass variant out of range");
+    }
     if (batch > 65535 && variant != 3) throw std::runtime_error("batch too large for the row grid");
     if (rowpair_step<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride, variant)) return;
     static int res[64] = {};
@@ -442,6 +486,8 @@ PassOps<MS_REAL> make_pass_ops<MS_REAL, MS_N>() {
     o.cols_per_tile = CC::COLS;
     o.col_variants = tma_col_variants<R>();
     o.col_variant_name = col_variant_name;
+    o.row_variants = row_variant_count<R>();
+    o.row_variant_name = row_variant_name;
     o.row_step = row_step;
     o.row_fft = row_fft;
     o.col_step = col_step;

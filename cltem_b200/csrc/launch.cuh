@@ -17,10 +17,12 @@ struct PassOps {
     // row_step(..., xa, xb, load_all, tsel, tstride): active columns x < xa or x >= xb; tsel (or nullptr) the
     // transmission set of each wave, sets tstride elements apart (see k_row_step)
     // ..., variant): 0 plain; 1, 2 each block also prefetches into L2 the rows of the block one (two) residencies
-    // of the grid later; 3 the grid in wave-fastest order (kWaveFastRows) (row_variants of them)
+    // of the grid later; 3 the grid in wave-fastest order (kWaveFastRows); 4-7 the same four with the two-row
+    // step of the plain Stockham plan where the size's default row plan is a wide one (row_variants of them)
     void (*row_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R, int, int, int, const int *,
                      size_t, int) = nullptr;
-    int row_variants = 4;
+    int row_variants = 4;   // 8 where the two-row plain-plan step is the alternative plan (variants 4-7)
+    std::string (*row_variant_name)(int) = nullptr;   // a description of row variant v
     void (*row_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
     // col_step(..., mode, tiles_lo, tiles_hi, variant): the leading tiles_lo and trailing tiles_hi column tiles;
     // variant picks the kernel of the plain step (COL_STEP without a reciprocal copy), 0 <= variant <

@@ -304,6 +304,16 @@ template <int N, int PAIRS_ = rowpair_base<N>()> struct RowPairCfg {
 template <int N> constexpr int rowpair_pairs() { return (N == 384 || N == 768 ? 2 : 1) * rowpair_base<N>(); }
 template <int N> using RowPairStepCfg = RowPairCfg<N, rowpair_pairs<N>()>;
 template <int N> constexpr bool pair_rows() { return RowPairStepCfg<N>::ok; }
+// The two-row step on the sizes whose default row plan is a wide or radix-24 one: the plain Stockham plan of
+// fft.cuh (radix-8 at 2^k, radix-12 then radix-4 at 3·2^k) as the autotuner's alternative FFT plan for the row
+// pass (row variants 4 to 7). A different plan rounds differently: its results agree with the default plan's
+// to FP32 rounding, not bit for bit. 128 threads a block (256 where a row takes more).
+template <int N> constexpr int altrow_pairs() { return Plan<N>::NT >= 128 ? 1 : 128 / Plan<N>::NT; }
+template <int N> constexpr bool alt_pair_rows() {
+    return !RowPairStepCfg<N>::ok && (RowCfg<N, float>::WIDE || RowCfg<N, float>::WIDE3 || RowCfg<N, float>::WIDE24) &&
+           RowPairCfg<N, altrow_pairs<N>()>::THREADS <= 1024 && N % (2 * altrow_pairs<N>()) == 0 &&
+           RowPairCfg<N, altrow_pairs<N>()>::smem() <= kMaxBlockSmem;
+}
 // blocks per SM the two-row step is compiled for: a 128-register budget (measured against no cap: 2048² and
 // 4096² the same, 384² to 3072² 6-21% faster at the cap)
 template <int N, int PAIRS = rowpair_base<N>()> constexpr int rowpair_minb() {

@@ -422,9 +422,10 @@ class Simulation:
         return best.value, rate.value
 
     def set_step_variant(self, col_variant, row_variant=None):
-        """Kernels of the batched STEM step (mslice_set_step_variant): column 0 one block per tile, 1 / 2 the
-        persistent TMA-fed passes; row 0 plain, 1 / 2 with an L2 prefetch one / two grid residencies ahead. The
-        row variant is kept when not given."""
+        """Kernels of the batched STEM step (mslice_set_step_variant): column 0 one block per tile, then the
+        size's other column kernels (step_variant_name(0, v)); row 0 plain, 1 / 2 with an L2 prefetch one / two
+        grid residencies ahead, 3 in wave-fastest order, and where the size's default row plan is a wide one,
+        4-7 the same four with the plain Stockham plan. The row variant is kept when not given."""
         if row_variant is None:
             row_variant = self.tuning()["row_variant"]
         _check(self.lib.mslice_set_step_variant(self.h, int(col_variant), int(row_variant)))

@@ -1,5 +1,5 @@
-"""The probe-batch autotuner: it picks one of the candidates, later runs use that batch, and the results do
-not depend on the batch."""
+"""The autotuner: it picks one of the candidate batches and step kernels, later runs use them, and the results
+do not depend on the batch."""
 import numpy as np
 import pytest
 
@@ -13,14 +13,18 @@ def test_tune_batch_picks_a_candidate_and_keeps_results(gpu_ctx, kirkland):
     gpu_ctx.load_params(kirkland)
     s, st = small_stem(double_precision=False, scan=5)
     conf = phonons(st, 1)[0]
-    ref_sim = Simulation(gpu_ctx, s.cfg)
-    ref_sim.set_atoms(conf)
     pix = np.arange(25, dtype=np.int32)
-    ref = ref_sim.stem(pix)
     sim = Simulation(gpu_ctx, s.cfg)
     sim.set_atoms(conf)
     best, rate = sim.tune_batch([4, 8, 16], reps=2)
     assert best in (4, 8, 16) and rate > 0
+    # the reference: the same step kernels (the tuner may pick another FFT plan for the row pass, which rounds
+    # differently) at the engine's default batch
+    t = sim.tuning()
+    ref_sim = Simulation(gpu_ctx, s.cfg)
+    ref_sim.set_atoms(conf)
+    ref_sim.set_step_variant(t["col_variant"], t["row_variant"])
+    ref = ref_sim.stem(pix)
     sim.build_transmission()
     l0 = gpu_ctx.launch_count()
     got = sim.stem(pix)
@@ -45,7 +49,8 @@ def test_tune_batch_default_candidates_are_cached(gpu_ctx, kirkland):
 @pytest.mark.parametrize("res", [256, 512, 768, 1024, 2048])
 def test_column_step_variants_are_bit_identical(gpu_ctx, kirkland, res):
     """Every column-step kernel the tuner may pick (the persistent TMA-fed passes, the one-block-per-tile kernel
-    at other tile widths) does the default kernel's arithmetic in the same order: identical detector values
+    at other tile widths) and every launch mode of the row step does the default kernel's arithmetic in the
+    same order: identical detector values
     over a batch large enough that every persistent block loops over many (wave, tile) items and reuses each
     shared-memory stage many times."""
     gpu_ctx.load_params(kirkland)
@@ -56,11 +61,13 @@ def test_column_step_variants_are_bit_identical(gpu_ctx, kirkland, res):
     sim.set_atoms(conf)
     t = sim.tuning()
     nv = t["col_variants"]
-    assert t["row_variants"] == 4
+    nr = t["row_variants"]
+    # 4 prefetch / order modes; 8 where the plain Stockham plan is the alternative row plan (wide default plans)
+    assert nr == (8 if res in (256, 384, 512, 768, 1024, 2048) else 4)
     assert nv >= (2 if res <= 512 else 1)   # the persistent passes where their stages and tables fit
     names = [sim.step_variant_name(0, v) for v in range(nv)]
     assert len(set(names)) == nv and all(names)
-    assert len({sim.step_variant_name(1, v) for v in range(4)}) == 4
+    assert len({sim.step_variant_name(1, v) for v in range(nr)}) == nr
     with pytest.raises(MsliceError):
         sim.step_variant_name(0, nv)
     pix = np.arange(144, dtype=np.int32)
@@ -73,10 +80,21 @@ def test_column_step_variants_are_bit_identical(gpu_ctx, kirkland, res):
             out.append(sim.stem(pix))   # a second run replays the batch's CUDA graph
     for r in out[1:]:
         assert np.array_equal(r, out[0])
+    # the alternative row plan (variants 4-7): bit-identical among its four launch modes and with every column
+    # kernel, within FP32 rounding of the default plan
+    alt = []
+    for v in (0, nv - 1):
+        for rv in range(4, nr):
+            sim.set_step_variant(v, rv)
+            alt.append(sim.stem(pix))
+    for r in alt[1:]:
+        assert np.array_equal(r, alt[0])
+    if alt:
+        assert np.linalg.norm(alt[0] - out[0]) <= 1e-5 * np.linalg.norm(out[0])
     with pytest.raises(MsliceError):
         sim.set_step_variant(nv, 0)
     with pytest.raises(MsliceError):
-        sim.set_step_variant(0, 4)
+        sim.set_step_variant(0, nr)
     sim.close()
 
 
