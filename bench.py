@@ -40,9 +40,9 @@ UNIT = "probe·slices/s"
 WORKLOAD = "stem_adf_perovskite_10x10x20_512x512_64x64probes_40slices_phonon_u0.08"
 # DRAM bytes per wave of one launch of each step kernel at 512^2 FP32 (ncu dram__bytes_read.sum +
 # dram__bytes_write.sum over one launch of the timed configuration, divided by its waves), measured at this
-# workload's autotuned batch of 2048 waves on this build's kernels (row pass with its L2 prefetch, persistent
-# TMA-fed column pass); a kernel change needs a new capture
-NCU_DRAM_BYTES_PER_WAVE = {"row_step": (2956389120 + 2893711616) / 2048, "col_step": (3087454464 + 2890425600) / 2048}
+# workload's autotuned batch of 2048 waves on this build's kernels (plain row pass, per-pair-barrier persistent
+# column pass); a kernel change needs a new capture
+NCU_DRAM_BYTES_PER_WAVE = {"row_step": (2954973952 + 2895340288) / 2048, "col_step": (3023578880 + 2895932928) / 2048}
 
 
 def parse():
