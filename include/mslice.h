@@ -313,24 +313,27 @@ int mslice_incoherence_draws(const mslice_config *cfg, int pass, const int *pixe
 int mslice_plasmon_draws(const mslice_config *cfg, unsigned long long job, double thickness, double *depths, size_t cap,
                          size_t *n_depths, int n_events, double *angles);
 
-/* Autotuner of the probe batch and of the column step's kernel (no counterpart in the reference, which
- * propagates `parallel pixels` probes one at a time): times `reps` slice steps (one fused row and one
- * fused column pass) for each candidate batch size and each column-pass variant (see
- * mslice_set_step_variant) on zeroed scratch waves and makes the fastest pair the simulation's default
- * (the batch is used when cfg.probe_batch is 0). candidates = NULL tries 64..2048 and reuses a result
+/* Autotuner of the probe batch and of the step kernels (no counterpart in the reference, which propagates
+ * `parallel pixels` probes one at a time): times `reps` slice steps (one fused row and one fused column pass)
+ * for each candidate batch size and each column-pass variant, then each row-pass variant at the best pair (see
+ * mslice_set_step_variant), on zeroed scratch waves, and makes the fastest the simulation's default (the batch
+ * is used when cfg.probe_batch is 0). candidates = NULL tries 64..2048 and reuses a result
  * cached for this device, grid and precision in the process. Candidates whose waves would take more than
  * a quarter of the free device memory are skipped. best_batch / waves_per_second may be NULL. */
 int mslice_tune_batch(mslice_sim *sim, const int *candidates, int n_candidates, int reps, int *best_batch,
                       double *waves_per_second);
 /* The kernels of the batched STEM step (no counterpart in the reference). Column step: 0 = one block per
  * column tile and wave at the default tile width; the further variants of the grid and precision (FP32) are
- * the persistent passes, one or two blocks per SM, whose producer warp streams tiles into a ring of
- * shared-memory stages with TMA (power-of-two grids where their shared memory fits), and the one-block-per-tile
- * kernel at half and twice the default tile width (mslice_step_variant_name describes each). Row step: 0 =
- * plain; 1, 2 = each block also asks the copy engine to prefetch into L2 the rows that the blocks one or two
- * residencies of the grid later will read; 3 = the grid in wave-fastest order, so blocks issued together read
- * the same transmission rows. All variants give bit-identical results. Out-of-range values fail
- * with MSLICE_ERR_ARG. */
+ * the persistent passes, one or two blocks per SM, that stream tiles into a ring of shared-memory stages with
+ * TMA (power-of-two grids where their shared memory fits; among them the passes with one barrier domain per
+ * column pair at 256^2 to 2048^2), and the one-block-per-tile kernel at other tile widths and register budgets
+ * (mslice_step_variant_name describes each). Row step: 0 = plain; 1, 2 = each block also asks the copy engine
+ * to prefetch into L2 the rows that the blocks one or two residencies of the grid later will read; 3 = the
+ * grid in wave-fastest order, so blocks issued together read the same transmission rows; where the grid's
+ * default row plan is a wide one (FP32 256^2 to 8192^2 and the 3*2^k grids), 4-7 = the same four with the plain
+ * Stockham plan in the two-row step. All variants give bit-identical results except row variants 4-7, a
+ * different FFT plan, which agree with the others to FP32 rounding. Out-of-range values fail with
+ * MSLICE_ERR_ARG. */
 int mslice_set_step_variant(mslice_sim *sim, int col_variant, int row_variant);
 /* A description of step-kernel variant `index` (which: 0 column, 1 row) of this simulation's grid and
  * precision into buf (NUL-terminated, at most cap bytes). */
