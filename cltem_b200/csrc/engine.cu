@@ -592,6 +592,7 @@ struct Sim : SimBase {
         N = cfg.resolution;
         NN = (size_t)N * N;
         ops = pass_ops<R>(N);
+        col_variant = ops.default_col_variant;
         s2d = (double)(1.0f / sqrtf((float)((size_t)N * N)));
         if (ctx->params.form < 0) throw StateError("no parameterisation loaded (mslice_params_load)");
         if (cfg.full3d && ctx->params.form < 0) throw StateError("no parameterisation loaded");
@@ -1043,7 +1044,7 @@ struct Sim : SimBase {
     }
 
     int tuned_batch = 0;   // set by tune_batch (or the per-process cache of earlier tunings)
-    int col_variant = 0;   // kernel of the batched column step (PassOps::col_step), set by tune_batch
+    int col_variant = 0;   // kernel of the batched column step (PassOps::col_step): the size's default, then tune_batch's
     int row_variant = 0;   // L2 prefetch distance of the batched row step (PassOps::row_step), set by tune_batch
 
     // the error word of the persistent passes: read after the stream's work is done, reset, reported

@@ -136,6 +136,17 @@ template <class RR> constexpr KindList col_kinds() {
     return k;
 }
 template <class RR> constexpr int tma_col_variants() { return col_kinds<RR>().n; }
+// the default column kernel before any tuning: the per-pair-barrier pass where it exists (the tuner's pick in
+// every measured run at those grids: two blocks per SM at 256^2 and 512^2, one at 1024^2 and 2048^2), else 0
+template <class RR> constexpr int default_col_variant() {
+    constexpr KindList k = col_kinds<RR>();
+    const int want = N <= 512 ? 12 : 11;
+    for (int i = 0; i < k.n; i++)
+        if (k.kind[i] == want) return i;
+    for (int i = 0; i < k.n; i++)
+        if (k.kind[i] == 11 || k.kind[i] == 12) return i;
+    return 0;
+}
 // the name of column-step variant v of this size
 std::string col_variant_name(int v) {
     constexpr KindList k = col_kinds<R>();
@@ -485,6 +496,7 @@ PassOps<MS_REAL> make_pass_ops<MS_REAL, MS_N>() {
     o.col_blocks = N / CC::COLS;
     o.cols_per_tile = CC::COLS;
     o.col_variants = tma_col_variants<R>();
+    o.default_col_variant = default_col_variant<R>();
     o.col_variant_name = col_variant_name;
     o.row_variants = row_variant_count<R>();
     o.row_variant_name = row_variant_name;

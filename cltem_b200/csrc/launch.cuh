@@ -31,6 +31,7 @@ struct PassOps {
     void (*col_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, PropTables<R>, R, R, DetArgs, cplx<R> *, int, int,
                      int, int) = nullptr;
     int col_variants = 1;
+    int default_col_variant = 0;   // the column kernel a batched STEM run uses until tuned (bit-identical to 0)
     std::string (*col_variant_name)(int) = nullptr;   // a description of column variant v
     int cols_per_tile = 0;
     void (*col_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
