@@ -257,6 +257,14 @@ def cpu_baseline_leg(n_probes):
             "sample_rate": r["sample_rate"], "threads": threads, "reference_kernels": ref_kernel_leg()}
 
 
+def workload_config(probes, slices, steps):
+    """The workload both arms time (the same keys and values in both lines; each arm's engine details are under
+    the line's "engine" key)."""
+    return {"workload": WORKLOAD, "grid": 512, "probes": probes, "slices": slices, "phonon_configs_per_gpu": steps,
+            "precision": "complex64 waves and FFTs; FP64 phase arguments, offsets and Kahan accumulation",
+            "l2": "inputs larger than L2 (per configuration: 4096 waves x 2 MiB + 40 transmission slices x 2 MiB)"}
+
+
 def run_reference(args):
     rank, local, world = dist_env()
     if world > 1 and rank != 0:
@@ -279,8 +287,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": 512, "probes": 4096, "slices": S,
-                   "parallelism": "host threads (OpenMP over probes)", "sample_wall_s": wall},
+        "config": workload_config(4096, S, args.steps),
+        "engine": {"parallelism": "host threads (OpenMP over probes)", "sample_wall_s": wall},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": (f"per step (timed): transmission build of {S} slices + {n_probes} of 4096 probes "
                                     f"through all slices of one phonon configuration, FP32 (the reference's _f path); "
@@ -780,11 +788,9 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": 512, "probes": npx, "slices": S,
-                       "phonon_configs_per_gpu": args.steps, "probe_batch": sim.cfg.probe_batch or (f"{tuned[0]} (autotuned: {tuned[1]:.0f} waves/s per slice step)" if tuned else "engine default"),
+            "config": workload_config(npx, S, args.steps),
+            "engine": {"probe_batch": sim.cfg.probe_batch or (f"{tuned[0]} (autotuned: {tuned[1]:.0f} waves/s per slice step)" if tuned else "engine default"),
                        "step_kernels": step_kernels,
-                       "precision": "complex64 waves and FFTs; FP64 phase arguments, offsets and Kahan accumulation",
-                       "l2": "inputs larger than L2 (per configuration: 4096 waves x 2 MiB + 40 transmission slices x 2 MiB)",
                        "parallelism": f"dp{world} (phonon configurations sharded over GPUs)"},
             "roofline": roofline,
             "cpu_baseline": cpu,
