@@ -10,7 +10,8 @@
 //   - there is no producer warp: one thread of the first pair issues the tile loads and stores at item
 //     boundaries, so the block is 16 warps of 128 registers instead of 17 of 96;
 //   - each thread keeps the twiddles of its butterflies in registers (they depend only on its position in
-//     the transform), so the exchanges are the only shared-memory traffic of the FFTs.
+//     the transform), so the exchanges are the only shared-memory traffic of the FFTs (at 1024 the second
+//     and third stages' come from a shared copy of the table, see tmx_tw_reg_stages).
 // Tile layout in a stage: element (row y, pair p), 16 bytes, at slot PAIRS * y + (p ^ h(y)), h(y) =
 // (y * PAIRS >> 3) mod PAIRS: the copy engine's 128B / 64B / 32B swizzle for 8 / 4 / 2 pairs (16-byte chunks
 // of a 1024-byte atom XORed with the row's position in it), none for one pair. The FFT exchanges store
@@ -55,10 +56,16 @@ template <int N, int PAIRS, int S> __host__ __device__ constexpr int tmx_mask_w(
 // base combined with the constant c: the two share no bit when (c & mask) == 0, and then the sum is the XOR
 __device__ __forceinline__ int tmx_at(int base, int c, int mask) { return (c & mask) == 0 ? base + c : base ^ c; }
 
-// twiddles a thread holds: stage S >= 1 keeps NB (RAD - 1) of them, in stage order
+// twiddles a thread holds: stage S >= 1 keeps NB (RAD - 1) of them, in stage order, up to stage
+// tmx_tw_reg_stages; the later stages read theirs from a copy of the plan's table in shared memory. At 1024
+// (ptxas, 128 registers a thread) all three stages' twiddles in registers spill 120 bytes a thread, two stages'
+// 88 bytes, one stage's none; at the other grids every stage's are kept (2048 spills either way, and its
+// stages leave no room for the table).
+template <int N> __host__ __device__ constexpr int tmx_tw_reg_stages() { return N == 1024 ? 1 : Plan<N>::nstages - 1; }
+template <int N> __host__ __device__ constexpr bool tmx_tw_staged() { return tmx_tw_reg_stages<N>() < Plan<N>::nstages - 1; }
 template <int N> __host__ __device__ constexpr int tmx_tw_off(int S) {
     int o = 0;
-    for (int s = 1; s < S; s++) o += (Plan<N>::E / Plan<N>::radix(s)) * (Plan<N>::radix(s) - 1);
+    for (int s = 1; s < S && s <= tmx_tw_reg_stages<N>(); s++) o += (Plan<N>::E / Plan<N>::radix(s)) * (Plan<N>::radix(s) - 1);
     return o;
 }
 template <int N> constexpr int tmx_tw_count() { return tmx_tw_off<N>(Plan<N>::nstages); }
@@ -78,7 +85,10 @@ template <int N, int COLS_, int STAGES_, int MINB_ = 1> struct TmxColCfg {
     static constexpr int TWR = tmx_tw_count<N>();
     // 1024-byte alignment slack (the swizzle atom), stages, the propagator's row tables (py and its errors),
     // two mbarriers per stage
-    static constexpr size_t smem() { return 1024 + (size_t)STAGES * STAGE_BYTES + sizeof(float2) * 2 * N + 16 * STAGES; }
+    // (and, where some stages read their twiddles from shared memory, the plan's table)
+    static constexpr size_t smem() {
+        return 1024 + (size_t)STAGES * STAGE_BYTES + sizeof(float2) * (tmx_tw_staged<N>() ? 3 : 2) * N + 16 * STAGES;
+    }
     static constexpr bool ok = is_pow2(N) && P::E == 8 && (PAIRS == 1 || PAIRS == 2 || PAIRS == 4 || PAIRS == 8) &&
                                NT % 32 == 0 && THREADS <= 1024 && PAIRS <= 15 && STAGES >= 3 && N % BOX_ROWS == 0 &&
                                BOX_ROWS >= 16 && smem() <= kMaxBlockSmem && MINB * (smem() + 1024) <= 228 * 1024 &&
@@ -91,7 +101,8 @@ template <int N, int COLS_, int STAGES_, int MINB_ = 1> struct TmxColCfg {
 // rbase: tmx_lay(t) ^ p; wb[S]: tmx_lay(tmx_wrow<N, S>(t)) ^ p.
 template <int N, int PAIRS, int SIGN, int S, int TWR>
 __device__ __forceinline__ void tmx_stages(float2 (&va)[Plan<N>::E], float2 (&vb)[Plan<N>::E], float4 *sm, int rbase,
-                                           const int (&wb)[Plan<N>::nstages], const float2 (&twr)[TWR], NamedBar bar) {
+                                           const int (&wb)[Plan<N>::nstages], const float2 (&twr)[TWR],
+                                           const float2 *s_tw, int t, NamedBar bar) {
     using P = Plan<N>;
     constexpr int E = P::E, NT = P::NT;
     constexpr int RAD = P::radix(S);
@@ -99,6 +110,8 @@ __device__ __forceinline__ void tmx_stages(float2 (&va)[Plan<N>::E], float2 (&vb
     constexpr int NB = E / RAD;
     constexpr bool last = (S == P::nstages - 1);
     constexpr int TWO = tmx_tw_off<N>(S > 0 ? S : 1);
+    constexpr bool TWREG = S <= tmx_tw_reg_stages<N>();
+    constexpr int TWB = plan_tw_index(N, S > 0 ? S : 1, 0, 1);
     if constexpr (S > 0) {
         constexpr int RM = tmx_mask_lay<PAIRS, NT>();
 #pragma unroll
@@ -120,7 +133,8 @@ __device__ __forceinline__ void tmx_stages(float2 (&va)[Plan<N>::E], float2 (&vb
             float2 x = va[b + r * NB], y = vb[b + r * NB];
             if constexpr (S > 0) {
                 if (r > 0) {
-                    const float2 w = twr[TWO + b * (RAD - 1) + (r - 1)];
+                    const float2 w = TWREG ? twr[TWREG ? TWO + b * (RAD - 1) + (r - 1) : 0]
+                                           : s_tw[TWB + ((t + b * NT) % Ns) * (RAD - 1) + (r - 1)];
                     x = (SIGN < 0) ? cmul(x, w) : cmulc(x, w);
                     y = (SIGN < 0) ? cmul(y, w) : cmulc(y, w);
                 }
@@ -150,13 +164,13 @@ __device__ __forceinline__ void tmx_stages(float2 (&va)[Plan<N>::E], float2 (&vb
                     make_float4(oa[b + m * NB].x, oa[b + m * NB].y, ob[b + m * NB].x, ob[b + m * NB].y);
         }
         bar();
-        tmx_stages<N, PAIRS, SIGN, S + 1, TWR>(va, vb, sm, rbase, wb, twr, bar);
+        tmx_stages<N, PAIRS, SIGN, S + 1, TWR>(va, vb, sm, rbase, wb, twr, s_tw, t, bar);
     }
 }
 
 // thread t's twiddles: stage S, butterfly j = t + b NT, k = j mod Ns, entries r = 1..RAD-1 of the packed table
 template <int N, int S, int TWR> __device__ __forceinline__ void tmx_load_twiddles(float2 (&twr)[TWR], const float2 *twg, int t) {
-    if constexpr (S < Plan<N>::nstages) {
+    if constexpr (S <= tmx_tw_reg_stages<N>()) {
         using P = Plan<N>;
         constexpr int RAD = P::radix(S), Ns = P::ns(S), NB = P::E / RAD, NT = P::NT;
         constexpr int TWB = plan_tw_index(N, S, 0, 1);
@@ -194,7 +208,8 @@ k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict_
     unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
     float4 *stages = reinterpret_cast<float4 *>(base);
     float2 *s_py = reinterpret_cast<float2 *>(base + (size_t)K * TC::STAGE_BYTES), *s_pye = s_py + N;
-    uint64_t *full = reinterpret_cast<uint64_t *>(s_pye + N);
+    float2 *s_tw = s_pye + N;   // the plan's table, where some stages read their twiddles from shared memory
+    uint64_t *full = reinterpret_cast<uint64_t *>(s_tw + (tmx_tw_staged<N>() ? N : 0));
     uint64_t *empty = full + K;
     const int tid = threadIdx.x;
     const int p = tid / NT, t = tid % NT;
@@ -208,6 +223,7 @@ k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict_
     for (int i = tid; i < N; i += THREADS) {
         s_py[i] = pt.py[i];
         s_pye[i] = pt.pye[i];
+        if constexpr (tmx_tw_staged<N>()) s_tw[i] = twg[i];
     }
     float2 twr[TC::TWR];
     tmx_load_twiddles<N, 1, TC::TWR>(twr, twg, t);
@@ -280,7 +296,7 @@ k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict_
             va[m] = make_float2(q.x, q.y);
             vb[m] = make_float2(q.z, q.w);
         }
-        tmx_stages<N, PAIRS, -1, 0, TC::TWR>(va, vb, sm, rbase, wb, twr, bar);
+        tmx_stages<N, PAIRS, -1, 0, TC::TWR>(va, vb, sm, rbase, wb, twr, s_tw, t, bar);
 #pragma unroll
         for (int m = 0; m < E; m++) {
             const int y = t + m * NT;
@@ -288,7 +304,7 @@ k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict_
             va[m] = (y < ca.x || y >= ca.y) ? cscale(prop_mul<float>(va[m], pxa, py, exa, ey), bscale) : mk<float>(0, 0);
             vb[m] = (y < cb.x || y >= cb.y) ? cscale(prop_mul<float>(vb[m], pxb, py, exb, ey), bscale) : mk<float>(0, 0);
         }
-        tmx_stages<N, PAIRS, +1, 0, TC::TWR>(va, vb, sm, rbase, wb, twr, bar);
+        tmx_stages<N, PAIRS, +1, 0, TC::TWR>(va, vb, sm, rbase, wb, twr, s_tw, t, bar);
         bar();   // the pair's last exchange reads are done: the stage takes its results
 #pragma unroll
         for (int m = 0; m < E; m++)
