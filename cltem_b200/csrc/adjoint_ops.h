@@ -37,6 +37,13 @@ void atom_grad(cudaStream_t s, const GradSlices &sl, const double *ax, const dou
                int n, double startx, double starty, double dx, int form, const T *prm, int i_lim, const float2 *tabp,
                double *gxy, double *work);
 int atom_grad_work_doubles(int max_count);
+// Full 3-D potential: dL/d(x, y, z) of every sorted atom, accumulated into grad (3 per atom) from gV of `count`
+// slices starting at p.slice0 (gather3d.cu); wscale = the sub-slice thickness (dL/d(trapezoid sum) = wscale gV);
+// prm the FP64 parameterisation table
+struct PotParams;
+void atom_grad_3d(cudaStream_t s, int form, const double *ax, const double *ay, const double *az, const int *aZ,
+                  const int *block_start, const double *prm, const PotParams &p, int count, const double *gV,
+                  double wscale, double *grad);
 int reduction_blocks();
 
 }  // namespace ms

@@ -1995,7 +1995,6 @@ struct Sim : SimBase {
         adj_valid = false;
         const mslice_geometry &g = H.g;
         if (cfg.mode != MSLICE_MODE_CTEM) throw StateError("the image loss needs a CTEM simulation");
-        if (cfg.full3d) throw Unsupported("gradients are implemented for the projected potential");
         if (cfg.mixed_static > 1) throw Unsupported("gradients are implemented without mixed static potentials");
         if (cfg.plasmon) throw Unsupported("gradients are implemented without plasmon scattering");
         if (!atoms_set) throw StateError("atoms not set");
@@ -2087,7 +2086,8 @@ struct Sim : SimBase {
         MS_CUDA(cudaMemcpyAsync(hbs.data(), block_start.p, hbs.size() * sizeof(int), cudaMemcpyDeviceToHost, st()));
         MS_CUDA(cudaStreamSynchronize(st()));
         const int n_in = hbs.back();
-        gxy.ensure(ctx, 2 * (size_t)std::max(n_in, 1));
+        const int ncomp = cfg.full3d ? 3 : 2;   // gradient components gathered per atom (z only under the full 3-D model)
+        gxy.ensure(ctx, ncomp * (size_t)std::max(n_in, 1));
         {   // scratch of the atom gather: the atoms of the largest checkpoint segment
             int mx = 1;
             for (int s0 = 0; s0 < S; s0 += c) {
@@ -2096,7 +2096,7 @@ struct Sim : SimBase {
             }
             gwork.ensure(ctx, (size_t)atom_grad_work_doubles(mx));
         }
-        MS_CUDA(cudaMemsetAsync(gxy.p, 0, 2 * (size_t)std::max(n_in, 1) * sizeof(double), st()));
+        MS_CUDA(cudaMemsetAsync(gxy.p, 0, ncomp * (size_t)std::max(n_in, 1) * sizeof(double), st()));
         // gT and gV of every slice of a segment, so that the band limit, gV and the atom gather run once per
         // segment over all its slices (batch-1 launches of those kernels leave most of the GPU idle)
         fw.ensure(ctx, NN); gT.ensure(ctx, (size_t)c * NN); gV.ensure(ctx, (size_t)c * NN);
@@ -2121,7 +2121,13 @@ struct Sim : SimBase {
             band_limit(gT.p, m);   // G_E = bandlimit(G_T): the band limit is self-adjoint
             grad_v<R>(st(), (size_t)m * NN, E.p + (size_t)s0 * NN, gT.p, g.sigma, gV.p);
             ctx->launches++;
-            for (int t0 = 0; t0 < m; t0 += kGradMaxSlices) {
+            if (cfg.full3d) {   // the full 3-D trapezoid pairs samples across atoms: replayed per pixel
+                const PotParams pp = pot_params(s0);
+                atom_grad_3d(st(), ctx->params.form, axs.p, ays.p, azs.p, aZs.p, block_start.p, ctx->prm_d, pp, m, gV.p,
+                             g.dz / pp.integrals, gxy.p);
+                ctx->launches++;
+            }
+            for (int t0 = 0; t0 < m && !cfg.full3d; t0 += kGradMaxSlices) {
                 GradSlices gs{};
                 gs.n = std::min(kGradMaxSlices, m - t0);
                 gs.stride = NN;
@@ -2137,7 +2143,7 @@ struct Sim : SimBase {
             }
         }
         MS_CUDA(cudaMemcpyAsync(hp.data(), part.p, 3 * (size_t)nred * sizeof(double), cudaMemcpyDeviceToHost, st()));
-        std::vector<double> hg(2 * (size_t)std::max(n_in, 1));
+        std::vector<double> hg(ncomp * (size_t)std::max(n_in, 1));
         std::vector<int> hidx(std::max<size_t>(n_atoms, 1));
         MS_CUDA(cudaMemcpyAsync(hg.data(), gxy.p, hg.size() * sizeof(double), cudaMemcpyDeviceToHost, st()));
         if (n_atoms) MS_CUDA(cudaMemcpyAsync(hidx.data(), idx_out.p, n_atoms * sizeof(int), cudaMemcpyDeviceToHost, st()));
@@ -2150,8 +2156,7 @@ struct Sim : SimBase {
             std::fill(gxyz, gxyz + 3 * n_atoms, 0.0);
             for (int i = 0; i < n_in; i++) {   // sorted position i holds input atom idx_out[i]
                 const int o = hidx[i];
-                gxyz[3 * (size_t)o] = hg[2 * (size_t)i];
-                gxyz[3 * (size_t)o + 1] = hg[2 * (size_t)i + 1];
+                for (int q = 0; q < ncomp; q++) gxyz[3 * (size_t)o + q] = hg[ncomp * (size_t)i + q];
             }
         }
     }

@@ -238,12 +238,15 @@ int mslice_ctem_run(mslice_sim *sim, double *ew, double *diff, double *image);
 /* Loss L = sum over pixels of (I - target)^2 for the CTEM objective-lens image I of the current atom
  * configuration (simulateImagePerfect, microscope/simulationctem.cpp:114-166), and its gradients by the
  * hand-written adjoint of the multislice: dL/d(x, y, z) of every atom passed to mslice_set_atoms (input
- * order, 3 per atom; z is 0 in the projected model, where z only selects the slice), dL/dC10 and dL/dC30
- * (per Å). target holds res*res doubles (x fastest). Slice waves are checkpointed every
- * `checkpoint_every` slices (0: ceil(sqrt(n_slices)); 1: every slice, no recomputation) and recomputed
- * segment by segment in the backward pass. Projected potentials (with or without beam tilt) only; the
- * full 3-D model, mixed static potentials and plasmons fail with MSLICE_ERR_UNSUPPORTED. Any output
- * pointer may be NULL. The same as mslice_ctem_loss_forward followed by mslice_ctem_loss_backward. */
+ * order, 3 per atom; z is 0 in the projected model, where z only selects the slice, and a true derivative
+ * under the full 3-D model), dL/dC10 and dL/dC30 (per Å). target holds res*res doubles (x fastest). Slice
+ * waves are checkpointed every `checkpoint_every` slices (0: ceil(sqrt(n_slices)); 1: every slice, no
+ * recomputation) and recomputed segment by segment in the backward pass. Projected (with or without beam
+ * tilt) and full 3-D potentials; mixed static potentials and plasmons fail with MSLICE_ERR_UNSUPPORTED. The
+ * full 3-D gradients gather with FP64 atomics, so they are reproducible to FP64 rounding rather than bit for
+ * bit; they are the derivative within the current binning (the full 3-D loss jumps where an atom crosses a bin
+ * edge, which reorders the trapezoid's samples). Any output pointer may be NULL. The same as mslice_ctem_loss_forward followed by
+ * mslice_ctem_loss_backward. */
 int mslice_ctem_loss_grad(mslice_sim *sim, const double *target, double *loss, double *grad_xyz, double *grad_c10,
                           double *grad_c30, int checkpoint_every);
 /* The two halves of mslice_ctem_loss_grad, for autograd frameworks that run the backward pass later: the
