@@ -1216,7 +1216,7 @@ struct Sim : SimBase {
         for (int s = 0; s < g.n_slices; s++) {
             timed(st(), MSLICE_K_ROW_STEP, (double)nb * NN * sizeof(C) * ((s == 0 ? 1.0 : fa) + 1.0 + fa), [&] {
                 ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a, xa, xb, s == 0 ? 1 : 0,
-                             sel ? sel + (size_t)s * nb : nullptr, set_stride, row_variant);
+                             sel ? sel + (size_t)s * nb : nullptr, set_stride, row_variant, ctx->step_err);
             });
             bool is_out = oi < outs.size() && outs[oi] == s;
             int mode = !is_out ? COL_STEP : (s == g.n_slices - 1 ? COL_DET_ONLY : COL_STEP_DET);
@@ -1369,7 +1369,8 @@ struct Sim : SimBase {
             ctx->launches++;
             size_t oi = 0;
             for (int s = 0; s < g.n_slices; s++) {
-                ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a, xa, xb, s == 0 ? 1 : 0, nullptr, 0, 0);
+                ops.row_step(st(), wave.p, nb, trans.p + (size_t)s * NN, tw, a, xa, xb, s == 0 ? 1 : 0, nullptr, 0, 0,
+                             ctx->step_err);
                 const bool is_out = oi < outs.size() && outs[oi] == s;
                 const int mode = !is_out ? COL_STEP : (s == g.n_slices - 1 ? COL_DET_ONLY : COL_STEP_DET);
                 pt.px = px.p; pt.py = py.p; pt.pxe = pxe.p; pt.pye = pye.p;   // set_propagator keeps the buffers
@@ -1453,7 +1454,7 @@ struct Sim : SimBase {
             // single waves keep every column so the exit wave and the reciprocal copy are complete
             timed(st(), MSLICE_K_ROW_STEP, 3.0 * NN * sizeof(C), [&] {
                 ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1, K > 1 ? tsel.p + s : nullptr,
-                             set_stride, 0);
+                             set_stride, 0, ctx->step_err);
             });
             bool is_out = oi < outs.size() && outs[oi] == s;
             timed(st(), MSLICE_K_COL_STEP, (is_out ? 3.0 : 2.0) * NN * sizeof(C), [&] {
@@ -1910,7 +1911,7 @@ struct Sim : SimBase {
         // time one slice step of each (batch, row variant, column variant)
         auto rate_of = [&](int b, int row_v, int col_v) {
             auto step = [&] {
-                ops.row_step(st(), wave.p, b, trans.p, tw, a, xa, xb, 0, nullptr, 0, row_v);
+                ops.row_step(st(), wave.p, b, trans.p, tw, a, xa, xb, 0, nullptr, 0, row_v, ctx->step_err);
                 ops.col_step(st(), wave.p, b, tw, pt, b2, ds, det, nullptr, COL_STEP, tiles_lo, tiles_hi, col_v);
                 ctx->launches += 2;
             };
@@ -2029,7 +2030,7 @@ struct Sim : SimBase {
             if (want_grad && s % c == 0)
                 MS_CUDA(cudaMemcpyAsync(ck_buf.p + (size_t)(s / c) * NN, wave.p, NN * sizeof(C), cudaMemcpyDeviceToDevice, st()));
             if (want_grad && c == 1) ops.row_step_save(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, save.p + (size_t)s * NN);
-            else ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1, nullptr, 0, 0);
+            else ops.row_step(st(), wave.p, 1, trans.p + (size_t)s * NN, tw, a, N, N, 1, nullptr, 0, 0, ctx->step_err);
             bool last = s == S - 1;
             ops.col_step(st(), wave.p, 1, tw, pt, b, ds, nodet, last ? recip.p : nullptr, last ? COL_STEP_DET : COL_STEP,
                          all_tiles, 0, 0);

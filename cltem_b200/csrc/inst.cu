@@ -303,18 +303,50 @@ bool altrow_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tran
         return false;
     }
 }
-template <class RR> constexpr int row_variant_count() {
-    if constexpr (std::is_same<RR, float>::value) return alt_pair_rows<N>() ? 8 : 4;
-    else return 4;
+// row variants: 0-3 the default plan's kernel in the four prefetch / order modes; then, where they exist, the
+// plain Stockham plan's two-row step in the same four modes (4-7), and the default plan's kernel with staged
+// transmission rows (k_row_step_ts) in the same four modes (row_ts_first() on)
+template <class RR> constexpr bool row_alt_ok() {
+    if constexpr (std::is_same<RR, float>::value) return alt_pair_rows<N>();
+    else return false;
 }
+template <class RR> constexpr bool row_ts_here() {
+    if constexpr (std::is_same<RR, float>::value) return row_ts_ok<N>();
+    else return false;
+}
+template <class RR> constexpr int row_ts_first() { return row_alt_ok<RR>() ? 8 : 4; }
+template <class RR> constexpr int row_variant_count() { return row_ts_first<RR>() + (row_ts_here<RR>() ? 4 : 0); }
 std::string row_variant_name(int v) {
     static const char *modes[4] = {"plain", "L2 prefetch of the rows one grid residency ahead",
                                    "L2 prefetch of the rows two grid residencies ahead",
                                    "wave-fastest grid order (the same rows of consecutive waves together)"};
     if (v < 0 || v >= row_variant_count<R>()) return "";
     if (v < 4) return modes[v];
+    if (v >= row_ts_first<R>()) return std::string("transmission rows staged by the copy engine; ") + modes[v - row_ts_first<R>()];
     return std::string("plain Stockham plan (radix ") + (is_pow2(N) ? "8" : "12 then 4") + "), two rows a thread; " +
            modes[v - 4];
+}
+// the FP32 row step with staged transmission rows in prefetch / order mode `mode`
+template <class RR>
+bool row_step_ts(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *trans, const cplx<RR> *tw, RR a, int xa,
+                 int xb, int load_all, const int *tsel, size_t tstride, int mode, int *err) {
+    if constexpr (row_ts_here<RR>()) {
+        // the copy engine's source: the block's rows start 16-byte aligned when trans and the set stride are
+        if ((reinterpret_cast<uintptr_t>(trans) & 15) != 0 || (tstride * sizeof(cplx<RR>)) % 16 != 0 || err == nullptr)
+            throw std::runtime_error("staged transmission rows need a 16-byte aligned transmission and an error word");
+        static int res[64] = {};
+        int dev = 0;
+        MS_CUDA(cudaGetDevice(&dev));
+        if (mode > 0 && mode < 3 && !res[dev]) res[dev] = resident_blocks(k_row_step_ts<N>, RC::THREADS, row_ts_smem<N, RR>());
+        const int pf = mode == 3 ? kWaveFastRows : (mode > 0 ? mode * res[dev] : 0);
+        k_row_step_ts<N><<<pf == kWaveFastRows ? dim3(batch, N / RC::ROWS) : dim3(N / RC::ROWS, batch),
+                           dim3(RC::P::NT, RC::ROWS), row_ts_smem<N, RR>(), s>>>(wave, trans, tw, a, xa, xb, load_all,
+                                                                                 tsel, tstride, pf, err);
+        MS_CUDA(cudaGetLastError());
+        return true;
+    } else {
+        return false;
+    }
 }
 
 template <class RR> void row_w3_attrs() {
@@ -328,6 +360,7 @@ void ensure_attrs() {
     if (dev < 0 || dev >= 64 || g_attrs_done[dev]) return;
     set_smem(k_row_step<R, N>, RC::smem());
     row_w3_attrs<R>();
+    if constexpr (row_ts_here<R>()) set_smem(k_row_step_ts<N>, row_ts_smem<N, R>());
     if constexpr (std::is_same<R, double>::value && fp64_row_bounded<N>()) set_smem(k_row_step_d<N>, RC::smem());
     set_smem(k_row_fft<R, N, -1>, RC::smem());
     set_smem(k_row_fft<R, N, +1>, RC::smem());
@@ -399,9 +432,15 @@ inline dim3 col_grid(int batch) { return dim3(N / CC::COLS, batch); }
 inline dim3 col_block() { return dim3(CC::COLS, CC::P::NT); }
 
 void row_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *trans, const cplx<R> *tw, R a, int xa, int xb,
-              int load_all, const int *tsel, size_t tstride, int variant) {
+              int load_all, const int *tsel, size_t tstride, int variant, int *err) {
     ensure_attrs();
     if (variant < 0 || variant >= row_variant_count<R>()) throw std::runtime_error("row pass variant out of range");
+    if (variant >= row_ts_first<R>()) {
+        if (variant - row_ts_first<R>() != 3 && batch > 65535) throw std::runtime_error("batch too large for the row grid");
+        if (row_step_ts<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride, variant - row_ts_first<R>(), err))
+            return;
+        throw std::runtime_error("row pass variant out of range");
+    }
     if (variant >= 4) {
         if (altrow_step<R>(s, batch, wave, trans, tw, a, xa, xb, load_all, tsel, tstride, variant)) return;
         throw std::runtime_error("row pass variant out of range");

@@ -18,10 +18,12 @@ struct PassOps {
     // transmission set of each wave, sets tstride elements apart (see k_row_step)
     // ..., variant): 0 plain; 1, 2 each block also prefetches into L2 the rows of the block one (two) residencies
     // of the grid later; 3 the grid in wave-fastest order (kWaveFastRows); 4-7 the same four with the two-row
-    // step of the plain Stockham plan where the size's default row plan is a wide one (row_variants of them)
+    // step of the plain Stockham plan where the size's default row plan is a wide one; then (FP32 wide and
+    // radix-24 plans) the same four with the transmission rows staged in shared memory by the copy engine
+    // (row_variants of them); ..., err): the error word of the staged variants' bounded waits (tma.cuh StepError)
     void (*row_step)(cudaStream_t, cplx<R> *, int, const cplx<R> *, const cplx<R> *, R, int, int, int, const int *,
-                     size_t, int) = nullptr;
-    int row_variants = 4;   // 8 where the two-row plain-plan step is the alternative plan (variants 4-7)
+                     size_t, int, int *) = nullptr;
+    int row_variants = 4;   // 8 or 12 where the alternative plan and the staged rows exist
     std::string (*row_variant_name)(int) = nullptr;   // a description of row variant v
     void (*row_fft)(cudaStream_t, const cplx<R> *, cplx<R> *, int, const cplx<R> *, R, int) = nullptr;
     // col_step(..., mode, tiles_lo, tiles_hi, variant): the leading tiles_lo and trailing tiles_hi column tiles;

@@ -15,6 +15,7 @@
 #include "fft.cuh"
 #include "fft_wide.cuh"
 #include "fft_pair.cuh"
+#include "tma.cuh"
 
 #include <type_traits>
 
@@ -215,11 +216,21 @@ template <class R, int N, int THREADS, int OTHER> constexpr int fp64_step_minb()
     return (sizeof(R) == 8 && THREADS == 256 && Plan<N>::E == 8) ? 3
          : (sizeof(R) == 8 && Plan<N>::E == 12 && THREADS * 128 < 65536) ? 65536 / (THREADS * 128) : OTHER;
 }
-// the row step's body, shared by k_row_step and its FP64 3-blocks-per-SM build k_row_step_d
-template <class R, int N>
+// Row step with staged transmission rows (TST): the block's ROWS transmission rows are contiguous in HBM, and one
+// thread asks the copy engine for all of them (cp.async.bulk into shared memory, completion on an mbarrier) as
+// the block starts, so they arrive while the inverse row FFT runs. Without TST every thread loads its T
+// elements only after that FFT and waits for them there. The staged rows sit after the block's twiddles and
+// exchange rows (16-byte aligned), the mbarrier after them.
+template <int N, class R> constexpr size_t row_tstage_off() { return (RowCfg<N, R>::smem() + 15) / 16 * 16; }
+template <int N, class R> constexpr size_t row_ts_smem() {
+    return row_tstage_off<N, R>() + sizeof(cplx<R>) * (size_t)RowCfg<N, R>::ROWS * N + 8;
+}
+// the row step's body, shared by k_row_step and its FP64 3-blocks-per-SM build k_row_step_d; err (TST only):
+// the error word a wait that is abandoned writes (tma.cuh StepError)
+template <class R, int N, bool TST = false>
 __device__ __forceinline__ void row_step_body(cplx<R> *__restrict__ wave, const cplx<R> *__restrict__ trans,
                                               const cplx<R> *__restrict__ twg, R a, int xa, int xb, int load_all,
-                                              const int *__restrict__ tsel, size_t tstride, int pf) {
+                                              const int *__restrict__ tsel, size_t tstride, int pf, int *err = nullptr) {
     using RC = RowCfg<N, R>;
     using P = typename RC::P;
     constexpr int ROWS = RC::ROWS;
@@ -235,6 +246,17 @@ __device__ __forceinline__ void row_step_body(cplx<R> *__restrict__ wave, const 
     cplx<R> *row = wave + (size_t)w * N * N + (size_t)y * N;
     // tsel (optional): transmission set of each wave; set k of this slice starts k * tstride after trans
     const cplx<R> *trow = trans + (tsel ? (size_t)tsel[w] * tstride : (size_t)0) + (size_t)y * N;
+    cplx<R> *sT = reinterpret_cast<cplx<R> *>(smraw + row_tstage_off<N, R>());
+    uint64_t *tbar = reinterpret_cast<uint64_t *>(smraw + row_tstage_off<N, R>() + sizeof(cplx<R>) * ROWS * N);
+    if constexpr (TST) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            mbar_init(tbar, 1);
+            mbar_fence_init();
+            constexpr unsigned bytes = (unsigned)(sizeof(cplx<R>) * ROWS * N);
+            mbar_arrive_expect_tx(tbar, bytes);
+            bulk_load(sT, trow, bytes, tbar);   // thread (0, 0)'s row is the block's first
+        }
+    }
     cplx<R> v[P::E];
 #pragma unroll
     for (int m = 0; m < P::E; m++) {
@@ -243,8 +265,12 @@ __device__ __forceinline__ void row_step_body(cplx<R> *__restrict__ wave, const 
     }
     __syncthreads();
     row_transform<R, N, +1>(v, sm, t, tw);
+    if constexpr (TST) {   // (an abandoned wait still lets the copy land before the block goes on)
+        if (!mbar_wait(tbar, 0, err, STEP_WAIT_FULL)) mbar_wait(tbar, 0, err, STEP_WAIT_DRAIN);
+    }
+    const cplx<R> *tr = TST ? sT + threadIdx.y * N : trow;
 #pragma unroll
-    for (int m = 0; m < P::E; m++) v[m] = cscale(cmul(v[m], trow[t + m * P::NT]), a);
+    for (int m = 0; m < P::E; m++) v[m] = cscale(cmul(v[m], tr[t + m * P::NT]), a);
     row_transform<R, N, -1>(v, sm, t, tw);
 #pragma unroll
     for (int m = 0; m < P::E; m++) {
@@ -281,6 +307,26 @@ __global__ void __launch_bounds__(RowCfg<N, float>::THREADS, wide3_minb<N>())
 k_row_step_w3(float2 *__restrict__ wave, const float2 *__restrict__ trans, const float2 *__restrict__ twg, float a,
               int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride, int pf) {
     row_step_body<float, N>(wave, trans, twg, a, xa, xb, load_all, tsel, tstride, pf);
+}
+
+// The FP32 row step with staged transmission rows (TST above), for the wide, three-stage wide and radix-24 row
+// plans where the extra shared memory fits. Blocks per SM: what the shared memory allows, at most the
+// 128-register occupancy of the plain kernels.
+template <int N> constexpr bool row_ts_ok() {
+    return (RowCfg<N, float>::WIDE || RowCfg<N, float>::WIDE3 || RowCfg<N, float>::WIDE24) &&
+           row_ts_smem<N, float>() <= kMaxBlockSmem;
+}
+template <int N> constexpr int row_ts_minb() {
+    constexpr int by_smem = (int)((228 * 1024) / (row_ts_smem<N, float>() + 1024));
+    constexpr int by_regs = 65536 / (RowCfg<N, float>::THREADS * 128);
+    constexpr int m = by_smem < by_regs ? by_smem : by_regs;
+    return m < 1 ? 1 : m;
+}
+template <int N>
+__global__ void __launch_bounds__(RowCfg<N, float>::THREADS, row_ts_minb<N>())
+k_row_step_ts(float2 *__restrict__ wave, const float2 *__restrict__ trans, const float2 *__restrict__ twg, float a,
+              int xa, int xb, int load_all, const int *__restrict__ tsel, size_t tstride, int pf, int *err) {
+    row_step_body<float, N, true>(wave, trans, twg, a, xa, xb, load_all, tsel, tstride, pf, err);
 }
 
 // The row step of the FP32 radix-8 / 3·2^k row plans (sizes without the wide plan) with each thread carrying

@@ -86,6 +86,14 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap *m, int x, int y,
                  "r"(x), "r"(y), "r"(smem_u32(src))
                  : "memory");
 }
+// 1-D bulk copy of `bytes` from global memory at src into shared memory at dst (both 16-byte aligned, bytes a
+// multiple of 16); completion is signalled on `bar` as transferred bytes
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 // wait until this thread's bulk groups have finished reading their shared-memory sources (the stage may be
 // overwritten), or have completed entirely (their global writes are done)

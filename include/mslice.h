@@ -334,8 +334,9 @@ int mslice_tune_batch(mslice_sim *sim, const int *candidates, int n_candidates, 
  * to prefetch into L2 the rows that the blocks one or two residencies of the grid later will read; 3 = the
  * grid in wave-fastest order, so blocks issued together read the same transmission rows; where the grid's
  * default row plan is a wide one (FP32 256^2 to 8192^2 and the 3*2^k grids), 4-7 = the same four with the plain
- * Stockham plan in the two-row step. All variants give bit-identical results except row variants 4-7, a
- * different FFT plan, which agree with the others to FP32 rounding. Until it is tuned or set, a batched STEM
+ * Stockham plan in the two-row step, and 8-11 = the same four as 0-3 with each block's transmission rows staged
+ * into shared memory by the copy engine as the block starts. All variants give bit-identical results except
+ * row variants 4-7, a different FFT plan, which agree with the others to FP32 rounding. Until it is tuned or set, a batched STEM
  * run uses the grid's default column kernel (FP32 256^2 to 2048^2: the per-pair-barrier pass; otherwise 0) and
  * row variant 0; mslice_get_tuning reports them. Out-of-range values fail with MSLICE_ERR_ARG. */
 int mslice_set_step_variant(mslice_sim *sim, int col_variant, int row_variant);
