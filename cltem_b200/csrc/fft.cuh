@@ -9,8 +9,8 @@
 // t + m*NT a thread loads from global memory, and the last stage writes exactly the elements
 // t + m*NT it stores, so only the inner stage boundaries go through shared memory.
 //
-// Sizes: N = 2^k (E = 8, radix-8 stages plus one radix-2/4 stage) and N = 3*2^k (E = 12, one radix-12
-// stage, radix-4 stages and an optional radix-2 stage). Unnormalised transforms; callers scale.
+// Sizes: N = 2^k (E = 8, radix-8 stages plus one radix-2/4 stage) and N = 3*2^k (E = 12, radix-4 stages, an
+// optional radix-2 stage and a radix-12 stage last). Unnormalised transforms; callers scale.
 #pragma once
 
 #include "common.cuh"
@@ -22,16 +22,17 @@ __host__ __device__ constexpr bool is_pow2(int n) { return n > 0 && (n & (n - 1)
 
 // The radix plan of a length, shared by the device stages and the host twiddle-table builder:
 // 2^k: k/3 radix-8 stages, then one radix-2 or radix-4 stage if k%3 != 0;
-// 3*2^k (k >= 2): one radix-12 stage (a prime-factor 3 x 4 DFT: no twiddles inside, dft12), (k-2)/2 radix-4
-// stages, then a radix-2 stage if k is odd. One exchange fewer than radix-3 and radix-4 stages apart (768: 4
-// stages instead of 5).
+// 3*2^k (k >= 2): (k-2)/2 radix-4 stages, a radix-2 stage if k is odd, then one radix-12 stage (a prime-factor
+// 3 x 4 DFT: no twiddles inside, dft12). One exchange fewer than radix-3 and radix-4 stages apart (768: 4
+// stages instead of 5). With the radix-12 stage last, every stage that writes to shared memory has a
+// power-of-two span Ns, so its write positions (j / Ns) Ns R + j mod Ns + m Ns are bit fields of j and m.
 __host__ __device__ constexpr int plan_k(int n) { return is_pow2(n) ? ilog2c(n) : ilog2c(n / 3); }
 __host__ __device__ constexpr int plan_nstages(int n) {
     return is_pow2(n) ? (plan_k(n) / 3 + (plan_k(n) % 3 ? 1 : 0)) : (1 + (plan_k(n) - 2) / 2 + (plan_k(n) % 2));
 }
 __host__ __device__ constexpr int plan_radix(int n, int s) {
     return is_pow2(n) ? (s < plan_k(n) / 3 ? 8 : (plan_k(n) % 3 == 1 ? 2 : 4))
-                      : (s == 0 ? 12 : (s <= (plan_k(n) - 2) / 2 ? 4 : 2));
+                      : (s == plan_nstages(n) - 1 ? 12 : (s < (plan_k(n) - 2) / 2 ? 4 : 2));
 }
 __host__ __device__ constexpr int plan_ns(int n, int s) { return s == 0 ? 1 : plan_ns(n, s - 1) * plan_radix(n, s - 1); }
 // Twiddle table layout: stage s >= 1 stores W_n^(r*k*n/(Ns*R)) for k < Ns, 1 <= r < R at

@@ -92,8 +92,14 @@ template <> struct TmaVariant<7> {
 // stores, no producer warp: 11 a tile of 8192 / N columns (512 threads, one block per SM), 12 half that tile
 // (256 threads, two blocks per SM)
 template <int V> struct TmxVariant;
-template <> struct TmxVariant<11> { template <int NN> using Cfg = TmxColCfg<NN, (8192 / NN > 1 ? 8192 / NN : 2), 3, 1>; };
-template <> struct TmxVariant<12> { template <int NN> using Cfg = TmxColCfg<NN, (4096 / NN > 1 ? 4096 / NN : 2), 3, 2>; };
+// columns of a per-pair-barrier tile: the largest power of two at most budget / n (at least 2)
+constexpr int tmx_cols(int n, int budget) {
+    int c = 2;
+    while (2 * c <= budget / n) c *= 2;
+    return c;
+}
+template <> struct TmxVariant<11> { template <int NN> using Cfg = TmxColCfg<NN, tmx_cols(NN, 8192), 3, 1>; };
+template <> struct TmxVariant<12> { template <int NN> using Cfg = TmxColCfg<NN, tmx_cols(NN, 4096), 3, 2>; };
 template <class RR, int V> constexpr bool tmx_col_ok() {
     if constexpr (std::is_same<RR, float>::value && pair_columns<N>() && N >= 256) {
         using TC = typename TmxVariant<V>::template Cfg<N>;
@@ -137,10 +143,11 @@ template <class RR> constexpr KindList col_kinds() {
 }
 template <class RR> constexpr int tma_col_variants() { return col_kinds<RR>().n; }
 // the default column kernel before any tuning: the per-pair-barrier pass where it exists (the tuner's pick in
-// every measured run at those grids: two blocks per SM at 256^2 and 512^2, one at 1024^2 and 2048^2), else 0
+// every measured run at those grids: two blocks per SM at 256^2 to 768^2, one at 1024^2, 1536^2, 2048^2 and
+// 3072^2), else 0
 template <class RR> constexpr int default_col_variant() {
     constexpr KindList k = col_kinds<RR>();
-    const int want = N <= 512 ? 12 : 11;
+    const int want = N <= 768 ? 12 : 11;
     for (int i = 0; i < k.n; i++)
         if (k.kind[i] == want) return i;
     for (int i = 0; i < k.n; i++)
@@ -323,7 +330,7 @@ std::string row_variant_name(int v) {
     if (v < 0 || v >= row_variant_count<R>()) return "";
     if (v < 4) return modes[v];
     if (v >= row_ts_first<R>()) return std::string("transmission rows staged by the copy engine; ") + modes[v - row_ts_first<R>()];
-    return std::string("plain Stockham plan (radix ") + (is_pow2(N) ? "8" : "12 then 4") + "), two rows a thread; " +
+    return std::string("plain Stockham plan (radix ") + (is_pow2(N) ? "8" : "4 then 12") + "), two rows a thread; " +
            modes[v - 4];
 }
 // the FP32 row step with staged transmission rows in prefetch / order mode `mode`

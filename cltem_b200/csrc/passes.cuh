@@ -351,7 +351,7 @@ template <int N> constexpr int rowpair_pairs() { return (N == 384 || N == 768 ? 
 template <int N> using RowPairStepCfg = RowPairCfg<N, rowpair_pairs<N>()>;
 template <int N> constexpr bool pair_rows() { return RowPairStepCfg<N>::ok; }
 // The two-row step on the sizes whose default row plan is a wide or radix-24 one: the plain Stockham plan of
-// fft.cuh (radix-8 at 2^k, radix-12 then radix-4 at 3·2^k) as the autotuner's alternative FFT plan for the row
+// fft.cuh (radix-8 at 2^k, radix-4 then radix-12 at 3·2^k) as the autotuner's alternative FFT plan for the row
 // pass (row variants 4 to 7). A different plan rounds differently: its results agree with the default plan's
 // to FP32 rounding, not bit for bit. 128 threads a block (256 where a row takes more).
 template <int N> constexpr int altrow_pairs() { return Plan<N>::NT >= 128 ? 1 : 128 / Plan<N>::NT; }

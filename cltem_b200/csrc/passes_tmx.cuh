@@ -1,4 +1,4 @@
-// passes_tmx.cuh — persistent column pass with one barrier domain per column pair (FP32, 2^k plans).
+// passes_tmx.cuh — persistent column pass with one barrier domain per column pair (FP32, 2^k and 3·2^k plans).
 //
 // Same arithmetic per element, in the same order, as k_col_step_pair / k_col_step_tma (column FFT of two
 // adjacent columns a thread, times the propagator inside its cut and the scale b, inverse column FFT), so
@@ -15,11 +15,15 @@
 // Tile layout in a stage: element (row y, pair p), 16 bytes, at slot PAIRS * y + (p ^ h(y)), h(y) =
 // (y * PAIRS >> 3) mod PAIRS: the copy engine's 128B / 64B / 32B swizzle for 8 / 4 / 2 pairs (16-byte chunks
 // of a 1024-byte atom XORed with the row's position in it), none for one pair. The FFT exchanges store
-// logical row i at physical row g(i) = i ^ ((i >> 3) & 7) with the same swizzle. Both layouts give every pair
-// the same slots (each pair only ever touches its own), and every access pattern of the radix-8/4/2 stages
-// meets 8 distinct 16-byte bank groups per quarter warp. Both maps are linear over GF(2) in the bits of the
-// row, so an address is a per-thread base combined with a constant: an add folded into the instruction where
-// the constant's bits lie outside the base's, one XOR otherwise.
+// logical row i at physical row g(i) = i ^ H((i >> 3) & 7) with the same swizzle: H the identity for the 2^k
+// plans; for the 3·2^k plans (radix-4 stages, a radix-2 stage, radix 12 last) H maps bits (1, 2, 4) to
+// (1, 6, 4), since their radix-4 writes at span 4 gather rows that the identity folds onto 4 bank groups.
+// Both layouts give every pair the same slots (each pair only ever touches its own), and every access pattern
+// of the plans' stages meets 8 distinct 16-byte bank groups per quarter warp (checked exhaustively on the host
+// for every grid and pair count). Both maps are linear over GF(2) in the bits of the row, and so are the
+// stages' read and write positions (all spans Ns of stages that write are powers of two), so an address is a
+// per-thread base combined with a constant: an add folded into the instruction where the constant's bits lie
+// outside the base's, one XOR otherwise.
 // Only this GPU's own wave buffer is read and written; no load uses cluster multicast.
 #pragma once
 
@@ -32,7 +36,10 @@ template <int PAIRS> __host__ __device__ constexpr int tmx_swz(int row) {
 }
 // 16-byte slot of logical row i of pair 0 in the copy engine's layout / in the exchange layout
 template <int PAIRS> __host__ __device__ constexpr int tmx_tlay(int i) { return PAIRS * i ^ tmx_swz<PAIRS>(i); }
-template <int PAIRS> __host__ __device__ constexpr int tmx_lay(int i) { return tmx_tlay<PAIRS>(i ^ ((i >> 3) & 7)); }
+template <int N> __host__ __device__ constexpr int tmx_h(int q) { return is_pow2(N) ? q : (q & 5) ^ ((q & 2) * 3); }
+template <int N, int PAIRS> __host__ __device__ constexpr int tmx_lay(int i) {
+    return tmx_tlay<PAIRS>(i ^ tmx_h<N>((i >> 3) & 7));
+}
 // the exchange write position of butterfly j's output 0 at stage S (fft.cuh: (j / Ns) Ns RAD + j mod Ns)
 template <int N, int S> __host__ __device__ constexpr int tmx_wrow(int j) {
     return (j / Plan<N>::ns(S)) * Plan<N>::ns(S) * Plan<N>::radix(S) + j % Plan<N>::ns(S);
@@ -43,15 +50,20 @@ template <int PAIRS, int NT> __host__ __device__ constexpr int tmx_mask_tlay() {
     for (int b = 1; b < NT; b <<= 1) m |= tmx_tlay<PAIRS>(b);
     return m;
 }
-template <int PAIRS, int NT> __host__ __device__ constexpr int tmx_mask_lay() {
+template <int N, int PAIRS, int NT> __host__ __device__ constexpr int tmx_mask_lay() {
     int m = PAIRS - 1;
-    for (int b = 1; b < NT; b <<= 1) m |= tmx_lay<PAIRS>(b);
+    for (int b = 1; b < NT; b <<= 1) m |= tmx_lay<N, PAIRS>(b);
     return m;
 }
 template <int N, int PAIRS, int S> __host__ __device__ constexpr int tmx_mask_w() {
     int m = PAIRS - 1;
-    for (int b = 1; b < Plan<N>::NT; b <<= 1) m |= tmx_lay<PAIRS>(tmx_wrow<N, S>(b));
+    for (int b = 1; b < Plan<N>::NT; b <<= 1) m |= tmx_lay<N, PAIRS>(tmx_wrow<N, S>(b));
     return m;
+}
+// the plans whose stages that write to shared memory all have power-of-two spans: every 2^k plan (E = 8) and
+// the 3·2^k plans, whose radix-12 stage comes last
+template <int N> __host__ __device__ constexpr bool tmx_plan_ok() {
+    return (is_pow2(N) && Plan<N>::E == 8) || (!is_pow2(N) && Plan<N>::E == 12 && Plan<N>::radix(Plan<N>::nstages - 1) == 12);
 }
 // base combined with the constant c: the two share no bit when (c & mask) == 0, and then the sum is the XOR
 __device__ __forceinline__ int tmx_at(int base, int c, int mask) { return (c & mask) == 0 ? base + c : base ^ c; }
@@ -89,7 +101,7 @@ template <int N, int COLS_, int STAGES_, int MINB_ = 1> struct TmxColCfg {
     static constexpr size_t smem() {
         return 1024 + (size_t)STAGES * STAGE_BYTES + sizeof(float2) * (tmx_tw_staged<N>() ? 3 : 2) * N + 16 * STAGES;
     }
-    static constexpr bool ok = is_pow2(N) && P::E == 8 && (PAIRS == 1 || PAIRS == 2 || PAIRS == 4 || PAIRS == 8) &&
+    static constexpr bool ok = tmx_plan_ok<N>() && is_pow2(P::NT) && (PAIRS == 1 || PAIRS == 2 || PAIRS == 4 || PAIRS == 8) &&
                                NT % 32 == 0 && THREADS <= 1024 && PAIRS <= 15 && STAGES >= 3 && N % BOX_ROWS == 0 &&
                                BOX_ROWS >= 16 && smem() <= kMaxBlockSmem && MINB * (smem() + 1024) <= 228 * 1024 &&
                                (size_t)MINB * THREADS * 128 <= 65536;
@@ -113,12 +125,12 @@ __device__ __forceinline__ void tmx_stages(float2 (&va)[Plan<N>::E], float2 (&vb
     constexpr bool TWREG = S <= tmx_tw_reg_stages<N>();
     constexpr int TWB = plan_tw_index(N, S > 0 ? S : 1, 0, 1);
     if constexpr (S > 0) {
-        constexpr int RM = tmx_mask_lay<PAIRS, NT>();
+        constexpr int RM = tmx_mask_lay<N, PAIRS, NT>();
 #pragma unroll
         for (int b = 0; b < NB; b++) {
 #pragma unroll
             for (int r = 0; r < RAD; r++) {
-                const float4 q = sm[tmx_at(rbase, tmx_lay<PAIRS>(b * NT + r * (N / RAD)), RM)];
+                const float4 q = sm[tmx_at(rbase, tmx_lay<N, PAIRS>(b * NT + r * (N / RAD)), RM)];
                 va[b + r * NB] = make_float2(q.x, q.y);
                 vb[b + r * NB] = make_float2(q.z, q.w);
             }
@@ -160,7 +172,7 @@ __device__ __forceinline__ void tmx_stages(float2 (&va)[Plan<N>::E], float2 (&vb
         for (int b = 0; b < NB; b++) {
 #pragma unroll
             for (int m = 0; m < RAD; m++)
-                sm[tmx_at(wb[S], tmx_lay<PAIRS>(tmx_wrow<N, S>(b * NT) | (m * Ns)), WM)] =
+                sm[tmx_at(wb[S], tmx_lay<N, PAIRS>(tmx_wrow<N, S>(b * NT) | (m * Ns)), WM)] =
                     make_float4(oa[b + m * NB].x, oa[b + m * NB].y, ob[b + m * NB].x, ob[b + m * NB].y);
         }
         bar();
@@ -185,7 +197,7 @@ template <int N, int S, int TWR> __device__ __forceinline__ void tmx_load_twiddl
 }
 template <int N, int PAIRS, int S> __device__ __forceinline__ void tmx_write_bases(int (&wb)[Plan<N>::nstages], int t, int p) {
     if constexpr (S < Plan<N>::nstages) {
-        wb[S] = tmx_lay<PAIRS>(tmx_wrow<N, S>(t)) ^ p;
+        wb[S] = tmx_lay<N, PAIRS>(tmx_wrow<N, S>(t)) ^ p;
         tmx_write_bases<N, PAIRS, S + 1>(wb, t, p);
     }
 }
@@ -229,7 +241,7 @@ k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict_
     tmx_load_twiddles<N, 1, TC::TWR>(twr, twg, t);
     int wb[P::nstages];
     tmx_write_bases<N, PAIRS, 0>(wb, t, p);
-    const int rbase = tmx_lay<PAIRS>(t) ^ p, tbase = tmx_tlay<PAIRS>(t) ^ p;
+    const int rbase = tmx_lay<N, PAIRS>(t) ^ p, tbase = tmx_tlay<PAIRS>(t) ^ p;
     constexpr int TM = tmx_mask_tlay<PAIRS, NT>();
     const NamedBar bar{1 + p, NT};
     __syncthreads();

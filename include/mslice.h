@@ -328,8 +328,8 @@ int mslice_tune_batch(mslice_sim *sim, const int *candidates, int n_candidates, 
 /* The kernels of the batched STEM step (no counterpart in the reference). Column step: 0 = one block per
  * column tile and wave at the default tile width; the further variants of the grid and precision (FP32) are
  * the persistent passes, one or two blocks per SM, that stream tiles into a ring of shared-memory stages with
- * TMA (power-of-two grids where their shared memory fits; among them the passes with one barrier domain per
- * column pair at 256^2 to 2048^2), and the one-block-per-tile kernel at other tile widths and register budgets
+ * TMA (where their shared memory fits; among them the passes with one barrier domain per
+ * column pair at 256^2 to 3072^2), and the one-block-per-tile kernel at other tile widths and register budgets
  * (mslice_step_variant_name describes each). Row step: 0 = plain; 1, 2 = each block also asks the copy engine
  * to prefetch into L2 the rows that the blocks one or two residencies of the grid later will read; 3 = the
  * grid in wave-fastest order, so blocks issued together read the same transmission rows; where the grid's
@@ -337,7 +337,7 @@ int mslice_tune_batch(mslice_sim *sim, const int *candidates, int n_candidates, 
  * Stockham plan in the two-row step, and 8-11 = the same four as 0-3 with each block's transmission rows staged
  * into shared memory by the copy engine as the block starts. All variants give bit-identical results except
  * row variants 4-7, a different FFT plan, which agree with the others to FP32 rounding. Until it is tuned or set, a batched STEM
- * run uses the grid's default column kernel (FP32 256^2 to 2048^2: the per-pair-barrier pass; otherwise 0) and
+ * run uses the grid's default column kernel (FP32 256^2 to 3072^2: the per-pair-barrier pass; otherwise 0) and
  * row variant 0; mslice_get_tuning reports them. Out-of-range values fail with MSLICE_ERR_ARG. */
 int mslice_set_step_variant(mslice_sim *sim, int col_variant, int row_variant);
 /* A description of step-kernel variant `index` (which: 0 column, 1 row) of this simulation's grid and
