@@ -180,9 +180,12 @@ std::string col_variant_name(int v) {
         return "persistent, per-pair barriers, TMA loads and stores, " + cols(kind == 11 ? c11 : c12) +
                ", 3 stages, " + (kind == 11 ? "1 block" : "2 blocks") + " per SM";
     }
-    if (kind == 9)
-        return "one block per (" + cols(kPairC) + ", wave), two columns a thread, " +
-               (pair_loose<N>() ? "64" : "128") + "-register budget";
+    if (kind == 9) {   // the budget a thread gets: 64, or 128 where the block's threads leave room for it
+        constexpr int threads = PairCfg<N, kPairC, !pair_loose<N>()>::THREADS;
+        const int regs = pair_loose<N>() ? 64 : std::min(128, 65536 / threads);
+        return "one block per (" + cols(kPairC) + ", wave), two columns a thread, " + std::to_string(regs) +
+               "-register budget";
+    }
     return "persistent, TMA loads and stores, " + cols(kPairC / 2) + ", " + stages(TmaVariant<6>::Cfg<N>::STAGES) +
            ", 1 block per SM";
 }
