@@ -344,8 +344,10 @@ struct Ctx {
         // plan (fft_wide.cuh) entries [n, 2n) hold its table, W_n^(r k) at k (R2 - 1) + r - 1; for the
         // three-stage wide plan and the radix-24 plans they hold their stages' tables in the packed layout
         // (Wide3Plan::tw_base, Wide24Plan::tw_base)
+        // (FP32 at 1024, 2048 and 4096: entries [2n, 3n) hold the 16-element column plan's table, Plan16::tw_base)
         const bool wide = wide_plan<R>(n), wide3 = !wide && wide3_plan<R>(n), wide24 = wide24_plan<R>(n);
-        const size_t count = (size_t)n * ((wide || wide3 || wide24) ? 2 : 1);
+        const bool p16 = sizeof(R) == 4 && plan16_ok(n);
+        const size_t count = (size_t)n * (p16 ? 3 : ((wide || wide3 || wide24) ? 2 : 1));
         std::vector<cplx<R>> h(count, mk<R>(0, 0));
         const long double two_pi = 2.0L * 3.14159265358979323846264338327950288L;
         for (int s = 1; s < plan_nstages(n); s++) {
@@ -375,6 +377,22 @@ struct Ctx {
             else if (n == 768) fill(Wide24Plan<768>());
             else if (n == 1536) fill(Wide24Plan<1536>());
             else fill(Wide24Plan<3072>());
+        }
+        if (p16) {
+            auto fill16 = [&](auto plan) {
+                using P = decltype(plan);
+                for (int st = 1; st < P::nstages; st++) {
+                    const int Ns = P::ns(st), RAD = P::radix(st);
+                    for (int k = 0; k < Ns; k++)
+                        for (int r = 1; r < RAD; r++) {
+                            long double a = -two_pi * (long double)(r * k) / (long double)(Ns * RAD);
+                            h[2 * (size_t)n + P::tw_base(st) + k * (RAD - 1) + (r - 1)] = round_unit<R>(std::cos(a), std::sin(a));
+                        }
+                }
+            };
+            if (n == 1024) fill16(Plan16<1024>());
+            else if (n == 2048) fill16(Plan16<2048>());
+            else fill16(Plan16<4096>());
         }
         if (wide) {
             const int E = wide_E(n), R2 = n / E;

@@ -55,6 +55,25 @@ struct Plan {
     __host__ __device__ static constexpr int tw_base(int s) { return plan_tw_index(N, s, 0, 1); }
 };
 
+// A 16-element plan for the 2^k column passes at 1024 to 4096 (the per-pair-barrier kernels): a radix-16 stage,
+// then radix-8 / radix-16 stages, 1024 = 16·8·8, 2048 = 16·16·8, 4096 = 16·16·16: one shared-memory exchange
+// fewer than the 8-element plan (8·8·8·2, 8·8·8·4, 8·8·8·8) at twice the elements a thread. Its twiddle table
+// has the packed layout of plan_tw_index (stage s at ns(s) - ns(1), N - 16 entries).
+__host__ __device__ constexpr bool plan16_ok(int n) { return n == 1024 || n == 2048 || n == 4096; }
+__host__ __device__ constexpr int plan16_radix(int n, int s) {
+    return s == 0 ? 16 : (n == 1024 ? 8 : (n == 2048 ? (s == 1 ? 16 : 8) : 16));
+}
+template <int N>
+struct Plan16 {
+    static constexpr bool pow2 = true;
+    static constexpr int E = 16;
+    static constexpr int NT = N / E;
+    static constexpr int nstages = 3;
+    __host__ __device__ static constexpr int radix(int s) { return plan16_radix(N, s); }
+    __host__ __device__ static constexpr int ns(int s) { return s == 0 ? 1 : ns(s - 1) * radix(s - 1); }
+    __host__ __device__ static constexpr int tw_base(int s) { return ns(s) - ns(1); }
+};
+
 // ---- small DFTs in registers; SIGN = -1 forward, +1 inverse --------------------------------------
 template <class C> __device__ __forceinline__ C mul_i(C a, int sign) {   // a * (sign * i)
     C r;

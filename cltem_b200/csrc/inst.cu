@@ -100,8 +100,12 @@ constexpr int tmx_cols(int n, int budget) {
 }
 template <> struct TmxVariant<11> { template <int NN> using Cfg = TmxColCfg<NN, tmx_cols(NN, 8192), 3, 1>; };
 template <> struct TmxVariant<12> { template <int NN> using Cfg = TmxColCfg<NN, tmx_cols(NN, 4096), 3, 2>; };
+// the 16-element plan (Plan16: one exchange fewer a transform, twice the elements a thread) at 1024 and 2048
+template <> struct TmxVariant<13> {
+    template <int NN> using Cfg = TmxColCfg<NN, tmx_cols(NN, 8192), 3, 1, std::conditional_t<plan16_ok(NN), Plan16<NN>, Plan<NN>>>;
+};
 template <class RR, int V> constexpr bool tmx_col_ok() {
-    if constexpr (std::is_same<RR, float>::value && pair_columns<N>() && N >= 256) {
+    if constexpr (std::is_same<RR, float>::value && pair_columns<N>() && N >= 256 && (V != 13 || plan16_ok(N))) {
         using TC = typename TmxVariant<V>::template Cfg<N>;
         return TC::ok && TC::COLS % CC::COLS == 0 && N % TC::COLS == 0;
     } else {
@@ -122,7 +126,7 @@ template <class RR, int V> constexpr bool tma_col_ok() {
 // at its default tile with the other register budget, 11 / 12 the per-pair-barrier passes. A variant index of PassOps::col_step is a position in the
 // list of the kinds valid here (kind 0 always first).
 struct KindList {
-    int kind[13];
+    int kind[14];
     int n;
 };
 template <class RR> constexpr KindList col_kinds() {
@@ -139,6 +143,7 @@ template <class RR> constexpr KindList col_kinds() {
     if (tma_col_ok<RR, 7>()) k.kind[k.n++] = 10;
     if (tmx_col_ok<RR, 11>()) k.kind[k.n++] = 11;
     if (tmx_col_ok<RR, 12>()) k.kind[k.n++] = 12;
+    if (tmx_col_ok<RR, 13>()) k.kind[k.n++] = 13;
     return k;
 }
 template <class RR> constexpr int tma_col_variants() { return col_kinds<RR>().n; }
@@ -175,6 +180,9 @@ std::string col_variant_name(int v) {
     if (kind == 10)
         return "persistent, TMA loads and stores, " + cols(kPairC / 2) + ", " + stages(TmaVariant<7>::Cfg<N>::STAGES) +
                ", twiddles from L1, 1 block per SM";
+    if (kind == 13)
+        return "persistent, per-pair barriers, TMA loads and stores, 16-element FFT plan (radix 16 first; rounds "
+               "differently), " + cols(TmxVariant<13>::Cfg<N>::COLS) + ", 3 stages, 1 block per SM";
     if (kind == 11 || kind == 12) {
         constexpr int c11 = TmxVariant<11>::Cfg<N>::COLS, c12 = TmxVariant<12>::Cfg<N>::COLS;
         return "persistent, per-pair barriers, TMA loads and stores, " + cols(kind == 11 ? c11 : c12) +
@@ -229,7 +237,7 @@ bool tma_col_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw,
 template <class RR, int V> void tmx_col_attrs() {
     if constexpr (tmx_col_ok<RR, V>()) {
         using TC = typename TmxVariant<V>::template Cfg<N>;
-        set_smem(k_col_step_tmx<N, TC::COLS, TC::STAGES, TC::MINB>, TC::smem());
+        set_smem(k_col_step_tmx<N, TC::COLS, TC::STAGES, TC::MINB, typename TC::P>, TC::smem());
     }
 }
 template <class RR, int V>
@@ -246,8 +254,10 @@ bool tmx_col_step(cudaStream_t s, int batch, cplx<RR> *wave, const cplx<RR> *tw,
         const CUtensorMap tm =
             wave_tensor_map(wave, 2ull * N, (unsigned long long)batch * N, TC::BOX_FLOATS, TC::BOX_ROWS, TC::SWIZZLE);
         const int grid = (int)std::min<long long>(items, (long long)TC::MINB * sm_count());
-        k_col_step_tmx<N, TC::COLS, TC::STAGES, TC::MINB><<<grid, TC::THREADS, TC::smem(), s>>>(tm, tw, pt, b, lo, lo + hi,
-                                                                                              (int)items, pt.err);
+        // the 16-element plan's twiddles follow the other plans' tables (Ctx::twiddles, entries [2N, 3N))
+        const cplx<RR> *twp = TC::P::E == 16 ? tw + 2 * N : tw;
+        k_col_step_tmx<N, TC::COLS, TC::STAGES, TC::MINB, typename TC::P><<<grid, TC::THREADS, TC::smem(), s>>>(
+            tm, twp, pt, b, lo, lo + hi, (int)items, pt.err);
         MS_CUDA(cudaGetLastError());
         return true;
     } else {
@@ -388,6 +398,7 @@ void ensure_attrs() {
     tma_col_attrs<R, 7>();
     tmx_col_attrs<R, 11>();
     tmx_col_attrs<R, 12>();
+    tmx_col_attrs<R, 13>();
     rowpair_attrs<R>();
     set_smem(k_col_step<R, N, COL_STEP_DET>, CC::smem());
     set_smem(k_col_step<R, N, COL_DET_ONLY>, CC::smem());
@@ -494,6 +505,7 @@ void col_step(cudaStream_t s, cplx<R> *wave, int batch, const cplx<R> *tw, PropT
         if (kind == 10 && tma_col_step<R, 7>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 11 && tmx_col_step<R, 11>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 12 && tmx_col_step<R, 12>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
+        if (kind == 13 && tmx_col_step<R, 13>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 3 && pair_step<R, kPairC / 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (kind == 4 && pair_step<R, kPairC * 2>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;
         if (pair_step<R, kPairC>(s, batch, wave, tw, pt, b, tiles_lo, tiles_hi)) return;

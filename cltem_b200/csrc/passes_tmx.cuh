@@ -1,4 +1,5 @@
-// passes_tmx.cuh — persistent column pass with one barrier domain per column pair (FP32, 2^k and 3·2^k plans).
+// passes_tmx.cuh — persistent column pass with one barrier domain per column pair (FP32, 2^k and 3·2^k plans,
+// and the 16-element plans at 1024 and 2048, whose results round differently from the 8-element plan's).
 //
 // Same arithmetic per element, in the same order, as k_col_step_pair / k_col_step_tma (column FFT of two
 // adjacent columns a thread, times the propagator inside its cut and the scale b, inverse column FFT), so
@@ -36,13 +37,17 @@ template <int PAIRS> __host__ __device__ constexpr int tmx_swz(int row) {
 }
 // 16-byte slot of logical row i of pair 0 in the copy engine's layout / in the exchange layout
 template <int PAIRS> __host__ __device__ constexpr int tmx_tlay(int i) { return PAIRS * i ^ tmx_swz<PAIRS>(i); }
-template <int N> __host__ __device__ constexpr int tmx_h(int q) { return is_pow2(N) ? q : (q & 5) ^ ((q & 2) * 3); }
-template <int N, int PAIRS> __host__ __device__ constexpr int tmx_lay(int i) {
-    return tmx_tlay<PAIRS>(i ^ tmx_h<N>((i >> 3) & 7));
+// the exchange's row permutation g of a plan: i ^ ((i >> 3) & 7) for the 8-element 2^k plans, i ^ ((i >> 4) & 7)
+// for the 16-element plans (their radix-16 writes at span 1 put the rows of 8 consecutive threads 16 apart), and
+// i ^ H((i >> 3) & 7) with H mapping bits (1, 2, 4) to (1, 6, 4) for the 3·2^k plans
+template <class PL> __host__ __device__ constexpr int tmx_g(int i) {
+    return PL::E == 16 ? i ^ ((i >> 4) & 7)
+                       : (PL::pow2 ? i ^ ((i >> 3) & 7) : i ^ (((i >> 3) & 5) ^ (((i >> 3) & 2) * 3)));
 }
+template <class PL, int PAIRS> __host__ __device__ constexpr int tmx_lay(int i) { return tmx_tlay<PAIRS>(tmx_g<PL>(i)); }
 // the exchange write position of butterfly j's output 0 at stage S (fft.cuh: (j / Ns) Ns RAD + j mod Ns)
-template <int N, int S> __host__ __device__ constexpr int tmx_wrow(int j) {
-    return (j / Plan<N>::ns(S)) * Plan<N>::ns(S) * Plan<N>::radix(S) + j % Plan<N>::ns(S);
+template <class PL, int S> __host__ __device__ constexpr int tmx_wrow(int j) {
+    return (j / PL::ns(S)) * PL::ns(S) * PL::radix(S) + j % PL::ns(S);
 }
 // every bit a per-thread base f(t) ^ p can have (t < NT, p < PAIRS)
 template <int PAIRS, int NT> __host__ __device__ constexpr int tmx_mask_tlay() {
@@ -50,40 +55,43 @@ template <int PAIRS, int NT> __host__ __device__ constexpr int tmx_mask_tlay() {
     for (int b = 1; b < NT; b <<= 1) m |= tmx_tlay<PAIRS>(b);
     return m;
 }
-template <int N, int PAIRS, int NT> __host__ __device__ constexpr int tmx_mask_lay() {
+template <class PL, int PAIRS> __host__ __device__ constexpr int tmx_mask_lay() {
     int m = PAIRS - 1;
-    for (int b = 1; b < NT; b <<= 1) m |= tmx_lay<N, PAIRS>(b);
+    for (int b = 1; b < PL::NT; b <<= 1) m |= tmx_lay<PL, PAIRS>(b);
     return m;
 }
-template <int N, int PAIRS, int S> __host__ __device__ constexpr int tmx_mask_w() {
+template <class PL, int PAIRS, int S> __host__ __device__ constexpr int tmx_mask_w() {
     int m = PAIRS - 1;
-    for (int b = 1; b < Plan<N>::NT; b <<= 1) m |= tmx_lay<N, PAIRS>(tmx_wrow<N, S>(b));
+    for (int b = 1; b < PL::NT; b <<= 1) m |= tmx_lay<PL, PAIRS>(tmx_wrow<PL, S>(b));
     return m;
 }
-// the plans whose stages that write to shared memory all have power-of-two spans: every 2^k plan (E = 8) and
-// the 3·2^k plans, whose radix-12 stage comes last
-template <int N> __host__ __device__ constexpr bool tmx_plan_ok() {
-    return (is_pow2(N) && Plan<N>::E == 8) || (!is_pow2(N) && Plan<N>::E == 12 && Plan<N>::radix(Plan<N>::nstages - 1) == 12);
+// the plans whose stages that write to shared memory all have power-of-two spans: the 2^k plans (8 or 16
+// elements) and the 3·2^k plans, whose radix-12 stage comes last
+template <class PL> __host__ __device__ constexpr bool tmx_plan_ok() {
+    return (PL::pow2 && (PL::E == 8 || PL::E == 16)) || (!PL::pow2 && PL::E == 12 && PL::radix(PL::nstages - 1) == 12);
 }
 // base combined with the constant c: the two share no bit when (c & mask) == 0, and then the sum is the XOR
 __device__ __forceinline__ int tmx_at(int base, int c, int mask) { return (c & mask) == 0 ? base + c : base ^ c; }
 
 // twiddles a thread holds: stage S >= 1 keeps NB (RAD - 1) of them, in stage order, up to stage
-// tmx_tw_reg_stages; the later stages read theirs from a copy of the plan's table in shared memory. At 1024
-// (ptxas, 128 registers a thread) all three stages' twiddles in registers spill 120 bytes a thread, two stages'
-// 88 bytes, one stage's none; at the other grids every stage's are kept (2048 spills either way, and its
-// stages leave no room for the table).
-template <int N> __host__ __device__ constexpr int tmx_tw_reg_stages() { return N == 1024 ? 1 : Plan<N>::nstages - 1; }
-template <int N> __host__ __device__ constexpr bool tmx_tw_staged() { return tmx_tw_reg_stages<N>() < Plan<N>::nstages - 1; }
-template <int N> __host__ __device__ constexpr int tmx_tw_off(int S) {
+// tmx_tw_reg_stages; the later stages read theirs from a copy of the plan's table in shared memory. At 1024 with
+// the 8-element plan (ptxas, 128 registers a thread) all three stages' twiddles in registers spill 120 bytes a
+// thread, two stages' 88 bytes, one stage's none; at the other grids and plans every stage's are kept (2048
+// spills either way, and its stages leave no room for the table).
+template <int N, class PL> __host__ __device__ constexpr int tmx_tw_reg_stages() {
+    return (N == 1024 && PL::E == 8) ? 1 : PL::nstages - 1;
+}
+template <int N, class PL> __host__ __device__ constexpr bool tmx_tw_staged() { return tmx_tw_reg_stages<N, PL>() < PL::nstages - 1; }
+template <int N, class PL> __host__ __device__ constexpr int tmx_tw_off(int S) {
     int o = 0;
-    for (int s = 1; s < S && s <= tmx_tw_reg_stages<N>(); s++) o += (Plan<N>::E / Plan<N>::radix(s)) * (Plan<N>::radix(s) - 1);
+    for (int s = 1; s < S && s <= tmx_tw_reg_stages<N, PL>(); s++) o += (PL::E / PL::radix(s)) * (PL::radix(s) - 1);
     return o;
 }
-template <int N> constexpr int tmx_tw_count() { return tmx_tw_off<N>(Plan<N>::nstages); }
+template <int N, class PL> constexpr int tmx_tw_count() { return tmx_tw_off<N, PL>(PL::nstages); }
 
-template <int N, int COLS_, int STAGES_, int MINB_ = 1> struct TmxColCfg {
-    using P = Plan<N>;
+// PL: the FFT plan (Plan<N>, or Plan16<N> at 1024 and 2048)
+template <int N, int COLS_, int STAGES_, int MINB_ = 1, class PL = Plan<N>> struct TmxColCfg {
+    using P = PL;
     static constexpr int COLS = COLS_;
     static constexpr int PAIRS = COLS / 2;
     static constexpr int NT = P::NT;
@@ -94,14 +102,14 @@ template <int N, int COLS_, int STAGES_, int MINB_ = 1> struct TmxColCfg {
     static constexpr int BOX_ROWS = tma_box_rows(N);
     static constexpr int LOADS = N / BOX_ROWS;
     static constexpr int BOX_FLOATS = 2 * COLS;
-    static constexpr int TWR = tmx_tw_count<N>();
+    static constexpr int TWR = tmx_tw_count<N, PL>();
     // 1024-byte alignment slack (the swizzle atom), stages, the propagator's row tables (py and its errors),
     // two mbarriers per stage
     // (and, where some stages read their twiddles from shared memory, the plan's table)
     static constexpr size_t smem() {
-        return 1024 + (size_t)STAGES * STAGE_BYTES + sizeof(float2) * (tmx_tw_staged<N>() ? 3 : 2) * N + 16 * STAGES;
+        return 1024 + (size_t)STAGES * STAGE_BYTES + sizeof(float2) * (tmx_tw_staged<N, PL>() ? 3 : 2) * N + 16 * STAGES;
     }
-    static constexpr bool ok = tmx_plan_ok<N>() && is_pow2(P::NT) && (PAIRS == 1 || PAIRS == 2 || PAIRS == 4 || PAIRS == 8) &&
+    static constexpr bool ok = tmx_plan_ok<PL>() && is_pow2(P::NT) && (PAIRS == 1 || PAIRS == 2 || PAIRS == 4 || PAIRS == 8) &&
                                NT % 32 == 0 && THREADS <= 1024 && PAIRS <= 15 && STAGES >= 3 && N % BOX_ROWS == 0 &&
                                BOX_ROWS >= 16 && smem() <= kMaxBlockSmem && MINB * (smem() + 1024) <= 228 * 1024 &&
                                (size_t)MINB * THREADS * 128 <= 65536;
@@ -111,26 +119,26 @@ template <int N, int COLS_, int STAGES_, int MINB_ = 1> struct TmxColCfg {
 
 // Stage S of the pair FFT (fft_pair.cuh's fftp_stages with the layouts above and register twiddles).
 // rbase: tmx_lay(t) ^ p; wb[S]: tmx_lay(tmx_wrow<N, S>(t)) ^ p.
-template <int N, int PAIRS, int SIGN, int S, int TWR>
-__device__ __forceinline__ void tmx_stages(float2 (&va)[Plan<N>::E], float2 (&vb)[Plan<N>::E], float4 *sm, int rbase,
-                                           const int (&wb)[Plan<N>::nstages], const float2 (&twr)[TWR],
+template <int N, int PAIRS, int SIGN, int S, int TWR, class PL>
+__device__ __forceinline__ void tmx_stages(float2 (&va)[PL::E], float2 (&vb)[PL::E], float4 *sm, int rbase,
+                                           const int (&wb)[PL::nstages], const float2 (&twr)[TWR],
                                            const float2 *s_tw, int t, NamedBar bar) {
-    using P = Plan<N>;
+    using P = PL;
     constexpr int E = P::E, NT = P::NT;
     constexpr int RAD = P::radix(S);
     constexpr int Ns = P::ns(S);
     constexpr int NB = E / RAD;
     constexpr bool last = (S == P::nstages - 1);
-    constexpr int TWO = tmx_tw_off<N>(S > 0 ? S : 1);
-    constexpr bool TWREG = S <= tmx_tw_reg_stages<N>();
-    constexpr int TWB = plan_tw_index(N, S > 0 ? S : 1, 0, 1);
+    constexpr int TWO = tmx_tw_off<N, PL>(S > 0 ? S : 1);
+    constexpr bool TWREG = S <= tmx_tw_reg_stages<N, PL>();
+    constexpr int TWB = P::tw_base(S > 0 ? S : 1);
     if constexpr (S > 0) {
-        constexpr int RM = tmx_mask_lay<N, PAIRS, NT>();
+        constexpr int RM = tmx_mask_lay<PL, PAIRS>();
 #pragma unroll
         for (int b = 0; b < NB; b++) {
 #pragma unroll
             for (int r = 0; r < RAD; r++) {
-                const float4 q = sm[tmx_at(rbase, tmx_lay<N, PAIRS>(b * NT + r * (N / RAD)), RM)];
+                const float4 q = sm[tmx_at(rbase, tmx_lay<PL, PAIRS>(b * NT + r * (N / RAD)), RM)];
                 va[b + r * NB] = make_float2(q.x, q.y);
                 vb[b + r * NB] = make_float2(q.z, q.w);
             }
@@ -166,39 +174,40 @@ __device__ __forceinline__ void tmx_stages(float2 (&va)[Plan<N>::E], float2 (&vb
 #pragma unroll
         for (int i = 0; i < E; i++) { va[i] = oa[i]; vb[i] = ob[i]; }
     } else {
-        constexpr int WM = tmx_mask_w<N, PAIRS, S>();
+        constexpr int WM = tmx_mask_w<PL, PAIRS, S>();
         bar();   // the pair's reads of the previous layout are done
 #pragma unroll
         for (int b = 0; b < NB; b++) {
 #pragma unroll
             for (int m = 0; m < RAD; m++)
-                sm[tmx_at(wb[S], tmx_lay<N, PAIRS>(tmx_wrow<N, S>(b * NT) | (m * Ns)), WM)] =
+                sm[tmx_at(wb[S], tmx_lay<PL, PAIRS>(tmx_wrow<PL, S>(b * NT) | (m * Ns)), WM)] =
                     make_float4(oa[b + m * NB].x, oa[b + m * NB].y, ob[b + m * NB].x, ob[b + m * NB].y);
         }
         bar();
-        tmx_stages<N, PAIRS, SIGN, S + 1, TWR>(va, vb, sm, rbase, wb, twr, s_tw, t, bar);
+        tmx_stages<N, PAIRS, SIGN, S + 1, TWR, PL>(va, vb, sm, rbase, wb, twr, s_tw, t, bar);
     }
 }
 
 // thread t's twiddles: stage S, butterfly j = t + b NT, k = j mod Ns, entries r = 1..RAD-1 of the packed table
-template <int N, int S, int TWR> __device__ __forceinline__ void tmx_load_twiddles(float2 (&twr)[TWR], const float2 *twg, int t) {
-    if constexpr (S <= tmx_tw_reg_stages<N>()) {
-        using P = Plan<N>;
+template <int N, int S, int TWR, class PL>
+__device__ __forceinline__ void tmx_load_twiddles(float2 (&twr)[TWR], const float2 *twg, int t) {
+    if constexpr (S <= tmx_tw_reg_stages<N, PL>()) {
+        using P = PL;
         constexpr int RAD = P::radix(S), Ns = P::ns(S), NB = P::E / RAD, NT = P::NT;
-        constexpr int TWB = plan_tw_index(N, S, 0, 1);
+        constexpr int TWB = P::tw_base(S);
 #pragma unroll
         for (int b = 0; b < NB; b++) {
             const int k = (t + b * NT) % Ns;
 #pragma unroll
-            for (int r = 1; r < RAD; r++) twr[tmx_tw_off<N>(S) + b * (RAD - 1) + (r - 1)] = twg[TWB + k * (RAD - 1) + (r - 1)];
+            for (int r = 1; r < RAD; r++) twr[tmx_tw_off<N, PL>(S) + b * (RAD - 1) + (r - 1)] = twg[TWB + k * (RAD - 1) + (r - 1)];
         }
-        tmx_load_twiddles<N, S + 1, TWR>(twr, twg, t);
+        tmx_load_twiddles<N, S + 1, TWR, PL>(twr, twg, t);
     }
 }
-template <int N, int PAIRS, int S> __device__ __forceinline__ void tmx_write_bases(int (&wb)[Plan<N>::nstages], int t, int p) {
-    if constexpr (S < Plan<N>::nstages) {
-        wb[S] = tmx_lay<N, PAIRS>(tmx_wrow<N, S>(t)) ^ p;
-        tmx_write_bases<N, PAIRS, S + 1>(wb, t, p);
+template <int PAIRS, int S, class PL> __device__ __forceinline__ void tmx_write_bases(int (&wb)[PL::nstages], int t, int p) {
+    if constexpr (S < PL::nstages) {
+        wb[S] = tmx_lay<PL, PAIRS>(tmx_wrow<PL, S>(t)) ^ p;
+        tmx_write_bases<PAIRS, S + 1, PL>(wb, t, p);
     }
 }
 
@@ -209,19 +218,19 @@ template <int N, int PAIRS, int S> __device__ __forceinline__ void tmx_write_bas
 // that stage's store has read it). err: the error word (tma.cuh StepError), written only when a wait is
 // abandoned; a producer that gives up stops loading, and the consumers then give up at the first item that
 // was never loaded (no pair is left waiting at a barrier for a warp that left).
-template <int N, int COLS, int STAGES, int MINB>
-__global__ void __launch_bounds__(TmxColCfg<N, COLS, STAGES, MINB>::THREADS, MINB)
+template <int N, int COLS, int STAGES, int MINB, class PL = Plan<N>>
+__global__ void __launch_bounds__(TmxColCfg<N, COLS, STAGES, MINB, PL>::THREADS, MINB)
 k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict__ twg, PropTables<float> pt, float bscale,
                int tiles_lo, int n_active, int n_items, int *err) {
-    using TC = TmxColCfg<N, COLS, STAGES, MINB>;
-    using P = Plan<N>;
+    using TC = TmxColCfg<N, COLS, STAGES, MINB, PL>;
+    using P = PL;
     constexpr int PAIRS = TC::PAIRS, E = P::E, NT = P::NT, K = TC::STAGES, THREADS = TC::THREADS;
     extern __shared__ unsigned char smraw[];
     unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
     float4 *stages = reinterpret_cast<float4 *>(base);
     float2 *s_py = reinterpret_cast<float2 *>(base + (size_t)K * TC::STAGE_BYTES), *s_pye = s_py + N;
     float2 *s_tw = s_pye + N;   // the plan's table, where some stages read their twiddles from shared memory
-    uint64_t *full = reinterpret_cast<uint64_t *>(s_tw + (tmx_tw_staged<N>() ? N : 0));
+    uint64_t *full = reinterpret_cast<uint64_t *>(s_tw + (tmx_tw_staged<N, PL>() ? N : 0));
     uint64_t *empty = full + K;
     const int tid = threadIdx.x;
     const int p = tid / NT, t = tid % NT;
@@ -235,13 +244,13 @@ k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict_
     for (int i = tid; i < N; i += THREADS) {
         s_py[i] = pt.py[i];
         s_pye[i] = pt.pye[i];
-        if constexpr (tmx_tw_staged<N>()) s_tw[i] = twg[i];
+        if constexpr (tmx_tw_staged<N, PL>()) s_tw[i] = twg[i];
     }
     float2 twr[TC::TWR];
-    tmx_load_twiddles<N, 1, TC::TWR>(twr, twg, t);
+    tmx_load_twiddles<N, 1, TC::TWR, PL>(twr, twg, t);
     int wb[P::nstages];
-    tmx_write_bases<N, PAIRS, 0>(wb, t, p);
-    const int rbase = tmx_lay<N, PAIRS>(t) ^ p, tbase = tmx_tlay<PAIRS>(t) ^ p;
+    tmx_write_bases<PAIRS, 0, PL>(wb, t, p);
+    const int rbase = tmx_lay<PL, PAIRS>(t) ^ p, tbase = tmx_tlay<PAIRS>(t) ^ p;
     constexpr int TM = tmx_mask_tlay<PAIRS, NT>();
     const NamedBar bar{1 + p, NT};
     __syncthreads();
@@ -308,7 +317,7 @@ k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict_
             va[m] = make_float2(q.x, q.y);
             vb[m] = make_float2(q.z, q.w);
         }
-        tmx_stages<N, PAIRS, -1, 0, TC::TWR>(va, vb, sm, rbase, wb, twr, s_tw, t, bar);
+        tmx_stages<N, PAIRS, -1, 0, TC::TWR, PL>(va, vb, sm, rbase, wb, twr, s_tw, t, bar);
 #pragma unroll
         for (int m = 0; m < E; m++) {
             const int y = t + m * NT;
@@ -316,7 +325,7 @@ k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict_
             va[m] = (y < ca.x || y >= ca.y) ? cscale(prop_mul<float>(va[m], pxa, py, exa, ey), bscale) : mk<float>(0, 0);
             vb[m] = (y < cb.x || y >= cb.y) ? cscale(prop_mul<float>(vb[m], pxb, py, exb, ey), bscale) : mk<float>(0, 0);
         }
-        tmx_stages<N, PAIRS, +1, 0, TC::TWR>(va, vb, sm, rbase, wb, twr, s_tw, t, bar);
+        tmx_stages<N, PAIRS, +1, 0, TC::TWR, PL>(va, vb, sm, rbase, wb, twr, s_tw, t, bar);
         bar();   // the pair's last exchange reads are done: the stage takes its results
 #pragma unroll
         for (int m = 0; m < E; m++)
