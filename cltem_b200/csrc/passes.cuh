@@ -565,19 +565,22 @@ template <int N> using PairStepCfg = PairCfg<N, pair_mult<N>() * ColCfg<N, float
 template <int N> constexpr bool pair_columns() { return PairStepCfg<N>::ok; }
 
 // The propagator and scale b on the two columns x, x + 1 a thread holds (elements t + m NT), zero outside the
-// cut (the row band of PropTables::ycut): shared by the two-column step kernels.
+// cut (the row band of PropTables::ycut): shared by the two-column step kernels. b is folded into the column
+// factors once (b px), which saves a scaling of every element; b = 1/N is a power of two on the 2^k grids,
+// so there the products equal those of scaling afterwards bit for bit (the correction (1 + ex + ey) is relative).
+__device__ __forceinline__ float2 prop_col(const PropTables<float> &pt, int x, float bscale) { return cscale(pt.px[x], bscale); }
 template <int N>
 __device__ __forceinline__ void prop_pair(float2 (&va)[Plan<N>::E], float2 (&vb)[Plan<N>::E], const PropTables<float> &pt,
                                           int x, int t, float bscale) {
     constexpr int E = Plan<N>::E, NT = Plan<N>::NT;
-    const float2 pxa = pt.px[x], pxb = pt.px[x + 1], exa = pt.pxe[x], exb = pt.pxe[x + 1];
+    const float2 pxa = prop_col(pt, x, bscale), pxb = prop_col(pt, x + 1, bscale), exa = pt.pxe[x], exb = pt.pxe[x + 1];
     const int2 ca = pt.ycut[x], cb = pt.ycut[x + 1];
 #pragma unroll
     for (int m = 0; m < E; m++) {
         const int y = t + m * NT;
         const float2 py = pt.py[y], ey = pt.pye[y];
-        va[m] = (y < ca.x || y >= ca.y) ? cscale(prop_mul<float>(va[m], pxa, py, exa, ey), bscale) : mk<float>(0, 0);
-        vb[m] = (y < cb.x || y >= cb.y) ? cscale(prop_mul<float>(vb[m], pxb, py, exb, ey), bscale) : mk<float>(0, 0);
+        va[m] = (y < ca.x || y >= ca.y) ? prop_mul<float>(va[m], pxa, py, exa, ey) : mk<float>(0, 0);
+        vb[m] = (y < cb.x || y >= cb.y) ? prop_mul<float>(vb[m], pxb, py, exb, ey) : mk<float>(0, 0);
     }
 }
 

@@ -306,7 +306,7 @@ k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict_
         const int w = item / n_active, j = item - w * n_active;
         const int tile = j < tiles_lo ? j : N / COLS - (n_active - j);
         const int x = tile * COLS + 2 * p;
-        const float2 pxa = pt.px[x], pxb = pt.px[x + 1], exa = pt.pxe[x], exb = pt.pxe[x + 1];
+        const float2 pxa = prop_col(pt, x, bscale), pxb = prop_col(pt, x + 1, bscale), exa = pt.pxe[x], exb = pt.pxe[x + 1];
         const int2 ca = pt.ycut[x], cb = pt.ycut[x + 1];
         if (!mbar_wait(&full[s], (unsigned)(k / K) & 1, err, STEP_WAIT_FULL)) break;
         float4 *sm = stages + (size_t)s * (TC::STAGE_BYTES / 16);
@@ -322,8 +322,8 @@ k_col_step_tmx(const __grid_constant__ CUtensorMap tm, const float2 *__restrict_
         for (int m = 0; m < E; m++) {
             const int y = t + m * NT;
             const float2 py = s_py[y], ey = s_pye[y];
-            va[m] = (y < ca.x || y >= ca.y) ? cscale(prop_mul<float>(va[m], pxa, py, exa, ey), bscale) : mk<float>(0, 0);
-            vb[m] = (y < cb.x || y >= cb.y) ? cscale(prop_mul<float>(vb[m], pxb, py, exb, ey), bscale) : mk<float>(0, 0);
+            va[m] = (y < ca.x || y >= ca.y) ? prop_mul<float>(va[m], pxa, py, exa, ey) : mk<float>(0, 0);
+            vb[m] = (y < cb.x || y >= cb.y) ? prop_mul<float>(vb[m], pxb, py, exb, ey) : mk<float>(0, 0);
         }
         tmx_stages<N, PAIRS, +1, 0, TC::TWR, PL>(va, vb, sm, rbase, wb, twr, s_tw, t, bar);
         bar();   // the pair's last exchange reads are done: the stage takes its results
