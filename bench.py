@@ -42,7 +42,7 @@ WORKLOAD = "stem_adf_perovskite_10x10x20_512x512_64x64probes_40slices_phonon_u0.
 # dram__bytes_write.sum over one launch of the timed configuration, divided by its waves), measured at this
 # workload's autotuned batch of 2048 waves on this build's kernels (plain row pass, per-pair-barrier persistent
 # column pass); a kernel change needs a new capture
-NCU_DRAM_BYTES_PER_WAVE = {"row_step": (2954973952 + 2895340288) / 2048, "col_step": (3023578880 + 2895932928) / 2048}
+NCU_DRAM_BYTES_PER_WAVE = {"row_step": (2954996480 + 2893525504) / 2048, "col_step": (3021943552 + 2895444480) / 2048}
 
 
 def parse():
