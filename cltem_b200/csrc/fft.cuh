@@ -214,12 +214,16 @@ struct RowAddr {
     static constexpr int size(int n) { return n; }
 };
 // Column tiles: element i of column c at s(i)*COLS + c, threads of one row consecutive. The row swizzle
-// s(i) = i ^ ((i >> 3) & (RP - 1)), RP = rows per 128-byte wavefront, separates the rows a wavefront's
-// threads touch in the stride-8 stage writes.
-template <int COLS, int ELEM_BYTES> struct ColAddr {
+// s(i) = i ^ ((i >> SHIFT) & (RP - 1)), RP = rows per 128-byte wavefront, separates the rows a wavefront's
+// threads touch in the first stage's writes (rows R t + m for radix R = 2^SHIFT: col_swz_shift).
+template <int COLS, int ELEM_BYTES, int SHIFT = 3> struct ColAddr {
     static constexpr int RP = (128 / (COLS * ELEM_BYTES)) > 0 ? (128 / (COLS * ELEM_BYTES)) : 1;
-    __device__ __forceinline__ int operator()(int i) const { return (i ^ ((i >> 3) & (RP - 1))) * COLS; }
+    __device__ __forceinline__ int operator()(int i) const { return (i ^ ((i >> SHIFT) & (RP - 1))) * COLS; }
 };
+// the swizzle shift of a plan: log2 of its first radix (8 for the 2^k plans, 4 for the 3·2^k plans, whose
+// radix-12 stage comes last); with it every stage's reads and writes of ColAddr tiles of 1 to 8 columns meet
+// distinct banks (checked on the host for 384 to 3072)
+template <int N> __host__ __device__ constexpr int col_swz_shift() { return Plan<N>::pow2 ? 3 : 2; }
 
 // ---- synchronisation of the threads sharing a transform's shared memory ---------------------------
 struct BlockSync {

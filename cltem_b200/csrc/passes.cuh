@@ -147,7 +147,7 @@ template <class R, int N, int SIGN>
 __device__ __forceinline__ void col_transform(cplx<R> (&v)[ColCfg<N, R>::P::E], cplx<R> *sm, int t, const cplx<R> *tw) {
     using CC = ColCfg<N, R>;
     if constexpr (CC::WIDE) fft_wide<R, N, SIGN>(v, sm, WideColAddr<CC::P::E, CC::COLS>(), t, tw, BlockSync());
-    else fft<R, N, SIGN>(v, sm, ColAddr<CC::COLS, (int)sizeof(cplx<R>)>(), t, tw);
+    else fft<R, N, SIGN>(v, sm, ColAddr<CC::COLS, (int)sizeof(cplx<R>), col_swz_shift<N>()>(), t, tw);
 }
 
 template <class R>
@@ -393,13 +393,13 @@ k_row_step_pair(float2 *__restrict__ wave, const float2 *__restrict__ trans, con
         vb[m] = in ? rb[x] : mk<float>(0, 0);
     }
     __syncthreads();
-    fft_pair<N, +1>(va, vb, sm, ColAddr<1, 16>(), t, tw);
+    fft_pair<N, +1>(va, vb, sm, ColAddr<1, 16, col_swz_shift<N>()>(), t, tw);
 #pragma unroll
     for (int m = 0; m < E; m++) {
         va[m] = cscale(cmul(va[m], ta[t + m * NT]), a);
         vb[m] = cscale(cmul(vb[m], tb[t + m * NT]), a);
     }
-    fft_pair<N, -1>(va, vb, sm, ColAddr<1, 16>(), t, tw);
+    fft_pair<N, -1>(va, vb, sm, ColAddr<1, 16, col_swz_shift<N>()>(), t, tw);
 #pragma unroll
     for (int m = 0; m < E; m++) {
         const int x = t + m * NT;
@@ -607,9 +607,9 @@ k_col_step_pair(float2 *__restrict__ wave, const float2 *__restrict__ twg, PropT
         vb[m] = make_float2(q.z, q.w);
     }
     __syncthreads();
-    fft_pair<N, -1>(va, vb, sm, ColAddr<PAIRS, 16>(), t, tw);
+    fft_pair<N, -1>(va, vb, sm, ColAddr<PAIRS, 16, col_swz_shift<N>()>(), t, tw);
     prop_pair<N>(va, vb, pt, x, t, bscale);
-    fft_pair<N, +1>(va, vb, sm, ColAddr<PAIRS, 16>(), t, tw);
+    fft_pair<N, +1>(va, vb, sm, ColAddr<PAIRS, 16, col_swz_shift<N>()>(), t, tw);
 #pragma unroll
     for (int m = 0; m < E; m++)
         base[(size_t)(t + m * NT) * (N / 2)] = make_float4(va[m].x, va[m].y, vb[m].x, vb[m].y);

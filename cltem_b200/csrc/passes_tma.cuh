@@ -173,9 +173,9 @@ k_col_step_tma(const __grid_constant__ CUtensorMap tm, float2 *__restrict__ wave
             va[m] = make_float2(q.x, q.y);
             vb[m] = make_float2(q.z, q.w);
         }
-        fft_pair<N, -1>(va, vb, sm + p, ColAddr<PAIRS, 16>(), t, tw, cbar);
+        fft_pair<N, -1>(va, vb, sm + p, ColAddr<PAIRS, 16, col_swz_shift<N>()>(), t, tw, cbar);
         prop_pair<N>(va, vb, spt, x, t, bscale);
-        fft_pair<N, +1>(va, vb, sm + p, ColAddr<PAIRS, 16>(), t, tw, cbar);
+        fft_pair<N, +1>(va, vb, sm + p, ColAddr<PAIRS, 16, col_swz_shift<N>()>(), t, tw, cbar);
         if constexpr (TS) {
             // every consumer has read its last exchange values: the stage takes the results, which the
             // producer's TMA store then reads (the writes are ordered before it by the proxy fence and the
