@@ -216,14 +216,32 @@ template <class R, int N, int THREADS, int OTHER> constexpr int fp64_step_minb()
     return (sizeof(R) == 8 && THREADS == 256 && Plan<N>::E == 8) ? 3
          : (sizeof(R) == 8 && Plan<N>::E == 12 && THREADS * 128 < 65536) ? 65536 / (THREADS * 128) : OTHER;
 }
-// Row step with staged transmission rows (TST): the block's ROWS transmission rows are contiguous in HBM, and one
-// thread asks the copy engine for all of them (cp.async.bulk into shared memory, completion on an mbarrier) as
-// the block starts, so they arrive while the inverse row FFT runs. Without TST every thread loads its T
-// elements only after that FFT and waits for them there. The staged rows sit after the block's twiddles and
-// exchange rows (16-byte aligned), the mbarrier after them.
+// Row step with staged transmission rows (TST): the block's transmission rows are contiguous in HBM, and one
+// thread asks the copy engine for the first row_ts_rows of them (cp.async.bulk into shared memory, completion
+// on an mbarrier) as the block starts, so they arrive while the inverse row FFT runs. Without TST (and in a
+// block's rows beyond those) every thread loads its T elements only after that FFT and waits for them there.
+// The staged rows sit after the block's twiddles and exchange rows (16-byte aligned), the mbarrier after them.
 template <int N, class R> constexpr size_t row_tstage_off() { return (RowCfg<N, R>::smem() + 15) / 16 * 16; }
+// Rows of a block that are staged (the first TSR; the rest load T themselves): with 4 or more rows a block,
+// as many as leave the plain kernel's blocks per SM (128 registers a thread, its shared memory); with fewer,
+// all of them. Measured per probe·slice, row pass: 1024² with 4 of 8 rows staged (2 blocks an SM) 4.13 →
+// 3.94 µs, where all 8 (1 block an SM) were slower than none; 384², 768² all rows fit at the plain kernel's
+// 4 blocks; 1536², 3072², 8192² (1-2 rows a block) staging all rows wins although it costs blocks.
+template <int N, class R> constexpr int row_ts_blocks(int r) {
+    return (int)((228 * 1024) / (row_tstage_off<N, R>() + sizeof(cplx<R>) * (size_t)r * N + 8 + 1024));
+}
+template <int N, class R> constexpr int row_ts_rows() {
+    constexpr int ROWS = RowCfg<N, R>::ROWS;
+    constexpr int by_regs = 65536 / (RowCfg<N, R>::THREADS * 128);
+    constexpr int by_smem = (int)((228 * 1024) / (RowCfg<N, R>::smem() + 1024));
+    constexpr int plain = by_regs < by_smem ? by_regs : by_smem;
+    if (ROWS < 4) return ROWS;
+    for (int r = ROWS; r >= 1; r--)
+        if (row_ts_blocks<N, R>(r) >= plain) return r;
+    return ROWS;
+}
 template <int N, class R> constexpr size_t row_ts_smem() {
-    return row_tstage_off<N, R>() + sizeof(cplx<R>) * (size_t)RowCfg<N, R>::ROWS * N + 8;
+    return row_tstage_off<N, R>() + sizeof(cplx<R>) * (size_t)row_ts_rows<N, R>() * N + 8;
 }
 // the row step's body, shared by k_row_step and its FP64 3-blocks-per-SM build k_row_step_d; err (TST only):
 // the error word a wait that is abandoned writes (tma.cuh StepError)
@@ -247,12 +265,13 @@ __device__ __forceinline__ void row_step_body(cplx<R> *__restrict__ wave, const 
     // tsel (optional): transmission set of each wave; set k of this slice starts k * tstride after trans
     const cplx<R> *trow = trans + (tsel ? (size_t)tsel[w] * tstride : (size_t)0) + (size_t)y * N;
     cplx<R> *sT = reinterpret_cast<cplx<R> *>(smraw + row_tstage_off<N, R>());
-    uint64_t *tbar = reinterpret_cast<uint64_t *>(smraw + row_tstage_off<N, R>() + sizeof(cplx<R>) * ROWS * N);
+    constexpr int TSR = row_ts_rows<N, R>();
+    uint64_t *tbar = reinterpret_cast<uint64_t *>(smraw + row_tstage_off<N, R>() + sizeof(cplx<R>) * TSR * N);
     if constexpr (TST) {
         if (threadIdx.x == 0 && threadIdx.y == 0) {
             mbar_init(tbar, 1);
             mbar_fence_init();
-            constexpr unsigned bytes = (unsigned)(sizeof(cplx<R>) * ROWS * N);
+            constexpr unsigned bytes = (unsigned)(sizeof(cplx<R>) * TSR * N);
             mbar_arrive_expect_tx(tbar, bytes);
             bulk_load(sT, trow, bytes, tbar);   // thread (0, 0)'s row is the block's first
         }
@@ -265,10 +284,11 @@ __device__ __forceinline__ void row_step_body(cplx<R> *__restrict__ wave, const 
     }
     __syncthreads();
     row_transform<R, N, +1>(v, sm, t, tw);
+    const bool staged = TST && (int)threadIdx.y < TSR;
     if constexpr (TST) {   // (an abandoned wait still lets the copy land before the block goes on)
-        if (!mbar_wait(tbar, 0, err, STEP_WAIT_FULL)) mbar_wait(tbar, 0, err, STEP_WAIT_DRAIN);
+        if (staged && !mbar_wait(tbar, 0, err, STEP_WAIT_FULL)) mbar_wait(tbar, 0, err, STEP_WAIT_DRAIN);
     }
-    const cplx<R> *tr = TST ? sT + threadIdx.y * N : trow;
+    const cplx<R> *tr = staged ? sT + threadIdx.y * N : trow;
 #pragma unroll
     for (int m = 0; m < P::E; m++) v[m] = cscale(cmul(v[m], tr[t + m * P::NT]), a);
     row_transform<R, N, -1>(v, sm, t, tw);
