@@ -1,9 +1,10 @@
 // passes_tmx.cuh — persistent column pass with one barrier domain per column pair (FP32, 2^k and 3·2^k plans,
 // and the 16-element plans at 1024 and 2048, whose results round differently from the 8-element plan's).
 //
-// Same arithmetic per element, in the same order, as k_col_step_pair / k_col_step_tma (column FFT of two
-// adjacent columns a thread, times the propagator inside its cut and the scale b, inverse column FFT), so
-// the results are bit-identical. What changes is who waits for whom:
+// With the size's own plan (Plan<N>): same arithmetic per element, in the same order, as k_col_step_pair /
+// k_col_step_tma (column FFT of two adjacent columns a thread, times the propagator inside its cut with the
+// scale b folded into its column factor, inverse column FFT), so the results are bit-identical. What changes
+// is who waits for whom:
 //   - the NT threads of one column pair are whole warps (thread t of pair p is thread p * NT + t), and each
 //     pair synchronises its FFT exchanges on its own named barrier, so a pair that waits on shared memory
 //     does not hold up the other pairs of the block (k_col_step_tma makes all 16 consumer warps meet at
@@ -19,6 +20,8 @@
 // logical row i at physical row g(i) = i ^ H((i >> 3) & 7) with the same swizzle: H the identity for the 2^k
 // plans; for the 3·2^k plans (radix-4 stages, a radix-2 stage, radix 12 last) H maps bits (1, 2, 4) to
 // (1, 6, 4), since their radix-4 writes at span 4 gather rows that the identity folds onto 4 bank groups.
+// The 16-element plans use g(i) = i ^ ((i >> 4) & 7) instead: their radix-16 first stage writes the rows of
+// 8 consecutive threads 16 apart.
 // Both layouts give every pair the same slots (each pair only ever touches its own), and every access pattern
 // of the plans' stages meets 8 distinct 16-byte bank groups per quarter warp (checked exhaustively on the host
 // for every grid and pair count). Both maps are linear over GF(2) in the bits of the row, and so are the
